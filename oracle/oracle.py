@@ -1,0 +1,209 @@
+"""ctypes wrapper of the CPU FP64 oracle (liboracle.so).
+
+TEST INFRASTRUCTURE ONLY.  Imported by tests/, __graft_entry__.smoke() and the
+cpu_baseline leg of bench.py -- never by the product package.  The oracle is a
+restatement of the reference's coupling step; see sg_oracle.h for the reference
+file:line each entry point follows.
+"""
+import ctypes
+import os
+import subprocess
+
+import numpy as np
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+_LIB = None
+
+_dp = ctypes.POINTER(ctypes.c_double)
+_ip = ctypes.POINTER(ctypes.c_int)
+
+
+def build():
+    """Compile liboracle.so (and oracle/_ref when the reference tree exists)."""
+    subprocess.run(["make", "-s", "-C", _HERE], check=True)
+
+
+def lib():
+    global _LIB
+    if _LIB is None:
+        path = os.path.join(_HERE, "liboracle.so")
+        if not os.path.exists(path):
+            build()
+        L = ctypes.CDLL(path)
+        i, d, l = ctypes.c_int, ctypes.c_double, ctypes.c_long
+        L.or_gaqd.argtypes = [i, _dp, _dp]
+        L.or_legendre.argtypes = [d, i, i, _dp, _dp, _dp]
+        L.or_legendre.restype = None
+        L.or_shagc.argtypes = [i, i, i, _dp, _dp, _dp]
+        L.or_shsgc.argtypes = [i, i, i, _dp, _dp, _dp]
+        L.or_trssph.argtypes = [i, i, i, _dp, i, i, _dp]
+        L.or_kernel.argtypes = [d]
+        L.or_kernel.restype = d
+        L.or_kerneltest.argtypes = []
+        L.or_kerneltest.restype = d
+        L.or_complagrforces.argtypes = [i, d, d, d, i] + [_dp] * 10
+        L.or_capsule_spectra.argtypes = [i, d, d, d] + [_dp] * 7
+        L.or_interp.argtypes = [i, i, i, d, d, d, i, _dp, _dp, _dp, l, _dp, _dp, _dp, _dp, _dp, _dp]
+        L.or_spread.argtypes = [i, i, i, d, d, d, i, l] + [_dp] * 10
+        L.or_update_pos.argtypes = [l, d, d] + [_dp] * 6
+        L.or_update_pos.restype = None
+        L.or_surf_vol.argtypes = [l] + [_dp] * 7 + [d, _dp]
+        L.or_surf_vol.restype = None
+        L.or_collisions.argtypes = [l, _dp, _dp, d, d, d, d, d, d, _dp]
+        L.or_collisions.restype = None
+        L.or_coupling_step.argtypes = ([i, i, i, d, d, d, i, _ip, _dp, d, d, i, i] + [_dp] * 20)
+        _LIB = L
+    return _LIB
+
+
+def _p(a):
+    assert a.dtype == np.float64 and a.flags.c_contiguous
+    return a.ctypes.data_as(_dp)
+
+
+def _f64(a):
+    return np.ascontiguousarray(a, dtype=np.float64)
+
+
+def gaqd(nlat):
+    th, w = np.zeros(nlat), np.zeros(nlat)
+    assert lib().or_gaqd(nlat, _p(th), _p(w)) == 0
+    return th, w
+
+
+def legendre(theta, mm, nn):
+    """P, dP/dtheta, d2P/dtheta2 as [m, n] arrays (SPHEREPACK normalisation)."""
+    P, D, D2 = (np.zeros((mm, nn)) for _ in range(3))
+    lib().or_legendre(float(theta), mm, nn, _p(P), _p(D), _p(D2))
+    return P, D, D2
+
+
+def trunc_l(nlat, nlon):
+    l = (nlon + 2) // 2 if nlon % 2 == 0 else (nlon + 1) // 2
+    return min(l, nlat)
+
+
+def shagc(g):
+    """Analysis of g[nf, nlat, nlon] (or [nlat, nlon]) -> a, b [nf, l, nlat]."""
+    g = _f64(g)
+    squeeze = g.ndim == 2
+    if squeeze:
+        g = g[None]
+    nf, nlat, nlon = g.shape
+    l = trunc_l(nlat, nlon)
+    a, b = np.zeros((nf, l, nlat)), np.zeros((nf, l, nlat))
+    assert lib().or_shagc(nlat, nlon, nf, _p(g), _p(a), _p(b)) == 0
+    return (a[0], b[0]) if squeeze else (a, b)
+
+
+def shsgc(a, b, nlon):
+    a, b = _f64(a), _f64(b)
+    squeeze = a.ndim == 2
+    if squeeze:
+        a, b = a[None], b[None]
+    nf, l, nlat = a.shape
+    assert l == trunc_l(nlat, nlon)
+    g = np.zeros((nf, nlat, nlon))
+    assert lib().or_shsgc(nlat, nlon, nf, _p(a), _p(b), _p(g)) == 0
+    return g[0] if squeeze else g
+
+
+def trssph(da, nlatb, nlonb):
+    da = _f64(da)
+    squeeze = da.ndim == 2
+    if squeeze:
+        da = da[None]
+    nf, nlata, nlona = da.shape
+    db = np.zeros((nf, nlatb, nlonb))
+    assert lib().or_trssph(nlata, nlona, nf, _p(da), nlatb, nlonb, _p(db)) == 0
+    return db[0] if squeeze else db
+
+
+def kernel(r):
+    return lib().or_kernel(float(r))
+
+
+def kerneltest():
+    return lib().or_kerneltest()
+
+
+def complagrforces(L, radius, x, y, z, gs=1.0, csk=1.0, faithful=False):
+    """One capsule: flat force-grid positions -> (f[3,nl], n[3,nl], area[nl])."""
+    nl = 8 * (L + 1) ** 2
+    x, y, z = _f64(x), _f64(y), _f64(z)
+    assert x.size == nl
+    out = [np.zeros(nl) for _ in range(7)]
+    rc = lib().or_complagrforces(L, radius, gs, csk, int(faithful), _p(x), _p(y), _p(z), *[_p(o) for o in out])
+    assert rc == 0, rc
+    return np.stack(out[0:3]), np.stack(out[3:6]), out[6]
+
+
+def capsule_spectra(L, radius, x, y, z, gs=1.0, csk=1.0):
+    """Shape and filtered-force SH coefficients (degree < L+1), [3, N, N] each (a, b)."""
+    N = L + 1
+    outs = [np.zeros((3, N, N)) for _ in range(4)]
+    rc = lib().or_capsule_spectra(L, radius, gs, csk, _p(_f64(x)), _p(_f64(y)), _p(_f64(z)), *[_p(o) for o in outs])
+    assert rc == 0
+    return outs
+
+
+def interp(grid, u, v, w, x, y, z, faithful=False):
+    itot, jtot, ktot, dx, dy, dz = grid
+    n = x.size
+    ul, vl, wl = np.zeros(n), np.zeros(n), np.zeros(n)
+    lib().or_interp(itot, jtot, ktot, dx, dy, dz, int(faithful), _p(_f64(u)), _p(_f64(v)), _p(_f64(w)), n,
+                    _p(_f64(x)), _p(_f64(y)), _p(_f64(z)), _p(ul), _p(vl), _p(wl))
+    return ul, vl, wl
+
+
+def spread(grid, x, y, z, fx, fy, fz, area, faithful=False):
+    itot, jtot, ktot, dx, dy, dz = grid
+    shape = (ktot + 2, jtot + 2, itot + 2)  # C view of Fortran (0:i1,0:j1,0:k1)
+    gx, gy, gz = np.zeros(shape), np.zeros(shape), np.zeros(shape)
+    lib().or_spread(itot, jtot, ktot, dx, dy, dz, int(faithful), x.size, _p(_f64(x)), _p(_f64(y)), _p(_f64(z)),
+                    _p(_f64(fx)), _p(_f64(fy)), _p(_f64(fz)), _p(_f64(area)), _p(gx), _p(gy), _p(gz))
+    return gx, gy, gz
+
+
+def update_pos(dt, lz, x, y, z, u, v, w):
+    x, y, z = _f64(x).copy(), _f64(y).copy(), _f64(z).copy()
+    lib().or_update_pos(x.size, dt, lz, _p(x), _p(y), _p(z), _p(_f64(u)), _p(_f64(v)), _p(_f64(w)))
+    return x, y, z
+
+
+def surf_vol(x, y, z, nx, ny, nz, area, exy1_prev=0.0):
+    out = np.zeros(7)
+    lib().or_surf_vol(x.size, *[_p(_f64(a)) for a in (x, y, z, nx, ny, nz, area)], float(exy1_prev), _p(out))
+    return out
+
+
+def coupling_step(grid, degree, radius, u, v, w, x, y, z, gs=1.0, csk=1.0, faithful=False, nthreads=1):
+    """Whole step over all capsules; returns dict of outputs and per-stage seconds."""
+    itot, jtot, ktot, dx, dy, dz = grid
+    degree = np.ascontiguousarray(degree, dtype=np.int32)
+    radius = _f64(radius)
+    n = x.size
+    shape = (ktot + 2, jtot + 2, itot + 2)
+    lag = [np.zeros(n) for _ in range(10)]
+    eul = [np.zeros(shape) for _ in range(3)]
+    t = np.zeros(3)
+    rc = lib().or_coupling_step(itot, jtot, ktot, dx, dy, dz, degree.size, degree.ctypes.data_as(_ip), _p(radius),
+                                gs, csk, int(faithful), int(nthreads), _p(_f64(u)), _p(_f64(v)), _p(_f64(w)),
+                                _p(_f64(x)), _p(_f64(y)), _p(_f64(z)), *[_p(a) for a in lag], *[_p(a) for a in eul],
+                                _p(t))
+    assert rc == 0
+    return dict(u=np.stack(lag[0:3]), f=np.stack(lag[3:6]), n=np.stack(lag[6:9]), area=lag[9],
+                fgrid=np.stack(eul), seconds=t)
+
+
+def ref_membmodel(law="skalak"):
+    """The reference's own membmodel.c, compiled into oracle/_ref (None if absent)."""
+    path = os.path.join(_HERE, "_ref", "libmembmodel_%s.so" % law)
+    if not os.path.exists(path):
+        return None
+    L = ctypes.CDLL(path)
+    L.calpwspi_deri_.argtypes = [_dp] * 10
+    L.calpwspi_deri_.restype = None
+    L.ref_set_hf_gscell.argtypes = [ctypes.c_double]
+    L.ref_set_hf_gscell.restype = None
+    return L
