@@ -1,0 +1,137 @@
+/*
+ * sg_coupling.h -- C ABI of the B200 fluid-structure coupling step.
+ *
+ * Drop-in boundary for the reference's coupling step (WhiteTshirtXI/Suguru,
+ * Fortran 90).  The reference calls, once per time step (main.f90:225-241):
+ *
+ *   call eulr2lagr        ! interp_spread.f90:12   Eulerian velocity -> ul,vl,wl
+ *   call complagrforces   ! forcing.f90:11         membrane force fxl.., normals xn.., area
+ *   call collisions       ! collisions.f90:10      (wall Morse term, optional)
+ *   call lagr2eulr        ! interp_spread.f90:510  fxl.. * area -> forcex,forcey,forcez
+ *   call Update_Pos       ! Update_Pos.f90:12      xfp += ul*dt, wall clamp
+ *   call surf_vol         ! surf_vol.f90:12        volume / deformation diagnostics
+ *
+ * None of those subroutines takes arguments; they act on module globals
+ * (common.f90:6-9,67-90).  The functions below take the same arrays as plain
+ * pointers, so a thin iso_c_binding shim keeps the Fortran
+ * names and packs ap(p)%xfp... into contiguous buffers.
+ *
+ * Conventions
+ *  - Eulerian arrays: Fortran (0:i1,0:j1,0:k1), x fastest, i1=itot+1 etc.
+ *    (common.f90:6); u at faces i*dx, v at j*dy, w at k*dz (MAC grid).
+ *  - Lagrangian arrays: capsules concatenated; capsule c of SH degree L owns
+ *    8(L+1)^2 points in the reference flat order cap=(i-1)*m_capf+j on the
+ *    2(L+1) x 4(L+1) Gauss force grid (forcing.f90:37-44).
+ *  - Precision SG_PREC_FP64: every array is double.  SG_PREC_MIXED: positions
+ *    X,Y,Z stay double; Eulerian fields and Lagrangian outputs are float.
+ *  - mem = SG_MEM_HOST: arrays are host memory, copied in and out per call;
+ *    SG_MEM_DEVICE: arrays are device pointers on cfg->device.
+ *  - Every function returns 0 on success or an SG_ERR_* code; sg_last_error
+ *    gives the text.  Errors are integer status codes in the spirit of
+ *    SPHEREPACK's ierror (shagc.f:221-231), never aborts.
+ *  - One host thread per context; calls are synchronous at return unless
+ *    cfg->async is set.
+ */
+#ifndef SG_COUPLING_H
+#define SG_COUPLING_H
+#include <stddef.h>
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define SG_OK 0
+#define SG_ERR_CONFIG 1   /* invalid configuration */
+#define SG_ERR_CUDA 2     /* CUDA runtime error */
+#define SG_ERR_TIMEOUT 3  /* a bounded device wait expired */
+#define SG_ERR_FALLBACK 4 /* surrogate fallback count above the allowed maximum */
+#define SG_ERR_ARG 5      /* bad argument (null pointer, size) */
+#define SG_ERR_STATE 6    /* call not valid in the current state */
+
+#define SG_PREC_FP64 0
+#define SG_PREC_MIXED 1
+#define SG_MEM_HOST 0
+#define SG_MEM_DEVICE 1
+
+typedef struct sg_ctx sg_ctx;
+
+typedef struct sg_config {
+  int itot, jtot, ktot;   /* interior cells imax, jmax, kmax (param.f90:18-21) */
+  double lx, ly, lz;      /* domain lengths (param.f90:23); periodic x,y, walls z */
+  int ncap;               /* number of capsules (np, param.f90:43) */
+  const int* degree;      /* [ncap] SH degree L per capsule, 2 <= L <= 31 */
+  const double* radius;   /* [ncap] reference-sphere radius (sph.f90:60-88) */
+  double gs;              /* surface shear modulus Gs (gscell, param.f90:88) */
+  double csk;             /* Skalak area-dilation constant C (CSK, param.f90:88) */
+  int precision;          /* SG_PREC_FP64 or SG_PREC_MIXED */
+  int surrogate;          /* 1: learned membrane force with plain fallback (mixed only) */
+  int mem;                /* SG_MEM_HOST or SG_MEM_DEVICE */
+  int device;             /* CUDA device ordinal */
+  int async;              /* 1: return without synchronising the context stream */
+  void* stream;           /* cudaStream_t to run on, or NULL for a private stream */
+} sg_config;
+
+/* Create / destroy a context.  All device memory is allocated here; the step
+ * calls below allocate nothing. */
+int sg_create(const sg_config* cfg, sg_ctx** out);
+void sg_destroy(sg_ctx* ctx);
+const char* sg_last_error(const sg_ctx* ctx);
+int sg_synchronize(sg_ctx* ctx);
+
+/* eulr2lagr (interp_spread.f90:12-475): U,V,W = J(X) [u,v,w]. */
+int sg_interp(sg_ctx* ctx, const void* u, const void* v, const void* w,
+              const double* X, const double* Y, const double* Z,
+              void* U, void* V, void* W);
+
+/* complagrforces (forcing.f90:11-114): membrane force, unit normals and
+ * area of every force point. */
+int sg_membrane_force(sg_ctx* ctx, const double* X, const double* Y, const double* Z,
+                      void* FX, void* FY, void* FZ, void* NX, void* NY, void* NZ, void* AREA);
+
+/* lagr2eulr (interp_spread.f90:510-922): fx,fy,fz = S(X)[F * AREA / dV],
+ * whole field written, periodic halos copied as updthalos does (bound.f90:141-190). */
+int sg_spread(sg_ctx* ctx, const double* X, const double* Y, const double* Z,
+              const void* FX, const void* FY, const void* FZ, const void* AREA,
+              void* fx, void* fy, void* fz);
+
+/* One coupling step in the reference order (main.f90:225-233): interpolation,
+ * membrane force, spreading; the points are binned once. */
+int sg_step(sg_ctx* ctx, const void* u, const void* v, const void* w,
+            const double* X, const double* Y, const double* Z,
+            void* U, void* V, void* W,
+            void* FX, void* FY, void* FZ, void* NX, void* NY, void* NZ, void* AREA,
+            void* fx, void* fy, void* fz);
+
+/* Update_Pos.f90:95-126: X += U*dt, then clamp z into [0, lz]. */
+int sg_update_pos(sg_ctx* ctx, double dt, double* X, double* Y, double* Z,
+                  const void* U, const void* V, const void* W);
+
+/* surf_vol.f90:12-131 per capsule, FP64: out[7*c + {0..6}] = volume, area,
+ * exy1, exy2, centroid x, y, z.  exy1_prev[c] is kept when no principal axis
+ * matches (as the reference keeps the global exy1); may be NULL. */
+int sg_surf_vol(sg_ctx* ctx, const double* X, const double* Y, const double* Z,
+                const void* NX, const void* NY, const void* NZ, const void* AREA,
+                const double* exy1_prev, double* out);
+
+/* Host-side tables (tests): Gauss colatitudes and SPHEREPACK-normalised
+ * Legendre functions with theta derivatives, [m*nn+n] layout. */
+int sg_gauss(int nlat, double* theta, double* weights);
+int sg_legendre(double theta, int mm, int nn, double* P, double* dP, double* d2P);
+
+/* Number of this library's kernels launched by the last step call. */
+int sg_last_launch_count(const sg_ctx* ctx);
+
+/* Stage timing with CUDA events on the context stream.  When enabled, each
+ * step call records events around its stages; sg_stage_times returns the last
+ * step's milliseconds for SG_STAGE_* (bin, interp, membrane, spread). */
+#define SG_STAGE_BIN 0
+#define SG_STAGE_INTERP 1
+#define SG_STAGE_MEMBRANE 2
+#define SG_STAGE_SPREAD 3
+#define SG_NSTAGE 4
+int sg_set_profiling(sg_ctx* ctx, int on);
+int sg_stage_times(sg_ctx* ctx, float* ms, int n);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

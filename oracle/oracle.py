@@ -51,6 +51,8 @@ def lib():
         L.or_surf_vol.restype = None
         L.or_collisions.argtypes = [l, _dp, _dp, d, d, d, d, d, d, _dp]
         L.or_collisions.restype = None
+        L.or_skalak.argtypes = [d, d, _dp, _dp, d, d, _dp]
+        L.or_skalak.restype = None
         L.or_coupling_step.argtypes = ([i, i, i, d, d, d, i, _ip, _dp, d, d, i, i] + [_dp] * 20)
         _LIB = L
     return _LIB
@@ -194,6 +196,12 @@ def coupling_step(grid, degree, radius, u, v, w, x, y, z, gs=1.0, csk=1.0, faith
     assert rc == 0
     return dict(u=np.stack(lag[0:3]), f=np.stack(lag[3:6]), n=np.stack(lag[6:9]), area=lag[9],
                 fgrid=np.stack(eul), seconds=t)
+
+
+def skalak(I1, I2, I1de, I2de, gs=1.0, csk=1.0):
+    out = np.zeros(6)
+    lib().or_skalak(float(I1), float(I2), _p(_f64(I1de)), _p(_f64(I2de)), gs, csk, _p(out))
+    return out
 
 
 def ref_membmodel(law="skalak"):

@@ -31,7 +31,7 @@ const double kPi = 3.14159265358979323846264338327950288;
 // ---------------------------------------------------------------- gaqd ------
 // gaqd.f:45-180: Gauss points in colatitude, north to south, and weights.
 // Restated with Newton iterations on P_n(cos theta) in theta.
-void pn_eval(int n, double x, double* pn, double* pnm1) {
+[[maybe_unused]] void pn_eval(int n, double x, double* pn, double* pnm1) {
   double p0 = 1.0, p1 = x;
   if (n == 0) { *pn = 1.0; *pnm1 = 0.0; return; }
   for (int k = 2; k <= n; ++k) {
@@ -43,6 +43,23 @@ void pn_eval(int n, double x, double* pn, double* pnm1) {
   *pnm1 = p0;
 }
 
+// P_n(cos t) = sum_k a_k a_{n-k} cos((n-2k) t), a_k = binom(2k,k)/4^k, and its
+// t-derivative: evaluated in t, this keeps full relative accuracy near the
+// poles where x = cos t has lost digits (gaqd.f works in theta for the same reason).
+void pn_theta(int n, double t, double* p, double* dp) {
+  std::vector<double> a(n + 1);
+  a[0] = 1.0;
+  for (int k = 1; k <= n; ++k) a[k] = a[k - 1] * (2.0 * k - 1.0) / (2.0 * k);
+  double s = 0.0, d = 0.0;
+  for (int k = 0; k <= n; ++k) {
+    const double c = a[k] * a[n - k], q = (double)(n - 2 * k);
+    s += c * std::cos(q * t);
+    d -= c * q * std::sin(q * t);
+  }
+  *p = s;
+  *dp = d;
+}
+
 void gauss(int n, double* th, double* w) {
   int half = (n + 1) / 2;
   for (int k = 1; k <= half; ++k) {
@@ -51,18 +68,16 @@ void gauss(int n, double* th, double* w) {
       t = 0.5 * kPi;
     } else {
       for (int it = 0; it < 100; ++it) {
-        double x = std::cos(t), s = std::sin(t), pn, pm;
-        pn_eval(n, x, &pn, &pm);
-        // d/dtheta P_n(cos t) = n (x P_n - P_{n-1}) / sin t
-        double dp = n * (x * pn - pm) / s;
+        double pn, dp;
+        pn_theta(n, t, &pn, &dp);
         double dt = -pn / dp;
         t += dt;
         if (std::fabs(dt) < 1e-17) break;
       }
     }
-    double x = std::cos(t), s = std::sin(t), pn, pm;
-    pn_eval(n, x, &pn, &pm);
-    double ww = 2.0 * s * s / ((double)n * n * pm * pm);
+    double pn, dp;
+    pn_theta(n, t, &pn, &dp);
+    double ww = 2.0 / (dp * dp);  // w = 2 / ((1-x^2) P_n'(x)^2) = 2 / (dP_n/dt)^2
     th[k - 1] = t;
     w[k - 1] = ww;
     th[n - k] = kPi - t;
@@ -627,11 +642,28 @@ int capsule_force(int L, double R, double gs, double csk, bool faithful,
   const Capsule& C = *Cp;
   const int N = C.N, nO = C.nO, mO = C.mO, nD = C.nD, mD = C.mD;
   const size_t nF = (size_t)nD * mD, nS = (size_t)nO * mO;
+  // The geometry is translation invariant.  Unless `faithful`, the capsule's
+  // mean position is subtracted first: a constant offset (e.g. a capsule at
+  // (2,1,1) of radius 0.25) otherwise leaks roundoff of order eps*|offset|
+  // into every coefficient, which the second-derivative and 1/sin^3 terms
+  // amplify to ~2e-9 absolute force on an undeformed sphere.
+  std::vector<double> xc(3 * nF);
+  {
+    double mx = 0, my = 0, mz = 0;
+    for (size_t p = 0; p < nF; ++p) { mx += xfp[p]; my += yfp[p]; mz += zfp[p]; }
+    mx /= (double)nF; my /= (double)nF; mz /= (double)nF;
+    if (faithful) mx = my = mz = 0.0;
+    for (size_t p = 0; p < nF; ++p) {
+      xc[p] = xfp[p] - mx;
+      xc[nF + p] = yfp[p] - my;
+      xc[2 * nF + p] = zfp[p] - mz;
+    }
+  }
   // (1) TRSSPH force grid -> SH grid (forcing.f90:48-55)
   std::vector<double> xs(3 * nS);
-  trssph1(nD, mD, xfp, nO, mO, &xs[0], faithful);
-  trssph1(nD, mD, yfp, nO, mO, &xs[nS], faithful);
-  trssph1(nD, mD, zfp, nO, mO, &xs[2 * nS], faithful);
+  trssph1(nD, mD, &xc[0], nO, mO, &xs[0], faithful);
+  trssph1(nD, mD, &xc[nF], nO, mO, &xs[nS], faithful);
+  trssph1(nD, mD, &xc[2 * nF], nO, mO, &xs[2 * nS], faithful);
   // (2) cal_3dcrd_spectral_coeff (sph1.f90:29-79, re-initialised per call)
   auto pO = get_plan(nO, mO, faithful);
   std::vector<double> a((size_t)3 * N * N), b((size_t)3 * N * N);
@@ -1051,6 +1083,17 @@ void or_collisions(long nl, const double* zp, const double* area, double dx, dou
       }
     fzl[i] += fc;
   }
+}
+
+void or_skalak(double I1, double I2, const double* I1de, const double* I2de, double gs, double csk, double* out) {
+  // membmodel.c:81-99 restated: out = W1, W2, dW1[2], dW2[2]
+  const double hf = 0.5 * gs;
+  out[0] = hf * (1 + I1);
+  out[1] = hf * (csk * I2 - 1);
+  out[2] = hf * I1de[0];
+  out[3] = hf * I1de[1];
+  out[4] = csk * hf * I2de[0];
+  out[5] = csk * hf * I2de[1];
 }
 
 int or_coupling_step(int itot, int jtot, int ktot, double dx, double dy, double dz, int ncap, const int* degree,

@@ -89,6 +89,9 @@ void or_surf_vol(long nl, const double* xp, const double* yp, const double* zp,
 void or_collisions(long nl, const double* zp, const double* area, double dx, double dy,
                    double col, double betacol, double rep, double rad0, double* fzl);
 
+/* membmodel.c:81-99 (Skalak) restated: out = W1, W2, dW1/dxi[2], dW2/dxi[2]. */
+void or_skalak(double I1, double I2, const double* I1de, const double* I2de, double gs, double csk, double* out);
+
 /* Whole step over ncap capsules (interp, forces, spread) with OpenMP over
  * capsules when nthreads>1; returns seconds spent per stage in t[3]. */
 int or_coupling_step(int itot, int jtot, int ktot, double dx, double dy, double dz,

@@ -1,0 +1,240 @@
+"""Host-side mirror of the reference's coupling-step subroutines over the C ABI.
+
+The reference (Fortran, WhiteTshirtXI/Suguru) calls per time step
+(main.f90:225-241) ``eulr2lagr``, ``complagrforces``, ``lagr2eulr``,
+``Update_Pos`` and ``surf_vol`` on module globals.  ``CouplingStep`` keeps
+those names; each method calls the matching ``sg_*`` entry point of
+``libsuguru_b200.so`` (include/sg_coupling.h).
+
+Arrays are either numpy host arrays (``mem="host"``: the library copies them
+in and out) or torch CUDA tensors (``mem="device"``).  Eulerian arrays have the
+Fortran (0:i1, 0:j1, 0:k1) layout, i.e. numpy shape (ktot+2, jtot+2, itot+2)
+C-contiguous; Lagrangian arrays are flat, capsules concatenated, each in the
+reference order cap = i*m_capf + j.
+
+There is no CPU fallback: constructing a ``CouplingStep`` without the built
+library or without a CUDA device raises.
+"""
+import ctypes
+import os
+
+import numpy as np
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+_LIBPATH = os.path.join(_HERE, "libsuguru_b200.so")
+_LIB = None
+
+SG_PREC_FP64, SG_PREC_MIXED = 0, 1
+SG_MEM_HOST, SG_MEM_DEVICE = 0, 1
+ERRORS = {0: "SG_OK", 1: "SG_ERR_CONFIG", 2: "SG_ERR_CUDA", 3: "SG_ERR_TIMEOUT", 4: "SG_ERR_FALLBACK",
+          5: "SG_ERR_ARG", 6: "SG_ERR_STATE"}
+
+# every symbol declared in include/sg_coupling.h
+EXPORTS = ["sg_create", "sg_destroy", "sg_last_error", "sg_synchronize", "sg_interp", "sg_membrane_force",
+           "sg_spread", "sg_step", "sg_update_pos", "sg_surf_vol", "sg_gauss", "sg_legendre",
+           "sg_last_launch_count", "sg_set_profiling", "sg_stage_times"]
+STAGES = ("bin", "interp", "membrane", "spread")
+
+
+class SgError(RuntimeError):
+    def __init__(self, code, msg):
+        super().__init__("%s: %s" % (ERRORS.get(code, code), msg))
+        self.code = code
+
+
+class sg_config(ctypes.Structure):
+    _fields_ = [("itot", ctypes.c_int), ("jtot", ctypes.c_int), ("ktot", ctypes.c_int),
+                ("lx", ctypes.c_double), ("ly", ctypes.c_double), ("lz", ctypes.c_double),
+                ("ncap", ctypes.c_int), ("degree", ctypes.POINTER(ctypes.c_int)),
+                ("radius", ctypes.POINTER(ctypes.c_double)), ("gs", ctypes.c_double), ("csk", ctypes.c_double),
+                ("precision", ctypes.c_int), ("surrogate", ctypes.c_int), ("mem", ctypes.c_int),
+                ("device", ctypes.c_int), ("async_", ctypes.c_int), ("stream", ctypes.c_void_p)]
+
+
+def library_path():
+    return _LIBPATH
+
+
+def lib():
+    """Load libsuguru_b200.so (raises if it has not been built)."""
+    global _LIB
+    if _LIB is not None:
+        return _LIB
+    if not os.path.exists(_LIBPATH):
+        raise RuntimeError("libsuguru_b200.so is not built; run suguru_b200/build.py (no CPU fallback exists)")
+    L = ctypes.CDLL(_LIBPATH)
+    vp, dp = ctypes.c_void_p, ctypes.POINTER(ctypes.c_double)
+    L.sg_create.argtypes = [ctypes.POINTER(sg_config), ctypes.POINTER(ctypes.c_void_p)]
+    L.sg_destroy.argtypes = [vp]
+    L.sg_destroy.restype = None
+    L.sg_last_error.argtypes = [vp]
+    L.sg_last_error.restype = ctypes.c_char_p
+    L.sg_synchronize.argtypes = [vp]
+    L.sg_interp.argtypes = [vp] * 10
+    L.sg_membrane_force.argtypes = [vp] * 11
+    L.sg_spread.argtypes = [vp] * 11
+    L.sg_step.argtypes = [vp] * 20
+    L.sg_update_pos.argtypes = [vp, ctypes.c_double] + [vp] * 6
+    L.sg_surf_vol.argtypes = [vp] * 10
+    L.sg_gauss.argtypes = [ctypes.c_int, dp, dp]
+    L.sg_legendre.argtypes = [ctypes.c_double, ctypes.c_int, ctypes.c_int, dp, dp, dp]
+    L.sg_last_launch_count.argtypes = [vp]
+    L.sg_set_profiling.argtypes = [vp, ctypes.c_int]
+    L.sg_stage_times.argtypes = [vp, ctypes.POINTER(ctypes.c_float), ctypes.c_int]
+    _LIB = L
+    return L
+
+
+def gauss(nlat):
+    th, w = np.zeros(nlat), np.zeros(nlat)
+    dp = ctypes.POINTER(ctypes.c_double)
+    rc = lib().sg_gauss(nlat, th.ctypes.data_as(dp), w.ctypes.data_as(dp))
+    if rc:
+        raise SgError(rc, "sg_gauss")
+    return th, w
+
+
+def legendre(theta, mm, nn):
+    P, D, D2 = (np.zeros((mm, nn)) for _ in range(3))
+    dp = ctypes.POINTER(ctypes.c_double)
+    rc = lib().sg_legendre(float(theta), mm, nn, P.ctypes.data_as(dp), D.ctypes.data_as(dp), D2.ctypes.data_as(dp))
+    if rc:
+        raise SgError(rc, "sg_legendre")
+    return P, D, D2
+
+
+def _ptr(a):
+    if a is None:
+        return None
+    if hasattr(a, "data_ptr"):  # torch tensor
+        assert a.is_contiguous()
+        return ctypes.c_void_p(a.data_ptr())
+    assert a.flags.c_contiguous
+    return ctypes.c_void_p(a.ctypes.data)
+
+
+class CouplingStep:
+    """One coupling-step context (sg_create) over a fixed set of capsules."""
+
+    def __init__(self, grid, degree, radius, gs=1.0, csk=1.0, precision="fp64", mem="host", device=0,
+                 surrogate=False, stream=None, async_=False):
+        self.grid = tuple(grid)
+        itot, jtot, ktot, dx, dy, dz = self.grid
+        self.degree = np.ascontiguousarray(degree, dtype=np.int32)
+        self.radius = np.ascontiguousarray(radius, dtype=np.float64)
+        self.precision = precision
+        self.mem = mem
+        self.rdtype = np.float64 if precision == "fp64" else np.float32
+        self.npts = int(sum(8 * (int(L) + 1) ** 2 for L in self.degree))
+        self.field_shape = (ktot + 2, jtot + 2, itot + 2)
+        cfg = sg_config()
+        cfg.itot, cfg.jtot, cfg.ktot = itot, jtot, ktot
+        cfg.lx, cfg.ly, cfg.lz = itot * dx, jtot * dy, ktot * dz
+        cfg.ncap = int(self.degree.size)
+        cfg.degree = self.degree.ctypes.data_as(ctypes.POINTER(ctypes.c_int))
+        cfg.radius = self.radius.ctypes.data_as(ctypes.POINTER(ctypes.c_double))
+        cfg.gs, cfg.csk = float(gs), float(csk)
+        cfg.precision = SG_PREC_FP64 if precision == "fp64" else SG_PREC_MIXED
+        cfg.surrogate = int(bool(surrogate))
+        cfg.mem = SG_MEM_HOST if mem == "host" else SG_MEM_DEVICE
+        cfg.device = int(device)
+        cfg.async_ = int(bool(async_))
+        cfg.stream = stream
+        self._cfg = cfg
+        h = ctypes.c_void_p()
+        rc = lib().sg_create(ctypes.byref(cfg), ctypes.byref(h))
+        self._h = h
+        if rc:
+            msg = lib().sg_last_error(h).decode() if h else ""
+            if h:
+                lib().sg_destroy(h)
+            self._h = None
+            raise SgError(rc, "sg_create: " + msg)
+
+    def close(self):
+        if getattr(self, "_h", None):
+            lib().sg_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def _check(self, rc, where):
+        if rc:
+            raise SgError(rc, "%s: %s" % (where, lib().sg_last_error(self._h).decode()))
+
+    # ---- allocation helpers (host numpy or device torch)
+    def _lag(self, n=1):
+        if self.mem == "host":
+            return [np.zeros(self.npts, self.rdtype) for _ in range(n)]
+        import torch
+        dt = torch.float64 if self.rdtype == np.float64 else torch.float32
+        return [torch.zeros(self.npts, dtype=dt, device="cuda") for _ in range(n)]
+
+    def _eul(self, n=1):
+        if self.mem == "host":
+            return [np.zeros(self.field_shape, self.rdtype) for _ in range(n)]
+        import torch
+        dt = torch.float64 if self.rdtype == np.float64 else torch.float32
+        return [torch.empty(self.field_shape, dtype=dt, device="cuda") for _ in range(n)]
+
+    # ---- the reference's subroutines
+    def eulr2lagr(self, u, v, w, X, Y, Z, out=None):
+        """interp_spread.f90:12 -- velocity at the force points."""
+        U, V, W = out if out is not None else self._lag(3)
+        self._check(lib().sg_interp(self._h, *map(_ptr, (u, v, w, X, Y, Z, U, V, W))), "sg_interp")
+        return U, V, W
+
+    def complagrforces(self, X, Y, Z, out=None):
+        """forcing.f90:11 -- membrane force, unit normals and area."""
+        o = out if out is not None else self._lag(7)
+        self._check(lib().sg_membrane_force(self._h, *map(_ptr, (X, Y, Z, *o))), "sg_membrane_force")
+        return (o[0], o[1], o[2]), (o[3], o[4], o[5]), o[6]
+
+    def lagr2eulr(self, X, Y, Z, FX, FY, FZ, AREA, out=None):
+        """interp_spread.f90:510 -- spread force * area onto the Eulerian grid."""
+        fx, fy, fz = out if out is not None else self._eul(3)
+        self._check(lib().sg_spread(self._h, *map(_ptr, (X, Y, Z, FX, FY, FZ, AREA, fx, fy, fz))), "sg_spread")
+        return fx, fy, fz
+
+    def step(self, u, v, w, X, Y, Z, lag_out=None, eul_out=None):
+        """eulr2lagr + complagrforces + lagr2eulr with one binning of the points."""
+        L = lag_out if lag_out is not None else self._lag(10)
+        E = eul_out if eul_out is not None else self._eul(3)
+        self._check(lib().sg_step(self._h, *map(_ptr, (u, v, w, X, Y, Z, *L, *E))), "sg_step")
+        return dict(u=L[0:3], f=L[3:6], n=L[6:9], area=L[9], fgrid=E)
+
+    def update_pos(self, dt, X, Y, Z, U, V, W):
+        """Update_Pos.f90:95-126 -- in place on X, Y, Z."""
+        self._check(lib().sg_update_pos(self._h, ctypes.c_double(dt), *map(_ptr, (X, Y, Z, U, V, W))),
+                    "sg_update_pos")
+
+    def surf_vol(self, X, Y, Z, NX, NY, NZ, AREA, exy1_prev=None):
+        """surf_vol.f90:12 -- [ncap, 7]: volume, area, exy1, exy2, centroid."""
+        ncap = self.degree.size
+        if self.mem == "host":
+            out = np.zeros((ncap, 7))
+        else:
+            import torch
+            out = torch.zeros((ncap, 7), dtype=torch.float64, device="cuda")
+        self._check(lib().sg_surf_vol(self._h, *map(_ptr, (X, Y, Z, NX, NY, NZ, AREA, exy1_prev, out))),
+                    "sg_surf_vol")
+        return out
+
+    def synchronize(self):
+        self._check(lib().sg_synchronize(self._h), "sg_synchronize")
+
+    def last_launch_count(self):
+        return lib().sg_last_launch_count(self._h)
+
+    def set_profiling(self, on=True):
+        self._check(lib().sg_set_profiling(self._h, int(bool(on))), "sg_set_profiling")
+
+    def stage_times(self):
+        """Milliseconds of the last step's stages (CUDA events on the context stream)."""
+        ms = (ctypes.c_float * len(STAGES))()
+        self._check(lib().sg_stage_times(self._h, ms, len(STAGES)), "sg_stage_times")
+        return dict(zip(STAGES, list(ms)))

@@ -1,0 +1,58 @@
+// sg_common.cuh -- shared device helpers for the B200 coupling-step library.
+#pragma once
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#define SG_HD __host__ __device__ __forceinline__
+
+namespace sg {
+
+// Roma-Peskin 3-point regularised delta, multiplied by the grid spacing
+// (kernel.f90:7-25).  Same expression shape as the reference.
+template <class T>
+SG_HD T delta3(T r) {
+  T ar = r < T(0) ? -r : r;
+  if (ar > T(1.5)) return T(0);
+  if (ar > T(0.5))
+    return (T(1) / T(6)) * (T(5) - T(3) * ar - sqrt(-T(3) * ((T(1) - ar) * (T(1) - ar)) + T(1)));
+  return (T(1) / T(3)) * (T(1) + sqrt(-T(3) * (r * r) + T(1)));
+}
+
+SG_HD int wrap1(int i, int n) {  // periodic storage index in [1, n]
+  int r = (i - 1) % n;
+  if (r < 0) r += n;
+  return r + 1;
+}
+
+SG_HD long long fidx(int i, int j, int k, int ldi, int ldj) {
+  return (long long)i + (long long)ldi * ((long long)j + (long long)ldj * (long long)k);
+}
+
+template <class T>
+struct V3 {
+  T x, y, z;
+};
+
+template <class T>
+SG_HD void cross3(const T* u, const T* v, T* w) {
+  w[0] = u[1] * v[2] - u[2] * v[1];
+  w[1] = u[2] * v[0] - u[0] * v[2];
+  w[2] = u[0] * v[1] - u[1] * v[0];
+}
+template <class T>
+SG_HD T dot3(const T* u, const T* v) {
+  return u[0] * v[0] + u[1] * v[1] + u[2] * v[2];
+}
+
+#if defined(__CUDACC__)
+// Bounded spin on a global flag; returns false on timeout (never traps).
+__device__ __forceinline__ bool spin_until_ge(volatile int* flag, int target, long long max_iter) {
+  for (long long it = 0; it < max_iter; ++it) {
+    if (*flag >= target) return true;
+    __nanosleep(64);
+  }
+  return false;
+}
+#endif
+
+}  // namespace sg

@@ -1,0 +1,701 @@
+// sg_context.cu -- the C ABI (include/sg_coupling.h): context set-up, device
+// memory, per-degree tables, work lists, and the step pipeline.
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <map>
+#include <string>
+#include <vector>
+
+#include "sg_coupling.h"
+#include "sg_kernels.h"
+
+using namespace sg;
+
+namespace {
+const double kPi = 3.14159265358979323846264338327950288;
+
+struct Group {
+  int L = 0, N = 0, nD = 0, mD = 0, nO = 0, mO = 0;
+  std::vector<int> caps;
+  DegreeTables tab;
+  SpecBuffers buf{};
+};
+}  // namespace
+
+struct sg_ctx {
+  sg_config cfg{};
+  std::vector<int> degree;
+  std::vector<double> radius;
+  int mixed = 0;
+  size_t esz = 8;
+  IBGrid grid{};
+  IBWork ibw{};
+  long npts = 0;
+  long long nfield = 0;
+  std::vector<long long> off;
+  std::vector<Group> groups;
+  CapInfo* d_caps = nullptr;
+  GroupDev* d_groups = nullptr;
+  double* d_cen = nullptr;
+  RowWork* d_wpos = nullptr;
+  RowWork* d_wmem = nullptr;
+  RowWork* d_wsh = nullptr;
+  RowWork* d_wfin = nullptr;
+  int nwpos = 0, nwmem = 0, nwsh = 0, nwfin = 0;
+  LegProblem* d_probs = nullptr;
+  LegWork* d_lw[6] = {};
+  int nlw[6] = {};
+  int maxJ[6] = {}, maxK[6] = {};
+  int nmax = 0;
+  // host-mode staging
+  void* s_u = nullptr;
+  void* s_v = nullptr;
+  void* s_w = nullptr;
+  double* s_X = nullptr;
+  double* s_Y = nullptr;
+  double* s_Z = nullptr;
+  void* s_lag[10] = {};
+  void* s_f[3] = {};
+  double* s_out = nullptr;
+  double* s_exy = nullptr;
+  cudaStream_t st = nullptr;
+  bool own_stream = false;
+  std::vector<void*> allocs;
+  std::string err;
+  int launches = 0;
+  bool profiling = false;
+  cudaEvent_t ev[SG_NSTAGE + 1] = {};
+  bool ev_used[SG_NSTAGE] = {};
+};
+
+namespace {
+
+int fail(sg_ctx* c, int code, const std::string& msg) {
+  if (c) c->err = msg;
+  return code;
+}
+
+int cuda_fail(sg_ctx* c, cudaError_t e, const char* where) {
+  return fail(c, SG_ERR_CUDA, std::string(where) + ": " + cudaGetErrorString(e));
+}
+
+#define SG_TRY(expr, where)                       \
+  do {                                            \
+    cudaError_t _e = (expr);                      \
+    if (_e != cudaSuccess) return cuda_fail(c, _e, where); \
+  } while (0)
+
+template <class P>
+cudaError_t dalloc(sg_ctx* c, P*& p, size_t bytes) {
+  void* q = nullptr;
+  cudaError_t e = cudaMalloc(&q, bytes ? bytes : 16);
+  if (e == cudaSuccess) {
+    c->allocs.push_back(q);
+    p = (P*)q;
+  }
+  return e;
+}
+
+template <class V>
+cudaError_t upload(sg_ctx* c, void*& dst, const std::vector<V>& v) {
+  cudaError_t e = dalloc(c, dst, sizeof(V) * v.size());
+  if (e != cudaSuccess) return e;
+  return cudaMemcpy(dst, v.data(), sizeof(V) * v.size(), cudaMemcpyHostToDevice);
+}
+
+template <class V>
+cudaError_t upload2(sg_ctx* c, void* (&dst)[2], const std::vector<double>& v) {
+  (void)sizeof(V);
+  cudaError_t e = upload(c, dst[0], v);
+  if (e != cudaSuccess) return e;
+  std::vector<float> f(v.begin(), v.end());
+  return upload(c, dst[1], f);
+}
+
+// Per-degree FP64 tables -> device (double and float copies).
+cudaError_t build_tables(sg_ctx* c, Group& g) {
+  const int N = g.N, nD = g.nD, mD = g.mD, nO = g.nO, mO = g.mO;
+  std::vector<double> thD(nD), wD(nD), thO(nO), wO(nO);
+  host_gauss(nD, thD.data(), wD.data());
+  host_gauss(nO, thO.data(), wO.data());
+  std::vector<double> P((size_t)N * N), dP((size_t)N * N), d2P((size_t)N * N);
+  std::vector<double> synD((size_t)N * 3 * nD * N, 0.0), anaD((size_t)N * N * nD, 0.0);
+  std::vector<double> synO((size_t)N * 2 * nO * N, 0.0), anaO((size_t)N * N * nO, 0.0);
+  for (int i = 0; i < nD; ++i) {
+    host_legendre(thD[i], N, N, P.data(), dP.data(), d2P.data());
+    for (int m = 0; m < N; ++m) {
+      const double h = (m == 0) ? 0.5 : 1.0;  // sph3.f90:69-71, shsgc m=0 half weight
+      for (int n = 0; n < N; ++n) {
+        const double p = P[(size_t)m * N + n], d = dP[(size_t)m * N + n], e = d2P[(size_t)m * N + n];
+        synD[((size_t)m * 3 * nD + 0 * nD + i) * N + n] = h * p;
+        synD[((size_t)m * 3 * nD + 1 * nD + i) * N + n] = h * d;
+        synD[((size_t)m * 3 * nD + 2 * nD + i) * N + n] = h * e;
+        anaD[((size_t)m * N + n) * nD + i] = wD[i] * p;
+      }
+    }
+  }
+  for (int i = 0; i < nO; ++i) {
+    host_legendre(thO[i], N, N, P.data(), dP.data(), nullptr);
+    for (int m = 0; m < N; ++m) {
+      const double h = (m == 0) ? 0.5 : 1.0;
+      for (int n = 0; n < N; ++n) {
+        synO[((size_t)m * 2 * nO + 0 * nO + i) * N + n] = h * P[(size_t)m * N + n];
+        synO[((size_t)m * 2 * nO + 1 * nO + i) * N + n] = h * dP[(size_t)m * N + n];
+        anaO[((size_t)m * N + n) * nO + i] = wO[i] * P[(size_t)m * N + n];
+      }
+    }
+  }
+  std::vector<double> latD((size_t)nD * 4), latO((size_t)nO * 4);
+  for (int i = 0; i < nD; ++i) {
+    latD[4 * i] = std::sin(thD[i]);
+    latD[4 * i + 1] = std::cos(thD[i]);
+    latD[4 * i + 2] = wD[i] / std::sin(thD[i]) * (2.0 * kPi / mD);  // wgtdsinf, sph.f90:130
+    latD[4 * i + 3] = thD[i];
+  }
+  for (int i = 0; i < nO; ++i) {
+    latO[4 * i] = std::sin(thO[i]);
+    latO[4 * i + 1] = std::cos(thO[i]);
+    latO[4 * i + 2] = wO[i] / std::sin(thO[i]) * (2.0 * kPi / mO);
+    latO[4 * i + 3] = thO[i];
+  }
+  auto trig = [&](int nlon) {
+    std::vector<double> t((size_t)2 * N * nlon);
+    for (int m = 0; m < N; ++m)
+      for (int j = 0; j < nlon; ++j) {
+        const double a = 2.0 * kPi * (double)(((long long)m * j) % nlon) / nlon;
+        t[(size_t)m * nlon + j] = std::cos(a);
+        t[(size_t)N * nlon + (size_t)m * nlon + j] = std::sin(a);
+      }
+    return t;
+  };
+  cudaError_t e;
+  if ((e = upload2<double>(c, g.tab.syn_D, synD)) != cudaSuccess) return e;
+  if ((e = upload2<double>(c, g.tab.ana_D, anaD)) != cudaSuccess) return e;
+  if ((e = upload2<double>(c, g.tab.syn_O, synO)) != cudaSuccess) return e;
+  if ((e = upload2<double>(c, g.tab.ana_O, anaO)) != cudaSuccess) return e;
+  if ((e = upload2<double>(c, g.tab.latD, latD)) != cudaSuccess) return e;
+  if ((e = upload2<double>(c, g.tab.latO, latO)) != cudaSuccess) return e;
+  if ((e = upload2<double>(c, g.tab.trigD, trig(mD))) != cudaSuccess) return e;
+  if ((e = upload2<double>(c, g.tab.trigO, trig(mO))) != cudaSuccess) return e;
+  return cudaSuccess;
+}
+
+void add_problem(std::vector<LegProblem>& P, std::vector<LegWork>& W, const LegProblem& p, int& maxJ, int& maxK) {
+  const int id = (int)P.size();
+  P.push_back(p);
+  for (int m = 0; m < p.M; ++m)
+    for (int q0 = 0; q0 < p.Q; q0 += 32) W.push_back(LegWork{id, m, q0});
+  maxJ = std::max(maxJ, p.J);
+  maxK = std::max(maxK, p.K);
+}
+
+LegProblem prob(const void* A, long long sAc, long long sAr, long long sAm, const void* B, long long sBm, void* D,
+                long long sDc, long long sDr, long long sDm, int rpc, int ncap, int M, int J, int K, int tri,
+                int group, int kind) {
+  LegProblem p{};
+  p.A = A; p.sAc = sAc; p.sAr = sAr; p.sAm = sAm;
+  p.B = B; p.sBm = sBm;
+  p.D = D; p.sDc = sDc; p.sDr = sDr; p.sDm = sDm;
+  p.rpc = rpc; p.Q = rpc * ncap; p.M = M; p.J = J; p.K = K;
+  p.tri = tri; p.group = group; p.kind = kind;
+  return p;
+}
+
+int setup(sg_ctx* c) {
+  const sg_config& cfg = c->cfg;
+  c->mixed = cfg.precision == SG_PREC_MIXED;
+  c->esz = c->mixed ? 4 : 8;
+  const size_t E = c->esz;
+  const int pi = c->mixed ? 1 : 0;
+  SG_TRY(cudaSetDevice(cfg.device), "cudaSetDevice");
+  if (cfg.stream) {
+    c->st = (cudaStream_t)cfg.stream;
+  } else {
+    SG_TRY(cudaStreamCreateWithFlags(&c->st, cudaStreamNonBlocking), "cudaStreamCreate");
+    c->own_stream = true;
+  }
+  if (!make_ib_grid(cfg.itot, cfg.jtot, cfg.ktot, cfg.lx, cfg.ly, cfg.lz, c->grid))
+    return fail(c, SG_ERR_CONFIG, "grid too small: need itot, jtot >= 8");
+  const IBGrid& g = c->grid;
+  c->nfield = (long long)g.ldi * g.ldj * g.ldk;
+  // capsules, offsets, degree groups
+  const int ncap = cfg.ncap;
+  c->off.assign(ncap + 1, 0);
+  std::map<int, int> gid;
+  for (int k = 0; k < ncap; ++k) {
+    const int L = c->degree[k];
+    c->off[k + 1] = c->off[k] + 8LL * (L + 1) * (L + 1);
+    if (!gid.count(L)) {
+      gid[L] = (int)c->groups.size();
+      Group gr;
+      gr.L = L; gr.N = L + 1; gr.nD = 2 * (L + 1); gr.mD = 4 * (L + 1); gr.nO = L + 1; gr.mO = 2 * (L + 1);
+      c->groups.push_back(gr);
+    }
+    c->groups[gid[L]].caps.push_back(k);
+  }
+  c->npts = (long)c->off[ncap];
+  std::vector<CapInfo> caps(ncap);
+  for (size_t gi = 0; gi < c->groups.size(); ++gi) {
+    Group& gr = c->groups[gi];
+    c->nmax = std::max(c->nmax, gr.N);
+    for (size_t q = 0; q < gr.caps.size(); ++q) {
+      const int k = gr.caps[q];
+      caps[k].L = gr.L; caps[k].N = gr.N; caps[k].group = (int)gi; caps[k].pad = 0;
+      caps[k].pt_off = c->off[k]; caps[k].gidx = (long long)q; caps[k].R = c->radius[k];
+    }
+    cudaError_t e = build_tables(c, gr);
+    if (e != cudaSuccess) return cuda_fail(c, e, "tables");
+    const long long n = (long long)gr.caps.size(), N = gr.N;
+    SG_TRY(dalloc(c, gr.buf.Fpos, E * n * 6 * N * gr.nD), "alloc");
+    SG_TRY(dalloc(c, gr.buf.Cpos, E * n * 6 * N * N), "alloc");
+    SG_TRY(dalloc(c, gr.buf.G, E * n * 6 * N * 3 * gr.nD), "alloc");
+    SG_TRY(dalloc(c, gr.buf.Fout, E * n * 12 * N * gr.nD), "alloc");
+    SG_TRY(dalloc(c, gr.buf.Cout, E * n * 12 * N * N), "alloc");
+    SG_TRY(dalloc(c, gr.buf.GO, E * n * 12 * N * 2 * gr.nO), "alloc");
+    SG_TRY(dalloc(c, gr.buf.Fsh, E * n * 8 * N * gr.nO), "alloc");
+    SG_TRY(dalloc(c, gr.buf.Csh, E * n * 8 * N * N), "alloc");
+    SG_TRY(dalloc(c, gr.buf.GF, E * n * 14 * N * gr.nD), "alloc");
+  }
+  std::vector<GroupDev> gdev(c->groups.size());
+  for (size_t gi = 0; gi < c->groups.size(); ++gi) {
+    const Group& gr = c->groups[gi];
+    GroupDev& d = gdev[gi];
+    d.L = gr.L; d.N = gr.N; d.nD = gr.nD; d.mD = gr.mD; d.nO = gr.nO; d.mO = gr.mO;
+    for (int q = 0; q < 2; ++q) {
+      d.latD[q] = gr.tab.latD[q]; d.latO[q] = gr.tab.latO[q];
+      d.trigD[q] = gr.tab.trigD[q]; d.trigO[q] = gr.tab.trigO[q];
+    }
+    d.buf = gr.buf;
+  }
+  void* tmp = nullptr;
+  SG_TRY(upload(c, tmp, caps), "caps");
+  c->d_caps = (CapInfo*)tmp;
+  SG_TRY(upload(c, tmp, gdev), "groups");
+  c->d_groups = (GroupDev*)tmp;
+  SG_TRY(dalloc(c, c->d_cen, sizeof(double) * 3 * std::max(ncap, 1)), "alloc");
+  // row work lists
+  std::vector<RowWork> wpos, wmem, wsh, wfin;
+  for (size_t gi = 0; gi < c->groups.size(); ++gi) {
+    const Group& gr = c->groups[gi];
+    const int rD = std::max(1, 128 / gr.mD), rO = std::max(1, 128 / gr.mO);
+    for (int k : gr.caps) {
+      for (int i = 0; i < gr.nD; ++i) wpos.push_back(RowWork{k, i, 1, (int)gi});
+      for (int i = 0; i < gr.nD; i += rD) wmem.push_back(RowWork{k, i, std::min(rD, gr.nD - i), (int)gi});
+      for (int i = 0; i < gr.nO; i += rO) wsh.push_back(RowWork{k, i, std::min(rO, gr.nO - i), (int)gi});
+    }
+  }
+  wfin = wmem;
+  c->nwpos = (int)wpos.size(); c->nwmem = (int)wmem.size(); c->nwsh = (int)wsh.size(); c->nwfin = (int)wfin.size();
+  SG_TRY(upload(c, tmp, wpos), "work"); c->d_wpos = (RowWork*)tmp;
+  SG_TRY(upload(c, tmp, wmem), "work"); c->d_wmem = (RowWork*)tmp;
+  SG_TRY(upload(c, tmp, wsh), "work"); c->d_wsh = (RowWork*)tmp;
+  SG_TRY(upload(c, tmp, wfin), "work"); c->d_wfin = (RowWork*)tmp;
+  // Legendre problems per stage
+  std::vector<LegProblem> P;
+  std::vector<LegWork> W[6];
+  for (size_t gi = 0; gi < c->groups.size(); ++gi) {
+    const Group& gr = c->groups[gi];
+    const int n = (int)gr.caps.size();
+    const long long N = gr.N, nD = gr.nD, nO = gr.nO;
+    const SpecBuffers& b = gr.buf;
+    const int G = (int)gi;
+    // S0: analysis of the displacement (force grid, truncated to degree < N)
+    add_problem(P, W[0], prob(b.Fpos, 6 * N * nD, N * nD, nD, gr.tab.ana_D[pi], N * nD, b.Cpos, 6 * N * N, N * N, N,
+                              6, n, N, N, nD, 0, G, 1), c->maxJ[0], c->maxK[0]);
+    // S1: synthesis of P, dP, d2P series on the dealias grid
+    add_problem(P, W[1], prob(b.Cpos, 6 * N * N, N * N, N, gr.tab.syn_D[pi], 3 * nD * N, b.G, 6 * N * 3 * nD,
+                              N * 3 * nD, 3 * nD, 6, n, N, 3 * nD, N, 1, G, 0), c->maxJ[1], c->maxK[1]);
+    // S2: analysis of force and normals (dealias grid, truncated)
+    add_problem(P, W[2], prob(b.Fout, 12 * N * nD, N * nD, nD, gr.tab.ana_D[pi], N * nD, b.Cout, 12 * N * N, N * N, N,
+                              12, n, N, N, nD, 0, G, 1), c->maxJ[2], c->maxK[2]);
+    // S3: synthesis on the SH grid: normals (rows 0-5) and shape (rows 6-11)
+    add_problem(P, W[3], prob((const char*)b.Cout + E * 6 * N * N, 12 * N * N, N * N, N, gr.tab.syn_O[pi],
+                              2 * nO * N, b.GO, 12 * N * 2 * nO, N * 2 * nO, 2 * nO, 6, n, N, 2 * nO, N, 1, G, 2),
+                c->maxJ[3], c->maxK[3]);
+    add_problem(P, W[3], prob(b.Cpos, 6 * N * N, N * N, N, gr.tab.syn_O[pi], 2 * nO * N,
+                              (char*)b.GO + E * 6 * N * 2 * nO, 12 * N * 2 * nO, N * 2 * nO, 2 * nO, 6, n, N, 2 * nO,
+                              N, 1, G, 2),
+                c->maxJ[3], c->maxK[3]);
+    // S4: analysis on the SH grid of renormalised normals and surface metric
+    add_problem(P, W[4], prob(b.Fsh, 8 * N * nO, N * nO, nO, gr.tab.ana_O[pi], N * nO, b.Csh, 8 * N * N, N * N, N, 8,
+                              n, N, N, nO, 0, G, 3), c->maxJ[4], c->maxK[4]);
+    // S5: synthesis on the force grid (P only): force rows 0-5, normals+surfmet rows 6-13
+    add_problem(P, W[5], prob(b.Cout, 12 * N * N, N * N, N, gr.tab.syn_D[pi], 3 * nD * N, b.GF, 14 * N * nD, N * nD,
+                              nD, 6, n, N, nD, N, 1, G, 0), c->maxJ[5], c->maxK[5]);
+    add_problem(P, W[5], prob(b.Csh, 8 * N * N, N * N, N, gr.tab.syn_D[pi], 3 * nD * N,
+                              (char*)b.GF + E * 6 * N * nD, 14 * N * nD, N * nD, nD, 8, n, N, nD, N, 1, G, 0),
+                c->maxJ[5], c->maxK[5]);
+  }
+  SG_TRY(upload(c, tmp, P), "problems");
+  c->d_probs = (LegProblem*)tmp;
+  for (int s = 0; s < 6; ++s) {
+    c->nlw[s] = (int)W[s].size();
+    SG_TRY(upload(c, tmp, W[s]), "work");
+    c->d_lw[s] = (LegWork*)tmp;
+  }
+  // binning work
+  const long np = std::max(c->npts, 1L);
+  SG_TRY(dalloc(c, c->ibw.bx, sizeof(int) * np), "alloc");
+  SG_TRY(dalloc(c, c->ibw.by, sizeof(int) * np), "alloc");
+  SG_TRY(dalloc(c, c->ibw.bz, sizeof(int) * np), "alloc");
+  SG_TRY(dalloc(c, c->ibw.entries, sizeof(int) * 8 * np), "alloc");
+  SG_TRY(dalloc(c, c->ibw.fx, E * np), "alloc");
+  SG_TRY(dalloc(c, c->ibw.fy, E * np), "alloc");
+  SG_TRY(dalloc(c, c->ibw.fz, E * np), "alloc");
+  SG_TRY(dalloc(c, c->ibw.counts, sizeof(int) * g.ntiles), "alloc");
+  SG_TRY(dalloc(c, c->ibw.starts, sizeof(int) * (g.ntiles + 1)), "alloc");
+  SG_TRY(dalloc(c, c->ibw.fill, sizeof(int) * g.ntiles), "alloc");
+  if (cfg.mem == SG_MEM_HOST) {
+    SG_TRY(dalloc(c, c->s_u, E * c->nfield), "alloc");
+    SG_TRY(dalloc(c, c->s_v, E * c->nfield), "alloc");
+    SG_TRY(dalloc(c, c->s_w, E * c->nfield), "alloc");
+    for (int q = 0; q < 3; ++q) SG_TRY(dalloc(c, c->s_f[q], E * c->nfield), "alloc");
+    SG_TRY(dalloc(c, c->s_X, sizeof(double) * np), "alloc");
+    SG_TRY(dalloc(c, c->s_Y, sizeof(double) * np), "alloc");
+    SG_TRY(dalloc(c, c->s_Z, sizeof(double) * np), "alloc");
+    for (int q = 0; q < 10; ++q) SG_TRY(dalloc(c, c->s_lag[q], E * np), "alloc");
+    SG_TRY(dalloc(c, c->s_out, sizeof(double) * 7 * std::max(ncap, 1)), "alloc");
+    SG_TRY(dalloc(c, c->s_exy, sizeof(double) * std::max(ncap, 1)), "alloc");
+  }
+  SG_TRY(cudaDeviceSynchronize(), "setup");
+  return SG_OK;
+}
+
+// ------------------------------------------------------------ pipeline ----
+template <class T>
+int dev_bin(sg_ctx* c, const double* X, const double* Y, const double* Z) {
+  SG_TRY(launch_bin<T>(c->grid, c->npts, X, Y, Z, c->ibw, c->st), "bin");
+  c->launches += c->npts > 0 ? 3 : 1;
+  return SG_OK;
+}
+
+template <class T>
+int dev_interp(sg_ctx* c, const T* u, const T* v, const T* w, T* U, T* V, T* W) {
+  SG_TRY(launch_interp<T>(c->grid, c->npts, c->ibw, u, v, w, U, V, W, c->st), "interp");
+  c->launches += 1;
+  return SG_OK;
+}
+
+template <class T>
+int dev_forces(sg_ctx* c, const double* X, const double* Y, const double* Z, T* FX, T* FY, T* FZ, T* NX, T* NY,
+               T* NZ, T* A) {
+  const int nc = c->cfg.ncap;
+  if (nc == 0) return SG_OK;
+  SG_TRY(launch_centroid<T>(nc, c->d_caps, X, Y, Z, c->d_cen, c->st), "centroid");
+  SG_TRY(launch_posfwd<T>(c->d_wpos, c->nwpos, c->d_caps, c->d_groups, X, Y, Z, c->d_cen, c->st), "posfwd");
+  SG_TRY(launch_legendre<T>(c->d_probs, c->d_lw[0], c->nlw[0], c->maxJ[0], c->maxK[0], c->st), "legendre0");
+  SG_TRY(launch_legendre<T>(c->d_probs, c->d_lw[1], c->nlw[1], c->maxJ[1], c->maxK[1], c->st), "legendre1");
+  SG_TRY(launch_membrane<T>(c->d_wmem, c->nwmem, c->d_caps, c->d_groups, c->cfg.gs, c->cfg.csk, c->nmax, c->st),
+         "membrane");
+  SG_TRY(launch_legendre<T>(c->d_probs, c->d_lw[2], c->nlw[2], c->maxJ[2], c->maxK[2], c->st), "legendre2");
+  SG_TRY(launch_legendre<T>(c->d_probs, c->d_lw[3], c->nlw[3], c->maxJ[3], c->maxK[3], c->st), "legendre3");
+  SG_TRY(launch_shgrid<T>(c->d_wsh, c->nwsh, c->d_caps, c->d_groups, c->nmax, c->st), "shgrid");
+  SG_TRY(launch_legendre<T>(c->d_probs, c->d_lw[4], c->nlw[4], c->maxJ[4], c->maxK[4], c->st), "legendre4");
+  SG_TRY(launch_legendre<T>(c->d_probs, c->d_lw[5], c->nlw[5], c->maxJ[5], c->maxK[5], c->st), "legendre5");
+  SG_TRY(launch_final<T>(c->d_wfin, c->nwfin, c->d_caps, c->d_groups, FX, FY, FZ, NX, NY, NZ, A, c->nmax, c->st),
+         "final");
+  c->launches += 12;
+  return SG_OK;
+}
+
+template <class T>
+int dev_spread(sg_ctx* c, const T* FX, const T* FY, const T* FZ, const T* A, T* fx, T* fy, T* fz) {
+  SG_TRY(launch_spread<T>(c->grid, c->ibw, FX, FY, FZ, A, fx, fy, fz, c->st), "spread");
+  c->launches += 1;
+  return SG_OK;
+}
+
+int finish(sg_ctx* c) {
+  if (!c->cfg.async || c->cfg.mem == SG_MEM_HOST) SG_TRY(cudaStreamSynchronize(c->st), "synchronize");
+  return SG_OK;
+}
+
+int h2d(sg_ctx* c, void* dst, const void* src, size_t bytes) {
+  SG_TRY(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyHostToDevice, c->st), "h2d");
+  return SG_OK;
+}
+int d2h(sg_ctx* c, void* dst, const void* src, size_t bytes) {
+  SG_TRY(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyDeviceToHost, c->st), "d2h");
+  return SG_OK;
+}
+
+#define SG_RET(x)             \
+  do {                        \
+    int _r = (x);             \
+    if (_r != SG_OK) return _r; \
+  } while (0)
+
+template <class T>
+int run_step(sg_ctx* c, int what, const void* u, const void* v, const void* w, const double* X, const double* Y,
+             const double* Z, void* U, void* V, void* W, void* FX, void* FY, void* FZ, void* NX, void* NY, void* NZ,
+             void* A, void* fx, void* fy, void* fz) {
+  // what: bit0 interp, bit1 forces, bit2 spread (spread reads FX.. and A as inputs when bit1 is clear)
+  const bool host = c->cfg.mem == SG_MEM_HOST;
+  const size_t pb = sizeof(double) * c->npts, lb = sizeof(T) * c->npts, fb = sizeof(T) * c->nfield;
+  c->launches = 0;
+  const double *dX = X, *dY = Y, *dZ = Z;
+  const T *du = (const T*)u, *dv = (const T*)v, *dw = (const T*)w;
+  T* L[10] = {(T*)U, (T*)V, (T*)W, (T*)FX, (T*)FY, (T*)FZ, (T*)NX, (T*)NY, (T*)NZ, (T*)A};
+  T *dfx = (T*)fx, *dfy = (T*)fy, *dfz = (T*)fz;
+  if (host) {
+    SG_RET(h2d(c, c->s_X, X, pb));
+    SG_RET(h2d(c, c->s_Y, Y, pb));
+    SG_RET(h2d(c, c->s_Z, Z, pb));
+    dX = c->s_X; dY = c->s_Y; dZ = c->s_Z;
+    if (what & 1) {
+      SG_RET(h2d(c, c->s_u, u, fb));
+      SG_RET(h2d(c, c->s_v, v, fb));
+      SG_RET(h2d(c, c->s_w, w, fb));
+      du = (const T*)c->s_u; dv = (const T*)c->s_v; dw = (const T*)c->s_w;
+    }
+    for (int q = 0; q < 10; ++q) L[q] = (T*)c->s_lag[q];
+    if ((what & 4) && !(what & 2)) {
+      SG_RET(h2d(c, L[3], FX, lb));
+      SG_RET(h2d(c, L[4], FY, lb));
+      SG_RET(h2d(c, L[5], FZ, lb));
+      SG_RET(h2d(c, L[9], A, lb));
+    }
+    dfx = (T*)c->s_f[0]; dfy = (T*)c->s_f[1]; dfz = (T*)c->s_f[2];
+  }
+  auto mark = [&](int k) -> int {
+    if (c->profiling) SG_TRY(cudaEventRecord(c->ev[k], c->st), "event");
+    return SG_OK;
+  };
+  SG_RET(mark(0));
+  if (what & 5) SG_RET(dev_bin<T>(c, dX, dY, dZ));
+  SG_RET(mark(1));
+  if (what & 1) SG_RET(dev_interp<T>(c, du, dv, dw, L[0], L[1], L[2]));
+  SG_RET(mark(2));
+  if (what & 2) SG_RET(dev_forces<T>(c, dX, dY, dZ, L[3], L[4], L[5], L[6], L[7], L[8], L[9]));
+  SG_RET(mark(3));
+  if (what & 4) SG_RET(dev_spread<T>(c, L[3], L[4], L[5], L[9], dfx, dfy, dfz));
+  SG_RET(mark(4));
+  c->ev_used[0] = (what & 5) != 0;
+  c->ev_used[1] = (what & 1) != 0;
+  c->ev_used[2] = (what & 2) != 0;
+  c->ev_used[3] = (what & 4) != 0;
+  if (host) {
+    if (what & 1) {
+      SG_RET(d2h(c, U, L[0], lb));
+      SG_RET(d2h(c, V, L[1], lb));
+      SG_RET(d2h(c, W, L[2], lb));
+    }
+    if (what & 2) {
+      void* outs[7] = {FX, FY, FZ, NX, NY, NZ, A};
+      for (int q = 0; q < 7; ++q) SG_RET(d2h(c, outs[q], L[3 + q], lb));
+    }
+    if (what & 4) {
+      SG_RET(d2h(c, fx, dfx, fb));
+      SG_RET(d2h(c, fy, dfy, fb));
+      SG_RET(d2h(c, fz, dfz, fb));
+    }
+  }
+  SG_TRY(cudaGetLastError(), "step");
+  return finish(c);
+}
+
+int check_ptrs(sg_ctx* c, std::initializer_list<const void*> ps) {
+  if (c->npts == 0) return SG_OK;
+  for (const void* p : ps)
+    if (!p) return fail(c, SG_ERR_ARG, "null array argument");
+  return SG_OK;
+}
+
+}  // namespace
+
+// ================================================================ C ABI ===
+extern "C" {
+
+int sg_create(const sg_config* cfg, sg_ctx** out) {
+  if (!cfg || !out) return SG_ERR_ARG;
+  *out = nullptr;
+  sg_ctx* c = new sg_ctx();
+  c->cfg = *cfg;
+  int rc = SG_OK;
+  if (cfg->ncap < 0 || (cfg->ncap > 0 && (!cfg->degree || !cfg->radius))) {
+    rc = fail(c, SG_ERR_CONFIG, "ncap < 0 or missing degree/radius arrays");
+  } else if (cfg->precision != SG_PREC_FP64 && cfg->precision != SG_PREC_MIXED) {
+    rc = fail(c, SG_ERR_CONFIG, "precision must be SG_PREC_FP64 or SG_PREC_MIXED");
+  } else if (cfg->mem != SG_MEM_HOST && cfg->mem != SG_MEM_DEVICE) {
+    rc = fail(c, SG_ERR_CONFIG, "mem must be SG_MEM_HOST or SG_MEM_DEVICE");
+  } else if (!(cfg->lx > 0 && cfg->ly > 0 && cfg->lz > 0)) {
+    rc = fail(c, SG_ERR_CONFIG, "domain lengths must be positive");
+  } else if (cfg->surrogate && cfg->precision != SG_PREC_MIXED) {
+    rc = fail(c, SG_ERR_CONFIG, "the surrogate runs on the mixed path only");
+  } else {
+    c->degree.assign(cfg->degree, cfg->degree + cfg->ncap);
+    c->radius.assign(cfg->radius, cfg->radius + cfg->ncap);
+    for (int k = 0; k < cfg->ncap && rc == SG_OK; ++k) {
+      if (c->degree[k] < 2 || c->degree[k] > 31) rc = fail(c, SG_ERR_CONFIG, "SH degree must be in [2, 31]");
+      if (!(c->radius[k] > 0)) rc = fail(c, SG_ERR_CONFIG, "capsule radius must be positive");
+    }
+    c->cfg.degree = nullptr;
+    c->cfg.radius = nullptr;
+    if (rc == SG_OK) rc = setup(c);
+  }
+  *out = c;  // returned even on failure so sg_last_error can report; caller destroys
+  return rc;
+}
+
+void sg_destroy(sg_ctx* c) {
+  if (!c) return;
+  cudaSetDevice(c->cfg.device);
+  if (c->st) cudaStreamSynchronize(c->st);
+  for (void* p : c->allocs) cudaFree(p);
+  for (int k = 0; k <= SG_NSTAGE; ++k)
+    if (c->ev[k]) cudaEventDestroy(c->ev[k]);
+  if (c->own_stream && c->st) cudaStreamDestroy(c->st);
+  delete c;
+}
+
+const char* sg_last_error(const sg_ctx* c) { return c ? c->err.c_str() : "null context"; }
+
+int sg_synchronize(sg_ctx* c) {
+  if (!c) return SG_ERR_ARG;
+  SG_TRY(cudaStreamSynchronize(c->st), "synchronize");
+  return SG_OK;
+}
+
+int sg_interp(sg_ctx* c, const void* u, const void* v, const void* w, const double* X, const double* Y,
+              const double* Z, void* U, void* V, void* W) {
+  if (!c) return SG_ERR_ARG;
+  SG_RET(check_ptrs(c, {u, v, w, X, Y, Z, U, V, W}));
+  if (c->mixed)
+    return run_step<float>(c, 1, u, v, w, X, Y, Z, U, V, W, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0);
+  return run_step<double>(c, 1, u, v, w, X, Y, Z, U, V, W, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0);
+}
+
+int sg_membrane_force(sg_ctx* c, const double* X, const double* Y, const double* Z, void* FX, void* FY, void* FZ,
+                      void* NX, void* NY, void* NZ, void* AREA) {
+  if (!c) return SG_ERR_ARG;
+  SG_RET(check_ptrs(c, {X, Y, Z, FX, FY, FZ, NX, NY, NZ, AREA}));
+  if (c->mixed)
+    return run_step<float>(c, 2, 0, 0, 0, X, Y, Z, 0, 0, 0, FX, FY, FZ, NX, NY, NZ, AREA, 0, 0, 0);
+  return run_step<double>(c, 2, 0, 0, 0, X, Y, Z, 0, 0, 0, FX, FY, FZ, NX, NY, NZ, AREA, 0, 0, 0);
+}
+
+int sg_spread(sg_ctx* c, const double* X, const double* Y, const double* Z, const void* FX, const void* FY,
+              const void* FZ, const void* AREA, void* fx, void* fy, void* fz) {
+  if (!c) return SG_ERR_ARG;
+  if (!fx || !fy || !fz) return fail(c, SG_ERR_ARG, "null field argument");
+  SG_RET(check_ptrs(c, {X, Y, Z, FX, FY, FZ, AREA}));
+  if (c->mixed)
+    return run_step<float>(c, 4, 0, 0, 0, X, Y, Z, 0, 0, 0, (void*)FX, (void*)FY, (void*)FZ, 0, 0, 0, (void*)AREA,
+                           fx, fy, fz);
+  return run_step<double>(c, 4, 0, 0, 0, X, Y, Z, 0, 0, 0, (void*)FX, (void*)FY, (void*)FZ, 0, 0, 0, (void*)AREA, fx,
+                          fy, fz);
+}
+
+int sg_step(sg_ctx* c, const void* u, const void* v, const void* w, const double* X, const double* Y,
+            const double* Z, void* U, void* V, void* W, void* FX, void* FY, void* FZ, void* NX, void* NY, void* NZ,
+            void* AREA, void* fx, void* fy, void* fz) {
+  if (!c) return SG_ERR_ARG;
+  if (!fx || !fy || !fz) return fail(c, SG_ERR_ARG, "null field argument");
+  SG_RET(check_ptrs(c, {u, v, w, X, Y, Z, U, V, W, FX, FY, FZ, NX, NY, NZ, AREA}));
+  if (c->mixed) return run_step<float>(c, 7, u, v, w, X, Y, Z, U, V, W, FX, FY, FZ, NX, NY, NZ, AREA, fx, fy, fz);
+  return run_step<double>(c, 7, u, v, w, X, Y, Z, U, V, W, FX, FY, FZ, NX, NY, NZ, AREA, fx, fy, fz);
+}
+
+int sg_update_pos(sg_ctx* c, double dt, double* X, double* Y, double* Z, const void* U, const void* V,
+                  const void* W) {
+  if (!c) return SG_ERR_ARG;
+  SG_RET(check_ptrs(c, {X, Y, Z, U, V, W}));
+  const bool host = c->cfg.mem == SG_MEM_HOST;
+  const size_t pb = sizeof(double) * c->npts, lb = c->esz * c->npts;
+  double *dX = X, *dY = Y, *dZ = Z;
+  const void *dU = U, *dV = V, *dW = W;
+  if (host) {
+    SG_RET(h2d(c, c->s_X, X, pb));
+    SG_RET(h2d(c, c->s_Y, Y, pb));
+    SG_RET(h2d(c, c->s_Z, Z, pb));
+    SG_RET(h2d(c, c->s_lag[0], U, lb));
+    SG_RET(h2d(c, c->s_lag[1], V, lb));
+    SG_RET(h2d(c, c->s_lag[2], W, lb));
+    dX = c->s_X; dY = c->s_Y; dZ = c->s_Z;
+    dU = c->s_lag[0]; dV = c->s_lag[1]; dW = c->s_lag[2];
+  }
+  cudaError_t e = c->mixed ? launch_update_pos<float>(c->npts, dt, c->cfg.lz, dX, dY, dZ, (const float*)dU,
+                                                      (const float*)dV, (const float*)dW, c->st)
+                           : launch_update_pos<double>(c->npts, dt, c->cfg.lz, dX, dY, dZ, (const double*)dU,
+                                                       (const double*)dV, (const double*)dW, c->st);
+  if (e != cudaSuccess) return cuda_fail(c, e, "update_pos");
+  if (host) {
+    SG_RET(d2h(c, X, dX, pb));
+    SG_RET(d2h(c, Y, dY, pb));
+    SG_RET(d2h(c, Z, dZ, pb));
+  }
+  return finish(c);
+}
+
+int sg_surf_vol(sg_ctx* c, const double* X, const double* Y, const double* Z, const void* NX, const void* NY,
+                const void* NZ, const void* AREA, const double* exy1_prev, double* out) {
+  if (!c) return SG_ERR_ARG;
+  if (!out) return fail(c, SG_ERR_ARG, "null output");
+  SG_RET(check_ptrs(c, {X, Y, Z, NX, NY, NZ, AREA}));
+  const bool host = c->cfg.mem == SG_MEM_HOST;
+  const size_t pb = sizeof(double) * c->npts, lb = c->esz * c->npts;
+  const double *dX = X, *dY = Y, *dZ = Z, *dexy = exy1_prev;
+  const void *dNX = NX, *dNY = NY, *dNZ = NZ, *dA = AREA;
+  double* dout = out;
+  if (host) {
+    SG_RET(h2d(c, c->s_X, X, pb));
+    SG_RET(h2d(c, c->s_Y, Y, pb));
+    SG_RET(h2d(c, c->s_Z, Z, pb));
+    SG_RET(h2d(c, c->s_lag[6], NX, lb));
+    SG_RET(h2d(c, c->s_lag[7], NY, lb));
+    SG_RET(h2d(c, c->s_lag[8], NZ, lb));
+    SG_RET(h2d(c, c->s_lag[9], AREA, lb));
+    if (exy1_prev) SG_RET(h2d(c, c->s_exy, exy1_prev, sizeof(double) * c->cfg.ncap));
+    dX = c->s_X; dY = c->s_Y; dZ = c->s_Z;
+    dNX = c->s_lag[6]; dNY = c->s_lag[7]; dNZ = c->s_lag[8]; dA = c->s_lag[9];
+    dexy = exy1_prev ? c->s_exy : nullptr;
+    dout = c->s_out;
+  }
+  cudaError_t e = c->mixed ? launch_surf_vol<float>(c->cfg.ncap, c->d_caps, dX, dY, dZ, (const float*)dNX,
+                                                    (const float*)dNY, (const float*)dNZ, (const float*)dA, dexy,
+                                                    dout, c->st)
+                           : launch_surf_vol<double>(c->cfg.ncap, c->d_caps, dX, dY, dZ, (const double*)dNX,
+                                                     (const double*)dNY, (const double*)dNZ, (const double*)dA, dexy,
+                                                     dout, c->st);
+  if (e != cudaSuccess) return cuda_fail(c, e, "surf_vol");
+  if (host) SG_RET(d2h(c, out, c->s_out, sizeof(double) * 7 * c->cfg.ncap));
+  return finish(c);
+}
+
+int sg_gauss(int nlat, double* theta, double* weights) {
+  if (nlat < 1 || !theta || !weights) return SG_ERR_ARG;
+  host_gauss(nlat, theta, weights);
+  return SG_OK;
+}
+
+int sg_legendre(double theta, int mm, int nn, double* P, double* dP, double* d2P) {
+  if (mm < 1 || nn < 1) return SG_ERR_ARG;
+  host_legendre(theta, mm, nn, P, dP, d2P);
+  return SG_OK;
+}
+
+int sg_last_launch_count(const sg_ctx* c) { return c ? c->launches : 0; }
+
+int sg_set_profiling(sg_ctx* c, int on) {
+  if (!c) return SG_ERR_ARG;
+  if (on && !c->ev[0])
+    for (int k = 0; k <= SG_NSTAGE; ++k) SG_TRY(cudaEventCreate(&c->ev[k]), "cudaEventCreate");
+  c->profiling = on != 0;
+  return SG_OK;
+}
+
+int sg_stage_times(sg_ctx* c, float* ms, int n) {
+  if (!c || !ms) return SG_ERR_ARG;
+  if (!c->profiling) return fail(c, SG_ERR_STATE, "profiling is off");
+  SG_TRY(cudaEventSynchronize(c->ev[SG_NSTAGE]), "event sync");
+  for (int k = 0; k < n && k < SG_NSTAGE; ++k) {
+    float t = 0.f;
+    if (c->ev_used[k]) SG_TRY(cudaEventElapsedTime(&t, c->ev[k], c->ev[k + 1]), "elapsed");
+    ms[k] = t;
+  }
+  return SG_OK;
+}
+
+}  // extern "C"

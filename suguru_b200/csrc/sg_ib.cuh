@@ -1,0 +1,38 @@
+// sg_ib.cuh -- Lagrangian <-> Eulerian transfer on the staggered MAC grid.
+//
+// Replaces eulr2lagr (interp_spread.f90:12-475) and lagr2eulr
+// (interp_spread.f90:510-922) on one GPU.  The reference's master/slave image
+// copies and MPI halo exchange reduce, on a single domain, to periodic index
+// wrap in x and y and clipping of the stencil to [1,kmax] in z
+// (interp_spread.f90:340-351, 846-851); the force halo is the copy of
+// bound.f90:141-190.
+//
+// Points are binned by tile (counting sort, then each tile's list sorted by
+// point index so the order is deterministic).  Interpolation is a per-point
+// gather in tile order.  Spreading is a per-cell gather over the points staged
+// for the cell's tile: no float atomics, fixed summation order.
+#pragma once
+#include "sg_common.cuh"
+
+namespace sg {
+
+struct IBGrid {
+  int itot, jtot, ktot;  // interior cells (imax, jmax, kmax)
+  int ldi, ldj, ldk;     // itot+2, jtot+2, ktot+2 (halo of one cell)
+  double dxi, dyi, dzi;  // inverse spacings
+  double dvi;            // 1 / (dx dy dz)
+  int TX, TY, TZ;        // tile shape
+  int ntx, nty, ntz;     // tiles per dimension
+  int ntiles;
+};
+
+// Per point after binning: base face index b = floor(c) per dimension (x, y
+// wrapped into [0, n), z raw) and the fractional offsets c - b.
+struct PointBins {
+  int* bx;
+  int* by;
+  int* bz;
+  int* tile;
+};
+
+}  // namespace sg

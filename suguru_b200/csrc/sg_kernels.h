@@ -1,0 +1,155 @@
+// sg_kernels.h -- internal declarations shared by the .cu files of the library.
+#pragma once
+#include <cuda_runtime.h>
+#include <stdint.h>
+#include <vector>
+
+#include "sg_ib.cuh"
+
+namespace sg {
+
+// ------------------------------------------------------------ IB transfer --
+struct IBWork {
+  int* bx = nullptr;
+  int* by = nullptr;
+  int* bz = nullptr;
+  void* fx = nullptr;  // T[npts] fractional offsets
+  void* fy = nullptr;
+  void* fz = nullptr;
+  int* counts = nullptr;  // [ntiles]
+  int* starts = nullptr;  // [ntiles+1]
+  int* fill = nullptr;    // [ntiles]
+  int* entries = nullptr; // [8*npts] point index per (tile, point) pair
+};
+
+bool make_ib_grid(int itot, int jtot, int ktot, double lx, double ly, double lz, IBGrid& g);
+template <class T>
+cudaError_t launch_bin(const IBGrid& g, long n, const double* X, const double* Y, const double* Z, IBWork& w,
+                       cudaStream_t st);
+template <class T>
+cudaError_t launch_interp(const IBGrid& g, long n, const IBWork& w, const T* u, const T* v, const T* ww, T* U, T* V,
+                          T* W, cudaStream_t st);
+template <class T>
+cudaError_t launch_spread(const IBGrid& g, const IBWork& w, const T* FX, const T* FY, const T* FZ, const T* A, T* ox,
+                          T* oy, T* oz, cudaStream_t st);
+
+// ------------------------------------------------------------ host tables --
+// Gauss-Legendre colatitudes north->south and weights (gaqd.f:45 semantics).
+void host_gauss(int n, double* th, double* w);
+// SPHEREPACK-normalised P, dP/dtheta, d2P/dtheta2 at one colatitude as
+// [m*nn+n] for m<mm, n<nn (zero for n<m).
+void host_legendre(double th, int mm, int nn, double* P, double* dP, double* d2P);
+
+// ---------------------------------------------------------- spectral stage --
+// Per-degree constant data on the device (built from FP64 host tables).
+struct DegreeTables {
+  int L = 0, N = 0, nD = 0, mD = 0, nO = 0, mO = 0;
+  // Legendre GEMM operands, K fastest: B[m][j][k]
+  //  syn_D : j = kind*nD + i (kind 0:P 1:dP 2:d2P, m=0 row halved), k = n < N   (J=3nD, K=N)
+  //  ana_D : j = n,  k = i  (w_i P)                                            (J=N,   K=nD)
+  //  syn_O : j = kind*nO + i (kind 0:P 1:dP), k = n                             (J=2nO, K=N)
+  //  ana_O : j = n,  k = i  (w_i P on the SH grid)                              (J=N,   K=nO)
+  void* syn_D[2] = {nullptr, nullptr};  // [0] double, [1] float
+  void* ana_D[2] = {nullptr, nullptr};
+  void* syn_O[2] = {nullptr, nullptr};
+  void* ana_O[2] = {nullptr, nullptr};
+  // per-latitude data: sin, cos of theta on both grids, area weight w/sin*dphi
+  void* latD[2] = {nullptr, nullptr};  // [nD][4]: sin, cos, wgtdsinf, theta
+  void* latO[2] = {nullptr, nullptr};  // [nO][4]
+  // cos/sin(m phi_j), [m][j], on both longitude grids
+  void* trigD[2] = {nullptr, nullptr};  // [2][N][mD]
+  void* trigO[2] = {nullptr, nullptr};  // [2][N][mO]
+  // BF16x3 split operands in UMMA canonical K-major layout (mixed path)
+  void* umma_syn_D = nullptr;
+  void* umma_ana_D = nullptr;
+  void* umma_syn_O = nullptr;
+  void* umma_ana_O = nullptr;
+};
+
+// One batched Legendre contraction over the capsules of one degree group.
+// Row q = (c, r) with c = q / rpc, r = q % rpc; for m < M, j < J:
+//   D[c*sDc + r*sDr + m*sDm + j] = sum_{k<K} A[c*sAc + r*sAr + m*sAm + k] * B[m*sBm + j*K + k]
+struct LegProblem {
+  const void* A;
+  long long sAc, sAr, sAm;
+  const void* B;
+  long long sBm;
+  void* D;
+  long long sDc, sDr, sDm;
+  int rpc;
+  int Q, M, J, K;
+  int tri;       // 1: k starts at m (synthesis: coefficients vanish for n<m)
+  int group;     // degree group (for the UMMA operand lookup)
+  int kind;      // 0 syn_D, 1 ana_D, 2 syn_O, 3 ana_O
+};
+
+struct LegWork {  // one tile of a problem
+  int prob, m, q0;
+};
+
+template <class T>
+cudaError_t launch_legendre(const LegProblem* d_probs, const LegWork* d_work, int nwork, int maxJ, int maxK,
+                            cudaStream_t st);
+
+// Capsule-row work items for the pointwise kernels.
+struct RowWork {
+  int cap;    // capsule index (global)
+  int row0;   // first latitude row
+  int nrows;  // rows in this item
+  int group;  // degree group
+};
+
+struct CapInfo {  // per capsule, device
+  int L, N, group;
+  int pad;
+  long long pt_off;   // first point (global flat index)
+  long long gidx;     // index within its degree group
+  double R;
+};
+
+struct SpecBuffers {  // per degree group base pointers (T)
+  void* Fpos;   // [ncap_g][3][2][N][nD]
+  void* Cpos;   // [ncap_g][3][2][N][N]
+  void* G;      // [ncap_g][3][2][N][3*nD]
+  void* Fout;   // [ncap_g][6][2][N][nD]
+  void* Cout;   // [ncap_g][6][2][N][N]   fields: f0 f1 f2 n0 n1 n2
+  void* GO;     // [ncap_g][6][2][N][2*nO]  (normals: rows 0-2 from Cout n; shape: rows 3-5 from Cpos)
+  void* Fsh;    // [ncap_g][4][2][N][nO]
+  void* Csh;    // [ncap_g][4][2][N][N]    n0 n1 n2 surfmet
+  void* GF;     // [ncap_g][7][2][N][nD]   f0 f1 f2 n0 n1 n2 surfmet (P only)
+};
+
+struct GroupDev {  // device copy of per-group constants; [0] double, [1] float
+  int L, N, nD, mD, nO, mO;
+  const void* latD[2];
+  const void* latO[2];
+  const void* trigD[2];
+  const void* trigO[2];
+  SpecBuffers buf;
+};
+
+template <class T>
+cudaError_t launch_centroid(int ncap, const CapInfo* caps, const double* X, const double* Y, const double* Z,
+                            double* cen, cudaStream_t st);
+template <class T>
+cudaError_t launch_posfwd(const RowWork* work, int nwork, const CapInfo* caps, const GroupDev* groups,
+                          const double* X, const double* Y, const double* Z, const double* cen, cudaStream_t st);
+template <class T>
+cudaError_t launch_membrane(const RowWork* work, int nwork, const CapInfo* caps, const GroupDev* groups, double gs,
+                            double csk, int nmax, cudaStream_t st);
+template <class T>
+cudaError_t launch_shgrid(const RowWork* work, int nwork, const CapInfo* caps, const GroupDev* groups, int nmax,
+                          cudaStream_t st);
+template <class T>
+cudaError_t launch_final(const RowWork* work, int nwork, const CapInfo* caps, const GroupDev* groups, T* FX, T* FY,
+                         T* FZ, T* NX, T* NY, T* NZ, T* AREA, int nmax, cudaStream_t st);
+
+template <class T>
+cudaError_t launch_update_pos(long n, double dt, double lz, double* X, double* Y, double* Z, const T* U, const T* V,
+                              const T* W, cudaStream_t st);
+template <class T>
+cudaError_t launch_surf_vol(int ncap, const CapInfo* caps, const double* X, const double* Y, const double* Z,
+                            const T* NX, const T* NY, const T* NZ, const T* AREA, const double* exy1_prev,
+                            double* out, cudaStream_t st);
+
+}  // namespace sg

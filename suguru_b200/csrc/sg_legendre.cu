@@ -1,0 +1,67 @@
+// sg_legendre.cu -- batched Legendre contractions (the theta half of the
+// SPHEREPACK Gauss-grid analysis shagc.f:384-470 and synthesis shsgc.f:329-470)
+// on CUDA cores, for the FP64 plain path and as the FP32 fallback.
+//
+// Each LegWork item is one (problem, m, 32-row tile): the m-th table slice
+// B_m[J][K] is staged in shared memory (row stride K+1 to avoid bank
+// conflicts), the tile's A rows next to it, and each thread forms dot
+// products over K.  Synthesis problems start K at m (coefficients vanish for
+// n < m).
+#include "sg_common.cuh"
+#include "sg_kernels.h"
+
+namespace sg {
+
+constexpr int LEG_QT = 32;
+
+template <class T>
+__global__ void __launch_bounds__(256) legendre_kernel(const LegProblem* __restrict__ probs,
+                                                       const LegWork* __restrict__ work, int nwork) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  const LegWork wk = work[blockIdx.x];
+  const LegProblem P = probs[wk.prob];
+  const int m = wk.m, q0 = wk.q0;
+  const int nq = min(LEG_QT, P.Q - q0);
+  const int K = P.K, J = P.J, Kp = K + 1;
+  const int k0 = P.tri ? m : 0;
+  T* sB = (T*)smem_raw;       // [J][Kp]
+  T* sA = sB + J * Kp;        // [QT][Kp]
+  const T* B = (const T*)P.B + (long long)m * P.sBm;
+  for (int e = threadIdx.x; e < J * K; e += blockDim.x) {
+    const int j = e / K, k = e % K;
+    sB[j * Kp + k] = B[e];
+  }
+  const T* A = (const T*)P.A;
+  for (int e = threadIdx.x; e < nq * K; e += blockDim.x) {
+    const int q = e / K, k = e % K;
+    const int qq = q0 + q, c = qq / P.rpc, r = qq % P.rpc;
+    sA[q * Kp + k] = A[(long long)c * P.sAc + (long long)r * P.sAr + (long long)m * P.sAm + k];
+  }
+  __syncthreads();
+  T* D = (T*)P.D;
+  for (int e = threadIdx.x; e < nq * J; e += blockDim.x) {
+    const int q = e / J, j = e % J;
+    const T* a = sA + q * Kp;
+    const T* b = sB + j * Kp;
+    T s = 0;
+    for (int k = k0; k < K; ++k) s += a[k] * b[k];
+    const int qq = q0 + q, c = qq / P.rpc, r = qq % P.rpc;
+    D[(long long)c * P.sDc + (long long)r * P.sDr + (long long)m * P.sDm + j] = s;
+  }
+}
+
+template <class T>
+cudaError_t launch_legendre(const LegProblem* d_probs, const LegWork* d_work, int nwork, int maxJ, int maxK,
+                            cudaStream_t st) {
+  if (nwork <= 0) return cudaSuccess;
+  size_t smem = sizeof(T) * (size_t)(maxJ + LEG_QT) * (maxK + 1);
+  cudaError_t e = cudaFuncSetAttribute(legendre_kernel<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  if (e != cudaSuccess) return e;
+  legendre_kernel<T><<<nwork, 256, smem, st>>>(d_probs, d_work, nwork);
+  return cudaGetLastError();
+}
+
+template cudaError_t launch_legendre<double>(const LegProblem*, const LegWork*, int, int, int, cudaStream_t);
+template cudaError_t launch_legendre<float>(const LegProblem*, const LegWork*, int, int, int, cudaStream_t);
+
+}  // namespace sg

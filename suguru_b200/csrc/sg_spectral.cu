@@ -1,0 +1,562 @@
+// sg_spectral.cu -- spherical-harmonic transforms and the Skalak membrane force.
+//
+// Replaces complagrforces (forcing.f90:11-114) -> cal_spectral_force
+// (sph.f90:1523-1755) with its SPHEREPACK TRSSPH/shagc/shsgc transforms, for
+// all capsules at once.  The reference's chain per capsule is
+//   TRSSPH force grid -> SH grid, analysis (degree < N), synthesis of the
+//   tangent basis and its derivatives on the dealias grid, pointwise geometry
+//   and mechanics, analysis of force and normals on the dealias grid,
+//   truncated synthesis on the SH grid, renormalised normals, surface metric,
+//   TRSSPH SH grid -> force grid, area = surfmet * w/sin(theta) * dphi.
+// Here the transforms are split into longitude DFTs (CUDA cores, one capsule
+// row per warp/block) and batched Legendre contractions over all capsules of
+// a degree group (sg_legendre.cu).  TRSSPH-in followed by the SH-grid
+// analysis is exact for band-limited data, so it is fused into one analysis
+// of the force grid truncated to degree < N; the force filter followed by
+// TRSSPH-out is likewise one truncated analysis followed by synthesis.
+//
+// The reference sphere x = R (sin t sin p, sin t cos p, cos t) (sph.f90:84-86)
+// is subtracted from the positions before the transforms and its geometry
+// added back analytically, so the transforms only carry the displacement.
+#include "sg_common.cuh"
+#include "sg_kernels.h"
+
+namespace sg {
+
+template <class T>
+constexpr int pidx() {
+  return sizeof(T) == 8 ? 0 : 1;
+}
+
+// ------------------------------------------------------------ centroid -----
+__global__ void centroid_kernel(int ncap, const CapInfo* __restrict__ caps, const double* __restrict__ X,
+                                const double* __restrict__ Y, const double* __restrict__ Z, double* __restrict__ cen) {
+  __shared__ double s[3][256];
+  const int c = blockIdx.x, t = threadIdx.x;
+  const CapInfo ci = caps[c];
+  const long long n = 8LL * ci.N * ci.N;
+  double sx = 0, sy = 0, sz = 0;
+  for (long long p = t; p < n; p += blockDim.x) {
+    sx += X[ci.pt_off + p];
+    sy += Y[ci.pt_off + p];
+    sz += Z[ci.pt_off + p];
+  }
+  s[0][t] = sx;
+  s[1][t] = sy;
+  s[2][t] = sz;
+  __syncthreads();
+  for (int o = blockDim.x / 2; o > 0; o >>= 1) {
+    if (t < o) {
+      s[0][t] += s[0][t + o];
+      s[1][t] += s[1][t + o];
+      s[2][t] += s[2][t + o];
+    }
+    __syncthreads();
+  }
+  if (t == 0) {
+    cen[3 * c + 0] = s[0][0] / (double)n;
+    cen[3 * c + 1] = s[1][0] / (double)n;
+    cen[3 * c + 2] = s[2][0] / (double)n;
+  }
+}
+
+// ------------------------------------------------- positions -> Fourier ---
+// Warp per dealias row i: displacement d = X - cen - R s(t_i, p_j) in FP64,
+// then the real DFT of shagc (shagc.f:364-380: 2/nlon scaling, forward
+// transform carries -sin) for m < N.
+template <class T>
+__global__ void __launch_bounds__(128) posfwd_kernel(const RowWork* __restrict__ work, int nwork,
+                                                     const CapInfo* __restrict__ caps,
+                                                     const GroupDev* __restrict__ groups, const double* __restrict__ X,
+                                                     const double* __restrict__ Y, const double* __restrict__ Z,
+                                                     const double* __restrict__ cen) {
+  __shared__ T sd[4][3][128];
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int w = blockIdx.x * 4 + warp;
+  if (w >= nwork) return;
+  const RowWork it = work[w];
+  const CapInfo ci = caps[it.cap];
+  const GroupDev gd = groups[it.group];
+  const int N = gd.N, nD = gd.nD, mD = gd.mD;
+  const double* lat64 = (const double*)gd.latD[0];
+  const double* trig64 = (const double*)gd.trigD[0];
+  const T* trig = (const T*)gd.trigD[pidx<T>()];
+  const double R = ci.R;
+  const double c0 = cen[3 * it.cap], c1 = cen[3 * it.cap + 1], c2 = cen[3 * it.cap + 2];
+  T* Fpos = (T*)gd.buf.Fpos + (long long)ci.gidx * 6 * N * nD;
+  for (int r = 0; r < it.nrows; ++r) {
+    const int i = it.row0 + r;
+    const double st = lat64[4 * i], ct = lat64[4 * i + 1];
+    for (int j = lane; j < mD; j += 32) {
+      const long long p = ci.pt_off + (long long)i * mD + j;
+      const double cp = trig64[1 * mD + j], sp = trig64[N * mD + 1 * mD + j];
+      sd[warp][0][j] = (T)(X[p] - c0 - R * (st * sp));
+      sd[warp][1][j] = (T)(Y[p] - c1 - R * (st * cp));
+      sd[warp][2][j] = (T)(Z[p] - c2 - R * ct);
+    }
+    __syncwarp();
+    if (lane < N) {
+      const int m = lane;
+      const T* cs = trig + (long long)m * mD;
+      const T* sn = trig + (long long)N * mD + (long long)m * mD;
+      T a0 = 0, a1 = 0, a2 = 0, b0 = 0, b1 = 0, b2 = 0;
+      for (int j = 0; j < mD; ++j) {
+        const T c = cs[j], s = sn[j];
+        a0 += sd[warp][0][j] * c;
+        a1 += sd[warp][1][j] * c;
+        a2 += sd[warp][2][j] * c;
+        b0 += sd[warp][0][j] * s;
+        b1 += sd[warp][1][j] * s;
+        b2 += sd[warp][2][j] * s;
+      }
+      const T sfn = T(2) / T(mD);
+      const long long rs = (long long)N * nD;  // (comp, cs) row stride
+      Fpos[0 * rs + m * nD + i] = sfn * a0;
+      Fpos[1 * rs + m * nD + i] = -sfn * b0;
+      Fpos[2 * rs + m * nD + i] = sfn * a1;
+      Fpos[3 * rs + m * nD + i] = -sfn * b1;
+      Fpos[4 * rs + m * nD + i] = sfn * a2;
+      Fpos[5 * rs + m * nD + i] = -sfn * b2;
+    }
+    __syncwarp();
+  }
+}
+
+// ------------------------------------------------- geometry + mechanics ---
+template <class T>
+struct Geo {
+  T a1[3], a2[3], d11[3], d12[3], d22[3];
+  T n[3];
+  T c1[3], c2[3];
+  T cat[3], catd1[2][3], conat[3], conatd1[2][3], bcur[3], chf[8];
+};
+
+// sph1.f90:581-651 (normal), sph.f90:442-476 (curvature), sph1.f90:197-297
+// with co2contra (capsulesolid.f90:106-146), sph.f90:735-893 (christof),
+// sph.f90:896-961 (metrics).  Same operation order as the reference.
+template <class T>
+__device__ __forceinline__ void geometry(Geo<T>& G) {
+  const T* cd1[2] = {G.d11, G.d12};
+  const T* cd2[2] = {G.d12, G.d22};
+  T cc[3];
+  cross3(G.a1, G.a2, cc);
+  const T sm = sqrt(cc[0] * cc[0] + cc[1] * cc[1] + cc[2] * cc[2]);
+  for (int c = 0; c < 3; ++c) G.n[c] = cc[c] / sm;
+  T nde[2][3];
+#pragma unroll
+  for (int al = 0; al < 2; ++al) {
+    T x1[3], x2[3], dc[3];
+    cross3(cd1[al], G.a2, x1);
+    cross3(G.a1, cd2[al], x2);
+    for (int c = 0; c < 3; ++c) dc[c] = x1[c] + x2[c];
+    const T tmp = dot3(cc, dc) / sqrt(cc[0] * cc[0] + cc[1] * cc[1] + cc[2] * cc[2]);
+    for (int c = 0; c < 3; ++c) nde[al][c] = T(1) / sm * (x1[c] + x2[c] - tmp * G.n[c]);
+  }
+  G.bcur[0] = dot3(G.n, G.d11);
+  G.bcur[1] = dot3(G.n, G.d22);
+  G.bcur[2] = dot3(G.n, G.d12);
+  T a2n[3], na1[3];
+  cross3(G.a2, G.n, a2n);
+  cross3(G.n, G.a1, na1);
+  const T hyb1 = dot3(G.a1, a2n), hyb2 = dot3(G.a2, na1);
+  for (int c = 0; c < 3; ++c) {
+    G.c1[c] = a2n[c] / hyb1;
+    G.c2[c] = na1[c] / hyb2;
+  }
+  const T g = hyb1;
+  T cdc1[2][3], cdc2[2][3];
+#pragma unroll
+  for (int al = 0; al < 2; ++al) {
+    T a2de_n3[3], a2_n3de[3], n3de_a1[3], n3_a1de[3], vt[3];
+    cross3(cd2[al], G.n, a2de_n3);
+    cross3(G.a2, nde[al], a2_n3de);
+    cross3(nde[al], G.a1, n3de_a1);
+    cross3(G.n, cd1[al], n3_a1de);
+    for (int c = 0; c < 3; ++c) vt[c] = a2de_n3[c] + a2_n3de[c];
+    const T gde = dot3(cd1[al], a2n) + dot3(G.a1, vt);
+    for (int c = 0; c < 3; ++c) {
+      cdc1[al][c] = T(1) / g * (-gde * G.c1[c] + a2de_n3[c] + a2_n3de[c]);
+      cdc2[al][c] = T(1) / g * (-gde * G.c2[c] + n3de_a1[c] + n3_a1de[c]);
+    }
+  }
+  // christof(gamma,beta,alpha) at [(gamma-1) + 2(beta-1) + 4(alpha-1)]
+  G.chf[0 + 0 + 0] = dot3(G.d11, G.c1);  // (1,1,1)
+  G.chf[1 + 0 + 0] = dot3(G.d12, G.c1);  // (2,1,1)
+  G.chf[0 + 2 + 0] = dot3(G.d11, G.c2);  // (1,2,1)
+  G.chf[1 + 2 + 0] = dot3(G.d12, G.c2);  // (2,2,1)
+  G.chf[1 + 0 + 4] = dot3(G.d22, G.c1);  // (2,1,2)
+  G.chf[1 + 2 + 4] = dot3(G.d22, G.c2);  // (2,2,2)
+  G.chf[0 + 0 + 4] = G.chf[1];           // (1,1,2) = (2,1,1)
+  G.chf[0 + 2 + 4] = G.chf[3];           // (1,2,2) = (2,2,1)
+  G.cat[0] = G.a1[0] * G.a1[0] + G.a1[1] * G.a1[1] + G.a1[2] * G.a1[2];
+  G.cat[1] = G.a2[0] * G.a2[0] + G.a2[1] * G.a2[1] + G.a2[2] * G.a2[2];
+  G.cat[2] = dot3(G.a1, G.a2);
+  G.conat[0] = G.c1[0] * G.c1[0] + G.c1[1] * G.c1[1] + G.c1[2] * G.c1[2];
+  G.conat[1] = G.c2[0] * G.c2[0] + G.c2[1] * G.c2[1] + G.c2[2] * G.c2[2];
+  G.conat[2] = dot3(G.c1, G.c2);
+#pragma unroll
+  for (int al = 0; al < 2; ++al) {
+    G.catd1[al][0] = T(2) * dot3(G.a1, cd1[al]);
+    G.catd1[al][1] = T(2) * dot3(G.a2, cd2[al]);
+    G.catd1[al][2] = dot3(G.a1, cd2[al]) + dot3(G.a2, cd1[al]);
+    G.conatd1[al][0] = T(2) * dot3(G.c1, cdc1[al]);
+    G.conatd1[al][1] = T(2) * dot3(G.c2, cdc2[al]);
+    G.conatd1[al][2] = dot3(G.c1, cdc2[al]) + dot3(G.c2, cdc1[al]);
+  }
+}
+
+// sph.f90:1668-1715 with cal_Js_I1_I2_deri (sph.f90:1115-1156), the Skalak
+// law of membmodel.c:81-99 and calculate_cauchy_tensor_deri (sph.f90:1179-1234).
+// A: reference contravariant metric (11,22,12); Ad[al]: its derivatives.
+template <class T>
+__device__ __forceinline__ void mechanics(const Geo<T>& G, const T* A, const T (*Ad)[3], T hf, T csk, T* f) {
+  const T A11 = A[0], A22 = A[1], A12 = A[2];
+  const T c11 = G.cat[0], c22 = G.cat[1], c12 = G.cat[2];
+  const T abs_conA = A11 * A22 - A12 * A12;
+  const T abs_ca = c11 * c22 - c12 * c12;
+  const T I1 = A11 * c11 + A22 * c22 + T(2) * A12 * c12 - T(2);
+  const T I2 = abs_conA * abs_ca - T(1);
+  const T Js = sqrt(T(1) + I2);
+  T I1de[2], I2de[2], Jsde[2];
+#pragma unroll
+  for (int al = 0; al < 2; ++al) {
+    const T Ad11 = Ad[al][0], Ad22 = Ad[al][1], Ad12 = Ad[al][2];
+    const T cd11 = G.catd1[al][0], cd22 = G.catd1[al][1], cd12 = G.catd1[al][2];
+    I1de[al] = Ad11 * c11 + A11 * cd11 + Ad22 * c22 + A22 * cd22 + T(2) * (Ad12 * c12 + A12 * cd12);
+    const T abs_conAd = Ad11 * A22 + A11 * Ad22 - T(2) * A12 * Ad12;
+    const T abs_cad = cd11 * c22 + c11 * cd22 - T(2) * c12 * cd12;
+    I2de[al] = abs_conAd * abs_ca + abs_cad * abs_conA;
+    Jsde[al] = T(0.5) / Js * I2de[al];
+  }
+  const T W1 = hf * (T(1) + I1);
+  const T W2 = hf * (csk * I2 - T(1));
+  const T coef1 = T(2) / Js * W1, coef2 = T(2) * Js * W2;
+  const T a11 = G.conat[0], a22 = G.conat[1], a12 = G.conat[2];
+  const T T11 = coef1 * A11 + coef2 * a11;
+  const T T22 = coef1 * A22 + coef2 * a22;
+  const T T12 = coef1 * A12 + coef2 * a12;
+  T Td11[2], Td22[2], Td12[2];
+#pragma unroll
+  for (int al = 0; al < 2; ++al) {
+    const T W1de = hf * I1de[al], W2de = csk * hf * I2de[al];
+    const T v1 = -T(2) / (Js * Js) * Jsde[al] * W1;
+    const T v2 = T(2) / Js * W1de;
+    const T v3 = T(2) / Js * W1;
+    const T v4 = T(2) * Jsde[al] * W2;
+    const T v5 = T(2) * Js * W2de;
+    const T v6 = T(2) * Js * W2;
+    Td11[al] = v1 * A11 + v2 * A11 + v3 * Ad[al][0] + v4 * a11 + v5 * a11 + v6 * G.conatd1[al][0];
+    Td22[al] = v1 * A22 + v2 * A22 + v3 * Ad[al][1] + v4 * a22 + v5 * a22 + v6 * G.conatd1[al][1];
+    Td12[al] = v1 * A12 + v2 * A12 + v3 * Ad[al][2] + v4 * a12 + v5 * a12 + v6 * G.conatd1[al][2];
+  }
+  const T* ch = G.chf;
+  // ch index: (g,b,a) -> (g-1) + 2(b-1) + 4(a-1)
+  const T c111 = ch[0], c211 = ch[1], c121 = ch[2], c221 = ch[3], c112 = ch[4], c212 = ch[5], c122 = ch[6],
+          c222 = ch[7];
+  const T q1 = Td11[0] + Td12[1] + c111 * T11 + c211 * T12 + c122 * T11 + c222 * T12 + c111 * T11 + c211 * T12 +
+               c112 * T12 + c212 * T22;
+  const T q2 = Td12[0] + Td22[1] + c111 * T12 + c211 * T22 + c122 * T12 + c222 * T22 + c121 * T11 + c221 * T12 +
+               c122 * T12 + c222 * T22;
+  const T q3 = T11 * G.bcur[0] + T22 * G.bcur[1] + T(2) * T12 * G.bcur[2];
+  for (int c = 0; c < 3; ++c) f[c] = q1 * G.a1[c] + q2 * G.a2[c] + q3 * G.n[c];
+}
+
+// ------------------------------------------------- membrane pointwise -----
+// One block per item of `nrows` dealias rows of one capsule.  Synthesises the
+// 15 basis fields of cal_co_tang_basis2 (sph3.f90:111-134) from the Legendre
+// output G, adds the reference sphere's analytic part, evaluates geometry and
+// mechanics, and takes the forward DFT of force and normal.
+template <class T>
+__global__ void __launch_bounds__(128) membrane_kernel(const RowWork* __restrict__ work, int nwork,
+                                                       const CapInfo* __restrict__ caps,
+                                                       const GroupDev* __restrict__ groups, T hf, T csk) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  const RowWork it = work[blockIdx.x];
+  const CapInfo ci = caps[it.cap];
+  const GroupDev gd = groups[it.group];
+  const int N = gd.N, nD = gd.nD, mD = gd.mD, rows = it.nrows;
+  T* sG = (T*)smem_raw;                      // [rows][18][N]  ((c*2+cs)*3+kind)
+  T* sTrig = sG + rows * 18 * N;             // [2][N][mD]
+  T* sOut = sTrig + 2 * N * mD;              // [rows][6][mD]
+  const T* G = (const T*)gd.buf.G + (long long)ci.gidx * 6 * N * 3 * nD;
+  const T* trig = (const T*)gd.trigD[pidx<T>()];
+  const T* lat = (const T*)gd.latD[pidx<T>()];
+  const int tid = threadIdx.x;
+  for (int q = tid; q < rows * 18 * N; q += blockDim.x) {
+    const int m = q % N, rest = q / N, kind = rest % 3, ccs = (rest / 3) % 6, r = rest / 18;
+    sG[q] = G[((long long)ccs * N + m) * 3 * nD + kind * nD + it.row0 + r];
+  }
+  for (int q = tid; q < 2 * N * mD; q += blockDim.x) sTrig[q] = trig[q];
+  __syncthreads();
+  const int r = tid / mD, j = tid % mD;
+  if (r < rows) {
+    const int i = it.row0 + r;
+    const T st = lat[4 * i], ct = lat[4 * i + 1];
+    const T R = (T)ci.R;
+    const T cp = sTrig[1 * mD + j], sp = sTrig[N * mD + 1 * mD + j];
+    Geo<T> Gm;
+    // reference sphere: a1 = x_t, a2 = x_p and second derivatives (sph.f90:84-86)
+    Gm.a1[0] = R * (ct * sp); Gm.a1[1] = R * (ct * cp); Gm.a1[2] = -R * st;
+    Gm.a2[0] = R * (st * cp); Gm.a2[1] = -R * (st * sp); Gm.a2[2] = T(0);
+    Gm.d11[0] = -R * (st * sp); Gm.d11[1] = -R * (st * cp); Gm.d11[2] = -R * ct;
+    Gm.d12[0] = R * (ct * cp); Gm.d12[1] = -R * (ct * sp); Gm.d12[2] = T(0);
+    Gm.d22[0] = -R * (st * sp); Gm.d22[1] = -R * (st * cp); Gm.d22[2] = T(0);
+    const T* g = sG + r * 18 * N;
+    for (int c = 0; c < 3; ++c) {
+      const T* gc = g + (c * 2 + 0) * 3 * N;  // cos rows: kind 0,1,2
+      const T* gs = g + (c * 2 + 1) * 3 * N;  // sin rows
+      T v1 = 0, v2 = 0, v11 = 0, v12 = 0, v22 = 0;
+      for (int m = 0; m < N; ++m) {
+        const T cm = sTrig[m * mD + j], sm = sTrig[N * mD + m * mD + j];
+        const T P_a = gc[m], P_b = gs[m];
+        const T D_a = gc[N + m], D_b = gs[N + m];
+        const T E_a = gc[2 * N + m], E_b = gs[2 * N + m];
+        const T fm = (T)m;
+        const T t0P = P_a * cm - P_b * sm;
+        const T t1P = fm * (P_a * (-sm) - P_b * cm);
+        v1 += D_a * cm - D_b * sm;               // vat1 = sum dP * parthe0
+        v2 += t1P;                               // vat2 = sum P * parthe1
+        v11 += E_a * cm - E_b * sm;              // deFvat1(:,1) = sum d2P * parthe0
+        v12 += fm * (D_a * (-sm) - D_b * cm);    // deFvat1(:,2) = sum dP * parthe1
+        v22 += -fm * fm * t0P;                   // deFvat2(:,2) = sum P * parthe2
+      }
+      Gm.a1[c] += v1;
+      Gm.a2[c] += v2;
+      Gm.d11[c] += v11;
+      Gm.d12[c] += v12;
+      Gm.d22[c] += v22;
+    }
+    geometry<T>(Gm);
+    // reference contravariant metric of the sphere: A^11 = 1/R^2,
+    // A^22 = 1/(R^2 sin^2 t), d/dt A^22 = -2 cos t / (R^2 sin^3 t)
+    const T iR2 = T(1) / (R * R);
+    T A[3] = {iR2, iR2 / (st * st), T(0)};
+    T Ad[2][3] = {{T(0), -T(2) * ct * iR2 / (st * st * st), T(0)}, {T(0), T(0), T(0)}};
+    T f[3];
+    mechanics<T>(Gm, A, Ad, hf, csk, f);
+    T* o = sOut + r * 6 * mD;
+    o[0 * mD + j] = f[0];
+    o[1 * mD + j] = f[1];
+    o[2 * mD + j] = f[2];
+    o[3 * mD + j] = Gm.n[0];
+    o[4 * mD + j] = Gm.n[1];
+    o[5 * mD + j] = Gm.n[2];
+  }
+  __syncthreads();
+  // forward DFT of the six outputs (force, normal) per row
+  T* Fout = (T*)gd.buf.Fout + (long long)ci.gidx * 12 * N * nD;
+  const T sfn = T(2) / T(mD);
+  for (int q = tid; q < rows * 6 * N; q += blockDim.x) {
+    const int m = q % N, f = (q / N) % 6, rr = q / (6 * N);
+    const T* o = sOut + (rr * 6 + f) * mD;
+    const T* cs = sTrig + m * mD;
+    const T* sn = sTrig + N * mD + m * mD;
+    T a = 0, b = 0;
+    for (int jj = 0; jj < mD; ++jj) {
+      a += o[jj] * cs[jj];
+      b += o[jj] * sn[jj];
+    }
+    const int i = it.row0 + rr;
+    Fout[((long long)(f * 2 + 0) * N + m) * nD + i] = sfn * a;
+    Fout[((long long)(f * 2 + 1) * N + m) * nD + i] = -sfn * b;
+  }
+}
+
+// ------------------------------------------------- SH-grid stage ----------
+// cal_unitO_filter (sph1.f90:1378-1402): truncated normals on the SH grid,
+// renormalised; cal_surface_metric_sph__OPT (sph3.f90:186-277): |a1 x a2| on
+// the SH grid from the shape coefficients.  Then their forward DFT.
+template <class T>
+__global__ void __launch_bounds__(128) shgrid_kernel(const RowWork* __restrict__ work, int nwork,
+                                                     const CapInfo* __restrict__ caps,
+                                                     const GroupDev* __restrict__ groups) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  const RowWork it = work[blockIdx.x];
+  const CapInfo ci = caps[it.cap];
+  const GroupDev gd = groups[it.group];
+  const int N = gd.N, nO = gd.nO, mO = gd.mO, rows = it.nrows;
+  T* sG = (T*)smem_raw;              // [rows][12][2][N]  (rr, kind, m)
+  T* sTrig = sG + rows * 24 * N;     // [2][N][mO]
+  T* sOut = sTrig + 2 * N * mO;      // [rows][4][mO]
+  const T* GO = (const T*)gd.buf.GO + (long long)ci.gidx * 12 * N * 2 * nO;
+  const T* trig = (const T*)gd.trigO[pidx<T>()];
+  const T* lat = (const T*)gd.latO[pidx<T>()];
+  const int tid = threadIdx.x;
+  for (int q = tid; q < rows * 24 * N; q += blockDim.x) {
+    const int m = q % N, kind = (q / N) % 2, rr = (q / (2 * N)) % 12, r = q / (24 * N);
+    sG[q] = GO[((long long)rr * N + m) * 2 * nO + kind * nO + it.row0 + r];
+  }
+  for (int q = tid; q < 2 * N * mO; q += blockDim.x) sTrig[q] = trig[q];
+  __syncthreads();
+  const int r = tid / mO, j = tid % mO;
+  if (r < rows) {
+    const int i = it.row0 + r;
+    const T st = lat[4 * i], ct = lat[4 * i + 1];
+    const T R = (T)ci.R;
+    const T cp = sTrig[1 * mO + j], sp = sTrig[N * mO + 1 * mO + j];
+    const T* g = sG + r * 24 * N;
+    T nv[3], a1[3] = {R * (ct * sp), R * (ct * cp), -R * st}, a2[3] = {R * (st * cp), -R * (st * sp), T(0)};
+    for (int c = 0; c < 3; ++c) {
+      const T* nc = g + ((c * 2 + 0) * 2 + 0) * N;  // normal comp c, cos, kind P
+      const T* ns = g + ((c * 2 + 1) * 2 + 0) * N;
+      const T* xc = g + (((3 + c) * 2 + 0) * 2) * N;  // shape comp c, cos: kind P at +0, dP at +N
+      const T* xs = g + (((3 + c) * 2 + 1) * 2) * N;
+      T vn = 0, v1 = 0, v2 = 0;
+      for (int m = 0; m < N; ++m) {
+        const T cm = sTrig[m * mO + j], sm = sTrig[N * mO + m * mO + j];
+        vn += nc[m] * cm - ns[m] * sm;
+        v1 += xc[N + m] * cm - xs[N + m] * sm;
+        v2 += (T)m * (xc[m] * (-sm) - xs[m] * cm);
+      }
+      nv[c] = vn;
+      a1[c] += v1;
+      a2[c] += v2;
+    }
+    const T rn = sqrt(nv[0] * nv[0] + nv[1] * nv[1] + nv[2] * nv[2]);
+    T cc[3];
+    cross3(a1, a2, cc);
+    T* o = sOut + r * 4 * mO;
+    o[0 * mO + j] = nv[0] / rn;
+    o[1 * mO + j] = nv[1] / rn;
+    o[2 * mO + j] = nv[2] / rn;
+    o[3 * mO + j] = sqrt(cc[0] * cc[0] + cc[1] * cc[1] + cc[2] * cc[2]);
+  }
+  __syncthreads();
+  T* Fsh = (T*)gd.buf.Fsh + (long long)ci.gidx * 8 * N * nO;
+  const T sfn = T(2) / T(mO);
+  for (int q = tid; q < rows * 4 * N; q += blockDim.x) {
+    const int m = q % N, f = (q / N) % 4, rr = q / (4 * N);
+    const T* o = sOut + (rr * 4 + f) * mO;
+    const T* cs = sTrig + m * mO;
+    const T* sn = sTrig + N * mO + m * mO;
+    T a = 0, b = 0;
+    for (int jj = 0; jj < mO; ++jj) {
+      a += o[jj] * cs[jj];
+      b += o[jj] * sn[jj];
+    }
+    const int i = it.row0 + rr;
+    Fsh[((long long)(f * 2 + 0) * N + m) * nO + i] = sfn * a;
+    Fsh[((long long)(f * 2 + 1) * N + m) * nO + i] = -sfn * b;
+  }
+}
+
+// ------------------------------------------------- final synthesis --------
+// TRSSPH SH grid -> force grid of force, normals and surface metric
+// (forcing.f90:67-88), area = surfmetDf * wgtdsinf (forcing.f90:91).
+template <class T>
+__global__ void __launch_bounds__(128) final_kernel(const RowWork* __restrict__ work, int nwork,
+                                                    const CapInfo* __restrict__ caps,
+                                                    const GroupDev* __restrict__ groups, T* __restrict__ FX,
+                                                    T* __restrict__ FY, T* __restrict__ FZ, T* __restrict__ NX,
+                                                    T* __restrict__ NY, T* __restrict__ NZ, T* __restrict__ AREA) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  const RowWork it = work[blockIdx.x];
+  const CapInfo ci = caps[it.cap];
+  const GroupDev gd = groups[it.group];
+  const int N = gd.N, nD = gd.nD, mD = gd.mD, rows = it.nrows;
+  T* sG = (T*)smem_raw;            // [rows][14][N]
+  T* sTrig = sG + rows * 14 * N;   // [2][N][mD]
+  const T* GF = (const T*)gd.buf.GF + (long long)ci.gidx * 14 * N * nD;
+  const T* trig = (const T*)gd.trigD[pidx<T>()];
+  const T* lat = (const T*)gd.latD[pidx<T>()];
+  const int tid = threadIdx.x;
+  for (int q = tid; q < rows * 14 * N; q += blockDim.x) {
+    const int m = q % N, rr = (q / N) % 14, r = q / (14 * N);
+    sG[q] = GF[((long long)rr * N + m) * nD + it.row0 + r];
+  }
+  for (int q = tid; q < 2 * N * mD; q += blockDim.x) sTrig[q] = trig[q];
+  __syncthreads();
+  const int r = tid / mD, j = tid % mD;
+  if (r >= rows) return;
+  const int i = it.row0 + r;
+  const T* g = sG + r * 14 * N;
+  T v[7];
+  for (int f = 0; f < 7; ++f) {
+    const T* a = g + (2 * f) * N;
+    const T* b = g + (2 * f + 1) * N;
+    T s = 0;
+    for (int m = 0; m < N; ++m) s += a[m] * sTrig[m * mD + j] - b[m] * sTrig[N * mD + m * mD + j];
+    v[f] = s;
+  }
+  const long long p = ci.pt_off + (long long)i * mD + j;
+  FX[p] = v[0];
+  FY[p] = v[1];
+  FZ[p] = v[2];
+  NX[p] = v[3];
+  NY[p] = v[4];
+  NZ[p] = v[5];
+  AREA[p] = v[6] * lat[4 * i + 2];
+}
+
+// ------------------------------------------------- launchers --------------
+template <class T>
+cudaError_t launch_centroid(int ncap, const CapInfo* caps, const double* X, const double* Y, const double* Z,
+                            double* cen, cudaStream_t st) {
+  if (ncap <= 0) return cudaSuccess;
+  centroid_kernel<<<ncap, 256, 0, st>>>(ncap, caps, X, Y, Z, cen);
+  return cudaGetLastError();
+}
+
+template <class T>
+cudaError_t launch_posfwd(const RowWork* work, int nwork, const CapInfo* caps, const GroupDev* groups, const double* X,
+                          const double* Y, const double* Z, const double* cen, cudaStream_t st) {
+  if (nwork <= 0) return cudaSuccess;
+  posfwd_kernel<T><<<(nwork + 3) / 4, 128, 0, st>>>(work, nwork, caps, groups, X, Y, Z, cen);
+  return cudaGetLastError();
+}
+
+// Shared memory of the pointwise kernels for degrees up to nmax (rows*mD <= 128):
+// Legendre rows (<= 1536 el.) + trig tables 2*N*4N + outputs (<= 6*128).
+template <class T>
+size_t pointwise_smem(int nmax) {
+  return sizeof(T) * (size_t)(1536 + 8 * nmax * nmax + 768);
+}
+
+template <class T>
+cudaError_t launch_membrane(const RowWork* work, int nwork, const CapInfo* caps, const GroupDev* groups, double gs,
+                            double csk, int nmax, cudaStream_t st) {
+  if (nwork <= 0) return cudaSuccess;
+  size_t smem = pointwise_smem<T>(nmax);
+  cudaError_t e = cudaFuncSetAttribute(membrane_kernel<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  if (e != cudaSuccess) return e;
+  // hf_gscell = 0.5 * gscell (sph.f90:35)
+  membrane_kernel<T><<<nwork, 128, smem, st>>>(work, nwork, caps, groups, (T)(0.5 * gs), (T)csk);
+  return cudaGetLastError();
+}
+
+template <class T>
+cudaError_t launch_shgrid(const RowWork* work, int nwork, const CapInfo* caps, const GroupDev* groups, int nmax,
+                          cudaStream_t st) {
+  if (nwork <= 0) return cudaSuccess;
+  size_t smem = pointwise_smem<T>(nmax);
+  cudaError_t e = cudaFuncSetAttribute(shgrid_kernel<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  if (e != cudaSuccess) return e;
+  shgrid_kernel<T><<<nwork, 128, smem, st>>>(work, nwork, caps, groups);
+  return cudaGetLastError();
+}
+
+template <class T>
+cudaError_t launch_final(const RowWork* work, int nwork, const CapInfo* caps, const GroupDev* groups, T* FX, T* FY,
+                         T* FZ, T* NX, T* NY, T* NZ, T* AREA, int nmax, cudaStream_t st) {
+  if (nwork <= 0) return cudaSuccess;
+  size_t smem = pointwise_smem<T>(nmax);
+  cudaError_t e = cudaFuncSetAttribute(final_kernel<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  if (e != cudaSuccess) return e;
+  final_kernel<T><<<nwork, 128, smem, st>>>(work, nwork, caps, groups, FX, FY, FZ, NX, NY, NZ, AREA);
+  return cudaGetLastError();
+}
+
+#define SG_INST(T)                                                                                                    \
+  template cudaError_t launch_centroid<T>(int, const CapInfo*, const double*, const double*, const double*, double*, \
+                                          cudaStream_t);                                                            \
+  template cudaError_t launch_posfwd<T>(const RowWork*, int, const CapInfo*, const GroupDev*, const double*,         \
+                                        const double*, const double*, const double*, cudaStream_t);                 \
+  template cudaError_t launch_membrane<T>(const RowWork*, int, const CapInfo*, const GroupDev*, double, double, int, \
+                                          cudaStream_t);                                                            \
+  template cudaError_t launch_shgrid<T>(const RowWork*, int, const CapInfo*, const GroupDev*, int, cudaStream_t);    \
+  template cudaError_t launch_final<T>(const RowWork*, int, const CapInfo*, const GroupDev*, T*, T*, T*, T*, T*, T*,  \
+                                       T*, int, cudaStream_t);
+SG_INST(double)
+SG_INST(float)
+
+}  // namespace sg
