@@ -153,153 +153,6 @@ __global__ void __launch_bounds__(256) interp_kernel(IBGrid g, long n, const int
   W[p] = sw;
 }
 
-// ------------------------------------------------------------------ spread
-// One CTA per output tile of TX x TY x TZ interior cells.  Every point whose
-// stencil reaches the tile is one of the tile's entries.  Contributions
-// f*area/dV * phi*phi*phi (interp_spread.f90:870-874) are quantised to 64-bit
-// fixed point with a per-tile power-of-two scale and summed with integer
-// atomics in shared memory: integer addition is exact and associative, so
-// the result is bitwise independent of the order (no float atomics, fully
-// deterministic).  The scale keeps |sum| < 2^60 from the tile's largest
-// contribution times its entry count.  lagr2eulr zeroes the whole field
-// (interp_spread.f90:811-815), so untouched cells are written as zero.
-template <class T, int TX, int TY, int TZ>
-__global__ void __launch_bounds__(256) spread_kernel(IBGrid g, const int* __restrict__ entries,
-                                                     const int* __restrict__ starts, const int* __restrict__ bx,
-                                                     const int* __restrict__ by, const int* __restrict__ bz,
-                                                     const T* __restrict__ fx, const T* __restrict__ fy,
-                                                     const T* __restrict__ fz, const T* __restrict__ FX,
-                                                     const T* __restrict__ FY, const T* __restrict__ FZ,
-                                                     const T* __restrict__ AREA, T* __restrict__ ox,
-                                                     T* __restrict__ oy, T* __restrict__ oz) {
-  constexpr int NC = TX * TY * TZ;
-  __shared__ unsigned long long acc[3][NC];
-  __shared__ T s_max[8];
-  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-  const int tile = blockIdx.x;
-  const int tx = tile % g.ntx, ty = (tile / g.ntx) % g.nty, tz = tile / (g.ntx * g.nty);
-  const int cw = min(TX, g.itot - TX * tx), ch = min(TY, g.jtot - TY * ty), cd = min(TZ, g.ktot - TZ * tz);
-  const int i0 = 1 + TX * tx, j0 = 1 + TY * ty, k0 = 1 + TZ * tz;
-  const int e0 = starts[tile], e1 = starts[tile + 1];
-  for (int q = tid; q < 3 * NC; q += 256) (&acc[0][0])[q] = 0ull;
-  // pass 1: largest |f * area / dV| of the tile's entries -> fixed-point scale
-  T mx = T(0);
-  for (int e = e0 + tid; e < e1; e += 256) {
-    const int p = entries[e];
-    const T s = fabs(AREA[p] * (T)g.dvi);
-    mx = fmax(mx, fmax(fabs(FX[p]) * s, fmax(fabs(FY[p]) * s, fabs(FZ[p]) * s)));
-  }
-#pragma unroll
-  for (int o = 16; o > 0; o >>= 1) mx = fmax(mx, __shfl_xor_sync(0xffffffffu, mx, o));
-  if (lane == 0) s_max[warp] = mx;
-  __syncthreads();
-  mx = s_max[0];
-#pragma unroll
-  for (int q = 1; q < 8; ++q) mx = fmax(mx, s_max[q]);
-  const double bound = (double)mx * (double)max(1, e1 - e0);
-  int ex = 0;
-  if (bound > 0.0) frexp(bound, &ex);  // bound < 2^ex
-  const double scale = ldexp(1.0, 60 - ex);
-  const double iscale = ldexp(1.0, ex - 60);
-  // pass 2: contributions
-  for (int e = e0 + tid; e < e1; e += 256) {
-    const int p = entries[e];
-    const T f0 = fx[p], f1 = fy[p], f2 = fz[p];
-    const int b0 = bx[p], b1 = by[p], b2 = bz[p];
-    const T s = AREA[p] * (T)g.dvi;
-    const T cu = FX[p] * s, cv = FY[p] * s, cwv = FZ[p] * s;
-    T wfx[4], wcx[4], wfy[4], wcy[4], wfz[4], wcz[4];
-    int li[4], lj[4], lk[4];
-#pragma unroll
-    for (int t = 0; t < 4; ++t) {
-      wfx[t] = delta3<T>(T(t - 1) - f0);
-      wcx[t] = delta3<T>(T(t - 1) - T(0.5) - f0);
-      wfy[t] = delta3<T>(T(t - 1) - f1);
-      wcy[t] = delta3<T>(T(t - 1) - T(0.5) - f1);
-      wfz[t] = delta3<T>(T(t - 1) - f2);
-      wcz[t] = delta3<T>(T(t - 1) - T(0.5) - f2);
-      const int a = wrap_near(b0 + t - 1, g.itot) - i0;
-      const int b = wrap_near(b1 + t - 1, g.jtot) - j0;
-      const int c = b2 + t - 1 - k0;  // z cells outside [1, ktot] fall outside every tile
-      li[t] = (a >= 0 && a < cw) ? a : -1;
-      lj[t] = (b >= 0 && b < ch) ? b : -1;
-      lk[t] = (c >= 0 && c < cd && b2 + t - 1 >= 1 && b2 + t - 1 <= g.ktot) ? c : -1;
-    }
-#pragma unroll
-    for (int tk = 0; tk < 4; ++tk) {
-      if (lk[tk] < 0) continue;
-#pragma unroll
-      for (int tj = 0; tj < 4; ++tj) {
-        if (lj[tj] < 0) continue;
-        const int rowc = TX * (lj[tj] + TY * lk[tk]);
-#pragma unroll
-        for (int ti = 0; ti < 4; ++ti) {
-          if (li[ti] < 0) continue;
-          const int cell = rowc + li[ti];
-          const T wu = wfx[ti] * wcy[tj] * wcz[tk];
-          const T wv = wcx[ti] * wfy[tj] * wcz[tk];
-          const T ww = wcx[ti] * wcy[tj] * wfz[tk];
-          if (wu != T(0)) atomicAdd(&acc[0][cell], (unsigned long long)__double2ll_rn((double)(cu * wu) * scale));
-          if (wv != T(0)) atomicAdd(&acc[1][cell], (unsigned long long)__double2ll_rn((double)(cv * wv) * scale));
-          if (ww != T(0)) atomicAdd(&acc[2][cell], (unsigned long long)__double2ll_rn((double)(cwv * ww) * scale));
-        }
-      }
-    }
-  }
-  __syncthreads();
-  // write the tile, its periodic halo copies (bound.f90:153-187) and, on the
-  // z-boundary tiles, the zero z-halo planes.
-  for (int q = tid; q < NC; q += 256) {
-    const int lx = q % TX, ly = (q / TX) % TY, lz = q / (TX * TY);
-    if (lx >= cw || ly >= ch || lz >= cd) continue;
-    const int i = i0 + lx, j = j0 + ly, k = k0 + lz;
-    const T vu = (T)((double)(long long)acc[0][q] * iscale);
-    const T vv = (T)((double)(long long)acc[1][q] * iscale);
-    const T vw = (T)((double)(long long)acc[2][q] * iscale);
-    int is[2] = {i, -1}, js[2] = {j, -1};
-    if (i == g.itot) is[1] = 0;
-    if (i == 1) is[1] = g.itot + 1;
-    if (j == g.jtot) js[1] = 0;
-    if (j == 1) js[1] = g.jtot + 1;
-    for (int a = 0; a < 2; ++a) {
-      if (is[a] < 0) continue;
-      for (int b = 0; b < 2; ++b) {
-        if (js[b] < 0) continue;
-        const long long o = fidx(is[a], js[b], k, g.ldi, g.ldj);
-        ox[o] = vu;
-        oy[o] = vv;
-        oz[o] = vw;
-      }
-    }
-  }
-  if (tz == 0 || tz == g.ntz - 1) {
-    for (int q = tid; q < TX * TY; q += 256) {
-      const int lx = q % TX, ly = q / TX;
-      if (lx >= cw || ly >= ch) continue;
-      const int i = i0 + lx, j = j0 + ly;
-      int is[2] = {i, -1}, js[2] = {j, -1};
-      if (i == g.itot) is[1] = 0;
-      if (i == 1) is[1] = g.itot + 1;
-      if (j == g.jtot) js[1] = 0;
-      if (j == 1) js[1] = g.jtot + 1;
-      for (int a = 0; a < 2; ++a) {
-        if (is[a] < 0) continue;
-        for (int b = 0; b < 2; ++b) {
-          if (js[b] < 0) continue;
-          if (tz == 0) {
-            const long long o = fidx(is[a], js[b], 0, g.ldi, g.ldj);
-            ox[o] = T(0); oy[o] = T(0); oz[o] = T(0);
-          }
-          if (tz == g.ntz - 1) {
-            const long long o = fidx(is[a], js[b], g.ktot + 1, g.ldi, g.ldj);
-            ox[o] = T(0); oy[o] = T(0); oz[o] = T(0);
-          }
-        }
-      }
-    }
-  }
-}
-
 // ------------------------------------------------------------------ launchers
 template <class T>
 cudaError_t launch_bin(const IBGrid& g, long n, const double* X, const double* Y, const double* Z, IBWork& w,
@@ -325,18 +178,6 @@ cudaError_t launch_interp(const IBGrid& g, long n, const IBWork& w, const T* u, 
   return cudaGetLastError();
 }
 
-template <class T>
-cudaError_t launch_spread(const IBGrid& g, const IBWork& w, const T* FX, const T* FY, const T* FZ, const T* A, T* ox,
-                          T* oy, T* oz, cudaStream_t st) {
-  if (g.TX == 32)
-    spread_kernel<T, 32, 8, 4><<<g.ntiles, 256, 0, st>>>(g, w.entries, w.starts, w.bx, w.by, w.bz, (const T*)w.fx,
-                                                          (const T*)w.fy, (const T*)w.fz, FX, FY, FZ, A, ox, oy, oz);
-  else
-    spread_kernel<T, 8, 8, 4><<<g.ntiles, 256, 0, st>>>(g, w.entries, w.starts, w.bx, w.by, w.bz, (const T*)w.fx,
-                                                         (const T*)w.fy, (const T*)w.fz, FX, FY, FZ, A, ox, oy, oz);
-  return cudaGetLastError();
-}
-
 template cudaError_t launch_bin<double>(const IBGrid&, long, const double*, const double*, const double*, IBWork&,
                                         cudaStream_t);
 template cudaError_t launch_bin<float>(const IBGrid&, long, const double*, const double*, const double*, IBWork&,
@@ -345,10 +186,6 @@ template cudaError_t launch_interp<double>(const IBGrid&, long, const IBWork&, c
                                            const double*, double*, double*, double*, cudaStream_t);
 template cudaError_t launch_interp<float>(const IBGrid&, long, const IBWork&, const float*, const float*, const float*,
                                           float*, float*, float*, cudaStream_t);
-template cudaError_t launch_spread<double>(const IBGrid&, const IBWork&, const double*, const double*, const double*,
-                                           const double*, double*, double*, double*, cudaStream_t);
-template cudaError_t launch_spread<float>(const IBGrid&, const IBWork&, const float*, const float*, const float*,
-                                          const float*, float*, float*, float*, cudaStream_t);
 
 bool make_ib_grid(int itot, int jtot, int ktot, double lx, double ly, double lz, IBGrid& g) {
   if (itot < 8 || jtot < 8 || ktot < 1) return false;

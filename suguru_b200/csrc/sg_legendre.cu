@@ -27,26 +27,28 @@ __global__ void __launch_bounds__(256) legendre_kernel(const LegProblem* __restr
   T* sB = (T*)smem_raw;       // [J][Kp]
   T* sA = sB + J * Kp;        // [QT][Kp]
   const T* B = (const T*)P.B + (long long)m * P.sBm;
-  for (int e = threadIdx.x; e < J * K; e += blockDim.x) {
-    const int j = e / K, k = e % K;
-    sB[j * Kp + k] = B[e];
-  }
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarp = blockDim.x >> 5;
+  // warp per row, lanes along K: no integer division by runtime values
+  for (int j = warp; j < J; j += nwarp)
+    for (int k = lane; k < K; k += 32) sB[j * Kp + k] = B[(long long)j * K + k];
   const T* A = (const T*)P.A;
-  for (int e = threadIdx.x; e < nq * K; e += blockDim.x) {
-    const int q = e / K, k = e % K;
-    const int qq = q0 + q, c = qq / P.rpc, r = qq % P.rpc;
-    sA[q * Kp + k] = A[(long long)c * P.sAc + (long long)r * P.sAr + (long long)m * P.sAm + k];
+  for (int q = warp; q < nq; q += nwarp) {
+    const int qq = q0 + q, c = qq / P.rpc, r = qq - c * P.rpc;
+    const T* arow = A + (long long)c * P.sAc + (long long)r * P.sAr + (long long)m * P.sAm;
+    for (int k = lane; k < K; k += 32) sA[q * Kp + k] = arow[k];
   }
   __syncthreads();
   T* D = (T*)P.D;
-  for (int e = threadIdx.x; e < nq * J; e += blockDim.x) {
-    const int q = e / J, j = e % J;
+  for (int q = warp; q < nq; q += nwarp) {
+    const int qq = q0 + q, c = qq / P.rpc, r = qq - c * P.rpc;
+    T* drow = D + (long long)c * P.sDc + (long long)r * P.sDr + (long long)m * P.sDm;
     const T* a = sA + q * Kp;
-    const T* b = sB + j * Kp;
-    T s = 0;
-    for (int k = k0; k < K; ++k) s += a[k] * b[k];
-    const int qq = q0 + q, c = qq / P.rpc, r = qq % P.rpc;
-    D[(long long)c * P.sDc + (long long)r * P.sDr + (long long)m * P.sDm + j] = s;
+    for (int j = lane; j < J; j += 32) {
+      const T* b = sB + j * Kp;
+      T s = 0;
+      for (int k = k0; k < K; ++k) s += a[k] * b[k];
+      drow[j] = s;
+    }
   }
 }
 

@@ -277,23 +277,26 @@ __global__ void __launch_bounds__(128) membrane_kernel(const RowWork* __restrict
   const int N = gd.N, nD = gd.nD, mD = gd.mD, rows = it.nrows;
   T* sG = (T*)smem_raw;                      // [rows][18][N]  ((c*2+cs)*3+kind)
   T* sTrig = sG + rows * 18 * N;             // [2][N][mD]
-  T* sOut = sTrig + 2 * N * mD;              // [rows][6][mD]
+  T* sOut = sTrig + 2 * N * (mD + 1);              // [rows][6][mD]
   const T* G = (const T*)gd.buf.G + (long long)ci.gidx * 6 * N * 3 * nD;
   const T* trig = (const T*)gd.trigD[pidx<T>()];
   const T* lat = (const T*)gd.latD[pidx<T>()];
-  const int tid = threadIdx.x;
-  for (int q = tid; q < rows * 18 * N; q += blockDim.x) {
-    const int m = q % N, rest = q / N, kind = rest % 3, ccs = (rest / 3) % 6, r = rest / 18;
-    sG[q] = G[((long long)ccs * N + m) * 3 * nD + kind * nD + it.row0 + r];
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5, nwarp = blockDim.x >> 5;
+  // one warp per (row, comp/cs, kind) line of N values; divisions by constants only
+  for (int line = warp; line < rows * 18; line += nwarp) {
+    const int kind = line % 3, ccs = (line / 3) % 6, r = line / 18;
+    for (int m = lane; m < N; m += 32)
+      sG[line * N + m] = G[((long long)ccs * N + m) * 3 * nD + kind * nD + it.row0 + r];
   }
-  for (int q = tid; q < 2 * N * mD; q += blockDim.x) sTrig[q] = trig[q];
+  for (int hm = warp; hm < 2 * N; hm += nwarp)
+    for (int j = lane; j < mD; j += 32) sTrig[hm * (mD + 1) + j] = trig[hm * mD + j];
   __syncthreads();
   const int r = tid / mD, j = tid % mD;
   if (r < rows) {
     const int i = it.row0 + r;
     const T st = lat[4 * i], ct = lat[4 * i + 1];
     const T R = (T)ci.R;
-    const T cp = sTrig[1 * mD + j], sp = sTrig[N * mD + 1 * mD + j];
+    const T cp = sTrig[1 * (mD + 1) + j], sp = sTrig[(N + 1) * (mD + 1) + j];
     Geo<T> Gm;
     // reference sphere: a1 = x_t, a2 = x_p and second derivatives (sph.f90:84-86)
     Gm.a1[0] = R * (ct * sp); Gm.a1[1] = R * (ct * cp); Gm.a1[2] = -R * st;
@@ -307,7 +310,7 @@ __global__ void __launch_bounds__(128) membrane_kernel(const RowWork* __restrict
       const T* gs = g + (c * 2 + 1) * 3 * N;  // sin rows
       T v1 = 0, v2 = 0, v11 = 0, v12 = 0, v22 = 0;
       for (int m = 0; m < N; ++m) {
-        const T cm = sTrig[m * mD + j], sm = sTrig[N * mD + m * mD + j];
+        const T cm = sTrig[m * (mD + 1) + j], sm = sTrig[(N + m) * (mD + 1) + j];
         const T P_a = gc[m], P_b = gs[m];
         const T D_a = gc[N + m], D_b = gs[N + m];
         const T E_a = gc[2 * N + m], E_b = gs[2 * N + m];
@@ -334,23 +337,24 @@ __global__ void __launch_bounds__(128) membrane_kernel(const RowWork* __restrict
     T Ad[2][3] = {{T(0), -T(2) * ct * iR2 / (st * st * st), T(0)}, {T(0), T(0), T(0)}};
     T f[3];
     mechanics<T>(Gm, A, Ad, hf, csk, f);
-    T* o = sOut + r * 6 * mD;
-    o[0 * mD + j] = f[0];
-    o[1 * mD + j] = f[1];
-    o[2 * mD + j] = f[2];
-    o[3 * mD + j] = Gm.n[0];
-    o[4 * mD + j] = Gm.n[1];
-    o[5 * mD + j] = Gm.n[2];
+    T* o = sOut + r * 6 * (mD + 1);
+    o[0 * (mD + 1) + j] = f[0];
+    o[1 * (mD + 1) + j] = f[1];
+    o[2 * (mD + 1) + j] = f[2];
+    o[3 * (mD + 1) + j] = Gm.n[0];
+    o[4 * (mD + 1) + j] = Gm.n[1];
+    o[5 * (mD + 1) + j] = Gm.n[2];
   }
   __syncthreads();
   // forward DFT of the six outputs (force, normal) per row
   T* Fout = (T*)gd.buf.Fout + (long long)ci.gidx * 12 * N * nD;
   const T sfn = T(2) / T(mD);
-  for (int q = tid; q < rows * 6 * N; q += blockDim.x) {
-    const int m = q % N, f = (q / N) % 6, rr = q / (6 * N);
-    const T* o = sOut + (rr * 6 + f) * mD;
-    const T* cs = sTrig + m * mD;
-    const T* sn = sTrig + N * mD + m * mD;
+  // lane = m (N <= 32), warp = (row, field) line
+  for (int line = warp; line < rows * 6 && lane < N; line += nwarp) {
+    const int m = lane, f = line % 6, rr = line / 6;
+    const T* o = sOut + (rr * 6 + f) * (mD + 1);
+    const T* cs = sTrig + m * (mD + 1);
+    const T* sn = sTrig + (N + m) * (mD + 1);
     T a = 0, b = 0;
     for (int jj = 0; jj < mD; ++jj) {
       a += o[jj] * cs[jj];
@@ -377,23 +381,25 @@ __global__ void __launch_bounds__(128) shgrid_kernel(const RowWork* __restrict__
   const int N = gd.N, nO = gd.nO, mO = gd.mO, rows = it.nrows;
   T* sG = (T*)smem_raw;              // [rows][12][2][N]  (rr, kind, m)
   T* sTrig = sG + rows * 24 * N;     // [2][N][mO]
-  T* sOut = sTrig + 2 * N * mO;      // [rows][4][mO]
+  T* sOut = sTrig + 2 * N * (mO + 1);      // [rows][4][mO]
   const T* GO = (const T*)gd.buf.GO + (long long)ci.gidx * 12 * N * 2 * nO;
   const T* trig = (const T*)gd.trigO[pidx<T>()];
   const T* lat = (const T*)gd.latO[pidx<T>()];
-  const int tid = threadIdx.x;
-  for (int q = tid; q < rows * 24 * N; q += blockDim.x) {
-    const int m = q % N, kind = (q / N) % 2, rr = (q / (2 * N)) % 12, r = q / (24 * N);
-    sG[q] = GO[((long long)rr * N + m) * 2 * nO + kind * nO + it.row0 + r];
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5, nwarp = blockDim.x >> 5;
+  for (int line = warp; line < rows * 24; line += nwarp) {
+    const int kind = line % 2, rr = (line / 2) % 12, r = line / 24;
+    for (int m = lane; m < N; m += 32)
+      sG[line * N + m] = GO[((long long)rr * N + m) * 2 * nO + kind * nO + it.row0 + r];
   }
-  for (int q = tid; q < 2 * N * mO; q += blockDim.x) sTrig[q] = trig[q];
+  for (int hm = warp; hm < 2 * N; hm += nwarp)
+    for (int j = lane; j < mO; j += 32) sTrig[hm * (mO + 1) + j] = trig[hm * mO + j];
   __syncthreads();
   const int r = tid / mO, j = tid % mO;
   if (r < rows) {
     const int i = it.row0 + r;
     const T st = lat[4 * i], ct = lat[4 * i + 1];
     const T R = (T)ci.R;
-    const T cp = sTrig[1 * mO + j], sp = sTrig[N * mO + 1 * mO + j];
+    const T cp = sTrig[1 * (mO + 1) + j], sp = sTrig[(N + 1) * (mO + 1) + j];
     const T* g = sG + r * 24 * N;
     T nv[3], a1[3] = {R * (ct * sp), R * (ct * cp), -R * st}, a2[3] = {R * (st * cp), -R * (st * sp), T(0)};
     for (int c = 0; c < 3; ++c) {
@@ -403,7 +409,7 @@ __global__ void __launch_bounds__(128) shgrid_kernel(const RowWork* __restrict__
       const T* xs = g + (((3 + c) * 2 + 1) * 2) * N;
       T vn = 0, v1 = 0, v2 = 0;
       for (int m = 0; m < N; ++m) {
-        const T cm = sTrig[m * mO + j], sm = sTrig[N * mO + m * mO + j];
+        const T cm = sTrig[m * (mO + 1) + j], sm = sTrig[(N + m) * (mO + 1) + j];
         vn += nc[m] * cm - ns[m] * sm;
         v1 += xc[N + m] * cm - xs[N + m] * sm;
         v2 += (T)m * (xc[m] * (-sm) - xs[m] * cm);
@@ -415,20 +421,20 @@ __global__ void __launch_bounds__(128) shgrid_kernel(const RowWork* __restrict__
     const T rn = sqrt(nv[0] * nv[0] + nv[1] * nv[1] + nv[2] * nv[2]);
     T cc[3];
     cross3(a1, a2, cc);
-    T* o = sOut + r * 4 * mO;
-    o[0 * mO + j] = nv[0] / rn;
-    o[1 * mO + j] = nv[1] / rn;
-    o[2 * mO + j] = nv[2] / rn;
-    o[3 * mO + j] = sqrt(cc[0] * cc[0] + cc[1] * cc[1] + cc[2] * cc[2]);
+    T* o = sOut + r * 4 * (mO + 1);
+    o[0 * (mO + 1) + j] = nv[0] / rn;
+    o[1 * (mO + 1) + j] = nv[1] / rn;
+    o[2 * (mO + 1) + j] = nv[2] / rn;
+    o[3 * (mO + 1) + j] = sqrt(cc[0] * cc[0] + cc[1] * cc[1] + cc[2] * cc[2]);
   }
   __syncthreads();
   T* Fsh = (T*)gd.buf.Fsh + (long long)ci.gidx * 8 * N * nO;
   const T sfn = T(2) / T(mO);
-  for (int q = tid; q < rows * 4 * N; q += blockDim.x) {
-    const int m = q % N, f = (q / N) % 4, rr = q / (4 * N);
-    const T* o = sOut + (rr * 4 + f) * mO;
-    const T* cs = sTrig + m * mO;
-    const T* sn = sTrig + N * mO + m * mO;
+  for (int line = warp; line < rows * 4 && lane < N; line += nwarp) {
+    const int m = lane, f = line % 4, rr = line / 4;
+    const T* o = sOut + (rr * 4 + f) * (mO + 1);
+    const T* cs = sTrig + m * (mO + 1);
+    const T* sn = sTrig + (N + m) * (mO + 1);
     T a = 0, b = 0;
     for (int jj = 0; jj < mO; ++jj) {
       a += o[jj] * cs[jj];
@@ -459,10 +465,10 @@ __global__ void __launch_bounds__(128) final_kernel(const RowWork* __restrict__ 
   const T* GF = (const T*)gd.buf.GF + (long long)ci.gidx * 14 * N * nD;
   const T* trig = (const T*)gd.trigD[pidx<T>()];
   const T* lat = (const T*)gd.latD[pidx<T>()];
-  const int tid = threadIdx.x;
-  for (int q = tid; q < rows * 14 * N; q += blockDim.x) {
-    const int m = q % N, rr = (q / N) % 14, r = q / (14 * N);
-    sG[q] = GF[((long long)rr * N + m) * nD + it.row0 + r];
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5, nwarp = blockDim.x >> 5;
+  for (int line = warp; line < rows * 14; line += nwarp) {
+    const int rr = line % 14, r = line / 14;
+    for (int m = lane; m < N; m += 32) sG[line * N + m] = GF[((long long)rr * N + m) * nD + it.row0 + r];
   }
   for (int q = tid; q < 2 * N * mD; q += blockDim.x) sTrig[q] = trig[q];
   __syncthreads();
@@ -509,7 +515,8 @@ cudaError_t launch_posfwd(const RowWork* work, int nwork, const CapInfo* caps, c
 // Legendre rows (<= 1536 el.) + trig tables 2*N*4N + outputs (<= 6*128).
 template <class T>
 size_t pointwise_smem(int nmax) {
-  return sizeof(T) * (size_t)(1536 + 8 * nmax * nmax + 768);
+  // trig and output rows are padded by one element against bank conflicts
+  return sizeof(T) * (size_t)(1536 + 8 * nmax * nmax + 2 * nmax + 1024);
 }
 
 template <class T>
