@@ -46,6 +46,7 @@ extern "C" {
 #define SG_ERR_FALLBACK 4 /* surrogate fallback count above the allowed maximum */
 #define SG_ERR_ARG 5      /* bad argument (null pointer, size) */
 #define SG_ERR_STATE 6    /* call not valid in the current state */
+#define SG_ERR_TOO_LARGE 7 /* problem larger than sg_spread_noalloc's fixed scratch */
 
 #define SG_PREC_FP64 0
 #define SG_PREC_MIXED 1
@@ -111,6 +112,32 @@ int sg_update_pos(sg_ctx* ctx, double dt, double* X, double* Y, double* Z,
 int sg_surf_vol(sg_ctx* ctx, const double* X, const double* Y, const double* Z,
                 const void* NX, const void* NY, const void* NZ, const void* AREA,
                 const double* exy1_prev, double* out);
+
+/* Spreading for callers that cannot allocate device memory.  It has no
+ * counterpart in the reference; it is sg_spread (lagr2eulr) without a
+ * context.  It is for host codes whose device memory is all owned by their
+ * own pool, and for code that must not call cudaMalloc or create an sg_ctx
+ * (sg_create allocates).
+ * The caller passes device arrays: the points X,Y,Z, force FX,FY,FZ and AREA
+ * (npts each, FP64), and the fields fx,fy,fz in the Eulerian layout above.
+ * The binning scratch is one fixed array of SG_NOALLOC_SCRATCH_BYTES compiled
+ * into the library; every GPU that loads the library holds it until exit.
+ * Limits: npts <= SG_NOALLOC_MAX_POINTS and at most SG_NOALLOC_MAX_TILES
+ * output tiles (32x8x4 cells each, 8x8x4 when itot < 32); a larger problem
+ * returns SG_ERR_TOO_LARGE before doing anything.  The first call on a device
+ * looks up the array's device address (cudaGetSymbolAddress), so make that
+ * first call before any stream capture.  Work is queued on `stream` (NULL:
+ * the default stream) and the call returns without waiting.  All calls share
+ * the one array, so calls that overlap on the GPU race; each call clears the
+ * counters it needs, and otherwise the previous call's contents stay there.
+ * Returns SG_OK, SG_ERR_ARG, SG_ERR_TOO_LARGE or SG_ERR_CUDA. */
+#define SG_NOALLOC_MAX_POINTS 65536
+#define SG_NOALLOC_MAX_TILES 16384
+#define SG_NOALLOC_SCRATCH_BYTES (4608u * 1024u)
+int sg_spread_noalloc(int itot, int jtot, int ktot, double lx, double ly, double lz, long npts,
+                      const double* X, const double* Y, const double* Z,
+                      const double* FX, const double* FY, const double* FZ, const double* AREA,
+                      double* fx, double* fy, double* fz, void* stream);
 
 /* Host-side tables (tests): Gauss colatitudes and SPHEREPACK-normalised
  * Legendre functions with theta derivatives, [m*nn+n] layout. */

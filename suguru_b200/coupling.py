@@ -32,7 +32,7 @@ ERRORS = {0: "SG_OK", 1: "SG_ERR_CONFIG", 2: "SG_ERR_CUDA", 3: "SG_ERR_TIMEOUT",
 # every symbol declared in include/sg_coupling.h
 EXPORTS = ["sg_create", "sg_destroy", "sg_last_error", "sg_synchronize", "sg_interp", "sg_membrane_force",
            "sg_spread", "sg_step", "sg_update_pos", "sg_surf_vol", "sg_gauss", "sg_legendre",
-           "sg_last_launch_count", "sg_set_profiling", "sg_stage_times"]
+           "sg_last_launch_count", "sg_set_profiling", "sg_stage_times", "sg_spread_noalloc"]
 STAGES = ("bin", "interp", "membrane", "spread")
 
 
@@ -81,6 +81,8 @@ def lib():
     L.sg_last_launch_count.argtypes = [vp]
     L.sg_set_profiling.argtypes = [vp, ctypes.c_int]
     L.sg_stage_times.argtypes = [vp, ctypes.POINTER(ctypes.c_float), ctypes.c_int]
+    d = ctypes.c_double
+    L.sg_spread_noalloc.argtypes = ([ctypes.c_int] * 3 + [d] * 3 + [ctypes.c_long] + [vp] * 11)
     _LIB = L
     return L
 
