@@ -147,6 +147,37 @@ int sg_legendre(double theta, int mm, int nn, double* P, double* dP, double* d2P
 /* Number of this library's kernels launched by the last step call. */
 int sg_last_launch_count(const sg_ctx* ctx);
 
+/* Spreading tile shape (no counterpart in the reference, whose spreading loops
+ * over points, interp_spread.f90:817-884).  shape indexes the cell tiles
+ * 0: 32x8x4, 1: 16x16x8, 2: 32x8x8, 3: 8x8x4, or -1 for the grid's default;
+ * FP64 contexts take shapes 0 and 3 only.  Results do not depend on the shape
+ * beyond rounding of the per-tile fixed-point scale.  Not allowed while a
+ * graph is captured. */
+int sg_set_tile_shape(sg_ctx* ctx, int shape);
+int sg_get_tile_shape(const sg_ctx* ctx, int* shape, int* tx, int* ty, int* tz);
+
+/* Autotuner: times `reps` sg_step calls with the same arguments for every
+ * tile shape valid for the context, keeps the fastest and returns it with its
+ * milliseconds per step.  The outputs hold the last step's results. */
+int sg_autotune(sg_ctx* ctx, const void* u, const void* v, const void* w,
+                const double* X, const double* Y, const double* Z,
+                void* U, void* V, void* W,
+                void* FX, void* FY, void* FZ, void* NX, void* NY, void* NZ, void* AREA,
+                void* fx, void* fy, void* fz, int reps, int* best_shape, float* best_ms);
+
+/* CUDA graph of one sg_step on fixed device arrays (SG_MEM_DEVICE only): the
+ * capture records every launch of the step on the context stream; each
+ * sg_graph_launch replays it (same pointers, current array contents).
+ * sg_graph_release drops the graph.  The stream must not be the legacy
+ * default stream. */
+int sg_graph_capture(sg_ctx* ctx, const void* u, const void* v, const void* w,
+                     const double* X, const double* Y, const double* Z,
+                     void* U, void* V, void* W,
+                     void* FX, void* FY, void* FZ, void* NX, void* NY, void* NZ, void* AREA,
+                     void* fx, void* fy, void* fz);
+int sg_graph_launch(sg_ctx* ctx);
+int sg_graph_release(sg_ctx* ctx);
+
 /* Stage timing with CUDA events on the context stream.  When enabled, each
  * step call records events around its stages; sg_stage_times returns the last
  * step's milliseconds for SG_STAGE_* (bin, interp, membrane, spread). */

@@ -27,12 +27,15 @@ _LIB = None
 SG_PREC_FP64, SG_PREC_MIXED = 0, 1
 SG_MEM_HOST, SG_MEM_DEVICE = 0, 1
 ERRORS = {0: "SG_OK", 1: "SG_ERR_CONFIG", 2: "SG_ERR_CUDA", 3: "SG_ERR_TIMEOUT", 4: "SG_ERR_FALLBACK",
-          5: "SG_ERR_ARG", 6: "SG_ERR_STATE"}
+          5: "SG_ERR_ARG", 6: "SG_ERR_STATE", 7: "SG_ERR_TOO_LARGE"}
 
 # every symbol declared in include/sg_coupling.h
 EXPORTS = ["sg_create", "sg_destroy", "sg_last_error", "sg_synchronize", "sg_interp", "sg_membrane_force",
            "sg_spread", "sg_step", "sg_update_pos", "sg_surf_vol", "sg_gauss", "sg_legendre",
-           "sg_last_launch_count", "sg_set_profiling", "sg_stage_times", "sg_spread_noalloc"]
+           "sg_last_launch_count", "sg_set_profiling", "sg_stage_times", "sg_spread_noalloc",
+           "sg_set_tile_shape", "sg_get_tile_shape", "sg_autotune", "sg_graph_capture", "sg_graph_launch",
+           "sg_graph_release"]
+TILE_SHAPES = ((32, 8, 4), (16, 16, 8), (32, 8, 8), (8, 8, 4))
 STAGES = ("bin", "interp", "membrane", "spread")
 
 
@@ -81,6 +84,13 @@ def lib():
     L.sg_last_launch_count.argtypes = [vp]
     L.sg_set_profiling.argtypes = [vp, ctypes.c_int]
     L.sg_stage_times.argtypes = [vp, ctypes.POINTER(ctypes.c_float), ctypes.c_int]
+    ip = ctypes.POINTER(ctypes.c_int)
+    L.sg_set_tile_shape.argtypes = [vp, ctypes.c_int]
+    L.sg_get_tile_shape.argtypes = [vp, ip, ip, ip, ip]
+    L.sg_autotune.argtypes = [vp] * 20 + [ctypes.c_int, ip, ctypes.POINTER(ctypes.c_float)]
+    L.sg_graph_capture.argtypes = [vp] * 20
+    L.sg_graph_launch.argtypes = [vp]
+    L.sg_graph_release.argtypes = [vp]
     d = ctypes.c_double
     L.sg_spread_noalloc.argtypes = ([ctypes.c_int] * 3 + [d] * 3 + [ctypes.c_long] + [vp] * 11)
     _LIB = L
@@ -208,6 +218,35 @@ class CouplingStep:
         E = eul_out if eul_out is not None else self._eul(3)
         self._check(lib().sg_step(self._h, *map(_ptr, (u, v, w, X, Y, Z, *L, *E))), "sg_step")
         return dict(u=L[0:3], f=L[3:6], n=L[6:9], area=L[9], fgrid=E)
+
+    def set_tile_shape(self, shape):
+        """Spreading tile shape: index into TILE_SHAPES, or -1 for the default."""
+        self._check(lib().sg_set_tile_shape(self._h, int(shape)), "sg_set_tile_shape")
+
+    def tile_shape(self):
+        v = [ctypes.c_int() for _ in range(4)]
+        self._check(lib().sg_get_tile_shape(self._h, *[ctypes.byref(x) for x in v]), "sg_get_tile_shape")
+        return v[0].value, (v[1].value, v[2].value, v[3].value)
+
+    def autotune(self, u, v, w, X, Y, Z, lag_out=None, eul_out=None, reps=3):
+        """Time `reps` steps per valid tile shape and keep the fastest; returns (shape, ms per step)."""
+        L = lag_out if lag_out is not None else self._lag(10)
+        E = eul_out if eul_out is not None else self._eul(3)
+        best, ms = ctypes.c_int(), ctypes.c_float()
+        self._check(lib().sg_autotune(self._h, *map(_ptr, (u, v, w, X, Y, Z, *L, *E)), int(reps),
+                                      ctypes.byref(best), ctypes.byref(ms)), "sg_autotune")
+        return best.value, ms.value
+
+    def graph_capture(self, u, v, w, X, Y, Z, lag_out, eul_out):
+        """Capture one step on fixed device arrays into a CUDA graph."""
+        self._check(lib().sg_graph_capture(self._h, *map(_ptr, (u, v, w, X, Y, Z, *lag_out, *eul_out))),
+                    "sg_graph_capture")
+
+    def graph_launch(self):
+        self._check(lib().sg_graph_launch(self._h), "sg_graph_launch")
+
+    def graph_release(self):
+        self._check(lib().sg_graph_release(self._h), "sg_graph_release")
 
     def update_pos(self, dt, X, Y, Z, U, V, W):
         """Update_Pos.f90:95-126 -- in place on X, Y, Z."""

@@ -18,6 +18,33 @@ SG_HD T delta3(T r) {
   return (T(1) / T(3)) * (T(1) + sqrt(-T(3) * (r * r) + T(1)));
 }
 
+// The three nonzero values of delta3 around the nearest node, with one square
+// root.  For a node at offset o from the base index and a point at fraction f
+// in [0,1): faces sit at o, cell centres at o - 1/2.  With r = (nearest node)
+// - f, |r| <= 1/2 and s = sqrt(1 - 3 r^2), kernel.f90:7-25 gives
+//   phi(r) = (1 + s)/3,  phi(r - 1) = (2 + 3r - s)/6,  phi(r + 1) = (2 - 3r - s)/6.
+// face: w[t] is the weight of node o = hi - 1 + t, hi = (f >= 1/2);
+// centre: w[t] is the weight of the centre at o = t.
+template <class T>
+SG_HD void delta3_face(T f, T* w, bool& hi) {
+  hi = !(f < T(0.5));
+  const T r = (hi ? T(1) : T(0)) - f;
+  const T s = sqrt(T(1) - T(3) * r * r);
+  w[0] = (T(2) + T(3) * r - s) * (T(1) / T(6));
+  w[1] = (T(1) + s) * (T(1) / T(3));
+  w[2] = (T(2) - T(3) * r - s) * (T(1) / T(6));
+}
+template <class T>
+SG_HD void delta3_centre(T f, T* w) {
+  const T r = T(0.5) - f;
+  const T s = sqrt(T(1) - T(3) * r * r);
+  w[0] = (T(2) + T(3) * r - s) * (T(1) / T(6));
+  w[1] = (T(1) + s) * (T(1) / T(3));
+  w[2] = (T(2) - T(3) * r - s) * (T(1) / T(6));
+}
+
+SG_HD int wrap_near(int r, int n) { return r < 1 ? r + n : (r > n ? r - n : r); }
+
 SG_HD int wrap1(int i, int n) {  // periodic storage index in [1, n]
   int r = (i - 1) % n;
   if (r < 0) r += n;

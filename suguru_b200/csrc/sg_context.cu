@@ -68,6 +68,11 @@ struct sg_ctx {
   bool profiling = false;
   cudaEvent_t ev[SG_NSTAGE + 1] = {};
   bool ev_used[SG_NSTAGE] = {};
+  int max_tiles = 0;            // binning arrays are sized for the largest tile count
+  bool capturing = false;       // inside sg_graph_capture: no synchronisation, no events
+  cudaGraph_t graph = nullptr;  // captured step (device memory mode)
+  cudaGraphExec_t graph_exec = nullptr;
+  int graph_launches = 0;
 };
 
 namespace {
@@ -216,8 +221,11 @@ int setup(sg_ctx* c) {
     SG_TRY(cudaStreamCreateWithFlags(&c->st, cudaStreamNonBlocking), "cudaStreamCreate");
     c->own_stream = true;
   }
-  if (!make_ib_grid(cfg.itot, cfg.jtot, cfg.ktot, cfg.lx, cfg.ly, cfg.lz, c->grid))
-    return fail(c, SG_ERR_CONFIG, "grid too small: need itot, jtot >= 8");
+  // FP32 spreads on 16 x 16 x 8 tiles (fewer points straddle a tile edge);
+  // FP64 keeps 1024-cell tiles for its three-limb shared accumulators
+  const int shape = (c->mixed && cfg.itot >= 16 && cfg.jtot >= 16) ? 1 : -1;
+  if (!make_ib_grid(cfg.itot, cfg.jtot, cfg.ktot, cfg.lx, cfg.ly, cfg.lz, c->grid, shape))
+    return fail(c, SG_ERR_CONFIG, "grid out of range: need itot, jtot >= 8 and (itot+2)(jtot+2)(ktot+2) < 2^31");
   const IBGrid& g = c->grid;
   c->nfield = (long long)g.ldi * g.ldj * g.ldk;
   // capsules, offsets, degree groups
@@ -344,9 +352,15 @@ int setup(sg_ctx* c) {
   SG_TRY(dalloc(c, c->ibw.fx, E * np), "alloc");
   SG_TRY(dalloc(c, c->ibw.fy, E * np), "alloc");
   SG_TRY(dalloc(c, c->ibw.fz, E * np), "alloc");
-  SG_TRY(dalloc(c, c->ibw.counts, sizeof(int) * g.ntiles), "alloc");
-  SG_TRY(dalloc(c, c->ibw.starts, sizeof(int) * (g.ntiles + 1)), "alloc");
-  SG_TRY(dalloc(c, c->ibw.fill, sizeof(int) * g.ntiles), "alloc");
+  c->max_tiles = g.ntiles;
+  for (int sh = 0; sh < kNumTileShapes; ++sh) {
+    IBGrid t{};
+    if (make_ib_grid(cfg.itot, cfg.jtot, cfg.ktot, cfg.lx, cfg.ly, cfg.lz, t, sh))
+      c->max_tiles = std::max(c->max_tiles, t.ntiles);
+  }
+  SG_TRY(dalloc(c, c->ibw.counts, sizeof(int) * c->max_tiles), "alloc");
+  SG_TRY(dalloc(c, c->ibw.starts, sizeof(int) * (c->max_tiles + 1)), "alloc");
+  SG_TRY(dalloc(c, c->ibw.fill, sizeof(int) * c->max_tiles), "alloc");
   if (cfg.mem == SG_MEM_HOST) {
     SG_TRY(dalloc(c, c->s_u, E * c->nfield), "alloc");
     SG_TRY(dalloc(c, c->s_v, E * c->nfield), "alloc");
@@ -408,6 +422,7 @@ int dev_spread(sg_ctx* c, const T* FX, const T* FY, const T* FZ, const T* A, T* 
 }
 
 int finish(sg_ctx* c) {
+  if (c->capturing) return SG_OK;
   if (!c->cfg.async || c->cfg.mem == SG_MEM_HOST) SG_TRY(cudaStreamSynchronize(c->st), "synchronize");
   return SG_OK;
 }
@@ -460,7 +475,7 @@ int run_step(sg_ctx* c, int what, const void* u, const void* v, const void* w, c
     dfx = (T*)c->s_f[0]; dfy = (T*)c->s_f[1]; dfz = (T*)c->s_f[2];
   }
   auto mark = [&](int k) -> int {
-    if (c->profiling) SG_TRY(cudaEventRecord(c->ev[k], c->st), "event");
+    if (c->profiling && !c->capturing) SG_TRY(cudaEventRecord(c->ev[k], c->st), "event");
     return SG_OK;
   };
   SG_RET(mark(0));
@@ -543,6 +558,8 @@ void sg_destroy(sg_ctx* c) {
   if (!c) return;
   cudaSetDevice(c->cfg.device);
   if (c->st) cudaStreamSynchronize(c->st);
+  if (c->graph_exec) cudaGraphExecDestroy(c->graph_exec);
+  if (c->graph) cudaGraphDestroy(c->graph);
   for (void* p : c->allocs) cudaFree(p);
   for (int k = 0; k <= SG_NSTAGE; ++k)
     if (c->ev[k]) cudaEventDestroy(c->ev[k]);
@@ -683,6 +700,123 @@ int sg_set_profiling(sg_ctx* c, int on) {
   if (on && !c->ev[0])
     for (int k = 0; k <= SG_NSTAGE; ++k) SG_TRY(cudaEventCreate(&c->ev[k]), "cudaEventCreate");
   c->profiling = on != 0;
+  return SG_OK;
+}
+
+int sg_set_tile_shape(sg_ctx* c, int shape) {
+  if (!c) return SG_ERR_ARG;
+  if (shape < -1 || shape >= kNumTileShapes) return fail(c, SG_ERR_ARG, "tile shape out of range");
+  if (shape >= 0 && !c->mixed) {
+    const TileShape& t = kTileShapes[shape];
+    if (t.TX * t.TY * t.TZ > 1024) return fail(c, SG_ERR_ARG, "FP64 spreading takes tiles of at most 1024 cells");
+  }
+  if (c->graph) return fail(c, SG_ERR_STATE, "release the captured graph before changing the tile shape");
+  IBGrid g{};
+  const sg_config& cfg = c->cfg;
+  if (!make_ib_grid(cfg.itot, cfg.jtot, cfg.ktot, cfg.lx, cfg.ly, cfg.lz, g, shape) || g.ntiles > c->max_tiles)
+    return fail(c, SG_ERR_ARG, "tile shape not valid for this grid");
+  c->grid = g;
+  return SG_OK;
+}
+
+int sg_get_tile_shape(const sg_ctx* c, int* shape, int* tx, int* ty, int* tz) {
+  if (!c) return SG_ERR_ARG;
+  if (shape) *shape = c->grid.shape;
+  if (tx) *tx = c->grid.TX;
+  if (ty) *ty = c->grid.TY;
+  if (tz) *tz = c->grid.TZ;
+  return SG_OK;
+}
+
+int sg_autotune(sg_ctx* c, const void* u, const void* v, const void* w, const double* X, const double* Y,
+                const double* Z, void* U, void* V, void* W, void* FX, void* FY, void* FZ, void* NX, void* NY,
+                void* NZ, void* AREA, void* fx, void* fy, void* fz, int reps, int* best_shape, float* best_ms) {
+  if (!c) return SG_ERR_ARG;
+  if (reps < 1) return fail(c, SG_ERR_ARG, "reps must be >= 1");
+  if (c->graph) return fail(c, SG_ERR_STATE, "release the captured graph before tuning");
+  cudaEvent_t e0 = nullptr, e1 = nullptr;
+  SG_TRY(cudaEventCreate(&e0), "cudaEventCreate");
+  if (cudaEventCreate(&e1) != cudaSuccess) {
+    cudaEventDestroy(e0);
+    return fail(c, SG_ERR_CUDA, "cudaEventCreate");
+  }
+  const int async = c->cfg.async;
+  c->cfg.async = 1;  // queue the repetitions back to back
+  int best = -1, rc = SG_OK;
+  float bms = 0.f;
+  for (int sh = 0; sh < kNumTileShapes && rc == SG_OK; ++sh) {
+    if (sg_set_tile_shape(c, sh) != SG_OK) continue;  // not valid for this precision or grid
+    rc = sg_step(c, u, v, w, X, Y, Z, U, V, W, FX, FY, FZ, NX, NY, NZ, AREA, fx, fy, fz);  // warm-up
+    if (rc == SG_OK && cudaEventRecord(e0, c->st) != cudaSuccess) rc = fail(c, SG_ERR_CUDA, "event");
+    for (int r = 0; r < reps && rc == SG_OK; ++r)
+      rc = sg_step(c, u, v, w, X, Y, Z, U, V, W, FX, FY, FZ, NX, NY, NZ, AREA, fx, fy, fz);
+    float ms = 0.f;
+    if (rc == SG_OK && (cudaEventRecord(e1, c->st) != cudaSuccess || cudaEventSynchronize(e1) != cudaSuccess ||
+                        cudaEventElapsedTime(&ms, e0, e1) != cudaSuccess))
+      rc = fail(c, SG_ERR_CUDA, "autotune timing");
+    ms /= (float)reps;
+    if (rc == SG_OK && (best < 0 || ms < bms)) {
+      best = sh;
+      bms = ms;
+    }
+  }
+  c->cfg.async = async;
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  if (rc != SG_OK) return rc;
+  if (best < 0) return fail(c, SG_ERR_STATE, "no tile shape is valid for this grid");
+  SG_RET(sg_set_tile_shape(c, best));
+  if (best_shape) *best_shape = best;
+  if (best_ms) *best_ms = bms;
+  return SG_OK;
+}
+
+int sg_graph_capture(sg_ctx* c, const void* u, const void* v, const void* w, const double* X, const double* Y,
+                     const double* Z, void* U, void* V, void* W, void* FX, void* FY, void* FZ, void* NX, void* NY,
+                     void* NZ, void* AREA, void* fx, void* fy, void* fz) {
+  if (!c) return SG_ERR_ARG;
+  if (c->cfg.mem != SG_MEM_DEVICE) return fail(c, SG_ERR_STATE, "graph capture needs device memory mode");
+  if (c->graph) return fail(c, SG_ERR_STATE, "a graph is already captured");
+  if (!c->st) return fail(c, SG_ERR_STATE, "no stream");
+  SG_TRY(cudaStreamSynchronize(c->st), "synchronize");
+  SG_TRY(cudaStreamBeginCapture(c->st, cudaStreamCaptureModeThreadLocal), "cudaStreamBeginCapture");
+  c->capturing = true;
+  const int rc = sg_step(c, u, v, w, X, Y, Z, U, V, W, FX, FY, FZ, NX, NY, NZ, AREA, fx, fy, fz);
+  c->capturing = false;
+  cudaGraph_t g = nullptr;
+  const cudaError_t e = cudaStreamEndCapture(c->st, &g);
+  if (rc != SG_OK) {
+    if (g) cudaGraphDestroy(g);
+    return rc;
+  }
+  if (e != cudaSuccess) return cuda_fail(c, e, "cudaStreamEndCapture");
+  cudaGraphExec_t x = nullptr;
+  const cudaError_t ei = cudaGraphInstantiate(&x, g, 0);
+  if (ei != cudaSuccess) {
+    cudaGraphDestroy(g);
+    return cuda_fail(c, ei, "cudaGraphInstantiate");
+  }
+  c->graph = g;
+  c->graph_exec = x;
+  c->graph_launches = c->launches;
+  return SG_OK;
+}
+
+int sg_graph_launch(sg_ctx* c) {
+  if (!c) return SG_ERR_ARG;
+  if (!c->graph_exec) return fail(c, SG_ERR_STATE, "no captured graph");
+  SG_TRY(cudaGraphLaunch(c->graph_exec, c->st), "cudaGraphLaunch");
+  c->launches = c->graph_launches;
+  return finish(c);
+}
+
+int sg_graph_release(sg_ctx* c) {
+  if (!c) return SG_ERR_ARG;
+  if (c->graph_exec) SG_TRY(cudaStreamSynchronize(c->st), "synchronize");
+  if (c->graph_exec) cudaGraphExecDestroy(c->graph_exec);
+  if (c->graph) cudaGraphDestroy(c->graph);
+  c->graph_exec = nullptr;
+  c->graph = nullptr;
   return SG_OK;
 }
 

@@ -6,10 +6,9 @@
 namespace sg {
 
 // ------------------------------------------------------------------ binning
-// Storage index of a base-relative stencil cell, periodic in [1, n]: the
-// stencil of a point with base b covers b-1 .. b+2 (kernel support |r|<1.5
-// for both face and cell-centre locations).
-SG_HD int wrap_near(int r, int n) { return r < 1 ? r + n : (r > n ? r - n : r); }
+// The stencil of a point with base b covers b-1 .. b+2 (kernel support
+// |r| < 1.5 for both face and cell-centre locations); wrap_near gives the
+// periodic storage index in [1, n].
 
 // Tiles touched by the stencil of a point in one periodic dimension: the
 // tiles of its first and last cell (the stencil is narrower than a tile).
@@ -101,8 +100,11 @@ __global__ void bin_scatter_kernel(IBGrid g, long n, const int* __restrict__ bx,
 
 // ------------------------------------------------------------------ interp
 // eulr2lagr hot loop (interp_spread.f90:335-378) as a per-point gather in the
-// reference's point order (consecutive points share cache lines):
-// u at faces i*dx (kernel(i-c)), cell centres at (i-0.5)dx (kernel(i-0.5-c)).
+// reference's point order (consecutive points share cache lines).  u sits at
+// faces i*dx (kernel(i-c)), cell centres at (i-0.5)dx (kernel(i-0.5-c)); each
+// component has 3 x 3 x 3 nonzero weights, face weights along its own
+// direction and centre weights along the other two (delta3_face/_centre).
+// z-levels outside [1,kmax] are skipped (interp_spread.f90:346-351).
 template <class T>
 __global__ void __launch_bounds__(256) interp_kernel(IBGrid g, long n, const int* __restrict__ bx,
                                                      const int* __restrict__ by, const int* __restrict__ bz,
@@ -112,45 +114,59 @@ __global__ void __launch_bounds__(256) interp_kernel(IBGrid g, long n, const int
                                                      T* __restrict__ U, T* __restrict__ V, T* __restrict__ W) {
   const long p = (long)blockIdx.x * blockDim.x + threadIdx.x;
   if (p >= n) return;
-  const int b0 = bx[p], b1 = by[p], b2 = bz[p];
-  const T f0 = fx[p], f1 = fy[p], f2 = fz[p];
-  T wfx[4], wcx[4], wfy[4], wcy[4], wfz[4], wcz[4];
-  int ii[4], jj[4], kk[4];
+  const int bb[3] = {bx[p], by[p], bz[p]};
+  const T fr[3] = {fx[p], fy[p], fz[p]};
+  T wF[3][3], wC[3][3];
+  bool hi[3];
+#pragma unroll
+  for (int d = 0; d < 3; ++d) {
+    delta3_face<T>(fr[d], wF[d], hi[d]);
+    delta3_centre<T>(fr[d], wC[d]);
+  }
+  // storage offsets of the stencil nodes o = -1..2 per dimension, then of
+  // the face nodes (o = hi-1 .. hi+1) and the centres (o = 0..2); z-levels
+  // outside [1,kmax] get offset -1
+  // (32-bit: make_ib_grid caps the field at 2^31 - 1 elements)
+  int o4[3][4];
 #pragma unroll
   for (int t = 0; t < 4; ++t) {
-    wfx[t] = delta3<T>(T(t - 1) - f0);
-    wcx[t] = delta3<T>(T(t - 1) - T(0.5) - f0);
-    wfy[t] = delta3<T>(T(t - 1) - f1);
-    wcy[t] = delta3<T>(T(t - 1) - T(0.5) - f1);
-    wfz[t] = delta3<T>(T(t - 1) - f2);
-    wcz[t] = delta3<T>(T(t - 1) - T(0.5) - f2);
-    ii[t] = wrap_near(b0 + t - 1, g.itot);
-    jj[t] = wrap_near(b1 + t - 1, g.jtot);
-    const int k = b2 + t - 1;
-    kk[t] = (k >= 1 && k <= g.ktot) ? k : -1;  // window clipped to [1,kmax]
+    o4[0][t] = wrap_near(bb[0] + t - 1, g.itot);
+    o4[1][t] = g.ldi * wrap_near(bb[1] + t - 1, g.jtot);
+    const int k = bb[2] + t - 1;
+    o4[2][t] = (k >= 1 && k <= g.ktot) ? g.ldi * g.ldj * k : -1;
   }
-  T su = 0, sv = 0, sw = 0;
+  int oF[3][3], oC[3][3];
 #pragma unroll
-  for (int tk = 0; tk < 4; ++tk) {
-    if (kk[tk] < 0) continue;
+  for (int d = 0; d < 3; ++d)
 #pragma unroll
-    for (int tj = 0; tj < 4; ++tj) {
-      const long long row = (long long)g.ldi * ((long long)jj[tj] + (long long)g.ldj * kk[tk]);
+    for (int t = 0; t < 3; ++t) {
+      oF[d][t] = hi[d] ? o4[d][t + 1] : o4[d][t];
+      oC[d][t] = o4[d][t + 1];
+    }
+  T out[3];
 #pragma unroll
-      for (int ti = 0; ti < 4; ++ti) {
-        const long long o = row + ii[ti];
-        const T wu = wfx[ti] * wcy[tj] * wcz[tk];
-        const T wv = wcx[ti] * wfy[tj] * wcz[tk];
-        const T ww = wcx[ti] * wcy[tj] * wfz[tk];
-        if (wu != T(0)) su += u[o] * wu;
-        if (wv != T(0)) sv += v[o] * wv;
-        if (ww != T(0)) sw += w[o] * ww;
+  for (int c = 0; c < 3; ++c) {
+    const T* src = c == 0 ? u : (c == 1 ? v : w);
+    T sum = T(0);
+#pragma unroll
+    for (int tz = 0; tz < 3; ++tz) {
+      const int zo = (c == 2) ? oF[2][tz] : oC[2][tz];
+      if (zo < 0) continue;
+      const T wz = (c == 2) ? wF[2][tz] : wC[2][tz];
+#pragma unroll
+      for (int ty = 0; ty < 3; ++ty) {
+        const T wyz = ((c == 1) ? wF[1][ty] : wC[1][ty]) * wz;
+        const T* row = src + zo + ((c == 1) ? oF[1][ty] : oC[1][ty]);
+#pragma unroll
+        for (int tx = 0; tx < 3; ++tx)
+          sum += row[(c == 0) ? oF[0][tx] : oC[0][tx]] * (((c == 0) ? wF[0][tx] : wC[0][tx]) * wyz);
       }
     }
+    out[c] = sum;
   }
-  U[p] = su;
-  V[p] = sv;
-  W[p] = sw;
+  U[p] = out[0];
+  V[p] = out[1];
+  W[p] = out[2];
 }
 
 // ------------------------------------------------------------------ launchers
@@ -187,8 +203,10 @@ template cudaError_t launch_interp<double>(const IBGrid&, long, const IBWork&, c
 template cudaError_t launch_interp<float>(const IBGrid&, long, const IBWork&, const float*, const float*, const float*,
                                           float*, float*, float*, cudaStream_t);
 
-bool make_ib_grid(int itot, int jtot, int ktot, double lx, double ly, double lz, IBGrid& g) {
+bool make_ib_grid(int itot, int jtot, int ktot, double lx, double ly, double lz, IBGrid& g, int shape) {
   if (itot < 8 || jtot < 8 || ktot < 1) return false;
+  if (shape >= kNumTileShapes) return false;
+  if ((long long)(itot + 2) * (jtot + 2) * (ktot + 2) > 2147483647LL) return false;  // 32-bit offsets
   g.itot = itot;
   g.jtot = jtot;
   g.ktot = ktot;
@@ -200,12 +218,12 @@ bool make_ib_grid(int itot, int jtot, int ktot, double lx, double ly, double lz,
   g.dyi = 1.0 / dy;
   g.dzi = 1.0 / dz;
   g.dvi = 1.0 / (dx * dy * dz);
-  // tile shape: 32 x 8 x 4 (128-byte rows in x) or 8 x 8 x 4 on narrow grids
-  if (itot >= 32) {
-    g.TX = 32; g.TY = 8; g.TZ = 4;
-  } else {
-    g.TX = 8; g.TY = 8; g.TZ = 4;
-  }
+  // default tile shape: 32 x 8 x 4 (128-byte rows in x), 8 x 8 x 4 on narrow grids
+  if (shape < 0) shape = itot >= 32 ? 0 : 3;
+  g.shape = shape;
+  g.TX = kTileShapes[shape].TX;
+  g.TY = kTileShapes[shape].TY;
+  g.TZ = kTileShapes[shape].TZ;
   g.ntx = (itot + g.TX - 1) / g.TX;
   g.nty = (jtot + g.TY - 1) / g.TY;
   g.ntz = (ktot + g.TZ - 1) / g.TZ;

@@ -7,20 +7,29 @@
 // (interp_spread.f90:340-351, 846-851); the force halo is the copy of
 // bound.f90:141-190.
 //
-// Points are binned by tile (counting sort, then each tile's list sorted by
-// point index so the order is deterministic).  Interpolation is a per-point
-// gather in tile order.  Spreading is a per-cell gather over the points staged
-// for the cell's tile: no float atomics, fixed summation order.
+// Points are binned by output tile: a counting sort lists, for every tile,
+// each point whose stencil reaches it.  Interpolation is a per-point gather.
+// Spreading runs one CTA per tile over that list and sums in fixed point in
+// shared memory (integer atomics, so the result does not depend on order).
 #pragma once
 #include "sg_common.cuh"
 
 namespace sg {
+
+// Spreading tile shapes (cells).  FP64 spreading takes shapes of at most 1024
+// cells (three 32-bit limbs per cell and component in static shared memory).
+struct TileShape {
+  int TX, TY, TZ;
+};
+constexpr TileShape kTileShapes[] = {{32, 8, 4}, {16, 16, 8}, {32, 8, 8}, {8, 8, 4}};
+constexpr int kNumTileShapes = 4;
 
 struct IBGrid {
   int itot, jtot, ktot;  // interior cells (imax, jmax, kmax)
   int ldi, ldj, ldk;     // itot+2, jtot+2, ktot+2 (halo of one cell)
   double dxi, dyi, dzi;  // inverse spacings
   double dvi;            // 1 / (dx dy dz)
+  int shape;             // index into kTileShapes
   int TX, TY, TZ;        // tile shape
   int ntx, nty, ntz;     // tiles per dimension
   int ntiles;

@@ -22,7 +22,8 @@ struct IBWork {
   int* entries = nullptr; // [8*npts] point index per (tile, point) pair
 };
 
-bool make_ib_grid(int itot, int jtot, int ktot, double lx, double ly, double lz, IBGrid& g);
+// shape: index into kTileShapes, or -1 for the default of the grid size.
+bool make_ib_grid(int itot, int jtot, int ktot, double lx, double ly, double lz, IBGrid& g, int shape = -1);
 template <class T>
 cudaError_t launch_bin(const IBGrid& g, long n, const double* X, const double* Y, const double* Z, IBWork& w,
                        cudaStream_t st);

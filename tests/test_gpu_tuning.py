@@ -1,0 +1,113 @@
+"""Spreading tile shapes, the autotuner and CUDA-graph replay of the step.
+
+Every tile shape must give the oracle's spread field within the path's
+tolerance (FP64 relative L2 <= 1e-12, mixed <= 1e-4) and be bitwise
+reproducible; the autotuner must leave the context on a valid shape with the
+same results; a captured graph must reproduce sg_step bit for bit on the same
+device arrays, also after their contents change.
+"""
+import numpy as np
+import pytest
+
+import oracle as O
+from suguru_b200 import workloads as W
+from suguru_b200.coupling import TILE_SHAPES, CouplingStep, SgError
+from util import rel_l2
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.fixture(scope="module")
+def case():
+    wl = W.small_config()
+    rng = np.random.default_rng(21)
+    f = rng.normal(size=(3, wl.npts))
+    a = rng.uniform(0.5, 1.5, wl.npts) * wl.grid[3] ** 2
+    ref = O.spread(wl.grid, wl.x, wl.y, wl.z, f[0], f[1], f[2], a)
+    return wl, f, a, ref
+
+
+@pytest.mark.parametrize("shape", range(len(TILE_SHAPES)))
+def test_tile_shape_mixed(cuda, case, shape):
+    wl, f, a, ref = case
+    cs = CouplingStep(wl.grid, wl.degree, wl.radius, precision="mixed")
+    cs.set_tile_shape(shape)
+    assert cs.tile_shape() == (shape, TILE_SHAPES[shape])
+    f32 = [x.astype(np.float32) for x in f]
+    g1 = cs.lagr2eulr(wl.x, wl.y, wl.z, *f32, a.astype(np.float32))
+    g2 = cs.lagr2eulr(wl.x, wl.y, wl.z, *f32, a.astype(np.float32))
+    for x, y, r in zip(g1, g2, ref):
+        assert np.array_equal(x, y)
+        assert rel_l2(x, r) <= 1e-4
+
+
+@pytest.mark.parametrize("shape", range(len(TILE_SHAPES)))
+def test_tile_shape_fp64(cuda, case, shape):
+    wl, f, a, ref = case
+    cs = CouplingStep(wl.grid, wl.degree, wl.radius, precision="fp64")
+    n = np.prod(TILE_SHAPES[shape])
+    if n > 1024:  # three-limb FP64 accumulators fit 1024-cell tiles only
+        with pytest.raises(SgError):
+            cs.set_tile_shape(shape)
+        return
+    cs.set_tile_shape(shape)
+    got = cs.lagr2eulr(wl.x, wl.y, wl.z, f[0].copy(), f[1].copy(), f[2].copy(), a)
+    for g, r in zip(got, ref):
+        assert rel_l2(g, r) <= 1e-12
+
+
+def test_autotune_mixed(cuda):
+    wl = W.small_config()
+    u, v, w = (x.astype(np.float32) for x in wl.velocity())
+    ref = O.coupling_step(wl.grid, wl.degree, wl.radius, *wl.velocity(), wl.x, wl.y, wl.z, wl.gs, wl.csk)
+    cs = CouplingStep(wl.grid, wl.degree, wl.radius, precision="mixed")
+    best, ms = cs.autotune(u, v, w, wl.x, wl.y, wl.z, reps=2)
+    assert 0 <= best < len(TILE_SHAPES) and ms > 0
+    assert cs.tile_shape()[0] == best
+    out = cs.step(u, v, w, wl.x, wl.y, wl.z)
+    for c in range(3):
+        assert rel_l2(out["fgrid"][c], ref["fgrid"][c]) <= 1e-4
+        assert rel_l2(out["u"][c], ref["u"][c]) <= 1e-4
+
+
+@pytest.mark.parametrize("precision", ["fp64", "mixed"])
+def test_graph_replay(cuda, precision):
+    torch = cuda
+    wl = W.small_config()
+    dt = torch.float64 if precision == "fp64" else torch.float32
+    dev = lambda a, t=dt: torch.from_numpy(np.ascontiguousarray(a)).to("cuda", t)
+    st = torch.cuda.Stream()
+    cs = CouplingStep(wl.grid, wl.degree, wl.radius, precision=precision, mem="device",
+                      stream=st.cuda_stream)
+    u, v, w = (dev(x) for x in wl.velocity())
+    X, Y, Z = (dev(x, torch.float64) for x in (wl.x, wl.y, wl.z))
+    lag = [torch.zeros(wl.npts, dtype=dt, device="cuda") for _ in range(10)]
+    eul = [torch.zeros_like(u) for _ in range(3)]
+    torch.cuda.synchronize()  # inputs were written on torch's stream
+    cs.step(u, v, w, X, Y, Z, lag_out=lag, eul_out=eul)
+    torch.cuda.synchronize()
+    want = [t.clone() for t in lag + eul]
+    n_launch = cs.last_launch_count()
+    cs.graph_capture(u, v, w, X, Y, Z, lag, eul)
+    for t in lag + eul:
+        t.fill_(float("nan"))
+    torch.cuda.synchronize()
+    cs.graph_launch()
+    torch.cuda.synchronize()
+    assert cs.last_launch_count() == n_launch
+    for a, b in zip(lag + eul, want):
+        assert torch.equal(a, b)
+    # new contents, same arrays: the replay follows them
+    u.mul_(0.5)
+    X.add_(0.25 * wl.grid[3])
+    torch.cuda.synchronize()
+    cs.graph_launch()
+    torch.cuda.synchronize()
+    got = [t.clone() for t in lag + eul]
+    cs.graph_release()
+    cs.step(u, v, w, X, Y, Z, lag_out=lag, eul_out=eul)
+    torch.cuda.synchronize()
+    for a, b in zip(got, lag + eul):
+        assert torch.equal(a, b)
+    with pytest.raises(SgError):
+        cs.graph_launch()
