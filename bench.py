@@ -261,7 +261,8 @@ def run_ours(args):
             "higher_is_better": True,
             "scaling": "weak",
             "vs_baseline": None,
-            "dtype": "f32 (Legendre contractions f32; FP64 positions, centroids, tables)",
+            "dtype": "f32 (Legendre contractions BF16x3 on tcgen05 tensor cores, FP32 accumulation; "
+                     "FP64 positions, centroids, tables)",
             "data": "synthetic (seeded shapes and velocity modes, no reference fixtures exist)",
             "config": {"workload": "dense suspension: 256 capsules, SH degree 15 (524,288 points), "
                                    "grid 256x256x128, dx=1/32, Skalak Gs=1 C=1",

@@ -35,6 +35,8 @@ EXPORTS = ["sg_create", "sg_destroy", "sg_last_error", "sg_synchronize", "sg_int
            "sg_last_launch_count", "sg_set_profiling", "sg_stage_times", "sg_spread_noalloc",
            "sg_set_tile_shape", "sg_get_tile_shape", "sg_autotune", "sg_graph_capture", "sg_graph_launch",
            "sg_graph_release"]
+# test hooks declared in include/sg_testing.h
+TEST_EXPORTS = ["sg_test_legendre"]
 TILE_SHAPES = ((32, 8, 4), (16, 16, 8), (32, 8, 8), (8, 8, 4))
 STAGES = ("bin", "interp", "membrane", "spread")
 
@@ -91,10 +93,25 @@ def lib():
     L.sg_graph_capture.argtypes = [vp] * 20
     L.sg_graph_launch.argtypes = [vp]
     L.sg_graph_release.argtypes = [vp]
+    L.sg_test_legendre.argtypes = [ctypes.c_int] * 6 + [vp] * 3
     d = ctypes.c_double
     L.sg_spread_noalloc.argtypes = ([ctypes.c_int] * 3 + [d] * 3 + [ctypes.c_long] + [vp] * 11)
     _LIB = L
     return L
+
+
+def test_legendre(A, B, tensor_cores=True, tri=False):
+    """D[m,q,j] = sum_k A[m,q,k] B[m,j,k] through one Legendre kernel (test hook)."""
+    A = np.ascontiguousarray(A, dtype=np.float32)
+    B = np.ascontiguousarray(B, dtype=np.float64)
+    M, Q, K = A.shape
+    J = B.shape[1]
+    assert B.shape == (M, J, K)
+    D = np.zeros((M, Q, J), dtype=np.float32)
+    rc = lib().sg_test_legendre(int(bool(tensor_cores)), M, Q, J, K, int(bool(tri)), _ptr(B), _ptr(A), _ptr(D))
+    if rc:
+        raise SgError(rc, "sg_test_legendre")
+    return D
 
 
 def gauss(nlat):

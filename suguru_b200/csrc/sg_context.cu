@@ -21,6 +21,7 @@ struct Group {
   std::vector<int> caps;
   DegreeTables tab;
   SpecBuffers buf{};
+  std::vector<double> h_tab[4];  // host FP64 syn_D, ana_D, syn_O, ana_O (by LegProblem::kind)
 };
 }  // namespace
 
@@ -48,6 +49,14 @@ struct sg_ctx {
   LegWork* d_lw[6] = {};
   int nlw[6] = {};
   int maxJ[6] = {}, maxK[6] = {};
+  // tensor-core Legendre path (mixed precision): 128-row work lists
+  bool leg_tc = false;
+  LegWork* d_lw128[6] = {};
+  int nlw128[6] = {};
+  int maxJp[6] = {}, maxKp[6] = {};
+  int num_sms = 148;
+  int* d_err = nullptr;   // device error flag (bounded waits that expired)
+  int* h_err = nullptr;   // pinned copy, refreshed at the end of every step
   int nmax = 0;
   // host-mode staging
   void* s_u = nullptr;
@@ -90,6 +99,12 @@ int cuda_fail(sg_ctx* c, cudaError_t e, const char* where) {
   do {                                            \
     cudaError_t _e = (expr);                      \
     if (_e != cudaSuccess) return cuda_fail(c, _e, where); \
+  } while (0)
+
+#define SG_RET(x)             \
+  do {                        \
+    int _r = (x);             \
+    if (_r != SG_OK) return _r; \
   } while (0)
 
 template <class P>
@@ -175,6 +190,10 @@ cudaError_t build_tables(sg_ctx* c, Group& g) {
       }
     return t;
   };
+  g.h_tab[0] = synD;
+  g.h_tab[1] = anaD;
+  g.h_tab[2] = synO;
+  g.h_tab[3] = anaO;
   cudaError_t e;
   if ((e = upload2<double>(c, g.tab.syn_D, synD)) != cudaSuccess) return e;
   if ((e = upload2<double>(c, g.tab.ana_D, anaD)) != cudaSuccess) return e;
@@ -336,6 +355,42 @@ int setup(sg_ctx* c) {
                               (char*)b.GF + E * 6 * N * nD, 14 * N * nD, N * nD, nD, 8, n, N, nD, N, 1, G, 0),
                 c->maxJ[5], c->maxK[5]);
   }
+  // tensor-core operands: bf16 hi/lo images of every problem's table, and
+  // work lists of 128-row tiles (FP32 data only)
+  if (c->mixed) {
+    std::vector<uint16_t> img;
+    std::vector<size_t> img_off(P.size());
+    std::vector<LegWork> W128[6];
+    for (size_t pi2 = 0; pi2 < P.size(); ++pi2) {
+      LegProblem& p = P[pi2];
+      p.Jp = (p.J + 15) / 16 * 16;
+      p.Kp = (p.K + 15) / 16 * 16;
+      p.sBimg = 2LL * p.Jp * p.Kp;
+      img_off[pi2] = img.size();
+      img.resize(img.size() + (size_t)p.M * p.sBimg);
+      const std::vector<double>& hb = c->groups[p.group].h_tab[p.kind];
+      host_umma_image(hb.data(), p.sBm, p.M, p.J, p.K, p.Jp, p.Kp, img.data() + img_off[pi2]);
+      auto al4 = [](const void* ptr) { return ((uintptr_t)ptr & 15u) == 0; };
+      p.vecA = (al4(p.A) && p.sAc % 4 == 0 && p.sAr % 4 == 0 && p.sAm % 4 == 0 && p.K % 8 == 0) ? 1 : 0;
+      p.vecD = (al4(p.D) && p.sDc % 4 == 0 && p.sDr % 4 == 0 && p.sDm % 4 == 0 && p.J % 4 == 0) ? 1 : 0;
+    }
+    void* dimg = nullptr;
+    SG_TRY(upload(c, dimg, img), "umma images");
+    for (size_t pi2 = 0; pi2 < P.size(); ++pi2) P[pi2].Bimg = (const uint16_t*)dimg + img_off[pi2];
+    for (int s = 0; s < 6; ++s) {
+      for (const LegWork& w : W[s]) {
+        if (w.q0 % 128) continue;  // one 128-row tile per four 32-row items
+        W128[s].push_back(w);
+        const LegProblem& p = P[w.prob];
+        c->maxJp[s] = std::max(c->maxJp[s], p.Jp);
+        c->maxKp[s] = std::max(c->maxKp[s], p.Kp);
+      }
+      c->nlw128[s] = (int)W128[s].size();
+      SG_TRY(upload(c, tmp, W128[s]), "work");
+      c->d_lw128[s] = (LegWork*)tmp;
+    }
+    c->leg_tc = true;
+  }
   SG_TRY(upload(c, tmp, P), "problems");
   c->d_probs = (LegProblem*)tmp;
   for (int s = 0; s < 6; ++s) {
@@ -343,6 +398,11 @@ int setup(sg_ctx* c) {
     SG_TRY(upload(c, tmp, W[s]), "work");
     c->d_lw[s] = (LegWork*)tmp;
   }
+  SG_TRY(dalloc(c, c->d_err, sizeof(int)), "alloc");
+  SG_TRY(cudaMemset(c->d_err, 0, sizeof(int)), "memset");
+  SG_TRY(cudaMallocHost(&c->h_err, sizeof(int)), "cudaMallocHost");
+  *c->h_err = 0;
+  SG_TRY(cudaDeviceGetAttribute(&c->num_sms, cudaDevAttrMultiProcessorCount, cfg.device), "attribute");
   // binning work
   const long np = std::max(c->npts, 1L);
   SG_TRY(dalloc(c, c->ibw.bx, sizeof(int) * np), "alloc");
@@ -393,21 +453,33 @@ int dev_interp(sg_ctx* c, const T* u, const T* v, const T* w, T* U, T* V, T* W) 
 }
 
 template <class T>
+int dev_legendre(sg_ctx* c, int s) {
+  if (sizeof(T) == 4 && c->leg_tc) {
+    SG_TRY(launch_legendre_mma(c->d_probs, c->d_lw128[s], c->nlw128[s], c->maxJp[s], c->maxKp[s], c->d_err,
+                               c->num_sms, c->st),
+           "legendre (tensor cores)");
+  } else {
+    SG_TRY(launch_legendre<T>(c->d_probs, c->d_lw[s], c->nlw[s], c->maxJ[s], c->maxK[s], c->st), "legendre");
+  }
+  return SG_OK;
+}
+
+template <class T>
 int dev_forces(sg_ctx* c, const double* X, const double* Y, const double* Z, T* FX, T* FY, T* FZ, T* NX, T* NY,
                T* NZ, T* A) {
   const int nc = c->cfg.ncap;
   if (nc == 0) return SG_OK;
   SG_TRY(launch_centroid<T>(nc, c->d_caps, X, Y, Z, c->d_cen, c->st), "centroid");
   SG_TRY(launch_posfwd<T>(c->d_wpos, c->nwpos, c->d_caps, c->d_groups, X, Y, Z, c->d_cen, c->st), "posfwd");
-  SG_TRY(launch_legendre<T>(c->d_probs, c->d_lw[0], c->nlw[0], c->maxJ[0], c->maxK[0], c->st), "legendre0");
-  SG_TRY(launch_legendre<T>(c->d_probs, c->d_lw[1], c->nlw[1], c->maxJ[1], c->maxK[1], c->st), "legendre1");
+  SG_RET(dev_legendre<T>(c, 0));
+  SG_RET(dev_legendre<T>(c, 1));
   SG_TRY(launch_membrane<T>(c->d_wmem, c->nwmem, c->d_caps, c->d_groups, c->cfg.gs, c->cfg.csk, c->nmax, c->st),
          "membrane");
-  SG_TRY(launch_legendre<T>(c->d_probs, c->d_lw[2], c->nlw[2], c->maxJ[2], c->maxK[2], c->st), "legendre2");
-  SG_TRY(launch_legendre<T>(c->d_probs, c->d_lw[3], c->nlw[3], c->maxJ[3], c->maxK[3], c->st), "legendre3");
+  SG_RET(dev_legendre<T>(c, 2));
+  SG_RET(dev_legendre<T>(c, 3));
   SG_TRY(launch_shgrid<T>(c->d_wsh, c->nwsh, c->d_caps, c->d_groups, c->nmax, c->st), "shgrid");
-  SG_TRY(launch_legendre<T>(c->d_probs, c->d_lw[4], c->nlw[4], c->maxJ[4], c->maxK[4], c->st), "legendre4");
-  SG_TRY(launch_legendre<T>(c->d_probs, c->d_lw[5], c->nlw[5], c->maxJ[5], c->maxK[5], c->st), "legendre5");
+  SG_RET(dev_legendre<T>(c, 4));
+  SG_RET(dev_legendre<T>(c, 5));
   SG_TRY(launch_final<T>(c->d_wfin, c->nwfin, c->d_caps, c->d_groups, FX, FY, FZ, NX, NY, NZ, A, c->nmax, c->st),
          "final");
   c->launches += 12;
@@ -421,9 +493,23 @@ int dev_spread(sg_ctx* c, const T* FX, const T* FY, const T* FZ, const T* A, T* 
   return SG_OK;
 }
 
+// Reports a bounded device wait that expired (flag copied to pinned memory
+// at the end of each step) once the stream has been synchronised.
+int check_err(sg_ctx* c) {
+  if (c->h_err && *c->h_err) {
+    *c->h_err = 0;
+    SG_TRY(cudaMemsetAsync(c->d_err, 0, sizeof(int), c->st), "memset");
+    return fail(c, SG_ERR_TIMEOUT, "a tensor-core completion wait timed out");
+  }
+  return SG_OK;
+}
+
 int finish(sg_ctx* c) {
   if (c->capturing) return SG_OK;
-  if (!c->cfg.async || c->cfg.mem == SG_MEM_HOST) SG_TRY(cudaStreamSynchronize(c->st), "synchronize");
+  if (!c->cfg.async || c->cfg.mem == SG_MEM_HOST) {
+    SG_TRY(cudaStreamSynchronize(c->st), "synchronize");
+    SG_RET(check_err(c));
+  }
   return SG_OK;
 }
 
@@ -436,11 +522,6 @@ int d2h(sg_ctx* c, void* dst, const void* src, size_t bytes) {
   return SG_OK;
 }
 
-#define SG_RET(x)             \
-  do {                        \
-    int _r = (x);             \
-    if (_r != SG_OK) return _r; \
-  } while (0)
 
 template <class T>
 int run_step(sg_ctx* c, int what, const void* u, const void* v, const void* w, const double* X, const double* Y,
@@ -507,6 +588,8 @@ int run_step(sg_ctx* c, int what, const void* u, const void* v, const void* w, c
       SG_RET(d2h(c, fz, dfz, fb));
     }
   }
+  if (c->leg_tc && (what & 2))
+    SG_TRY(cudaMemcpyAsync(c->h_err, c->d_err, sizeof(int), cudaMemcpyDeviceToHost, c->st), "error flag");
   SG_TRY(cudaGetLastError(), "step");
   return finish(c);
 }
@@ -564,6 +647,7 @@ void sg_destroy(sg_ctx* c) {
   for (int k = 0; k <= SG_NSTAGE; ++k)
     if (c->ev[k]) cudaEventDestroy(c->ev[k]);
   if (c->own_stream && c->st) cudaStreamDestroy(c->st);
+  if (c->h_err) cudaFreeHost(c->h_err);
   delete c;
 }
 
@@ -572,7 +656,7 @@ const char* sg_last_error(const sg_ctx* c) { return c ? c->err.c_str() : "null c
 int sg_synchronize(sg_ctx* c) {
   if (!c) return SG_ERR_ARG;
   SG_TRY(cudaStreamSynchronize(c->st), "synchronize");
-  return SG_OK;
+  return check_err(c);
 }
 
 int sg_interp(sg_ctx* c, const void* u, const void* v, const void* w, const double* X, const double* Y,

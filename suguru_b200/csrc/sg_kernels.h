@@ -80,8 +80,15 @@ struct LegProblem {
   int rpc;
   int Q, M, J, K;
   int tri;       // 1: k starts at m (synthesis: coefficients vanish for n<m)
-  int group;     // degree group (for the UMMA operand lookup)
+  int group;     // degree group
   int kind;      // 0 syn_D, 1 ana_D, 2 syn_O, 3 ana_O
+  // tensor-core operands (mixed path): per m, the bf16 hi image then the lo
+  // image of B_m, each Jp x Kp in UMMA core-matrix order; sBimg = 2 Jp Kp
+  const void* Bimg;
+  long long sBimg;
+  int Jp, Kp;    // J, K rounded up to multiples of 16
+  int vecA;      // A rows 16-byte aligned with K % 8 == 0: float4 loads
+  int vecD;      // D rows 16-byte aligned with J % 4 == 0: float4 stores
 };
 
 struct LegWork {  // one tile of a problem
@@ -91,6 +98,13 @@ struct LegWork {  // one tile of a problem
 template <class T>
 cudaError_t launch_legendre(const LegProblem* d_probs, const LegWork* d_work, int nwork, int maxJ, int maxK,
                             cudaStream_t st);
+// Tensor-core (tcgen05, BF16x3) contraction of FP32 problems; work items are
+// 128-row tiles.  d_err is set to 1 if an MMA completion wait times out.
+cudaError_t launch_legendre_mma(const LegProblem* d_probs, const LegWork* d_work, int nwork, int maxJp, int maxKp,
+                                int* d_err, int num_sms, cudaStream_t st);
+// bf16 hi/lo images of a table B[m][j][k] (row stride K, m stride sBm) in
+// UMMA core-matrix order: out[m][2][Jp/8][Kp/8][8][8]
+void host_umma_image(const double* B, long long sBm, int M, int J, int K, int Jp, int Kp, uint16_t* out);
 
 // Capsule-row work items for the pointwise kernels.
 struct RowWork {

@@ -1,0 +1,293 @@
+// sg_legendre_mma.cu -- the Legendre contractions of the mixed-precision path
+// on the 5th-generation tensor cores (tcgen05), in BF16x3 split precision.
+//
+// Each Legendre stage of the coupling step (the theta half of SPHEREPACK's
+// Gauss-grid analysis shagc.f:384-470 and synthesis shsgc.f:329-470, batched
+// over capsules and fields) is, for every zonal wavenumber m, a product
+//   D[q][j] = sum_k A[q][k] B_m[j][k]
+// of FP32 data rows A (one per capsule and field) with a per-degree FP64
+// table B_m (Legendre functions times Gauss weights).  Both operands are
+// K-major, so one tile is a single "TN" UMMA: M = 128 data rows, N = J padded
+// to a multiple of 16, K padded to a multiple of 16.
+//
+// Split precision: x = hi + lo with hi = bf16(x), lo = bf16(x - hi), and
+//   A B^T ~ A_hi B_hi^T + A_hi B_lo^T + A_lo B_hi^T
+// accumulated in FP32 in tensor memory (the dropped A_lo B_lo^T term is
+// ~2^-18 relative).  The tables are split once on the host into bf16 hi/lo
+// images laid out as UMMA operands; the data rows are split while staged.
+//
+// Shared-memory operand layout (no swizzle, K-major canonical form): an
+// R x Kp bf16 tile is stored as [R/8][Kp/8] core matrices of 8 rows x 16
+// bytes, so the leading-dimension byte offset (next core matrix along K) is
+// 128 B, the stride byte offset (next 8-row group) is Kp*16 B, and each K step
+// of 16 advances the start address by 256 B.
+//
+// Persistent CTAs of 128 threads (one warp per 32-lane TMEM subpartition)
+// loop over the (problem, m, 128-row tile) work list.  Thread 0 issues the
+// MMAs and commits them to an mbarrier; all threads wait with a bounded spin
+// (error flag, no trap, on timeout), read the accumulator with tcgen05.ld and
+// store the rows.
+#include <cuda_bf16.h>
+
+#include "sg_common.cuh"
+#include "sg_kernels.h"
+
+namespace sg {
+
+namespace {
+
+constexpr int MMA_M = 128;
+constexpr long long kSpinLimit = 1ll << 24;  // bounded mbarrier waits
+
+__device__ __forceinline__ uint32_t smem_u32(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
+
+// Shared-memory matrix descriptor: K-major, no swizzle (layout type 0),
+// descriptor version 1, base offset 0.
+__device__ __forceinline__ uint64_t umma_desc(uint32_t saddr, uint32_t lbo, uint32_t sbo) {
+  uint64_t d = 0;
+  d |= (uint64_t)((saddr >> 4) & 0x3FFFu);
+  d |= (uint64_t)((lbo >> 4) & 0x3FFFu) << 16;
+  d |= (uint64_t)((sbo >> 4) & 0x3FFFu) << 32;
+  d |= (uint64_t)1 << 46;
+  return d;
+}
+
+// Instruction descriptor of kind::f16: FP32 accumulator (bits 4-5 = 1), A and
+// B BF16 (bits 7-9 = 1, bits 10-12 = 1), both K-major (bits 15, 16 = 0),
+// N >> 3 in bits 17-22, M >> 4 in bits 24-28.
+__host__ __device__ constexpr uint32_t idesc_bf16(int M, int N) {
+  return (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(N >> 3) << 17) | ((uint32_t)(M >> 4) << 24);
+}
+
+__device__ __forceinline__ void umma_bf16(uint32_t tmem_d, uint64_t a, uint64_t b, uint32_t idesc, uint32_t acc) {
+  asm volatile(
+      "{\n\t.reg .pred p;\n\tsetp.ne.b32 p, %4, 0;\n\t"
+      "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n\t}\n" ::"r"(tmem_d),
+      "l"(a), "l"(b), "r"(idesc), "r"(acc));
+}
+
+__device__ __forceinline__ void umma_commit(uint64_t* bar) {
+  asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(smem_u32(bar))
+               : "memory");
+}
+
+__device__ __forceinline__ void fence_before() { asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory"); }
+__device__ __forceinline__ void fence_after() { asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory"); }
+__device__ __forceinline__ void fence_async_smem() { asm volatile("fence.proxy.async.shared::cta;" ::: "memory"); }
+
+__device__ __forceinline__ void mbar_init(uint64_t* bar, uint32_t count) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count) : "memory");
+  asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+}
+
+// Waits for the phase of the given parity to complete; false after the limit.
+__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity) {
+  const uint32_t a = smem_u32(bar);
+  for (long long it = 0; it < kSpinLimit; ++it) {
+    uint32_t done;
+    asm volatile(
+        "{\n\t.reg .pred p;\n\tmbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+        "selp.u32 %0, 1, 0, p;\n\t}\n"
+        : "=r"(done)
+        : "r"(a), "r"(parity)
+        : "memory");
+    if (done) return true;
+  }
+  return false;
+}
+
+__device__ __forceinline__ void tmem_ld16(uint32_t taddr, float* v) {
+  uint32_t r[16];
+  asm volatile(
+      "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15}, [%16];"
+      : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),
+        "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15])
+      : "r"(taddr));
+  asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+#pragma unroll
+  for (int i = 0; i < 16; ++i) v[i] = __uint_as_float(r[i]);
+}
+
+__device__ __forceinline__ void split8(const float* x, uint4& hi, uint4& lo) {
+  uint32_t h[4], l[4];
+#pragma unroll
+  for (int i = 0; i < 4; ++i) {
+    const __nv_bfloat16 h0 = __float2bfloat16_rn(x[2 * i]), h1 = __float2bfloat16_rn(x[2 * i + 1]);
+    const __nv_bfloat16 l0 = __float2bfloat16_rn(x[2 * i] - __bfloat162float(h0));
+    const __nv_bfloat16 l1 = __float2bfloat16_rn(x[2 * i + 1] - __bfloat162float(h1));
+    h[i] = (uint32_t)__bfloat16_as_ushort(h0) | ((uint32_t)__bfloat16_as_ushort(h1) << 16);
+    l[i] = (uint32_t)__bfloat16_as_ushort(l0) | ((uint32_t)__bfloat16_as_ushort(l1) << 16);
+  }
+  hi = make_uint4(h[0], h[1], h[2], h[3]);
+  lo = make_uint4(l[0], l[1], l[2], l[3]);
+}
+
+}  // namespace
+
+// smem: A hi, A lo (128 x maxKp each), B hi, B lo (maxJp x maxKp each), bf16.
+__global__ void __launch_bounds__(128) legendre_mma_kernel(const LegProblem* __restrict__ probs,
+                                                           const LegWork* __restrict__ work, int nwork, int maxJp,
+                                                           int maxKp, int tmem_cols, int* __restrict__ err) {
+  extern __shared__ __align__(128) unsigned char smem_raw[];
+  __shared__ __align__(8) uint64_t s_bar;
+  __shared__ uint32_t s_tmem;
+  uint16_t* sAh = (uint16_t*)smem_raw;
+  uint16_t* sAl = sAh + MMA_M * maxKp;
+  uint16_t* sBh = sAl + MMA_M * maxKp;
+  uint16_t* sBl = sBh + maxJp * maxKp;
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+
+  if (warp == 0) {
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(&s_tmem)),
+                 "r"(tmem_cols));
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
+  }
+  if (tid == 0) mbar_init(&s_bar, 1);
+  fence_before();
+  __syncthreads();
+  fence_after();
+  const uint32_t tmem = s_tmem;
+  uint32_t phase = 0;
+  bool ok = true;
+
+  for (int it = blockIdx.x; it < nwork && ok; it += gridDim.x) {
+    const LegWork wk = work[it];
+    const LegProblem& P = probs[wk.prob];
+    const int m = wk.m, q0 = wk.q0, K = P.K, J = P.J, Kp = P.Kp, Jp = P.Jp, KC = Kp >> 3;
+    const int nq = min(MMA_M, P.Q - q0);
+    // ---- table image for this m: a straight 16-byte copy (already split and laid out)
+    {
+      const uint4* src = (const uint4*)((const uint16_t*)P.Bimg + (long long)m * P.sBimg);
+      const int n16 = (Jp * Kp) >> 3;  // uint4 per image
+      uint4* dh = (uint4*)sBh;
+      uint4* dl = (uint4*)sBl;
+      for (int i = tid; i < n16; i += 128) {
+        dh[i] = src[i];
+        dl[i] = src[n16 + i];
+      }
+    }
+    // ---- data rows: FP32 -> bf16 hi/lo, one 8-element core-matrix row per
+    // thread and step; consecutive threads take consecutive rows
+    {
+      const float* A = (const float*)P.A;
+      for (int idx = tid; idx < MMA_M * KC; idx += 128) {
+        const int kc = idx >> 7, q = idx & 127, k0 = kc << 3;
+        float x[8];
+        if (q < nq) {
+          const int qq = q0 + q, c = qq / P.rpc, r = qq - c * P.rpc;
+          const float* row = A + (long long)c * P.sAc + (long long)r * P.sAr + (long long)m * P.sAm;
+          if (P.vecA && k0 + 8 <= K) {
+            const float4 a = *(const float4*)(row + k0), b = *(const float4*)(row + k0 + 4);
+            x[0] = a.x; x[1] = a.y; x[2] = a.z; x[3] = a.w;
+            x[4] = b.x; x[5] = b.y; x[6] = b.z; x[7] = b.w;
+          } else {
+#pragma unroll
+            for (int i = 0; i < 8; ++i) x[i] = (k0 + i < K) ? row[k0 + i] : 0.f;
+          }
+        } else {
+#pragma unroll
+          for (int i = 0; i < 8; ++i) x[i] = 0.f;
+        }
+        uint4 hi, lo;
+        split8(x, hi, lo);
+        const int o = (((q >> 3) * KC + kc) << 6) + ((q & 7) << 3);
+        *(uint4*)(sAh + o) = hi;
+        *(uint4*)(sAl + o) = lo;
+      }
+    }
+    fence_async_smem();  // generic-proxy smem writes -> visible to the tensor core
+    fence_before();
+    __syncthreads();
+    fence_after();
+    // ---- MMAs: one thread issues 3 per K step of 16 (hi.hi, hi.lo, lo.hi)
+    if (tid == 0) {
+      const uint32_t idesc = idesc_bf16(MMA_M, Jp);
+      const uint32_t lbo = 128, sbo = (uint32_t)Kp * 16;
+      const uint32_t aH = smem_u32(sAh), aL = smem_u32(sAl), bH = smem_u32(sBh), bL = smem_u32(sBl);
+      const int s0 = P.tri ? (m >> 4) : 0;  // synthesis: coefficients below n = m vanish
+      uint32_t acc = 0;
+      for (int s = s0; s < (Kp >> 4); ++s) {
+        const uint32_t o = (uint32_t)s * 256;
+        umma_bf16(tmem, umma_desc(aH + o, lbo, sbo), umma_desc(bH + o, lbo, sbo), idesc, acc);
+        acc = 1;
+        umma_bf16(tmem, umma_desc(aH + o, lbo, sbo), umma_desc(bL + o, lbo, sbo), idesc, 1);
+        umma_bf16(tmem, umma_desc(aL + o, lbo, sbo), umma_desc(bH + o, lbo, sbo), idesc, 1);
+      }
+      umma_commit(&s_bar);
+    }
+    __syncwarp();
+    // every thread waits; the CTA then agrees on the outcome so that all of
+    // its threads leave the loop together on a timeout
+    const int waited = mbar_wait(&s_bar, phase) ? 1 : 0;
+    if (!__syncthreads_and(waited)) {
+      if (tid == 0) atomicExch(err, 1);
+      ok = false;
+      break;
+    }
+    phase ^= 1u;
+    fence_after();
+    // ---- epilogue: warp w holds rows 32w..32w+31 of the tile (TMEM lanes)
+    {
+      const int q = warp * 32 + lane;
+      float* drow = nullptr;
+      if (q < nq) {
+        const int qq = q0 + q, c = qq / P.rpc, r = qq - c * P.rpc;
+        drow = (float*)P.D + (long long)c * P.sDc + (long long)r * P.sDr + (long long)m * P.sDm;
+      }
+      for (int j0 = 0; j0 < Jp; j0 += 16) {
+        float v[16];
+        tmem_ld16(tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)j0, v);
+        if (drow) {
+          if (P.vecD && j0 + 16 <= J) {
+#pragma unroll
+            for (int i = 0; i < 16; i += 4) *(float4*)(drow + j0 + i) = make_float4(v[i], v[i + 1], v[i + 2], v[i + 3]);
+          } else {
+#pragma unroll
+            for (int i = 0; i < 16; ++i)
+              if (j0 + i < J) drow[j0 + i] = v[i];
+          }
+        }
+      }
+    }
+    fence_before();
+    __syncthreads();  // TMEM reads and smem operands done before the next tile
+    fence_after();
+  }
+  if (!ok) {
+    // a commit that never arrived: give the tensor core a bounded chance to
+    // finish before freeing its accumulator
+    mbar_wait(&s_bar, phase);
+  }
+  fence_before();
+  __syncthreads();
+  fence_after();
+  if (warp == 0)
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(tmem_cols));
+}
+
+size_t legendre_mma_smem(int maxJp, int maxKp) {
+  return (size_t)2 * sizeof(uint16_t) * (MMA_M + maxJp) * maxKp;
+}
+
+cudaError_t launch_legendre_mma(const LegProblem* d_probs, const LegWork* d_work, int nwork, int maxJp, int maxKp,
+                                int* d_err, int num_sms, cudaStream_t st) {
+  if (nwork <= 0) return cudaSuccess;
+  if (maxJp < 16 || maxJp > 256 || (maxJp & 15) || maxKp < 16 || (maxKp & 15)) return cudaErrorInvalidValue;
+  // TMEM columns: a power of two >= 32 covering N = Jp; CTAs per SM limited
+  // (through shared memory) so that their allocations always fit in 512 columns
+  int cols = 32;
+  while (cols < maxJp) cols <<= 1;
+  const int per_sm = 512 / cols < 4 ? 512 / cols : 4;
+  size_t smem = legendre_mma_smem(maxJp, maxKp);
+  // (per_sm + 1) CTAs of this size exceed the SM's 228 KB of shared memory
+  const size_t floor_smem = (size_t)(228 * 1024) / (size_t)(per_sm + 1);
+  if (smem < floor_smem) smem = floor_smem;
+  if (smem > (size_t)227 * 1024) return cudaErrorInvalidValue;
+  cudaError_t e = cudaFuncSetAttribute(legendre_mma_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  if (e != cudaSuccess) return e;
+  const int grid = nwork < num_sms * per_sm ? nwork : num_sms * per_sm;
+  legendre_mma_kernel<<<grid, 128, smem, st>>>(d_probs, d_work, nwork, maxJp, maxKp, cols, d_err);
+  return cudaGetLastError();
+}
+
+}  // namespace sg

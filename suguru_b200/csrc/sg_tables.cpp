@@ -9,6 +9,7 @@
 // the standard normalised three-term recurrence for P^m_n, and the m+-1
 // ladder identity for d/dtheta (applied twice for the second derivative).
 #include <cmath>
+#include <cstring>
 #include <vector>
 
 #include "sg_kernels.h"
@@ -98,6 +99,41 @@ void host_legendre(double th, int mm, int nn, double* P, double* dP, double* d2P
       if (dP) dP[o] = ok ? D[q] : 0.0;
       if (d2P) d2P[o] = ok ? D2[q] : 0.0;
     }
+}
+
+
+// ---------------------------------------------------------------- bf16 split
+// Round-to-nearest-even FP32 -> bf16 (bit pattern), and back.
+static uint16_t f32_to_bf16(float f) {
+  uint32_t u;
+  std::memcpy(&u, &f, 4);
+  if ((u & 0x7fffffffu) > 0x7f800000u) return (uint16_t)((u >> 16) | 0x40u);  // NaN stays NaN
+  u += 0x7fffu + ((u >> 16) & 1u);
+  return (uint16_t)(u >> 16);
+}
+static double bf16_to_double(uint16_t h) {
+  const uint32_t u = (uint32_t)h << 16;
+  float f;
+  std::memcpy(&f, &u, 4);
+  return (double)f;
+}
+
+void host_umma_image(const double* B, long long sBm, int M, int J, int K, int Jp, int Kp, uint16_t* out) {
+  const int KC = Kp / 8;
+  const size_t img = (size_t)Jp * Kp;
+  for (int m = 0; m < M; ++m) {
+    uint16_t* hi = out + (size_t)m * 2 * img;
+    uint16_t* lo = hi + img;
+    for (int j = 0; j < Jp; ++j)
+      for (int k = 0; k < Kp; ++k) {
+        const double x = (j < J && k < K) ? B[(size_t)m * sBm + (size_t)j * K + k] : 0.0;
+        const uint16_t h = f32_to_bf16((float)x);
+        const uint16_t l = f32_to_bf16((float)(x - bf16_to_double(h)));
+        const size_t o = ((size_t)(j / 8) * KC + k / 8) * 64 + (j % 8) * 8 + (k % 8);
+        hi[o] = h;
+        lo[o] = l;
+      }
+  }
 }
 
 }  // namespace sg

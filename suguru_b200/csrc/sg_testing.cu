@@ -1,0 +1,81 @@
+// sg_testing.cu -- test hooks (include/sg_testing.h): run one batched
+// Legendre contraction through the tensor-core or the CUDA-core kernel on
+// caller data, so that the tests can check the UMMA operand layout, the
+// BF16x3 split and the epilogue element by element against numpy.
+#include <cstring>
+#include <vector>
+
+#include "sg_kernels.h"
+#include "sg_testing.h"
+
+using namespace sg;
+
+extern "C" int sg_test_legendre(int tensor_cores, int M, int Q, int J, int K, int tri, const double* B,
+                                const float* A, float* D) {
+  if (M < 1 || Q < 1 || J < 1 || K < 1 || J > 256 || K > 256 || !B || !A || !D) return 5;
+  const int Jp = (J + 15) / 16 * 16, Kp = (K + 15) / 16 * 16;
+  // problem: A[m][q][k] rows, B[m][j][k], D[m][q][j]
+  LegProblem p{};
+  p.sAc = (long long)K;  // capsule index = q (one row per capsule)
+  p.sAr = 0;
+  p.sAm = (long long)Q * K;
+  p.sBm = (long long)J * K;
+  p.sDc = J;
+  p.sDr = 0;
+  p.sDm = (long long)Q * J;
+  p.rpc = 1;
+  p.Q = Q;
+  p.M = M;
+  p.J = J;
+  p.K = K;
+  p.tri = tri;
+  p.Jp = Jp;
+  p.Kp = Kp;
+  p.sBimg = 2LL * Jp * Kp;
+  std::vector<uint16_t> img((size_t)M * p.sBimg);
+  host_umma_image(B, p.sBm, M, J, K, Jp, Kp, img.data());
+  std::vector<float> Bf((size_t)M * J * K);
+  for (size_t i = 0; i < Bf.size(); ++i) Bf[i] = (float)B[i];
+  std::vector<LegWork> work;
+  const int qt = tensor_cores ? 128 : 32;
+  for (int m = 0; m < M; ++m)
+    for (int q0 = 0; q0 < Q; q0 += qt) work.push_back(LegWork{0, m, q0});
+  void *dA = nullptr, *dB = nullptr, *dD = nullptr, *dI = nullptr, *dP = nullptr, *dW = nullptr, *dE = nullptr;
+  const size_t na = (size_t)M * Q * K, nd = (size_t)M * Q * J;
+  int rc = 0;
+  auto ok = [&](cudaError_t e) {
+    if (e != cudaSuccess && rc == 0) rc = 2;
+    return rc == 0;
+  };
+  if (ok(cudaMalloc(&dA, 4 * na)) && ok(cudaMalloc(&dB, 4 * Bf.size())) && ok(cudaMalloc(&dD, 4 * nd)) &&
+      ok(cudaMalloc(&dI, 2 * img.size())) && ok(cudaMalloc(&dP, sizeof(LegProblem))) &&
+      ok(cudaMalloc(&dW, sizeof(LegWork) * work.size())) && ok(cudaMalloc(&dE, sizeof(int)))) {
+    p.A = dA;
+    p.B = dB;
+    p.D = dD;
+    p.Bimg = dI;
+    p.vecA = (K % 8 == 0) ? 1 : 0;
+    p.vecD = (J % 4 == 0) ? 1 : 0;
+    int dev = 0, sms = 148;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    if (ok(cudaMemcpy(dA, A, 4 * na, cudaMemcpyHostToDevice)) &&
+        ok(cudaMemcpy(dB, Bf.data(), 4 * Bf.size(), cudaMemcpyHostToDevice)) &&
+        ok(cudaMemcpy(dI, img.data(), 2 * img.size(), cudaMemcpyHostToDevice)) &&
+        ok(cudaMemcpy(dP, &p, sizeof(p), cudaMemcpyHostToDevice)) &&
+        ok(cudaMemcpy(dW, work.data(), sizeof(LegWork) * work.size(), cudaMemcpyHostToDevice)) &&
+        ok(cudaMemset(dE, 0, sizeof(int))) && ok(cudaMemset(dD, 0xff, 4 * nd))) {
+      if (tensor_cores)
+        ok(launch_legendre_mma((const LegProblem*)dP, (const LegWork*)dW, (int)work.size(), Jp, Kp, (int*)dE, sms, 0));
+      else
+        ok(launch_legendre<float>((const LegProblem*)dP, (const LegWork*)dW, (int)work.size(), J, K, 0));
+      int err = 0;
+      if (ok(cudaDeviceSynchronize()) && ok(cudaMemcpy(&err, dE, sizeof(int), cudaMemcpyDeviceToHost)) &&
+          ok(cudaMemcpy(D, dD, 4 * nd, cudaMemcpyDeviceToHost)))
+        if (err) rc = 3;
+    }
+  }
+  for (void* q : {dA, dB, dD, dI, dP, dW, dE})
+    if (q) cudaFree(q);
+  return rc;
+}

@@ -20,8 +20,8 @@ def lib():
     return coupling.lib()
 
 
-def header_symbols():
-    text = open(os.path.join(ROOT, "include", "sg_coupling.h")).read()
+def header_symbols(name="sg_coupling.h"):
+    text = open(os.path.join(ROOT, "include", name)).read()
     text = re.sub(r"/\*.*?\*/", "", text, flags=re.S)
     return sorted(set(re.findall(r"\b(sg_[a-z_]+)\s*\(", text)))
 
@@ -32,6 +32,15 @@ def test_exports_every_declared_symbol(lib):
     for s in syms:
         assert hasattr(lib, s), s
     assert sorted(coupling.EXPORTS) == syms
+
+
+def test_every_header_is_covered(lib):
+    headers = sorted(f for f in os.listdir(os.path.join(ROOT, "include")) if f.endswith(".h"))
+    assert headers == ["sg_coupling.h", "sg_testing.h"]
+    syms = header_symbols("sg_testing.h")
+    for s in syms:
+        assert hasattr(lib, s), s
+    assert sorted(coupling.TEST_EXPORTS) == syms
 
 
 def test_build_flags_target_sm100a():
