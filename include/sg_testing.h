@@ -19,6 +19,15 @@ extern "C" {
 int sg_test_legendre(int tensor_cores, int M, int Q, int J, int K, int tri, const double* B,
                      const float* A, float* D);
 
+/* One dense product of the surrogate network (sg_gemm.cu) on host data:
+ *   C = alpha A B^T (+ bias[n]) (then GELU if gelu != 0), A [M][K], B [N][K],
+ * K a multiple of 64.  split = 0: A, B are bf16 bit patterns (uint16);
+ * split = 1: A, B are FP32 and run as BF16x3.  Optional outputs (may be
+ * NULL): Cpre the FP32 value before GELU, Cb the bf16 result [M][N], CbT the
+ * bf16 result transposed [N][M].  Returns 0, 5, 2 or 3 as above. */
+int sg_test_gemm(int split, int M, int N, int K, const void* A, const void* B, const float* bias,
+                 int gelu, float alpha, float* C, float* Cpre, unsigned short* Cb, unsigned short* CbT);
+
 #ifdef __cplusplus
 }
 #endif

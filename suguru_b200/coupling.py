@@ -36,7 +36,7 @@ EXPORTS = ["sg_create", "sg_destroy", "sg_last_error", "sg_synchronize", "sg_int
            "sg_set_tile_shape", "sg_get_tile_shape", "sg_autotune", "sg_graph_capture", "sg_graph_launch",
            "sg_graph_release"]
 # test hooks declared in include/sg_testing.h
-TEST_EXPORTS = ["sg_test_legendre"]
+TEST_EXPORTS = ["sg_test_legendre", "sg_test_gemm"]
 TILE_SHAPES = ((32, 8, 4), (16, 16, 8), (32, 8, 8), (8, 8, 4))
 STAGES = ("bin", "interp", "membrane", "spread")
 
@@ -94,6 +94,7 @@ def lib():
     L.sg_graph_launch.argtypes = [vp]
     L.sg_graph_release.argtypes = [vp]
     L.sg_test_legendre.argtypes = [ctypes.c_int] * 6 + [vp] * 3
+    L.sg_test_gemm.argtypes = [ctypes.c_int] * 4 + [vp] * 3 + [ctypes.c_int, ctypes.c_float] + [vp] * 4
     d = ctypes.c_double
     L.sg_spread_noalloc.argtypes = ([ctypes.c_int] * 3 + [d] * 3 + [ctypes.c_long] + [vp] * 11)
     _LIB = L
@@ -112,6 +113,40 @@ def test_legendre(A, B, tensor_cores=True, tri=False):
     if rc:
         raise SgError(rc, "sg_test_legendre")
     return D
+
+
+def to_bf16_bits(x):
+    """Round-to-nearest-even FP32 -> bf16 bit patterns (uint16)."""
+    u = np.ascontiguousarray(x, dtype=np.float32).view(np.uint32).astype(np.uint64)
+    r = ((u + 0x7FFF + ((u >> 16) & 1)) >> 16).astype(np.uint16)
+    return r
+
+
+def from_bf16_bits(b):
+    return (np.asarray(b, dtype=np.uint32) << 16).view(np.float32)
+
+
+def test_gemm(A, B, split=False, bias=None, gelu=False, alpha=1.0):
+    """C = alpha A B^T (+ bias) (GELU) on the tensor cores (test hook).
+
+    split=False: A, B are rounded to bf16 first; split=True: FP32 in, BF16x3.
+    Returns (C, Cpre, Cb, CbT) with the bf16 outputs as FP32 values."""
+    A = np.ascontiguousarray(A, dtype=np.float32)
+    B = np.ascontiguousarray(B, dtype=np.float32)
+    M, K = A.shape
+    N = B.shape[0]
+    a = A if split else to_bf16_bits(A)
+    b = B if split else to_bf16_bits(B)
+    C = np.zeros((M, N), np.float32)
+    P = np.zeros((M, N), np.float32)
+    Cb = np.zeros((M, N), np.uint16)
+    CbT = np.zeros((N, M), np.uint16)
+    bi = None if bias is None else np.ascontiguousarray(bias, dtype=np.float32)
+    rc = lib().sg_test_gemm(int(split), M, N, K, _ptr(a), _ptr(b), _ptr(bi), int(gelu), ctypes.c_float(alpha),
+                            _ptr(C), _ptr(P), _ptr(Cb), _ptr(CbT))
+    if rc:
+        raise SgError(rc, "sg_test_gemm")
+    return C, P, from_bf16_bits(Cb), from_bf16_bits(CbT)
 
 
 def gauss(nlat):

@@ -1,5 +1,6 @@
 // sg_kernels.h -- internal declarations shared by the .cu files of the library.
 #pragma once
+#include <cuda_bf16.h>
 #include <cuda_runtime.h>
 #include <stdint.h>
 #include <vector>
@@ -102,6 +103,32 @@ cudaError_t launch_legendre(const LegProblem* d_probs, const LegWork* d_work, in
 // 128-row tiles.  d_err is set to 1 if an MMA completion wait times out.
 cudaError_t launch_legendre_mma(const LegProblem* d_probs, const LegWork* d_work, int nwork, int maxJp, int maxKp,
                                 int* d_err, int num_sms, cudaStream_t st);
+// Dense product on the tensor cores (sg_gemm.cu):
+//   C = alpha A B^T (+ bias[n]) (then GELU), A [M][K], B [N][K], K % 64 == 0.
+// split = 0: A, B bf16; split = 1: A, B FP32, split into bf16 hi/lo (BF16x3).
+// Outputs that are null are skipped; CbT is [N][M] (transposed).
+struct GemmArgs {
+  int M = 0, N = 0, K = 0;
+  int split = 0;
+  const void* A = nullptr;
+  long long lda = 0;
+  const void* B = nullptr;
+  long long ldb = 0;
+  float alpha = 1.f;
+  const float* bias = nullptr;
+  int gelu = 0;
+  int accumulate = 0;  // Cf += result
+  float* Cf = nullptr;
+  long long ldc = 0;
+  float* Cpre = nullptr;  // FP32 value after bias, before GELU
+  long long ldpre = 0;
+  __nv_bfloat16* Cb = nullptr;
+  long long ldcb = 0;
+  __nv_bfloat16* CbT = nullptr;
+  long long ldcbt = 0;
+};
+cudaError_t launch_gemm(const GemmArgs& g, int* d_err, cudaStream_t st);
+
 // bf16 hi/lo images of a table B[m][j][k] (row stride K, m stride sBm) in
 // UMMA core-matrix order: out[m][2][Jp/8][Kp/8][8][8]
 void host_umma_image(const double* B, long long sBm, int M, int J, int K, int Jp, int Kp, uint16_t* out);

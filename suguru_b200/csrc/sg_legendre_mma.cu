@@ -27,100 +27,16 @@
 // MMAs and commits them to an mbarrier; all threads wait with a bounded spin
 // (error flag, no trap, on timeout), read the accumulator with tcgen05.ld and
 // store the rows.
-#include <cuda_bf16.h>
-
 #include "sg_common.cuh"
 #include "sg_kernels.h"
+#include "sg_umma.cuh"
 
 namespace sg {
 
 namespace {
 
 constexpr int MMA_M = 128;
-constexpr long long kSpinLimit = 1ll << 24;  // bounded mbarrier waits
-
-__device__ __forceinline__ uint32_t smem_u32(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
-
-// Shared-memory matrix descriptor: K-major, no swizzle (layout type 0),
-// descriptor version 1, base offset 0.
-__device__ __forceinline__ uint64_t umma_desc(uint32_t saddr, uint32_t lbo, uint32_t sbo) {
-  uint64_t d = 0;
-  d |= (uint64_t)((saddr >> 4) & 0x3FFFu);
-  d |= (uint64_t)((lbo >> 4) & 0x3FFFu) << 16;
-  d |= (uint64_t)((sbo >> 4) & 0x3FFFu) << 32;
-  d |= (uint64_t)1 << 46;
-  return d;
-}
-
-// Instruction descriptor of kind::f16: FP32 accumulator (bits 4-5 = 1), A and
-// B BF16 (bits 7-9 = 1, bits 10-12 = 1), both K-major (bits 15, 16 = 0),
-// N >> 3 in bits 17-22, M >> 4 in bits 24-28.
-__host__ __device__ constexpr uint32_t idesc_bf16(int M, int N) {
-  return (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(N >> 3) << 17) | ((uint32_t)(M >> 4) << 24);
-}
-
-__device__ __forceinline__ void umma_bf16(uint32_t tmem_d, uint64_t a, uint64_t b, uint32_t idesc, uint32_t acc) {
-  asm volatile(
-      "{\n\t.reg .pred p;\n\tsetp.ne.b32 p, %4, 0;\n\t"
-      "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n\t}\n" ::"r"(tmem_d),
-      "l"(a), "l"(b), "r"(idesc), "r"(acc));
-}
-
-__device__ __forceinline__ void umma_commit(uint64_t* bar) {
-  asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(smem_u32(bar))
-               : "memory");
-}
-
-__device__ __forceinline__ void fence_before() { asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory"); }
-__device__ __forceinline__ void fence_after() { asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory"); }
-__device__ __forceinline__ void fence_async_smem() { asm volatile("fence.proxy.async.shared::cta;" ::: "memory"); }
-
-__device__ __forceinline__ void mbar_init(uint64_t* bar, uint32_t count) {
-  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count) : "memory");
-  asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
-}
-
-// Waits for the phase of the given parity to complete; false after the limit.
-__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity) {
-  const uint32_t a = smem_u32(bar);
-  for (long long it = 0; it < kSpinLimit; ++it) {
-    uint32_t done;
-    asm volatile(
-        "{\n\t.reg .pred p;\n\tmbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
-        "selp.u32 %0, 1, 0, p;\n\t}\n"
-        : "=r"(done)
-        : "r"(a), "r"(parity)
-        : "memory");
-    if (done) return true;
-  }
-  return false;
-}
-
-__device__ __forceinline__ void tmem_ld16(uint32_t taddr, float* v) {
-  uint32_t r[16];
-  asm volatile(
-      "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15}, [%16];"
-      : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),
-        "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15])
-      : "r"(taddr));
-  asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
-#pragma unroll
-  for (int i = 0; i < 16; ++i) v[i] = __uint_as_float(r[i]);
-}
-
-__device__ __forceinline__ void split8(const float* x, uint4& hi, uint4& lo) {
-  uint32_t h[4], l[4];
-#pragma unroll
-  for (int i = 0; i < 4; ++i) {
-    const __nv_bfloat16 h0 = __float2bfloat16_rn(x[2 * i]), h1 = __float2bfloat16_rn(x[2 * i + 1]);
-    const __nv_bfloat16 l0 = __float2bfloat16_rn(x[2 * i] - __bfloat162float(h0));
-    const __nv_bfloat16 l1 = __float2bfloat16_rn(x[2 * i + 1] - __bfloat162float(h1));
-    h[i] = (uint32_t)__bfloat16_as_ushort(h0) | ((uint32_t)__bfloat16_as_ushort(h1) << 16);
-    l[i] = (uint32_t)__bfloat16_as_ushort(l0) | ((uint32_t)__bfloat16_as_ushort(l1) << 16);
-  }
-  hi = make_uint4(h[0], h[1], h[2], h[3]);
-  lo = make_uint4(l[0], l[1], l[2], l[3]);
-}
+using namespace umma;
 
 }  // namespace
 
@@ -138,9 +54,7 @@ __global__ void __launch_bounds__(128) legendre_mma_kernel(const LegProblem* __r
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
 
   if (warp == 0) {
-    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(&s_tmem)),
-                 "r"(tmem_cols));
-    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
+    tmem_alloc(&s_tmem, (uint32_t)tmem_cols);
   }
   if (tid == 0) mbar_init(&s_bar, 1);
   fence_before();
@@ -208,12 +122,12 @@ __global__ void __launch_bounds__(128) legendre_mma_kernel(const LegProblem* __r
       uint32_t acc = 0;
       for (int s = s0; s < (Kp >> 4); ++s) {
         const uint32_t o = (uint32_t)s * 256;
-        umma_bf16(tmem, umma_desc(aH + o, lbo, sbo), umma_desc(bH + o, lbo, sbo), idesc, acc);
+        mma_bf16(tmem, desc(aH + o, lbo, sbo), desc(bH + o, lbo, sbo), idesc, acc);
         acc = 1;
-        umma_bf16(tmem, umma_desc(aH + o, lbo, sbo), umma_desc(bL + o, lbo, sbo), idesc, 1);
-        umma_bf16(tmem, umma_desc(aL + o, lbo, sbo), umma_desc(bH + o, lbo, sbo), idesc, 1);
+        mma_bf16(tmem, desc(aH + o, lbo, sbo), desc(bL + o, lbo, sbo), idesc, 1);
+        mma_bf16(tmem, desc(aL + o, lbo, sbo), desc(bH + o, lbo, sbo), idesc, 1);
       }
-      umma_commit(&s_bar);
+      commit(&s_bar);
     }
     __syncwarp();
     // every thread waits; the CTA then agrees on the outcome so that all of
@@ -262,7 +176,7 @@ __global__ void __launch_bounds__(128) legendre_mma_kernel(const LegProblem* __r
   __syncthreads();
   fence_after();
   if (warp == 0)
-    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(tmem_cols));
+    tmem_free(tmem, (uint32_t)tmem_cols);
 }
 
 size_t legendre_mma_smem(int maxJp, int maxKp) {

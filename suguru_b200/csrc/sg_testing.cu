@@ -79,3 +79,43 @@ extern "C" int sg_test_legendre(int tensor_cores, int M, int Q, int J, int K, in
     if (q) cudaFree(q);
   return rc;
 }
+
+extern "C" int sg_test_gemm(int split, int M, int N, int K, const void* A, const void* B, const float* bias,
+                            int gelu, float alpha, float* C, float* Cpre, unsigned short* Cb, unsigned short* CbT) {
+  if (M < 1 || N < 1 || K < 0 || K % 64 || !A || !B || !C) return 5;
+  const size_t es = split ? 4 : 2;
+  void *dA = nullptr, *dB = nullptr, *dC = nullptr, *dP = nullptr, *dCb = nullptr, *dCbT = nullptr, *dbias = nullptr,
+       *dE = nullptr;
+  int rc = 0;
+  auto ok = [&](cudaError_t e) {
+    if (e != cudaSuccess && rc == 0) rc = 2;
+    return rc == 0;
+  };
+  const size_t nc = (size_t)M * N;
+  if (ok(cudaMalloc(&dA, es * M * (size_t)K + 16)) && ok(cudaMalloc(&dB, es * N * (size_t)K + 16)) &&
+      ok(cudaMalloc(&dC, 4 * nc)) && ok(cudaMalloc(&dP, 4 * nc)) && ok(cudaMalloc(&dCb, 2 * nc)) &&
+      ok(cudaMalloc(&dCbT, 2 * nc)) && ok(cudaMalloc(&dbias, 4 * (size_t)N)) && ok(cudaMalloc(&dE, sizeof(int))) &&
+      ok(cudaMemcpy(dA, A, es * M * (size_t)K, cudaMemcpyHostToDevice)) &&
+      ok(cudaMemcpy(dB, B, es * N * (size_t)K, cudaMemcpyHostToDevice)) && ok(cudaMemset(dE, 0, sizeof(int))) &&
+      ok(cudaMemset(dC, 0xff, 4 * nc)) && (!bias || ok(cudaMemcpy(dbias, bias, 4 * (size_t)N, cudaMemcpyHostToDevice)))) {
+    GemmArgs g;
+    g.M = M; g.N = N; g.K = K; g.split = split;
+    g.A = dA; g.lda = K; g.B = dB; g.ldb = K;
+    g.alpha = alpha; g.bias = bias ? (const float*)dbias : nullptr; g.gelu = gelu;
+    g.Cf = (float*)dC; g.ldc = N;
+    g.Cpre = Cpre ? (float*)dP : nullptr; g.ldpre = N;
+    g.Cb = Cb ? (__nv_bfloat16*)dCb : nullptr; g.ldcb = N;
+    g.CbT = CbT ? (__nv_bfloat16*)dCbT : nullptr; g.ldcbt = M;
+    int err = 0;
+    if (ok(launch_gemm(g, (int*)dE, 0)) && ok(cudaDeviceSynchronize()) &&
+        ok(cudaMemcpy(&err, dE, sizeof(int), cudaMemcpyDeviceToHost)) &&
+        ok(cudaMemcpy(C, dC, 4 * nc, cudaMemcpyDeviceToHost)) &&
+        (!Cpre || ok(cudaMemcpy(Cpre, dP, 4 * nc, cudaMemcpyDeviceToHost))) &&
+        (!Cb || ok(cudaMemcpy(Cb, dCb, 2 * nc, cudaMemcpyDeviceToHost))) &&
+        (!CbT || ok(cudaMemcpy(CbT, dCbT, 2 * nc, cudaMemcpyDeviceToHost))))
+      if (err) rc = 3;
+  }
+  for (void* q : {dA, dB, dC, dP, dCb, dCbT, dbias, dE})
+    if (q) cudaFree(q);
+  return rc;
+}
