@@ -43,6 +43,10 @@ def parse_args():
     p.add_argument("--only", default=None, choices=["mixed", "fp64"],
                    help="time one path only, no e2e (for profiler captures)")
     p.add_argument("--cpu-sample-caps", type=int, default=64)
+    p.add_argument("--no-surrogate", action="store_true", help="skip training and timing the surrogate path")
+    p.add_argument("--sur-samples", type=int, default=200000)
+    p.add_argument("--sur-epochs", type=int, default=40)
+    p.add_argument("--sur-loose-tol", type=float, default=3e-2)
     return p.parse_args()
 
 
@@ -134,6 +138,12 @@ def cs_tile_shape(shape):
     return TILE_SHAPES[shape]
 
 
+def rel_l2_t(a, b):
+    import torch
+    d = torch.linalg.vector_norm((a.double() - b.double()).ravel())
+    return float(d / torch.clamp(torch.linalg.vector_norm(b.double().ravel()), min=1e-300))
+
+
 def run_ours(args):
     import torch
     import torch.distributed as dist
@@ -163,17 +173,21 @@ def run_ours(args):
     X = [torch.from_numpy(a).to(dev) for a in (wl.x, wl.y, wl.z)]
     flush = torch.empty(2 * L2_BYTES // 4, dtype=torch.float32, device=dev)
 
-    def time_path(precision):
+    def make_cs(precision, surrogate=False):
+        return CouplingStep(wl.grid, wl.degree, wl.radius, wl.gs, wl.csk, precision=precision, mem="device",
+                            device=local, stream=stream.cuda_stream, async_=True, surrogate=surrogate)
+
+    def time_path(cs, precision, tune=True):
         dtype = np.float64 if precision == "fp64" else np.float32
         uvw, td = dev_inputs(dtype)
-        cs = CouplingStep(wl.grid, wl.degree, wl.radius, wl.gs, wl.csk, precision=precision, mem="device",
-                          device=local, stream=stream.cuda_stream, async_=True)
-        cs.set_profiling(True)
         lag = [torch.empty(n, dtype=td, device=dev) for _ in range(10)]
         eul = [torch.empty(cs.field_shape, dtype=td, device=dev) for _ in range(3)]
-        # the library's autotuner picks the spreading tile shape (untimed set-up)
-        cs.set_profiling(False)
-        tile, _ = cs.autotune(*uvw, *X, lag_out=lag, eul_out=eul, reps=3)
+        tile = 0
+        if tune:  # the library's autotuner picks the spreading tile shape (untimed set-up)
+            cs.set_profiling(False)
+            tile, _ = cs.autotune(*uvw, *X, lag_out=lag, eul_out=eul, reps=3)
+        else:
+            tile = cs.tile_shape()[0]
         cs.set_profiling(True)
         for _ in range(args.warmup):
             cs.step(*uvw, *X, lag_out=lag, eul_out=eul)
@@ -201,28 +215,78 @@ def run_ours(args):
             t = torch.tensor([ms], device=dev)
             dist.all_reduce(t, op=dist.ReduceOp.MAX)
             ms = float(t.item())
-        cs.close()
         return dict(ms_per_step=ms / args.steps, stages={k: v / args.steps for k, v in stages.items()},
                     launches=launches, clocks=clk.summary(), s=4 if precision != "fp64" else 8,
-                    tile="x".join(map(str, cs_tile_shape(tile))))
+                    tile="x".join(map(str, cs_tile_shape(tile))), out=[t.clone() for t in lag + eul])
+
+    def errors(out, ref):
+        """Relative L2 of the mixed-path results against the FP64 plain path (itself within 1e-10 of the oracle)."""
+        return {"velocity": max(rel_l2_t(out[c], ref[c]) for c in range(3)),
+                "force": max(rel_l2_t(out[3 + c], ref[3 + c]) for c in range(3)),
+                "spread_field": max(rel_l2_t(out[10 + c], ref[10 + c]) for c in range(3))}
 
     if args.only:
-        r = time_path(args.only)
+        cs = make_cs(args.only)
+        r = time_path(cs, args.only)
+        cs.close()
         if rank == 0:
             print(json.dumps({"only": args.only, "ms_per_step": r["ms_per_step"], "stages_ms": r["stages"],
                               "points_per_s": world * n / (r["ms_per_step"] / 1e3)}))
         if world > 1:
             dist.destroy_process_group()
         return None
-    mixed = time_path("mixed")
-    fp64 = time_path("fp64")
 
-    # e2e through the public API with pinned host buffers (mixed path)
+    cs64 = make_cs("fp64")
+    fp64 = time_path(cs64, "fp64")
+    cs64.close()
+    csm = make_cs("mixed")
+    mixed = time_path(csm, "mixed")
+    csm.close()
+
+    # ---- surrogate: linear response, plain-model training data, the library's training kernels
+    sur = None
+    if not args.no_surrogate:
+        from suguru_b200 import surrogate as S
+        t0 = time.perf_counter()
+        L0, L1 = S.linear_response()
+        Xtr, Ytr, _ = S.make_dataset(args.sur_samples, seed=31)
+        Xv, Yv, Av = S.make_dataset(8192, seed=32)
+        t1 = time.perf_counter()
+        css = make_cs("mixed", surrogate=True)
+        hist = S.train(css, Xtr, Ytr, L0, L1, epochs=args.sur_epochs, batch=1024, lr=1e-3, seed=3)
+        t2 = time.perf_counter()
+        e_lin = S.rel_err_rows(css.surrogate_predict(Xv, parts=1), Yv)
+        e_net = S.rel_err_rows(css.surrogate_predict(Xv, parts=3), Yv)
+        variants = {}
+        # residual-check limits calibrated for 1e-4 (the headline) and for a
+        # loose tolerance, and with no limit (every capsule on the network)
+        for tol in (1e-4, args.sur_loose_tol, None):
+            if tol is None:
+                css.surrogate_set_trust(1e30, 1e30, 0.0, 1e30)
+                info = dict(amp_max=float("inf"), ratio_max=float("inf"))
+            else:
+                info = S.calibrate_trust(css, Xv, Yv, tol=tol)
+            css.set_tile_shape(-1)
+            r = time_path(css, "mixed", tune=True)
+            ns, nf = css.surrogate_counts()
+            variants[tol] = dict(r=r, on_surrogate=ns, fallback=nf, amp_max=info["amp_max"],
+                                 ratio_max=info["ratio_max"], errors=errors(r["out"], fp64["out"]))
+        params = css.surrogate_params()
+        css.close()
+        sur = dict(variants=variants, hist=hist, t_data=t1 - t0, t_train=t2 - t1, params=params,
+                   med_lin=float(np.median(e_lin)), med_net=float(np.median(e_net)))
+
+    # e2e through the public API with pinned host buffers (the headline path)
     u32, v32, w32 = wl.velocity(dtype=np.float32)
     pin = lambda a: torch.from_numpy(np.ascontiguousarray(a)).pin_memory()
     hu, hv, hw = pin(u32), pin(v32), pin(w32)
     hX = [pin(a) for a in (wl.x, wl.y, wl.z)]
-    cs_h = CouplingStep(wl.grid, wl.degree, wl.radius, wl.gs, wl.csk, precision="mixed", mem="host", device=local)
+    cs_h = CouplingStep(wl.grid, wl.degree, wl.radius, wl.gs, wl.csk, precision="mixed", mem="host", device=local,
+                        surrogate=sur is not None)
+    if sur is not None:  # the headline path: trained network, limits for 1e-4
+        cs_h.surrogate_params(sur["params"])
+        v = sur["variants"][1e-4]
+        cs_h.surrogate_set_trust(v["amp_max"], v["ratio_max"], 0.5, 2.0)
     hlag = [torch.empty(n, dtype=torch.float32).pin_memory() for _ in range(10)]
     heul = [torch.empty(cs_h.field_shape, dtype=torch.float32).pin_memory() for _ in range(3)]
     for _ in range(max(1, args.warmup // 2)):
@@ -244,9 +308,14 @@ def run_ours(args):
 
     result = None
     if rank == 0:
-        value = world * n / (mixed["ms_per_step"] / 1e3)
+        head = mixed
+        path = "mixed (surrogate off)"
+        if sur is not None:
+            head = sur["variants"][1e-4]["r"]
+            path = "mixed + surrogate, residual check calibrated for 1e-4 force error"
+        value = world * n / (head["ms_per_step"] / 1e3)
         fp64_value = world * n / (fp64["ms_per_step"] / 1e3)
-        sp_ms = mixed["stages"]["spread"]
+        sp_ms = head["stages"]["spread"]
         sbytes = spread_bytes(wl, 4)
         achieved = sbytes / (sp_ms / 1e3) / 1e9
         traffic = load_traffic().get("spread_c1_mixed_bytes_per_launch")
@@ -257,7 +326,7 @@ def run_ours(args):
             "n_gpus": world,
             "steps": args.steps,
             "warmup": args.warmup,
-            "ms_per_step": mixed["ms_per_step"],
+            "ms_per_step": head["ms_per_step"],
             "higher_is_better": True,
             "scaling": "weak",
             "vs_baseline": None,
@@ -266,21 +335,38 @@ def run_ours(args):
             "data": "synthetic (seeded shapes and velocity modes, no reference fixtures exist)",
             "config": {"workload": "dense suspension: 256 capsules, SH degree 15 (524,288 points), "
                                    "grid 256x256x128, dx=1/32, Skalak Gs=1 C=1",
-                       "path": "mixed (surrogate off)", "points": n, "parallelism": "replicas" if world > 1 else
+                       "path": path, "points": n, "parallelism": "replicas" if world > 1 else
                        "single GPU", "l2": "flushed (256 MB write) between timed iterations",
-                       "spread_tile": mixed["tile"], "spread_tile_fp64": fp64["tile"]},
+                       "spread_tile": head["tile"], "spread_tile_fp64": fp64["tile"]},
             "fp64_plain": {"value": fp64_value, "unit": "points/s", "ms_per_step": fp64["ms_per_step"],
                            "stages_ms": fp64["stages"]},
+            "mixed_plain": {"value": world * n / (mixed["ms_per_step"] / 1e3), "unit": "points/s",
+                            "ms_per_step": mixed["ms_per_step"], "stages_ms": mixed["stages"],
+                            "errors_vs_fp64": errors(mixed["out"], fp64["out"])},
             "speedup_vs_fp64_plain": value / fp64_value,
-            "stages_ms": mixed["stages"],
+            "stages_ms": head["stages"],
             "roofline": {"kernel": "spread_kernel<float> (deterministic gather spread)", "bound": "hbm",
                          "achieved": achieved, "peak": hbm_peak, "unit": "GB/s", "frac": achieved / hbm_peak,
                          "peak_kind": peak_kind, "algorithmic_bytes": sbytes, "traffic": traffic},
             "e2e": {"value": world * n / e2e_s, "unit": "points/s", "h2d_bytes_per_step": h2d,
                     "d2h_bytes_per_step": d2h, "ms_per_step": e2e_s * 1e3},
-            "gpu_launches": mixed["launches"],
-            "clocks": mixed["clocks"],
+            "gpu_launches": head["launches"],
+            "clocks": head["clocks"],
         }
+        if sur is not None:
+            vv = {}
+            for tol, v in sur["variants"].items():
+                vv["no limit" if tol is None else "%g" % tol] = {"points_per_s": world * n / (v["r"]["ms_per_step"] / 1e3),
+                                  "ms_per_step": v["r"]["ms_per_step"], "on_surrogate": v["on_surrogate"],
+                                  "fallback": v["fallback"], "amp_max": min(v["amp_max"], 1e30),
+                                  "ratio_max": min(v["ratio_max"], 1e30),
+                                  "errors_vs_fp64": v["errors"], "stages_ms": v["r"]["stages"]}
+            result["surrogate"] = {
+                "training": {"samples": args.sur_samples, "epochs": args.sur_epochs, "batch": 1024,
+                             "data_s": sur["t_data"], "train_s": sur["t_train"],
+                             "loss_first_last": [float(sur["hist"][0]), float(sur["hist"][-1])]},
+                "heldout_median_rel_err": {"linear_response": sur["med_lin"], "linear_plus_network": sur["med_net"]},
+                "by_tolerance": vv}
     if world > 1:
         dist.barrier()
         dist.destroy_process_group()

@@ -139,6 +139,54 @@ int sg_spread_noalloc(int itot, int jtot, int ktot, double lx, double ly, double
                       const double* FX, const double* FY, const double* FZ, const double* AREA,
                       double* fx, double* fy, double* fz, void* stream);
 
+/* Per-capsule Skalak constants (both NULL-able; default cfg->gs, cfg->csk).
+ * The reference has one pair per run (gscell, CSK, param.f90:88); per-capsule
+ * values serve training-data generation over a range of C. */
+int sg_set_capsule_membrane(sg_ctx* ctx, const double* gs, const double* csk);
+
+/* Spectral coefficients of the plain membrane model, per capsule: the
+ * displacement from the reference sphere after the centroid is removed
+ * (the analysis of cal_3dcrd_spectral_coeff, sph1.f90:29-79) and the force
+ * after its filter (filter_modes4__OPT, sph1.f90:919-932).  Capsule k of
+ * degree L writes 3 (L+1)^2 doubles to each array at offset
+ * 3 * sum_{j<k} (L_j+1)^2: per component x, y, z, the SPHEREPACK a(m,n) for
+ * 0 <= m <= n <= L in m-major order, then b(m,n) for 1 <= m <= n <= L.
+ * Arrays follow cfg->mem.  Allocates its scratch on the first call. */
+int sg_capsule_spectra(sg_ctx* ctx, const double* X, const double* Y, const double* Z,
+                       double* disp, double* force);
+
+/* Learned membrane-force surrogate (mixed precision, capsules of degree 15;
+ * no counterpart in the reference, whose force is always the plain model).
+ * Per capsule, with x the 768 displacement coefficients above divided by R
+ * (slot 0, the x translation, carrying C; slots 256 and 512 zero), the force
+ * coefficients times R/Gs are predicted as
+ *   y = (L0 + C L1) x + a^2 MLP(x / a, C, log a),  a = |x|,
+ * MLP 768 -> 1024 -> 1024 -> 768, GELU, bf16 weights, FP32 accumulation,
+ * trained by the library's own kernels on the O(a^2) remainder.
+ * When cfg->surrogate is set and a trained network and trust limits are
+ * present, sg_step and sg_membrane_force use it for every degree-15 capsule
+ * that passes the residual check (|x| <= amp_max, |MLP(x)| <= ratio_max
+ * |(L0 + C L1) x|, c_min <= C <= c_max); the others, and all capsules of
+ * other degrees, take the plain model. */
+long sg_surrogate_param_count(void);
+/* set != 0: load parameters from buf (marks the network trained); set == 0:
+ * copy them out.  Order: W1, b1, W2, b2, W3, b3, L0, L1, mu_x, sd_x, mu_y, sd_y. */
+int sg_surrogate_params(sg_ctx* ctx, int set, float* buf, long n);
+/* The linear response about the sphere, [768][768] each, row = output slot. */
+int sg_surrogate_set_linear(sg_ctx* ctx, const float* L0, const float* L1);
+/* Train on n host rows X [n][768], Y [n][768] (dimensionless as above):
+ * residual targets (Y - (L0 + C L1) X) / a^2, normalisation from the data, Adam with
+ * cosine decay, minibatches of `batch` (a multiple of 64, <= 1024) in seeded
+ * random order; loss_hist[epochs] receives the mean training loss per epoch. */
+int sg_surrogate_train(sg_ctx* ctx, const float* X, const float* Y, long n, int epochs, int batch,
+                       float lr, unsigned long long seed, float* loss_hist);
+/* Predict Y [n][768] for host rows X; parts: 1 linear only, 2 MLP only, 3 both. */
+int sg_surrogate_predict(sg_ctx* ctx, const float* X, long n, int parts, float* Y);
+/* Residual-check limits; amp_max = 0 turns the surrogate off. */
+int sg_surrogate_set_trust(sg_ctx* ctx, float amp_max, float ratio_max, float c_min, float c_max);
+/* Capsules that used the surrogate and that fell back, in the last step. */
+int sg_surrogate_last_counts(sg_ctx* ctx, int* n_surrogate, int* n_fallback);
+
 /* Host-side tables (tests): Gauss colatitudes and SPHEREPACK-normalised
  * Legendre functions with theta derivatives, [m*nn+n] layout. */
 int sg_gauss(int nlat, double* theta, double* weights);

@@ -24,9 +24,20 @@ int sg_test_legendre(int tensor_cores, int M, int Q, int J, int K, int tri, cons
  * K a multiple of 64.  split = 0: A, B are bf16 bit patterns (uint16);
  * split = 1: A, B are FP32 and run as BF16x3.  Optional outputs (may be
  * NULL): Cpre the FP32 value before GELU, Cb the bf16 result [M][N], CbT the
- * bf16 result transposed [N][M].  Returns 0, 5, 2 or 3 as above. */
+ * bf16 result transposed [N][M].  splitk != 0 gives the kernel a workspace
+ * so that outputs of few tiles are computed in K slices and summed in order.
+ * Returns 0, 5, 2 or 3 as above. */
 int sg_test_gemm(int split, int M, int N, int K, const void* A, const void* B, const float* bias,
-                 int gelu, float alpha, float* C, float* Cpre, unsigned short* Cb, unsigned short* CbT);
+                 int gelu, float alpha, float* C, float* Cpre, unsigned short* Cb, unsigned short* CbT,
+                 int splitk);
+
+/* One forward and backward pass of the surrogate network's kernels with
+ * given parameters (FP32, in the order W1 [dh][din], b1, W2 [dh][dh], b2,
+ * W3 [dout][dh], b3), input rows X [B][din] (already normalised) and targets
+ * T [B][dout]: loss = mean((yhat - T)^2) and its gradients (same layout as
+ * params).  Dimensions and B are multiples of 64.  Returns 0, 5, 2 or 3. */
+int sg_test_mlp_grad(int din, int dh, int dout, int B, const float* params, const float* X,
+                     const float* T, float* loss, float* grads);
 
 #ifdef __cplusplus
 }

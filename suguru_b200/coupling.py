@@ -34,9 +34,11 @@ EXPORTS = ["sg_create", "sg_destroy", "sg_last_error", "sg_synchronize", "sg_int
            "sg_spread", "sg_step", "sg_update_pos", "sg_surf_vol", "sg_gauss", "sg_legendre",
            "sg_last_launch_count", "sg_set_profiling", "sg_stage_times", "sg_spread_noalloc",
            "sg_set_tile_shape", "sg_get_tile_shape", "sg_autotune", "sg_graph_capture", "sg_graph_launch",
-           "sg_graph_release"]
+           "sg_graph_release", "sg_set_capsule_membrane", "sg_capsule_spectra", "sg_surrogate_param_count",
+           "sg_surrogate_params", "sg_surrogate_set_linear", "sg_surrogate_train", "sg_surrogate_predict",
+           "sg_surrogate_set_trust", "sg_surrogate_last_counts"]
 # test hooks declared in include/sg_testing.h
-TEST_EXPORTS = ["sg_test_legendre", "sg_test_gemm"]
+TEST_EXPORTS = ["sg_test_legendre", "sg_test_gemm", "sg_test_mlp_grad"]
 TILE_SHAPES = ((32, 8, 4), (16, 16, 8), (32, 8, 8), (8, 8, 4))
 STAGES = ("bin", "interp", "membrane", "spread")
 
@@ -94,7 +96,20 @@ def lib():
     L.sg_graph_launch.argtypes = [vp]
     L.sg_graph_release.argtypes = [vp]
     L.sg_test_legendre.argtypes = [ctypes.c_int] * 6 + [vp] * 3
-    L.sg_test_gemm.argtypes = [ctypes.c_int] * 4 + [vp] * 3 + [ctypes.c_int, ctypes.c_float] + [vp] * 4
+    L.sg_test_mlp_grad.argtypes = [ctypes.c_int] * 4 + [vp] * 5
+    L.sg_set_capsule_membrane.argtypes = [vp] * 3
+    L.sg_capsule_spectra.argtypes = [vp] * 6
+    L.sg_surrogate_param_count.argtypes = []
+    L.sg_surrogate_param_count.restype = ctypes.c_long
+    L.sg_surrogate_params.argtypes = [vp, ctypes.c_int, vp, ctypes.c_long]
+    L.sg_surrogate_set_linear.argtypes = [vp] * 3
+    L.sg_surrogate_train.argtypes = [vp, vp, vp, ctypes.c_long, ctypes.c_int, ctypes.c_int, ctypes.c_float,
+                                     ctypes.c_ulonglong, vp]
+    L.sg_surrogate_predict.argtypes = [vp, vp, ctypes.c_long, ctypes.c_int, vp]
+    L.sg_surrogate_set_trust.argtypes = [vp] + [ctypes.c_float] * 4
+    L.sg_surrogate_last_counts.argtypes = [vp, ip, ip]
+    L.sg_test_gemm.argtypes = [ctypes.c_int] * 4 + [vp] * 3 + [ctypes.c_int, ctypes.c_float] + [vp] * 4 + [
+        ctypes.c_int]
     d = ctypes.c_double
     L.sg_spread_noalloc.argtypes = ([ctypes.c_int] * 3 + [d] * 3 + [ctypes.c_long] + [vp] * 11)
     _LIB = L
@@ -126,7 +141,7 @@ def from_bf16_bits(b):
     return (np.asarray(b, dtype=np.uint32) << 16).view(np.float32)
 
 
-def test_gemm(A, B, split=False, bias=None, gelu=False, alpha=1.0):
+def test_gemm(A, B, split=False, bias=None, gelu=False, alpha=1.0, splitk=False):
     """C = alpha A B^T (+ bias) (GELU) on the tensor cores (test hook).
 
     split=False: A, B are rounded to bf16 first; split=True: FP32 in, BF16x3.
@@ -143,10 +158,24 @@ def test_gemm(A, B, split=False, bias=None, gelu=False, alpha=1.0):
     CbT = np.zeros((N, M), np.uint16)
     bi = None if bias is None else np.ascontiguousarray(bias, dtype=np.float32)
     rc = lib().sg_test_gemm(int(split), M, N, K, _ptr(a), _ptr(b), _ptr(bi), int(gelu), ctypes.c_float(alpha),
-                            _ptr(C), _ptr(P), _ptr(Cb), _ptr(CbT))
+                            _ptr(C), _ptr(P), _ptr(Cb), _ptr(CbT), int(splitk))
     if rc:
         raise SgError(rc, "sg_test_gemm")
     return C, P, from_bf16_bits(Cb), from_bf16_bits(CbT)
+
+
+def test_mlp_grad(params, X, T, din, dh, dout):
+    """Loss and parameter gradients of one forward/backward pass (test hook)."""
+    params = np.ascontiguousarray(params, dtype=np.float32)
+    X = np.ascontiguousarray(X, dtype=np.float32)
+    T = np.ascontiguousarray(T, dtype=np.float32)
+    B = X.shape[0]
+    loss = np.zeros(1, np.float32)
+    grads = np.zeros_like(params)
+    rc = lib().sg_test_mlp_grad(din, dh, dout, B, _ptr(params), _ptr(X), _ptr(T), _ptr(loss), _ptr(grads))
+    if rc:
+        raise SgError(rc, "sg_test_mlp_grad")
+    return float(loss[0]), grads
 
 
 def gauss(nlat):
@@ -299,6 +328,69 @@ class CouplingStep:
 
     def graph_release(self):
         self._check(lib().sg_graph_release(self._h), "sg_graph_release")
+
+    # ---------------------------------------------------------- surrogate
+    def set_capsule_membrane(self, gs=None, csk=None):
+        """Per-capsule Skalak Gs and C (None keeps the current values)."""
+        n = self.degree.size
+        g = None if gs is None else np.ascontiguousarray(np.broadcast_to(gs, n), dtype=np.float64)
+        c = None if csk is None else np.ascontiguousarray(np.broadcast_to(csk, n), dtype=np.float64)
+        self._check(lib().sg_set_capsule_membrane(self._h, _ptr(g), _ptr(c)), "sg_set_capsule_membrane")
+
+    def capsule_spectra(self, X, Y, Z):
+        """Plain-model displacement and filtered-force coefficients, [sum 3(L+1)^2] each (host mode)."""
+        n = int(sum(3 * (int(L) + 1) ** 2 for L in self.degree))
+        if self.mem == "host":
+            d, f = np.zeros(n), np.zeros(n)
+        else:
+            import torch
+            d = torch.zeros(n, dtype=torch.float64, device="cuda")
+            f = torch.zeros(n, dtype=torch.float64, device="cuda")
+        self._check(lib().sg_capsule_spectra(self._h, *map(_ptr, (X, Y, Z, d, f))), "sg_capsule_spectra")
+        return d, f
+
+    def surrogate_params(self, values=None):
+        """Get (values=None) or set the surrogate's parameters as one float32 vector."""
+        n = lib().sg_surrogate_param_count()
+        if values is None:
+            buf = np.zeros(n, np.float32)
+            self._check(lib().sg_surrogate_params(self._h, 0, _ptr(buf), n), "sg_surrogate_params")
+            return buf
+        buf = np.ascontiguousarray(values, dtype=np.float32)
+        self._check(lib().sg_surrogate_params(self._h, 1, _ptr(buf), buf.size), "sg_surrogate_params")
+        return buf
+
+    def surrogate_set_linear(self, L0, L1):
+        a = np.ascontiguousarray(L0, dtype=np.float32)
+        b = np.ascontiguousarray(L1, dtype=np.float32)
+        self._check(lib().sg_surrogate_set_linear(self._h, _ptr(a), _ptr(b)), "sg_surrogate_set_linear")
+
+    def surrogate_train(self, X, Y, epochs, batch=1024, lr=1e-3, seed=0):
+        X = np.ascontiguousarray(X, dtype=np.float32)
+        Y = np.ascontiguousarray(Y, dtype=np.float32)
+        hist = np.zeros(epochs, np.float32)
+        self._check(lib().sg_surrogate_train(self._h, _ptr(X), _ptr(Y), X.shape[0], int(epochs), int(batch),
+                                             ctypes.c_float(lr), ctypes.c_ulonglong(seed), _ptr(hist)),
+                    "sg_surrogate_train")
+        return hist
+
+    def surrogate_predict(self, X, parts=3):
+        X = np.ascontiguousarray(X, dtype=np.float32)
+        Y = np.zeros_like(X)
+        self._check(lib().sg_surrogate_predict(self._h, _ptr(X), X.shape[0], int(parts), _ptr(Y)),
+                    "sg_surrogate_predict")
+        return Y
+
+    def surrogate_set_trust(self, amp_max, ratio_max, c_min=0.0, c_max=1e30):
+        self._check(lib().sg_surrogate_set_trust(self._h, ctypes.c_float(amp_max), ctypes.c_float(ratio_max),
+                                                 ctypes.c_float(c_min), ctypes.c_float(c_max)),
+                    "sg_surrogate_set_trust")
+
+    def surrogate_counts(self):
+        a, b = ctypes.c_int(), ctypes.c_int()
+        self._check(lib().sg_surrogate_last_counts(self._h, ctypes.byref(a), ctypes.byref(b)),
+                    "sg_surrogate_last_counts")
+        return a.value, b.value
 
     def update_pos(self, dt, X, Y, Z, U, V, W):
         """Update_Pos.f90:95-126 -- in place on X, Y, Z."""

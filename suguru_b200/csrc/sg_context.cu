@@ -8,115 +8,13 @@
 #include <string>
 #include <vector>
 
-#include "sg_coupling.h"
-#include "sg_kernels.h"
+#include "sg_ctx.h"
 
 using namespace sg;
 
-namespace {
 const double kPi = 3.14159265358979323846264338327950288;
 
-struct Group {
-  int L = 0, N = 0, nD = 0, mD = 0, nO = 0, mO = 0;
-  std::vector<int> caps;
-  DegreeTables tab;
-  SpecBuffers buf{};
-  std::vector<double> h_tab[4];  // host FP64 syn_D, ana_D, syn_O, ana_O (by LegProblem::kind)
-};
-}  // namespace
-
-struct sg_ctx {
-  sg_config cfg{};
-  std::vector<int> degree;
-  std::vector<double> radius;
-  int mixed = 0;
-  size_t esz = 8;
-  IBGrid grid{};
-  IBWork ibw{};
-  long npts = 0;
-  long long nfield = 0;
-  std::vector<long long> off;
-  std::vector<Group> groups;
-  CapInfo* d_caps = nullptr;
-  GroupDev* d_groups = nullptr;
-  double* d_cen = nullptr;
-  RowWork* d_wpos = nullptr;
-  RowWork* d_wmem = nullptr;
-  RowWork* d_wsh = nullptr;
-  RowWork* d_wfin = nullptr;
-  int nwpos = 0, nwmem = 0, nwsh = 0, nwfin = 0;
-  LegProblem* d_probs = nullptr;
-  LegWork* d_lw[6] = {};
-  int nlw[6] = {};
-  int maxJ[6] = {}, maxK[6] = {};
-  // tensor-core Legendre path (mixed precision): 128-row work lists
-  bool leg_tc = false;
-  LegWork* d_lw128[6] = {};
-  int nlw128[6] = {};
-  int maxJp[6] = {}, maxKp[6] = {};
-  int num_sms = 148;
-  int* d_err = nullptr;   // device error flag (bounded waits that expired)
-  int* h_err = nullptr;   // pinned copy, refreshed at the end of every step
-  int nmax = 0;
-  // host-mode staging
-  void* s_u = nullptr;
-  void* s_v = nullptr;
-  void* s_w = nullptr;
-  double* s_X = nullptr;
-  double* s_Y = nullptr;
-  double* s_Z = nullptr;
-  void* s_lag[10] = {};
-  void* s_f[3] = {};
-  double* s_out = nullptr;
-  double* s_exy = nullptr;
-  cudaStream_t st = nullptr;
-  bool own_stream = false;
-  std::vector<void*> allocs;
-  std::string err;
-  int launches = 0;
-  bool profiling = false;
-  cudaEvent_t ev[SG_NSTAGE + 1] = {};
-  bool ev_used[SG_NSTAGE] = {};
-  int max_tiles = 0;            // binning arrays are sized for the largest tile count
-  bool capturing = false;       // inside sg_graph_capture: no synchronisation, no events
-  cudaGraph_t graph = nullptr;  // captured step (device memory mode)
-  cudaGraphExec_t graph_exec = nullptr;
-  int graph_launches = 0;
-};
-
 namespace {
-
-int fail(sg_ctx* c, int code, const std::string& msg) {
-  if (c) c->err = msg;
-  return code;
-}
-
-int cuda_fail(sg_ctx* c, cudaError_t e, const char* where) {
-  return fail(c, SG_ERR_CUDA, std::string(where) + ": " + cudaGetErrorString(e));
-}
-
-#define SG_TRY(expr, where)                       \
-  do {                                            \
-    cudaError_t _e = (expr);                      \
-    if (_e != cudaSuccess) return cuda_fail(c, _e, where); \
-  } while (0)
-
-#define SG_RET(x)             \
-  do {                        \
-    int _r = (x);             \
-    if (_r != SG_OK) return _r; \
-  } while (0)
-
-template <class P>
-cudaError_t dalloc(sg_ctx* c, P*& p, size_t bytes) {
-  void* q = nullptr;
-  cudaError_t e = cudaMalloc(&q, bytes ? bytes : 16);
-  if (e == cudaSuccess) {
-    c->allocs.push_back(q);
-    p = (P*)q;
-  }
-  return e;
-}
 
 template <class V>
 cudaError_t upload(sg_ctx* c, void*& dst, const std::vector<V>& v) {
@@ -271,6 +169,7 @@ int setup(sg_ctx* c) {
       const int k = gr.caps[q];
       caps[k].L = gr.L; caps[k].N = gr.N; caps[k].group = (int)gi; caps[k].pad = 0;
       caps[k].pt_off = c->off[k]; caps[k].gidx = (long long)q; caps[k].R = c->radius[k];
+      caps[k].gs = cfg.gs; caps[k].csk = cfg.csk;
     }
     cudaError_t e = build_tables(c, gr);
     if (e != cudaSuccess) return cuda_fail(c, e, "tables");
@@ -299,6 +198,7 @@ int setup(sg_ctx* c) {
   void* tmp = nullptr;
   SG_TRY(upload(c, tmp, caps), "caps");
   c->d_caps = (CapInfo*)tmp;
+  c->h_caps = caps;
   SG_TRY(upload(c, tmp, gdev), "groups");
   c->d_groups = (GroupDev*)tmp;
   SG_TRY(dalloc(c, c->d_cen, sizeof(double) * 3 * std::max(ncap, 1)), "alloc");
@@ -403,6 +303,7 @@ int setup(sg_ctx* c) {
   SG_TRY(cudaMallocHost(&c->h_err, sizeof(int)), "cudaMallocHost");
   *c->h_err = 0;
   SG_TRY(cudaDeviceGetAttribute(&c->num_sms, cudaDevAttrMultiProcessorCount, cfg.device), "attribute");
+  SG_RET(sur_setup(c));
   // binning work
   const long np = std::max(c->npts, 1L);
   SG_TRY(dalloc(c, c->ibw.bx, sizeof(int) * np), "alloc");
@@ -472,10 +373,14 @@ int dev_forces(sg_ctx* c, const double* X, const double* Y, const double* Z, T* 
   SG_TRY(launch_centroid<T>(nc, c->d_caps, X, Y, Z, c->d_cen, c->st), "centroid");
   SG_TRY(launch_posfwd<T>(c->d_wpos, c->nwpos, c->d_caps, c->d_groups, X, Y, Z, c->d_cen, c->st), "posfwd");
   SG_RET(dev_legendre<T>(c, 0));
+  const bool f32 = sizeof(T) == 4;
+  if (f32) SG_RET(sur_step_pre(c));  // surrogate force and its residual check
   SG_RET(dev_legendre<T>(c, 1));
-  SG_TRY(launch_membrane<T>(c->d_wmem, c->nwmem, c->d_caps, c->d_groups, c->cfg.gs, c->cfg.csk, c->nmax, c->st),
+  SG_TRY(launch_membrane<T>(c->d_wmem, c->nwmem, c->d_caps, c->d_groups, f32 ? sur_flags(c) : nullptr, c->nmax,
+                            c->st),
          "membrane");
   SG_RET(dev_legendre<T>(c, 2));
+  if (f32) SG_RET(sur_step_post(c));
   SG_RET(dev_legendre<T>(c, 3));
   SG_TRY(launch_shgrid<T>(c->d_wsh, c->nwsh, c->d_caps, c->d_groups, c->nmax, c->st), "shgrid");
   SG_RET(dev_legendre<T>(c, 4));
@@ -594,6 +499,34 @@ int run_step(sg_ctx* c, int what, const void* u, const void* v, const void* w, c
   return finish(c);
 }
 
+}  // namespace
+
+int sg::run_forces_only(sg_ctx* c, const double* X, const double* Y, const double* Z, void* const* lag) {
+  const bool host = c->cfg.mem == SG_MEM_HOST;
+  const size_t pb = sizeof(double) * c->npts;
+  const double *dX = X, *dY = Y, *dZ = Z;
+  if (host) {
+    SG_RET(h2d(c, c->s_X, X, pb));
+    SG_RET(h2d(c, c->s_Y, Y, pb));
+    SG_RET(h2d(c, c->s_Z, Z, pb));
+    dX = c->s_X; dY = c->s_Y; dZ = c->s_Z;
+  }
+  c->launches = 0;
+  if (c->mixed) {
+    float* L[7];
+    for (int q = 0; q < 7; ++q) L[q] = (float*)lag[q];
+    SG_RET(dev_forces<float>(c, dX, dY, dZ, L[0], L[1], L[2], L[3], L[4], L[5], L[6]));
+  } else {
+    double* L[7];
+    for (int q = 0; q < 7; ++q) L[q] = (double*)lag[q];
+    SG_RET(dev_forces<double>(c, dX, dY, dZ, L[0], L[1], L[2], L[3], L[4], L[5], L[6]));
+  }
+  SG_TRY(cudaStreamSynchronize(c->st), "synchronize");
+  return check_err(c);
+}
+
+namespace {
+
 int check_ptrs(sg_ctx* c, std::initializer_list<const void*> ps) {
   if (c->npts == 0) return SG_OK;
   for (const void* p : ps)
@@ -648,6 +581,7 @@ void sg_destroy(sg_ctx* c) {
     if (c->ev[k]) cudaEventDestroy(c->ev[k]);
   if (c->own_stream && c->st) cudaStreamDestroy(c->st);
   if (c->h_err) cudaFreeHost(c->h_err);
+  if (c->h_sur_count) cudaFreeHost(c->h_sur_count);
   delete c;
 }
 

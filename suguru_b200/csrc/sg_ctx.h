@@ -1,0 +1,152 @@
+// sg_ctx.h -- the context behind the opaque sg_ctx handle of the C ABI
+// (internal to the library): configuration, degree groups with their tables
+// and spectral buffers, binning work, work lists, staging buffers, the
+// surrogate network, and the helpers shared by the files that implement the
+// ABI functions.
+#pragma once
+#include <string>
+#include <vector>
+
+#include "sg_coupling.h"
+#include "sg_kernels.h"
+#include "sg_surrogate.h"
+
+namespace sg {
+
+struct Group {
+  int L = 0, N = 0, nD = 0, mD = 0, nO = 0, mO = 0;
+  std::vector<int> caps;
+  DegreeTables tab;
+  SpecBuffers buf{};
+  std::vector<double> h_tab[4];  // host FP64 syn_D, ana_D, syn_O, ana_O (by LegProblem::kind)
+};
+
+}  // namespace sg
+
+struct sg_ctx {
+  using Group = sg::Group;
+  using IBGrid = sg::IBGrid;
+  using IBWork = sg::IBWork;
+  using CapInfo = sg::CapInfo;
+  using GroupDev = sg::GroupDev;
+  using RowWork = sg::RowWork;
+  using LegProblem = sg::LegProblem;
+  using LegWork = sg::LegWork;
+  sg_config cfg{};
+  std::vector<int> degree;
+  std::vector<double> radius;
+  int mixed = 0;
+  size_t esz = 8;
+  IBGrid grid{};
+  IBWork ibw{};
+  long npts = 0;
+  long long nfield = 0;
+  std::vector<long long> off;
+  std::vector<Group> groups;
+  CapInfo* d_caps = nullptr;
+  std::vector<CapInfo> h_caps;
+  GroupDev* d_groups = nullptr;
+  double* d_cen = nullptr;
+  RowWork* d_wpos = nullptr;
+  RowWork* d_wmem = nullptr;
+  RowWork* d_wsh = nullptr;
+  RowWork* d_wfin = nullptr;
+  int nwpos = 0, nwmem = 0, nwsh = 0, nwfin = 0;
+  LegProblem* d_probs = nullptr;
+  LegWork* d_lw[6] = {};
+  int nlw[6] = {};
+  int maxJ[6] = {}, maxK[6] = {};
+  // tensor-core Legendre path (mixed precision): 128-row work lists
+  bool leg_tc = false;
+  LegWork* d_lw128[6] = {};
+  int nlw128[6] = {};
+  int maxJp[6] = {}, maxKp[6] = {};
+  int num_sms = 148;
+  int* d_err = nullptr;   // device error flag (bounded waits that expired)
+  int* h_err = nullptr;   // pinned copy, refreshed at the end of every step
+  int nmax = 0;
+  // host-mode staging
+  void* s_u = nullptr;
+  void* s_v = nullptr;
+  void* s_w = nullptr;
+  double* s_X = nullptr;
+  double* s_Y = nullptr;
+  double* s_Z = nullptr;
+  void* s_lag[10] = {};
+  void* s_f[3] = {};
+  double* s_out = nullptr;
+  double* s_exy = nullptr;
+  cudaStream_t st = nullptr;
+  bool own_stream = false;
+  std::vector<void*> allocs;
+  std::string err;
+  int launches = 0;
+  bool profiling = false;
+  cudaEvent_t ev[SG_NSTAGE + 1] = {};
+  bool ev_used[SG_NSTAGE] = {};
+  int max_tiles = 0;            // binning arrays are sized for the largest tile count
+  bool capturing = false;       // inside sg_graph_capture: no synchronisation, no events
+  cudaGraph_t graph = nullptr;  // captured step (device memory mode)
+  cudaGraphExec_t graph_exec = nullptr;
+  int graph_launches = 0;
+  // surrogate of the membrane force (mixed path, capsules of SH degree 15)
+  sg::SurrogateNet sur;
+  bool sur_ready = false;       // network allocated (cfg.surrogate)
+  int sur_group = -1;           // degree group with L = 15, or -1
+  int sur_n = 0;                // capsules in that group
+  int* d_sur_caps = nullptr;    // [sur_n] capsule ids in group order
+  int* d_sur_flag = nullptr;    // [ncap] 1: this step's force comes from the surrogate
+  float* d_sur_x = nullptr;     // [sur_n][768] inputs
+  float* d_sur_ylin = nullptr;  // [sur_n][768] linear response
+  float* d_sur_y = nullptr;     // [sur_n][768] predicted force coefficients
+  int* d_sur_count = nullptr;   // [2] capsules on the surrogate, on the fallback
+  int* h_sur_count = nullptr;   // pinned copy of the last step's counts
+  float sur_trust[5] = {0.f, 0.f, 0.f, 0.f, 0.f};  // amp_max, ratio_max, c_min, c_max, enabled
+  // Lagrangian scratch for sg_capsule_spectra in device mode (allocated on first use)
+  void* spec_scratch[7] = {};
+};
+
+namespace sg {
+
+inline int fail(sg_ctx* c, int code, const std::string& msg) {
+  if (c) c->err = msg;
+  return code;
+}
+
+inline int cuda_fail(sg_ctx* c, cudaError_t e, const char* where) {
+  return fail(c, SG_ERR_CUDA, std::string(where) + ": " + cudaGetErrorString(e));
+}
+
+#define SG_TRY(expr, where)                       \
+  do {                                            \
+    cudaError_t _e = (expr);                      \
+    if (_e != cudaSuccess) return cuda_fail(c, _e, where); \
+  } while (0)
+
+#define SG_RET(x)             \
+  do {                        \
+    int _r = (x);             \
+    if (_r != SG_OK) return _r; \
+  } while (0)
+
+// surrogate hooks (sg_surrogate_abi.cu)
+int sur_setup(sg_ctx* c);
+int sur_step_pre(sg_ctx* c);   // after Legendre stage 0
+int sur_step_post(sg_ctx* c);  // after Legendre stage 2
+const int* sur_flags(sg_ctx* c);
+// force pipeline only, outputs into device arrays lag[0..6] (sg_context.cu)
+int run_forces_only(sg_ctx* c, const double* X, const double* Y, const double* Z, void* const* lag);
+
+template <class P>
+cudaError_t dalloc(sg_ctx* c, P*& p, size_t bytes) {
+  void* q = nullptr;
+  cudaError_t e = cudaMalloc(&q, bytes ? bytes : 16);
+  if (e == cudaSuccess) {
+    c->allocs.push_back(q);
+    p = (P*)q;
+  }
+  return e;
+}
+
+
+}  // namespace sg

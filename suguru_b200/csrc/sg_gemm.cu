@@ -41,7 +41,10 @@ __global__ void __launch_bounds__(128) gemm_kernel(GemmArgs g, int* __restrict__
   uint16_t* smem = (uint16_t*)smem_raw;
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
   const int m0 = blockIdx.y * BM, n0 = blockIdx.x * BN;
-  const int nk = g.K / BK;
+  // K slice of this CTA (split-K: blockIdx.z of gridDim.z slices)
+  const int nk_all = g.K / BK, nsl = gridDim.z, z = blockIdx.z;
+  const int kt0 = (int)((long long)nk_all * z / nsl), kt1 = (int)((long long)nk_all * (z + 1) / nsl);
+  const int nk = kt1 - kt0;
 
   if (warp == 0) tmem_alloc(&s_tmem, 128);
   if (tid == 0) {
@@ -68,7 +71,7 @@ __global__ void __launch_bounds__(128) gemm_kernel(GemmArgs g, int* __restrict__
         break;
       }
     }
-    const int k0 = kt * BK;
+    const int k0 = (kt0 + kt) * BK;
     // ---- stage A and B: consecutive threads take consecutive rows of one
     // 8-wide K chunk (conflict-free 16-byte shared stores)
 #pragma unroll 2
@@ -139,6 +142,13 @@ __global__ void __launch_bounds__(128) gemm_kernel(GemmArgs g, int* __restrict__
       float v[16];
       tmem_ld16(tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)j0, v);
       if (r >= g.M) continue;
+      if (nsl > 1) {  // partial product of this K slice
+        float* w = g.ws + ((long long)z * g.M + r) * g.N + n0 + j0;
+#pragma unroll
+        for (int i = 0; i < 16; ++i)
+          if (n0 + j0 + i < g.N) w[i] = nk > 0 ? v[i] : 0.f;
+        continue;
+      }
 #pragma unroll
       for (int i = 0; i < 16; ++i) {
         const int n = n0 + j0 + i;
@@ -162,6 +172,25 @@ __global__ void __launch_bounds__(128) gemm_kernel(GemmArgs g, int* __restrict__
   if (warp == 0) tmem_free(tmem, 128);
 }
 
+// split-K: sum the slices in order, then the epilogue of gemm_kernel
+__global__ void gemm_splitk_reduce_kernel(GemmArgs g, int nsl) {
+  const long long q = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (q >= (long long)g.M * g.N) return;
+  const int r = (int)(q / g.N), n = (int)(q - (long long)r * g.N);
+  float acc = 0.f;
+  for (int z = 0; z < nsl; ++z) acc += g.ws[(long long)z * g.M * g.N + q];
+  float x = g.alpha * acc;
+  if (g.bias) x += g.bias[n];
+  if (g.Cpre) g.Cpre[(long long)r * g.ldpre + n] = x;
+  if (g.gelu) x = gelu(x);
+  if (g.Cf) {
+    float* c = g.Cf + (long long)r * g.ldc + n;
+    *c = g.accumulate ? *c + x : x;
+  }
+  if (g.Cb) g.Cb[(long long)r * g.ldcb + n] = __float2bfloat16_rn(x);
+  if (g.CbT) g.CbT[(long long)n * g.ldcbt + r] = __float2bfloat16_rn(x);
+}
+
 size_t gemm_smem(int split) { return (size_t)2 * (split ? 4 : 2) * BM * BK * sizeof(uint16_t); }
 
 cudaError_t launch_gemm(const GemmArgs& g, int* d_err, cudaStream_t st) {
@@ -171,16 +200,32 @@ cudaError_t launch_gemm(const GemmArgs& g, int* d_err, cudaStream_t st) {
   const int q = g.split ? 4 : 8;
   if (g.lda % q || g.ldb % q || ((uintptr_t)g.A & 15) || ((uintptr_t)g.B & 15)) return cudaErrorInvalidValue;
   const size_t smem = gemm_smem(g.split);
-  dim3 grid((g.N + BN - 1) / BN, (g.M + BM - 1) / BM);
+  dim3 grid((g.N + BN - 1) / BN, (g.M + BM - 1) / BM, 1);
+  // split K when the output has too few tiles to fill the SMs (about 148)
+  const int tiles = (int)(grid.x * grid.y), nk = g.K / BK;
+  int ks = 1;
+  if (g.ws && tiles < 96 && nk >= 4) {
+    ks = 148 / tiles;
+    if (ks > nk / 2) ks = nk / 2;
+    while (ks > 1 && (long long)ks * g.M * g.N > g.ws_floats) --ks;
+    if (ks < 1) ks = 1;
+  }
+  grid.z = ks;
+  GemmArgs ga = g;
+  ga.ksplit = ks;
   cudaError_t e;
   if (g.split) {
     e = cudaFuncSetAttribute(gemm_kernel<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e != cudaSuccess) return e;
-    gemm_kernel<1><<<grid, 128, smem, st>>>(g, d_err);
+    gemm_kernel<1><<<grid, 128, smem, st>>>(ga, d_err);
   } else {
     e = cudaFuncSetAttribute(gemm_kernel<0>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e != cudaSuccess) return e;
-    gemm_kernel<0><<<grid, 128, smem, st>>>(g, d_err);
+    gemm_kernel<0><<<grid, 128, smem, st>>>(ga, d_err);
+  }
+  if (ks > 1) {
+    const long long nq = (long long)g.M * g.N;
+    gemm_splitk_reduce_kernel<<<(unsigned)((nq + 255) / 256), 256, 0, st>>>(ga, ks);
   }
   return cudaGetLastError();
 }

@@ -126,6 +126,12 @@ struct GemmArgs {
   long long ldcb = 0;
   __nv_bfloat16* CbT = nullptr;
   long long ldcbt = 0;
+  // optional FP32 workspace for split-K when the output has few tiles: each
+  // K slice writes its partial product there and a second kernel sums the
+  // slices in fixed order and applies the epilogue
+  float* ws = nullptr;
+  long long ws_floats = 0;
+  int ksplit = 0;  // set by launch_gemm
 };
 cudaError_t launch_gemm(const GemmArgs& g, int* d_err, cudaStream_t st);
 
@@ -147,6 +153,7 @@ struct CapInfo {  // per capsule, device
   long long pt_off;   // first point (global flat index)
   long long gidx;     // index within its degree group
   double R;
+  double gs, csk;     // Skalak shear modulus and area-dilation constant
 };
 
 struct SpecBuffers {  // per degree group base pointers (T)
@@ -177,8 +184,8 @@ template <class T>
 cudaError_t launch_posfwd(const RowWork* work, int nwork, const CapInfo* caps, const GroupDev* groups,
                           const double* X, const double* Y, const double* Z, const double* cen, cudaStream_t st);
 template <class T>
-cudaError_t launch_membrane(const RowWork* work, int nwork, const CapInfo* caps, const GroupDev* groups, double gs,
-                            double csk, int nmax, cudaStream_t st);
+cudaError_t launch_membrane(const RowWork* work, int nwork, const CapInfo* caps, const GroupDev* groups,
+                            const int* sur_flag, int nmax, cudaStream_t st);
 template <class T>
 cudaError_t launch_shgrid(const RowWork* work, int nwork, const CapInfo* caps, const GroupDev* groups, int nmax,
                           cudaStream_t st);

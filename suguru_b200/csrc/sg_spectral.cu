@@ -266,13 +266,19 @@ __device__ __forceinline__ void mechanics(const Geo<T>& G, const T* A, const T (
 // 15 basis fields of cal_co_tang_basis2 (sph3.f90:111-134) from the Legendre
 // output G, adds the reference sphere's analytic part, evaluates geometry and
 // mechanics, and takes the forward DFT of force and normal.
+// Capsules whose force comes from the surrogate (sur_flag[cap] != 0) need only
+// the normal here: their force rows are written as zeros and replaced after
+// the force analysis.
 template <class T>
 __global__ void __launch_bounds__(128) membrane_kernel(const RowWork* __restrict__ work, int nwork,
                                                        const CapInfo* __restrict__ caps,
-                                                       const GroupDev* __restrict__ groups, T hf, T csk) {
+                                                       const GroupDev* __restrict__ groups,
+                                                       const int* __restrict__ sur_flag) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   const RowWork it = work[blockIdx.x];
   const CapInfo ci = caps[it.cap];
+  const T hf = (T)(0.5 * ci.gs), csk = (T)ci.csk;  // hf_gscell = 0.5 gscell (sph.f90:35)
+  const bool normals_only = sur_flag && sur_flag[it.cap];
   const GroupDev gd = groups[it.group];
   const int N = gd.N, nD = gd.nD, mD = gd.mD, rows = it.nrows;
   T* sG = (T*)smem_raw;                      // [rows][18][N]  ((c*2+cs)*3+kind)
@@ -329,14 +335,21 @@ __global__ void __launch_bounds__(128) membrane_kernel(const RowWork* __restrict
       Gm.d12[c] += v12;
       Gm.d22[c] += v22;
     }
-    geometry<T>(Gm);
-    // reference contravariant metric of the sphere: A^11 = 1/R^2,
-    // A^22 = 1/(R^2 sin^2 t), d/dt A^22 = -2 cos t / (R^2 sin^3 t)
-    const T iR2 = T(1) / (R * R);
-    T A[3] = {iR2, iR2 / (st * st), T(0)};
-    T Ad[2][3] = {{T(0), -T(2) * ct * iR2 / (st * st * st), T(0)}, {T(0), T(0), T(0)}};
-    T f[3];
-    mechanics<T>(Gm, A, Ad, hf, csk, f);
+    T f[3] = {T(0), T(0), T(0)};
+    if (normals_only) {
+      T cc[3];
+      cross3(Gm.a1, Gm.a2, cc);  // sph1.f90:611-651
+      const T sm = sqrt(cc[0] * cc[0] + cc[1] * cc[1] + cc[2] * cc[2]);
+      for (int c = 0; c < 3; ++c) Gm.n[c] = cc[c] / sm;
+    } else {
+      geometry<T>(Gm);
+      // reference contravariant metric of the sphere: A^11 = 1/R^2,
+      // A^22 = 1/(R^2 sin^2 t), d/dt A^22 = -2 cos t / (R^2 sin^3 t)
+      const T iR2 = T(1) / (R * R);
+      T A[3] = {iR2, iR2 / (st * st), T(0)};
+      T Ad[2][3] = {{T(0), -T(2) * ct * iR2 / (st * st * st), T(0)}, {T(0), T(0), T(0)}};
+      mechanics<T>(Gm, A, Ad, hf, csk, f);
+    }
     T* o = sOut + r * 6 * (mD + 1);
     o[0 * (mD + 1) + j] = f[0];
     o[1 * (mD + 1) + j] = f[1];
@@ -520,14 +533,13 @@ size_t pointwise_smem(int nmax) {
 }
 
 template <class T>
-cudaError_t launch_membrane(const RowWork* work, int nwork, const CapInfo* caps, const GroupDev* groups, double gs,
-                            double csk, int nmax, cudaStream_t st) {
+cudaError_t launch_membrane(const RowWork* work, int nwork, const CapInfo* caps, const GroupDev* groups,
+                            const int* sur_flag, int nmax, cudaStream_t st) {
   if (nwork <= 0) return cudaSuccess;
   size_t smem = pointwise_smem<T>(nmax);
   cudaError_t e = cudaFuncSetAttribute(membrane_kernel<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   if (e != cudaSuccess) return e;
-  // hf_gscell = 0.5 * gscell (sph.f90:35)
-  membrane_kernel<T><<<nwork, 128, smem, st>>>(work, nwork, caps, groups, (T)(0.5 * gs), (T)csk);
+  membrane_kernel<T><<<nwork, 128, smem, st>>>(work, nwork, caps, groups, sur_flag);
   return cudaGetLastError();
 }
 
@@ -558,7 +570,7 @@ cudaError_t launch_final(const RowWork* work, int nwork, const CapInfo* caps, co
                                           cudaStream_t);                                                            \
   template cudaError_t launch_posfwd<T>(const RowWork*, int, const CapInfo*, const GroupDev*, const double*,         \
                                         const double*, const double*, const double*, cudaStream_t);                 \
-  template cudaError_t launch_membrane<T>(const RowWork*, int, const CapInfo*, const GroupDev*, double, double, int, \
+  template cudaError_t launch_membrane<T>(const RowWork*, int, const CapInfo*, const GroupDev*, const int*, int,     \
                                           cudaStream_t);                                                            \
   template cudaError_t launch_shgrid<T>(const RowWork*, int, const CapInfo*, const GroupDev*, int, cudaStream_t);    \
   template cudaError_t launch_final<T>(const RowWork*, int, const CapInfo*, const GroupDev*, T*, T*, T*, T*, T*, T*,  \

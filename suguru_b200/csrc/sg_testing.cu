@@ -81,7 +81,8 @@ extern "C" int sg_test_legendre(int tensor_cores, int M, int Q, int J, int K, in
 }
 
 extern "C" int sg_test_gemm(int split, int M, int N, int K, const void* A, const void* B, const float* bias,
-                            int gelu, float alpha, float* C, float* Cpre, unsigned short* Cb, unsigned short* CbT) {
+                            int gelu, float alpha, float* C, float* Cpre, unsigned short* Cb, unsigned short* CbT,
+                            int splitk) {
   if (M < 1 || N < 1 || K < 0 || K % 64 || !A || !B || !C) return 5;
   const size_t es = split ? 4 : 2;
   void *dA = nullptr, *dB = nullptr, *dC = nullptr, *dP = nullptr, *dCb = nullptr, *dCbT = nullptr, *dbias = nullptr,
@@ -106,6 +107,12 @@ extern "C" int sg_test_gemm(int split, int M, int N, int K, const void* A, const
     g.Cpre = Cpre ? (float*)dP : nullptr; g.ldpre = N;
     g.Cb = Cb ? (__nv_bfloat16*)dCb : nullptr; g.ldcb = N;
     g.CbT = CbT ? (__nv_bfloat16*)dCbT : nullptr; g.ldcbt = M;
+    float* ws = nullptr;
+    if (splitk) {
+      g.ws_floats = 16ll * M * N;
+      ok(cudaMalloc(&ws, 4 * (size_t)g.ws_floats));
+      g.ws = ws;
+    }
     int err = 0;
     if (ok(launch_gemm(g, (int*)dE, 0)) && ok(cudaDeviceSynchronize()) &&
         ok(cudaMemcpy(&err, dE, sizeof(int), cudaMemcpyDeviceToHost)) &&
@@ -114,8 +121,45 @@ extern "C" int sg_test_gemm(int split, int M, int N, int K, const void* A, const
         (!Cb || ok(cudaMemcpy(Cb, dCb, 2 * nc, cudaMemcpyDeviceToHost))) &&
         (!CbT || ok(cudaMemcpy(CbT, dCbT, 2 * nc, cudaMemcpyDeviceToHost))))
       if (err) rc = 3;
+    if (ws) cudaFree(ws);
   }
   for (void* q : {dA, dB, dC, dP, dCb, dCbT, dbias, dE})
     if (q) cudaFree(q);
+  return rc;
+}
+
+#include "sg_surrogate.h"
+
+extern "C" int sg_test_mlp_grad(int din, int dh, int dout, int B, const float* params, const float* X,
+                                const float* T, float* loss, float* grads) {
+  if (din < 64 || dh < 64 || dout < 64 || din % 64 || dh % 64 || dout % 64 || B < 64 || B % 64 || !params || !X ||
+      !T || !loss || !grads)
+    return 5;
+  SurrogateNet s;
+  s.din = din;
+  s.dh = dh;
+  s.dout = dout;
+  int rc = 0;
+  auto ok = [&](cudaError_t e) {
+    if (e != cudaSuccess && rc == 0) rc = 2;
+    return rc == 0;
+  };
+  int* dE = nullptr;
+  float* dX = nullptr;
+  if (ok(sur_alloc(s, B)) && ok(cudaMalloc(&dE, sizeof(int))) && ok(cudaMemset(dE, 0, sizeof(int))) &&
+      ok(cudaMalloc(&dX, 4 * (size_t)B * din)) &&
+      ok(cudaMemcpy(dX, X, 4 * (size_t)B * din, cudaMemcpyHostToDevice)) &&
+      ok(cudaMemcpy(s.P, params, 4 * s.np, cudaMemcpyHostToDevice)) &&
+      ok(cudaMemcpy(s.tgt, T, 4 * (size_t)B * dout, cudaMemcpyHostToDevice)) && ok(cudaMemset(s.loss, 0, 4)) &&
+      ok(sur_refresh_bf16(s, 0)) && ok(sur_normalise(s, dX, nullptr, B, 0)) && ok(sur_forward(s, B, dE, 0)) &&
+      ok(sur_backward(s, B, dE, 0)) && ok(cudaDeviceSynchronize()) &&
+      ok(cudaMemcpy(grads, s.G, 4 * s.np, cudaMemcpyDeviceToHost)) &&
+      ok(cudaMemcpy(loss, s.loss, 4, cudaMemcpyDeviceToHost))) {
+    int err = 0;
+    if (ok(cudaMemcpy(&err, dE, sizeof(int), cudaMemcpyDeviceToHost)) && err) rc = 3;
+  }
+  if (dE) cudaFree(dE);
+  if (dX) cudaFree(dX);
+  sur_free(s);
   return rc;
 }

@@ -23,26 +23,28 @@ def _bf(x):
     return from_bf16_bits(to_bf16_bits(x)).astype(np.float64)
 
 
+@pytest.mark.parametrize("splitk", [False, True])
 @pytest.mark.parametrize("shape", SHAPES)
-def test_gemm_bf16(cuda, shape):
+def test_gemm_bf16(cuda, shape, splitk):
     M, N, K = shape
     rng = np.random.default_rng(M + N + K)
     A = rng.normal(size=(M, K)).astype(np.float32)
     B = rng.normal(size=(N, K)).astype(np.float32)
-    C, _, _, _ = run_gemm(A, B, split=False)
+    C, _, _, _ = run_gemm(A, B, split=False, splitk=splitk)
     Ab, Bb = _bf(A), _bf(B)
     exact = Ab @ Bb.T
     scale = np.abs(Ab) @ np.abs(Bb).T
     assert (np.abs(C - exact) / scale).max() <= 1e-6
 
 
+@pytest.mark.parametrize("splitk", [False, True])
 @pytest.mark.parametrize("shape", SHAPES[:4])
-def test_gemm_split(cuda, shape):
+def test_gemm_split(cuda, shape, splitk):
     M, N, K = shape
     rng = np.random.default_rng(1 + M + N + K)
     A = (rng.normal(size=(M, K)) * np.exp(rng.uniform(-2, 2, size=(M, 1)))).astype(np.float32)
     B = rng.normal(size=(N, K)).astype(np.float32)
-    C, _, _, _ = run_gemm(A, B, split=True)
+    C, _, _, _ = run_gemm(A, B, split=True, splitk=splitk)
     A64, B64 = A.astype(np.float64), B.astype(np.float64)
     exact = A64 @ B64.T
     scale = np.abs(A64) @ np.abs(B64).T
@@ -51,13 +53,14 @@ def test_gemm_split(cuda, shape):
     assert np.median(err) <= 2e-6
 
 
-def test_gemm_epilogue(cuda):
-    M, N, K = 260, 136, 128
+@pytest.mark.parametrize("splitk", [False, True])
+def test_gemm_epilogue(cuda, splitk):
+    M, N, K = 260, 136, 512
     rng = np.random.default_rng(9)
     A = rng.normal(size=(M, K)).astype(np.float32)
     B = (0.2 * rng.normal(size=(N, K))).astype(np.float32)
     bias = rng.normal(size=N).astype(np.float32)
-    C, P, Cb, CbT = run_gemm(A, B, split=False, bias=bias, gelu=True, alpha=0.5)
+    C, P, Cb, CbT = run_gemm(A, B, split=False, bias=bias, gelu=True, alpha=0.5, splitk=splitk)
     pre = 0.5 * (_bf(A) @ _bf(B).T) + bias
     gel = 0.5 * pre * (1.0 + np.vectorize(math.erf)(pre / math.sqrt(2.0)))
     assert np.abs(P - pre).max() <= 1e-5 * (1 + np.abs(pre).max())
