@@ -202,15 +202,19 @@ int setup(sg_ctx* c) {
   SG_TRY(upload(c, tmp, gdev), "groups");
   c->d_groups = (GroupDev*)tmp;
   SG_TRY(dalloc(c, c->d_cen, sizeof(double) * 3 * std::max(ncap, 1)), "alloc");
-  // row work lists
+  // capsule work lists of the persistent pointwise kernels: one item per
+  // capsule (all rows of its grid), largest degree first so that the
+  // heaviest items start early
   std::vector<RowWork> wpos, wmem, wsh, wfin;
-  for (size_t gi = 0; gi < c->groups.size(); ++gi) {
+  std::vector<int> gorder(c->groups.size());
+  for (size_t gi = 0; gi < gorder.size(); ++gi) gorder[gi] = (int)gi;
+  std::sort(gorder.begin(), gorder.end(), [&](int a, int b) { return c->groups[a].L > c->groups[b].L; });
+  for (int gi : gorder) {
     const Group& gr = c->groups[gi];
-    const int rD = std::max(1, 128 / gr.mD), rO = std::max(1, 128 / gr.mO);
     for (int k : gr.caps) {
-      for (int i = 0; i < gr.nD; ++i) wpos.push_back(RowWork{k, i, 1, (int)gi});
-      for (int i = 0; i < gr.nD; i += rD) wmem.push_back(RowWork{k, i, std::min(rD, gr.nD - i), (int)gi});
-      for (int i = 0; i < gr.nO; i += rO) wsh.push_back(RowWork{k, i, std::min(rO, gr.nO - i), (int)gi});
+      wpos.push_back(RowWork{k, 0, gr.nD, gi});
+      wmem.push_back(RowWork{k, 0, gr.nD, gi});
+      wsh.push_back(RowWork{k, 0, gr.nO, gi});
     }
   }
   wfin = wmem;
@@ -371,21 +375,22 @@ int dev_forces(sg_ctx* c, const double* X, const double* Y, const double* Z, T* 
   const int nc = c->cfg.ncap;
   if (nc == 0) return SG_OK;
   SG_TRY(launch_centroid<T>(nc, c->d_caps, X, Y, Z, c->d_cen, c->st), "centroid");
-  SG_TRY(launch_posfwd<T>(c->d_wpos, c->nwpos, c->d_caps, c->d_groups, X, Y, Z, c->d_cen, c->st), "posfwd");
+  SG_TRY(launch_posfwd<T>(c->d_wpos, c->nwpos, c->d_caps, c->d_groups, X, Y, Z, c->d_cen, c->nmax, c->st), "posfwd");
   SG_RET(dev_legendre<T>(c, 0));
   const bool f32 = sizeof(T) == 4;
   if (f32) SG_RET(sur_step_pre(c));  // surrogate force and its residual check
   SG_RET(dev_legendre<T>(c, 1));
   SG_TRY(launch_membrane<T>(c->d_wmem, c->nwmem, c->d_caps, c->d_groups, f32 ? sur_flags(c) : nullptr, c->nmax,
-                            c->st),
+                            c->d_err, c->st),
          "membrane");
   SG_RET(dev_legendre<T>(c, 2));
   if (f32) SG_RET(sur_step_post(c));
   SG_RET(dev_legendre<T>(c, 3));
-  SG_TRY(launch_shgrid<T>(c->d_wsh, c->nwsh, c->d_caps, c->d_groups, c->nmax, c->st), "shgrid");
+  SG_TRY(launch_shgrid<T>(c->d_wsh, c->nwsh, c->d_caps, c->d_groups, c->nmax, c->d_err, c->st), "shgrid");
   SG_RET(dev_legendre<T>(c, 4));
   SG_RET(dev_legendre<T>(c, 5));
-  SG_TRY(launch_final<T>(c->d_wfin, c->nwfin, c->d_caps, c->d_groups, FX, FY, FZ, NX, NY, NZ, A, c->nmax, c->st),
+  SG_TRY(launch_final<T>(c->d_wfin, c->nwfin, c->d_caps, c->d_groups, FX, FY, FZ, NX, NY, NZ, A, c->nmax, c->d_err,
+                         c->st),
          "final");
   c->launches += 12;
   return SG_OK;
@@ -493,7 +498,7 @@ int run_step(sg_ctx* c, int what, const void* u, const void* v, const void* w, c
       SG_RET(d2h(c, fz, dfz, fb));
     }
   }
-  if (c->leg_tc && (what & 2))
+  if (what & 2)  // bounded waits of the force kernels
     SG_TRY(cudaMemcpyAsync(c->h_err, c->d_err, sizeof(int), cudaMemcpyDeviceToHost, c->st), "error flag");
   SG_TRY(cudaGetLastError(), "step");
   return finish(c);

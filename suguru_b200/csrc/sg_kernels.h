@@ -182,16 +182,16 @@ cudaError_t launch_centroid(int ncap, const CapInfo* caps, const double* X, cons
                             double* cen, cudaStream_t st);
 template <class T>
 cudaError_t launch_posfwd(const RowWork* work, int nwork, const CapInfo* caps, const GroupDev* groups,
-                          const double* X, const double* Y, const double* Z, const double* cen, cudaStream_t st);
+                          const double* X, const double* Y, const double* Z, const double* cen, int nmax, cudaStream_t st);
 template <class T>
 cudaError_t launch_membrane(const RowWork* work, int nwork, const CapInfo* caps, const GroupDev* groups,
-                            const int* sur_flag, int nmax, cudaStream_t st);
+                            const int* sur_flag, int nmax, int* err, cudaStream_t st);
 template <class T>
 cudaError_t launch_shgrid(const RowWork* work, int nwork, const CapInfo* caps, const GroupDev* groups, int nmax,
-                          cudaStream_t st);
+                          int* err, cudaStream_t st);
 template <class T>
 cudaError_t launch_final(const RowWork* work, int nwork, const CapInfo* caps, const GroupDev* groups, T* FX, T* FY,
-                         T* FZ, T* NX, T* NY, T* NZ, T* AREA, int nmax, cudaStream_t st);
+                         T* FZ, T* NX, T* NY, T* NZ, T* AREA, int nmax, int* err, cudaStream_t st);
 
 template <class T>
 cudaError_t launch_update_pos(long n, double dt, double lz, double* X, double* Y, double* Z, const T* U, const T* V,

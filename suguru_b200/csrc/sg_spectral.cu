@@ -20,6 +20,7 @@
 // added back analytically, so the transforms only carry the displacement.
 #include "sg_common.cuh"
 #include "sg_kernels.h"
+#include "sg_umma.cuh"
 
 namespace sg {
 
@@ -61,64 +62,72 @@ __global__ void centroid_kernel(int ncap, const CapInfo* __restrict__ caps, cons
 }
 
 // ------------------------------------------------- positions -> Fourier ---
-// Warp per dealias row i: displacement d = X - cen - R s(t_i, p_j) in FP64,
-// then the real DFT of shagc (shagc.f:364-380: 2/nlon scaling, forward
-// transform carries -sin) for m < N.
+// Persistent CTAs over capsules (work items of whole capsules); per capsule
+// the trig table is staged once, then rows are taken in chunks of
+// blockDim/mD: the displacement d = X - cen - R s(t_i, p_j) in FP64 (one
+// thread per point), then the real DFT of shagc (shagc.f:364-380: 2/nlon
+// scaling, forward transform carries -sin) for m < N, one warp per
+// (row, component) line with lane = m.
 template <class T>
-__global__ void __launch_bounds__(128) posfwd_kernel(const RowWork* __restrict__ work, int nwork,
+__global__ void __launch_bounds__(256) posfwd_kernel(const RowWork* __restrict__ work, int nwork,
                                                      const CapInfo* __restrict__ caps,
                                                      const GroupDev* __restrict__ groups, const double* __restrict__ X,
                                                      const double* __restrict__ Y, const double* __restrict__ Z,
                                                      const double* __restrict__ cen) {
-  __shared__ T sd[4][3][128];
-  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  const int w = blockIdx.x * 4 + warp;
-  if (w >= nwork) return;
-  const RowWork it = work[w];
-  const CapInfo ci = caps[it.cap];
-  const GroupDev gd = groups[it.group];
-  const int N = gd.N, nD = gd.nD, mD = gd.mD;
-  const double* lat64 = (const double*)gd.latD[0];
-  const double* trig64 = (const double*)gd.trigD[0];
-  const T* trig = (const T*)gd.trigD[pidx<T>()];
-  const double R = ci.R;
-  const double c0 = cen[3 * it.cap], c1 = cen[3 * it.cap + 1], c2 = cen[3 * it.cap + 2];
-  T* Fpos = (T*)gd.buf.Fpos + (long long)ci.gidx * 6 * N * nD;
-  for (int r = 0; r < it.nrows; ++r) {
-    const int i = it.row0 + r;
-    const double st = lat64[4 * i], ct = lat64[4 * i + 1];
-    for (int j = lane; j < mD; j += 32) {
-      const long long p = ci.pt_off + (long long)i * mD + j;
-      const double cp = trig64[1 * mD + j], sp = trig64[N * mD + 1 * mD + j];
-      sd[warp][0][j] = (T)(X[p] - c0 - R * (st * sp));
-      sd[warp][1][j] = (T)(Y[p] - c1 - R * (st * cp));
-      sd[warp][2][j] = (T)(Z[p] - c2 - R * ct);
-    }
-    __syncwarp();
-    if (lane < N) {
-      const int m = lane;
-      const T* cs = trig + (long long)m * mD;
-      const T* sn = trig + (long long)N * mD + (long long)m * mD;
-      T a0 = 0, a1 = 0, a2 = 0, b0 = 0, b1 = 0, b2 = 0;
-      for (int j = 0; j < mD; ++j) {
-        const T c = cs[j], s = sn[j];
-        a0 += sd[warp][0][j] * c;
-        a1 += sd[warp][1][j] * c;
-        a2 += sd[warp][2][j] * c;
-        b0 += sd[warp][0][j] * s;
-        b1 += sd[warp][1][j] * s;
-        b2 += sd[warp][2][j] * s;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5, nwarp = blockDim.x >> 5;
+  for (int w = blockIdx.x; w < nwork; w += gridDim.x) {
+    const RowWork it = work[w];
+    const CapInfo ci = caps[it.cap];
+    const GroupDev gd = groups[it.group];
+    const int N = gd.N, nD = gd.nD, mD = gd.mD, mP = mD + 1;
+    const int RP = blockDim.x / mD > 0 ? blockDim.x / mD : 1;
+    T* sTrig = (T*)smem_raw;       // [2][N][mD+1]
+    T* sd = sTrig + 2 * N * mP;    // [RP][3][mD+1]
+    const double* lat64 = (const double*)gd.latD[0];
+    const double* trig64 = (const double*)gd.trigD[0];
+    const T* trig = (const T*)gd.trigD[pidx<T>()];
+    const double R = ci.R;
+    const double c0 = cen[3 * it.cap], c1 = cen[3 * it.cap + 1], c2 = cen[3 * it.cap + 2];
+    T* Fpos = (T*)gd.buf.Fpos + (long long)ci.gidx * 6 * N * nD;
+    __syncthreads();  // the previous capsule's reads of shared memory are done
+    for (int hm = warp; hm < 2 * N; hm += nwarp)
+      for (int j = lane; j < mD; j += 32) sTrig[hm * mP + j] = trig[hm * mD + j];
+    for (int rb = it.row0; rb < it.row0 + it.nrows; rb += RP) {
+      const int rows = min(RP, it.row0 + it.nrows - rb);
+      __syncthreads();
+      {
+        const int r = tid / mD, j = tid - (tid / mD) * mD;
+        if (r < rows) {
+          const int i = rb + r;
+          const double st = lat64[4 * i], ct = lat64[4 * i + 1];
+          const long long p = ci.pt_off + (long long)i * mD + j;
+          const double cp = trig64[1 * mD + j], sp = trig64[N * mD + 1 * mD + j];
+          T* o = sd + r * 3 * mP;
+          o[0 * mP + j] = (T)(X[p] - c0 - R * (st * sp));
+          o[1 * mP + j] = (T)(Y[p] - c1 - R * (st * cp));
+          o[2 * mP + j] = (T)(Z[p] - c2 - R * ct);
+        }
       }
+      __syncthreads();
       const T sfn = T(2) / T(mD);
       const long long rs = (long long)N * nD;  // (comp, cs) row stride
-      Fpos[0 * rs + m * nD + i] = sfn * a0;
-      Fpos[1 * rs + m * nD + i] = -sfn * b0;
-      Fpos[2 * rs + m * nD + i] = sfn * a1;
-      Fpos[3 * rs + m * nD + i] = -sfn * b1;
-      Fpos[4 * rs + m * nD + i] = sfn * a2;
-      Fpos[5 * rs + m * nD + i] = -sfn * b2;
+      for (int line = warp; line < rows * 3; line += nwarp) {
+        if (lane >= N) continue;
+        const int m = lane, c = line % 3, r = line / 3;
+        const T* o = sd + (r * 3 + c) * mP;
+        const T* cs = sTrig + m * mP;
+        const T* sn = sTrig + (N + m) * mP;
+        T a = 0, bq = 0;
+        for (int j = 0; j < mD; ++j) {
+          a += o[j] * cs[j];
+          bq += o[j] * sn[j];
+        }
+        const int i = rb + r;
+        Fpos[(2 * c + 0) * rs + m * nD + i] = sfn * a;
+        Fpos[(2 * c + 1) * rs + m * nD + i] = -sfn * bq;
+      }
     }
-    __syncwarp();
   }
 }
 
@@ -270,36 +279,53 @@ __device__ __forceinline__ void mechanics(const Geo<T>& G, const T* A, const T (
 // the normal here: their force rows are written as zeros and replaced after
 // the force analysis.
 template <class T>
-__global__ void __launch_bounds__(128) membrane_kernel(const RowWork* __restrict__ work, int nwork,
+__global__ void __launch_bounds__(256, sizeof(T) == 4 ? 3 : 2) membrane_kernel(const RowWork* __restrict__ work, int nwork,
                                                        const CapInfo* __restrict__ caps,
                                                        const GroupDev* __restrict__ groups,
-                                                       const int* __restrict__ sur_flag) {
+                                                       const int* __restrict__ sur_flag, int* __restrict__ err) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
-  const RowWork it = work[blockIdx.x];
-  const CapInfo ci = caps[it.cap];
-  const T hf = (T)(0.5 * ci.gs), csk = (T)ci.csk;  // hf_gscell = 0.5 gscell (sph.f90:35)
-  const bool normals_only = sur_flag && sur_flag[it.cap];
-  const GroupDev gd = groups[it.group];
-  const int N = gd.N, nD = gd.nD, mD = gd.mD, rows = it.nrows;
-  T* sG = (T*)smem_raw;                      // [rows][18][N]  ((c*2+cs)*3+kind)
-  T* sTrig = sG + rows * 18 * N;             // [2][N][mD]
-  T* sOut = sTrig + 2 * N * (mD + 1);              // [rows][6][mD]
-  const T* G = (const T*)gd.buf.G + (long long)ci.gidx * 6 * N * 3 * nD;
-  const T* trig = (const T*)gd.trigD[pidx<T>()];
-  const T* lat = (const T*)gd.latD[pidx<T>()];
+  __shared__ __align__(8) uint64_t s_bar;
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5, nwarp = blockDim.x >> 5;
-  // one warp per (row, comp/cs, kind) line of N values; divisions by constants only
-  for (int line = warp; line < rows * 18; line += nwarp) {
-    const int kind = line % 3, ccs = (line / 3) % 6, r = line / 18;
-    for (int m = lane; m < N; m += 32)
-      sG[line * N + m] = G[((long long)ccs * N + m) * 3 * nD + kind * nD + it.row0 + r];
-  }
-  for (int hm = warp; hm < 2 * N; hm += nwarp)
-    for (int j = lane; j < mD; j += 32) sTrig[hm * (mD + 1) + j] = trig[hm * mD + j];
+  if (tid == 0) umma::mbar_init(&s_bar, 1);
   __syncthreads();
-  const int r = tid / mD, j = tid % mD;
-  if (r < rows) {
-    const int i = it.row0 + r;
+  uint32_t phase = 0;
+  for (int w = blockIdx.x; w < nwork; w += gridDim.x) {
+    const RowWork it = work[w];
+    const CapInfo ci = caps[it.cap];
+    const T hf = (T)(0.5 * ci.gs), csk = (T)ci.csk;  // hf_gscell = 0.5 gscell (sph.f90:35)
+    const bool normals_only = sur_flag && sur_flag[it.cap];
+    const GroupDev gd = groups[it.group];
+    const int N = gd.N, nD = gd.nD, mD = gd.mD;
+    const int RP = blockDim.x / mD > 0 ? blockDim.x / mD : 1;
+    const int nG = 6 * N * 3 * nD;         // the capsule's Legendre output block [ccs][m][kind][lat]
+    T* sG = (T*)smem_raw;                  // [nG]
+    T* sTrig = sG + nG;                    // [2][N][mD+1]
+    T* sOut = sTrig + 2 * N * (mD + 1);    // [RP][6][mD+1]
+    const T* G = (const T*)gd.buf.G + (long long)ci.gidx * nG;
+    const T* trig = (const T*)gd.trigD[pidx<T>()];
+    const T* lat = (const T*)gd.latD[pidx<T>()];
+    T* Fout = (T*)gd.buf.Fout + (long long)ci.gidx * 12 * N * nD;
+    const T sfn = T(2) / T(mD);
+    __syncthreads();  // the previous capsule's reads of shared memory are done
+    if (tid == 0) {   // one bulk copy of the whole block (contiguous, 16-byte multiple)
+      umma::fence_async_smem();
+      umma::bulk_g2s(sG, G, (uint32_t)(sizeof(T) * nG), &s_bar);
+    }
+    for (int hm = warp; hm < 2 * N; hm += nwarp)
+      for (int j = lane; j < mD; j += 32) sTrig[hm * (mD + 1) + j] = trig[hm * mD + j];
+    const int got = umma::mbar_wait(&s_bar, phase) ? 1 : 0;
+    phase ^= 1u;
+    if (!__syncthreads_and(got)) {
+      if (tid == 0) atomicExch(err, 1);
+      return;
+    }
+    for (int rb = it.row0; rb < it.row0 + it.nrows; rb += RP) {
+      const int rows = min(RP, it.row0 + it.nrows - rb);
+      __syncthreads();
+  {
+    const int r = tid / mD, j = tid - (tid / mD) * mD;
+    if (r < rows) {
+    const int i = rb + r;
     const T st = lat[4 * i], ct = lat[4 * i + 1];
     const T R = (T)ci.R;
     const T cp = sTrig[1 * (mD + 1) + j], sp = sTrig[(N + 1) * (mD + 1) + j];
@@ -310,16 +336,17 @@ __global__ void __launch_bounds__(128) membrane_kernel(const RowWork* __restrict
     Gm.d11[0] = -R * (st * sp); Gm.d11[1] = -R * (st * cp); Gm.d11[2] = -R * ct;
     Gm.d12[0] = R * (ct * cp); Gm.d12[1] = -R * (ct * sp); Gm.d12[2] = T(0);
     Gm.d22[0] = -R * (st * sp); Gm.d22[1] = -R * (st * cp); Gm.d22[2] = T(0);
-    const T* g = sG + r * 18 * N;
     for (int c = 0; c < 3; ++c) {
-      const T* gc = g + (c * 2 + 0) * 3 * N;  // cos rows: kind 0,1,2
-      const T* gs = g + (c * 2 + 1) * 3 * N;  // sin rows
+      // block element (ccs, m, kind, lat) at ((ccs N + m) 3 + kind) nD + lat
+      const T* gc = sG + (long long)(c * 2 + 0) * N * 3 * nD + i;  // cos rows
+      const T* gs = sG + (long long)(c * 2 + 1) * N * 3 * nD + i;  // sin rows
       T v1 = 0, v2 = 0, v11 = 0, v12 = 0, v22 = 0;
       for (int m = 0; m < N; ++m) {
         const T cm = sTrig[m * (mD + 1) + j], sm = sTrig[(N + m) * (mD + 1) + j];
-        const T P_a = gc[m], P_b = gs[m];
-        const T D_a = gc[N + m], D_b = gs[N + m];
-        const T E_a = gc[2 * N + m], E_b = gs[2 * N + m];
+        const int o = m * 3 * nD;
+        const T P_a = gc[o], P_b = gs[o];
+        const T D_a = gc[o + nD], D_b = gs[o + nD];
+        const T E_a = gc[o + 2 * nD], E_b = gs[o + 2 * nD];
         const T fm = (T)m;
         const T t0P = P_a * cm - P_b * sm;
         const T t1P = fm * (P_a * (-sm) - P_b * cm);
@@ -358,24 +385,26 @@ __global__ void __launch_bounds__(128) membrane_kernel(const RowWork* __restrict
     o[4 * (mD + 1) + j] = Gm.n[1];
     o[5 * (mD + 1) + j] = Gm.n[2];
   }
-  __syncthreads();
-  // forward DFT of the six outputs (force, normal) per row
-  T* Fout = (T*)gd.buf.Fout + (long long)ci.gidx * 12 * N * nD;
-  const T sfn = T(2) / T(mD);
-  // lane = m (N <= 32), warp = (row, field) line
-  for (int line = warp; line < rows * 6 && lane < N; line += nwarp) {
-    const int m = lane, f = line % 6, rr = line / 6;
-    const T* o = sOut + (rr * 6 + f) * (mD + 1);
-    const T* cs = sTrig + m * (mD + 1);
-    const T* sn = sTrig + (N + m) * (mD + 1);
-    T a = 0, b = 0;
-    for (int jj = 0; jj < mD; ++jj) {
-      a += o[jj] * cs[jj];
-      b += o[jj] * sn[jj];
     }
-    const int i = it.row0 + rr;
-    Fout[((long long)(f * 2 + 0) * N + m) * nD + i] = sfn * a;
-    Fout[((long long)(f * 2 + 1) * N + m) * nD + i] = -sfn * b;
+      __syncthreads();
+      // forward DFT of the six outputs (force, normal) per row: lane = m
+      // (N <= 32), warp = (row, field) line
+      for (int line = warp; line < rows * 6; line += nwarp) {
+        if (lane >= N) continue;
+        const int m = lane, f = line % 6, rr = line / 6;
+        const T* o = sOut + (rr * 6 + f) * (mD + 1);
+        const T* cs = sTrig + m * (mD + 1);
+        const T* sn = sTrig + (N + m) * (mD + 1);
+        T a = 0, b = 0;
+        for (int jj = 0; jj < mD; ++jj) {
+          a += o[jj] * cs[jj];
+          b += o[jj] * sn[jj];
+        }
+        const int i = rb + rr;
+        Fout[((long long)(f * 2 + 0) * N + m) * nD + i] = sfn * a;
+        Fout[((long long)(f * 2 + 1) * N + m) * nD + i] = -sfn * b;
+      }
+    }
   }
 }
 
@@ -384,78 +413,97 @@ __global__ void __launch_bounds__(128) membrane_kernel(const RowWork* __restrict
 // renormalised; cal_surface_metric_sph__OPT (sph3.f90:186-277): |a1 x a2| on
 // the SH grid from the shape coefficients.  Then their forward DFT.
 template <class T>
-__global__ void __launch_bounds__(128) shgrid_kernel(const RowWork* __restrict__ work, int nwork,
+__global__ void __launch_bounds__(256) shgrid_kernel(const RowWork* __restrict__ work, int nwork,
                                                      const CapInfo* __restrict__ caps,
-                                                     const GroupDev* __restrict__ groups) {
+                                                     const GroupDev* __restrict__ groups, int* __restrict__ err) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
-  const RowWork it = work[blockIdx.x];
-  const CapInfo ci = caps[it.cap];
-  const GroupDev gd = groups[it.group];
-  const int N = gd.N, nO = gd.nO, mO = gd.mO, rows = it.nrows;
-  T* sG = (T*)smem_raw;              // [rows][12][2][N]  (rr, kind, m)
-  T* sTrig = sG + rows * 24 * N;     // [2][N][mO]
-  T* sOut = sTrig + 2 * N * (mO + 1);      // [rows][4][mO]
-  const T* GO = (const T*)gd.buf.GO + (long long)ci.gidx * 12 * N * 2 * nO;
-  const T* trig = (const T*)gd.trigO[pidx<T>()];
-  const T* lat = (const T*)gd.latO[pidx<T>()];
+  __shared__ __align__(8) uint64_t s_bar;
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5, nwarp = blockDim.x >> 5;
-  for (int line = warp; line < rows * 24; line += nwarp) {
-    const int kind = line % 2, rr = (line / 2) % 12, r = line / 24;
-    for (int m = lane; m < N; m += 32)
-      sG[line * N + m] = GO[((long long)rr * N + m) * 2 * nO + kind * nO + it.row0 + r];
-  }
-  for (int hm = warp; hm < 2 * N; hm += nwarp)
-    for (int j = lane; j < mO; j += 32) sTrig[hm * (mO + 1) + j] = trig[hm * mO + j];
+  if (tid == 0) umma::mbar_init(&s_bar, 1);
   __syncthreads();
-  const int r = tid / mO, j = tid % mO;
-  if (r < rows) {
-    const int i = it.row0 + r;
-    const T st = lat[4 * i], ct = lat[4 * i + 1];
+  uint32_t phase = 0;
+  for (int w = blockIdx.x; w < nwork; w += gridDim.x) {
+    const RowWork it = work[w];
+    const CapInfo ci = caps[it.cap];
+    const GroupDev gd = groups[it.group];
+    const int N = gd.N, nO = gd.nO, mO = gd.mO;
+    const int RP = blockDim.x / mO > 0 ? blockDim.x / mO : 1;
+    const int nG = 12 * N * 2 * nO;       // the capsule's block [rr][m][kind][lat]
+    T* sG = (T*)smem_raw;                 // [nG]
+    T* sTrig = sG + nG;                   // [2][N][mO+1]
+    T* sOut = sTrig + 2 * N * (mO + 1);   // [RP][4][mO+1]
+    const T* GO = (const T*)gd.buf.GO + (long long)ci.gidx * nG;
+    const T* trig = (const T*)gd.trigO[pidx<T>()];
+    const T* lat = (const T*)gd.latO[pidx<T>()];
+    T* Fsh = (T*)gd.buf.Fsh + (long long)ci.gidx * 8 * N * nO;
+    const T sfn = T(2) / T(mO);
     const T R = (T)ci.R;
-    const T cp = sTrig[1 * (mO + 1) + j], sp = sTrig[(N + 1) * (mO + 1) + j];
-    const T* g = sG + r * 24 * N;
-    T nv[3], a1[3] = {R * (ct * sp), R * (ct * cp), -R * st}, a2[3] = {R * (st * cp), -R * (st * sp), T(0)};
-    for (int c = 0; c < 3; ++c) {
-      const T* nc = g + ((c * 2 + 0) * 2 + 0) * N;  // normal comp c, cos, kind P
-      const T* ns = g + ((c * 2 + 1) * 2 + 0) * N;
-      const T* xc = g + (((3 + c) * 2 + 0) * 2) * N;  // shape comp c, cos: kind P at +0, dP at +N
-      const T* xs = g + (((3 + c) * 2 + 1) * 2) * N;
-      T vn = 0, v1 = 0, v2 = 0;
-      for (int m = 0; m < N; ++m) {
-        const T cm = sTrig[m * (mO + 1) + j], sm = sTrig[(N + m) * (mO + 1) + j];
-        vn += nc[m] * cm - ns[m] * sm;
-        v1 += xc[N + m] * cm - xs[N + m] * sm;
-        v2 += (T)m * (xc[m] * (-sm) - xs[m] * cm);
+    __syncthreads();  // the previous capsule's reads of shared memory are done
+    if (tid == 0) {
+      umma::fence_async_smem();
+      umma::bulk_g2s(sG, GO, (uint32_t)(sizeof(T) * nG), &s_bar);
+    }
+    for (int hm = warp; hm < 2 * N; hm += nwarp)
+      for (int j = lane; j < mO; j += 32) sTrig[hm * (mO + 1) + j] = trig[hm * mO + j];
+    const int got = umma::mbar_wait(&s_bar, phase) ? 1 : 0;
+    phase ^= 1u;
+    if (!__syncthreads_and(got)) {
+      if (tid == 0) atomicExch(err, 1);
+      return;
+    }
+    for (int rb = it.row0; rb < it.row0 + it.nrows; rb += RP) {
+      const int rows = min(RP, it.row0 + it.nrows - rb);
+      __syncthreads();
+      const int r = tid / mO, j = tid - (tid / mO) * mO;
+      if (r < rows) {
+        const int i = rb + r;
+        const T st = lat[4 * i], ct = lat[4 * i + 1];
+        const T cp = sTrig[1 * (mO + 1) + j], sp = sTrig[(N + 1) * (mO + 1) + j];
+        // block element (rr, m, kind, lat) at ((rr N + m) 2 + kind) nO + lat
+        T nv[3], a1[3] = {R * (ct * sp), R * (ct * cp), -R * st}, a2[3] = {R * (st * cp), -R * (st * sp), T(0)};
+        for (int c = 0; c < 3; ++c) {
+          const T* nc = sG + (long long)(c * 2 + 0) * N * 2 * nO + i;  // normal comp c, cos
+          const T* ns = sG + (long long)(c * 2 + 1) * N * 2 * nO + i;
+          const T* xc = sG + (long long)((3 + c) * 2 + 0) * N * 2 * nO + i;  // shape comp c, cos
+          const T* xs = sG + (long long)((3 + c) * 2 + 1) * N * 2 * nO + i;
+          T vn = 0, v1 = 0, v2 = 0;
+          for (int m = 0; m < N; ++m) {
+            const T cm = sTrig[m * (mO + 1) + j], sm = sTrig[(N + m) * (mO + 1) + j];
+            const int o = m * 2 * nO;  // kind P at +0, dP at +nO
+            vn += nc[o] * cm - ns[o] * sm;
+            v1 += xc[o + nO] * cm - xs[o + nO] * sm;
+            v2 += (T)m * (xc[o] * (-sm) - xs[o] * cm);
+          }
+          nv[c] = vn;
+          a1[c] += v1;
+          a2[c] += v2;
+        }
+        const T rn = sqrt(nv[0] * nv[0] + nv[1] * nv[1] + nv[2] * nv[2]);
+        T cc[3];
+        cross3(a1, a2, cc);
+        T* o = sOut + r * 4 * (mO + 1);
+        o[0 * (mO + 1) + j] = nv[0] / rn;
+        o[1 * (mO + 1) + j] = nv[1] / rn;
+        o[2 * (mO + 1) + j] = nv[2] / rn;
+        o[3 * (mO + 1) + j] = sqrt(cc[0] * cc[0] + cc[1] * cc[1] + cc[2] * cc[2]);
       }
-      nv[c] = vn;
-      a1[c] += v1;
-      a2[c] += v2;
+      __syncthreads();
+      for (int line = warp; line < rows * 4; line += nwarp) {
+        if (lane >= N) continue;
+        const int m = lane, f = line % 4, rr = line / 4;
+        const T* o = sOut + (rr * 4 + f) * (mO + 1);
+        const T* cs = sTrig + m * (mO + 1);
+        const T* sn = sTrig + (N + m) * (mO + 1);
+        T a = 0, b = 0;
+        for (int jj = 0; jj < mO; ++jj) {
+          a += o[jj] * cs[jj];
+          b += o[jj] * sn[jj];
+        }
+        const int i = rb + rr;
+        Fsh[((long long)(f * 2 + 0) * N + m) * nO + i] = sfn * a;
+        Fsh[((long long)(f * 2 + 1) * N + m) * nO + i] = -sfn * b;
+      }
     }
-    const T rn = sqrt(nv[0] * nv[0] + nv[1] * nv[1] + nv[2] * nv[2]);
-    T cc[3];
-    cross3(a1, a2, cc);
-    T* o = sOut + r * 4 * (mO + 1);
-    o[0 * (mO + 1) + j] = nv[0] / rn;
-    o[1 * (mO + 1) + j] = nv[1] / rn;
-    o[2 * (mO + 1) + j] = nv[2] / rn;
-    o[3 * (mO + 1) + j] = sqrt(cc[0] * cc[0] + cc[1] * cc[1] + cc[2] * cc[2]);
-  }
-  __syncthreads();
-  T* Fsh = (T*)gd.buf.Fsh + (long long)ci.gidx * 8 * N * nO;
-  const T sfn = T(2) / T(mO);
-  for (int line = warp; line < rows * 4 && lane < N; line += nwarp) {
-    const int m = lane, f = line % 4, rr = line / 4;
-    const T* o = sOut + (rr * 4 + f) * (mO + 1);
-    const T* cs = sTrig + m * (mO + 1);
-    const T* sn = sTrig + (N + m) * (mO + 1);
-    T a = 0, b = 0;
-    for (int jj = 0; jj < mO; ++jj) {
-      a += o[jj] * cs[jj];
-      b += o[jj] * sn[jj];
-    }
-    const int i = it.row0 + rr;
-    Fsh[((long long)(f * 2 + 0) * N + m) * nO + i] = sfn * a;
-    Fsh[((long long)(f * 2 + 1) * N + m) * nO + i] = -sfn * b;
   }
 }
 
@@ -463,48 +511,63 @@ __global__ void __launch_bounds__(128) shgrid_kernel(const RowWork* __restrict__
 // TRSSPH SH grid -> force grid of force, normals and surface metric
 // (forcing.f90:67-88), area = surfmetDf * wgtdsinf (forcing.f90:91).
 template <class T>
-__global__ void __launch_bounds__(128) final_kernel(const RowWork* __restrict__ work, int nwork,
+__global__ void __launch_bounds__(256) final_kernel(const RowWork* __restrict__ work, int nwork,
                                                     const CapInfo* __restrict__ caps,
                                                     const GroupDev* __restrict__ groups, T* __restrict__ FX,
                                                     T* __restrict__ FY, T* __restrict__ FZ, T* __restrict__ NX,
-                                                    T* __restrict__ NY, T* __restrict__ NZ, T* __restrict__ AREA) {
+                                                    T* __restrict__ NY, T* __restrict__ NZ, T* __restrict__ AREA,
+                                                    int* __restrict__ err) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
-  const RowWork it = work[blockIdx.x];
-  const CapInfo ci = caps[it.cap];
-  const GroupDev gd = groups[it.group];
-  const int N = gd.N, nD = gd.nD, mD = gd.mD, rows = it.nrows;
-  T* sG = (T*)smem_raw;            // [rows][14][N]
-  T* sTrig = sG + rows * 14 * N;   // [2][N][mD]
-  const T* GF = (const T*)gd.buf.GF + (long long)ci.gidx * 14 * N * nD;
-  const T* trig = (const T*)gd.trigD[pidx<T>()];
-  const T* lat = (const T*)gd.latD[pidx<T>()];
-  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5, nwarp = blockDim.x >> 5;
-  for (int line = warp; line < rows * 14; line += nwarp) {
-    const int rr = line % 14, r = line / 14;
-    for (int m = lane; m < N; m += 32) sG[line * N + m] = GF[((long long)rr * N + m) * nD + it.row0 + r];
-  }
-  for (int q = tid; q < 2 * N * mD; q += blockDim.x) sTrig[q] = trig[q];
+  __shared__ __align__(8) uint64_t s_bar;
+  const int tid = threadIdx.x;
+  if (tid == 0) umma::mbar_init(&s_bar, 1);
   __syncthreads();
-  const int r = tid / mD, j = tid % mD;
-  if (r >= rows) return;
-  const int i = it.row0 + r;
-  const T* g = sG + r * 14 * N;
-  T v[7];
-  for (int f = 0; f < 7; ++f) {
-    const T* a = g + (2 * f) * N;
-    const T* b = g + (2 * f + 1) * N;
-    T s = 0;
-    for (int m = 0; m < N; ++m) s += a[m] * sTrig[m * mD + j] - b[m] * sTrig[N * mD + m * mD + j];
-    v[f] = s;
+  uint32_t phase = 0;
+  for (int w = blockIdx.x; w < nwork; w += gridDim.x) {
+    const RowWork it = work[w];
+    const CapInfo ci = caps[it.cap];
+    const GroupDev gd = groups[it.group];
+    const int N = gd.N, nD = gd.nD, mD = gd.mD;
+    const int nG = 14 * N * nD;   // the capsule's block [rr][m][lat]
+    T* sG = (T*)smem_raw;         // [nG]
+    T* sTrig = sG + nG;           // [2][N][mD]
+    const T* GF = (const T*)gd.buf.GF + (long long)ci.gidx * nG;
+    const T* trig = (const T*)gd.trigD[pidx<T>()];
+    const T* lat = (const T*)gd.latD[pidx<T>()];
+    __syncthreads();  // the previous capsule's reads of shared memory are done
+    if (tid == 0) {
+      umma::fence_async_smem();
+      umma::bulk_g2s(sG, GF, (uint32_t)(sizeof(T) * nG), &s_bar);
+    }
+    for (int q = tid; q < 2 * N * mD; q += blockDim.x) sTrig[q] = trig[q];
+    const int got = umma::mbar_wait(&s_bar, phase) ? 1 : 0;
+    phase ^= 1u;
+    if (!__syncthreads_and(got)) {
+      if (tid == 0) atomicExch(err, 1);
+      return;
+    }
+    // one thread per point of the capsule, rows in order
+    for (int q = tid; q < it.nrows * mD; q += blockDim.x) {
+      const int r = q / mD, j = q - r * mD;
+      const int i = it.row0 + r;
+      T v[7];
+      for (int f = 0; f < 7; ++f) {
+        const T* a = sG + (long long)(2 * f) * N * nD + i;  // block element (rr, m, lat) at (rr N + m) nD + lat
+        const T* b = sG + (long long)(2 * f + 1) * N * nD + i;
+        T s = 0;
+        for (int m = 0; m < N; ++m) s += a[m * nD] * sTrig[m * mD + j] - b[m * nD] * sTrig[N * mD + m * mD + j];
+        v[f] = s;
+      }
+      const long long p = ci.pt_off + (long long)i * mD + j;
+      FX[p] = v[0];
+      FY[p] = v[1];
+      FZ[p] = v[2];
+      NX[p] = v[3];
+      NY[p] = v[4];
+      NZ[p] = v[5];
+      AREA[p] = v[6] * lat[4 * i + 2];
+    }
   }
-  const long long p = ci.pt_off + (long long)i * mD + j;
-  FX[p] = v[0];
-  FY[p] = v[1];
-  FZ[p] = v[2];
-  NX[p] = v[3];
-  NY[p] = v[4];
-  NZ[p] = v[5];
-  AREA[p] = v[6] * lat[4 * i + 2];
 }
 
 // ------------------------------------------------- launchers --------------
@@ -516,52 +579,83 @@ cudaError_t launch_centroid(int ncap, const CapInfo* caps, const double* X, cons
   return cudaGetLastError();
 }
 
-template <class T>
-cudaError_t launch_posfwd(const RowWork* work, int nwork, const CapInfo* caps, const GroupDev* groups, const double* X,
-                          const double* Y, const double* Z, const double* cen, cudaStream_t st) {
-  if (nwork <= 0) return cudaSuccess;
-  posfwd_kernel<T><<<(nwork + 3) / 4, 128, 0, st>>>(work, nwork, caps, groups, X, Y, Z, cen);
-  return cudaGetLastError();
+// Persistent launches: CTAs of 256 threads loop over the capsule work items
+// (whole capsules, largest first); the grid is what the SMs hold at once.
+constexpr int kPointThreads = 256;
+
+template <class K>
+static int persistent_grid(K kernel, size_t smem, int nwork) {
+  int dev = 0, sms = 148, per = 1;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, kernel, kPointThreads, smem) != cudaSuccess || per < 1)
+    per = 1;
+  const int g = sms * per;
+  return nwork < g ? nwork : g;
 }
 
-// Shared memory of the pointwise kernels for degrees up to nmax (rows*mD <= 128):
-// Legendre rows (<= 1536 el.) + trig tables 2*N*4N + outputs (<= 6*128).
+// Shared memory of the pointwise kernels for degrees up to nmax: the
+// capsule's staged input block, the trig table, and per-chunk outputs of at
+// most kPointThreads points.
+enum PointKernel { kPosfwd, kMembrane, kShgrid, kFinal };
 template <class T>
-size_t pointwise_smem(int nmax) {
-  // trig and output rows are padded by one element against bank conflicts
-  return sizeof(T) * (size_t)(1536 + 8 * nmax * nmax + 2 * nmax + 1024);
+size_t pointwise_smem(int kind, int nmax) {
+  const size_t N = nmax, chunk = 6 * (size_t)(kPointThreads + kPointThreads / 8) + 64;
+  size_t e = 0;
+  switch (kind) {
+    case kPosfwd: e = 2 * N * (4 * N + 1) + 3 * (size_t)(kPointThreads + kPointThreads / 8) + 64; break;
+    case kMembrane: e = 36 * N * N + 2 * N * (4 * N + 1) + chunk; break;
+    case kShgrid: e = 24 * N * N + 2 * N * (2 * N + 1) + chunk; break;
+    default: e = 28 * N * N + 8 * N * N; break;
+  }
+  return sizeof(T) * e;
+}
+
+template <class T>
+cudaError_t launch_posfwd(const RowWork* work, int nwork, const CapInfo* caps, const GroupDev* groups, const double* X,
+                          const double* Y, const double* Z, const double* cen, int nmax, cudaStream_t st) {
+  if (nwork <= 0) return cudaSuccess;
+  const size_t smem = pointwise_smem<T>(kPosfwd, nmax);
+  cudaError_t e = cudaFuncSetAttribute(posfwd_kernel<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  if (e != cudaSuccess) return e;
+  posfwd_kernel<T><<<persistent_grid(posfwd_kernel<T>, smem, nwork), kPointThreads, smem, st>>>(
+      work, nwork, caps, groups, X, Y, Z, cen);
+  return cudaGetLastError();
 }
 
 template <class T>
 cudaError_t launch_membrane(const RowWork* work, int nwork, const CapInfo* caps, const GroupDev* groups,
-                            const int* sur_flag, int nmax, cudaStream_t st) {
+                            const int* sur_flag, int nmax, int* err, cudaStream_t st) {
   if (nwork <= 0) return cudaSuccess;
-  size_t smem = pointwise_smem<T>(nmax);
+  const size_t smem = pointwise_smem<T>(kMembrane, nmax);
   cudaError_t e = cudaFuncSetAttribute(membrane_kernel<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   if (e != cudaSuccess) return e;
-  membrane_kernel<T><<<nwork, 128, smem, st>>>(work, nwork, caps, groups, sur_flag);
+  membrane_kernel<T><<<persistent_grid(membrane_kernel<T>, smem, nwork), kPointThreads, smem, st>>>(
+      work, nwork, caps, groups, sur_flag, err);
   return cudaGetLastError();
 }
 
 template <class T>
 cudaError_t launch_shgrid(const RowWork* work, int nwork, const CapInfo* caps, const GroupDev* groups, int nmax,
-                          cudaStream_t st) {
+                          int* err, cudaStream_t st) {
   if (nwork <= 0) return cudaSuccess;
-  size_t smem = pointwise_smem<T>(nmax);
+  const size_t smem = pointwise_smem<T>(kShgrid, nmax);
   cudaError_t e = cudaFuncSetAttribute(shgrid_kernel<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   if (e != cudaSuccess) return e;
-  shgrid_kernel<T><<<nwork, 128, smem, st>>>(work, nwork, caps, groups);
+  shgrid_kernel<T><<<persistent_grid(shgrid_kernel<T>, smem, nwork), kPointThreads, smem, st>>>(work, nwork, caps,
+                                                                                                  groups, err);
   return cudaGetLastError();
 }
 
 template <class T>
 cudaError_t launch_final(const RowWork* work, int nwork, const CapInfo* caps, const GroupDev* groups, T* FX, T* FY,
-                         T* FZ, T* NX, T* NY, T* NZ, T* AREA, int nmax, cudaStream_t st) {
+                         T* FZ, T* NX, T* NY, T* NZ, T* AREA, int nmax, int* err, cudaStream_t st) {
   if (nwork <= 0) return cudaSuccess;
-  size_t smem = pointwise_smem<T>(nmax);
+  const size_t smem = pointwise_smem<T>(kFinal, nmax);
   cudaError_t e = cudaFuncSetAttribute(final_kernel<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   if (e != cudaSuccess) return e;
-  final_kernel<T><<<nwork, 128, smem, st>>>(work, nwork, caps, groups, FX, FY, FZ, NX, NY, NZ, AREA);
+  final_kernel<T><<<persistent_grid(final_kernel<T>, smem, nwork), kPointThreads, smem, st>>>(
+      work, nwork, caps, groups, FX, FY, FZ, NX, NY, NZ, AREA, err);
   return cudaGetLastError();
 }
 
@@ -569,12 +663,13 @@ cudaError_t launch_final(const RowWork* work, int nwork, const CapInfo* caps, co
   template cudaError_t launch_centroid<T>(int, const CapInfo*, const double*, const double*, const double*, double*, \
                                           cudaStream_t);                                                            \
   template cudaError_t launch_posfwd<T>(const RowWork*, int, const CapInfo*, const GroupDev*, const double*,         \
-                                        const double*, const double*, const double*, cudaStream_t);                 \
+                                        const double*, const double*, const double*, int, cudaStream_t);            \
   template cudaError_t launch_membrane<T>(const RowWork*, int, const CapInfo*, const GroupDev*, const int*, int,     \
-                                          cudaStream_t);                                                            \
-  template cudaError_t launch_shgrid<T>(const RowWork*, int, const CapInfo*, const GroupDev*, int, cudaStream_t);    \
+                                          int*, cudaStream_t);                                                      \
+  template cudaError_t launch_shgrid<T>(const RowWork*, int, const CapInfo*, const GroupDev*, int, int*,             \
+                                        cudaStream_t);                                                              \
   template cudaError_t launch_final<T>(const RowWork*, int, const CapInfo*, const GroupDev*, T*, T*, T*, T*, T*, T*,  \
-                                       T*, int, cudaStream_t);
+                                       T*, int, int*, cudaStream_t);
 SG_INST(double)
 SG_INST(float)
 
