@@ -204,9 +204,16 @@ int sg_last_launch_count(const sg_ctx* ctx);
 int sg_set_tile_shape(sg_ctx* ctx, int shape);
 int sg_get_tile_shape(const sg_ctx* ctx, int* shape, int* tx, int* ty, int* tz);
 
+/* Schedule of the persistent per-capsule kernels (no counterpart in the
+ * reference): every capsule is cut into `split` row ranges, 1 <= split <= 8,
+ * so that few capsules still fill every SM.  Results do not depend on it. */
+int sg_set_point_split(sg_ctx* ctx, int split);
+int sg_get_point_split(const sg_ctx* ctx);
+
 /* Autotuner: times `reps` sg_step calls with the same arguments for every
- * tile shape valid for the context, keeps the fastest and returns it with its
- * milliseconds per step.  The outputs hold the last step's results. */
+ * tile shape valid for the context and then for every point split (1, 2, 4,
+ * 8) with the best shape, keeps the fastest pair and returns the shape with
+ * its milliseconds per step.  The outputs hold the last step's results. */
 int sg_autotune(sg_ctx* ctx, const void* u, const void* v, const void* w,
                 const double* X, const double* Y, const double* Z,
                 void* U, void* V, void* W,

@@ -36,7 +36,7 @@ EXPORTS = ["sg_create", "sg_destroy", "sg_last_error", "sg_synchronize", "sg_int
            "sg_set_tile_shape", "sg_get_tile_shape", "sg_autotune", "sg_graph_capture", "sg_graph_launch",
            "sg_graph_release", "sg_set_capsule_membrane", "sg_capsule_spectra", "sg_surrogate_param_count",
            "sg_surrogate_params", "sg_surrogate_set_linear", "sg_surrogate_train", "sg_surrogate_predict",
-           "sg_surrogate_set_trust", "sg_surrogate_last_counts"]
+           "sg_surrogate_set_trust", "sg_surrogate_last_counts", "sg_set_point_split", "sg_get_point_split"]
 # test hooks declared in include/sg_testing.h
 TEST_EXPORTS = ["sg_test_legendre", "sg_test_gemm", "sg_test_mlp_grad"]
 TILE_SHAPES = ((32, 8, 4), (16, 16, 8), (32, 8, 8), (8, 8, 4))
@@ -90,6 +90,8 @@ def lib():
     L.sg_stage_times.argtypes = [vp, ctypes.POINTER(ctypes.c_float), ctypes.c_int]
     ip = ctypes.POINTER(ctypes.c_int)
     L.sg_set_tile_shape.argtypes = [vp, ctypes.c_int]
+    L.sg_set_point_split.argtypes = [vp, ctypes.c_int]
+    L.sg_get_point_split.argtypes = [vp]
     L.sg_get_tile_shape.argtypes = [vp, ip, ip, ip, ip]
     L.sg_autotune.argtypes = [vp] * 20 + [ctypes.c_int, ip, ctypes.POINTER(ctypes.c_float)]
     L.sg_graph_capture.argtypes = [vp] * 20
@@ -303,6 +305,13 @@ class CouplingStep:
     def set_tile_shape(self, shape):
         """Spreading tile shape: index into TILE_SHAPES, or -1 for the default."""
         self._check(lib().sg_set_tile_shape(self._h, int(shape)), "sg_set_tile_shape")
+
+    def set_point_split(self, split):
+        """Work items per capsule of the persistent pointwise kernels (1..8)."""
+        self._check(lib().sg_set_point_split(self._h, int(split)), "sg_set_point_split")
+
+    def point_split(self):
+        return lib().sg_get_point_split(self._h)
 
     def tile_shape(self):
         v = [ctypes.c_int() for _ in range(4)]

@@ -125,6 +125,44 @@ LegProblem prob(const void* A, long long sAc, long long sAr, long long sAm, cons
   return p;
 }
 
+// Work items of the persistent pointwise kernels: every capsule split into
+// `split` row ranges (each item stages the capsule's whole input block),
+// largest degree first so that the heaviest items start early.  More items
+// than capsules keep every SM busy when there are few capsules per SM.
+int set_point_split(sg_ctx* c, int split) {
+  if (split < 1 || split > kMaxPointSplit) return fail(c, SG_ERR_ARG, "point split out of range");
+  std::vector<RowWork> wpos, wmem, wsh;
+  std::vector<int> gorder(c->groups.size());
+  for (size_t gi = 0; gi < gorder.size(); ++gi) gorder[gi] = (int)gi;
+  std::sort(gorder.begin(), gorder.end(), [&](int a, int b) { return c->groups[a].L > c->groups[b].L; });
+  for (int q = 0; q < split; ++q)  // item q of every capsule, then item q+1: large items spread out
+    for (int gi : gorder)
+      for (int k : c->groups[gi].caps) {
+        const Group& gr = c->groups[gi];
+        const int pD = std::min(split, gr.nD), pO = std::min(split, gr.nO);
+        if (q < pD) {
+          const int r0 = gr.nD * q / pD, r1 = gr.nD * (q + 1) / pD;
+          wpos.push_back(RowWork{k, r0, r1 - r0, gi});
+          wmem.push_back(RowWork{k, r0, r1 - r0, gi});
+        }
+        if (q < pO) {
+          const int r0 = gr.nO * q / pO, r1 = gr.nO * (q + 1) / pO;
+          wsh.push_back(RowWork{k, r0, r1 - r0, gi});
+        }
+      }
+  c->nwpos = (int)wpos.size();
+  c->nwmem = (int)wmem.size();
+  c->nwsh = (int)wsh.size();
+  c->nwfin = c->nwmem;
+  SG_TRY(cudaStreamSynchronize(c->st), "synchronize");
+  SG_TRY(cudaMemcpy(c->d_wpos, wpos.data(), sizeof(RowWork) * wpos.size(), cudaMemcpyHostToDevice), "work");
+  SG_TRY(cudaMemcpy(c->d_wmem, wmem.data(), sizeof(RowWork) * wmem.size(), cudaMemcpyHostToDevice), "work");
+  SG_TRY(cudaMemcpy(c->d_wsh, wsh.data(), sizeof(RowWork) * wsh.size(), cudaMemcpyHostToDevice), "work");
+  SG_TRY(cudaMemcpy(c->d_wfin, wmem.data(), sizeof(RowWork) * wmem.size(), cudaMemcpyHostToDevice), "work");
+  c->point_split = split;
+  return SG_OK;
+}
+
 int setup(sg_ctx* c) {
   const sg_config& cfg = c->cfg;
   c->mixed = cfg.precision == SG_PREC_MIXED;
@@ -202,27 +240,13 @@ int setup(sg_ctx* c) {
   SG_TRY(upload(c, tmp, gdev), "groups");
   c->d_groups = (GroupDev*)tmp;
   SG_TRY(dalloc(c, c->d_cen, sizeof(double) * 3 * std::max(ncap, 1)), "alloc");
-  // capsule work lists of the persistent pointwise kernels: one item per
-  // capsule (all rows of its grid), largest degree first so that the
-  // heaviest items start early
-  std::vector<RowWork> wpos, wmem, wsh, wfin;
-  std::vector<int> gorder(c->groups.size());
-  for (size_t gi = 0; gi < gorder.size(); ++gi) gorder[gi] = (int)gi;
-  std::sort(gorder.begin(), gorder.end(), [&](int a, int b) { return c->groups[a].L > c->groups[b].L; });
-  for (int gi : gorder) {
-    const Group& gr = c->groups[gi];
-    for (int k : gr.caps) {
-      wpos.push_back(RowWork{k, 0, gr.nD, gi});
-      wmem.push_back(RowWork{k, 0, gr.nD, gi});
-      wsh.push_back(RowWork{k, 0, gr.nO, gi});
-    }
-  }
-  wfin = wmem;
-  c->nwpos = (int)wpos.size(); c->nwmem = (int)wmem.size(); c->nwsh = (int)wsh.size(); c->nwfin = (int)wfin.size();
-  SG_TRY(upload(c, tmp, wpos), "work"); c->d_wpos = (RowWork*)tmp;
-  SG_TRY(upload(c, tmp, wmem), "work"); c->d_wmem = (RowWork*)tmp;
-  SG_TRY(upload(c, tmp, wsh), "work"); c->d_wsh = (RowWork*)tmp;
-  SG_TRY(upload(c, tmp, wfin), "work"); c->d_wfin = (RowWork*)tmp;
+  // capsule work lists of the persistent pointwise kernels (set_point_split)
+  const size_t maxitems = (size_t)kMaxPointSplit * std::max(ncap, 1);
+  SG_TRY(dalloc(c, c->d_wpos, sizeof(RowWork) * maxitems), "alloc");
+  SG_TRY(dalloc(c, c->d_wmem, sizeof(RowWork) * maxitems), "alloc");
+  SG_TRY(dalloc(c, c->d_wsh, sizeof(RowWork) * maxitems), "alloc");
+  SG_TRY(dalloc(c, c->d_wfin, sizeof(RowWork) * maxitems), "alloc");
+  SG_RET(set_point_split(c, 2));
   // Legendre problems per stage
   std::vector<LegProblem> P;
   std::vector<LegWork> W[6];
@@ -742,6 +766,14 @@ int sg_set_tile_shape(sg_ctx* c, int shape) {
   return SG_OK;
 }
 
+int sg_set_point_split(sg_ctx* c, int split) {
+  if (!c) return SG_ERR_ARG;
+  if (c->graph) return fail(c, SG_ERR_STATE, "release the captured graph before changing the schedule");
+  return set_point_split(c, split);
+}
+
+int sg_get_point_split(const sg_ctx* c) { return c ? c->point_split : 0; }
+
 int sg_get_tile_shape(const sg_ctx* c, int* shape, int* tx, int* ty, int* tz) {
   if (!c) return SG_ERR_ARG;
   if (shape) *shape = c->grid.shape;
@@ -765,30 +797,48 @@ int sg_autotune(sg_ctx* c, const void* u, const void* v, const void* w, const do
   }
   const int async = c->cfg.async;
   c->cfg.async = 1;  // queue the repetitions back to back
-  int best = -1, rc = SG_OK;
+  int rc = SG_OK;
+  auto time_step = [&](float* ms) -> int {
+    int r = sg_step(c, u, v, w, X, Y, Z, U, V, W, FX, FY, FZ, NX, NY, NZ, AREA, fx, fy, fz);  // warm-up
+    if (r == SG_OK && cudaEventRecord(e0, c->st) != cudaSuccess) r = fail(c, SG_ERR_CUDA, "event");
+    for (int k = 0; k < reps && r == SG_OK; ++k)
+      r = sg_step(c, u, v, w, X, Y, Z, U, V, W, FX, FY, FZ, NX, NY, NZ, AREA, fx, fy, fz);
+    if (r == SG_OK && (cudaEventRecord(e1, c->st) != cudaSuccess || cudaEventSynchronize(e1) != cudaSuccess ||
+                       cudaEventElapsedTime(ms, e0, e1) != cudaSuccess))
+      r = fail(c, SG_ERR_CUDA, "autotune timing");
+    *ms /= (float)reps;
+    return r;
+  };
+  // 1) spreading tile shape
+  int best = -1;
   float bms = 0.f;
   for (int sh = 0; sh < kNumTileShapes && rc == SG_OK; ++sh) {
     if (sg_set_tile_shape(c, sh) != SG_OK) continue;  // not valid for this precision or grid
-    rc = sg_step(c, u, v, w, X, Y, Z, U, V, W, FX, FY, FZ, NX, NY, NZ, AREA, fx, fy, fz);  // warm-up
-    if (rc == SG_OK && cudaEventRecord(e0, c->st) != cudaSuccess) rc = fail(c, SG_ERR_CUDA, "event");
-    for (int r = 0; r < reps && rc == SG_OK; ++r)
-      rc = sg_step(c, u, v, w, X, Y, Z, U, V, W, FX, FY, FZ, NX, NY, NZ, AREA, fx, fy, fz);
     float ms = 0.f;
-    if (rc == SG_OK && (cudaEventRecord(e1, c->st) != cudaSuccess || cudaEventSynchronize(e1) != cudaSuccess ||
-                        cudaEventElapsedTime(&ms, e0, e1) != cudaSuccess))
-      rc = fail(c, SG_ERR_CUDA, "autotune timing");
-    ms /= (float)reps;
+    rc = time_step(&ms);
     if (rc == SG_OK && (best < 0 || ms < bms)) {
       best = sh;
       bms = ms;
     }
   }
+  if (rc == SG_OK && best >= 0) rc = sg_set_tile_shape(c, best);
+  // 2) work items per capsule of the persistent pointwise kernels
+  int bsplit = c->point_split;
+  for (int sp = 1; sp <= kMaxPointSplit && rc == SG_OK && best >= 0; sp *= 2) {
+    rc = set_point_split(c, sp);
+    float ms = 0.f;
+    if (rc == SG_OK) rc = time_step(&ms);
+    if (rc == SG_OK && ms < bms) {
+      bsplit = sp;
+      bms = ms;
+    }
+  }
+  if (rc == SG_OK && best >= 0) rc = set_point_split(c, bsplit);
   c->cfg.async = async;
   cudaEventDestroy(e0);
   cudaEventDestroy(e1);
   if (rc != SG_OK) return rc;
   if (best < 0) return fail(c, SG_ERR_STATE, "no tile shape is valid for this grid");
-  SG_RET(sg_set_tile_shape(c, best));
   if (best_shape) *best_shape = best;
   if (best_ms) *best_ms = bms;
   return SG_OK;

@@ -52,6 +52,7 @@ struct sg_ctx {
   RowWork* d_wsh = nullptr;
   RowWork* d_wfin = nullptr;
   int nwpos = 0, nwmem = 0, nwsh = 0, nwfin = 0;
+  int point_split = 1;  // work items per capsule of the pointwise kernels
   LegProblem* d_probs = nullptr;
   LegWork* d_lw[6] = {};
   int nlw[6] = {};
@@ -128,6 +129,8 @@ inline int cuda_fail(sg_ctx* c, cudaError_t e, const char* where) {
     int _r = (x);             \
     if (_r != SG_OK) return _r; \
   } while (0)
+
+constexpr int kMaxPointSplit = 8;
 
 // surrogate hooks (sg_surrogate_abi.cu)
 int sur_setup(sg_ctx* c);

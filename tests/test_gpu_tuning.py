@@ -111,3 +111,23 @@ def test_graph_replay(cuda, precision):
         assert torch.equal(a, b)
     with pytest.raises(SgError):
         cs.graph_launch()
+
+
+@pytest.mark.parametrize("precision", ["fp64", "mixed"])
+def test_point_split_does_not_change_results(cuda, precision):
+    """Every capsule cut into 1, 2, 4 or 8 work items: bitwise the same step."""
+    wl = W.small_config()
+    dt = np.float64 if precision == "fp64" else np.float32
+    u, v, w = (a.astype(dt) for a in wl.velocity())
+    cs = CouplingStep(wl.grid, wl.degree, wl.radius, precision=precision)
+    outs = []
+    for sp in (1, 2, 4, 8):
+        cs.set_point_split(sp)
+        assert cs.point_split() == sp
+        o = cs.step(u, v, w, wl.x, wl.y, wl.z)
+        outs.append([x.copy() for x in list(o["u"]) + list(o["f"]) + list(o["n"]) + [o["area"]] + list(o["fgrid"])])
+    for o in outs[1:]:
+        for a, b in zip(o, outs[0]):
+            assert np.array_equal(a, b)
+    with pytest.raises(SgError):
+        cs.set_point_split(9)
