@@ -112,21 +112,19 @@ __global__ void __launch_bounds__(256) posfwd_kernel(const RowWork* __restrict__
       __syncthreads();
       const T sfn = T(2) / T(mD);
       const long long rs = (long long)N * nD;  // (comp, cs) row stride
+      // lane p < 2N: trig row p (cos m = p, then sin m = p - N); rows of
+      // Fpos are (comp, cos/sin, m), so the output row is c 2N + p
       for (int line = warp; line < rows * 3; line += nwarp) {
-        if (lane >= N) continue;
-        const int m = lane, c = line % 3, r = line / 3;
+        const int c = line % 3, r = line / 3;
         const T* o = sd + (r * 3 + c) * mP;
-        const T* cs = sTrig + m * mP;
-        const T* sn = sTrig + (N + m) * mP;
-        T a = 0, bq = 0;
-        for (int j = 0; j < mD; ++j) {
-          a += o[j] * cs[j];
-          bq += o[j] * sn[j];
+        for (int p = lane; p < 2 * N; p += 32) {
+          const T* t = sTrig + p * mP;
+          T a = 0;
+          for (int j = 0; j < mD; ++j) a += o[j] * t[j];
+          Fpos[(long long)(c * 2 * N + p) * nD + rb + r] = (p < N ? sfn : -sfn) * a;
         }
-        const int i = rb + r;
-        Fpos[(2 * c + 0) * rs + m * nD + i] = sfn * a;
-        Fpos[(2 * c + 1) * rs + m * nD + i] = -sfn * bq;
       }
+      (void)rs;
     }
   }
 }
@@ -387,22 +385,17 @@ __global__ void __launch_bounds__(256, sizeof(T) == 4 ? 3 : 2) membrane_kernel(c
   }
     }
       __syncthreads();
-      // forward DFT of the six outputs (force, normal) per row: lane = m
-      // (N <= 32), warp = (row, field) line
+      // forward DFT of the six outputs (force, normal) per row: warp =
+      // (row, field) line, lane p < 2N = trig row p (cos m = p, sin m = p - N)
       for (int line = warp; line < rows * 6; line += nwarp) {
-        if (lane >= N) continue;
-        const int m = lane, f = line % 6, rr = line / 6;
+        const int f = line % 6, rr = line / 6;
         const T* o = sOut + (rr * 6 + f) * (mD + 1);
-        const T* cs = sTrig + m * (mD + 1);
-        const T* sn = sTrig + (N + m) * (mD + 1);
-        T a = 0, b = 0;
-        for (int jj = 0; jj < mD; ++jj) {
-          a += o[jj] * cs[jj];
-          b += o[jj] * sn[jj];
+        for (int p = lane; p < 2 * N; p += 32) {
+          const T* t = sTrig + p * (mD + 1);
+          T a = 0;
+          for (int jj = 0; jj < mD; ++jj) a += o[jj] * t[jj];
+          Fout[((long long)f * 2 * N + p) * nD + rb + rr] = (p < N ? sfn : -sfn) * a;
         }
-        const int i = rb + rr;
-        Fout[((long long)(f * 2 + 0) * N + m) * nD + i] = sfn * a;
-        Fout[((long long)(f * 2 + 1) * N + m) * nD + i] = -sfn * b;
       }
     }
   }
@@ -489,19 +482,14 @@ __global__ void __launch_bounds__(256) shgrid_kernel(const RowWork* __restrict__
       }
       __syncthreads();
       for (int line = warp; line < rows * 4; line += nwarp) {
-        if (lane >= N) continue;
-        const int m = lane, f = line % 4, rr = line / 4;
+        const int f = line % 4, rr = line / 4;
         const T* o = sOut + (rr * 4 + f) * (mO + 1);
-        const T* cs = sTrig + m * (mO + 1);
-        const T* sn = sTrig + (N + m) * (mO + 1);
-        T a = 0, b = 0;
-        for (int jj = 0; jj < mO; ++jj) {
-          a += o[jj] * cs[jj];
-          b += o[jj] * sn[jj];
+        for (int p = lane; p < 2 * N; p += 32) {
+          const T* t = sTrig + p * (mO + 1);
+          T a = 0;
+          for (int jj = 0; jj < mO; ++jj) a += o[jj] * t[jj];
+          Fsh[((long long)f * 2 * N + p) * nO + rb + rr] = (p < N ? sfn : -sfn) * a;
         }
-        const int i = rb + rr;
-        Fsh[((long long)(f * 2 + 0) * N + m) * nO + i] = sfn * a;
-        Fsh[((long long)(f * 2 + 1) * N + m) * nO + i] = -sfn * b;
       }
     }
   }

@@ -1,0 +1,134 @@
+"""Time-stepped coupling (config 4): capsules advected through a prescribed flow.
+
+Each step runs the library's coupling step (interpolation, membrane force,
+spreading; main.f90:225-233) and then Update_Pos (forward Euler with the
+interpolated velocity, Update_Pos.f90:95-126).  The Eulerian velocity is
+prescribed: the shear u = gamma z plus seeded random Fourier modes whose phases
+advance with seeded frequencies, sampled at each component's staggered
+location (the numpy form is workloads.velocity_field; here it is evaluated on
+the GPU every step).  There is no flow solver on this path, so the spread
+force is computed, as the reference does, but does not feed back.
+
+`run` returns the per-capsule volume and area (surf_vol, FP64) at the first
+and last step and the CUDA-event time of the stepping loop; `compare` runs the
+mixed and the FP64 paths from the same start and reports the drift of each
+and their difference.
+"""
+import numpy as np
+
+from . import workloads as W
+from .coupling import CouplingStep
+
+
+def frequencies(nmodes=16, seed=7):
+    return np.random.default_rng(seed).uniform(0.5, 2.0, size=nmodes) * 2.0 * np.pi
+
+
+class PrescribedFlow:
+    """u, v, w on the MAC grid (with halos) at time t, computed with torch on the GPU."""
+
+    def __init__(self, grid, modes, shear, omega, dtype, device="cuda"):
+        import torch
+        self.torch = torch
+        itot, jtot, ktot, dx, dy, dz = grid
+        self.L = (itot * dx, jtot * dy, ktot * dz)
+        td = torch.float64
+        i = torch.arange(itot + 2, dtype=td, device=device)
+        j = torch.arange(jtot + 2, dtype=td, device=device)
+        k = torch.arange(ktot + 2, dtype=td, device=device)
+        self.face = (i * dx, j * dy, k * dz)
+        self.cent = ((i - 0.5) * dx, (j - 0.5) * dy, (k - 0.5) * dz)
+        self.nx = torch.as_tensor(modes["nx"], dtype=td, device=device)
+        self.ny = torch.as_tensor(modes["ny"], dtype=td, device=device)
+        self.phase = torch.as_tensor(modes["phase"], dtype=td, device=device)
+        self.amp = torch.as_tensor(modes["amp"], dtype=td, device=device)
+        self.omega = torch.as_tensor(omega, dtype=td, device=device)
+        self.shear = float(shear)
+        self.dtype = dtype
+        self.out = [torch.empty((ktot + 2, jtot + 2, itot + 2), dtype=dtype, device=device) for _ in range(3)]
+
+    def __call__(self, t):
+        torch = self.torch
+        Lx, Ly, Lz = self.L
+        ph = self.phase + self.omega * t
+        for c in range(3):
+            xs = self.face[0] if c == 0 else self.cent[0]
+            ys = self.face[1] if c == 1 else self.cent[1]
+            zs = self.face[2] if c == 2 else self.cent[2]
+            ax = 2.0 * np.pi * self.nx[:, None] * xs[None, :] / Lx          # [q, i]
+            ay = 2.0 * np.pi * self.ny[:, None] * ys[None, :] / Ly + ph[:, None]  # [q, j]
+            # sum_q A_qc cos(ax + ay) = sum_q A_qc (cos ax cos ay - sin ax sin ay)
+            A = self.amp[:, c][:, None]
+            F = (A * torch.cos(ay)).T @ torch.cos(ax) - (A * torch.sin(ay)).T @ torch.sin(ax)  # [j, i]
+            U = torch.sin(np.pi * zs / Lz)[:, None, None] * F[None, :, :]
+            if c == 0 and self.shear:
+                U = U + (self.shear * zs)[:, None, None]
+            self.out[c].copy_(U)
+        return self.out
+
+
+def run(wl, steps, precision="mixed", dt=None, surrogate_params=None, trust=None, omega=None, stream=None):
+    """Advect the capsules of `wl` for `steps` steps; returns diagnostics and timing."""
+    import torch
+    dx = wl.grid[3]
+    dt = 0.01 * dx if dt is None else dt
+    omega = frequencies(len(wl.modes["phase"])) if omega is None else omega
+    td = torch.float64 if precision == "fp64" else torch.float32
+    st = torch.cuda.Stream() if stream is None else stream
+    cs = CouplingStep(wl.grid, wl.degree, wl.radius, wl.gs, wl.csk, precision=precision, mem="device",
+                      stream=st.cuda_stream, async_=True, surrogate=surrogate_params is not None)
+    if surrogate_params is not None:
+        cs.surrogate_params(surrogate_params)
+        cs.surrogate_set_trust(*trust)
+    with torch.cuda.stream(st):  # every torch op below is ordered with the library's work
+        flow = PrescribedFlow(wl.grid, wl.modes, wl.shear, omega, td)
+        X = [torch.from_numpy(np.ascontiguousarray(a)).cuda() for a in (wl.x, wl.y, wl.z)]
+        n = wl.npts
+        lag = [torch.empty(n, dtype=td, device="cuda") for _ in range(10)]
+        eul = [torch.empty_like(flow.out[0]) for _ in range(3)]
+
+        def diag():
+            cs.step(*flow(0.0), *X, lag_out=lag, eul_out=eul)  # normals and area of the current shape
+            out = cs.surf_vol(*X, lag[6], lag[7], lag[8], lag[9])
+            cs.synchronize()
+            return out.cpu().numpy()
+
+        d0 = diag()
+        on_sur = fb = 0
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(st)
+        for s in range(steps):
+            u, v, w = flow(s * dt)
+            cs.step(u, v, w, *X, lag_out=lag, eul_out=eul)
+            cs.update_pos(dt, *X, lag[0], lag[1], lag[2])
+        e1.record(st)
+        torch.cuda.synchronize()
+        ms = e0.elapsed_time(e1)
+        if surrogate_params is not None:
+            on_sur, fb = cs.surrogate_counts()
+        d1 = diag()
+        final = [x.cpu().numpy() for x in X]
+    cs.close()
+    return dict(vol0=d0[:, 0], area0=d0[:, 1], vol=d1[:, 0], area=d1[:, 1], positions=final,
+                steps_per_s=steps / (ms / 1e3), ms=ms, on_surrogate=on_sur, fallback=fb)
+
+
+def compare(wl, steps, **kw):
+    """Mixed vs FP64 trajectories from the same start."""
+    a = run(wl, steps, precision="mixed", **kw)
+    b = run(wl, steps, precision="fp64")
+    rel = lambda x, y: float(np.max(np.abs(x - y) / np.abs(y)))
+    return dict(
+        steps=steps,
+        mixed_steps_per_s=a["steps_per_s"], fp64_steps_per_s=b["steps_per_s"],
+        volume_drift_mixed=rel(a["vol"], a["vol0"]), volume_drift_fp64=rel(b["vol"], b["vol0"]),
+        area_drift_mixed=rel(a["area"], a["area0"]), area_drift_fp64=rel(b["area"], b["area0"]),
+        volume_mixed_vs_fp64=rel(a["vol"], b["vol"]), area_mixed_vs_fp64=rel(a["area"], b["area"]),
+        position_mixed_vs_fp64=float(max(np.abs(p - q).max() for p, q in zip(a["positions"], b["positions"]))),
+        on_surrogate=a["on_surrogate"], fallback=a["fallback"])
+
+
+def config4(ncap=1024):
+    """200 steps of config 2, dt = 0.01 dx, time-varying modes."""
+    return W.config2(ncap)
