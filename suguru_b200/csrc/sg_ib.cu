@@ -77,30 +77,47 @@ __global__ void bin_points_kernel(IBGrid g, long n, const double* __restrict__ X
   }
 }
 
-// Exclusive scan of tile counts by one block; starts has ntiles+1 entries.
-__global__ void scan_counts_kernel(int ntiles, const int* __restrict__ counts, int* __restrict__ starts,
-                                   int* __restrict__ fill) {
-  __shared__ int s_part[1024];
-  const int T = blockDim.x, t = threadIdx.x;
-  const int per = (ntiles + T - 1) / T;
-  const int lo = t * per, hi = min(ntiles, lo + per);
-  int sum = 0;
-  for (int i = lo; i < hi; ++i) sum += counts[i];
-  s_part[t] = sum;
+// Exclusive scan of tile counts by one block of 1024 threads; starts has
+// ntiles+1 entries.  Chunks of 1024 tiles are read coalesced and scanned with
+// warp shuffles, carrying the running total from chunk to chunk.
+__global__ void __launch_bounds__(1024) scan_counts_kernel(int ntiles, const int* __restrict__ counts,
+                                                           int* __restrict__ starts, int* __restrict__ fill) {
+  __shared__ int warp_sum[32];
+  __shared__ int carry;
+  const int t = threadIdx.x, lane = t & 31, warp = t >> 5;
+  if (t == 0) carry = 0;
   __syncthreads();
-  for (int off = 1; off < T; off <<= 1) {
-    int v = (t >= off) ? s_part[t - off] : 0;
+  for (int base = 0; base < ntiles; base += 1024) {
+    const int i = base + t;
+    const int v = i < ntiles ? counts[i] : 0;
+    int x = v;  // inclusive scan within the warp
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      const int y = __shfl_up_sync(0xffffffffu, x, o);
+      if (lane >= o) x += y;
+    }
+    if (lane == 31) warp_sum[warp] = x;
     __syncthreads();
-    s_part[t] += v;
+    if (warp == 0) {
+      int w = warp_sum[lane];
+#pragma unroll
+      for (int o = 1; o < 32; o <<= 1) {
+        const int y = __shfl_up_sync(0xffffffffu, w, o);
+        if (lane >= o) w += y;
+      }
+      warp_sum[lane] = w;
+    }
+    __syncthreads();
+    const int excl = carry + (warp > 0 ? warp_sum[warp - 1] : 0) + x - v;
+    if (i < ntiles) {
+      starts[i] = excl;
+      fill[i] = 0;
+    }
+    __syncthreads();  // every thread has read carry and warp_sum
+    if (t == 1023) carry = excl + v;
     __syncthreads();
   }
-  int run = s_part[t] - sum;
-  for (int i = lo; i < hi; ++i) {
-    starts[i] = run;
-    fill[i] = 0;
-    run += counts[i];
-  }
-  if (t == T - 1) starts[ntiles] = s_part[T - 1];
+  if (t == 0) starts[ntiles] = carry;
 }
 
 __global__ void bin_scatter_kernel(IBGrid g, long n, const int* __restrict__ bx, const int* __restrict__ by,
@@ -123,7 +140,10 @@ __global__ void bin_scatter_kernel(IBGrid g, long n, const int* __restrict__ bx,
     int base = 0;
     if (t >= 0 && (int)lane == leader) base = atomicAdd(&fill[t], __popc(same));
     base = __shfl_sync(same, base, leader);
-    if (t >= 0) entries[starts[t] + base + __popc(same & lt)] = (int)p;
+    if (t >= 0) {
+      const int slot = starts[t] + base + __popc(same & lt);
+      if (slot < starts[t + 1]) entries[slot] = (int)p;  // counts and entries agree by construction
+    }
   }
 }
 

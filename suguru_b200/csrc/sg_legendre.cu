@@ -18,6 +18,7 @@ template <class T>
 __global__ void __launch_bounds__(256) legendre_kernel(const LegProblem* __restrict__ probs,
                                                        const LegWork* __restrict__ work, int nwork) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
+  if ((int)blockIdx.x >= nwork) return;
   const LegWork wk = work[blockIdx.x];
   const LegProblem P = probs[wk.prob];
   const int m = wk.m, q0 = wk.q0;
