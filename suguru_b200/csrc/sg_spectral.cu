@@ -334,31 +334,40 @@ __global__ void __launch_bounds__(256, sizeof(T) == 4 ? 3 : 2) membrane_kernel(c
     Gm.d11[0] = -R * (st * sp); Gm.d11[1] = -R * (st * cp); Gm.d11[2] = -R * ct;
     Gm.d12[0] = R * (ct * cp); Gm.d12[1] = -R * (ct * sp); Gm.d12[2] = T(0);
     Gm.d22[0] = -R * (st * sp); Gm.d22[1] = -R * (st * cp); Gm.d22[2] = T(0);
-    for (int c = 0; c < 3; ++c) {
-      // block element (ccs, m, kind, lat) at ((ccs N + m) 3 + kind) nD + lat
-      const T* gc = sG + (long long)(c * 2 + 0) * N * 3 * nD + i;  // cos rows
-      const T* gs = sG + (long long)(c * 2 + 1) * N * 3 * nD + i;  // sin rows
-      T v1 = 0, v2 = 0, v11 = 0, v12 = 0, v22 = 0;
+    {
+      // block element (ccs, m, kind, lat) at ((ccs N + m) 3 + kind) nD + lat;
+      // m outermost so that each trig pair is read once for the three
+      // components (the order of the sums per component is unchanged)
+      T v1[3] = {T(0), T(0), T(0)}, v2[3] = {T(0), T(0), T(0)}, v11[3] = {T(0), T(0), T(0)};
+      T v12[3] = {T(0), T(0), T(0)}, v22[3] = {T(0), T(0), T(0)};
+      const T* g = sG + i;
       for (int m = 0; m < N; ++m) {
         const T cm = sTrig[m * (mD + 1) + j], sm = sTrig[(N + m) * (mD + 1) + j];
-        const int o = m * 3 * nD;
-        const T P_a = gc[o], P_b = gs[o];
-        const T D_a = gc[o + nD], D_b = gs[o + nD];
-        const T E_a = gc[o + 2 * nD], E_b = gs[o + 2 * nD];
         const T fm = (T)m;
-        const T t0P = P_a * cm - P_b * sm;
-        const T t1P = fm * (P_a * (-sm) - P_b * cm);
-        v1 += D_a * cm - D_b * sm;               // vat1 = sum dP * parthe0
-        v2 += t1P;                               // vat2 = sum P * parthe1
-        v11 += E_a * cm - E_b * sm;              // deFvat1(:,1) = sum d2P * parthe0
-        v12 += fm * (D_a * (-sm) - D_b * cm);    // deFvat1(:,2) = sum dP * parthe1
-        v22 += -fm * fm * t0P;                   // deFvat2(:,2) = sum P * parthe2
+#pragma unroll
+        for (int c = 0; c < 3; ++c) {
+          const T* gc = g + ((long long)((c * 2 + 0) * N + m) * 3) * nD;  // cos rows
+          const T* gs = g + ((long long)((c * 2 + 1) * N + m) * 3) * nD;  // sin rows
+          const T P_a = gc[0], P_b = gs[0];
+          const T D_a = gc[nD], D_b = gs[nD];
+          const T E_a = gc[2 * nD], E_b = gs[2 * nD];
+          const T t0P = P_a * cm - P_b * sm;
+          const T t1P = fm * (P_a * (-sm) - P_b * cm);
+          v1[c] += D_a * cm - D_b * sm;               // vat1 = sum dP * parthe0
+          v2[c] += t1P;                               // vat2 = sum P * parthe1
+          v11[c] += E_a * cm - E_b * sm;              // deFvat1(:,1) = sum d2P * parthe0
+          v12[c] += fm * (D_a * (-sm) - D_b * cm);    // deFvat1(:,2) = sum dP * parthe1
+          v22[c] += -fm * fm * t0P;                   // deFvat2(:,2) = sum P * parthe2
+        }
       }
-      Gm.a1[c] += v1;
-      Gm.a2[c] += v2;
-      Gm.d11[c] += v11;
-      Gm.d12[c] += v12;
-      Gm.d22[c] += v22;
+#pragma unroll
+      for (int c = 0; c < 3; ++c) {
+        Gm.a1[c] += v1[c];
+        Gm.a2[c] += v2[c];
+        Gm.d11[c] += v11[c];
+        Gm.d12[c] += v12[c];
+        Gm.d22[c] += v22[c];
+      }
     }
     T f[3] = {T(0), T(0), T(0)};
     if (normals_only) {
@@ -538,13 +547,15 @@ __global__ void __launch_bounds__(256) final_kernel(const RowWork* __restrict__ 
     for (int q = tid; q < it.nrows * mD; q += blockDim.x) {
       const int r = q / mD, j = q - r * mD;
       const int i = it.row0 + r;
-      T v[7];
-      for (int f = 0; f < 7; ++f) {
-        const T* a = sG + (long long)(2 * f) * N * nD + i;  // block element (rr, m, lat) at (rr N + m) nD + lat
-        const T* b = sG + (long long)(2 * f + 1) * N * nD + i;
-        T s = 0;
-        for (int m = 0; m < N; ++m) s += a[m * nD] * sTrig[m * mD + j] - b[m * nD] * sTrig[N * mD + m * mD + j];
-        v[f] = s;
+      // block element (rr, m, lat) at (rr N + m) nD + lat; m outermost so that
+      // each trig pair is read once for the seven fields (same order per field)
+      T v[7] = {T(0), T(0), T(0), T(0), T(0), T(0), T(0)};
+      const T* g = sG + i;
+      for (int m = 0; m < N; ++m) {
+        const T cm = sTrig[m * mD + j], sm = sTrig[N * mD + m * mD + j];
+#pragma unroll
+        for (int f = 0; f < 7; ++f)
+          v[f] += g[((2 * f) * N + m) * nD] * cm - g[((2 * f + 1) * N + m) * nD] * sm;
       }
       const long long p = ci.pt_off + (long long)i * mD + j;
       FX[p] = v[0];

@@ -37,6 +37,7 @@ namespace sg {
 namespace {
 
 constexpr int LB = 19;      // FP64 limb width
+constexpr int kOut = -(1 << 24);  // offset of a stencil node outside the tile
 constexpr int MAXC = 4096;  // FP64 contributions per pass: 19 + 12 <= 31 bits per limb
 
 template <class T>
@@ -87,7 +88,10 @@ __global__ void __launch_bounds__(256) spread_kernel(IBGrid g, const int* __rest
   constexpr int QB = Fixed<T>::QB;
   constexpr int CPT = (NC + 255) / 256;  // cells per thread in the fold / write loops
   constexpr int NT = F32 ? 1 : CPT;      // FP64 keeps running 64-bit totals
-  __shared__ unsigned int acc[NW][3][NC];
+  // per (limb, component): NC cells and 32 per-lane trash words that take the
+  // contributions falling outside the tile, so that the walk has no branches
+  constexpr int NCP = NC + 32;
+  __shared__ __align__(16) unsigned int acc[NW][3][NCP];
   __shared__ T s_red[8];
   long long tot[NT][3];
 #pragma unroll
@@ -101,7 +105,7 @@ __global__ void __launch_bounds__(256) spread_kernel(IBGrid g, const int* __rest
   T iscale = T(0);
 
   if (e1 > e0) {
-    for (int q = tid; q < NW * 3 * NC; q += 256) (&acc[0][0][0])[q] = 0u;
+    for (int q = tid; q < NW * 3 * NCP / 4; q += 256) ((uint4*)&acc[0][0][0])[q] = make_uint4(0u, 0u, 0u, 0u);
     // ---- fixed-point scale: FP32 from the sum, FP64 from the maximum of
     // max_c |f_c * area / dV| over the tile's entries (fixed reduction order)
     T red = T(0);
@@ -167,13 +171,13 @@ __global__ void __launch_bounds__(256) spread_kernel(IBGrid g, const int* __rest
           for (int t = 0; t < 4; ++t) {
             if (d == 0) {
               const int a = wrap_near(bb[0] + t - 1, g.itot) - i0;
-              lc[t] = (a >= 0 && a < cw) ? a : -1;
+              lc[t] = (a >= 0 && a < cw) ? a : kOut;
             } else if (d == 1) {
               const int b = wrap_near(bb[1] + t - 1, g.jtot) - j0;
-              lc[t] = (b >= 0 && b < ch) ? TX * b : -1;
+              lc[t] = (b >= 0 && b < ch) ? TX * b : kOut;
             } else {
               const int kk = bb[2] + t - 1;
-              lc[t] = (kk - k0 >= 0 && kk - k0 < cd && kk >= 1 && kk <= g.ktot) ? TX * TY * (kk - k0) : -1;
+              lc[t] = (kk - k0 >= 0 && kk - k0 < cd && kk >= 1 && kk <= g.ktot) ? TX * TY * (kk - k0) : kOut;
             }
           }
 #pragma unroll
@@ -182,25 +186,25 @@ __global__ void __launch_bounds__(256) spread_kernel(IBGrid g, const int* __rest
             lcC[d][q] = lc[q + 1];
           }
         }
-        // component c has face weights along dimension c, centre weights along the others
+        // component c has face weights along dimension c, centre weights along
+        // the others.  A cell outside the tile has a negative offset sum (kOut
+        // in at least one dimension) and goes to this lane's trash word.
+        const int trash = NC + lane;
 #pragma unroll
         for (int c = 0; c < 3; ++c) {
 #pragma unroll
           for (int iz = 0; iz < 3; ++iz) {
             const int cz_ = (c == 2) ? lcF[2][iz] : lcC[2][iz];
-            if (cz_ < 0) continue;
             const T wz = (c == 2) ? wF[2][iz] : wC[2][iz];
 #pragma unroll
             for (int iy = 0; iy < 3; ++iy) {
-              const int cy_ = (c == 1) ? lcF[1][iy] : lcC[1][iy];
-              if (cy_ < 0) continue;
+              const int cyz = cz_ + ((c == 1) ? lcF[1][iy] : lcC[1][iy]);
               const T pyz = cf[c] * (((c == 1) ? wF[1][iy] : wC[1][iy]) * wz);
 #pragma unroll
               for (int ix = 0; ix < 3; ++ix) {
-                const int cx_ = (c == 0) ? lcF[0][ix] : lcC[0][ix];
-                if (cx_ < 0) continue;
+                const int cell = cyz + ((c == 0) ? lcF[0][ix] : lcC[0][ix]);
                 const T wx = (c == 0) ? wF[0][ix] : wC[0][ix];
-                Fixed<T>::add(&acc[0][c][cx_ + cy_ + cz_], 3 * NC, pyz * wx);
+                Fixed<T>::add(&acc[0][c][cell >= 0 ? cell : trash], 3 * NCP, pyz * wx);
               }
             }
           }
@@ -215,7 +219,7 @@ __global__ void __launch_bounds__(256) spread_kernel(IBGrid g, const int* __rest
           if (q < NC) {
 #pragma unroll
             for (int c = 0; c < 3; ++c) {
-              tot[r][c] += Fixed<double>::fold(&acc[0][c][q], 3 * NC);
+              tot[r][c] += Fixed<double>::fold(&acc[0][c][q], 3 * NCP);
 #pragma unroll
               for (int w = 0; w < NW; ++w) acc[w][c][q] = 0u;
             }
@@ -226,7 +230,11 @@ __global__ void __launch_bounds__(256) spread_kernel(IBGrid g, const int* __rest
     }
   }
 
-  // ---- write the cells, their periodic halo copies and the zero z-halo planes
+  // ---- write the cells (32-bit offsets: make_ib_grid caps the field below
+  // 2^31 elements); tiles at a domain face also write the periodic halo
+  // copies and the zero z-halo planes (the test is uniform across the CTA)
+  const bool face = i0 == 1 || i0 + cw - 1 == g.itot || j0 == 1 || j0 + ch - 1 == g.jtot || k0 == 1 ||
+                    k0 + cd - 1 == g.ktot;
 #pragma unroll
   for (int r = 0; r < CPT; ++r) {
     const int q = tid + 256 * r;
@@ -247,6 +255,13 @@ __global__ void __launch_bounds__(256) spread_kernel(IBGrid g, const int* __rest
       }
     }
     const int i = i0 + lx, j = j0 + ly, k = k0 + lz;
+    if (!face) {
+      const int o = i + g.ldi * (j + g.ldj * k);
+      ox[o] = vu;
+      oy[o] = vv;
+      oz[o] = vw;
+      continue;
+    }
     int is[2] = {i, -1}, js[2] = {j, -1};
     if (i == g.itot) is[1] = 0;
     if (i == 1) is[1] = g.itot + 1;
