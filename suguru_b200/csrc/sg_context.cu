@@ -122,6 +122,7 @@ LegProblem prob(const void* A, long long sAc, long long sAr, long long sAm, cons
   p.D = D; p.sDc = sDc; p.sDr = sDr; p.sDm = sDm;
   p.rpc = rpc; p.Q = rpc * ncap; p.M = M; p.J = J; p.K = K;
   p.tri = tri; p.group = group; p.kind = kind;
+  p.next[0] = p.next[1] = -1;
   return p;
 }
 
@@ -283,12 +284,48 @@ int setup(sg_ctx* c) {
                               (char*)b.GF + E * 6 * N * nD, 14 * N * nD, N * nD, nD, 8, n, N, nD, N, 1, G, 0),
                 c->maxJ[5], c->maxK[5]);
   }
+  // tensor-core path (FP32 data): three launches of chained contractions.
+  // Per group the problems above are, in order, S0 S1 S2 S3a S3b S4 S5a S5b;
+  // S2 is split into its force rows (S2f) and normal rows (S2n) so that each
+  // half chains into the synthesis that consumes it:
+  //   launch 0: S0 -> {S1, S3b}      launch 1: S2n -> S3a, S2f -> S5a
+  //   launch 2: S4 -> S5b
+  // With the surrogate on, S5a runs in launch 2 instead, after the surrogate
+  // force has replaced the analysed force rows.
+  std::vector<int> roots[3];
+  if (c->mixed) {
+    const size_t ng = c->groups.size();
+    for (size_t gi = 0; gi < ng; ++gi) {
+      const Group& gr = c->groups[gi];
+      const long long N = gr.N, nD = gr.nD;
+      const int base = 8 * (int)gi;
+      LegProblem f = P[base + 2], nrm = P[base + 2];
+      f.rpc = 6;
+      f.Q = 6 * (int)gr.caps.size();
+      nrm.rpc = 6;
+      nrm.Q = f.Q;
+      nrm.A = (const char*)nrm.A + E * 6 * N * nD;
+      nrm.D = (char*)nrm.D + E * 6 * N * N;
+      const int iF = (int)P.size(), iN = iF + 1;
+      P.push_back(f);
+      P.push_back(nrm);
+      P[base + 0].next[0] = base + 1;  // S0 -> S1
+      P[base + 0].next[1] = base + 4;  // S0 -> S3b
+      P[iN].next[0] = base + 3;        // S2n -> S3a
+      if (!cfg.surrogate) P[iF].next[0] = base + 6;  // S2f -> S5a
+      P[base + 5].next[0] = base + 7;  // S4 -> S5b
+      roots[0].push_back(base + 0);
+      roots[1].push_back(iN);
+      roots[1].push_back(iF);
+      roots[2].push_back(base + 5);
+      if (cfg.surrogate) roots[2].push_back(base + 6);
+    }
+  }
   // tensor-core operands: bf16 hi/lo images of every problem's table, and
-  // work lists of 128-row tiles (FP32 data only)
+  // work lists of 128-row tiles of the root problems (FP32 data only)
   if (c->mixed) {
     std::vector<uint16_t> img;
     std::vector<size_t> img_off(P.size());
-    std::vector<LegWork> W128[6];
     for (size_t pi2 = 0; pi2 < P.size(); ++pi2) {
       LegProblem& p = P[pi2];
       p.Jp = (p.J + 15) / 16 * 16;
@@ -305,17 +342,22 @@ int setup(sg_ctx* c) {
     void* dimg = nullptr;
     SG_TRY(upload(c, dimg, img), "umma images");
     for (size_t pi2 = 0; pi2 < P.size(); ++pi2) P[pi2].Bimg = (const uint16_t*)dimg + img_off[pi2];
-    for (int s = 0; s < 6; ++s) {
-      for (const LegWork& w : W[s]) {
-        if (w.q0 % 128) continue;  // one 128-row tile per four 32-row items
-        W128[s].push_back(w);
-        const LegProblem& p = P[w.prob];
-        c->maxJp[s] = std::max(c->maxJp[s], p.Jp);
-        c->maxKp[s] = std::max(c->maxKp[s], p.Kp);
+    for (int f = 0; f < 3; ++f) {
+      std::vector<LegWork> WF;
+      for (int r : roots[f]) {
+        const LegProblem& p = P[r];
+        for (int m = 0; m < p.M; ++m)
+          for (int q0 = 0; q0 < p.Q; q0 += 128) WF.push_back(LegWork{r, m, q0});
+        int chain[3] = {r, p.next[0], p.next[1]};
+        for (int q : chain) {
+          if (q < 0) continue;
+          c->maxJpF[f] = std::max(c->maxJpF[f], P[q].Jp);
+          c->maxKpF[f] = std::max(c->maxKpF[f], P[q].Kp);
+        }
       }
-      c->nlw128[s] = (int)W128[s].size();
-      SG_TRY(upload(c, tmp, W128[s]), "work");
-      c->d_lw128[s] = (LegWork*)tmp;
+      c->nlwF[f] = (int)WF.size();
+      SG_TRY(upload(c, tmp, WF), "work");
+      c->d_lwF[f] = (LegWork*)tmp;
     }
     c->leg_tc = true;
   }
@@ -384,11 +426,16 @@ int dev_interp(sg_ctx* c, const T* u, const T* v, const T* w, T* U, T* V, T* W) 
 template <class T>
 int dev_legendre(sg_ctx* c, int s) {
   if (sizeof(T) == 4 && c->leg_tc) {
-    SG_TRY(launch_legendre_mma(c->d_probs, c->d_lw128[s], c->nlw128[s], c->maxJp[s], c->maxKp[s], c->d_err,
+    // stages 0, 2, 4 launch the chained products; 1, 3, 5 ran inside them
+    if (s % 2) return SG_OK;
+    const int f = s / 2;
+    SG_TRY(launch_legendre_mma(c->d_probs, c->d_lwF[f], c->nlwF[f], c->maxJpF[f], c->maxKpF[f], c->d_err,
                                c->num_sms, c->st),
            "legendre (tensor cores)");
+    c->launches += 1;
   } else {
     SG_TRY(launch_legendre<T>(c->d_probs, c->d_lw[s], c->nlw[s], c->maxJ[s], c->maxK[s], c->st), "legendre");
+    c->launches += 1;
   }
   return SG_OK;
 }
@@ -416,7 +463,7 @@ int dev_forces(sg_ctx* c, const double* X, const double* Y, const double* Z, T* 
   SG_TRY(launch_final<T>(c->d_wfin, c->nwfin, c->d_caps, c->d_groups, FX, FY, FZ, NX, NY, NZ, A, c->nmax, c->d_err,
                          c->st),
          "final");
-  c->launches += 12;
+  c->launches += 5;  // centroid, posfwd, membrane, shgrid, final (Legendre launches counted above)
   return SG_OK;
 }
 

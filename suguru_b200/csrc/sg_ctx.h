@@ -59,9 +59,9 @@ struct sg_ctx {
   int maxJ[6] = {}, maxK[6] = {};
   // tensor-core Legendre path (mixed precision): 128-row work lists
   bool leg_tc = false;
-  LegWork* d_lw128[6] = {};
-  int nlw128[6] = {};
-  int maxJp[6] = {}, maxKp[6] = {};
+  LegWork* d_lwF[3] = {};  // root work items of the three chained launches
+  int nlwF[3] = {};
+  int maxJpF[3] = {}, maxKpF[3] = {};
   int num_sms = 148;
   int* d_err = nullptr;   // device error flag (bounded waits that expired)
   int* h_err = nullptr;   // pinned copy, refreshed at the end of every step

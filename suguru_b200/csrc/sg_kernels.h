@@ -90,6 +90,7 @@ struct LegProblem {
   int Jp, Kp;    // J, K rounded up to multiples of 16
   int vecA;      // A rows 16-byte aligned with K % 8 == 0: float4 loads
   int vecD;      // D rows 16-byte aligned with J % 4 == 0: float4 stores
+  int next[2];   // tensor-core path: problems whose A operand is this problem's output (-1: none)
 };
 
 struct LegWork {  // one tile of a problem

@@ -40,6 +40,46 @@ using namespace umma;
 
 }  // namespace
 
+namespace {
+
+// B_m image of problem P (already split and laid out): a straight 16-byte copy
+__device__ __forceinline__ void stage_table(const LegProblem& P, int m, uint16_t* sBh, uint16_t* sBl, int tid) {
+  const uint4* src = (const uint4*)((const uint16_t*)P.Bimg + (long long)m * P.sBimg);
+  const int n16 = (P.Jp * P.Kp) >> 3;  // uint4 per image
+  uint4* dh = (uint4*)sBh;
+  uint4* dl = (uint4*)sBl;
+  for (int i = tid; i < n16; i += 128) {
+    dh[i] = src[i];
+    dl[i] = src[n16 + i];
+  }
+}
+
+// One thread issues 3 MMAs per K step of 16 (hi.hi, hi.lo, lo.hi), then commits.
+__device__ __forceinline__ void issue_mma(const LegProblem& P, int m, uint32_t tmem, const uint16_t* sAh,
+                                          const uint16_t* sAl, const uint16_t* sBh, const uint16_t* sBl,
+                                          uint64_t* bar) {
+  const uint32_t idesc = idesc_bf16(MMA_M, P.Jp);
+  const uint32_t lbo = 128, sbo = (uint32_t)P.Kp * 16;
+  const uint32_t aH = smem_u32(sAh), aL = smem_u32(sAl), bH = smem_u32(sBh), bL = smem_u32(sBl);
+  const int s0 = P.tri ? (m >> 4) : 0;  // synthesis: coefficients below n = m vanish
+  uint32_t acc = 0;
+  for (int s = s0; s < (P.Kp >> 4); ++s) {
+    const uint32_t o = (uint32_t)s * 256;
+    mma_bf16(tmem, desc(aH + o, lbo, sbo), desc(bH + o, lbo, sbo), idesc, acc);
+    acc = 1;
+    mma_bf16(tmem, desc(aH + o, lbo, sbo), desc(bL + o, lbo, sbo), idesc, 1);
+    mma_bf16(tmem, desc(aL + o, lbo, sbo), desc(bH + o, lbo, sbo), idesc, 1);
+  }
+  commit(bar);
+}
+
+}  // namespace
+
+// Work items name root problems; a root's next[] problems take its output
+// rows as their A operand for the same (m, tile) and run in the same CTA: the
+// accumulator is read once from TMEM, written to global memory, and split into
+// the next product's bf16 hi/lo operand tile in shared memory, so the data
+// never leaves the SM between the two contractions.
 // smem: A hi, A lo (128 x maxKp each), B hi, B lo (maxJp x maxKp each), bf16.
 __global__ void __launch_bounds__(128) legendre_mma_kernel(const LegProblem* __restrict__ probs,
                                                            const LegWork* __restrict__ work, int nwork, int maxJp,
@@ -66,31 +106,24 @@ __global__ void __launch_bounds__(128) legendre_mma_kernel(const LegProblem* __r
 
   for (int it = blockIdx.x; it < nwork && ok; it += gridDim.x) {
     const LegWork wk = work[it];
-    const LegProblem& P = probs[wk.prob];
-    const int m = wk.m, q0 = wk.q0, K = P.K, J = P.J, Kp = P.Kp, Jp = P.Jp, KC = Kp >> 3;
-    const int nq = min(MMA_M, P.Q - q0);
-    // ---- table image for this m: a straight 16-byte copy (already split and laid out)
+    const int m = wk.m, q0 = wk.q0;
+    int pid = wk.prob;
+    const LegProblem& R = probs[pid];
+    const int nq = min(MMA_M, R.Q - q0);
+    stage_table(R, m, sBh, sBl, tid);
+    // ---- data rows of the root: FP32 -> bf16 hi/lo, one 8-element
+    // core-matrix row per thread and step; consecutive threads take
+    // consecutive rows
     {
-      const uint4* src = (const uint4*)((const uint16_t*)P.Bimg + (long long)m * P.sBimg);
-      const int n16 = (Jp * Kp) >> 3;  // uint4 per image
-      uint4* dh = (uint4*)sBh;
-      uint4* dl = (uint4*)sBl;
-      for (int i = tid; i < n16; i += 128) {
-        dh[i] = src[i];
-        dl[i] = src[n16 + i];
-      }
-    }
-    // ---- data rows: FP32 -> bf16 hi/lo, one 8-element core-matrix row per
-    // thread and step; consecutive threads take consecutive rows
-    {
-      const float* A = (const float*)P.A;
+      const int K = R.K, KC = R.Kp >> 3;
+      const float* A = (const float*)R.A;
       for (int idx = tid; idx < MMA_M * KC; idx += 128) {
         const int kc = idx >> 7, q = idx & 127, k0 = kc << 3;
         float x[8];
         if (q < nq) {
-          const int qq = q0 + q, c = qq / P.rpc, r = qq - c * P.rpc;
-          const float* row = A + (long long)c * P.sAc + (long long)r * P.sAr + (long long)m * P.sAm;
-          if (P.vecA && k0 + 8 <= K) {
+          const int qq = q0 + q, c = qq / R.rpc, r = qq - c * R.rpc;
+          const float* row = A + (long long)c * R.sAc + (long long)r * R.sAr + (long long)m * R.sAm;
+          if (R.vecA && k0 + 8 <= K) {
             const float4 a = *(const float4*)(row + k0), b = *(const float4*)(row + k0 + 4);
             x[0] = a.x; x[1] = a.y; x[2] = a.z; x[3] = a.w;
             x[4] = b.x; x[5] = b.y; x[6] = b.z; x[7] = b.w;
@@ -104,64 +137,87 @@ __global__ void __launch_bounds__(128) legendre_mma_kernel(const LegProblem* __r
         }
         uint4 hi, lo;
         split8(x, hi, lo);
-        const int o = (((q >> 3) * KC + kc) << 6) + ((q & 7) << 3);
+        const int o = cm_offset(q, kc, KC);
         *(uint4*)(sAh + o) = hi;
         *(uint4*)(sAl + o) = lo;
       }
     }
-    fence_async_smem();  // generic-proxy smem writes -> visible to the tensor core
-    fence_before();
-    __syncthreads();
-    fence_after();
-    // ---- MMAs: one thread issues 3 per K step of 16 (hi.hi, hi.lo, lo.hi)
-    if (tid == 0) {
-      const uint32_t idesc = idesc_bf16(MMA_M, Jp);
-      const uint32_t lbo = 128, sbo = (uint32_t)Kp * 16;
-      const uint32_t aH = smem_u32(sAh), aL = smem_u32(sAl), bH = smem_u32(sBh), bL = smem_u32(sBl);
-      const int s0 = P.tri ? (m >> 4) : 0;  // synthesis: coefficients below n = m vanish
-      uint32_t acc = 0;
-      for (int s = s0; s < (Kp >> 4); ++s) {
-        const uint32_t o = (uint32_t)s * 256;
-        mma_bf16(tmem, desc(aH + o, lbo, sbo), desc(bH + o, lbo, sbo), idesc, acc);
-        acc = 1;
-        mma_bf16(tmem, desc(aH + o, lbo, sbo), desc(bL + o, lbo, sbo), idesc, 1);
-        mma_bf16(tmem, desc(aL + o, lbo, sbo), desc(bH + o, lbo, sbo), idesc, 1);
+    // ---- the root, then its chained products: one MMA group per problem
+    for (int level = 0; level < 3 && ok; ++level) {
+      const LegProblem& P = probs[pid];
+      fence_async_smem();  // generic-proxy smem writes -> visible to the tensor core
+      fence_before();
+      __syncthreads();
+      fence_after();
+      if (tid == 0) issue_mma(P, m, tmem, sAh, sAl, sBh, sBl, &s_bar);
+      __syncwarp();
+      // every thread waits; the CTA then agrees on the outcome so that all of
+      // its threads leave the loop together on a timeout
+      const int waited = mbar_wait(&s_bar, phase) ? 1 : 0;
+      if (!__syncthreads_and(waited)) {
+        if (tid == 0) atomicExch(err, 1);
+        ok = false;
+        break;
       }
-      commit(&s_bar);
-    }
-    __syncwarp();
-    // every thread waits; the CTA then agrees on the outcome so that all of
-    // its threads leave the loop together on a timeout
-    const int waited = mbar_wait(&s_bar, phase) ? 1 : 0;
-    if (!__syncthreads_and(waited)) {
-      if (tid == 0) atomicExch(err, 1);
-      ok = false;
-      break;
-    }
-    phase ^= 1u;
-    fence_after();
-    // ---- epilogue: warp w holds rows 32w..32w+31 of the tile (TMEM lanes)
-    {
-      const int q = warp * 32 + lane;
-      float* drow = nullptr;
-      if (q < nq) {
-        const int qq = q0 + q, c = qq / P.rpc, r = qq - c * P.rpc;
-        drow = (float*)P.D + (long long)c * P.sDc + (long long)r * P.sDr + (long long)m * P.sDm;
-      }
-      for (int j0 = 0; j0 < Jp; j0 += 16) {
-        float v[16];
-        tmem_ld16(tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)j0, v);
-        if (drow) {
-          if (P.vecD && j0 + 16 <= J) {
+      phase ^= 1u;
+      fence_after();
+      // chained products of the root take its rows as their A operand
+      const bool chain = level == 0 && P.next[0] >= 0;
+      const int KC2 = P.Jp >> 3;  // next K padded = this J padded
+      // ---- epilogue: warp w holds rows 32w..32w+31 of the tile (TMEM lanes)
+      {
+        const int q = warp * 32 + lane;
+        const int J = P.J;
+        float* drow = nullptr;
+        if (q < nq) {
+          const int qq = q0 + q, c = qq / P.rpc, r = qq - c * P.rpc;
+          drow = (float*)P.D + (long long)c * P.sDc + (long long)r * P.sDr + (long long)m * P.sDm;
+        }
+        for (int j0 = 0; j0 < P.Jp; j0 += 16) {
+          float v[16];
+          tmem_ld16(tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)j0, v);
+          if (drow) {
+            if (P.vecD && j0 + 16 <= J) {
 #pragma unroll
-            for (int i = 0; i < 16; i += 4) *(float4*)(drow + j0 + i) = make_float4(v[i], v[i + 1], v[i + 2], v[i + 3]);
-          } else {
+              for (int i = 0; i < 16; i += 4)
+                *(float4*)(drow + j0 + i) = make_float4(v[i], v[i + 1], v[i + 2], v[i + 3]);
+            } else {
 #pragma unroll
-            for (int i = 0; i < 16; ++i)
-              if (j0 + i < J) drow[j0 + i] = v[i];
+              for (int i = 0; i < 16; ++i)
+                if (j0 + i < J) drow[j0 + i] = v[i];
+            }
+          }
+          if (chain) {  // root MMA is complete: its A tile is free for the next operand
+#pragma unroll
+            for (int h = 0; h < 2; ++h) {
+              float x[8];
+#pragma unroll
+              for (int i = 0; i < 8; ++i) x[i] = (j0 + 8 * h + i < J && q < nq) ? v[8 * h + i] : 0.f;
+              uint4 hi, lo;
+              split8(x, hi, lo);
+              const int o = cm_offset(q, (j0 >> 3) + h, KC2);
+              *(uint4*)(sAh + o) = hi;
+              *(uint4*)(sAl + o) = lo;
+            }
           }
         }
       }
+      if (level == 0) {
+        if (!chain) break;
+        pid = P.next[0];
+      } else if (level == 1) {
+        // the second chained product of the root (same A operand), if any
+        const int n2 = probs[wk.prob].next[1];
+        if (n2 < 0) break;
+        pid = n2;
+      } else {
+        break;
+      }
+      // all TMEM reads and operand writes are done before the next MMA
+      fence_before();
+      __syncthreads();
+      fence_after();
+      stage_table(probs[pid], m, sBh, sBl, tid);
     }
     fence_before();
     __syncthreads();  // TMEM reads and smem operands done before the next tile
@@ -175,8 +231,7 @@ __global__ void __launch_bounds__(128) legendre_mma_kernel(const LegProblem* __r
   fence_before();
   __syncthreads();
   fence_after();
-  if (warp == 0)
-    tmem_free(tmem, (uint32_t)tmem_cols);
+  if (warp == 0) tmem_free(tmem, (uint32_t)tmem_cols);
 }
 
 size_t legendre_mma_smem(int maxJp, int maxKp) {

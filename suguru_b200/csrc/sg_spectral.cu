@@ -29,6 +29,19 @@ constexpr int pidx() {
   return sizeof(T) == 8 ? 0 : 1;
 }
 
+// Division in the pointwise geometry and mechanics: the FP32 path uses the
+// fast reciprocal-based division (2 ulp), the FP64 path the IEEE division.
+template <class T>
+__device__ __forceinline__ T fdiv(T a, T b);
+template <>
+__device__ __forceinline__ float fdiv<float>(float a, float b) {
+  return __fdividef(a, b);
+}
+template <>
+__device__ __forceinline__ double fdiv<double>(double a, double b) {
+  return a / b;
+}
+
 // ------------------------------------------------------------ centroid -----
 __global__ void centroid_kernel(int ncap, const CapInfo* __restrict__ caps, const double* __restrict__ X,
                                 const double* __restrict__ Y, const double* __restrict__ Z, double* __restrict__ cen) {
@@ -148,7 +161,7 @@ __device__ __forceinline__ void geometry(Geo<T>& G) {
   T cc[3];
   cross3(G.a1, G.a2, cc);
   const T sm = sqrt(cc[0] * cc[0] + cc[1] * cc[1] + cc[2] * cc[2]);
-  for (int c = 0; c < 3; ++c) G.n[c] = cc[c] / sm;
+  for (int c = 0; c < 3; ++c) G.n[c] = fdiv(cc[c], sm);
   T nde[2][3];
 #pragma unroll
   for (int al = 0; al < 2; ++al) {
@@ -156,8 +169,8 @@ __device__ __forceinline__ void geometry(Geo<T>& G) {
     cross3(cd1[al], G.a2, x1);
     cross3(G.a1, cd2[al], x2);
     for (int c = 0; c < 3; ++c) dc[c] = x1[c] + x2[c];
-    const T tmp = dot3(cc, dc) / sqrt(cc[0] * cc[0] + cc[1] * cc[1] + cc[2] * cc[2]);
-    for (int c = 0; c < 3; ++c) nde[al][c] = T(1) / sm * (x1[c] + x2[c] - tmp * G.n[c]);
+    const T tmp = fdiv(dot3(cc, dc), sqrt(cc[0] * cc[0] + cc[1] * cc[1] + cc[2] * cc[2]));
+    for (int c = 0; c < 3; ++c) nde[al][c] = fdiv(T(1), sm) * (x1[c] + x2[c] - tmp * G.n[c]);
   }
   G.bcur[0] = dot3(G.n, G.d11);
   G.bcur[1] = dot3(G.n, G.d22);
@@ -167,8 +180,8 @@ __device__ __forceinline__ void geometry(Geo<T>& G) {
   cross3(G.n, G.a1, na1);
   const T hyb1 = dot3(G.a1, a2n), hyb2 = dot3(G.a2, na1);
   for (int c = 0; c < 3; ++c) {
-    G.c1[c] = a2n[c] / hyb1;
-    G.c2[c] = na1[c] / hyb2;
+    G.c1[c] = fdiv(a2n[c], hyb1);
+    G.c2[c] = fdiv(na1[c], hyb2);
   }
   const T g = hyb1;
   T cdc1[2][3], cdc2[2][3];
@@ -182,8 +195,8 @@ __device__ __forceinline__ void geometry(Geo<T>& G) {
     for (int c = 0; c < 3; ++c) vt[c] = a2de_n3[c] + a2_n3de[c];
     const T gde = dot3(cd1[al], a2n) + dot3(G.a1, vt);
     for (int c = 0; c < 3; ++c) {
-      cdc1[al][c] = T(1) / g * (-gde * G.c1[c] + a2de_n3[c] + a2_n3de[c]);
-      cdc2[al][c] = T(1) / g * (-gde * G.c2[c] + n3de_a1[c] + n3_a1de[c]);
+      cdc1[al][c] = fdiv(T(1), g) * (-gde * G.c1[c] + a2de_n3[c] + a2_n3de[c]);
+      cdc2[al][c] = fdiv(T(1), g) * (-gde * G.c2[c] + n3de_a1[c] + n3_a1de[c]);
     }
   }
   // christof(gamma,beta,alpha) at [(gamma-1) + 2(beta-1) + 4(alpha-1)]
@@ -233,11 +246,11 @@ __device__ __forceinline__ void mechanics(const Geo<T>& G, const T* A, const T (
     const T abs_conAd = Ad11 * A22 + A11 * Ad22 - T(2) * A12 * Ad12;
     const T abs_cad = cd11 * c22 + c11 * cd22 - T(2) * c12 * cd12;
     I2de[al] = abs_conAd * abs_ca + abs_cad * abs_conA;
-    Jsde[al] = T(0.5) / Js * I2de[al];
+    Jsde[al] = fdiv(T(0.5), Js) * I2de[al];
   }
   const T W1 = hf * (T(1) + I1);
   const T W2 = hf * (csk * I2 - T(1));
-  const T coef1 = T(2) / Js * W1, coef2 = T(2) * Js * W2;
+  const T coef1 = fdiv(T(2), Js) * W1, coef2 = T(2) * Js * W2;
   const T a11 = G.conat[0], a22 = G.conat[1], a12 = G.conat[2];
   const T T11 = coef1 * A11 + coef2 * a11;
   const T T22 = coef1 * A22 + coef2 * a22;
@@ -246,9 +259,9 @@ __device__ __forceinline__ void mechanics(const Geo<T>& G, const T* A, const T (
 #pragma unroll
   for (int al = 0; al < 2; ++al) {
     const T W1de = hf * I1de[al], W2de = csk * hf * I2de[al];
-    const T v1 = -T(2) / (Js * Js) * Jsde[al] * W1;
-    const T v2 = T(2) / Js * W1de;
-    const T v3 = T(2) / Js * W1;
+    const T v1 = fdiv(-T(2), Js * Js) * Jsde[al] * W1;
+    const T v2 = fdiv(T(2), Js) * W1de;
+    const T v3 = fdiv(T(2), Js) * W1;
     const T v4 = T(2) * Jsde[al] * W2;
     const T v5 = T(2) * Js * W2de;
     const T v6 = T(2) * Js * W2;
@@ -374,14 +387,14 @@ __global__ void __launch_bounds__(256, sizeof(T) == 4 ? 3 : 2) membrane_kernel(c
       T cc[3];
       cross3(Gm.a1, Gm.a2, cc);  // sph1.f90:611-651
       const T sm = sqrt(cc[0] * cc[0] + cc[1] * cc[1] + cc[2] * cc[2]);
-      for (int c = 0; c < 3; ++c) Gm.n[c] = cc[c] / sm;
+      for (int c = 0; c < 3; ++c) Gm.n[c] = fdiv(cc[c], sm);
     } else {
       geometry<T>(Gm);
       // reference contravariant metric of the sphere: A^11 = 1/R^2,
       // A^22 = 1/(R^2 sin^2 t), d/dt A^22 = -2 cos t / (R^2 sin^3 t)
-      const T iR2 = T(1) / (R * R);
-      T A[3] = {iR2, iR2 / (st * st), T(0)};
-      T Ad[2][3] = {{T(0), -T(2) * ct * iR2 / (st * st * st), T(0)}, {T(0), T(0), T(0)}};
+      const T iR2 = fdiv(T(1), R * R);
+      T A[3] = {iR2, fdiv(iR2, st * st), T(0)};
+      T Ad[2][3] = {{T(0), fdiv(-T(2) * ct * iR2, st * st * st), T(0)}, {T(0), T(0), T(0)}};
       mechanics<T>(Gm, A, Ad, hf, csk, f);
     }
     T* o = sOut + r * 6 * (mD + 1);
@@ -484,9 +497,9 @@ __global__ void __launch_bounds__(256) shgrid_kernel(const RowWork* __restrict__
         T cc[3];
         cross3(a1, a2, cc);
         T* o = sOut + r * 4 * (mO + 1);
-        o[0 * (mO + 1) + j] = nv[0] / rn;
-        o[1 * (mO + 1) + j] = nv[1] / rn;
-        o[2 * (mO + 1) + j] = nv[2] / rn;
+        o[0 * (mO + 1) + j] = fdiv(nv[0], rn);
+        o[1 * (mO + 1) + j] = fdiv(nv[1], rn);
+        o[2 * (mO + 1) + j] = fdiv(nv[2], rn);
         o[3 * (mO + 1) + j] = sqrt(cc[0] * cc[0] + cc[1] * cc[1] + cc[2] * cc[2]);
       }
       __syncthreads();

@@ -31,6 +31,7 @@ extern "C" int sg_test_legendre(int tensor_cores, int M, int Q, int J, int K, in
   p.tri = tri;
   p.Jp = Jp;
   p.Kp = Kp;
+  p.next[0] = p.next[1] = -1;
   p.sBimg = 2LL * Jp * Kp;
   std::vector<uint16_t> img((size_t)M * p.sBimg);
   host_umma_image(B, p.sBm, M, J, K, Jp, Kp, img.data());
