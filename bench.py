@@ -46,6 +46,8 @@ def parse_args():
                    help="time one path only, no e2e (for profiler captures)")
     p.add_argument("--cpu-sample-caps", type=int, default=64)
     p.add_argument("--no-surrogate", action="store_true", help="skip training and timing the surrogate path")
+    p.add_argument("--legendre-terms", type=int, default=0, choices=[0, 3, 6],
+                   help="mixed path: split products of the tensor-core Legendre contractions (0: automatic by degree)")
     p.add_argument("--sur-samples", type=int, default=200000)
     p.add_argument("--sur-epochs", type=int, default=40)
     p.add_argument("--sur-loose-tol", type=float, default=3e-2)
@@ -176,8 +178,23 @@ def run_ours(args):
     flush = torch.empty(2 * L2_BYTES // 4, dtype=torch.float32, device=dev)
 
     def make_cs(precision, surrogate=False):
-        return CouplingStep(wl.grid, wl.degree, wl.radius, wl.gs, wl.csk, precision=precision, mem="device",
-                            device=local, stream=stream.cuda_stream, async_=True, surrogate=surrogate)
+        cs = CouplingStep(wl.grid, wl.degree, wl.radius, wl.gs, wl.csk, precision=precision, mem="device",
+                          device=local, stream=stream.cuda_stream, async_=True, surrogate=surrogate)
+        if precision != "fp64":
+            cs.set_legendre_terms(args.legendre_terms)
+        return cs
+
+    capidx = torch.repeat_interleave(torch.arange(wl.ncap, device=dev),
+                                     torch.from_numpy(np.diff(wl.offsets).astype(np.int64)).to(dev))
+
+    def worst_capsule(out, ref):
+        """Largest per-capsule relative L2 error of the force vectors."""
+        num = torch.zeros(wl.ncap, dtype=torch.float64, device=dev)
+        den = torch.zeros_like(num)
+        for c in range(3):
+            num.index_add_(0, capidx, (out[3 + c].double() - ref[3 + c].double()) ** 2)
+            den.index_add_(0, capidx, ref[3 + c].double() ** 2)
+        return float(torch.sqrt(num / torch.clamp(den, min=1e-300)).max())
 
     def time_path(cs, precision, tune=True):
         dtype = np.float64 if precision == "fp64" else np.float32
@@ -236,7 +253,8 @@ def run_ours(args):
         """Relative L2 of the mixed-path results against the FP64 plain path (itself within 1e-10 of the oracle)."""
         return {"velocity": max(rel_l2_t(out[c], ref[c]) for c in range(3)),
                 "force": max(rel_l2_t(out[3 + c], ref[3 + c]) for c in range(3)),
-                "spread_field": max(rel_l2_t(out[10 + c], ref[10 + c]) for c in range(3))}
+                "spread_field": max(rel_l2_t(out[10 + c], ref[10 + c]) for c in range(3)),
+                "force_worst_capsule": worst_capsule(out, ref)}
 
     if args.only:
         cs = make_cs(args.only)
@@ -343,7 +361,8 @@ def run_ours(args):
             "higher_is_better": True,
             "scaling": "weak",
             "vs_baseline": None,
-            "dtype": "f32 (Legendre contractions BF16x3 on tcgen05 tensor cores, FP32 accumulation; "
+            "dtype": "f32 (Legendre contractions on tcgen05 tensor cores, BF16x3 below SH degree 16 and "
+                     "BF16x6 from 16 up unless --legendre-terms forces one, FP32 accumulation; "
                      "FP64 positions, centroids, tables)",
             "data": "synthetic (seeded shapes and velocity modes, no reference fixtures exist)",
             "config": {"workload": "dense suspension: 256 capsules, SH degree 15 (524,288 points), "

@@ -204,6 +204,21 @@ int sg_last_launch_count(const sg_ctx* ctx);
 int sg_set_tile_shape(sg_ctx* ctx, int shape);
 int sg_get_tile_shape(const sg_ctx* ctx, int* shape, int* tx, int* ty, int* tz);
 
+/* Mixed precision only: split mode of the tensor-core Legendre contractions.
+ * terms = 3 (BF16x3: A0B0 + A0B1 + A1B0, about 16 significant bits per
+ * product), 6 (BF16x6: + A0B2 + A2B0 + A1B1, FP32-level products) or 0
+ * (automatic, the default: BF16x6 for capsules of SH degree >= 16, whose
+ * force error under BF16x3 approaches 1e-4, BF16x3 below).  Returns
+ * SG_ERR_STATE while a graph is captured. */
+int sg_set_legendre_terms(sg_ctx* ctx, int terms);
+/* The split products (3 or 6) a capsule of this SH degree runs with. */
+int sg_get_legendre_terms(sg_ctx* ctx, int degree);
+
+/* Mixed precision only: run the Legendre contractions on the tensor cores in
+ * BF16x3 (on = 1, the default) or on the CUDA cores in FP32 (on = 0), for
+ * comparisons of the two. */
+int sg_set_tensor_cores(sg_ctx* ctx, int on);
+
 /* Schedule of the persistent per-capsule kernels (no counterpart in the
  * reference): every capsule is cut into `split` row ranges, 1 <= split <= 8,
  * so that few capsules still fill every SM.  Results do not depend on it. */

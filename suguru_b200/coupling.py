@@ -36,7 +36,8 @@ EXPORTS = ["sg_create", "sg_destroy", "sg_last_error", "sg_synchronize", "sg_int
            "sg_set_tile_shape", "sg_get_tile_shape", "sg_autotune", "sg_graph_capture", "sg_graph_launch",
            "sg_graph_release", "sg_set_capsule_membrane", "sg_capsule_spectra", "sg_surrogate_param_count",
            "sg_surrogate_params", "sg_surrogate_set_linear", "sg_surrogate_train", "sg_surrogate_predict",
-           "sg_surrogate_set_trust", "sg_surrogate_last_counts", "sg_set_point_split", "sg_get_point_split"]
+           "sg_surrogate_set_trust", "sg_surrogate_last_counts", "sg_set_point_split", "sg_get_point_split",
+           "sg_set_tensor_cores", "sg_set_legendre_terms", "sg_get_legendre_terms"]
 # test hooks declared in include/sg_testing.h
 TEST_EXPORTS = ["sg_test_legendre", "sg_test_gemm", "sg_test_mlp_grad"]
 TILE_SHAPES = ((32, 8, 4), (16, 16, 8), (32, 8, 8), (8, 8, 4))
@@ -91,6 +92,9 @@ def lib():
     ip = ctypes.POINTER(ctypes.c_int)
     L.sg_set_tile_shape.argtypes = [vp, ctypes.c_int]
     L.sg_set_point_split.argtypes = [vp, ctypes.c_int]
+    L.sg_set_tensor_cores.argtypes = [vp, ctypes.c_int]
+    L.sg_set_legendre_terms.argtypes = [vp, ctypes.c_int]
+    L.sg_get_legendre_terms.argtypes = [vp, ctypes.c_int]
     L.sg_get_point_split.argtypes = [vp]
     L.sg_get_tile_shape.argtypes = [vp, ip, ip, ip, ip]
     L.sg_autotune.argtypes = [vp] * 20 + [ctypes.c_int, ip, ctypes.POINTER(ctypes.c_float)]
@@ -118,15 +122,20 @@ def lib():
     return L
 
 
-def test_legendre(A, B, tensor_cores=True, tri=False):
-    """D[m,q,j] = sum_k A[m,q,k] B[m,j,k] through one Legendre kernel (test hook)."""
+def test_legendre(A, B, tensor_cores=True, tri=False, terms=3):
+    """D[m,q,j] = sum_k A[m,q,k] B[m,j,k] through one Legendre kernel (test hook).
+
+    tensor_cores: the tcgen05 kernel with `terms` split products (3: BF16x3,
+    6: BF16x6); otherwise the FP32 CUDA-core kernel.
+    """
     A = np.ascontiguousarray(A, dtype=np.float32)
     B = np.ascontiguousarray(B, dtype=np.float64)
     M, Q, K = A.shape
     J = B.shape[1]
     assert B.shape == (M, J, K)
     D = np.zeros((M, Q, J), dtype=np.float32)
-    rc = lib().sg_test_legendre(int(bool(tensor_cores)), M, Q, J, K, int(bool(tri)), _ptr(B), _ptr(A), _ptr(D))
+    mode = int(terms) if tensor_cores else 0
+    rc = lib().sg_test_legendre(mode, M, Q, J, K, int(bool(tri)), _ptr(B), _ptr(A), _ptr(D))
     if rc:
         raise SgError(rc, "sg_test_legendre")
     return D
@@ -309,6 +318,18 @@ class CouplingStep:
     def set_point_split(self, split):
         """Work items per capsule of the persistent pointwise kernels (1..8)."""
         self._check(lib().sg_set_point_split(self._h, int(split)), "sg_set_point_split")
+
+    def set_legendre_terms(self, terms=0):
+        """Split mode of the tensor-core Legendre products: 3 (BF16x3), 6 (BF16x6), 0 automatic by degree."""
+        self._check(lib().sg_set_legendre_terms(self._h, int(terms)), "sg_set_legendre_terms")
+
+    def legendre_terms(self, degree):
+        """Split products (3 or 6) that capsules of this SH degree run with."""
+        return int(lib().sg_get_legendre_terms(self._h, int(degree)))
+
+    def set_tensor_cores(self, on=True):
+        """Mixed path: Legendre contractions on the tensor cores (BF16x3) or on CUDA cores (FP32)."""
+        self._check(lib().sg_set_tensor_cores(self._h, int(bool(on))), "sg_set_tensor_cores")
 
     def point_split(self):
         return lib().sg_get_point_split(self._h)

@@ -16,6 +16,29 @@ const double kPi = 3.14159265358979323846264338327950288;
 
 namespace {
 
+// Lowest SH degree whose tensor-core contractions run in BF16x6 under the
+// automatic split mode.  The force takes second derivatives of the analysed
+// shape, so the ~2^-17 relative error of a BF16x3 product grows about as
+// L^2 in the force: measured against the FP64 oracle, BF16x3 gives
+// 2e-5 (L = 8), 4e-5 to 8e-5 (L = 12 to 16) and 2.5e-4 (L = 22); BF16x6
+// keeps every degree at the FP32 CUDA-core level.
+constexpr int kSixTermDegree = 16;
+
+int terms_for(const sg_ctx* c, int degree) {
+  if (c->leg_terms) return c->leg_terms;
+  return degree >= kSixTermDegree ? 6 : 3;
+}
+
+// Split mode of every tensor-core problem (by its group's degree) and the
+// number of operand parts the launches stage.
+void assign_terms(sg_ctx* c, std::vector<sg::LegProblem>& P) {
+  c->leg_parts = 2;
+  for (sg::LegProblem& p : P) {
+    p.terms = terms_for(c, c->groups[p.group].L);
+    if (p.terms == 6) c->leg_parts = 3;
+  }
+}
+
 template <class V>
 cudaError_t upload(sg_ctx* c, void*& dst, const std::vector<V>& v) {
   cudaError_t e = dalloc(c, dst, sizeof(V) * v.size());
@@ -330,7 +353,7 @@ int setup(sg_ctx* c) {
       LegProblem& p = P[pi2];
       p.Jp = (p.J + 15) / 16 * 16;
       p.Kp = (p.K + 15) / 16 * 16;
-      p.sBimg = 2LL * p.Jp * p.Kp;
+      p.sBimg = 3LL * p.Jp * p.Kp;
       img_off[pi2] = img.size();
       img.resize(img.size() + (size_t)p.M * p.sBimg);
       const std::vector<double>& hb = c->groups[p.group].h_tab[p.kind];
@@ -360,7 +383,9 @@ int setup(sg_ctx* c) {
       c->d_lwF[f] = (LegWork*)tmp;
     }
     c->leg_tc = true;
+    assign_terms(c, P);
   }
+  c->h_probs = P;
   SG_TRY(upload(c, tmp, P), "problems");
   c->d_probs = (LegProblem*)tmp;
   for (int s = 0; s < 6; ++s) {
@@ -429,8 +454,8 @@ int dev_legendre(sg_ctx* c, int s) {
     // stages 0, 2, 4 launch the chained products; 1, 3, 5 ran inside them
     if (s % 2) return SG_OK;
     const int f = s / 2;
-    SG_TRY(launch_legendre_mma(c->d_probs, c->d_lwF[f], c->nlwF[f], c->maxJpF[f], c->maxKpF[f], c->d_err,
-                               c->num_sms, c->st),
+    SG_TRY(launch_legendre_mma(c->d_probs, c->d_lwF[f], c->nlwF[f], c->maxJpF[f], c->maxKpF[f], c->leg_parts,
+                               c->d_err, c->num_sms, c->st),
            "legendre (tensor cores)");
     c->launches += 1;
   } else {
@@ -810,6 +835,33 @@ int sg_set_tile_shape(sg_ctx* c, int shape) {
   if (!make_ib_grid(cfg.itot, cfg.jtot, cfg.ktot, cfg.lx, cfg.ly, cfg.lz, g, shape) || g.ntiles > c->max_tiles)
     return fail(c, SG_ERR_ARG, "tile shape not valid for this grid");
   c->grid = g;
+  return SG_OK;
+}
+
+int sg_set_legendre_terms(sg_ctx* c, int terms) {
+  if (!c) return SG_ERR_ARG;
+  if (terms != 0 && terms != 3 && terms != 6) return fail(c, SG_ERR_ARG, "terms must be 0 (automatic), 3 or 6");
+  if (c->graph) return fail(c, SG_ERR_STATE, "release the captured graph first");
+  if (!c->mixed) return fail(c, SG_ERR_CONFIG, "the split modes belong to the mixed-precision path");
+  c->leg_terms = terms;
+  if (c->h_probs.empty()) return SG_OK;
+  assign_terms(c, c->h_probs);
+  SG_TRY(cudaStreamSynchronize(c->st), "sync");
+  SG_TRY(cudaMemcpy(c->d_probs, c->h_probs.data(), sizeof(LegProblem) * c->h_probs.size(), cudaMemcpyHostToDevice),
+         "problems");
+  return SG_OK;
+}
+
+int sg_get_legendre_terms(sg_ctx* c, int degree) {
+  if (!c || degree < 0) return -1;
+  return terms_for(c, degree);
+}
+
+int sg_set_tensor_cores(sg_ctx* c, int on) {
+  if (!c) return SG_ERR_ARG;
+  if (c->graph) return fail(c, SG_ERR_STATE, "release the captured graph first");
+  if (on && !c->mixed) return fail(c, SG_ERR_CONFIG, "the tensor-core path is the mixed-precision path");
+  c->leg_tc = on != 0 && c->nlwF[0] > 0;
   return SG_OK;
 }
 

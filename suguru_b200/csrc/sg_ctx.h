@@ -59,6 +59,11 @@ struct sg_ctx {
   int maxJ[6] = {}, maxK[6] = {};
   // tensor-core Legendre path (mixed precision): 128-row work lists
   bool leg_tc = false;
+  // split mode of the tensor-core contractions: 0 automatic (BF16x6 from
+  // degree kSixTermDegree up, BF16x3 below), 3 or 6 for every group
+  int leg_terms = 0;
+  int leg_parts = 2;                  // bf16 parts staged per operand (3 if any group is BF16x6)
+  std::vector<LegProblem> h_probs;    // host copy of d_probs (the split mode is rewritten in place)
   LegWork* d_lwF[3] = {};  // root work items of the three chained launches
   int nlwF[3] = {};
   int maxJpF[3] = {}, maxKpF[3] = {};

@@ -83,11 +83,12 @@ struct LegProblem {
   int tri;       // 1: k starts at m (synthesis: coefficients vanish for n<m)
   int group;     // degree group
   int kind;      // 0 syn_D, 1 ana_D, 2 syn_O, 3 ana_O
-  // tensor-core operands (mixed path): per m, the bf16 hi image then the lo
-  // image of B_m, each Jp x Kp in UMMA core-matrix order; sBimg = 2 Jp Kp
+  // tensor-core operands (mixed path): per m, the three bf16 parts of B_m
+  // (B = B0 + B1 + B2), each Jp x Kp in UMMA core-matrix order; sBimg = 3 Jp Kp
   const void* Bimg;
   long long sBimg;
   int Jp, Kp;    // J, K rounded up to multiples of 16
+  int terms;     // split products: 3 (BF16x3) or 6 (BF16x6)
   int vecA;      // A rows 16-byte aligned with K % 8 == 0: float4 loads
   int vecD;      // D rows 16-byte aligned with J % 4 == 0: float4 stores
   int next[2];   // tensor-core path: problems whose A operand is this problem's output (-1: none)
@@ -100,10 +101,12 @@ struct LegWork {  // one tile of a problem
 template <class T>
 cudaError_t launch_legendre(const LegProblem* d_probs, const LegWork* d_work, int nwork, int maxJ, int maxK,
                             cudaStream_t st);
-// Tensor-core (tcgen05, BF16x3) contraction of FP32 problems; work items are
-// 128-row tiles.  d_err is set to 1 if an MMA completion wait times out.
+// Tensor-core (tcgen05, BF16x3 / BF16x6) contraction of FP32 problems; work
+// items are 128-row tiles.  nparts = 3 if any problem reached is BF16x6, else
+// 2.  d_err is set to 1 if an MMA completion wait times out, 2 if a problem's
+// mode does not fit nparts or differs along a chain.
 cudaError_t launch_legendre_mma(const LegProblem* d_probs, const LegWork* d_work, int nwork, int maxJp, int maxKp,
-                                int* d_err, int num_sms, cudaStream_t st);
+                                int nparts, int* d_err, int num_sms, cudaStream_t st);
 // Dense product on the tensor cores (sg_gemm.cu):
 //   C = alpha A B^T (+ bias[n]) (then GELU), A [M][K], B [N][K], K % 64 == 0.
 // split = 0: A, B bf16; split = 1: A, B FP32, split into bf16 hi/lo (BF16x3).
@@ -136,8 +139,9 @@ struct GemmArgs {
 };
 cudaError_t launch_gemm(const GemmArgs& g, int* d_err, cudaStream_t st);
 
-// bf16 hi/lo images of a table B[m][j][k] (row stride K, m stride sBm) in
-// UMMA core-matrix order: out[m][2][Jp/8][Kp/8][8][8]
+// The three bf16 parts (B = B0 + B1 + B2, Bi = bf16 of what the earlier parts
+// leave) of a table B[m][j][k] (row stride K, m stride sBm) in UMMA
+// core-matrix order: out[m][3][Jp/8][Kp/8][8][8]
 void host_umma_image(const double* B, long long sBm, int M, int J, int K, int Jp, int Kp, uint16_t* out);
 
 // Capsule-row work items for the pointwise kernels.

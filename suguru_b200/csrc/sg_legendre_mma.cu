@@ -1,5 +1,6 @@
 // sg_legendre_mma.cu -- the Legendre contractions of the mixed-precision path
-// on the 5th-generation tensor cores (tcgen05), in BF16x3 split precision.
+// on the 5th-generation tensor cores (tcgen05), in BF16x3 or BF16x6 split
+// precision.
 //
 // Each Legendre stage of the coupling step (the theta half of SPHEREPACK's
 // Gauss-grid analysis shagc.f:384-470 and synthesis shsgc.f:329-470, batched
@@ -10,11 +11,16 @@
 // K-major, so one tile is a single "TN" UMMA: M = 128 data rows, N = J padded
 // to a multiple of 16, K padded to a multiple of 16.
 //
-// Split precision: x = hi + lo with hi = bf16(x), lo = bf16(x - hi), and
-//   A B^T ~ A_hi B_hi^T + A_hi B_lo^T + A_lo B_hi^T
-// accumulated in FP32 in tensor memory (the dropped A_lo B_lo^T term is
-// ~2^-18 relative).  The tables are split once on the host into bf16 hi/lo
-// images laid out as UMMA operands; the data rows are split while staged.
+// Split precision: x = x0 + x1 + x2 with x0 = bf16(x), x1 = bf16(x - x0),
+// x2 = bf16(x - x0 - x1).  A problem runs in one of two modes:
+//   BF16x3 (terms = 3):  A B^T ~ A0 B0^T + A0 B1^T + A1 B0^T
+//     (the dropped terms are ~2^-18 relative, about 16 significant bits);
+//   BF16x6 (terms = 6):  + A0 B2^T + A2 B0^T + A1 B1^T
+//     (dropped terms ~2^-27: FP32-level products for high degrees, whose
+//     second derivatives amplify the BF16x3 error past 1e-4).
+// Products accumulate in FP32 in tensor memory.  The tables are split once on
+// the host into three bf16 images laid out as UMMA operands; the data rows are
+// split while staged.
 //
 // Shared-memory operand layout (no swizzle, K-major canonical form): an
 // R x Kp bf16 tile is stored as [R/8][Kp/8] core matrices of 8 rows x 16
@@ -42,33 +48,62 @@ using namespace umma;
 
 namespace {
 
+// bf16 parts of the data (A) and table (B) operands in shared memory
+struct Operands {
+  uint16_t* a[3];
+  uint16_t* b[3];
+};
+
+__device__ __forceinline__ int parts_of(const LegProblem& P) { return P.terms == 6 ? 3 : 2; }
+
 // B_m image of problem P (already split and laid out): a straight 16-byte copy
-__device__ __forceinline__ void stage_table(const LegProblem& P, int m, uint16_t* sBh, uint16_t* sBl, int tid) {
+// of the parts its mode reads
+__device__ __forceinline__ void stage_table(const LegProblem& P, int m, const Operands& op, int tid) {
   const uint4* src = (const uint4*)((const uint16_t*)P.Bimg + (long long)m * P.sBimg);
   const int n16 = (P.Jp * P.Kp) >> 3;  // uint4 per image
-  uint4* dh = (uint4*)sBh;
-  uint4* dl = (uint4*)sBl;
+  uint4* d0 = (uint4*)op.b[0];
+  uint4* d1 = (uint4*)op.b[1];
   for (int i = tid; i < n16; i += 128) {
-    dh[i] = src[i];
-    dl[i] = src[n16 + i];
+    d0[i] = src[i];
+    d1[i] = src[n16 + i];
+  }
+  if (parts_of(P) == 3) {
+    uint4* d2 = (uint4*)op.b[2];
+    for (int i = tid; i < n16; i += 128) d2[i] = src[2 * n16 + i];
   }
 }
 
-// One thread issues 3 MMAs per K step of 16 (hi.hi, hi.lo, lo.hi), then commits.
-__device__ __forceinline__ void issue_mma(const LegProblem& P, int m, uint32_t tmem, const uint16_t* sAh,
-                                          const uint16_t* sAl, const uint16_t* sBh, const uint16_t* sBl,
+// Eight consecutive K values of one data row, split into the operand parts.
+__device__ __forceinline__ void store_split(const float* x, int np, const Operands& op, int o) {
+  uint4 p0, p1, p2;
+  split8x3(x, p0, p1, p2);
+  *(uint4*)(op.a[0] + o) = p0;
+  *(uint4*)(op.a[1] + o) = p1;
+  if (np == 3) *(uint4*)(op.a[2] + o) = p2;
+}
+
+// One thread issues the split products of every K step of 16 (largest terms
+// first), then commits.
+__device__ __forceinline__ void issue_mma(const LegProblem& P, int m, uint32_t tmem, const Operands& op,
                                           uint64_t* bar) {
   const uint32_t idesc = idesc_bf16(MMA_M, P.Jp);
   const uint32_t lbo = 128, sbo = (uint32_t)P.Kp * 16;
-  const uint32_t aH = smem_u32(sAh), aL = smem_u32(sAl), bH = smem_u32(sBh), bL = smem_u32(sBl);
+  const uint32_t a0 = smem_u32(op.a[0]), a1 = smem_u32(op.a[1]), b0 = smem_u32(op.b[0]), b1 = smem_u32(op.b[1]);
+  const bool six = P.terms == 6;
+  const uint32_t a2 = six ? smem_u32(op.a[2]) : 0u, b2 = six ? smem_u32(op.b[2]) : 0u;
   const int s0 = P.tri ? (m >> 4) : 0;  // synthesis: coefficients below n = m vanish
   uint32_t acc = 0;
   for (int s = s0; s < (P.Kp >> 4); ++s) {
     const uint32_t o = (uint32_t)s * 256;
-    mma_bf16(tmem, desc(aH + o, lbo, sbo), desc(bH + o, lbo, sbo), idesc, acc);
+    mma_bf16(tmem, desc(a0 + o, lbo, sbo), desc(b0 + o, lbo, sbo), idesc, acc);
     acc = 1;
-    mma_bf16(tmem, desc(aH + o, lbo, sbo), desc(bL + o, lbo, sbo), idesc, 1);
-    mma_bf16(tmem, desc(aL + o, lbo, sbo), desc(bH + o, lbo, sbo), idesc, 1);
+    mma_bf16(tmem, desc(a0 + o, lbo, sbo), desc(b1 + o, lbo, sbo), idesc, 1);
+    mma_bf16(tmem, desc(a1 + o, lbo, sbo), desc(b0 + o, lbo, sbo), idesc, 1);
+    if (six) {
+      mma_bf16(tmem, desc(a0 + o, lbo, sbo), desc(b2 + o, lbo, sbo), idesc, 1);
+      mma_bf16(tmem, desc(a2 + o, lbo, sbo), desc(b0 + o, lbo, sbo), idesc, 1);
+      mma_bf16(tmem, desc(a1 + o, lbo, sbo), desc(b1 + o, lbo, sbo), idesc, 1);
+    }
   }
   commit(bar);
 }
@@ -80,17 +115,29 @@ __device__ __forceinline__ void issue_mma(const LegProblem& P, int m, uint32_t t
 // accumulator is read once from TMEM, written to global memory, and split into
 // the next product's bf16 hi/lo operand tile in shared memory, so the data
 // never leaves the SM between the two contractions.
-// smem: A hi, A lo (128 x maxKp each), B hi, B lo (maxJp x maxKp each), bf16.
+// A chain runs in its root's mode (one degree group: the same mode throughout).
+// smem: nparts A parts (128 x maxKp each), then nparts B parts (maxJp x maxKp
+// each), bf16; nparts = 3 when any problem of the launch is BF16x6, else 2.
 __global__ void __launch_bounds__(128) legendre_mma_kernel(const LegProblem* __restrict__ probs,
                                                            const LegWork* __restrict__ work, int nwork, int maxJp,
-                                                           int maxKp, int tmem_cols, int* __restrict__ err) {
+                                                           int maxKp, int nparts, int tmem_cols,
+                                                           int* __restrict__ err) {
   extern __shared__ __align__(128) unsigned char smem_raw[];
   __shared__ __align__(8) uint64_t s_bar;
   __shared__ uint32_t s_tmem;
-  uint16_t* sAh = (uint16_t*)smem_raw;
-  uint16_t* sAl = sAh + MMA_M * maxKp;
-  uint16_t* sBh = sAl + MMA_M * maxKp;
-  uint16_t* sBl = sBh + maxJp * maxKp;
+  Operands op;
+  {
+    uint16_t* p = (uint16_t*)smem_raw;
+    for (int i = 0; i < 3; ++i) {
+      op.a[i] = p;
+      if (i + 1 < nparts) p += MMA_M * maxKp;
+    }
+    p = (uint16_t*)smem_raw + nparts * MMA_M * maxKp;
+    for (int i = 0; i < 3; ++i) {
+      op.b[i] = p;
+      if (i + 1 < nparts) p += maxJp * maxKp;
+    }
+  }
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
 
   if (warp == 0) {
@@ -110,8 +157,13 @@ __global__ void __launch_bounds__(128) legendre_mma_kernel(const LegProblem* __r
     int pid = wk.prob;
     const LegProblem& R = probs[pid];
     const int nq = min(MMA_M, R.Q - q0);
-    stage_table(R, m, sBh, sBl, tid);
-    // ---- data rows of the root: FP32 -> bf16 hi/lo, one 8-element
+    const int np = parts_of(R);
+    if (np > nparts) {  // the launch's shared memory holds fewer parts (uniform per CTA)
+      if (tid == 0) atomicExch(err, 2);
+      continue;
+    }
+    stage_table(R, m, op, tid);
+    // ---- data rows of the root: FP32 -> bf16 parts, one 8-element
     // core-matrix row per thread and step; consecutive threads take
     // consecutive rows
     {
@@ -135,11 +187,7 @@ __global__ void __launch_bounds__(128) legendre_mma_kernel(const LegProblem* __r
 #pragma unroll
           for (int i = 0; i < 8; ++i) x[i] = 0.f;
         }
-        uint4 hi, lo;
-        split8(x, hi, lo);
-        const int o = cm_offset(q, kc, KC);
-        *(uint4*)(sAh + o) = hi;
-        *(uint4*)(sAl + o) = lo;
+        store_split(x, np, op, cm_offset(q, kc, KC));
       }
     }
     // ---- the root, then its chained products: one MMA group per problem
@@ -149,7 +197,7 @@ __global__ void __launch_bounds__(128) legendre_mma_kernel(const LegProblem* __r
       fence_before();
       __syncthreads();
       fence_after();
-      if (tid == 0) issue_mma(P, m, tmem, sAh, sAl, sBh, sBl, &s_bar);
+      if (tid == 0) issue_mma(P, m, tmem, op, &s_bar);
       __syncwarp();
       // every thread waits; the CTA then agrees on the outcome so that all of
       // its threads leave the loop together on a timeout
@@ -193,11 +241,7 @@ __global__ void __launch_bounds__(128) legendre_mma_kernel(const LegProblem* __r
               float x[8];
 #pragma unroll
               for (int i = 0; i < 8; ++i) x[i] = (j0 + 8 * h + i < J && q < nq) ? v[8 * h + i] : 0.f;
-              uint4 hi, lo;
-              split8(x, hi, lo);
-              const int o = cm_offset(q, (j0 >> 3) + h, KC2);
-              *(uint4*)(sAh + o) = hi;
-              *(uint4*)(sAl + o) = lo;
+              store_split(x, np, op, cm_offset(q, (j0 >> 3) + h, KC2));
             }
           }
         }
@@ -213,11 +257,15 @@ __global__ void __launch_bounds__(128) legendre_mma_kernel(const LegProblem* __r
       } else {
         break;
       }
+      if (parts_of(probs[pid]) != np) {  // a chain keeps its root's mode
+        if (tid == 0) atomicExch(err, 2);
+        break;
+      }
       // all TMEM reads and operand writes are done before the next MMA
       fence_before();
       __syncthreads();
       fence_after();
-      stage_table(probs[pid], m, sBh, sBl, tid);
+      stage_table(probs[pid], m, op, tid);
     }
     fence_before();
     __syncthreads();  // TMEM reads and smem operands done before the next tile
@@ -234,20 +282,21 @@ __global__ void __launch_bounds__(128) legendre_mma_kernel(const LegProblem* __r
   if (warp == 0) tmem_free(tmem, (uint32_t)tmem_cols);
 }
 
-size_t legendre_mma_smem(int maxJp, int maxKp) {
-  return (size_t)2 * sizeof(uint16_t) * (MMA_M + maxJp) * maxKp;
+size_t legendre_mma_smem(int maxJp, int maxKp, int nparts) {
+  return (size_t)nparts * sizeof(uint16_t) * (MMA_M + maxJp) * maxKp;
 }
 
 cudaError_t launch_legendre_mma(const LegProblem* d_probs, const LegWork* d_work, int nwork, int maxJp, int maxKp,
-                                int* d_err, int num_sms, cudaStream_t st) {
+                                int nparts, int* d_err, int num_sms, cudaStream_t st) {
   if (nwork <= 0) return cudaSuccess;
   if (maxJp < 16 || maxJp > 256 || (maxJp & 15) || maxKp < 16 || (maxKp & 15)) return cudaErrorInvalidValue;
+  if (nparts != 2 && nparts != 3) return cudaErrorInvalidValue;
   // TMEM columns: a power of two >= 32 covering N = Jp; CTAs per SM limited
   // (through shared memory) so that their allocations always fit in 512 columns
   int cols = 32;
   while (cols < maxJp) cols <<= 1;
   const int per_sm = 512 / cols < 4 ? 512 / cols : 4;
-  size_t smem = legendre_mma_smem(maxJp, maxKp);
+  size_t smem = legendre_mma_smem(maxJp, maxKp, nparts);
   // (per_sm + 1) CTAs of this size exceed the SM's 228 KB of shared memory
   const size_t floor_smem = (size_t)(228 * 1024) / (size_t)(per_sm + 1);
   if (smem < floor_smem) smem = floor_smem;
@@ -255,7 +304,7 @@ cudaError_t launch_legendre_mma(const LegProblem* d_probs, const LegWork* d_work
   cudaError_t e = cudaFuncSetAttribute(legendre_mma_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   if (e != cudaSuccess) return e;
   const int grid = nwork < num_sms * per_sm ? nwork : num_sms * per_sm;
-  legendre_mma_kernel<<<grid, 128, smem, st>>>(d_probs, d_work, nwork, maxJp, maxKp, cols, d_err);
+  legendre_mma_kernel<<<grid, 128, smem, st>>>(d_probs, d_work, nwork, maxJp, maxKp, nparts, cols, d_err);
   return cudaGetLastError();
 }
 

@@ -122,16 +122,16 @@ void host_umma_image(const double* B, long long sBm, int M, int J, int K, int Jp
   const int KC = Kp / 8;
   const size_t img = (size_t)Jp * Kp;
   for (int m = 0; m < M; ++m) {
-    uint16_t* hi = out + (size_t)m * 2 * img;
-    uint16_t* lo = hi + img;
+    uint16_t* part = out + (size_t)m * 3 * img;
     for (int j = 0; j < Jp; ++j)
       for (int k = 0; k < Kp; ++k) {
-        const double x = (j < J && k < K) ? B[(size_t)m * sBm + (size_t)j * K + k] : 0.0;
-        const uint16_t h = f32_to_bf16((float)x);
-        const uint16_t l = f32_to_bf16((float)(x - bf16_to_double(h)));
+        double x = (j < J && k < K) ? B[(size_t)m * sBm + (size_t)j * K + k] : 0.0;
         const size_t o = ((size_t)(j / 8) * KC + k / 8) * 64 + (j % 8) * 8 + (k % 8);
-        hi[o] = h;
-        lo[o] = l;
+        for (int t = 0; t < 3; ++t) {  // each part rounds what the earlier ones leave
+          const uint16_t h = f32_to_bf16((float)x);
+          part[t * img + o] = h;
+          x -= bf16_to_double(h);
+        }
       }
   }
 }

@@ -13,6 +13,8 @@ using namespace sg;
 extern "C" int sg_test_legendre(int tensor_cores, int M, int Q, int J, int K, int tri, const double* B,
                                 const float* A, float* D) {
   if (M < 1 || Q < 1 || J < 1 || K < 1 || J > 256 || K > 256 || !B || !A || !D) return 5;
+  if (tensor_cores != 0 && tensor_cores != 1 && tensor_cores != 3 && tensor_cores != 6) return 5;
+  const int terms = tensor_cores == 6 ? 6 : 3;
   const int Jp = (J + 15) / 16 * 16, Kp = (K + 15) / 16 * 16;
   // problem: A[m][q][k] rows, B[m][j][k], D[m][q][j]
   LegProblem p{};
@@ -32,7 +34,8 @@ extern "C" int sg_test_legendre(int tensor_cores, int M, int Q, int J, int K, in
   p.Jp = Jp;
   p.Kp = Kp;
   p.next[0] = p.next[1] = -1;
-  p.sBimg = 2LL * Jp * Kp;
+  p.terms = terms;
+  p.sBimg = 3LL * Jp * Kp;
   std::vector<uint16_t> img((size_t)M * p.sBimg);
   host_umma_image(B, p.sBm, M, J, K, Jp, Kp, img.data());
   std::vector<float> Bf((size_t)M * J * K);
@@ -67,7 +70,8 @@ extern "C" int sg_test_legendre(int tensor_cores, int M, int Q, int J, int K, in
         ok(cudaMemcpy(dW, work.data(), sizeof(LegWork) * work.size(), cudaMemcpyHostToDevice)) &&
         ok(cudaMemset(dE, 0, sizeof(int))) && ok(cudaMemset(dD, 0xff, 4 * nd))) {
       if (tensor_cores)
-        ok(launch_legendre_mma((const LegProblem*)dP, (const LegWork*)dW, (int)work.size(), Jp, Kp, (int*)dE, sms, 0));
+        ok(launch_legendre_mma((const LegProblem*)dP, (const LegWork*)dW, (int)work.size(), Jp, Kp,
+                                terms == 6 ? 3 : 2, (int*)dE, sms, 0));
       else
         ok(launch_legendre<float>((const LegProblem*)dP, (const LegWork*)dW, (int)work.size(), J, K, 0));
       int err = 0;

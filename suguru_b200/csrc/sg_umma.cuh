@@ -128,6 +128,34 @@ __device__ __forceinline__ void split8(const float* x, uint4& hi, uint4& lo) {
   lo = make_uint4(l[0], l[1], l[2], l[3]);
 }
 
+// Three-way split x = p0 + p1 + p2 with p0 = bf16(x), p1 = bf16(x - p0),
+// p2 = bf16(x - p0 - p1): every difference is exact in FP32 and the three
+// 8-bit significands cover FP32's 24, so the split itself loses nothing.
+__device__ __forceinline__ void split8x3(const float* x, uint4& p0, uint4& p1, uint4& p2) {
+  uint32_t a[4], b[4], c[4];
+#pragma unroll
+  for (int i = 0; i < 4; ++i) {
+    uint32_t w[3][2];
+#pragma unroll
+    for (int e = 0; e < 2; ++e) {
+      const float v = x[2 * i + e];
+      const __nv_bfloat16 h = __float2bfloat16_rn(v);
+      const float r = v - __bfloat162float(h);
+      const __nv_bfloat16 mid = __float2bfloat16_rn(r);
+      const __nv_bfloat16 lo = __float2bfloat16_rn(r - __bfloat162float(mid));
+      w[0][e] = __bfloat16_as_ushort(h);
+      w[1][e] = __bfloat16_as_ushort(mid);
+      w[2][e] = __bfloat16_as_ushort(lo);
+    }
+    a[i] = w[0][0] | (w[0][1] << 16);
+    b[i] = w[1][0] | (w[1][1] << 16);
+    c[i] = w[2][0] | (w[2][1] << 16);
+  }
+  p0 = make_uint4(a[0], a[1], a[2], a[3]);
+  p1 = make_uint4(b[0], b[1], b[2], b[3]);
+  p2 = make_uint4(c[0], c[1], c[2], c[3]);
+}
+
 // element offset of (row, k) in a [R/8][Kp/8][8][8] core-matrix tile
 __device__ __forceinline__ int cm_offset(int row, int kc, int KC) { return (((row >> 3) * KC + kc) << 6) + ((row & 7) << 3); }
 

@@ -1,9 +1,10 @@
-"""Tensor-core (tcgen05, BF16x3) Legendre contraction against numpy FP64.
+"""Tensor-core (tcgen05, BF16x3 and BF16x6) Legendre contraction against numpy FP64.
 
-The split-precision product A B^T ~ A_hi B_hi^T + A_hi B_lo^T + A_lo B_hi^T
+The split-precision product A B^T ~ A0 B0^T + A0 B1^T + A1 B0^T (BF16x3)
 keeps about 16 significant bits per operand, so every element must satisfy
-|D - D_exact| <= 3e-5 * sum_k |A_k| |B_k|  (BF16x3 bound, FP32 accumulation);
-the FP32 CUDA-core kernel must satisfy the same with 1e-6.  Shapes cover the
+|D - D_exact| <= 3e-5 * sum_k |A_k| |B_k|  (BF16x3 bound, FP32 accumulation).
+BF16x6 adds A0 B2^T + A2 B0^T + A1 B1^T (the operands are split exactly into
+three bf16 parts), so it must meet the FP32 CUDA-core kernel's bound, 1e-6.  Shapes cover the
 coupling step's stages (J = N, 3 nD, 2 nO, nD; K = N, nD, nO) and ragged
 sizes that exercise the padding of J, K to multiples of 16 and partial
 128-row tiles.
@@ -45,6 +46,18 @@ def test_tensor_core_contraction(cuda, shape):
     assert np.median(err) <= 2e-6
 
 
+@pytest.mark.parametrize("shape", SHAPES)
+def test_tensor_core_six_products(cuda, shape):
+    A, B, exact, scale = _case(*shape, seed=11 + sum(shape))
+    D6 = run_legendre(A, B, tensor_cores=True, terms=6)
+    D3 = run_legendre(A, B, tensor_cores=True, terms=3)
+    e6 = np.abs(D6 - exact) / scale
+    e3 = np.abs(D3 - exact) / scale
+    assert e6.max() <= 1e-6, e6.max()
+    # the three extra products are not a no-op: the median error drops by >= 8x
+    assert np.median(e6) * 8 <= np.median(e3)
+
+
 @pytest.mark.parametrize("shape", SHAPES[:3])
 def test_cuda_core_contraction(cuda, shape):
     A, B, exact, scale = _case(*shape, seed=7 + sum(shape))
@@ -61,5 +74,6 @@ def test_triangular_synthesis(cuda):
         B[m, :, :m] = 0.0
     exact = np.einsum("mqk,mjk->mqj", A.astype(np.float64), B)
     scale = np.einsum("mqk,mjk->mqj", np.abs(A.astype(np.float64)), np.abs(B)) + 1e-300
-    D = run_legendre(A, B, tensor_cores=True, tri=True)
-    assert (np.abs(D - exact) / scale).max() <= 3e-5
+    for terms, tol in ((3, 3e-5), (6, 1e-6)):
+        D = run_legendre(A, B, tensor_cores=True, tri=True, terms=terms)
+        assert (np.abs(D - exact) / scale).max() <= tol
