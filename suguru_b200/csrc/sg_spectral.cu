@@ -282,10 +282,98 @@ __device__ __forceinline__ void mechanics(const Geo<T>& G, const T* A, const T (
 }
 
 // ------------------------------------------------- membrane pointwise -----
+// Staged Legendre output of one dealias row: for each m, the 18 values
+// (ccs = 2c + cos/sin, kind = P, dP, d2P) at k = 3 ccs + kind, padded to 20 so
+// that a thread reads them with 16-byte loads.
+constexpr int kGK = 20;
+
+// The 15 basis sums of one point's longitude synthesis (per component c:
+// v1, v2, v11, v12, v22 of cal_co_tang_basis2) for one m, accumulated into acc.
+template <class T>
+__device__ __forceinline__ void synth_m(const T* g, T cm, T sm, T fm, T (&acc)[5][3]) {
+  T v[18];
+  if constexpr (sizeof(T) == 4) {
+#pragma unroll
+    for (int q = 0; q < 4; ++q) {
+      const float4 x = ((const float4*)g)[q];
+      v[4 * q] = x.x; v[4 * q + 1] = x.y; v[4 * q + 2] = x.z; v[4 * q + 3] = x.w;
+    }
+    const float2 x = ((const float2*)g)[8];
+    v[16] = x.x; v[17] = x.y;
+  } else {
+#pragma unroll
+    for (int q = 0; q < 9; ++q) {
+      const double2 x = ((const double2*)g)[q];
+      v[2 * q] = x.x; v[2 * q + 1] = x.y;
+    }
+  }
+#pragma unroll
+  for (int c = 0; c < 3; ++c) {
+    const T P_a = v[6 * c + 0], D_a = v[6 * c + 1], E_a = v[6 * c + 2];  // cos rows
+    const T P_b = v[6 * c + 3], D_b = v[6 * c + 4], E_b = v[6 * c + 5];  // sin rows
+    const T t0P = P_a * cm - P_b * sm;
+    const T t1P = fm * (P_a * (-sm) - P_b * cm);
+    acc[0][c] += D_a * cm - D_b * sm;             // vat1 = sum dP * parthe0
+    acc[1][c] += t1P;                             // vat2 = sum P * parthe1
+    acc[2][c] += E_a * cm - E_b * sm;             // deFvat1(:,1) = sum d2P * parthe0
+    acc[3][c] += fm * (D_a * (-sm) - D_b * cm);   // deFvat1(:,2) = sum dP * parthe1
+    acc[4][c] += -fm * fm * t0P;                  // deFvat2(:,2) = sum P * parthe2
+  }
+}
+
+// Geometry and Skalak force of one point from its synthesised sums v (the
+// perturbation part) and the reference sphere at (st, ct, cp, sp).
+template <class T>
+__device__ __forceinline__ void point_force(const T (&v)[5][3], T st, T ct, T cp, T sp, T R, T hf, T csk,
+                                            bool normals_only, T* f, T* nrm) {
+  Geo<T> Gm;
+  // reference sphere: a1 = x_t, a2 = x_p and second derivatives (sph.f90:84-86)
+  Gm.a1[0] = R * (ct * sp); Gm.a1[1] = R * (ct * cp); Gm.a1[2] = -R * st;
+  Gm.a2[0] = R * (st * cp); Gm.a2[1] = -R * (st * sp); Gm.a2[2] = T(0);
+  Gm.d11[0] = -R * (st * sp); Gm.d11[1] = -R * (st * cp); Gm.d11[2] = -R * ct;
+  Gm.d12[0] = R * (ct * cp); Gm.d12[1] = -R * (ct * sp); Gm.d12[2] = T(0);
+  Gm.d22[0] = -R * (st * sp); Gm.d22[1] = -R * (st * cp); Gm.d22[2] = T(0);
+#pragma unroll
+  for (int c = 0; c < 3; ++c) {
+    Gm.a1[c] += v[0][c];
+    Gm.a2[c] += v[1][c];
+    Gm.d11[c] += v[2][c];
+    Gm.d12[c] += v[3][c];
+    Gm.d22[c] += v[4][c];
+  }
+  f[0] = f[1] = f[2] = T(0);
+  if (normals_only) {
+    T cc[3];
+    cross3(Gm.a1, Gm.a2, cc);  // sph1.f90:611-651
+    const T sm = sqrt(cc[0] * cc[0] + cc[1] * cc[1] + cc[2] * cc[2]);
+    for (int c = 0; c < 3; ++c) Gm.n[c] = fdiv(cc[c], sm);
+  } else {
+    geometry<T>(Gm);
+    // reference contravariant metric of the sphere: A^11 = 1/R^2,
+    // A^22 = 1/(R^2 sin^2 t), d/dt A^22 = -2 cos t / (R^2 sin^3 t)
+    const T iR2 = fdiv(T(1), R * R);
+    T A[3] = {iR2, fdiv(iR2, st * st), T(0)};
+    T Ad[2][3] = {{T(0), fdiv(-T(2) * ct * iR2, st * st * st), T(0)}, {T(0), T(0), T(0)}};
+    mechanics<T>(Gm, A, Ad, hf, csk, f);
+  }
+  nrm[0] = Gm.n[0];
+  nrm[1] = Gm.n[1];
+  nrm[2] = Gm.n[2];
+}
+
 // One block per item of `nrows` dealias rows of one capsule.  Synthesises the
 // 15 basis fields of cal_co_tang_basis2 (sph3.f90:111-134) from the Legendre
 // output G, adds the reference sphere's analytic part, evaluates geometry and
 // mechanics, and takes the forward DFT of force and normal.
+//
+// Half-turn symmetry of the longitude grid (mD = 4N points, phi_{j+mD/2} =
+// phi_j + pi): cos and sin of m (phi + pi) are (-1)^m times those of m phi, so
+// a thread sums the even-m and odd-m terms of every series separately and gets
+// the point j from their sum and the point j + mD/2 from their difference --
+// two points for the loads and multiplies of one.  The forward DFT folds the
+// same way: the coefficient of an even (odd) m is the sum over j < mD/2 of
+// the sum (difference) of the outputs at j and j + mD/2.
+//
 // Capsules whose force comes from the surrogate (sur_flag[cap] != 0) need only
 // the normal here: their force rows are written as zeros and replaced after
 // the force analysis.
@@ -294,128 +382,95 @@ __global__ void __launch_bounds__(256, sizeof(T) == 4 ? 3 : 2) membrane_kernel(c
                                                        const CapInfo* __restrict__ caps,
                                                        const GroupDev* __restrict__ groups,
                                                        const int* __restrict__ sur_flag, int* __restrict__ err) {
+  (void)err;
   extern __shared__ __align__(16) unsigned char smem_raw[];
-  __shared__ __align__(8) uint64_t s_bar;
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5, nwarp = blockDim.x >> 5;
-  if (tid == 0) umma::mbar_init(&s_bar, 1);
-  __syncthreads();
-  uint32_t phase = 0;
   for (int w = blockIdx.x; w < nwork; w += gridDim.x) {
     const RowWork it = work[w];
     const CapInfo ci = caps[it.cap];
     const T hf = (T)(0.5 * ci.gs), csk = (T)ci.csk;  // hf_gscell = 0.5 gscell (sph.f90:35)
     const bool normals_only = sur_flag && sur_flag[it.cap];
     const GroupDev gd = groups[it.group];
-    const int N = gd.N, nD = gd.nD, mD = gd.mD;
-    const int RP = blockDim.x / mD > 0 ? blockDim.x / mD : 1;
-    const int nG = 6 * N * 3 * nD;         // the capsule's Legendre output block [ccs][m][kind][lat]
-    T* sG = (T*)smem_raw;                  // [nG]
-    T* sTrig = sG + nG;                    // [2][N][mD+1]
-    T* sOut = sTrig + 2 * N * (mD + 1);    // [RP][6][mD+1]
-    const T* G = (const T*)gd.buf.G + (long long)ci.gidx * nG;
+    const int N = gd.N, nD = gd.nD, mD = gd.mD, H = mD >> 1;
+    const int RP = (int)blockDim.x / H > 0 ? (int)blockDim.x / H : 1;  // rows per chunk, H threads each
+    const int SR = N * kGK + 16 / (int)sizeof(T);  // staged row stride (one 16-byte pad: fewer bank conflicts)
+    T* sG = (T*)smem_raw;                  // [RP][SR]
+    T* sTrig = sG + RP * SR;               // [2N][H+1]: cos m phi_j (rows m), sin m phi_j (rows N+m), j < H
+    T* sOut = sTrig + 2 * N * (H + 1);     // [RP][6][2H+2]: sum over the half turn at [j], difference at [H+1+j]
+    const T* G = (const T*)gd.buf.G + (long long)ci.gidx * (18 * N * nD);  // [ccs][m][kind][lat]
     const T* trig = (const T*)gd.trigD[pidx<T>()];
     const T* lat = (const T*)gd.latD[pidx<T>()];
     T* Fout = (T*)gd.buf.Fout + (long long)ci.gidx * 12 * N * nD;
     const T sfn = T(2) / T(mD);
-    __syncthreads();  // the previous capsule's reads of shared memory are done
-    if (tid == 0) {   // one bulk copy of the whole block (contiguous, 16-byte multiple)
-      umma::fence_async_smem();
-      umma::bulk_g2s(sG, G, (uint32_t)(sizeof(T) * nG), &s_bar);
-    }
-    for (int hm = warp; hm < 2 * N; hm += nwarp)
-      for (int j = lane; j < mD; j += 32) sTrig[hm * (mD + 1) + j] = trig[hm * mD + j];
-    const int got = umma::mbar_wait(&s_bar, phase) ? 1 : 0;
-    phase ^= 1u;
-    if (!__syncthreads_and(got)) {
-      if (tid == 0) atomicExch(err, 1);
-      return;
+    const T R = (T)ci.R;
+    __syncthreads();  // the previous item's reads of shared memory are done
+    for (int q = tid; q < 2 * N * H; q += blockDim.x) {
+      const int hm = q / H, j = q - hm * H;
+      sTrig[hm * (H + 1) + j] = trig[hm * mD + j];
     }
     for (int rb = it.row0; rb < it.row0 + it.nrows; rb += RP) {
       const int rows = min(RP, it.row0 + it.nrows - rb);
+      __syncthreads();  // the previous chunk's staged rows and outputs are consumed
+      // stage the chunk's rows, transposed to [row][m][3 ccs + kind]; a warp
+      // reads runs of `rows` consecutive latitudes of one (ccs, m, kind)
+      for (int q = tid; q < 18 * N * rows; q += blockDim.x) {
+        const int e = q / rows, r = q - e * rows;  // e = (ccs N + m) 3 + kind
+        const int kind = e % 3, cm_ = e / 3, m = cm_ % N, ccs = cm_ / N;
+        sG[r * SR + m * kGK + 3 * ccs + kind] = G[(long long)e * nD + rb + r];
+      }
       __syncthreads();
-  {
-    const int r = tid / mD, j = tid - (tid / mD) * mD;
-    if (r < rows) {
-    const int i = rb + r;
-    const T st = lat[4 * i], ct = lat[4 * i + 1];
-    const T R = (T)ci.R;
-    const T cp = sTrig[1 * (mD + 1) + j], sp = sTrig[(N + 1) * (mD + 1) + j];
-    Geo<T> Gm;
-    // reference sphere: a1 = x_t, a2 = x_p and second derivatives (sph.f90:84-86)
-    Gm.a1[0] = R * (ct * sp); Gm.a1[1] = R * (ct * cp); Gm.a1[2] = -R * st;
-    Gm.a2[0] = R * (st * cp); Gm.a2[1] = -R * (st * sp); Gm.a2[2] = T(0);
-    Gm.d11[0] = -R * (st * sp); Gm.d11[1] = -R * (st * cp); Gm.d11[2] = -R * ct;
-    Gm.d12[0] = R * (ct * cp); Gm.d12[1] = -R * (ct * sp); Gm.d12[2] = T(0);
-    Gm.d22[0] = -R * (st * sp); Gm.d22[1] = -R * (st * cp); Gm.d22[2] = T(0);
-    {
-      // block element (ccs, m, kind, lat) at ((ccs N + m) 3 + kind) nD + lat;
-      // m outermost so that each trig pair is read once for the three
-      // components (the order of the sums per component is unchanged)
-      T v1[3] = {T(0), T(0), T(0)}, v2[3] = {T(0), T(0), T(0)}, v11[3] = {T(0), T(0), T(0)};
-      T v12[3] = {T(0), T(0), T(0)}, v22[3] = {T(0), T(0), T(0)};
-      const T* g = sG + i;
-      for (int m = 0; m < N; ++m) {
-        const T cm = sTrig[m * (mD + 1) + j], sm = sTrig[(N + m) * (mD + 1) + j];
-        const T fm = (T)m;
+      {
+        const int r = tid / H, j = tid - (tid / H) * H;
+        if (r < rows) {
+          const int i = rb + r;
+          T ev[5][3], od[5][3];
 #pragma unroll
-        for (int c = 0; c < 3; ++c) {
-          const T* gc = g + ((long long)((c * 2 + 0) * N + m) * 3) * nD;  // cos rows
-          const T* gs = g + ((long long)((c * 2 + 1) * N + m) * 3) * nD;  // sin rows
-          const T P_a = gc[0], P_b = gs[0];
-          const T D_a = gc[nD], D_b = gs[nD];
-          const T E_a = gc[2 * nD], E_b = gs[2 * nD];
-          const T t0P = P_a * cm - P_b * sm;
-          const T t1P = fm * (P_a * (-sm) - P_b * cm);
-          v1[c] += D_a * cm - D_b * sm;               // vat1 = sum dP * parthe0
-          v2[c] += t1P;                               // vat2 = sum P * parthe1
-          v11[c] += E_a * cm - E_b * sm;              // deFvat1(:,1) = sum d2P * parthe0
-          v12[c] += fm * (D_a * (-sm) - D_b * cm);    // deFvat1(:,2) = sum dP * parthe1
-          v22[c] += -fm * fm * t0P;                   // deFvat2(:,2) = sum P * parthe2
+          for (int a = 0; a < 5; ++a)
+#pragma unroll
+            for (int c = 0; c < 3; ++c) ev[a][c] = od[a][c] = T(0);
+          const T* g = sG + r * SR;
+          for (int m = 0; m < N; m += 2) {
+            synth_m<T>(g + m * kGK, sTrig[m * (H + 1) + j], sTrig[(N + m) * (H + 1) + j], (T)m, ev);
+            if (m + 1 < N)
+              synth_m<T>(g + (m + 1) * kGK, sTrig[(m + 1) * (H + 1) + j], sTrig[(N + m + 1) * (H + 1) + j],
+                         (T)(m + 1), od);
+          }
+          // point j = even + odd, point j + mD/2 = even - odd
+#pragma unroll
+          for (int a = 0; a < 5; ++a)
+#pragma unroll
+            for (int c = 0; c < 3; ++c) {
+              const T e = ev[a][c];
+              ev[a][c] = e + od[a][c];
+              od[a][c] = e - od[a][c];
+            }
+          const T st = lat[4 * i], ct = lat[4 * i + 1];
+          const T cp = sTrig[1 * (H + 1) + j], sp = sTrig[(N + 1) * (H + 1) + j];
+          T fa[3], na[3], fb[3], nb[3];
+          point_force<T>(ev, st, ct, cp, sp, R, hf, csk, normals_only, fa, na);
+          point_force<T>(od, st, ct, -cp, -sp, R, hf, csk, normals_only, fb, nb);
+          T* o = sOut + r * 6 * (2 * H + 2);
+          const T va[6] = {fa[0], fa[1], fa[2], na[0], na[1], na[2]};
+          const T vb[6] = {fb[0], fb[1], fb[2], nb[0], nb[1], nb[2]};
+#pragma unroll
+          for (int f = 0; f < 6; ++f) {
+            o[f * (2 * H + 2) + j] = va[f] + vb[f];
+            o[f * (2 * H + 2) + H + 1 + j] = va[f] - vb[f];
+          }
         }
       }
-#pragma unroll
-      for (int c = 0; c < 3; ++c) {
-        Gm.a1[c] += v1[c];
-        Gm.a2[c] += v2[c];
-        Gm.d11[c] += v11[c];
-        Gm.d12[c] += v12[c];
-        Gm.d22[c] += v22[c];
-      }
-    }
-    T f[3] = {T(0), T(0), T(0)};
-    if (normals_only) {
-      T cc[3];
-      cross3(Gm.a1, Gm.a2, cc);  // sph1.f90:611-651
-      const T sm = sqrt(cc[0] * cc[0] + cc[1] * cc[1] + cc[2] * cc[2]);
-      for (int c = 0; c < 3; ++c) Gm.n[c] = fdiv(cc[c], sm);
-    } else {
-      geometry<T>(Gm);
-      // reference contravariant metric of the sphere: A^11 = 1/R^2,
-      // A^22 = 1/(R^2 sin^2 t), d/dt A^22 = -2 cos t / (R^2 sin^3 t)
-      const T iR2 = fdiv(T(1), R * R);
-      T A[3] = {iR2, fdiv(iR2, st * st), T(0)};
-      T Ad[2][3] = {{T(0), fdiv(-T(2) * ct * iR2, st * st * st), T(0)}, {T(0), T(0), T(0)}};
-      mechanics<T>(Gm, A, Ad, hf, csk, f);
-    }
-    T* o = sOut + r * 6 * (mD + 1);
-    o[0 * (mD + 1) + j] = f[0];
-    o[1 * (mD + 1) + j] = f[1];
-    o[2 * (mD + 1) + j] = f[2];
-    o[3 * (mD + 1) + j] = Gm.n[0];
-    o[4 * (mD + 1) + j] = Gm.n[1];
-    o[5 * (mD + 1) + j] = Gm.n[2];
-  }
-    }
       __syncthreads();
       // forward DFT of the six outputs (force, normal) per row: warp =
       // (row, field) line, lane p < 2N = trig row p (cos m = p, sin m = p - N)
       for (int line = warp; line < rows * 6; line += nwarp) {
         const int f = line % 6, rr = line / 6;
-        const T* o = sOut + (rr * 6 + f) * (mD + 1);
+        const T* o = sOut + line * (2 * H + 2);
         for (int p = lane; p < 2 * N; p += 32) {
-          const T* t = sTrig + p * (mD + 1);
+          const int m = p < N ? p : p - N;
+          const T* oo = o + ((m & 1) ? H + 1 : 0);
+          const T* t = sTrig + p * (H + 1);
           T a = 0;
-          for (int jj = 0; jj < mD; ++jj) a += o[jj] * t[jj];
+          for (int jj = 0; jj < H; ++jj) a += oo[jj] * t[jj];
           Fout[((long long)f * 2 * N + p) * nD + rb + rr] = (p < N ? sfn : -sfn) * a;
         }
       }
@@ -616,7 +671,16 @@ size_t pointwise_smem(int kind, int nmax) {
   size_t e = 0;
   switch (kind) {
     case kPosfwd: e = 2 * N * (4 * N + 1) + 3 * (size_t)(kPointThreads + kPointThreads / 8) + 64; break;
-    case kMembrane: e = 36 * N * N + 2 * N * (4 * N + 1) + chunk; break;
+    case kMembrane:
+      // staged rows RP (n kGK + pad) with RP = max(1, 256 / 2n), the half-turn
+      // trig table 2n (2n + 1), outputs RP 6 (4n + 2): the largest over the
+      // degrees n <= N (smaller degrees stage more rows per chunk)
+      for (size_t n = 1; n <= N; ++n) {
+        const size_t RP = kPointThreads / (2 * n) > 0 ? kPointThreads / (2 * n) : 1;
+        const size_t en = RP * (n * kGK + 16 / sizeof(T)) + 2 * n * (2 * n + 1) + RP * 6 * (4 * n + 2) + 64;
+        if (en > e) e = en;
+      }
+      break;
     case kShgrid: e = 24 * N * N + 2 * N * (2 * N + 1) + chunk; break;
     default: e = 28 * N * N + 8 * N * N; break;
   }
