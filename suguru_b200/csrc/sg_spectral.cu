@@ -75,12 +75,15 @@ __global__ void centroid_kernel(int ncap, const CapInfo* __restrict__ caps, cons
 }
 
 // ------------------------------------------------- positions -> Fourier ---
-// Persistent CTAs over capsules (work items of whole capsules); per capsule
-// the trig table is staged once, then rows are taken in chunks of
-// blockDim/mD: the displacement d = X - cen - R s(t_i, p_j) in FP64 (one
-// thread per point), then the real DFT of shagc (shagc.f:364-380: 2/nlon
-// scaling, forward transform carries -sin) for m < N, one warp per
-// (row, component) line with lane = m.
+// Persistent CTAs over capsule row ranges; per item the half-turn trig table
+// (j < mD/2) is staged once, then rows are taken in chunks of blockDim/(mD/2):
+// the displacement d = X - cen - R s(t_i, p_j) in FP64, one thread per pair of
+// points j and j + mD/2 (half a turn apart), stored as their sum and
+// difference; then the real DFT of shagc (shagc.f:364-380: 2/nlon scaling,
+// forward transform carries -sin) for m < N, one warp per (row, component)
+// line with lane = m: cos and sin of m (phi + pi) are (-1)^m those of m phi,
+// so an even m sums the pair sums and an odd m the pair differences over
+// j < mD/2.
 template <class T>
 __global__ void __launch_bounds__(256) posfwd_kernel(const RowWork* __restrict__ work, int nwork,
                                                      const CapInfo* __restrict__ caps,
@@ -93,51 +96,60 @@ __global__ void __launch_bounds__(256) posfwd_kernel(const RowWork* __restrict__
     const RowWork it = work[w];
     const CapInfo ci = caps[it.cap];
     const GroupDev gd = groups[it.group];
-    const int N = gd.N, nD = gd.nD, mD = gd.mD, mP = mD + 1;
-    const int RP = blockDim.x / mD > 0 ? blockDim.x / mD : 1;
-    T* sTrig = (T*)smem_raw;       // [2][N][mD+1]
-    T* sd = sTrig + 2 * N * mP;    // [RP][3][mD+1]
+    const int N = gd.N, nD = gd.nD, mD = gd.mD, H = mD >> 1, hP = H + 1, lP = 2 * H + 2;
+    const int RP = (int)blockDim.x / H > 0 ? (int)blockDim.x / H : 1;
+    T* sTrig = (T*)smem_raw;       // [2N][H+1]
+    T* sd = sTrig + 2 * N * hP;    // [RP][3][2H+2]: pair sums at [j], differences at [H+1+j]
     const double* lat64 = (const double*)gd.latD[0];
     const double* trig64 = (const double*)gd.trigD[0];
     const T* trig = (const T*)gd.trigD[pidx<T>()];
     const double R = ci.R;
     const double c0 = cen[3 * it.cap], c1 = cen[3 * it.cap + 1], c2 = cen[3 * it.cap + 2];
     T* Fpos = (T*)gd.buf.Fpos + (long long)ci.gidx * 6 * N * nD;
-    __syncthreads();  // the previous capsule's reads of shared memory are done
-    for (int hm = warp; hm < 2 * N; hm += nwarp)
-      for (int j = lane; j < mD; j += 32) sTrig[hm * mP + j] = trig[hm * mD + j];
+    __syncthreads();  // the previous item's reads of shared memory are done
+    for (int q = tid; q < 2 * N * H; q += blockDim.x) {
+      const int hm = q / H, j = q - hm * H;
+      sTrig[hm * hP + j] = trig[hm * mD + j];
+    }
     for (int rb = it.row0; rb < it.row0 + it.nrows; rb += RP) {
       const int rows = min(RP, it.row0 + it.nrows - rb);
       __syncthreads();
       {
-        const int r = tid / mD, j = tid - (tid / mD) * mD;
+        const int r = tid / H, j = tid - (tid / H) * H;
         if (r < rows) {
           const int i = rb + r;
           const double st = lat64[4 * i], ct = lat64[4 * i + 1];
           const long long p = ci.pt_off + (long long)i * mD + j;
+          // the point half a turn on has cos p, sin p of opposite sign
           const double cp = trig64[1 * mD + j], sp = trig64[N * mD + 1 * mD + j];
-          T* o = sd + r * 3 * mP;
-          o[0 * mP + j] = (T)(X[p] - c0 - R * (st * sp));
-          o[1 * mP + j] = (T)(Y[p] - c1 - R * (st * cp));
-          o[2 * mP + j] = (T)(Z[p] - c2 - R * ct);
+          const T ax = (T)(X[p] - c0 - R * (st * sp)), bx = (T)(X[p + H] - c0 + R * (st * sp));
+          const T ay = (T)(Y[p] - c1 - R * (st * cp)), by = (T)(Y[p + H] - c1 + R * (st * cp));
+          const T az = (T)(Z[p] - c2 - R * ct), bz = (T)(Z[p + H] - c2 - R * ct);
+          T* o = sd + r * 3 * lP;
+          o[0 * lP + j] = ax + bx;
+          o[0 * lP + hP + j] = ax - bx;
+          o[1 * lP + j] = ay + by;
+          o[1 * lP + hP + j] = ay - by;
+          o[2 * lP + j] = az + bz;
+          o[2 * lP + hP + j] = az - bz;
         }
       }
       __syncthreads();
       const T sfn = T(2) / T(mD);
-      const long long rs = (long long)N * nD;  // (comp, cs) row stride
       // lane p < 2N: trig row p (cos m = p, then sin m = p - N); rows of
       // Fpos are (comp, cos/sin, m), so the output row is c 2N + p
       for (int line = warp; line < rows * 3; line += nwarp) {
         const int c = line % 3, r = line / 3;
-        const T* o = sd + (r * 3 + c) * mP;
+        const T* o = sd + (r * 3 + c) * lP;
         for (int p = lane; p < 2 * N; p += 32) {
-          const T* t = sTrig + p * mP;
+          const int m = p < N ? p : p - N;
+          const T* oo = o + ((m & 1) ? hP : 0);
+          const T* t = sTrig + p * hP;
           T a = 0;
-          for (int j = 0; j < mD; ++j) a += o[j] * t[j];
+          for (int j = 0; j < H; ++j) a += oo[j] * t[j];
           Fpos[(long long)(c * 2 * N + p) * nD + rb + r] = (p < N ? sfn : -sfn) * a;
         }
       }
-      (void)rs;
     }
   }
 }
@@ -482,89 +494,135 @@ __global__ void __launch_bounds__(256, sizeof(T) == 4 ? 3 : 2) membrane_kernel(c
 // cal_unitO_filter (sph1.f90:1378-1402): truncated normals on the SH grid,
 // renormalised; cal_surface_metric_sph__OPT (sph3.f90:186-277): |a1 x a2| on
 // the SH grid from the shape coefficients.  Then their forward DFT.
+// The SH grid has mO = 2N longitudes, so points j and j + N are half a turn
+// apart: one thread per pair, even-m and odd-m sums kept apart (as in the
+// membrane kernel), and the forward DFT folded over j < N.
+// Staged per (row, m): normal P cos/sin, shape P cos/sin, shape dP cos/sin of
+// component c at 6c + 0..5.
+constexpr int kSK = 20;
+
+template <class T>
+__device__ __forceinline__ void load18(const T* g, T (&v)[18]) {
+  if constexpr (sizeof(T) == 4) {
+#pragma unroll
+    for (int q = 0; q < 4; ++q) {
+      const float4 x = ((const float4*)g)[q];
+      v[4 * q] = x.x; v[4 * q + 1] = x.y; v[4 * q + 2] = x.z; v[4 * q + 3] = x.w;
+    }
+    const float2 x = ((const float2*)g)[8];
+    v[16] = x.x; v[17] = x.y;
+  } else {
+#pragma unroll
+    for (int q = 0; q < 9; ++q) {
+      const double2 x = ((const double2*)g)[q];
+      v[2 * q] = x.x; v[2 * q + 1] = x.y;
+    }
+  }
+}
+
 template <class T>
 __global__ void __launch_bounds__(256) shgrid_kernel(const RowWork* __restrict__ work, int nwork,
                                                      const CapInfo* __restrict__ caps,
                                                      const GroupDev* __restrict__ groups, int* __restrict__ err) {
+  (void)err;
   extern __shared__ __align__(16) unsigned char smem_raw[];
-  __shared__ __align__(8) uint64_t s_bar;
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5, nwarp = blockDim.x >> 5;
-  if (tid == 0) umma::mbar_init(&s_bar, 1);
-  __syncthreads();
-  uint32_t phase = 0;
   for (int w = blockIdx.x; w < nwork; w += gridDim.x) {
     const RowWork it = work[w];
     const CapInfo ci = caps[it.cap];
     const GroupDev gd = groups[it.group];
-    const int N = gd.N, nO = gd.nO, mO = gd.mO;
-    const int RP = blockDim.x / mO > 0 ? blockDim.x / mO : 1;
-    const int nG = 12 * N * 2 * nO;       // the capsule's block [rr][m][kind][lat]
-    T* sG = (T*)smem_raw;                 // [nG]
-    T* sTrig = sG + nG;                   // [2][N][mO+1]
-    T* sOut = sTrig + 2 * N * (mO + 1);   // [RP][4][mO+1]
-    const T* GO = (const T*)gd.buf.GO + (long long)ci.gidx * nG;
+    const int N = gd.N, nO = gd.nO, mO = gd.mO, H = mO >> 1, hP = H + 1, lP = 2 * H + 2;
+    const int RP = (int)blockDim.x / H > 0 ? (int)blockDim.x / H : 1;
+    const int SR = N * kSK + 16 / (int)sizeof(T);
+    T* sG = (T*)smem_raw;                 // [RP][SR]
+    T* sTrig = sG + RP * SR;              // [2N][H+1]
+    T* sOut = sTrig + 2 * N * hP;         // [RP][4][2H+2]
+    const T* GO = (const T*)gd.buf.GO + (long long)ci.gidx * (24 * N * nO);  // [rr][m][kind][lat]
     const T* trig = (const T*)gd.trigO[pidx<T>()];
     const T* lat = (const T*)gd.latO[pidx<T>()];
     T* Fsh = (T*)gd.buf.Fsh + (long long)ci.gidx * 8 * N * nO;
     const T sfn = T(2) / T(mO);
     const T R = (T)ci.R;
-    __syncthreads();  // the previous capsule's reads of shared memory are done
-    if (tid == 0) {
-      umma::fence_async_smem();
-      umma::bulk_g2s(sG, GO, (uint32_t)(sizeof(T) * nG), &s_bar);
-    }
-    for (int hm = warp; hm < 2 * N; hm += nwarp)
-      for (int j = lane; j < mO; j += 32) sTrig[hm * (mO + 1) + j] = trig[hm * mO + j];
-    const int got = umma::mbar_wait(&s_bar, phase) ? 1 : 0;
-    phase ^= 1u;
-    if (!__syncthreads_and(got)) {
-      if (tid == 0) atomicExch(err, 1);
-      return;
+    __syncthreads();  // the previous item's reads of shared memory are done
+    for (int q = tid; q < 2 * N * H; q += blockDim.x) {
+      const int hm = q / H, j = q - hm * H;
+      sTrig[hm * hP + j] = trig[hm * mO + j];
     }
     for (int rb = it.row0; rb < it.row0 + it.nrows; rb += RP) {
       const int rows = min(RP, it.row0 + it.nrows - rb);
       __syncthreads();
-      const int r = tid / mO, j = tid - (tid / mO) * mO;
+      // stage: e = (s, c, cs, m) with s = 0 normal P (rr = 2c+cs, kind 0),
+      // s = 1 shape P (rr = 2(3+c)+cs, kind 0), s = 2 shape dP (kind 1)
+      for (int q = tid; q < 18 * N * rows; q += blockDim.x) {
+        const int e = q / rows, r = q - e * rows;
+        const int m = e % N, t = e / N, cs = t & 1, c = (t >> 1) % 3, sk = t / 6;
+        const int rr = sk == 0 ? 2 * c + cs : 2 * (3 + c) + cs, kind = sk == 2 ? 1 : 0;
+        sG[r * SR + m * kSK + 6 * c + 2 * sk + cs] = GO[(long long)((rr * N + m) * 2 + kind) * nO + rb + r];
+      }
+      __syncthreads();
+      const int r = tid / H, j = tid - (tid / H) * H;
       if (r < rows) {
         const int i = rb + r;
         const T st = lat[4 * i], ct = lat[4 * i + 1];
-        const T cp = sTrig[1 * (mO + 1) + j], sp = sTrig[(N + 1) * (mO + 1) + j];
-        // block element (rr, m, kind, lat) at ((rr N + m) 2 + kind) nO + lat
-        T nv[3], a1[3] = {R * (ct * sp), R * (ct * cp), -R * st}, a2[3] = {R * (st * cp), -R * (st * sp), T(0)};
-        for (int c = 0; c < 3; ++c) {
-          const T* nc = sG + (long long)(c * 2 + 0) * N * 2 * nO + i;  // normal comp c, cos
-          const T* ns = sG + (long long)(c * 2 + 1) * N * 2 * nO + i;
-          const T* xc = sG + (long long)((3 + c) * 2 + 0) * N * 2 * nO + i;  // shape comp c, cos
-          const T* xs = sG + (long long)((3 + c) * 2 + 1) * N * 2 * nO + i;
-          T vn = 0, v1 = 0, v2 = 0;
-          for (int m = 0; m < N; ++m) {
-            const T cm = sTrig[m * (mO + 1) + j], sm = sTrig[(N + m) * (mO + 1) + j];
-            const int o = m * 2 * nO;  // kind P at +0, dP at +nO
-            vn += nc[o] * cm - ns[o] * sm;
-            v1 += xc[o + nO] * cm - xs[o + nO] * sm;
-            v2 += (T)m * (xc[o] * (-sm) - xs[o] * cm);
+        T ev[3][3], od[3][3];  // [normal, a1 part, a2 part][c]
+#pragma unroll
+        for (int a2 = 0; a2 < 3; ++a2)
+#pragma unroll
+          for (int c = 0; c < 3; ++c) ev[a2][c] = od[a2][c] = T(0);
+        const T* g = sG + r * SR;
+        auto term = [&](int m, T(&acc)[3][3]) {
+          const T cm = sTrig[m * hP + j], sm = sTrig[(N + m) * hP + j];
+          T v[18];
+          load18<T>(g + m * kSK, v);
+#pragma unroll
+          for (int c = 0; c < 3; ++c) {
+            acc[0][c] += v[6 * c + 0] * cm - v[6 * c + 1] * sm;
+            acc[1][c] += v[6 * c + 4] * cm - v[6 * c + 5] * sm;
+            acc[2][c] += (T)m * (v[6 * c + 2] * (-sm) - v[6 * c + 3] * cm);
           }
-          nv[c] = vn;
-          a1[c] += v1;
-          a2[c] += v2;
+        };
+        for (int m = 0; m < N; m += 2) {
+          term(m, ev);
+          if (m + 1 < N) term(m + 1, od);
         }
-        const T rn = sqrt(nv[0] * nv[0] + nv[1] * nv[1] + nv[2] * nv[2]);
-        T cc[3];
-        cross3(a1, a2, cc);
-        T* o = sOut + r * 4 * (mO + 1);
-        o[0 * (mO + 1) + j] = fdiv(nv[0], rn);
-        o[1 * (mO + 1) + j] = fdiv(nv[1], rn);
-        o[2 * (mO + 1) + j] = fdiv(nv[2], rn);
-        o[3 * (mO + 1) + j] = sqrt(cc[0] * cc[0] + cc[1] * cc[1] + cc[2] * cc[2]);
+        const T cp = sTrig[1 * hP + j], sp = sTrig[(N + 1) * hP + j];
+        T out[2][4];
+#pragma unroll
+        for (int h = 0; h < 2; ++h) {  // h = 1: half a turn on (cos p, sin p change sign)
+          const T sg = h ? T(-1) : T(1);
+          T nv[3], a1[3] = {R * (ct * (sg * sp)), R * (ct * (sg * cp)), -R * st},
+                   a2[3] = {R * (st * (sg * cp)), -R * (st * (sg * sp)), T(0)};
+#pragma unroll
+          for (int c = 0; c < 3; ++c) {
+            nv[c] = h ? ev[0][c] - od[0][c] : ev[0][c] + od[0][c];
+            a1[c] += h ? ev[1][c] - od[1][c] : ev[1][c] + od[1][c];
+            a2[c] += h ? ev[2][c] - od[2][c] : ev[2][c] + od[2][c];
+          }
+          const T rn = sqrt(nv[0] * nv[0] + nv[1] * nv[1] + nv[2] * nv[2]);
+          T cc[3];
+          cross3(a1, a2, cc);
+          out[h][0] = fdiv(nv[0], rn);
+          out[h][1] = fdiv(nv[1], rn);
+          out[h][2] = fdiv(nv[2], rn);
+          out[h][3] = sqrt(cc[0] * cc[0] + cc[1] * cc[1] + cc[2] * cc[2]);
+        }
+        T* o = sOut + r * 4 * lP;
+#pragma unroll
+        for (int f = 0; f < 4; ++f) {
+          o[f * lP + j] = out[0][f] + out[1][f];
+          o[f * lP + hP + j] = out[0][f] - out[1][f];
+        }
       }
       __syncthreads();
       for (int line = warp; line < rows * 4; line += nwarp) {
         const int f = line % 4, rr = line / 4;
-        const T* o = sOut + (rr * 4 + f) * (mO + 1);
+        const T* o = sOut + line * lP;
         for (int p = lane; p < 2 * N; p += 32) {
-          const T* t = sTrig + p * (mO + 1);
+          const int m = p < N ? p : p - N;
+          const T* oo = o + ((m & 1) ? hP : 0);
+          const T* t = sTrig + p * hP;
           T a = 0;
-          for (int jj = 0; jj < mO; ++jj) a += o[jj] * t[jj];
+          for (int jj = 0; jj < H; ++jj) a += oo[jj] * t[jj];
           Fsh[((long long)f * 2 * N + p) * nO + rb + rr] = (p < N ? sfn : -sfn) * a;
         }
       }
@@ -575,6 +633,11 @@ __global__ void __launch_bounds__(256) shgrid_kernel(const RowWork* __restrict__
 // ------------------------------------------------- final synthesis --------
 // TRSSPH SH grid -> force grid of force, normals and surface metric
 // (forcing.f90:67-88), area = surfmetDf * wgtdsinf (forcing.f90:91).
+// One thread per pair of points half a turn apart (j, j + mD/2), even-m and
+// odd-m sums kept apart; the chunk's rows of the Legendre output are staged
+// transposed to [row][m][2f + cos/sin] (14 values, padded to 16).
+constexpr int kFK = 16;
+
 template <class T>
 __global__ void __launch_bounds__(256) final_kernel(const RowWork* __restrict__ work, int nwork,
                                                     const CapInfo* __restrict__ caps,
@@ -582,57 +645,82 @@ __global__ void __launch_bounds__(256) final_kernel(const RowWork* __restrict__ 
                                                     T* __restrict__ FY, T* __restrict__ FZ, T* __restrict__ NX,
                                                     T* __restrict__ NY, T* __restrict__ NZ, T* __restrict__ AREA,
                                                     int* __restrict__ err) {
+  (void)err;
   extern __shared__ __align__(16) unsigned char smem_raw[];
-  __shared__ __align__(8) uint64_t s_bar;
   const int tid = threadIdx.x;
-  if (tid == 0) umma::mbar_init(&s_bar, 1);
-  __syncthreads();
-  uint32_t phase = 0;
   for (int w = blockIdx.x; w < nwork; w += gridDim.x) {
     const RowWork it = work[w];
     const CapInfo ci = caps[it.cap];
     const GroupDev gd = groups[it.group];
-    const int N = gd.N, nD = gd.nD, mD = gd.mD;
-    const int nG = 14 * N * nD;   // the capsule's block [rr][m][lat]
-    T* sG = (T*)smem_raw;         // [nG]
-    T* sTrig = sG + nG;           // [2][N][mD]
-    const T* GF = (const T*)gd.buf.GF + (long long)ci.gidx * nG;
+    const int N = gd.N, nD = gd.nD, mD = gd.mD, H = mD >> 1, hP = H + 1;
+    const int RP = (int)blockDim.x / H > 0 ? (int)blockDim.x / H : 1;
+    const int SR = N * kFK + 16 / (int)sizeof(T);
+    T* sG = (T*)smem_raw;         // [RP][SR]
+    T* sTrig = sG + RP * SR;      // [2N][H+1]
+    const T* GF = (const T*)gd.buf.GF + (long long)ci.gidx * (14 * N * nD);  // [rr][m][lat]
     const T* trig = (const T*)gd.trigD[pidx<T>()];
     const T* lat = (const T*)gd.latD[pidx<T>()];
-    __syncthreads();  // the previous capsule's reads of shared memory are done
-    if (tid == 0) {
-      umma::fence_async_smem();
-      umma::bulk_g2s(sG, GF, (uint32_t)(sizeof(T) * nG), &s_bar);
+    __syncthreads();  // the previous item's reads of shared memory are done
+    for (int q = tid; q < 2 * N * H; q += blockDim.x) {
+      const int hm = q / H, j = q - hm * H;
+      sTrig[hm * hP + j] = trig[hm * mD + j];
     }
-    for (int q = tid; q < 2 * N * mD; q += blockDim.x) sTrig[q] = trig[q];
-    const int got = umma::mbar_wait(&s_bar, phase) ? 1 : 0;
-    phase ^= 1u;
-    if (!__syncthreads_and(got)) {
-      if (tid == 0) atomicExch(err, 1);
-      return;
-    }
-    // one thread per point of the capsule, rows in order
-    for (int q = tid; q < it.nrows * mD; q += blockDim.x) {
-      const int r = q / mD, j = q - r * mD;
-      const int i = it.row0 + r;
-      // block element (rr, m, lat) at (rr N + m) nD + lat; m outermost so that
-      // each trig pair is read once for the seven fields (same order per field)
-      T v[7] = {T(0), T(0), T(0), T(0), T(0), T(0), T(0)};
-      const T* g = sG + i;
-      for (int m = 0; m < N; ++m) {
-        const T cm = sTrig[m * mD + j], sm = sTrig[N * mD + m * mD + j];
-#pragma unroll
-        for (int f = 0; f < 7; ++f)
-          v[f] += g[((2 * f) * N + m) * nD] * cm - g[((2 * f + 1) * N + m) * nD] * sm;
+    for (int rb = it.row0; rb < it.row0 + it.nrows; rb += RP) {
+      const int rows = min(RP, it.row0 + it.nrows - rb);
+      __syncthreads();
+      for (int q = tid; q < 14 * N * rows; q += blockDim.x) {
+        const int e = q / rows, r = q - e * rows;  // e = rr N + m
+        const int m = e % N, rr = e / N;
+        sG[r * SR + m * kFK + rr] = GF[(long long)e * nD + rb + r];
       }
-      const long long p = ci.pt_off + (long long)i * mD + j;
-      FX[p] = v[0];
-      FY[p] = v[1];
-      FZ[p] = v[2];
-      NX[p] = v[3];
-      NY[p] = v[4];
-      NZ[p] = v[5];
-      AREA[p] = v[6] * lat[4 * i + 2];
+      __syncthreads();
+      const int r = tid / H, j = tid - (tid / H) * H;
+      if (r < rows) {
+        const int i = rb + r;
+        T ev[7], od[7];
+#pragma unroll
+        for (int f = 0; f < 7; ++f) ev[f] = od[f] = T(0);
+        const T* g = sG + r * SR;
+        auto term = [&](int m, T(&acc)[7]) {
+          const T cm = sTrig[m * hP + j], sm = sTrig[(N + m) * hP + j];
+          T v[16];
+          if constexpr (sizeof(T) == 4) {
+#pragma unroll
+            for (int q = 0; q < 4; ++q) {
+              const float4 x = ((const float4*)(g + m * kFK))[q];
+              v[4 * q] = x.x; v[4 * q + 1] = x.y; v[4 * q + 2] = x.z; v[4 * q + 3] = x.w;
+            }
+          } else {
+#pragma unroll
+            for (int q = 0; q < 7; ++q) {
+              const double2 x = ((const double2*)(g + m * kFK))[q];
+              v[2 * q] = x.x; v[2 * q + 1] = x.y;
+            }
+          }
+#pragma unroll
+          for (int f = 0; f < 7; ++f) acc[f] += v[2 * f] * cm - v[2 * f + 1] * sm;
+        };
+        for (int m = 0; m < N; m += 2) {
+          term(m, ev);
+          if (m + 1 < N) term(m + 1, od);
+        }
+        const long long p = ci.pt_off + (long long)i * mD + j;
+        const T wa = lat[4 * i + 2];
+        FX[p] = ev[0] + od[0];
+        FY[p] = ev[1] + od[1];
+        FZ[p] = ev[2] + od[2];
+        NX[p] = ev[3] + od[3];
+        NY[p] = ev[4] + od[4];
+        NZ[p] = ev[5] + od[5];
+        AREA[p] = (ev[6] + od[6]) * wa;
+        FX[p + H] = ev[0] - od[0];
+        FY[p + H] = ev[1] - od[1];
+        FZ[p + H] = ev[2] - od[2];
+        NX[p + H] = ev[3] - od[3];
+        NY[p + H] = ev[4] - od[4];
+        NZ[p + H] = ev[5] - od[5];
+        AREA[p + H] = (ev[6] - od[6]) * wa;
+      }
     }
   }
 }
@@ -667,10 +755,18 @@ static int persistent_grid(K kernel, size_t smem, int nwork) {
 enum PointKernel { kPosfwd, kMembrane, kShgrid, kFinal };
 template <class T>
 size_t pointwise_smem(int kind, int nmax) {
-  const size_t N = nmax, chunk = 6 * (size_t)(kPointThreads + kPointThreads / 8) + 64;
+  const size_t N = nmax;
   size_t e = 0;
   switch (kind) {
-    case kPosfwd: e = 2 * N * (4 * N + 1) + 3 * (size_t)(kPointThreads + kPointThreads / 8) + 64; break;
+    case kPosfwd:
+      // half-turn trig table 2n (2n + 1) and RP = max(1, 256 / 2n) rows of
+      // 3 (4n + 2) pair sums and differences, largest over n <= N
+      for (size_t n = 1; n <= N; ++n) {
+        const size_t RP = kPointThreads / (2 * n) > 0 ? kPointThreads / (2 * n) : 1;
+        const size_t en = 2 * n * (2 * n + 1) + RP * 3 * (4 * n + 2) + 64;
+        if (en > e) e = en;
+      }
+      break;
     case kMembrane:
       // staged rows RP (n kGK + pad) with RP = max(1, 256 / 2n), the half-turn
       // trig table 2n (2n + 1), outputs RP 6 (4n + 2): the largest over the
@@ -681,8 +777,23 @@ size_t pointwise_smem(int kind, int nmax) {
         if (en > e) e = en;
       }
       break;
-    case kShgrid: e = 24 * N * N + 2 * N * (2 * N + 1) + chunk; break;
-    default: e = 28 * N * N + 8 * N * N; break;
+    case kShgrid:
+      // staged rows RP (n kSK + pad) with RP = max(1, 256 / n), trig 2n (n + 1),
+      // outputs RP 4 (2n + 2)
+      for (size_t n = 1; n <= N; ++n) {
+        const size_t RP = kPointThreads / n > 0 ? kPointThreads / n : 1;
+        const size_t en = RP * (n * kSK + 16 / sizeof(T)) + 2 * n * (n + 1) + RP * 4 * (2 * n + 2) + 64;
+        if (en > e) e = en;
+      }
+      break;
+    default:
+      // staged rows RP (n kFK + pad) with RP = max(1, 256 / 2n), trig 2n (2n + 1)
+      for (size_t n = 1; n <= N; ++n) {
+        const size_t RP = kPointThreads / (2 * n) > 0 ? kPointThreads / (2 * n) : 1;
+        const size_t en = RP * (n * kFK + 16 / sizeof(T)) + 2 * n * (2 * n + 1) + 64;
+        if (en > e) e = en;
+      }
+      break;
   }
   return sizeof(T) * e;
 }
