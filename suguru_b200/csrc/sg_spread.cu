@@ -15,11 +15,17 @@
 // is exact and associative, so the field is bitwise independent of the order
 // in which threads add (no floating-point atomics, deterministic run to run).
 //
-//  - FP32: one signed 32-bit word per cell and component.  The scale puts
-//    0.3 * sum over the tile's entries of max_c |f_c * area / dV| at 2^30;
-//    since every 3-D kernel weight is at most (2/3)^3 < 0.3, no cell sum can
-//    reach 2^31.  The fixed-point step is then 2^-31 of that bound, finer than
-//    FP32 rounding of the typical cell value.
+//  - FP32: one signed 32-bit word per cell and component.  The scale is the
+//    smaller of two powers of two: one that puts 0.3 * sum over the tile's
+//    entries of max_c |f_c * area / dV| below 2^30 (every 3-D kernel weight is
+//    at most (2/3)^3 < 0.3, so no cell sum can reach 2^31), and one that puts
+//    0.3 * the largest single max_c |f_c * area / dV| below 2^22, so that every
+//    contribution v satisfies |v| < 2^22.  Then one FMA, v + 1.5 * 2^23, rounds
+//    v to the nearest integer (ties to even) in the low mantissa bits of a
+//    float whose exponent is fixed, and the integer is its bit pattern minus
+//    that of 1.5 * 2^23 -- no conversion instruction per contribution.  The
+//    fixed-point step is 2^-22 of 0.3 times the largest contribution's force,
+//    below FP32 rounding of a typical cell value.
 //  - FP64: 64-bit fixed point (|sum| < 2^56 from the tile's largest
 //    contribution times its entry count) kept as three limbs of 19 bits, the
 //    lower two unsigned, so that the atomics stay native 32-bit adds; with at
@@ -36,6 +42,8 @@ namespace sg {
 
 namespace {
 
+constexpr float kMagic = 12582912.0f;          // 1.5 * 2^23
+constexpr int kMagicBits = 0x4B400000;          // its bit pattern
 constexpr int LB = 19;      // FP64 limb width
 constexpr int kOut = -(1 << 24);  // offset of a stencil node outside the tile
 constexpr int MAXC = 4096;  // FP64 contributions per pass: 19 + 12 <= 31 bits per limb
@@ -47,9 +55,6 @@ struct Fixed<float> {
   static constexpr int NW = 1;
   static constexpr int QB = 30;
   static constexpr int PASS = 1 << 30;
-  __device__ static __forceinline__ void add(unsigned int* base, int, float v) {
-    atomicAdd(base, (unsigned int)__float2int_rn(v));
-  }
 };
 template <>
 struct Fixed<double> {
@@ -92,7 +97,7 @@ __global__ void __launch_bounds__(256) spread_kernel(IBGrid g, const int* __rest
   // contributions falling outside the tile, so that the walk has no branches
   constexpr int NCP = NC + 32;
   __shared__ __align__(16) unsigned int acc[NW][3][NCP];
-  __shared__ T s_red[8];
+  __shared__ T s_red[2][8];
   long long tot[NT][3];
 #pragma unroll
   for (int r = 0; r < NT; ++r) tot[r][0] = tot[r][1] = tot[r][2] = 0;
@@ -108,29 +113,46 @@ __global__ void __launch_bounds__(256) spread_kernel(IBGrid g, const int* __rest
     for (int q = tid; q < NW * 3 * NCP / 4; q += 256) ((uint4*)&acc[0][0][0])[q] = make_uint4(0u, 0u, 0u, 0u);
     // ---- fixed-point scale: FP32 from the sum, FP64 from the maximum of
     // max_c |f_c * area / dV| over the tile's entries (fixed reduction order)
-    T red = T(0);
+    T red = T(0), rmax = T(0);
     for (int e = e0 + tid; e < e1; e += 256) {
       const int p = entries[e];
       const T s = fabs(AREA[p] * (T)g.dvi);
       const T m = fmax(fabs(FX[p]) * s, fmax(fabs(FY[p]) * s, fabs(FZ[p]) * s));
       red = F32 ? red + m : fmax(red, m);
+      rmax = fmax(rmax, m);
     }
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) {
       const T other = __shfl_xor_sync(0xffffffffu, red, o);
       red = F32 ? red + other : fmax(red, other);
+      rmax = fmax(rmax, __shfl_xor_sync(0xffffffffu, rmax, o));
     }
-    if (lane == 0) s_red[warp] = red;
+    if (lane == 0) {
+      s_red[0][warp] = red;
+      s_red[1][warp] = rmax;
+    }
     __syncthreads();
-    red = s_red[0];
+    red = s_red[0][0];
+    rmax = s_red[1][0];
 #pragma unroll
-    for (int q = 1; q < 8; ++q) red = F32 ? red + s_red[q] : fmax(red, s_red[q]);
+    for (int q = 1; q < 8; ++q) {
+      red = F32 ? red + s_red[0][q] : fmax(red, s_red[0][q]);
+      rmax = fmax(rmax, s_red[1][q]);
+    }
     int ex = 0;
     const double bound = F32 ? 0.3 * (double)red : (double)red * (double)(e1 - e0);
     if (bound > 0.0) frexp(bound, &ex);  // bound < 2^ex
     if (ex < -60) ex = -60;              // keeps the scale finite in float
-    const T scale = (T)ldexp(1.0, QB - ex);  // |sum| < 2^QB
-    iscale = (T)ldexp(1.0, ex - QB);
+    int sh = QB - ex;                    // |sum| < 2^QB
+    if constexpr (F32) {                 // and every single contribution below 2^22
+      int ex1 = 0;
+      const double b1 = 0.3 * (double)rmax;
+      if (b1 > 0.0) frexp(b1, &ex1);
+      if (ex1 < -60) ex1 = -60;
+      sh = min(sh, 22 - ex1);
+    }
+    const T scale = (T)ldexp(1.0, sh);
+    iscale = (T)ldexp(1.0, -sh);
 
     // ---- one point per thread, in passes of at most PASS entries
     for (int c0 = e0; c0 < e1; c0 += Fixed<T>::PASS) {
@@ -204,7 +226,14 @@ __global__ void __launch_bounds__(256) spread_kernel(IBGrid g, const int* __rest
               for (int ix = 0; ix < 3; ++ix) {
                 const int cell = cyz + ((c == 0) ? lcF[0][ix] : lcC[0][ix]);
                 const T wx = (c == 0) ? wF[0][ix] : wC[0][ix];
-                Fixed<T>::add(&acc[0][c][cell >= 0 ? cell : trash], 3 * NCP, pyz * wx);
+                // valid cells are below NC, the negative ones wrap above it
+                const unsigned slot = min((unsigned)cell, (unsigned)trash);
+                if constexpr (F32) {
+                  const float t = fmaf(pyz, wx, kMagic);  // round(pyz * wx) in the low mantissa bits
+                  atomicAdd(&acc[0][c][slot], (unsigned int)(__float_as_int(t) - kMagicBits));
+                } else {
+                  Fixed<T>::add(&acc[0][c][slot], 3 * NCP, pyz * wx);
+                }
               }
             }
           }
