@@ -133,7 +133,7 @@ int sg_surf_vol(sg_ctx* ctx, const double* X, const double* Y, const double* Z,
  * Returns SG_OK, SG_ERR_ARG, SG_ERR_TOO_LARGE or SG_ERR_CUDA. */
 #define SG_NOALLOC_MAX_POINTS 65536
 #define SG_NOALLOC_MAX_TILES 16384
-#define SG_NOALLOC_SCRATCH_BYTES (4608u * 1024u)
+#define SG_NOALLOC_SCRATCH_BYTES (7424u * 1024u)
 int sg_spread_noalloc(int itot, int jtot, int ktot, double lx, double ly, double lz, long npts,
                       const double* X, const double* Y, const double* Z,
                       const double* FX, const double* FY, const double* FZ, const double* AREA,

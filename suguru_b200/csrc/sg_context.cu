@@ -203,8 +203,11 @@ int setup(sg_ctx* c) {
   // FP32 spreads on 16 x 16 x 8 tiles (fewer points straddle a tile edge);
   // FP64 keeps 1024-cell tiles for its three-limb shared accumulators
   const int shape = (c->mixed && cfg.itot >= 16 && cfg.jtot >= 16) ? 1 : -1;
-  if (!make_ib_grid(cfg.itot, cfg.jtot, cfg.ktot, cfg.lx, cfg.ly, cfg.lz, c->grid, shape))
-    return fail(c, SG_ERR_CONFIG, "grid out of range: need itot, jtot >= 8 and (itot+2)(jtot+2)(ktot+2) < 2^31");
+  if (!make_ib_grid(cfg.itot, cfg.jtot, cfg.ktot, cfg.lx, cfg.ly, cfg.lz, c->grid, shape) &&
+      !make_ib_grid(cfg.itot, cfg.jtot, cfg.ktot, cfg.lx, cfg.ly, cfg.lz, c->grid, -1))
+    return fail(c, SG_ERR_CONFIG,
+                "grid out of range: need itot, jtot >= 8, (itot+2)(jtot+2)(ktot+2) < 2^31, and a tile shape whose "
+                "last tile in x and y is not 1 or 2 cells wide");
   const IBGrid& g = c->grid;
   c->nfield = (long long)g.ldi * g.ldj * g.ldk;
   // capsules, offsets, degree groups
@@ -401,13 +404,9 @@ int setup(sg_ctx* c) {
   SG_RET(sur_setup(c));
   // binning work
   const long np = std::max(c->npts, 1L);
-  SG_TRY(dalloc(c, c->ibw.bx, sizeof(int) * np), "alloc");
-  SG_TRY(dalloc(c, c->ibw.by, sizeof(int) * np), "alloc");
-  SG_TRY(dalloc(c, c->ibw.bz, sizeof(int) * np), "alloc");
+  SG_TRY(dalloc(c, c->ibw.pos, (c->mixed ? sizeof(PosRec<float>) : sizeof(PosRec<double>)) * np), "alloc");
+  SG_TRY(dalloc(c, c->ibw.frc, (c->mixed ? sizeof(ForceRec<float>) : sizeof(ForceRec<double>)) * np), "alloc");
   SG_TRY(dalloc(c, c->ibw.entries, sizeof(int) * 8 * np), "alloc");
-  SG_TRY(dalloc(c, c->ibw.fx, E * np), "alloc");
-  SG_TRY(dalloc(c, c->ibw.fy, E * np), "alloc");
-  SG_TRY(dalloc(c, c->ibw.fz, E * np), "alloc");
   c->max_tiles = g.ntiles;
   for (int sh = 0; sh < kNumTileShapes; ++sh) {
     IBGrid t{};
@@ -485,16 +484,22 @@ int dev_forces(sg_ctx* c, const double* X, const double* Y, const double* Z, T* 
   SG_TRY(launch_shgrid<T>(c->d_wsh, c->nwsh, c->d_caps, c->d_groups, c->nmax, c->d_err, c->st), "shgrid");
   SG_RET(dev_legendre<T>(c, 4));
   SG_RET(dev_legendre<T>(c, 5));
-  SG_TRY(launch_final<T>(c->d_wfin, c->nwfin, c->d_caps, c->d_groups, FX, FY, FZ, NX, NY, NZ, A, c->nmax, c->d_err,
-                         c->st),
+  SG_TRY(launch_final<T>(c->d_wfin, c->nwfin, c->d_caps, c->d_groups, FX, FY, FZ, NX, NY, NZ, A, c->ibw.frc,
+                         c->grid.dvi, c->nmax, c->d_err, c->st),
          "final");
   c->launches += 5;  // centroid, posfwd, membrane, shgrid, final (Legendre launches counted above)
   return SG_OK;
 }
 
+// have_rec: the force records were written by this step's final synthesis;
+// otherwise they are packed from the caller's force and area arrays first.
 template <class T>
-int dev_spread(sg_ctx* c, const T* FX, const T* FY, const T* FZ, const T* A, T* fx, T* fy, T* fz) {
-  SG_TRY(launch_spread<T>(c->grid, c->ibw, FX, FY, FZ, A, fx, fy, fz, c->st), "spread");
+int dev_spread(sg_ctx* c, const T* FX, const T* FY, const T* FZ, const T* A, T* fx, T* fy, T* fz, bool have_rec) {
+  if (!have_rec) {
+    SG_TRY(launch_pack_forces<T>(c->grid, c->npts, FX, FY, FZ, A, c->ibw, c->st), "pack forces");
+    c->launches += c->npts > 0 ? 1 : 0;
+  }
+  SG_TRY(launch_spread<T>(c->grid, c->ibw, fx, fy, fz, c->st), "spread");
   c->launches += 1;
   return SG_OK;
 }
@@ -572,7 +577,7 @@ int run_step(sg_ctx* c, int what, const void* u, const void* v, const void* w, c
   SG_RET(mark(2));
   if (what & 2) SG_RET(dev_forces<T>(c, dX, dY, dZ, L[3], L[4], L[5], L[6], L[7], L[8], L[9]));
   SG_RET(mark(3));
-  if (what & 4) SG_RET(dev_spread<T>(c, L[3], L[4], L[5], L[9], dfx, dfy, dfz));
+  if (what & 4) SG_RET(dev_spread<T>(c, L[3], L[4], L[5], L[9], dfx, dfy, dfz, (what & 2) != 0));
   SG_RET(mark(4));
   c->ev_used[0] = (what & 5) != 0;
   c->ev_used[1] = (what & 1) != 0;

@@ -11,7 +11,9 @@ namespace sg {
 // periodic storage index in [1, n].
 
 // Tiles touched by the stencil of a point in one periodic dimension: the
-// tiles of its first and last cell (the stencil is narrower than a tile).
+// tiles of its first and last cell (the stencil is narrower than a tile, and
+// make_ib_grid keeps the last tile at 3 cells or more, so that a stencil
+// that wraps around the periodic end still meets two tiles at most).
 SG_HD int tiles_1d(int b, int n, int TW, int* t) {
   const int t0 = (wrap_near(b - 1, n) - 1) / TW, t1 = (wrap_near(b + 2, n) - 1) / TW;
   t[0] = t0;
@@ -46,8 +48,7 @@ __device__ __forceinline__ int wrap_cell(double v, int n) {
 // (neighbouring points usually do) are counted by one atomic.
 template <class T>
 __global__ void bin_points_kernel(IBGrid g, long n, const double* __restrict__ X, const double* __restrict__ Y,
-                                  const double* __restrict__ Z, int* __restrict__ bx, int* __restrict__ by,
-                                  int* __restrict__ bz, T* __restrict__ fx, T* __restrict__ fy, T* __restrict__ fz,
+                                  const double* __restrict__ Z, PosRec<T>* __restrict__ pos,
                                   int* __restrict__ counts) {
   const long p = (long)blockIdx.x * blockDim.x + threadIdx.x;
   const bool valid = p < n;
@@ -58,12 +59,16 @@ __global__ void bin_points_kernel(IBGrid g, long n, const double* __restrict__ X
     const double ffx = floor(cx), ffy = floor(cy), ffz = floor(cz);
     const int wx = wrap_cell(ffx, g.itot), wy = wrap_cell(ffy, g.jtot);
     const int zc = (int)(ffz < -4.0 ? -4.0 : (ffz > g.ktot + 4.0 ? g.ktot + 4.0 : ffz));
-    bx[p] = wx;
-    by[p] = wy;
-    bz[p] = zc;
-    fx[p] = (T)(cx - ffx);
-    fy[p] = (T)(cy - ffy);
-    fz[p] = (T)(cz - ffz);
+    PosRec<T> r;
+    r.b[0] = wx;
+    r.b[1] = wy;
+    r.b[2] = zc;
+    r.b[3] = 0;
+    r.f[0] = (T)(cx - ffx);
+    r.f[1] = (T)(cy - ffy);
+    r.f[2] = (T)(cz - ffz);
+    r.f[3] = T(0);
+    pos[p] = r;
     nx = tiles_1d(wx, g.itot, g.TX, tx);
     ny = tiles_1d(wy, g.jtot, g.TY, ty);
     nz = tiles_z(zc, g.ktot, g.TZ, tz);
@@ -120,15 +125,16 @@ __global__ void __launch_bounds__(1024) scan_counts_kernel(int ntiles, const int
   if (t == 0) starts[ntiles] = carry;
 }
 
-__global__ void bin_scatter_kernel(IBGrid g, long n, const int* __restrict__ bx, const int* __restrict__ by,
-                                   const int* __restrict__ bz, const int* __restrict__ starts, int* __restrict__ fill,
-                                   int* __restrict__ entries) {
+template <class T>
+__global__ void bin_scatter_kernel(IBGrid g, long n, const PosRec<T>* __restrict__ pos,
+                                   const int* __restrict__ starts, int* __restrict__ fill, int* __restrict__ entries) {
   const long p = (long)blockIdx.x * blockDim.x + threadIdx.x;
   int tx[2] = {0, 0}, ty[2] = {0, 0}, tz[2] = {0, 0}, nx = 0, ny = 0, nz = 0;
   if (p < n) {
-    nx = tiles_1d(bx[p], g.itot, g.TX, tx);
-    ny = tiles_1d(by[p], g.jtot, g.TY, ty);
-    nz = tiles_z(bz[p], g.ktot, g.TZ, tz);
+    const int4 b = *(const int4*)pos[p].b;
+    nx = tiles_1d(b.x, g.itot, g.TX, tx);
+    ny = tiles_1d(b.y, g.jtot, g.TY, ty);
+    nz = tiles_z(b.z, g.ktot, g.TZ, tz);
   }
   const unsigned lane = threadIdx.x & 31, lt = (1u << lane) - 1u;
 #pragma unroll
@@ -155,16 +161,15 @@ __global__ void bin_scatter_kernel(IBGrid g, long n, const int* __restrict__ bx,
 // direction and centre weights along the other two (delta3_face/_centre).
 // z-levels outside [1,kmax] are skipped (interp_spread.f90:346-351).
 template <class T>
-__global__ void __launch_bounds__(256) interp_kernel(IBGrid g, long n, const int* __restrict__ bx,
-                                                     const int* __restrict__ by, const int* __restrict__ bz,
-                                                     const T* __restrict__ fx, const T* __restrict__ fy,
-                                                     const T* __restrict__ fz, const T* __restrict__ u,
-                                                     const T* __restrict__ v, const T* __restrict__ w,
-                                                     T* __restrict__ U, T* __restrict__ V, T* __restrict__ W) {
+__global__ void __launch_bounds__(256) interp_kernel(IBGrid g, long n, const PosRec<T>* __restrict__ pos,
+                                                     const T* __restrict__ u, const T* __restrict__ v,
+                                                     const T* __restrict__ w, T* __restrict__ U, T* __restrict__ V,
+                                                     T* __restrict__ W) {
   const long p = (long)blockIdx.x * blockDim.x + threadIdx.x;
   if (p >= n) return;
-  const int bb[3] = {bx[p], by[p], bz[p]};
-  const T fr[3] = {fx[p], fy[p], fz[p]};
+  const PosRec<T> rec = pos[p];
+  const int bb[3] = {rec.b[0], rec.b[1], rec.b[2]};
+  const T fr[3] = {rec.f[0], rec.f[1], rec.f[2]};
   T wF[3][3], wC[3][3];
   bool hi[3];
 #pragma unroll
@@ -233,12 +238,11 @@ cudaError_t launch_bin(const IBGrid& g, long n, const double* X, const double* Y
   cudaError_t e = cudaMemsetAsync(w.counts, 0, sizeof(int) * g.ntiles, st);
   if (e != cudaSuccess) return e;
   if (n > 0)
-    bin_points_kernel<T><<<(unsigned)((n + 255) / 256), 256, 0, st>>>(g, n, X, Y, Z, w.bx, w.by, w.bz, (T*)w.fx,
-                                                                       (T*)w.fy, (T*)w.fz, w.counts);
+    bin_points_kernel<T><<<(unsigned)((n + 255) / 256), 256, 0, st>>>(g, n, X, Y, Z, (PosRec<T>*)w.pos, w.counts);
   scan_counts_kernel<<<1, 1024, 0, st>>>(g.ntiles, w.counts, w.starts, w.fill);
   if (n > 0)
-    bin_scatter_kernel<<<(unsigned)((n + 255) / 256), 256, 0, st>>>(g, n, w.bx, w.by, w.bz, w.starts, w.fill,
-                                                                     w.entries);
+    bin_scatter_kernel<T><<<(unsigned)((n + 255) / 256), 256, 0, st>>>(g, n, (const PosRec<T>*)w.pos, w.starts,
+                                                                        w.fill, w.entries);
   return cudaGetLastError();
 }
 
@@ -246,8 +250,7 @@ template <class T>
 cudaError_t launch_interp(const IBGrid& g, long n, const IBWork& w, const T* u, const T* v, const T* ww, T* U, T* V,
                           T* W, cudaStream_t st) {
   if (n <= 0) return cudaSuccess;
-  interp_kernel<T><<<(unsigned)((n + 255) / 256), 256, 0, st>>>(g, n, w.bx, w.by, w.bz, (const T*)w.fx,
-                                                                 (const T*)w.fy, (const T*)w.fz, u, v, ww, U, V, W);
+  interp_kernel<T><<<(unsigned)((n + 255) / 256), 256, 0, st>>>(g, n, (const PosRec<T>*)w.pos, u, v, ww, U, V, W);
   return cudaGetLastError();
 }
 
@@ -263,6 +266,24 @@ template cudaError_t launch_interp<float>(const IBGrid&, long, const IBWork&, co
 bool make_ib_grid(int itot, int jtot, int ktot, double lx, double ly, double lz, IBGrid& g, int shape) {
   if (itot < 8 || jtot < 8 || ktot < 1) return false;
   if (shape >= kNumTileShapes) return false;
+  // a last tile of 1 or 2 cells in a periodic dimension would let a
+  // stencil wrap across three tiles
+  auto fits = [&](int s) {
+    const int rx = itot % kTileShapes[s].TX, ry = jtot % kTileShapes[s].TY;
+    return rx != 1 && rx != 2 && ry != 1 && ry != 2;
+  };
+  if (shape < 0) {
+    // default tile shape: 32 x 8 x 4 (128-byte rows in x), 8 x 8 x 4 on
+    // narrow grids, else the first shape that fits
+    const int order[4] = {itot >= 32 ? 0 : 3, 2, 1, 3};
+    for (int s : order)
+      if (fits(s)) {
+        shape = s;
+        break;
+      }
+    if (shape < 0) return false;
+  }
+  if (!fits(shape)) return false;
   if ((long long)(itot + 2) * (jtot + 2) * (ktot + 2) > 2147483647LL) return false;  // 32-bit offsets
   g.itot = itot;
   g.jtot = jtot;
@@ -275,8 +296,6 @@ bool make_ib_grid(int itot, int jtot, int ktot, double lx, double ly, double lz,
   g.dyi = 1.0 / dy;
   g.dzi = 1.0 / dz;
   g.dvi = 1.0 / (dx * dy * dz);
-  // default tile shape: 32 x 8 x 4 (128-byte rows in x), 8 x 8 x 4 on narrow grids
-  if (shape < 0) shape = itot >= 32 ? 0 : 3;
   g.shape = shape;
   g.TX = kTileShapes[shape].TX;
   g.TY = kTileShapes[shape].TY;

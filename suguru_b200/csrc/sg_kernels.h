@@ -10,13 +10,25 @@
 namespace sg {
 
 // ------------------------------------------------------------ IB transfer --
+// Per point, written by the binning: base cell b[0..2] (b[3] unused) and the
+// fractional offsets f[0..2] in cell units (f[3] unused).  A record is 16-byte
+// aligned, so that the spread's gather of a point takes whole 16-byte loads
+// from one or two sectors instead of six scattered words.
+template <class T>
+struct alignas(16) PosRec {
+  int b[4];
+  T f[4];
+};
+// Per point, for the spread: cf[c] = F_c * area / dV (c = 0..2) and
+// cf[3] = max_c |cf[c]| (the bound of the fixed-point scale).
+template <class T>
+struct alignas(16) ForceRec {
+  T cf[4];
+};
+
 struct IBWork {
-  int* bx = nullptr;
-  int* by = nullptr;
-  int* bz = nullptr;
-  void* fx = nullptr;  // T[npts] fractional offsets
-  void* fy = nullptr;
-  void* fz = nullptr;
+  void* pos = nullptr;    // PosRec<T>[npts]
+  void* frc = nullptr;    // ForceRec<T>[npts]
   int* counts = nullptr;  // [ntiles]
   int* starts = nullptr;  // [ntiles+1]
   int* fill = nullptr;    // [ntiles]
@@ -24,6 +36,9 @@ struct IBWork {
 };
 
 // shape: index into kTileShapes, or -1 for the default of the grid size.
+// A shape whose last tile in x or y would have 1 or 2 cells is rejected (a
+// stencil could then reach three tiles in that periodic dimension); shape -1
+// takes the first shape that fits.
 bool make_ib_grid(int itot, int jtot, int ktot, double lx, double ly, double lz, IBGrid& g, int shape = -1);
 template <class T>
 cudaError_t launch_bin(const IBGrid& g, long n, const double* X, const double* Y, const double* Z, IBWork& w,
@@ -31,9 +46,14 @@ cudaError_t launch_bin(const IBGrid& g, long n, const double* X, const double* Y
 template <class T>
 cudaError_t launch_interp(const IBGrid& g, long n, const IBWork& w, const T* u, const T* v, const T* ww, T* U, T* V,
                           T* W, cudaStream_t st);
+// Force records from caller arrays (the coupling step's final synthesis
+// writes them itself): cf = F * (A / dV).
 template <class T>
-cudaError_t launch_spread(const IBGrid& g, const IBWork& w, const T* FX, const T* FY, const T* FZ, const T* A, T* ox,
-                          T* oy, T* oz, cudaStream_t st);
+cudaError_t launch_pack_forces(const IBGrid& g, long n, const T* FX, const T* FY, const T* FZ, const T* A, IBWork& w,
+                               cudaStream_t st);
+// Spreads the force records of w.frc (points binned in w).
+template <class T>
+cudaError_t launch_spread(const IBGrid& g, const IBWork& w, T* ox, T* oy, T* oz, cudaStream_t st);
 
 // ------------------------------------------------------------ host tables --
 // Gauss-Legendre colatitudes north->south and weights (gaqd.f:45 semantics).
@@ -195,8 +215,11 @@ template <class T>
 cudaError_t launch_shgrid(const RowWork* work, int nwork, const CapInfo* caps, const GroupDev* groups, int nmax,
                           int* err, cudaStream_t st);
 template <class T>
+// Also writes the spread's force records frc (ForceRec<T>[npts], cf = F * AREA
+// * dvi) when frc is not null.
 cudaError_t launch_final(const RowWork* work, int nwork, const CapInfo* caps, const GroupDev* groups, T* FX, T* FY,
-                         T* FZ, T* NX, T* NY, T* NZ, T* AREA, int nmax, int* err, cudaStream_t st);
+                         T* FZ, T* NX, T* NY, T* NZ, T* AREA, void* frc, double dvi, int nmax, int* err,
+                         cudaStream_t st);
 
 template <class T>
 cudaError_t launch_update_pos(long n, double dt, double lz, double* X, double* Y, double* Z, const T* U, const T* V,

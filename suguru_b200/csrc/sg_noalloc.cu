@@ -11,7 +11,7 @@
 // this step needs instead lives in one fixed array compiled into the library.
 //
 // The scratch array is a file-scope __device__ variable: every GPU that loads
-// the library holds it (SG_NOALLOC_SCRATCH_BYTES, about 4.6 MB) until the
+// the library holds it (SG_NOALLOC_SCRATCH_BYTES, about 7.3 MB) until the
 // process exits.  All calls share it, so calls that overlap on the GPU (two
 // streams, two host threads, or a call still running when the next one is
 // queued on another stream) race on it; the previous call's contents remain
@@ -28,12 +28,13 @@ namespace {
 
 constexpr size_t align256(size_t b) { return (b + 255) & ~size_t(255); }
 
-// scratch layout: per point base cells and fractions, per tile counters, entry lists
-constexpr size_t kPtsI = align256(sizeof(int) * SG_NOALLOC_MAX_POINTS);
-constexpr size_t kPtsD = align256(sizeof(double) * SG_NOALLOC_MAX_POINTS);
+// scratch layout: per point position and force records, per tile counters,
+// entry lists
+constexpr size_t kPos = align256(sizeof(PosRec<double>) * SG_NOALLOC_MAX_POINTS);
+constexpr size_t kFrc = align256(sizeof(ForceRec<double>) * SG_NOALLOC_MAX_POINTS);
 constexpr size_t kTile = align256(sizeof(int) * (SG_NOALLOC_MAX_TILES + 1));
 constexpr size_t kEntr = align256(sizeof(int) * 8 * SG_NOALLOC_MAX_POINTS);
-constexpr size_t kScratch = 3 * kPtsI + 3 * kPtsD + 3 * kTile + kEntr;
+constexpr size_t kScratch = kPos + kFrc + 3 * kTile + kEntr;
 static_assert(kScratch <= SG_NOALLOC_SCRATCH_BYTES, "scratch layout exceeds the stated size");
 
 }  // namespace
@@ -83,18 +84,15 @@ extern "C" int sg_spread_noalloc(int itot, int jtot, int ktot, double lx, double
   if (scratch_address(&base) != cudaSuccess) return SG_ERR_CUDA;
   unsigned char* s = (unsigned char*)base;
   IBWork w{};
-  w.bx = (int*)s; s += kPtsI;
-  w.by = (int*)s; s += kPtsI;
-  w.bz = (int*)s; s += kPtsI;
-  w.fx = s; s += kPtsD;
-  w.fy = s; s += kPtsD;
-  w.fz = s; s += kPtsD;
+  w.pos = s; s += kPos;
+  w.frc = s; s += kFrc;
   w.counts = (int*)s; s += kTile;  // zeroed by launch_bin on every call
   w.starts = (int*)s; s += kTile;
   w.fill = (int*)s; s += kTile;    // zeroed by the scan on every call
   w.entries = (int*)s;
   cudaStream_t st = (cudaStream_t)stream;
   if (launch_bin<double>(g, npts, X, Y, Z, w, st) != cudaSuccess) return SG_ERR_CUDA;
-  if (launch_spread<double>(g, w, FX, FY, FZ, AREA, fx, fy, fz, st) != cudaSuccess) return SG_ERR_CUDA;
+  if (launch_pack_forces<double>(g, npts, FX, FY, FZ, AREA, w, st) != cudaSuccess) return SG_ERR_CUDA;
+  if (launch_spread<double>(g, w, fx, fy, fz, st) != cudaSuccess) return SG_ERR_CUDA;
   return SG_OK;
 }

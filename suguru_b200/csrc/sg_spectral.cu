@@ -644,6 +644,7 @@ __global__ void __launch_bounds__(256) final_kernel(const RowWork* __restrict__ 
                                                     const GroupDev* __restrict__ groups, T* __restrict__ FX,
                                                     T* __restrict__ FY, T* __restrict__ FZ, T* __restrict__ NX,
                                                     T* __restrict__ NY, T* __restrict__ NZ, T* __restrict__ AREA,
+                                                    ForceRec<T>* __restrict__ frc, double dvi,
                                                     int* __restrict__ err) {
   (void)err;
   extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -720,6 +721,18 @@ __global__ void __launch_bounds__(256) final_kernel(const RowWork* __restrict__ 
         NY[p + H] = ev[4] - od[4];
         NZ[p + H] = ev[5] - od[5];
         AREA[p + H] = (ev[6] - od[6]) * wa;
+        if (frc) {  // the spread's force records: F * (area / dV), as pack_forces computes them
+#pragma unroll
+          for (int h = 0; h < 2; ++h) {
+            const T s = (h ? ev[6] - od[6] : ev[6] + od[6]) * wa * (T)dvi;
+            ForceRec<T> rc;
+            rc.cf[0] = (h ? ev[0] - od[0] : ev[0] + od[0]) * s;
+            rc.cf[1] = (h ? ev[1] - od[1] : ev[1] + od[1]) * s;
+            rc.cf[2] = (h ? ev[2] - od[2] : ev[2] + od[2]) * s;
+            rc.cf[3] = fmax(fabs(rc.cf[0]), fmax(fabs(rc.cf[1]), fabs(rc.cf[2])));
+            frc[p + h * H] = rc;
+          }
+        }
       }
     }
   }
@@ -836,13 +849,14 @@ cudaError_t launch_shgrid(const RowWork* work, int nwork, const CapInfo* caps, c
 
 template <class T>
 cudaError_t launch_final(const RowWork* work, int nwork, const CapInfo* caps, const GroupDev* groups, T* FX, T* FY,
-                         T* FZ, T* NX, T* NY, T* NZ, T* AREA, int nmax, int* err, cudaStream_t st) {
+                         T* FZ, T* NX, T* NY, T* NZ, T* AREA, void* frc, double dvi, int nmax, int* err,
+                         cudaStream_t st) {
   if (nwork <= 0) return cudaSuccess;
   const size_t smem = pointwise_smem<T>(kFinal, nmax);
   cudaError_t e = cudaFuncSetAttribute(final_kernel<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   if (e != cudaSuccess) return e;
   final_kernel<T><<<persistent_grid(final_kernel<T>, smem, nwork), kPointThreads, smem, st>>>(
-      work, nwork, caps, groups, FX, FY, FZ, NX, NY, NZ, AREA, err);
+      work, nwork, caps, groups, FX, FY, FZ, NX, NY, NZ, AREA, (ForceRec<T>*)frc, dvi, err);
   return cudaGetLastError();
 }
 
@@ -856,7 +870,7 @@ cudaError_t launch_final(const RowWork* work, int nwork, const CapInfo* caps, co
   template cudaError_t launch_shgrid<T>(const RowWork*, int, const CapInfo*, const GroupDev*, int, int*,             \
                                         cudaStream_t);                                                              \
   template cudaError_t launch_final<T>(const RowWork*, int, const CapInfo*, const GroupDev*, T*, T*, T*, T*, T*, T*,  \
-                                       T*, int, int*, cudaStream_t);
+                                       T*, void*, double, int, int*, cudaStream_t);
 SG_INST(double)
 SG_INST(float)
 

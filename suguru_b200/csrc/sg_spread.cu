@@ -78,14 +78,27 @@ struct Fixed<double> {
 
 }  // namespace
 
+// Force records cf = F * (A / dV) and their largest component magnitude
+// (interp_spread.f90:870-874 multiplies by area / dVeul in this order).
+template <class T>
+__global__ void pack_forces_kernel(long n, double dvi, const T* __restrict__ FX, const T* __restrict__ FY,
+                                   const T* __restrict__ FZ, const T* __restrict__ A, ForceRec<T>* __restrict__ frc) {
+  const long p = (long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (p >= n) return;
+  const T s = A[p] * (T)dvi;
+  ForceRec<T> r;
+  r.cf[0] = FX[p] * s;
+  r.cf[1] = FY[p] * s;
+  r.cf[2] = FZ[p] * s;
+  r.cf[3] = fmax(fabs(r.cf[0]), fmax(fabs(r.cf[1]), fabs(r.cf[2])));
+  frc[p] = r;
+}
+
 template <class T, int TX, int TY, int TZ>
 __global__ void __launch_bounds__(256) spread_kernel(IBGrid g, const int* __restrict__ entries,
-                                                     const int* __restrict__ starts, const int* __restrict__ bx,
-                                                     const int* __restrict__ by, const int* __restrict__ bz,
-                                                     const T* __restrict__ fx, const T* __restrict__ fy,
-                                                     const T* __restrict__ fz, const T* __restrict__ FX,
-                                                     const T* __restrict__ FY, const T* __restrict__ FZ,
-                                                     const T* __restrict__ AREA, T* __restrict__ ox,
+                                                     const int* __restrict__ starts,
+                                                     const PosRec<T>* __restrict__ pos,
+                                                     const ForceRec<T>* __restrict__ frc, T* __restrict__ ox,
                                                      T* __restrict__ oy, T* __restrict__ oz) {
   constexpr bool F32 = sizeof(T) == 4;
   constexpr int NC = TX * TY * TZ;
@@ -115,9 +128,7 @@ __global__ void __launch_bounds__(256) spread_kernel(IBGrid g, const int* __rest
     // max_c |f_c * area / dV| over the tile's entries (fixed reduction order)
     T red = T(0), rmax = T(0);
     for (int e = e0 + tid; e < e1; e += 256) {
-      const int p = entries[e];
-      const T s = fabs(AREA[p] * (T)g.dvi);
-      const T m = fmax(fabs(FX[p]) * s, fmax(fabs(FY[p]) * s, fabs(FZ[p]) * s));
+      const T m = frc[entries[e]].cf[3];
       red = F32 ? red + m : fmax(red, m);
       rmax = fmax(rmax, m);
     }
@@ -165,11 +176,12 @@ __global__ void __launch_bounds__(256) spread_kernel(IBGrid g, const int* __rest
         if (warp >= nw || idx >= k) continue;
         const int e = eb + idx;
         const int p = entries[e];
-        const int bb[3] = {bx[p], by[p], bz[p]};
-        const T fr[3] = {fx[p], fy[p], fz[p]};
-        const T s = AREA[p] * (T)g.dvi;  // interp_spread.f90:870-874
+        const PosRec<T> rec = pos[p];
+        const ForceRec<T> fo = frc[p];
+        const int bb[3] = {rec.b[0], rec.b[1], rec.b[2]};
+        const T fr[3] = {rec.f[0], rec.f[1], rec.f[2]};
         // scaled forces; scale is a power of two, so this multiply is exact
-        const T cf[3] = {(FX[p] * s) * scale, (FY[p] * s) * scale, (FZ[p] * s) * scale};
+        const T cf[3] = {fo.cf[0] * scale, fo.cf[1] * scale, fo.cf[2] * scale};
         // 1-D weights: the three nonzero values of the 3-point kernel around the
         // nearest node share one square root.  With r = (nearest node) - c,
         // |r| <= 1/2, s = sqrt(1 - 3 r^2):
@@ -318,32 +330,40 @@ __global__ void __launch_bounds__(256) spread_kernel(IBGrid g, const int* __rest
 }
 
 template <class T, int TX, int TY, int TZ>
-static void spread_one(const IBGrid& g, const IBWork& w, const T* FX, const T* FY, const T* FZ, const T* A, T* ox,
-                       T* oy, T* oz, cudaStream_t st) {
-  spread_kernel<T, TX, TY, TZ><<<g.ntiles, 256, 0, st>>>(g, w.entries, w.starts, w.bx, w.by, w.bz, (const T*)w.fx,
-                                                          (const T*)w.fy, (const T*)w.fz, FX, FY, FZ, A, ox, oy, oz);
+static void spread_one(const IBGrid& g, const IBWork& w, T* ox, T* oy, T* oz, cudaStream_t st) {
+  spread_kernel<T, TX, TY, TZ><<<g.ntiles, 256, 0, st>>>(g, w.entries, w.starts, (const PosRec<T>*)w.pos,
+                                                          (const ForceRec<T>*)w.frc, ox, oy, oz);
 }
 
 template <class T>
-cudaError_t launch_spread(const IBGrid& g, const IBWork& w, const T* FX, const T* FY, const T* FZ, const T* A, T* ox,
-                          T* oy, T* oz, cudaStream_t st) {
+cudaError_t launch_pack_forces(const IBGrid& g, long n, const T* FX, const T* FY, const T* FZ, const T* A, IBWork& w,
+                               cudaStream_t st) {
+  if (n <= 0) return cudaSuccess;
+  pack_forces_kernel<T><<<(unsigned)((n + 255) / 256), 256, 0, st>>>(n, g.dvi, FX, FY, FZ, A, (ForceRec<T>*)w.frc);
+  return cudaGetLastError();
+}
+
+template <class T>
+cudaError_t launch_spread(const IBGrid& g, const IBWork& w, T* ox, T* oy, T* oz, cudaStream_t st) {
   switch (g.shape) {
-    case 0: spread_one<T, 32, 8, 4>(g, w, FX, FY, FZ, A, ox, oy, oz, st); break;
-    case 3: spread_one<T, 8, 8, 4>(g, w, FX, FY, FZ, A, ox, oy, oz, st); break;
+    case 0: spread_one<T, 32, 8, 4>(g, w, ox, oy, oz, st); break;
+    case 3: spread_one<T, 8, 8, 4>(g, w, ox, oy, oz, st); break;
     case 1:
-      if constexpr (sizeof(T) == 4) { spread_one<T, 16, 16, 8>(g, w, FX, FY, FZ, A, ox, oy, oz, st); break; }
+      if constexpr (sizeof(T) == 4) { spread_one<T, 16, 16, 8>(g, w, ox, oy, oz, st); break; }
       return cudaErrorInvalidValue;
     case 2:
-      if constexpr (sizeof(T) == 4) { spread_one<T, 32, 8, 8>(g, w, FX, FY, FZ, A, ox, oy, oz, st); break; }
+      if constexpr (sizeof(T) == 4) { spread_one<T, 32, 8, 8>(g, w, ox, oy, oz, st); break; }
       return cudaErrorInvalidValue;
     default: return cudaErrorInvalidValue;
   }
   return cudaGetLastError();
 }
 
-template cudaError_t launch_spread<double>(const IBGrid&, const IBWork&, const double*, const double*, const double*,
-                                           const double*, double*, double*, double*, cudaStream_t);
-template cudaError_t launch_spread<float>(const IBGrid&, const IBWork&, const float*, const float*, const float*,
-                                          const float*, float*, float*, float*, cudaStream_t);
+template cudaError_t launch_pack_forces<double>(const IBGrid&, long, const double*, const double*, const double*,
+                                                const double*, IBWork&, cudaStream_t);
+template cudaError_t launch_pack_forces<float>(const IBGrid&, long, const float*, const float*, const float*,
+                                               const float*, IBWork&, cudaStream_t);
+template cudaError_t launch_spread<double>(const IBGrid&, const IBWork&, double*, double*, double*, cudaStream_t);
+template cudaError_t launch_spread<float>(const IBGrid&, const IBWork&, float*, float*, float*, cudaStream_t);
 
 }  // namespace sg

@@ -1,0 +1,77 @@
+"""Spreading on grids whose sizes are not multiples of the tile, and into
+fields that do not start on an aligned address.
+
+  - ragged grids (last tile in x or y narrower than the tile, down to 3
+    cells) give the oracle's field;
+  - a grid whose every tile shape would leave a last tile of 1 or 2 cells in
+    a periodic dimension is refused at set-up (a stencil that wraps around
+    the periodic end could reach three tiles there, and the binning records
+    two per dimension);
+  - output arrays offset by one element from an aligned allocation give the
+    same field, bit for bit, as aligned ones, and nothing is written outside.
+Tolerances: FP64 relative L2 <= 1e-12, mixed <= 1e-4 (the path tolerances).
+"""
+import numpy as np
+import pytest
+
+import oracle as O
+from suguru_b200 import workloads as W
+from suguru_b200.coupling import CouplingStep, SgError
+from util import rel_l2
+
+pytestmark = pytest.mark.gpu
+
+
+def _case(grid, seed=31):
+    wl = W.small_config(grid=grid)
+    rng = np.random.default_rng(seed)
+    f = rng.normal(size=(3, wl.npts))
+    a = rng.uniform(0.5, 1.5, wl.npts) * wl.grid[3] ** 2
+    ref = O.spread(wl.grid, wl.x, wl.y, wl.z, f[0], f[1], f[2], a)
+    return wl, f, a, ref
+
+
+@pytest.mark.parametrize("grid", [(61, 45, 40), (67, 53, 37), (75, 48, 40), (35, 43, 37)])
+@pytest.mark.parametrize("precision", ["fp64", "mixed"])
+def test_ragged_grids(cuda, grid, precision):
+    wl, f, a, ref = _case(grid)
+    cs = CouplingStep(wl.grid, wl.degree, wl.radius, precision=precision)
+    dt = np.float64 if precision == "fp64" else np.float32
+    tol = 1e-12 if precision == "fp64" else 1e-4
+    got = cs.lagr2eulr(wl.x, wl.y, wl.z, *(x.astype(dt) for x in f), a.astype(dt))
+    for g, r in zip(got, ref):
+        assert rel_l2(g, r) <= tol
+
+
+def test_grid_without_a_valid_tile_shape_is_refused(cuda):
+    # 66 = 2 mod 8, 16 and 32: every tile shape leaves a 2-cell last tile in x
+    wl = W.small_config()
+    grid = (66,) + tuple(wl.grid[1:])
+    with pytest.raises(SgError):
+        CouplingStep(grid, wl.degree, wl.radius, precision="fp64")
+
+
+@pytest.mark.parametrize("precision", ["fp64", "mixed"])
+def test_unaligned_output_fields(cuda, precision):
+    torch = cuda
+    wl, f, a, ref = _case((64, 48, 40), seed=32)
+    td = torch.float64 if precision == "fp64" else torch.float32
+    dt = np.float64 if precision == "fp64" else np.float32
+    dev = torch.device("cuda", 0)
+    cs = CouplingStep(wl.grid, wl.degree, wl.radius, precision=precision, mem="device")
+    X = [torch.from_numpy(x).to(dev) for x in (wl.x, wl.y, wl.z)]
+    F = [torch.from_numpy(x.astype(dt)).to(dev) for x in f]
+    A = torch.from_numpy(a.astype(dt)).to(dev)
+    shape = cs.field_shape
+    n = int(np.prod(shape))
+    aligned = [torch.empty(shape, dtype=td, device=dev) for _ in range(3)]
+    bufs = [torch.full((n + 1,), 7.0, dtype=td, device=dev) for _ in range(3)]
+    shifted = [b[1:].view(shape) for b in bufs]  # one element past a 256-byte boundary
+    cs.lagr2eulr(*X, *F, A, out=aligned)
+    cs.lagr2eulr(*X, *F, A, out=shifted)
+    torch.cuda.synchronize()
+    tol = 1e-12 if precision == "fp64" else 1e-4
+    for g, s, b, r in zip(aligned, shifted, bufs, ref):
+        assert torch.equal(g, s)
+        assert float(b[0]) == 7.0  # nothing written before the field
+        assert rel_l2(g.cpu().numpy(), r) <= tol
