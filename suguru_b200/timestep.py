@@ -60,10 +60,16 @@ class PrescribedFlow:
             # sum_q A_qc cos(ax + ay) = sum_q A_qc (cos ax cos ay - sin ax sin ay)
             A = self.amp[:, c][:, None]
             F = (A * torch.cos(ay)).T @ torch.cos(ax) - (A * torch.sin(ay)).T @ torch.sin(ax)  # [j, i]
-            U = torch.sin(np.pi * zs / Lz)[:, None, None] * F[None, :, :]
+            # U = sin(pi z / Lz) F (+ shear z for u): one broadcast pass that
+            # writes the output array directly (the 2-D F and 1-D factors are
+            # rounded to the output type first)
+            dt = self.out[c].dtype
+            sz = torch.sin(np.pi * zs / Lz).to(dt)[:, None, None]
+            Fd = F.to(dt)[None, :, :]
             if c == 0 and self.shear:
-                U = U + (self.shear * zs)[:, None, None]
-            self.out[c].copy_(U)
+                torch.addcmul((self.shear * zs).to(dt)[:, None, None], sz, Fd, out=self.out[c])
+            else:
+                torch.mul(sz, Fd, out=self.out[c])
         return self.out
 
 
