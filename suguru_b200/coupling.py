@@ -40,6 +40,7 @@ EXPORTS = ["sg_create", "sg_destroy", "sg_last_error", "sg_synchronize", "sg_int
            "sg_set_tensor_cores", "sg_set_legendre_terms", "sg_get_legendre_terms"]
 # test hooks declared in include/sg_testing.h
 TEST_EXPORTS = ["sg_test_legendre", "sg_test_gemm", "sg_test_mlp_grad"]
+WORKLOAD_EXPORTS = ["sg_prescribed_flow"]  # include/sg_workload.h
 TILE_SHAPES = ((32, 8, 4), (16, 16, 8), (32, 8, 8), (8, 8, 4))
 STAGES = ("bin", "interp", "membrane", "spread")
 
@@ -101,6 +102,8 @@ def lib():
     L.sg_graph_capture.argtypes = [vp] * 20
     L.sg_graph_launch.argtypes = [vp]
     L.sg_graph_release.argtypes = [vp]
+    L.sg_prescribed_flow.argtypes = [ctypes.c_int] * 3 + [ctypes.c_double] * 3 + [ctypes.c_int] + [vp] * 5 + \
+        [ctypes.c_double, vp, ctypes.c_int] + [vp] * 5
     L.sg_test_legendre.argtypes = [ctypes.c_int] * 6 + [vp] * 3
     L.sg_test_mlp_grad.argtypes = [ctypes.c_int] * 4 + [vp] * 5
     L.sg_set_capsule_membrane.argtypes = [vp] * 3

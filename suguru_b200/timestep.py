@@ -25,56 +25,57 @@ def frequencies(nmodes=16, seed=7):
 
 
 class PrescribedFlow:
-    """u, v, w on the MAC grid (with halos) at time t, computed with torch on the GPU."""
+    """u, v, w on the MAC grid (with halos) at time t, from the library's flow
+    kernels (include/sg_workload.h) on the current torch stream.
+
+    Called with a float t, or with a 0-d float64 CUDA tensor that the work
+    reads when it runs (a captured CUDA graph can then advance it)."""
 
     def __init__(self, grid, modes, shear, omega, dtype, device="cuda"):
         import torch
         self.torch = torch
-        itot, jtot, ktot, dx, dy, dz = grid
-        self.L = (itot * dx, jtot * dy, ktot * dz)
-        td = torch.float64
-        i = torch.arange(itot + 2, dtype=td, device=device)
-        j = torch.arange(jtot + 2, dtype=td, device=device)
-        k = torch.arange(ktot + 2, dtype=td, device=device)
-        self.face = (i * dx, j * dy, k * dz)
-        self.cent = ((i - 0.5) * dx, (j - 0.5) * dy, (k - 0.5) * dz)
-        self.nx = torch.as_tensor(modes["nx"], dtype=td, device=device)
-        self.ny = torch.as_tensor(modes["ny"], dtype=td, device=device)
-        self.phase = torch.as_tensor(modes["phase"], dtype=td, device=device)
-        self.amp = torch.as_tensor(modes["amp"], dtype=td, device=device)
-        self.omega = torch.as_tensor(omega, dtype=td, device=device)
+        self.grid = grid
+        itot, jtot, ktot = grid[:3]
+        f64 = lambda a: np.ascontiguousarray(a, dtype=np.float64)
+        self.modes = [f64(modes["nx"]), f64(modes["ny"]), f64(modes["phase"]), f64(modes["amp"]).reshape(-1, 3),
+                      f64(omega)]
         self.shear = float(shear)
         self.dtype = dtype
         self.out = [torch.empty((ktot + 2, jtot + 2, itot + 2), dtype=dtype, device=device) for _ in range(3)]
+        self.work = torch.empty(3 * (jtot + 2) * (itot + 2), dtype=torch.float64, device=device)
+        self.t = torch.zeros((), dtype=torch.float64, device=device)
 
     def __call__(self, t):
+        import ctypes
+        from .coupling import SgError, lib
         torch = self.torch
-        Lx, Ly, Lz = self.L
-        ph = self.phase + self.omega * t
-        for c in range(3):
-            xs = self.face[0] if c == 0 else self.cent[0]
-            ys = self.face[1] if c == 1 else self.cent[1]
-            zs = self.face[2] if c == 2 else self.cent[2]
-            ax = 2.0 * np.pi * self.nx[:, None] * xs[None, :] / Lx          # [q, i]
-            ay = 2.0 * np.pi * self.ny[:, None] * ys[None, :] / Ly + ph[:, None]  # [q, j]
-            # sum_q A_qc cos(ax + ay) = sum_q A_qc (cos ax cos ay - sin ax sin ay)
-            A = self.amp[:, c][:, None]
-            F = (A * torch.cos(ay)).T @ torch.cos(ax) - (A * torch.sin(ay)).T @ torch.sin(ax)  # [j, i]
-            # U = sin(pi z / Lz) F (+ shear z for u): one broadcast pass that
-            # writes the output array directly (the 2-D F and 1-D factors are
-            # rounded to the output type first)
-            dt = self.out[c].dtype
-            sz = torch.sin(np.pi * zs / Lz).to(dt)[:, None, None]
-            Fd = F.to(dt)[None, :, :]
-            if c == 0 and self.shear:
-                torch.addcmul((self.shear * zs).to(dt)[:, None, None], sz, Fd, out=self.out[c])
-            else:
-                torch.mul(sz, Fd, out=self.out[c])
+        if isinstance(t, torch.Tensor):
+            tt = t
+        else:
+            self.t.fill_(float(t))
+            tt = self.t
+        itot, jtot, ktot, dx, dy, dz = self.grid
+        nx, ny, ph, amp, om = self.modes
+        p = lambda a: ctypes.c_void_p(a.ctypes.data)
+        d = lambda x: ctypes.c_void_p(x.data_ptr())
+        rc = lib().sg_prescribed_flow(itot, jtot, ktot, dx, dy, dz, len(ph), p(nx), p(ny), p(ph), p(amp), p(om),
+                                      self.shear, d(tt), int(self.dtype == torch.float32), *map(d, self.out),
+                                      d(self.work), ctypes.c_void_p(torch.cuda.current_stream().cuda_stream))
+        if rc:
+            raise SgError(rc, "sg_prescribed_flow")
         return self.out
 
 
-def run(wl, steps, precision="mixed", dt=None, surrogate_params=None, trust=None, omega=None, stream=None):
-    """Advect the capsules of `wl` for `steps` steps; returns diagnostics and timing."""
+def run(wl, steps, precision="mixed", dt=None, surrogate_params=None, trust=None, omega=None, stream=None,
+        graph=True, tune=True):
+    """Advect the capsules of `wl` for `steps` steps; returns diagnostics and timing.
+
+    graph: capture one step (flow evaluation, coupling step, Update_Pos and
+    the time increment, which lives on the device) in a CUDA graph and replay
+    it `steps` times, so that no host work is left between the steps.
+    tune: let the library's autotuner pick the spreading tile and the capsule
+    split first (untimed; the points do not move).
+    """
     import torch
     dx = wl.grid[3]
     dt = 0.01 * dx if dt is None else dt
@@ -103,14 +104,34 @@ def run(wl, steps, precision="mixed", dt=None, surrogate_params=None, trust=None
         on_sur = fb = 0
         e0 = torch.cuda.Event(enable_timing=True)
         e1 = torch.cuda.Event(enable_timing=True)
-        e0.record(st)
-        for s in range(steps):
-            u, v, w = flow(s * dt)
-            cs.step(u, v, w, *X, lag_out=lag, eul_out=eul)
-            cs.update_pos(dt, *X, lag[0], lag[1], lag[2])
-        e1.record(st)
+        if tune:  # tile shape and capsule split from the library's autotuner (does not move the points)
+            cs.autotune(*flow(0.0), *X, lag_out=lag, eul_out=eul, reps=2)
+        if graph:
+            t_dev = torch.zeros((), dtype=torch.float64, device="cuda")
+            flow(t_dev)  # library handles of the flow's products exist before the capture
+            cs.update_pos(0.0, *X, lag[0], lag[1], lag[2])  # loads the kernel; X + 0 U leaves X as it is
+            st.synchronize()
+            g = torch.cuda.CUDAGraph()
+            with torch.cuda.graph(g, stream=st):
+                u, v, w = flow(t_dev)
+                cs.step(u, v, w, *X, lag_out=lag, eul_out=eul)
+                cs.update_pos(dt, *X, lag[0], lag[1], lag[2])
+                t_dev.add_(dt)
+            e0.record(st)
+            for _ in range(steps):
+                g.replay()
+            e1.record(st)
+        else:
+            e0.record(st)
+            for s in range(steps):
+                u, v, w = flow(s * dt)
+                cs.step(u, v, w, *X, lag_out=lag, eul_out=eul)
+                cs.update_pos(dt, *X, lag[0], lag[1], lag[2])
+            e1.record(st)
         torch.cuda.synchronize()
         ms = e0.elapsed_time(e1)
+        if graph:
+            del g
         if surrogate_params is not None:
             on_sur, fb = cs.surrogate_counts()
         d1 = diag()

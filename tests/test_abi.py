@@ -36,11 +36,15 @@ def test_exports_every_declared_symbol(lib):
 
 def test_every_header_is_covered(lib):
     headers = sorted(f for f in os.listdir(os.path.join(ROOT, "include")) if f.endswith(".h"))
-    assert headers == ["sg_coupling.h", "sg_testing.h"]
+    assert headers == ["sg_coupling.h", "sg_testing.h", "sg_workload.h"]
     syms = header_symbols("sg_testing.h")
     for s in syms:
         assert hasattr(lib, s), s
     assert sorted(coupling.TEST_EXPORTS) == syms
+    syms = header_symbols("sg_workload.h")
+    for s in syms:
+        assert hasattr(lib, s), s
+    assert sorted(coupling.WORKLOAD_EXPORTS) == syms
 
 
 def test_build_flags_target_sm100a():
