@@ -417,6 +417,9 @@ int setup(sg_ctx* c) {
   SG_TRY(dalloc(c, c->ibw.starts, sizeof(int) * (c->max_tiles + 1)), "alloc");
   SG_TRY(dalloc(c, c->ibw.fill, sizeof(int) * c->max_tiles), "alloc");
   if (cfg.mem == SG_MEM_HOST) {
+    SG_TRY(cudaStreamCreateWithFlags(&c->st2, cudaStreamNonBlocking), "cudaStreamCreate");
+    SG_TRY(cudaEventCreateWithFlags(&c->ev_bin, cudaEventDisableTiming), "cudaEventCreate");
+    SG_TRY(cudaEventCreateWithFlags(&c->ev_join, cudaEventDisableTiming), "cudaEventCreate");
     SG_TRY(dalloc(c, c->s_u, E * c->nfield), "alloc");
     SG_TRY(dalloc(c, c->s_v, E * c->nfield), "alloc");
     SG_TRY(dalloc(c, c->s_w, E * c->nfield), "alloc");
@@ -441,8 +444,8 @@ int dev_bin(sg_ctx* c, const double* X, const double* Y, const double* Z) {
 }
 
 template <class T>
-int dev_interp(sg_ctx* c, const T* u, const T* v, const T* w, T* U, T* V, T* W) {
-  SG_TRY(launch_interp<T>(c->grid, c->npts, c->ibw, u, v, w, U, V, W, c->st), "interp");
+int dev_interp(sg_ctx* c, const T* u, const T* v, const T* w, T* U, T* V, T* W, cudaStream_t st) {
+  SG_TRY(launch_interp<T>(c->grid, c->npts, c->ibw, u, v, w, U, V, W, st), "interp");
   c->launches += 1;
   return SG_OK;
 }
@@ -524,12 +527,12 @@ int finish(sg_ctx* c) {
   return SG_OK;
 }
 
-int h2d(sg_ctx* c, void* dst, const void* src, size_t bytes) {
-  SG_TRY(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyHostToDevice, c->st), "h2d");
+int h2d(sg_ctx* c, void* dst, const void* src, size_t bytes, cudaStream_t st = nullptr) {
+  SG_TRY(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyHostToDevice, st ? st : c->st), "h2d");
   return SG_OK;
 }
-int d2h(sg_ctx* c, void* dst, const void* src, size_t bytes) {
-  SG_TRY(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyDeviceToHost, c->st), "d2h");
+int d2h(sg_ctx* c, void* dst, const void* src, size_t bytes, cudaStream_t st = nullptr) {
+  SG_TRY(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyDeviceToHost, st ? st : c->st), "d2h");
   return SG_OK;
 }
 
@@ -546,15 +549,27 @@ int run_step(sg_ctx* c, int what, const void* u, const void* v, const void* w, c
   const T *du = (const T*)u, *dv = (const T*)v, *dw = (const T*)w;
   T* L[10] = {(T*)U, (T*)V, (T*)W, (T*)FX, (T*)FY, (T*)FZ, (T*)NX, (T*)NY, (T*)NZ, (T*)A};
   T *dfx = (T*)fx, *dfy = (T*)fy, *dfz = (T*)fz;
+  // Host memory, full step: the interpolation branch (velocity upload,
+  // interp, velocity download) runs on st2 and the force branch (binning,
+  // forces, spread, their downloads) on st, so that the velocity upload on one
+  // stream overlaps the downloads on the other -- the spread does not read
+  // the velocity.  st2 starts after the work already queued on st and waits
+  // for the binning; st waits for st2 before the step ends.
+  const bool dual = host && c->st2 && (what & 1) && (what & 6) && !c->profiling && !c->capturing;
+  cudaStream_t sB = dual ? c->st2 : c->st;
+  if (dual) {
+    SG_TRY(cudaEventRecord(c->ev_join, c->st), "event");
+    SG_TRY(cudaStreamWaitEvent(sB, c->ev_join, 0), "stream wait");
+  }
   if (host) {
     SG_RET(h2d(c, c->s_X, X, pb));
     SG_RET(h2d(c, c->s_Y, Y, pb));
     SG_RET(h2d(c, c->s_Z, Z, pb));
     dX = c->s_X; dY = c->s_Y; dZ = c->s_Z;
     if (what & 1) {
-      SG_RET(h2d(c, c->s_u, u, fb));
-      SG_RET(h2d(c, c->s_v, v, fb));
-      SG_RET(h2d(c, c->s_w, w, fb));
+      SG_RET(h2d(c, c->s_u, u, fb, sB));
+      SG_RET(h2d(c, c->s_v, v, fb, sB));
+      SG_RET(h2d(c, c->s_w, w, fb, sB));
       du = (const T*)c->s_u; dv = (const T*)c->s_v; dw = (const T*)c->s_w;
     }
     for (int q = 0; q < 10; ++q) L[q] = (T*)c->s_lag[q];
@@ -572,33 +587,43 @@ int run_step(sg_ctx* c, int what, const void* u, const void* v, const void* w, c
   };
   SG_RET(mark(0));
   if (what & 5) SG_RET(dev_bin<T>(c, dX, dY, dZ));
+  if (dual) {
+    SG_TRY(cudaEventRecord(c->ev_bin, c->st), "event");
+    SG_TRY(cudaStreamWaitEvent(sB, c->ev_bin, 0), "stream wait");
+  }
   SG_RET(mark(1));
-  if (what & 1) SG_RET(dev_interp<T>(c, du, dv, dw, L[0], L[1], L[2]));
-  SG_RET(mark(2));
-  if (what & 2) SG_RET(dev_forces<T>(c, dX, dY, dZ, L[3], L[4], L[5], L[6], L[7], L[8], L[9]));
-  SG_RET(mark(3));
-  if (what & 4) SG_RET(dev_spread<T>(c, L[3], L[4], L[5], L[9], dfx, dfy, dfz, (what & 2) != 0));
-  SG_RET(mark(4));
-  c->ev_used[0] = (what & 5) != 0;
-  c->ev_used[1] = (what & 1) != 0;
-  c->ev_used[2] = (what & 2) != 0;
-  c->ev_used[3] = (what & 4) != 0;
-  if (host) {
-    if (what & 1) {
-      SG_RET(d2h(c, U, L[0], lb));
-      SG_RET(d2h(c, V, L[1], lb));
-      SG_RET(d2h(c, W, L[2], lb));
+  if (what & 1) {
+    SG_RET(dev_interp<T>(c, du, dv, dw, L[0], L[1], L[2], sB));
+    if (host) {
+      SG_RET(d2h(c, U, L[0], lb, sB));
+      SG_RET(d2h(c, V, L[1], lb, sB));
+      SG_RET(d2h(c, W, L[2], lb, sB));
     }
-    if (what & 2) {
+  }
+  if (dual) SG_TRY(cudaEventRecord(c->ev_join, sB), "event");
+  SG_RET(mark(2));
+  if (what & 2) {
+    SG_RET(dev_forces<T>(c, dX, dY, dZ, L[3], L[4], L[5], L[6], L[7], L[8], L[9]));
+    if (host) {
       void* outs[7] = {FX, FY, FZ, NX, NY, NZ, A};
       for (int q = 0; q < 7; ++q) SG_RET(d2h(c, outs[q], L[3 + q], lb));
     }
-    if (what & 4) {
+  }
+  SG_RET(mark(3));
+  if (what & 4) {
+    SG_RET(dev_spread<T>(c, L[3], L[4], L[5], L[9], dfx, dfy, dfz, (what & 2) != 0));
+    if (host) {
       SG_RET(d2h(c, fx, dfx, fb));
       SG_RET(d2h(c, fy, dfy, fb));
       SG_RET(d2h(c, fz, dfz, fb));
     }
   }
+  SG_RET(mark(4));
+  c->ev_used[0] = (what & 5) != 0;
+  c->ev_used[1] = (what & 1) != 0;
+  c->ev_used[2] = (what & 2) != 0;
+  c->ev_used[3] = (what & 4) != 0;
+  if (dual) SG_TRY(cudaStreamWaitEvent(c->st, c->ev_join, 0), "stream wait");
   if (what & 2)  // bounded waits of the force kernels
     SG_TRY(cudaMemcpyAsync(c->h_err, c->d_err, sizeof(int), cudaMemcpyDeviceToHost, c->st), "error flag");
   SG_TRY(cudaGetLastError(), "step");
@@ -686,6 +711,12 @@ void sg_destroy(sg_ctx* c) {
   for (int k = 0; k <= SG_NSTAGE; ++k)
     if (c->ev[k]) cudaEventDestroy(c->ev[k]);
   if (c->own_stream && c->st) cudaStreamDestroy(c->st);
+  if (c->st2) {
+    cudaStreamSynchronize(c->st2);
+    cudaStreamDestroy(c->st2);
+  }
+  if (c->ev_bin) cudaEventDestroy(c->ev_bin);
+  if (c->ev_join) cudaEventDestroy(c->ev_join);
   if (c->h_err) cudaFreeHost(c->h_err);
   if (c->h_sur_count) cudaFreeHost(c->h_sur_count);
   delete c;

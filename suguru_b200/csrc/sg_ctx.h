@@ -84,6 +84,11 @@ struct sg_ctx {
   double* s_exy = nullptr;
   cudaStream_t st = nullptr;
   bool own_stream = false;
+  // host-memory contexts: a second stream for the interpolation branch of a
+  // full step (velocity upload, interp, velocity download), so that its copies
+  // overlap the force branch's in the other direction; events join the two
+  cudaStream_t st2 = nullptr;
+  cudaEvent_t ev_bin = nullptr, ev_join = nullptr;
   std::vector<void*> allocs;
   std::string err;
   int launches = 0;
