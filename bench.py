@@ -46,6 +46,9 @@ def parse_args():
                    help="time one path only, no e2e (for profiler captures)")
     p.add_argument("--cpu-sample-caps", type=int, default=64)
     p.add_argument("--no-surrogate", action="store_true", help="skip training and timing the surrogate path")
+    p.add_argument("--tile", type=int, default=None, choices=[0, 1, 2, 3],
+                   help="fixed spreading tile shape (index into TILE_SHAPES; FP64 takes shape 0) instead of the "
+                        "autotuner, so that profiler captures see one launch sequence")
     p.add_argument("--legendre-terms", type=int, default=0, choices=[0, 3, 6],
                    help="mixed path: split products of the tensor-core Legendre contractions (0: automatic by degree)")
     p.add_argument("--sur-samples", type=int, default=200000)
@@ -129,9 +132,9 @@ class Clocks:
 
 def spread_bytes(wl, s):
     """Algorithmic bytes of one spread launch: the whole force field written
-    (lagr2eulr zeroes and writes every cell) plus, per point, force and area
-    (4 reals), base cell indices (3 int32), fractional offsets (3 reals) and
-    the sorted index (int32)."""
+    (lagr2eulr zeroes and writes every cell) plus, per point, its force record
+    (force * area / dV and the largest component: 4 reals), base cell indices
+    (3 int32), fractional offsets (3 reals) and the sorted index (int32)."""
     itot, jtot, ktot = wl.grid[:3]
     nfield = (itot + 2) * (jtot + 2) * (ktot + 2)
     return 3 * nfield * s + wl.npts * (4 * s + 12 + 3 * s + 4)
@@ -202,6 +205,9 @@ def run_ours(args):
         lag = [torch.empty(n, dtype=td, device=dev) for _ in range(10)]
         eul = [torch.empty(cs.field_shape, dtype=td, device=dev) for _ in range(3)]
         tile = 0
+        if args.tile is not None:  # a fixed tile shape, no autotuning (profiler captures)
+            cs.set_tile_shape(args.tile if precision != "fp64" else 0)
+            tune = False
         if tune:  # the library's autotuner picks the spreading tile shape (untimed set-up)
             cs.set_profiling(False)
             tile, _ = cs.autotune(*uvw, *X, lag_out=lag, eul_out=eul, reps=3)
@@ -349,7 +355,7 @@ def run_ours(args):
         sp_ms = head["stages"]["spread"]
         sbytes = spread_bytes(wl, 4)
         achieved = sbytes / (sp_ms / 1e3) / 1e9
-        traffic = load_traffic().get("spread_c1_mixed_bytes_per_launch")
+        traffic = load_traffic().get("spread_%s_mixed_bytes_per_launch" % args.config)  # this workload's capture only
         result = {
             "metric": "Lagrangian pts/s per IB step, mixed+surrogate vs FP64 plain, 1 B200, <=1e-4 err",
             "value": value,
