@@ -144,6 +144,16 @@ int sg_spread_noalloc(int itot, int jtot, int ktot, double lx, double ly, double
  * values serve training-data generation over a range of C. */
 int sg_set_capsule_membrane(sg_ctx* ctx, const double* gs, const double* csk);
 
+/* Membrane law per capsule (host array of ncap): SG_LAW_SKALAK (the default;
+ * membmodel.c:81-99) or SG_LAW_NEO_HOOKEAN (membmodel.c:60-79, which the
+ * reference selects at compile time with -DNONHOOK; C plays no part in it).
+ * The surrogate, trained on the Skalak law, never takes neo-Hookean capsules.
+ * Returns SG_ERR_ARG for another value, SG_ERR_STATE while a graph is
+ * captured. */
+#define SG_LAW_SKALAK 0
+#define SG_LAW_NEO_HOOKEAN 1
+int sg_set_capsule_law(sg_ctx* ctx, const int* law);
+
 /* Spectral coefficients of the plain membrane model, per capsule: the
  * displacement from the reference sphere after the centroid is removed
  * (the analysis of cal_3dcrd_spectral_coeff, sph1.f90:29-79) and the force

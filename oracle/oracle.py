@@ -53,6 +53,9 @@ def lib():
         L.or_collisions.restype = None
         L.or_skalak.argtypes = [d, d, _dp, _dp, d, d, _dp]
         L.or_skalak.restype = None
+        L.or_membrane_law.argtypes = [i, d, d, _dp, _dp, d, d, _dp]
+        L.or_membrane_law.restype = None
+        L.or_complagrforces_law.argtypes = [i, d, d, d, i, i] + [_dp] * 10
         L.or_coupling_step.argtypes = ([i, i, i, d, d, d, i, _ip, _dp, d, d, i, i] + [_dp] * 20)
         _LIB = L
     return _LIB
@@ -129,13 +132,16 @@ def kerneltest():
     return lib().or_kerneltest()
 
 
-def complagrforces(L, radius, x, y, z, gs=1.0, csk=1.0, faithful=False):
-    """One capsule: flat force-grid positions -> (f[3,nl], n[3,nl], area[nl])."""
+def complagrforces(L, radius, x, y, z, gs=1.0, csk=1.0, faithful=False, law=0):
+    """One capsule: flat force-grid positions -> (f[3,nl], n[3,nl], area[nl]).
+
+    law: 0 Skalak (membmodel.c:81-99), 1 neo-Hookean (membmodel.c:60-79)."""
     nl = 8 * (L + 1) ** 2
     x, y, z = _f64(x), _f64(y), _f64(z)
     assert x.size == nl
     out = [np.zeros(nl) for _ in range(7)]
-    rc = lib().or_complagrforces(L, radius, gs, csk, int(faithful), _p(x), _p(y), _p(z), *[_p(o) for o in out])
+    rc = lib().or_complagrforces_law(L, radius, gs, csk, int(law), int(faithful), _p(x), _p(y), _p(z),
+                                     *[_p(o) for o in out])
     assert rc == 0, rc
     return np.stack(out[0:3]), np.stack(out[3:6]), out[6]
 
@@ -201,6 +207,13 @@ def coupling_step(grid, degree, radius, u, v, w, x, y, z, gs=1.0, csk=1.0, faith
 def skalak(I1, I2, I1de, I2de, gs=1.0, csk=1.0):
     out = np.zeros(6)
     lib().or_skalak(float(I1), float(I2), _p(_f64(I1de)), _p(_f64(I2de)), gs, csk, _p(out))
+    return out
+
+
+def membrane_law(law, I1, I2, I1de, I2de, gs=1.0, csk=1.0):
+    """W1, W2, dW1[2], dW2[2] of law 0 (Skalak) or 1 (neo-Hookean)."""
+    out = np.zeros(6)
+    lib().or_membrane_law(int(law), float(I1), float(I2), _p(_f64(I1de)), _p(_f64(I2de)), gs, csk, _p(out))
     return out
 
 

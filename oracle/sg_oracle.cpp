@@ -422,10 +422,35 @@ void geometry(const double* f15, Geo& G) {
   }
 }
 
+// Strain-energy derivatives of the membrane law (membmodel.c, selected there
+// at compile time: -DSKALAK or -DNONHOOK): W1 = dW/dI1, W2 = dW/dI2 and their
+// derivatives along xi_1, xi_2.  law 0: Skalak, calpwspi_deri_sk
+// (membmodel.c:81-99); law 1: neo-Hookean, calpwspi_deri_nh (:60-79).
+void membrane_law(int law, double hf, double csk, double I1, double I2, const double* I1de, const double* I2de,
+                  double& W1, double& W2, double* W1de, double* W2de) {
+  if (law == 1) {
+    const double gs = 2.0 * hf;
+    W1 = hf;
+    W2 = -hf * std::pow(I2 + 1, -2);
+    const double coeff = gs * std::pow(I2 + 1, -3);
+    for (int al = 0; al < 2; ++al) {
+      W1de[al] = 0;
+      W2de[al] = coeff * I2de[al];
+    }
+    return;
+  }
+  W1 = hf * (1 + I1);
+  W2 = hf * (csk * I2 - 1);
+  for (int al = 0; al < 2; ++al) {
+    W1de[al] = hf * I1de[al];
+    W2de[al] = csk * hf * I2de[al];
+  }
+}
+
 // Mechanics at one point: sph.f90:1668-1715 with cal_Js_I1_I2_deri
-// (sph.f90:1115-1156), Skalak calpwspi_deri (membmodel.c:81-99) and
+// (sph.f90:1115-1156), the membrane law (membrane_law) and
 // calculate_cauchy_tensor_deri (sph.f90:1179-1234).  A* = reference (conAR).
-void mechanics(const Geo& G, const double* A, const double* Ad, double hf, double csk, double* f) {
+void mechanics(const Geo& G, const double* A, const double* Ad, double hf, double csk, int law, double* f) {
   const double A11 = A[0], A22 = A[3], A12 = A[1];
   const double c11 = G.cat[0], c22 = G.cat[1], c12 = G.cat[2];
   double abs_conA = A11 * A22 - A12 * A12;
@@ -443,11 +468,8 @@ void mechanics(const Geo& G, const double* A, const double* Ad, double hf, doubl
     I2de[al] = abs_conAd * abs_ca + abs_cad * abs_conA;
   }
   for (int al = 0; al < 2; ++al) Jsde[al] = 0.5 / Js * I2de[al];
-  // membmodel.c:81-99 (Skalak)
-  double W1 = hf * (1 + I1);
-  double W2 = hf * (csk * I2 - 1);
-  double W1de[2] = {hf * I1de[0], hf * I1de[1]};
-  double W2de[2] = {csk * hf * I2de[0], csk * hf * I2de[1]};
+  double W1, W2, W1de[2], W2de[2];
+  membrane_law(law, hf, csk, I1, I2, I1de, I2de, W1, W2, W1de, W2de);
   // Cauchy tension and derivatives
   double coef1 = 2. / Js * W1, coef2 = 2. * Js * W2;
   double a11 = G.conat[0], a22 = G.conat[1], a12 = G.conat[2];
@@ -633,7 +655,7 @@ void surface_metric(const Capsule& C, const double* a, const double* b, double* 
 // complagrforces for one capsule (forcing.f90:11-114 -> cal_spectral_force
 // sph.f90:1523-1755).  Optionally returns the shape and filtered-force
 // coefficients (degree < N) for the surrogate data path.
-int capsule_force(int L, double R, double gs, double csk, bool faithful,
+int capsule_force(int L, double R, double gs, double csk, int law, bool faithful,
                   const double* xfp, const double* yfp, const double* zfp,
                   double* fxl, double* fyl, double* fzl, double* xn, double* yn, double* zn, double* area,
                   double* shape_a, double* shape_b, double* force_a, double* force_b) {
@@ -679,7 +701,7 @@ int capsule_force(int L, double R, double gs, double csk, bool faithful,
   for (size_t p = 0; p < nF; ++p) {
     geometry(&f15[p * 15], G);
     double f[3];
-    mechanics(G, &C.conAR[p * 4], &C.conARd1[p * 8], hf, csk, f);
+    mechanics(G, &C.conAR[p * 4], &C.conARd1[p * 8], hf, csk, law, f);
     for (int c = 0; c < 3; ++c) {
       fN[c * nF + p] = f[c];
       unitN[c * nF + p] = G.n[c];
@@ -973,13 +995,22 @@ double or_kerneltest(void) {
 int or_complagrforces(int L, double radius, double gs, double csk, int faithful, const double* xfp,
                       const double* yfp, const double* zfp, double* fx, double* fy, double* fz, double* nx,
                       double* ny, double* nz, double* area) {
-  return capsule_force(L, radius, gs, csk, faithful != 0, xfp, yfp, zfp, fx, fy, fz, nx, ny, nz, area, nullptr,
+  return capsule_force(L, radius, gs, csk, 0, faithful != 0, xfp, yfp, zfp, fx, fy, fz, nx, ny, nz, area, nullptr,
+                       nullptr, nullptr, nullptr);
+}
+
+// complagrforces with a chosen membrane law (0 Skalak, 1 neo-Hookean)
+int or_complagrforces_law(int L, double radius, double gs, double csk, int law, int faithful, const double* xfp,
+                          const double* yfp, const double* zfp, double* fx, double* fy, double* fz, double* nx,
+                          double* ny, double* nz, double* area) {
+  if (law != 0 && law != 1) return 1;
+  return capsule_force(L, radius, gs, csk, law, faithful != 0, xfp, yfp, zfp, fx, fy, fz, nx, ny, nz, area, nullptr,
                        nullptr, nullptr, nullptr);
 }
 
 int or_capsule_spectra(int L, double radius, double gs, double csk, const double* xfp, const double* yfp,
                        const double* zfp, double* shape_a, double* shape_b, double* force_a, double* force_b) {
-  return capsule_force(L, radius, gs, csk, false, xfp, yfp, zfp, nullptr, nullptr, nullptr, nullptr, nullptr,
+  return capsule_force(L, radius, gs, csk, 0, false, xfp, yfp, zfp, nullptr, nullptr, nullptr, nullptr, nullptr,
                        nullptr, nullptr, shape_a, shape_b, force_a, force_b);
 }
 
@@ -1087,13 +1118,13 @@ void or_collisions(long nl, const double* zp, const double* area, double dx, dou
 
 void or_skalak(double I1, double I2, const double* I1de, const double* I2de, double gs, double csk, double* out) {
   // membmodel.c:81-99 restated: out = W1, W2, dW1[2], dW2[2]
-  const double hf = 0.5 * gs;
-  out[0] = hf * (1 + I1);
-  out[1] = hf * (csk * I2 - 1);
-  out[2] = hf * I1de[0];
-  out[3] = hf * I1de[1];
-  out[4] = csk * hf * I2de[0];
-  out[5] = csk * hf * I2de[1];
+  membrane_law(0, 0.5 * gs, csk, I1, I2, I1de, I2de, out[0], out[1], out + 2, out + 4);
+}
+
+void or_membrane_law(int law, double I1, double I2, const double* I1de, const double* I2de, double gs, double csk,
+                     double* out) {
+  // membmodel.c:60-99 restated (law 0 Skalak, 1 neo-Hookean): out = W1, W2, dW1[2], dW2[2]
+  membrane_law(law, 0.5 * gs, csk, I1, I2, I1de, I2de, out[0], out[1], out + 2, out + 4);
 }
 
 int or_coupling_step(int itot, int jtot, int ktot, double dx, double dy, double dz, int ncap, const int* degree,
@@ -1125,7 +1156,7 @@ int or_coupling_step(int itot, int jtot, int ktot, double dx, double dy, double 
 #endif
   for (int c = 0; c < ncap; ++c) {
     long o = off[c];
-    err |= capsule_force(degree[c], radius[c], gs, csk, fa, xp + o, yp + o, zp + o, fxl + o, fyl + o, fzl + o, nx + o,
+    err |= capsule_force(degree[c], radius[c], gs, csk, 0, fa, xp + o, yp + o, zp + o, fxl + o, fyl + o, fzl + o, nx + o,
                          ny + o, nz + o, area + o, nullptr, nullptr, nullptr, nullptr);
   }
   auto t2 = clk::now();

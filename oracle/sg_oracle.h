@@ -51,6 +51,12 @@ int or_complagrforces(int L, double radius, double gs, double csk, int faithful,
                       const double* xfp, const double* yfp, const double* zfp,
                       double* fx, double* fy, double* fz,
                       double* nx, double* ny, double* nz, double* area);
+/* Same with the membrane law chosen: law 0 Skalak (membmodel.c:81-99), 1
+ * neo-Hookean (membmodel.c:60-79, the reference's -DNONHOOK build). */
+int or_complagrforces_law(int L, double radius, double gs, double csk, int law, int faithful,
+                          const double* xfp, const double* yfp, const double* zfp,
+                          double* fx, double* fy, double* fz,
+                          double* nx, double* ny, double* nz, double* area);
 
 /* Same, but also returns the dealias-grid pointwise force before filtering
  * (fxN..) and the shape coefficients; used by the surrogate data path tests.
@@ -91,6 +97,9 @@ void or_collisions(long nl, const double* zp, const double* area, double dx, dou
 
 /* membmodel.c:81-99 (Skalak) restated: out = W1, W2, dW1/dxi[2], dW2/dxi[2]. */
 void or_skalak(double I1, double I2, const double* I1de, const double* I2de, double gs, double csk, double* out);
+/* membmodel.c:60-99 restated for law 0 (Skalak) or 1 (neo-Hookean). */
+void or_membrane_law(int law, double I1, double I2, const double* I1de, const double* I2de, double gs, double csk,
+                     double* out);
 
 /* Whole step over ncap capsules (interp, forces, spread) with OpenMP over
  * capsules when nthreads>1; returns seconds spent per stage in t[3]. */

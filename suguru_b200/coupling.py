@@ -37,7 +37,7 @@ EXPORTS = ["sg_create", "sg_destroy", "sg_last_error", "sg_synchronize", "sg_int
            "sg_graph_release", "sg_set_capsule_membrane", "sg_capsule_spectra", "sg_surrogate_param_count",
            "sg_surrogate_params", "sg_surrogate_set_linear", "sg_surrogate_train", "sg_surrogate_predict",
            "sg_surrogate_set_trust", "sg_surrogate_last_counts", "sg_set_point_split", "sg_get_point_split",
-           "sg_set_tensor_cores", "sg_set_legendre_terms", "sg_get_legendre_terms"]
+           "sg_set_tensor_cores", "sg_set_legendre_terms", "sg_get_legendre_terms", "sg_set_capsule_law"]
 # test hooks declared in include/sg_testing.h
 TEST_EXPORTS = ["sg_test_legendre", "sg_test_gemm", "sg_test_mlp_grad"]
 WORKLOAD_EXPORTS = ["sg_prescribed_flow"]  # include/sg_workload.h
@@ -94,6 +94,7 @@ def lib():
     L.sg_set_tile_shape.argtypes = [vp, ctypes.c_int]
     L.sg_set_point_split.argtypes = [vp, ctypes.c_int]
     L.sg_set_tensor_cores.argtypes = [vp, ctypes.c_int]
+    L.sg_set_capsule_law.argtypes = [vp, vp]
     L.sg_set_legendre_terms.argtypes = [vp, ctypes.c_int]
     L.sg_get_legendre_terms.argtypes = [vp, ctypes.c_int]
     L.sg_get_point_split.argtypes = [vp]
@@ -321,6 +322,12 @@ class CouplingStep:
     def set_point_split(self, split):
         """Work items per capsule of the persistent pointwise kernels (1..8)."""
         self._check(lib().sg_set_point_split(self._h, int(split)), "sg_set_point_split")
+
+    def set_capsule_law(self, law):
+        """Membrane law per capsule: 0 Skalak, 1 neo-Hookean (membmodel.c:60-99)."""
+        law = np.ascontiguousarray(law, dtype=np.int32)
+        assert law.size == self.degree.size
+        self._check(lib().sg_set_capsule_law(self._h, law.ctypes.data_as(ctypes.c_void_p)), "sg_set_capsule_law")
 
     def set_legendre_terms(self, terms=0):
         """Split mode of the tensor-core Legendre products: 3 (BF16x3), 6 (BF16x6), 0 automatic by degree."""

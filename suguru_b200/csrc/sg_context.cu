@@ -232,7 +232,7 @@ int setup(sg_ctx* c) {
     c->nmax = std::max(c->nmax, gr.N);
     for (size_t q = 0; q < gr.caps.size(); ++q) {
       const int k = gr.caps[q];
-      caps[k].L = gr.L; caps[k].N = gr.N; caps[k].group = (int)gi; caps[k].pad = 0;
+      caps[k].L = gr.L; caps[k].N = gr.N; caps[k].group = (int)gi; caps[k].law = SG_LAW_SKALAK;
       caps[k].pt_off = c->off[k]; caps[k].gidx = (long long)q; caps[k].R = c->radius[k];
       caps[k].gs = cfg.gs; caps[k].csk = cfg.csk;
     }

@@ -174,11 +174,11 @@ struct RowWork {
 
 struct CapInfo {  // per capsule, device
   int L, N, group;
-  int pad;
+  int law;            // membrane law: 0 Skalak (membmodel.c:81-99), 1 neo-Hookean (:60-79)
   long long pt_off;   // first point (global flat index)
   long long gidx;     // index within its degree group
   double R;
-  double gs, csk;     // Skalak shear modulus and area-dilation constant
+  double gs, csk;     // shear modulus and (Skalak) area-dilation constant
 };
 
 struct SpecBuffers {  // per degree group base pointers (T)

@@ -241,7 +241,8 @@ __device__ __forceinline__ void geometry(Geo<T>& G) {
 // law of membmodel.c:81-99 and calculate_cauchy_tensor_deri (sph.f90:1179-1234).
 // A: reference contravariant metric (11,22,12); Ad[al]: its derivatives.
 template <class T>
-__device__ __forceinline__ void mechanics(const Geo<T>& G, const T* A, const T (*Ad)[3], T hf, T csk, T* f) {
+__device__ __forceinline__ void mechanics(const Geo<T>& G, const T* A, const T (*Ad)[3], T hf, T csk, int law,
+                                          T* f) {
   const T A11 = A[0], A22 = A[1], A12 = A[2];
   const T c11 = G.cat[0], c22 = G.cat[1], c12 = G.cat[2];
   const T abs_conA = A11 * A22 - A12 * A12;
@@ -260,8 +261,13 @@ __device__ __forceinline__ void mechanics(const Geo<T>& G, const T* A, const T (
     I2de[al] = abs_conAd * abs_ca + abs_cad * abs_conA;
     Jsde[al] = fdiv(T(0.5), Js) * I2de[al];
   }
-  const T W1 = hf * (T(1) + I1);
-  const T W2 = hf * (csk * I2 - T(1));
+  // strain-energy derivatives: Skalak W1 = hf (1 + I1), W2 = hf (C I2 - 1)
+  // (membmodel.c:81-99); neo-Hookean W1 = hf, W2 = -hf (I2 + 1)^-2
+  // (membmodel.c:60-79, the reference's -DNONHOOK build)
+  const bool nh = law == 1;
+  const T iJ2 = fdiv(T(1), T(1) + I2);  // neo-Hookean: (I2 + 1)^-1
+  const T W1 = nh ? hf : hf * (T(1) + I1);
+  const T W2 = nh ? -hf * iJ2 * iJ2 : hf * (csk * I2 - T(1));
   const T coef1 = fdiv(T(2), Js) * W1, coef2 = T(2) * Js * W2;
   const T a11 = G.conat[0], a22 = G.conat[1], a12 = G.conat[2];
   const T T11 = coef1 * A11 + coef2 * a11;
@@ -270,7 +276,8 @@ __device__ __forceinline__ void mechanics(const Geo<T>& G, const T* A, const T (
   T Td11[2], Td22[2], Td12[2];
 #pragma unroll
   for (int al = 0; al < 2; ++al) {
-    const T W1de = hf * I1de[al], W2de = csk * hf * I2de[al];
+    const T W1de = nh ? T(0) : hf * I1de[al];
+    const T W2de = nh ? (T(2) * hf) * (iJ2 * iJ2 * iJ2) * I2de[al] : csk * hf * I2de[al];
     const T v1 = fdiv(-T(2), Js * Js) * Jsde[al] * W1;
     const T v2 = fdiv(T(2), Js) * W1de;
     const T v3 = fdiv(T(2), Js) * W1;
@@ -337,7 +344,7 @@ __device__ __forceinline__ void synth_m(const T* g, T cm, T sm, T fm, T (&acc)[5
 // perturbation part) and the reference sphere at (st, ct, cp, sp).
 template <class T>
 __device__ __forceinline__ void point_force(const T (&v)[5][3], T st, T ct, T cp, T sp, T R, T hf, T csk,
-                                            bool normals_only, T* f, T* nrm) {
+                                            int law, bool normals_only, T* f, T* nrm) {
   Geo<T> Gm;
   // reference sphere: a1 = x_t, a2 = x_p and second derivatives (sph.f90:84-86)
   Gm.a1[0] = R * (ct * sp); Gm.a1[1] = R * (ct * cp); Gm.a1[2] = -R * st;
@@ -366,7 +373,7 @@ __device__ __forceinline__ void point_force(const T (&v)[5][3], T st, T ct, T cp
     const T iR2 = fdiv(T(1), R * R);
     T A[3] = {iR2, fdiv(iR2, st * st), T(0)};
     T Ad[2][3] = {{T(0), fdiv(-T(2) * ct * iR2, st * st * st), T(0)}, {T(0), T(0), T(0)}};
-    mechanics<T>(Gm, A, Ad, hf, csk, f);
+    mechanics<T>(Gm, A, Ad, hf, csk, law, f);
   }
   nrm[0] = Gm.n[0];
   nrm[1] = Gm.n[1];
@@ -459,8 +466,8 @@ __global__ void __launch_bounds__(256, sizeof(T) == 4 ? 3 : 2) membrane_kernel(c
           const T st = lat[4 * i], ct = lat[4 * i + 1];
           const T cp = sTrig[1 * (H + 1) + j], sp = sTrig[(N + 1) * (H + 1) + j];
           T fa[3], na[3], fb[3], nb[3];
-          point_force<T>(ev, st, ct, cp, sp, R, hf, csk, normals_only, fa, na);
-          point_force<T>(od, st, ct, -cp, -sp, R, hf, csk, normals_only, fb, nb);
+          point_force<T>(ev, st, ct, cp, sp, R, hf, csk, ci.law, normals_only, fa, na);
+          point_force<T>(od, st, ct, -cp, -sp, R, hf, csk, ci.law, normals_only, fb, nb);
           T* o = sOut + r * 6 * (2 * H + 2);
           const T va[6] = {fa[0], fa[1], fa[2], na[0], na[1], na[2]};
           const T vb[6] = {fb[0], fb[1], fb[2], nb[0], nb[1], nb[2]};

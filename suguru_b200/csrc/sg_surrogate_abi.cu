@@ -75,10 +75,12 @@ __global__ void sur_pack_kernel(const CapInfo* __restrict__ caps, const GroupDev
   }
 }
 
-// Residual check per capsule: the surrogate is used when the displacement
-// amplitude |x|, the size of the learned nonlinear residual relative to the
-// linear response |y_mlp| / |y_lin|, and C lie in the validated ranges.
-__global__ void sur_trust_kernel(const int* __restrict__ capids, int n, int din, const float* __restrict__ x,
+// Residual check per capsule: the surrogate is used when the capsule follows
+// the Skalak law it was trained on, and the displacement amplitude |x|, the
+// size of the learned nonlinear residual relative to the linear response
+// |y_mlp| / |y_lin|, and C lie in the validated ranges.
+__global__ void sur_trust_kernel(const CapInfo* __restrict__ caps, const int* __restrict__ capids, int n, int din,
+                                 const float* __restrict__ x,
                                  const float* __restrict__ ylin, const float* __restrict__ y,
                                  const float* __restrict__ ampv, float amp_max, float ratio_max, float c_min,
                                  float c_max, int* __restrict__ flag, int* __restrict__ count) {
@@ -105,7 +107,8 @@ __global__ void sur_trust_kernel(const int* __restrict__ capids, int n, int din,
   if (t == 0) {
     const float amp = ampv[b], lin = sqrtf(red[0][0]), res = sqrtf(red[1][0]);
     const float C = xb[0];
-    const bool ok = amp <= amp_max && res <= ratio_max * lin && C >= c_min && C <= c_max;
+    const bool ok = caps[capids[b]].law == SG_LAW_SKALAK && amp <= amp_max && res <= ratio_max * lin &&
+                    C >= c_min && C <= c_max;
     flag[capids[b]] = ok ? 1 : 0;
     atomicAdd(&count[ok ? 0 : 1], 1);
   }
@@ -266,7 +269,7 @@ int sur_step_pre(sg_ctx* c) {
   SG_TRY(sur_forward(s, n, c->d_err, c->st), "surrogate forward");
   SG_TRY(sur_linear(s, c->d_sur_x, n, c->d_sur_ylin, c->d_err, c->st), "surrogate linear");
   SG_TRY(sur_combine(s, c->d_sur_ylin, s.yhat, s.amp, n, 1, 1, c->d_sur_y, c->st), "surrogate combine");
-  sur_trust_kernel<<<n, 128, 0, c->st>>>(c->d_sur_caps, n, s.din, c->d_sur_x, c->d_sur_ylin, c->d_sur_y, s.amp,
+  sur_trust_kernel<<<n, 128, 0, c->st>>>(c->d_caps, c->d_sur_caps, n, s.din, c->d_sur_x, c->d_sur_ylin, c->d_sur_y, s.amp,
                                          c->sur_trust[0], c->sur_trust[1], c->sur_trust[2], c->sur_trust[3],
                                          c->d_sur_flag, c->d_sur_count);
   SG_TRY(cudaGetLastError(), "surrogate check");
@@ -366,6 +369,18 @@ int sg_set_capsule_membrane(sg_ctx* c, const double* gs, const double* csk) {
     }
     if (csk) c->h_caps[k].csk = csk[k];
   }
+  SG_TRY(cudaStreamSynchronize(c->st), "synchronize");
+  SG_TRY(cudaMemcpy(c->d_caps, c->h_caps.data(), sizeof(CapInfo) * c->h_caps.size(), cudaMemcpyHostToDevice),
+         "upload");
+  return SG_OK;
+}
+
+int sg_set_capsule_law(sg_ctx* c, const int* law) {
+  if (!c || !law) return SG_ERR_ARG;
+  if (c->graph) return fail(c, SG_ERR_STATE, "release the captured graph first");
+  for (int k = 0; k < c->cfg.ncap; ++k)
+    if (law[k] != SG_LAW_SKALAK && law[k] != SG_LAW_NEO_HOOKEAN) return fail(c, SG_ERR_ARG, "unknown membrane law");
+  for (int k = 0; k < c->cfg.ncap; ++k) c->h_caps[k].law = law[k];
   SG_TRY(cudaStreamSynchronize(c->st), "synchronize");
   SG_TRY(cudaMemcpy(c->d_caps, c->h_caps.data(), sizeof(CapInfo) * c->h_caps.size(), cudaMemcpyHostToDevice),
          "upload");

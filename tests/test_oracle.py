@@ -143,6 +143,32 @@ def test_skalak_matches_reference_membmodel():
         assert np.allclose(mine, [w1[0], w2[0], w1d[0], w1d[1], w2d[0], w2d[1]], rtol=1e-15, atol=0)
 
 
+def test_neo_hookean_matches_reference_membmodel():
+    """The restated neo-Hookean law against the reference's own membmodel.c
+    compiled with -DNONHOOK (its default build; oracle/_ref)."""
+    ref = O.ref_membmodel("nh")
+    if ref is None:
+        pytest.skip("oracle/_ref not built (reference tree absent)")
+    import ctypes
+    dp = ctypes.POINTER(ctypes.c_double)
+    rng = np.random.default_rng(1)
+    for _ in range(50):
+        gs, csk = rng.uniform(0.2, 3), rng.uniform(0.5, 50)
+        I1, I2 = rng.normal(0, 0.3), rng.uniform(-0.5, 0.8)
+        I1de, I2de = rng.normal(size=2), rng.normal(size=2)
+        ref.ref_set_hf_gscell(0.5 * gs)  # sph.f90:35
+        w1, w2 = np.zeros(1), np.zeros(1)
+        w1d, w2d = np.zeros(2), np.zeros(2)
+        args = [np.array([gs]), np.array([csk]), np.array([I1]), np.array([I2]), I1de.copy(), I2de.copy()]
+        ref.calpwspi_deri_(w1.ctypes.data_as(dp), w2.ctypes.data_as(dp), w1d.ctypes.data_as(dp),
+                           w2d.ctypes.data_as(dp), *[a.ctypes.data_as(dp) for a in args])
+        mine = O.membrane_law(1, I1, I2, I1de, I2de, gs, csk)
+        assert np.allclose(mine, [w1[0], w2[0], w1d[0], w1d[1], w2d[0], w2d[1]], rtol=1e-15, atol=0)
+        # law 0 through the same entry point is the Skalak law
+        assert np.array_equal(O.membrane_law(0, I1, I2, I1de, I2de, gs, csk),
+                              O.skalak(I1, I2, I1de, I2de, gs, csk))
+
+
 L15 = 15
 
 
@@ -167,6 +193,23 @@ def test_uniform_dilation_laplace_law(lam, csk):
     r = lam * R
     xh = np.stack([x - 1, y - 1, z - 1]) / r
     assert np.abs(f + (2 * tau / r) * xh).max() < 1e-8 * abs(2 * tau / r) + 1e-8
+
+
+@pytest.mark.parametrize("lam", [0.9, 1.05, 1.2])
+def test_uniform_dilation_neo_hookean(lam):
+    """Neo-Hookean isotropic stretch: W1 = Gs/2, W2 = -Gs/2 (I2+1)^-2 with I2 = l^4 - 1,
+    so T = Gs (l^-2 - l^-8) A, tau = T:a / 2 = Gs (1 - l^-6) and f = 2 tau / r (inward);
+    a sphere at the reference radius carries no force."""
+    R, gs = 0.25, 1.3
+    x, y, z = W.capsule_points(L15, lam * R, (1.0, 1.0, 1.0))
+    f, n, a = O.complagrforces(L15, R, x, y, z, gs=gs, csk=7.0, law=1)  # C plays no part
+    tau = gs * (1 - lam ** -6)
+    r = lam * R
+    xh = np.stack([x - 1, y - 1, z - 1]) / r
+    assert np.abs(f + (2 * tau / r) * xh).max() < 1e-8 * abs(2 * tau / r) + 1e-8
+    x0, y0, z0 = W.capsule_points(L15, R, (1.0, 1.0, 1.0))
+    f0, _, _ = O.complagrforces(L15, R, x0, y0, z0, gs=gs, law=1)
+    assert np.abs(f0).max() < 1e-9
 
 
 def test_translation_noise_floor():
