@@ -374,11 +374,14 @@ int setup(sg_ctx* c) {
         const LegProblem& p = P[r];
         for (int m = 0; m < p.M; ++m)
           for (int q0 = 0; q0 < p.Q; q0 += 128) WF.push_back(LegWork{r, m, q0});
-        int chain[3] = {r, p.next[0], p.next[1]};
-        for (int q : chain) {
+        const int chain[3] = {r, p.next[0], p.next[0] >= 0 ? p.next[1] : -1};
+        LegLevels& lv = c->lvF[f];
+        for (int l = 0; l < 3; ++l) {
+          const int q = chain[l];
           if (q < 0) continue;
-          c->maxJpF[f] = std::max(c->maxJpF[f], P[q].Jp);
-          c->maxKpF[f] = std::max(c->maxKpF[f], P[q].Kp);
+          lv.jp[l] = std::max(lv.jp[l], P[q].Jp);
+          lv.kp[l] = std::max(lv.kp[l], P[q].Kp);
+          lv.a_kp = std::max(lv.a_kp, P[q].Kp);
         }
       }
       c->nlwF[f] = (int)WF.size();
@@ -456,8 +459,8 @@ int dev_legendre(sg_ctx* c, int s) {
     // stages 0, 2, 4 launch the chained products; 1, 3, 5 ran inside them
     if (s % 2) return SG_OK;
     const int f = s / 2;
-    SG_TRY(launch_legendre_mma(c->d_probs, c->d_lwF[f], c->nlwF[f], c->maxJpF[f], c->maxKpF[f], c->leg_parts,
-                               c->d_err, c->num_sms, c->st),
+    SG_TRY(launch_legendre_mma(c->d_probs, c->d_lwF[f], c->nlwF[f], c->lvF[f], c->leg_parts, c->d_err,
+                               c->num_sms, c->st),
            "legendre (tensor cores)");
     c->launches += 1;
   } else {

@@ -32,6 +32,7 @@ struct sg_ctx {
   using RowWork = sg::RowWork;
   using LegProblem = sg::LegProblem;
   using LegWork = sg::LegWork;
+  using LegLevels = sg::LegLevels;
   sg_config cfg{};
   std::vector<int> degree;
   std::vector<double> radius;
@@ -66,7 +67,7 @@ struct sg_ctx {
   std::vector<LegProblem> h_probs;    // host copy of d_probs (the split mode is rewritten in place)
   LegWork* d_lwF[3] = {};  // root work items of the three chained launches
   int nlwF[3] = {};
-  int maxJpF[3] = {}, maxKpF[3] = {};
+  LegLevels lvF[3] = {};    // shared-memory sizes of the three chained launches
   int num_sms = 148;
   int* d_err = nullptr;   // device error flag (bounded waits that expired)
   int* h_err = nullptr;   // pinned copy, refreshed at the end of every step

@@ -154,81 +154,64 @@ __global__ void bin_scatter_kernel(IBGrid g, long n, const PosRec<T>* __restrict
 }
 
 // ------------------------------------------------------------------ interp
-// eulr2lagr hot loop (interp_spread.f90:335-378) as a per-point gather in the
-// reference's point order (consecutive points share cache lines).  u sits at
-// faces i*dx (kernel(i-c)), cell centres at (i-0.5)dx (kernel(i-0.5-c)); each
-// component has 3 x 3 x 3 nonzero weights, face weights along its own
-// direction and centre weights along the other two (delta3_face/_centre).
-// z-levels outside [1,kmax] are skipped (interp_spread.f90:346-351).
+// eulr2lagr hot loop (interp_spread.f90:335-378) as a gather: one thread per
+// (component, point), component-major, so that a warp takes 32 consecutive
+// points (consecutive points share cache lines) of one component and each
+// thread keeps only its component's 27 loads in flight.  u sits at faces i*dx
+// (kernel(i-c)), cell centres at (i-0.5)dx (kernel(i-0.5-c)); each component
+// has 3 x 3 x 3 nonzero weights, face weights along its own direction and
+// centre weights along the other two (delta3_face/_centre).  z-levels outside
+// [1,kmax] are skipped (interp_spread.f90:346-351).
 template <class T>
 __global__ void __launch_bounds__(256) interp_kernel(IBGrid g, long n, const PosRec<T>* __restrict__ pos,
                                                      const T* __restrict__ u, const T* __restrict__ v,
                                                      const T* __restrict__ w, T* __restrict__ U, T* __restrict__ V,
                                                      T* __restrict__ W) {
-  const long p = (long)blockIdx.x * blockDim.x + threadIdx.x;
-  if (p >= n) return;
+  const long t = (long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= 3 * n) return;
+  const int c = (int)(t / n);
+  const long p = t - (long)c * n;
   const PosRec<T> rec = pos[p];
-  const int bb[3] = {rec.b[0], rec.b[1], rec.b[2]};
-  const T fr[3] = {rec.f[0], rec.f[1], rec.f[2]};
-  T wF[3][3], wC[3][3];
-  bool hi[3];
+  // weights along each dimension: face weights along c (nearest face node
+  // o = hi, nodes o = hi-1 .. hi+1), centre weights otherwise (o = 0..2)
+  T wt[3][3];
+  int o0[3];  // first node offset (o) per dimension
 #pragma unroll
   for (int d = 0; d < 3; ++d) {
-    delta3_face<T>(fr[d], wF[d], hi[d]);
-    delta3_centre<T>(fr[d], wC[d]);
-  }
-  // storage offsets of the stencil nodes o = -1..2 per dimension, then of
-  // the face nodes (o = hi-1 .. hi+1) and the centres (o = 0..2).  z-levels
-  // outside [1,kmax] are read at the nearest level inside and weighted by
-  // zero, so that all 81 loads are independent (no branch between them).
-  // (32-bit: make_ib_grid caps the field at 2^31 - 1 elements)
-  int o4[3][4];
-  T zin4[4];
-#pragma unroll
-  for (int t = 0; t < 4; ++t) {
-    o4[0][t] = wrap_near(bb[0] + t - 1, g.itot);
-    o4[1][t] = g.ldi * wrap_near(bb[1] + t - 1, g.jtot);
-    const int k = bb[2] + t - 1;
-    const bool kin = k >= 1 && k <= g.ktot;
-    zin4[t] = kin ? T(1) : T(0);
-    o4[2][t] = g.ldi * g.ldj * (k < 1 ? 1 : (k > g.ktot ? g.ktot : k));
-  }
-  int oF[3][3], oC[3][3];
-#pragma unroll
-  for (int d = 0; d < 3; ++d)
-#pragma unroll
-    for (int t = 0; t < 3; ++t) {
-      oF[d][t] = hi[d] ? o4[d][t + 1] : o4[d][t];
-      oC[d][t] = o4[d][t + 1];
+    if (d == c) {
+      bool hi;
+      delta3_face<T>(rec.f[d], wt[d], hi);
+      o0[d] = hi ? 0 : -1;
+    } else {
+      delta3_centre<T>(rec.f[d], wt[d]);
+      o0[d] = 0;
     }
-#pragma unroll
-  for (int t = 0; t < 3; ++t) {
-    wF[2][t] *= hi[2] ? zin4[t + 1] : zin4[t];
-    wC[2][t] *= zin4[t + 1];
   }
-  T out[3];
+  // storage offsets of the three nodes per dimension (periodic x, y; z read
+  // at the nearest level inside [1, kmax] and weighted by zero outside, so
+  // that the 27 loads are independent; 32-bit: make_ib_grid caps the field
+  // at 2^31 - 1 elements)
+  int ox[3], oy[3], oz[3];
 #pragma unroll
-  for (int c = 0; c < 3; ++c) {
-    const T* src = c == 0 ? u : (c == 1 ? v : w);
-    T sum = T(0);
+  for (int q = 0; q < 3; ++q) {
+    ox[q] = wrap_near(rec.b[0] + o0[0] + q, g.itot);
+    oy[q] = g.ldi * wrap_near(rec.b[1] + o0[1] + q, g.jtot);
+    const int k = rec.b[2] + o0[2] + q;
+    if (k < 1 || k > g.ktot) wt[2][q] = T(0);
+    oz[q] = g.ldi * g.ldj * (k < 1 ? 1 : (k > g.ktot ? g.ktot : k));
+  }
+  const T* src = c == 0 ? u : (c == 1 ? v : w);
+  T sum = T(0);
 #pragma unroll
-    for (int tz = 0; tz < 3; ++tz) {
-      const int zo = (c == 2) ? oF[2][tz] : oC[2][tz];
-      const T wz = (c == 2) ? wF[2][tz] : wC[2][tz];
+  for (int tz = 0; tz < 3; ++tz)
 #pragma unroll
-      for (int ty = 0; ty < 3; ++ty) {
-        const T wyz = ((c == 1) ? wF[1][ty] : wC[1][ty]) * wz;
-        const T* row = src + zo + ((c == 1) ? oF[1][ty] : oC[1][ty]);
+    for (int ty = 0; ty < 3; ++ty) {
+      const T wyz = wt[1][ty] * wt[2][tz];
+      const T* row = src + oz[tz] + oy[ty];
 #pragma unroll
-        for (int tx = 0; tx < 3; ++tx)
-          sum += row[(c == 0) ? oF[0][tx] : oC[0][tx]] * (((c == 0) ? wF[0][tx] : wC[0][tx]) * wyz);
-      }
+      for (int tx = 0; tx < 3; ++tx) sum += row[ox[tx]] * (wt[0][tx] * wyz);
     }
-    out[c] = sum;
-  }
-  U[p] = out[0];
-  V[p] = out[1];
-  W[p] = out[2];
+  (c == 0 ? U : (c == 1 ? V : W))[p] = sum;
 }
 
 // ------------------------------------------------------------------ launchers
@@ -250,7 +233,8 @@ template <class T>
 cudaError_t launch_interp(const IBGrid& g, long n, const IBWork& w, const T* u, const T* v, const T* ww, T* U, T* V,
                           T* W, cudaStream_t st) {
   if (n <= 0) return cudaSuccess;
-  interp_kernel<T><<<(unsigned)((n + 255) / 256), 256, 0, st>>>(g, n, (const PosRec<T>*)w.pos, u, v, ww, U, V, W);
+  interp_kernel<T><<<(unsigned)((3 * n + 255) / 256), 256, 0, st>>>(g, n, (const PosRec<T>*)w.pos, u, v, ww, U, V,
+                                                                     W);
   return cudaGetLastError();
 }
 

@@ -121,11 +121,20 @@ struct LegWork {  // one tile of a problem
 template <class T>
 cudaError_t launch_legendre(const LegProblem* d_probs, const LegWork* d_work, int nwork, int maxJ, int maxK,
                             cudaStream_t st);
+// Shared-memory sizes of one tensor-core launch: for each chain level (0 the
+// root problems, 1 their next[0], 2 their next[1]) the largest padded J and K
+// of its problems (0 for a level no chain reaches), and the largest padded K
+// of any data operand.
+struct LegLevels {
+  int jp[3], kp[3];
+  int a_kp;
+};
 // Tensor-core (tcgen05, BF16x3 / BF16x6) contraction of FP32 problems; work
-// items are 128-row tiles.  nparts = 3 if any problem reached is BF16x6, else
-// 2.  d_err is set to 1 if an MMA completion wait times out, 2 if a problem's
-// mode does not fit nparts or differs along a chain.
-cudaError_t launch_legendre_mma(const LegProblem* d_probs, const LegWork* d_work, int nwork, int maxJp, int maxKp,
+// items are 128-row tiles of root problems and their chains.  nparts = 3 if
+// any problem reached is BF16x6, else 2.  d_err is set to 1 if an MMA or a
+// table copy wait times out, 2 if a problem does not fit the sizes of lv and
+// nparts or its mode differs along a chain.
+cudaError_t launch_legendre_mma(const LegProblem* d_probs, const LegWork* d_work, int nwork, const LegLevels& lv,
                                 int nparts, int* d_err, int num_sms, cudaStream_t st);
 // Dense product on the tensor cores (sg_gemm.cu):
 //   C = alpha A B^T (+ bias[n]) (then GELU), A [M][K], B [N][K], K % 64 == 0.

@@ -48,7 +48,9 @@ using namespace umma;
 
 namespace {
 
-// bf16 parts of the data (A) and table (B) operands in shared memory
+// bf16 parts of the data operand (A) in shared memory, and the table (B)
+// region of each chain level (its parts follow one another at the level's
+// problem's own stride Jp Kp, as in the global image)
 struct Operands {
   uint16_t* a[3];
   uint16_t* b[3];
@@ -56,21 +58,13 @@ struct Operands {
 
 __device__ __forceinline__ int parts_of(const LegProblem& P) { return P.terms == 6 ? 3 : 2; }
 
-// B_m image of problem P (already split and laid out): a straight 16-byte copy
-// of the parts its mode reads
-__device__ __forceinline__ void stage_table(const LegProblem& P, int m, const Operands& op, int tid) {
-  const uint4* src = (const uint4*)((const uint16_t*)P.Bimg + (long long)m * P.sBimg);
-  const int n16 = (P.Jp * P.Kp) >> 3;  // uint4 per image
-  uint4* d0 = (uint4*)op.b[0];
-  uint4* d1 = (uint4*)op.b[1];
-  for (int i = tid; i < n16; i += 128) {
-    d0[i] = src[i];
-    d1[i] = src[n16 + i];
-  }
-  if (parts_of(P) == 3) {
-    uint4* d2 = (uint4*)op.b[2];
-    for (int i = tid; i < n16; i += 128) d2[i] = src[2 * n16 + i];
-  }
+// The B_m image of problem P (the parts its mode reads, contiguous in the
+// global image) into its level's region: one bulk copy on the TMA engine,
+// completing on the level's mbarrier.  Issued by one thread.
+__device__ __forceinline__ void fetch_table(const LegProblem& P, int m, uint16_t* dst, uint64_t* bar) {
+  const uint16_t* src = (const uint16_t*)P.Bimg + (long long)m * P.sBimg;
+  const uint32_t bytes = (uint32_t)(parts_of(P) * P.Jp * P.Kp) * 2u;
+  bulk_g2s(dst, src, bytes, bar);
 }
 
 // Eight consecutive K values of one data row, split into the operand parts.
@@ -83,14 +77,15 @@ __device__ __forceinline__ void store_split(const float* x, int np, const Operan
 }
 
 // One thread issues the split products of every K step of 16 (largest terms
-// first), then commits.
+// first), then commits.  bt: the level's table region.
 __device__ __forceinline__ void issue_mma(const LegProblem& P, int m, uint32_t tmem, const Operands& op,
-                                          uint64_t* bar) {
+                                          const uint16_t* bt, uint64_t* bar) {
   const uint32_t idesc = idesc_bf16(MMA_M, P.Jp);
   const uint32_t lbo = 128, sbo = (uint32_t)P.Kp * 16;
-  const uint32_t a0 = smem_u32(op.a[0]), a1 = smem_u32(op.a[1]), b0 = smem_u32(op.b[0]), b1 = smem_u32(op.b[1]);
+  const uint32_t pb = (uint32_t)(P.Jp * P.Kp) * 2u;  // bytes per table part
+  const uint32_t a0 = smem_u32(op.a[0]), a1 = smem_u32(op.a[1]), b0 = smem_u32(bt), b1 = b0 + pb;
   const bool six = P.terms == 6;
-  const uint32_t a2 = six ? smem_u32(op.a[2]) : 0u, b2 = six ? smem_u32(op.b[2]) : 0u;
+  const uint32_t a2 = six ? smem_u32(op.a[2]) : 0u, b2 = b0 + 2u * pb;
   const int s0 = P.tri ? (m >> 4) : 0;  // synthesis: coefficients below n = m vanish
   uint32_t acc = 0;
   for (int s = s0; s < (P.Kp >> 4); ++s) {
@@ -116,26 +111,29 @@ __device__ __forceinline__ void issue_mma(const LegProblem& P, int m, uint32_t t
 // the next product's bf16 hi/lo operand tile in shared memory, so the data
 // never leaves the SM between the two contractions.
 // A chain runs in its root's mode (one degree group: the same mode throughout).
-// smem: nparts A parts (128 x maxKp each), then nparts B parts (maxJp x maxKp
-// each), bf16; nparts = 3 when any problem of the launch is BF16x6, else 2.
+// smem (bf16): nparts A parts of 128 x lv.a_kp, then for each chain level l a
+// table region of nparts x lv.jp[l] x lv.kp[l]; nparts = 3 when any problem of
+// the launch is BF16x6, else 2.  At the start of a work item one thread issues
+// the bulk copies of every level's table (each on its own mbarrier), so they
+// overlap the staging of the data rows and the earlier products.
 __global__ void __launch_bounds__(128) legendre_mma_kernel(const LegProblem* __restrict__ probs,
-                                                           const LegWork* __restrict__ work, int nwork, int maxJp,
-                                                           int maxKp, int nparts, int tmem_cols,
-                                                           int* __restrict__ err) {
+                                                           const LegWork* __restrict__ work, int nwork, LegLevels lv,
+                                                           int nparts, int tmem_cols, int* __restrict__ err) {
   extern __shared__ __align__(128) unsigned char smem_raw[];
   __shared__ __align__(8) uint64_t s_bar;
+  __shared__ __align__(8) uint64_t s_tbar[3];
   __shared__ uint32_t s_tmem;
   Operands op;
   {
     uint16_t* p = (uint16_t*)smem_raw;
     for (int i = 0; i < 3; ++i) {
       op.a[i] = p;
-      if (i + 1 < nparts) p += MMA_M * maxKp;
+      if (i + 1 < nparts) p += MMA_M * lv.a_kp;
     }
-    p = (uint16_t*)smem_raw + nparts * MMA_M * maxKp;
-    for (int i = 0; i < 3; ++i) {
-      op.b[i] = p;
-      if (i + 1 < nparts) p += maxJp * maxKp;
+    p = (uint16_t*)smem_raw + nparts * MMA_M * lv.a_kp;
+    for (int l = 0; l < 3; ++l) {
+      op.b[l] = p;
+      p += nparts * lv.jp[l] * lv.kp[l];
     }
   }
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
@@ -143,12 +141,17 @@ __global__ void __launch_bounds__(128) legendre_mma_kernel(const LegProblem* __r
   if (warp == 0) {
     tmem_alloc(&s_tmem, (uint32_t)tmem_cols);
   }
-  if (tid == 0) mbar_init(&s_bar, 1);
+  if (tid == 0) {
+    mbar_init(&s_bar, 1);
+    for (int l = 0; l < 3; ++l) mbar_init(&s_tbar[l], 1);
+  }
   fence_before();
   __syncthreads();
   fence_after();
   const uint32_t tmem = s_tmem;
-  uint32_t phase = 0;
+  uint32_t phase = 0;             // MMA commits
+  uint32_t tphase[3] = {0, 0, 0};  // table copies, per level (a level completes one phase per item using it)
+  int pending = 0;                 // levels whose copy was issued and not yet waited for (thread 0)
   bool ok = true;
 
   for (int it = blockIdx.x; it < nwork && ok; it += gridDim.x) {
@@ -158,36 +161,53 @@ __global__ void __launch_bounds__(128) legendre_mma_kernel(const LegProblem* __r
     const LegProblem& R = probs[pid];
     const int nq = min(MMA_M, R.Q - q0);
     const int np = parts_of(R);
-    if (np > nparts) {  // the launch's shared memory holds fewer parts (uniform per CTA)
+    // the chain: level 0 the root, 1 its next[0], 2 its next[1] (only after a level 1)
+    const int chain[3] = {pid, R.next[0], R.next[0] >= 0 ? R.next[1] : -1};
+    bool fits = np <= nparts;
+    for (int l = 0; l < 3; ++l)
+      if (chain[l] >= 0) {
+        const LegProblem& P = probs[chain[l]];
+        fits = fits && parts_of(P) == np && P.Jp <= lv.jp[l] && P.Kp <= lv.kp[l] && P.Kp <= lv.a_kp;
+      }
+    if (!fits) {  // the launch's shared memory was sized for other problems (uniform per CTA)
       if (tid == 0) atomicExch(err, 2);
       continue;
     }
-    stage_table(R, m, op, tid);
-    // ---- data rows of the root: FP32 -> bf16 parts, one 8-element
-    // core-matrix row per thread and step; consecutive threads take
-    // consecutive rows
+    if (tid == 0) {
+      fence_async_smem();  // earlier generic accesses of the regions before the async copies
+      for (int l = 0; l < 3; ++l)
+        if (chain[l] >= 0) {
+          fetch_table(probs[chain[l]], m, op.b[l], &s_tbar[l]);
+          pending |= 1 << l;
+        }
+    }
+    // ---- data rows of the root: FP32 -> bf16 parts.  Thread q stages row q
+    // of the tile; all of its loads (up to 8 core-matrix rows of 8 values)
+    // are issued before any is split and stored, so their latencies overlap.
     {
-      const int K = R.K, KC = R.Kp >> 3;
-      const float* A = (const float*)R.A;
-      for (int idx = tid; idx < MMA_M * KC; idx += 128) {
-        const int kc = idx >> 7, q = idx & 127, k0 = kc << 3;
-        float x[8];
-        if (q < nq) {
-          const int qq = q0 + q, c = qq / R.rpc, r = qq - c * R.rpc;
-          const float* row = A + (long long)c * R.sAc + (long long)r * R.sAr + (long long)m * R.sAm;
-          if (R.vecA && k0 + 8 <= K) {
+      const int K = R.K, KC = R.Kp >> 3, q = tid;
+      const float* row = nullptr;
+      if (q < nq) {
+        const int qq = q0 + q, c = qq / R.rpc, r = qq - c * R.rpc;
+        row = (const float*)R.A + (long long)c * R.sAc + (long long)r * R.sAr + (long long)m * R.sAm;
+      }
+      for (int kc0 = 0; kc0 < KC; kc0 += 8) {
+        float x[8][8];
+#pragma unroll
+        for (int u = 0; u < 8; ++u) {
+          const int k0 = (kc0 + u) << 3;
+          if (row && kc0 + u < KC && R.vecA && k0 + 8 <= K) {
             const float4 a = *(const float4*)(row + k0), b = *(const float4*)(row + k0 + 4);
-            x[0] = a.x; x[1] = a.y; x[2] = a.z; x[3] = a.w;
-            x[4] = b.x; x[5] = b.y; x[6] = b.z; x[7] = b.w;
+            x[u][0] = a.x; x[u][1] = a.y; x[u][2] = a.z; x[u][3] = a.w;
+            x[u][4] = b.x; x[u][5] = b.y; x[u][6] = b.z; x[u][7] = b.w;
           } else {
 #pragma unroll
-            for (int i = 0; i < 8; ++i) x[i] = (k0 + i < K) ? row[k0 + i] : 0.f;
+            for (int i = 0; i < 8; ++i) x[u][i] = (row && kc0 + u < KC && k0 + i < K) ? row[k0 + i] : 0.f;
           }
-        } else {
-#pragma unroll
-          for (int i = 0; i < 8; ++i) x[i] = 0.f;
         }
-        store_split(x, np, op, cm_offset(q, kc, KC));
+#pragma unroll
+        for (int u = 0; u < 8; ++u)
+          if (kc0 + u < KC) store_split(x[u], np, op, cm_offset(q, kc0 + u, KC));
       }
     }
     // ---- the root, then its chained products: one MMA group per problem
@@ -197,7 +217,17 @@ __global__ void __launch_bounds__(128) legendre_mma_kernel(const LegProblem* __r
       fence_before();
       __syncthreads();
       fence_after();
-      if (tid == 0) issue_mma(P, m, tmem, op, &s_bar);
+      if (tid == 0) {
+        // the level's table has landed (bounded wait; on timeout the MMA wait
+        // below runs out too and the CTA leaves with the error flag set)
+        const bool landed = mbar_wait(&s_tbar[level], tphase[level]);
+        pending &= ~(1 << level);
+        tphase[level] ^= 1u;
+        if (landed)
+          issue_mma(P, m, tmem, op, op.b[level], &s_bar);
+        else
+          atomicExch(err, 1);
+      }
       __syncwarp();
       // every thread waits; the CTA then agrees on the outcome so that all of
       // its threads leave the loop together on a timeout
@@ -257,15 +287,10 @@ __global__ void __launch_bounds__(128) legendre_mma_kernel(const LegProblem* __r
       } else {
         break;
       }
-      if (parts_of(probs[pid]) != np) {  // a chain keeps its root's mode
-        if (tid == 0) atomicExch(err, 2);
-        break;
-      }
       // all TMEM reads and operand writes are done before the next MMA
       fence_before();
       __syncthreads();
       fence_after();
-      stage_table(probs[pid], m, op, tid);
     }
     fence_before();
     __syncthreads();  // TMEM reads and smem operands done before the next tile
@@ -273,8 +298,12 @@ __global__ void __launch_bounds__(128) legendre_mma_kernel(const LegProblem* __r
   }
   if (!ok) {
     // a commit that never arrived: give the tensor core a bounded chance to
-    // finish before freeing its accumulator
+    // finish before freeing its accumulator, and the table copies still in
+    // flight a bounded chance to land before the shared memory is released
     mbar_wait(&s_bar, phase);
+    if (tid == 0)
+      for (int l = 0; l < 3; ++l)
+        if (pending & (1 << l)) mbar_wait(&s_tbar[l], tphase[l]);
   }
   fence_before();
   __syncthreads();
@@ -282,21 +311,29 @@ __global__ void __launch_bounds__(128) legendre_mma_kernel(const LegProblem* __r
   if (warp == 0) tmem_free(tmem, (uint32_t)tmem_cols);
 }
 
-size_t legendre_mma_smem(int maxJp, int maxKp, int nparts) {
-  return (size_t)nparts * sizeof(uint16_t) * (MMA_M + maxJp) * maxKp;
+size_t legendre_mma_smem(const LegLevels& lv, int nparts) {
+  size_t e = (size_t)MMA_M * lv.a_kp;
+  for (int l = 0; l < 3; ++l) e += (size_t)lv.jp[l] * lv.kp[l];
+  return (size_t)nparts * sizeof(uint16_t) * e;
 }
 
-cudaError_t launch_legendre_mma(const LegProblem* d_probs, const LegWork* d_work, int nwork, int maxJp, int maxKp,
+cudaError_t launch_legendre_mma(const LegProblem* d_probs, const LegWork* d_work, int nwork, const LegLevels& lv,
                                 int nparts, int* d_err, int num_sms, cudaStream_t st) {
   if (nwork <= 0) return cudaSuccess;
-  if (maxJp < 16 || maxJp > 256 || (maxJp & 15) || maxKp < 16 || (maxKp & 15)) return cudaErrorInvalidValue;
+  int maxJp = 0;
+  for (int l = 0; l < 3; ++l) {
+    if (lv.jp[l] < 0 || lv.jp[l] > 256 || (lv.jp[l] & 15) || lv.kp[l] < 0 || (lv.kp[l] & 15))
+      return cudaErrorInvalidValue;
+    maxJp = lv.jp[l] > maxJp ? lv.jp[l] : maxJp;
+  }
+  if (lv.jp[0] < 16 || lv.kp[0] < 16 || lv.a_kp < 16 || (lv.a_kp & 15)) return cudaErrorInvalidValue;
   if (nparts != 2 && nparts != 3) return cudaErrorInvalidValue;
   // TMEM columns: a power of two >= 32 covering N = Jp; CTAs per SM limited
   // (through shared memory) so that their allocations always fit in 512 columns
   int cols = 32;
   while (cols < maxJp) cols <<= 1;
   const int per_sm = 512 / cols < 4 ? 512 / cols : 4;
-  size_t smem = legendre_mma_smem(maxJp, maxKp, nparts);
+  size_t smem = legendre_mma_smem(lv, nparts);
   // (per_sm + 1) CTAs of this size exceed the SM's 228 KB of shared memory
   const size_t floor_smem = (size_t)(228 * 1024) / (size_t)(per_sm + 1);
   if (smem < floor_smem) smem = floor_smem;
@@ -304,7 +341,7 @@ cudaError_t launch_legendre_mma(const LegProblem* d_probs, const LegWork* d_work
   cudaError_t e = cudaFuncSetAttribute(legendre_mma_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   if (e != cudaSuccess) return e;
   const int grid = nwork < num_sms * per_sm ? nwork : num_sms * per_sm;
-  legendre_mma_kernel<<<grid, 128, smem, st>>>(d_probs, d_work, nwork, maxJp, maxKp, nparts, cols, d_err);
+  legendre_mma_kernel<<<grid, 128, smem, st>>>(d_probs, d_work, nwork, lv, nparts, cols, d_err);
   return cudaGetLastError();
 }
 

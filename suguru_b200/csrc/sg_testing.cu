@@ -69,11 +69,16 @@ extern "C" int sg_test_legendre(int tensor_cores, int M, int Q, int J, int K, in
         ok(cudaMemcpy(dP, &p, sizeof(p), cudaMemcpyHostToDevice)) &&
         ok(cudaMemcpy(dW, work.data(), sizeof(LegWork) * work.size(), cudaMemcpyHostToDevice)) &&
         ok(cudaMemset(dE, 0, sizeof(int))) && ok(cudaMemset(dD, 0xff, 4 * nd))) {
-      if (tensor_cores)
-        ok(launch_legendre_mma((const LegProblem*)dP, (const LegWork*)dW, (int)work.size(), Jp, Kp,
-                                terms == 6 ? 3 : 2, (int*)dE, sms, 0));
-      else
+      if (tensor_cores) {
+        LegLevels lv{};
+        lv.jp[0] = Jp;
+        lv.kp[0] = Kp;
+        lv.a_kp = Kp;
+        ok(launch_legendre_mma((const LegProblem*)dP, (const LegWork*)dW, (int)work.size(), lv, terms == 6 ? 3 : 2,
+                               (int*)dE, sms, 0));
+      } else {
         ok(launch_legendre<float>((const LegProblem*)dP, (const LegWork*)dW, (int)work.size(), J, K, 0));
+      }
       int err = 0;
       if (ok(cudaDeviceSynchronize()) && ok(cudaMemcpy(&err, dE, sizeof(int), cudaMemcpyDeviceToHost)) &&
           ok(cudaMemcpy(D, dD, 4 * nd, cudaMemcpyDeviceToHost)))
