@@ -47,7 +47,6 @@ struct sg_ctx {
   CapInfo* d_caps = nullptr;
   std::vector<CapInfo> h_caps;
   GroupDev* d_groups = nullptr;
-  double* d_cen = nullptr;
   RowWork* d_wpos = nullptr;
   RowWork* d_wmem = nullptr;
   RowWork* d_wsh = nullptr;

@@ -212,11 +212,8 @@ struct GroupDev {  // device copy of per-group constants; [0] double, [1] float
 };
 
 template <class T>
-cudaError_t launch_centroid(int ncap, const CapInfo* caps, const double* X, const double* Y, const double* Z,
-                            double* cen, cudaStream_t st);
-template <class T>
 cudaError_t launch_posfwd(const RowWork* work, int nwork, const CapInfo* caps, const GroupDev* groups,
-                          const double* X, const double* Y, const double* Z, const double* cen, int nmax, cudaStream_t st);
+                          const double* X, const double* Y, const double* Z, int nmax, cudaStream_t st);
 template <class T>
 cudaError_t launch_membrane(const RowWork* work, int nwork, const CapInfo* caps, const GroupDev* groups,
                             const int* sur_flag, int nmax, int* err, cudaStream_t st);

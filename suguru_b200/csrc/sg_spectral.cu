@@ -42,38 +42,6 @@ __device__ __forceinline__ double fdiv<double>(double a, double b) {
   return a / b;
 }
 
-// ------------------------------------------------------------ centroid -----
-__global__ void centroid_kernel(int ncap, const CapInfo* __restrict__ caps, const double* __restrict__ X,
-                                const double* __restrict__ Y, const double* __restrict__ Z, double* __restrict__ cen) {
-  __shared__ double s[3][256];
-  const int c = blockIdx.x, t = threadIdx.x;
-  const CapInfo ci = caps[c];
-  const long long n = 8LL * ci.N * ci.N;
-  double sx = 0, sy = 0, sz = 0;
-  for (long long p = t; p < n; p += blockDim.x) {
-    sx += X[ci.pt_off + p];
-    sy += Y[ci.pt_off + p];
-    sz += Z[ci.pt_off + p];
-  }
-  s[0][t] = sx;
-  s[1][t] = sy;
-  s[2][t] = sz;
-  __syncthreads();
-  for (int o = blockDim.x / 2; o > 0; o >>= 1) {
-    if (t < o) {
-      s[0][t] += s[0][t + o];
-      s[1][t] += s[1][t + o];
-      s[2][t] += s[2][t + o];
-    }
-    __syncthreads();
-  }
-  if (t == 0) {
-    cen[3 * c + 0] = s[0][0] / (double)n;
-    cen[3 * c + 1] = s[1][0] / (double)n;
-    cen[3 * c + 2] = s[2][0] / (double)n;
-  }
-}
-
 // ------------------------------------------------- positions -> Fourier ---
 // Persistent CTAs over capsule row ranges; per item the half-turn trig table
 // (j < mD/2) is staged once, then rows are taken in chunks of blockDim/(mD/2):
@@ -84,17 +52,42 @@ __global__ void centroid_kernel(int ncap, const CapInfo* __restrict__ caps, cons
 // line with lane = m: cos and sin of m (phi + pi) are (-1)^m those of m phi,
 // so an even m sums the pair sums and an odd m the pair differences over
 // j < mD/2.
+// The capsule's centroid (the mean of its points, subtracted before the
+// analysis) is computed by each item itself: 256 strided FP64 sums reduced by
+// a fixed tree, so every item of a capsule gets the same value.
 template <class T>
 __global__ void __launch_bounds__(256) posfwd_kernel(const RowWork* __restrict__ work, int nwork,
                                                      const CapInfo* __restrict__ caps,
                                                      const GroupDev* __restrict__ groups, const double* __restrict__ X,
-                                                     const double* __restrict__ Y, const double* __restrict__ Z,
-                                                     const double* __restrict__ cen) {
+                                                     const double* __restrict__ Y, const double* __restrict__ Z) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
+  __shared__ double s_cen[3][256];
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5, nwarp = blockDim.x >> 5;
   for (int w = blockIdx.x; w < nwork; w += gridDim.x) {
     const RowWork it = work[w];
     const CapInfo ci = caps[it.cap];
+    {
+      const long long n = 8LL * ci.N * ci.N;
+      double sx = 0, sy = 0, sz = 0;
+      for (long long p = tid; p < n; p += blockDim.x) {
+        sx += X[ci.pt_off + p];
+        sy += Y[ci.pt_off + p];
+        sz += Z[ci.pt_off + p];
+      }
+      __syncthreads();  // the previous item's reads of s_cen are done
+      s_cen[0][tid] = sx;
+      s_cen[1][tid] = sy;
+      s_cen[2][tid] = sz;
+      __syncthreads();
+      for (int o = blockDim.x / 2; o > 0; o >>= 1) {
+        if (tid < o) {
+          s_cen[0][tid] += s_cen[0][tid + o];
+          s_cen[1][tid] += s_cen[1][tid + o];
+          s_cen[2][tid] += s_cen[2][tid + o];
+        }
+        __syncthreads();
+      }
+    }
     const GroupDev gd = groups[it.group];
     const int N = gd.N, nD = gd.nD, mD = gd.mD, H = mD >> 1, hP = H + 1, lP = 2 * H + 2;
     const int RP = (int)blockDim.x / H > 0 ? (int)blockDim.x / H : 1;
@@ -104,7 +97,8 @@ __global__ void __launch_bounds__(256) posfwd_kernel(const RowWork* __restrict__
     const double* trig64 = (const double*)gd.trigD[0];
     const T* trig = (const T*)gd.trigD[pidx<T>()];
     const double R = ci.R;
-    const double c0 = cen[3 * it.cap], c1 = cen[3 * it.cap + 1], c2 = cen[3 * it.cap + 2];
+    const double nl = (double)(8LL * ci.N * ci.N);
+    const double c0 = s_cen[0][0] / nl, c1 = s_cen[1][0] / nl, c2 = s_cen[2][0] / nl;
     T* Fpos = (T*)gd.buf.Fpos + (long long)ci.gidx * 6 * N * nD;
     __syncthreads();  // the previous item's reads of shared memory are done
     for (int q = tid; q < 2 * N * H; q += blockDim.x) {
@@ -746,13 +740,6 @@ __global__ void __launch_bounds__(256) final_kernel(const RowWork* __restrict__ 
 }
 
 // ------------------------------------------------- launchers --------------
-template <class T>
-cudaError_t launch_centroid(int ncap, const CapInfo* caps, const double* X, const double* Y, const double* Z,
-                            double* cen, cudaStream_t st) {
-  if (ncap <= 0) return cudaSuccess;
-  centroid_kernel<<<ncap, 256, 0, st>>>(ncap, caps, X, Y, Z, cen);
-  return cudaGetLastError();
-}
 
 // Persistent launches: CTAs of 256 threads loop over the capsule work items
 // (whole capsules, largest first); the grid is what the SMs hold at once.
@@ -820,13 +807,13 @@ size_t pointwise_smem(int kind, int nmax) {
 
 template <class T>
 cudaError_t launch_posfwd(const RowWork* work, int nwork, const CapInfo* caps, const GroupDev* groups, const double* X,
-                          const double* Y, const double* Z, const double* cen, int nmax, cudaStream_t st) {
+                          const double* Y, const double* Z, int nmax, cudaStream_t st) {
   if (nwork <= 0) return cudaSuccess;
   const size_t smem = pointwise_smem<T>(kPosfwd, nmax);
   cudaError_t e = cudaFuncSetAttribute(posfwd_kernel<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   if (e != cudaSuccess) return e;
   posfwd_kernel<T><<<persistent_grid(posfwd_kernel<T>, smem, nwork), kPointThreads, smem, st>>>(
-      work, nwork, caps, groups, X, Y, Z, cen);
+      work, nwork, caps, groups, X, Y, Z);
   return cudaGetLastError();
 }
 
@@ -868,10 +855,8 @@ cudaError_t launch_final(const RowWork* work, int nwork, const CapInfo* caps, co
 }
 
 #define SG_INST(T)                                                                                                    \
-  template cudaError_t launch_centroid<T>(int, const CapInfo*, const double*, const double*, const double*, double*, \
-                                          cudaStream_t);                                                            \
   template cudaError_t launch_posfwd<T>(const RowWork*, int, const CapInfo*, const GroupDev*, const double*,         \
-                                        const double*, const double*, const double*, int, cudaStream_t);            \
+                                        const double*, const double*, int, cudaStream_t);                           \
   template cudaError_t launch_membrane<T>(const RowWork*, int, const CapInfo*, const GroupDev*, const int*, int,     \
                                           int*, cudaStream_t);                                                      \
   template cudaError_t launch_shgrid<T>(const RowWork*, int, const CapInfo*, const GroupDev*, int, int*,             \
