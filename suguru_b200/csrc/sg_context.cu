@@ -418,10 +418,10 @@ int setup(sg_ctx* c) {
   SG_TRY(dalloc(c, c->ibw.counts, sizeof(int) * c->max_tiles), "alloc");
   SG_TRY(dalloc(c, c->ibw.starts, sizeof(int) * (c->max_tiles + 1)), "alloc");
   SG_TRY(dalloc(c, c->ibw.fill, sizeof(int) * c->max_tiles), "alloc");
+  SG_TRY(cudaStreamCreateWithFlags(&c->st2, cudaStreamNonBlocking), "cudaStreamCreate");
+  SG_TRY(cudaEventCreateWithFlags(&c->ev_bin, cudaEventDisableTiming), "cudaEventCreate");
+  SG_TRY(cudaEventCreateWithFlags(&c->ev_join, cudaEventDisableTiming), "cudaEventCreate");
   if (cfg.mem == SG_MEM_HOST) {
-    SG_TRY(cudaStreamCreateWithFlags(&c->st2, cudaStreamNonBlocking), "cudaStreamCreate");
-    SG_TRY(cudaEventCreateWithFlags(&c->ev_bin, cudaEventDisableTiming), "cudaEventCreate");
-    SG_TRY(cudaEventCreateWithFlags(&c->ev_join, cudaEventDisableTiming), "cudaEventCreate");
     SG_TRY(dalloc(c, c->s_u, E * c->nfield), "alloc");
     SG_TRY(dalloc(c, c->s_v, E * c->nfield), "alloc");
     SG_TRY(dalloc(c, c->s_w, E * c->nfield), "alloc");
@@ -439,8 +439,8 @@ int setup(sg_ctx* c) {
 
 // ------------------------------------------------------------ pipeline ----
 template <class T>
-int dev_bin(sg_ctx* c, const double* X, const double* Y, const double* Z) {
-  SG_TRY(launch_bin<T>(c->grid, c->npts, X, Y, Z, c->ibw, c->st), "bin");
+int dev_bin(sg_ctx* c, const double* X, const double* Y, const double* Z, cudaStream_t st) {
+  SG_TRY(launch_bin<T>(c->grid, c->npts, X, Y, Z, c->ibw, st), "bin");
   c->launches += c->npts > 0 ? 3 : 1;
   return SG_OK;
 }
@@ -550,29 +550,21 @@ int run_step(sg_ctx* c, int what, const void* u, const void* v, const void* w, c
   const T *du = (const T*)u, *dv = (const T*)v, *dw = (const T*)w;
   T* L[10] = {(T*)U, (T*)V, (T*)W, (T*)FX, (T*)FY, (T*)FZ, (T*)NX, (T*)NY, (T*)NZ, (T*)A};
   T *dfx = (T*)fx, *dfy = (T*)fy, *dfz = (T*)fz;
-  // Host memory, full step: the interpolation branch (velocity upload,
-  // interp, velocity download) runs on st2 and the force branch (binning,
-  // forces, spread, their downloads) on st, so that the velocity upload on one
-  // stream overlaps the downloads on the other -- the spread does not read
-  // the velocity.  st2 starts after the work already queued on st and waits
-  // for the binning; st waits for st2 before the step ends.
-  const bool dual = host && c->st2 && (what & 1) && (what & 6) && !c->profiling && !c->capturing;
+  // Full step on two streams (when not profiling): binning and the
+  // interpolation branch (velocity upload, interp, velocity download) run on
+  // st2, the force branch (forces, spread, their downloads) on st.  The force
+  // stage reads only the positions, so it runs beside the binning and the
+  // interpolation; the spread waits for the binning, and st waits for st2
+  // before the step ends.  In host memory the velocity upload on one stream
+  // also overlaps the downloads on the other (the spread does not read the
+  // velocity).  A captured graph takes the same fork and join.
+  const bool dual = c->st2 && (what & 1) && (what & 6) && !c->profiling;
   cudaStream_t sB = dual ? c->st2 : c->st;
-  if (dual) {
-    SG_TRY(cudaEventRecord(c->ev_join, c->st), "event");
-    SG_TRY(cudaStreamWaitEvent(sB, c->ev_join, 0), "stream wait");
-  }
   if (host) {
     SG_RET(h2d(c, c->s_X, X, pb));
     SG_RET(h2d(c, c->s_Y, Y, pb));
     SG_RET(h2d(c, c->s_Z, Z, pb));
     dX = c->s_X; dY = c->s_Y; dZ = c->s_Z;
-    if (what & 1) {
-      SG_RET(h2d(c, c->s_u, u, fb, sB));
-      SG_RET(h2d(c, c->s_v, v, fb, sB));
-      SG_RET(h2d(c, c->s_w, w, fb, sB));
-      du = (const T*)c->s_u; dv = (const T*)c->s_v; dw = (const T*)c->s_w;
-    }
     for (int q = 0; q < 10; ++q) L[q] = (T*)c->s_lag[q];
     if ((what & 4) && !(what & 2)) {
       SG_RET(h2d(c, L[3], FX, lb));
@@ -582,18 +574,25 @@ int run_step(sg_ctx* c, int what, const void* u, const void* v, const void* w, c
     }
     dfx = (T*)c->s_f[0]; dfy = (T*)c->s_f[1]; dfz = (T*)c->s_f[2];
   }
+  if (dual) {  // st2 starts after everything queued on st so far (positions included)
+    SG_TRY(cudaEventRecord(c->ev_join, c->st), "event");
+    SG_TRY(cudaStreamWaitEvent(sB, c->ev_join, 0), "stream wait");
+  }
   auto mark = [&](int k) -> int {
     if (c->profiling && !c->capturing) SG_TRY(cudaEventRecord(c->ev[k], c->st), "event");
     return SG_OK;
   };
   SG_RET(mark(0));
-  if (what & 5) SG_RET(dev_bin<T>(c, dX, dY, dZ));
-  if (dual) {
-    SG_TRY(cudaEventRecord(c->ev_bin, c->st), "event");
-    SG_TRY(cudaStreamWaitEvent(sB, c->ev_bin, 0), "stream wait");
-  }
+  if (what & 5) SG_RET(dev_bin<T>(c, dX, dY, dZ, sB));
+  if (dual) SG_TRY(cudaEventRecord(c->ev_bin, sB), "event");
   SG_RET(mark(1));
   if (what & 1) {
+    if (host) {
+      SG_RET(h2d(c, c->s_u, u, fb, sB));
+      SG_RET(h2d(c, c->s_v, v, fb, sB));
+      SG_RET(h2d(c, c->s_w, w, fb, sB));
+      du = (const T*)c->s_u; dv = (const T*)c->s_v; dw = (const T*)c->s_w;
+    }
     SG_RET(dev_interp<T>(c, du, dv, dw, L[0], L[1], L[2], sB));
     if (host) {
       SG_RET(d2h(c, U, L[0], lb, sB));
@@ -612,6 +611,7 @@ int run_step(sg_ctx* c, int what, const void* u, const void* v, const void* w, c
   }
   SG_RET(mark(3));
   if (what & 4) {
+    if (dual) SG_TRY(cudaStreamWaitEvent(c->st, c->ev_bin, 0), "stream wait");
     SG_RET(dev_spread<T>(c, L[3], L[4], L[5], L[9], dfx, dfy, dfz, (what & 2) != 0));
     if (host) {
       SG_RET(d2h(c, fx, dfx, fb));
