@@ -224,6 +224,13 @@ int sg_set_legendre_terms(sg_ctx* ctx, int terms);
 /* The split products (3 or 6) a capsule of this SH degree runs with. */
 int sg_get_legendre_terms(sg_ctx* ctx, int degree);
 
+/* Mixed precision only: data rows per tile of the tensor-core Legendre
+ * contractions, 128 (the default; M = 128 products) or 64 (M = 64: twice the
+ * work items, for launches with few tiles).  sg_autotune times both.
+ * Results do not depend on it.  SG_ERR_STATE while a graph is captured. */
+int sg_set_legendre_tile_rows(sg_ctx* ctx, int rows);
+int sg_get_legendre_tile_rows(sg_ctx* ctx);
+
 /* Mixed precision only: run the Legendre contractions on the tensor cores in
  * BF16x3 (on = 1, the default) or on the CUDA cores in FP32 (on = 0), for
  * comparisons of the two. */
@@ -236,9 +243,10 @@ int sg_set_point_split(sg_ctx* ctx, int split);
 int sg_get_point_split(const sg_ctx* ctx);
 
 /* Autotuner: times `reps` sg_step calls with the same arguments for every
- * tile shape valid for the context and then for every point split (1, 2, 4,
- * 8) with the best shape, keeps the fastest pair and returns the shape with
- * its milliseconds per step.  The outputs hold the last step's results. */
+ * tile shape valid for the context, then for every point split (1, 2, 4, 8)
+ * with the best shape, then (mixed precision) for both tensor-core Legendre
+ * tile heights; keeps the fastest choices and returns the shape with the
+ * best milliseconds per step.  The outputs hold the last step's results. */
 int sg_autotune(sg_ctx* ctx, const void* u, const void* v, const void* w,
                 const double* X, const double* Y, const double* Z,
                 void* U, void* V, void* W,

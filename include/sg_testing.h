@@ -12,8 +12,9 @@ extern "C" {
 /* One batched Legendre contraction, as the coupling step runs it:
  *   D[m][q][j] = sum_k A[m][q][k] * B[m][j][k]   (k >= m only when tri != 0)
  * for m < M, q < Q, j < J, k < K, on the current device.  tensor_cores = 1
- * or 3 runs the tcgen05 kernel of the mixed path in BF16x3, 6 in BF16x6, 0
- * the FP32 CUDA-core kernel.  A, D are host FP32 arrays, B host FP64 (split
+ * or 3 runs the tcgen05 kernel of the mixed path in BF16x3, 6 in BF16x6, on
+ * 128-row tiles; 103 and 106 the same on 64-row tiles; 0 the FP32 CUDA-core
+ * kernel.  A, D are host FP32 arrays, B host FP64 (split
  * to bf16 parts for the tensor cores).  Returns 0, 5 (bad argument), 2 (CUDA
  * error) or 3 (the kernel raised its error flag). */
 int sg_test_legendre(int tensor_cores, int M, int Q, int J, int K, int tri, const double* B,

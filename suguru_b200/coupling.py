@@ -37,7 +37,8 @@ EXPORTS = ["sg_create", "sg_destroy", "sg_last_error", "sg_synchronize", "sg_int
            "sg_graph_release", "sg_set_capsule_membrane", "sg_capsule_spectra", "sg_surrogate_param_count",
            "sg_surrogate_params", "sg_surrogate_set_linear", "sg_surrogate_train", "sg_surrogate_predict",
            "sg_surrogate_set_trust", "sg_surrogate_last_counts", "sg_set_point_split", "sg_get_point_split",
-           "sg_set_tensor_cores", "sg_set_legendre_terms", "sg_get_legendre_terms", "sg_set_capsule_law"]
+           "sg_set_tensor_cores", "sg_set_legendre_terms", "sg_get_legendre_terms", "sg_set_capsule_law",
+           "sg_set_legendre_tile_rows", "sg_get_legendre_tile_rows"]
 # test hooks declared in include/sg_testing.h
 TEST_EXPORTS = ["sg_test_legendre", "sg_test_gemm", "sg_test_mlp_grad"]
 WORKLOAD_EXPORTS = ["sg_prescribed_flow"]  # include/sg_workload.h
@@ -95,6 +96,8 @@ def lib():
     L.sg_set_point_split.argtypes = [vp, ctypes.c_int]
     L.sg_set_tensor_cores.argtypes = [vp, ctypes.c_int]
     L.sg_set_capsule_law.argtypes = [vp, vp]
+    L.sg_set_legendre_tile_rows.argtypes = [vp, ctypes.c_int]
+    L.sg_get_legendre_tile_rows.argtypes = [vp]
     L.sg_set_legendre_terms.argtypes = [vp, ctypes.c_int]
     L.sg_get_legendre_terms.argtypes = [vp, ctypes.c_int]
     L.sg_get_point_split.argtypes = [vp]
@@ -126,11 +129,12 @@ def lib():
     return L
 
 
-def test_legendre(A, B, tensor_cores=True, tri=False, terms=3):
+def test_legendre(A, B, tensor_cores=True, tri=False, terms=3, tile_rows=128):
     """D[m,q,j] = sum_k A[m,q,k] B[m,j,k] through one Legendre kernel (test hook).
 
     tensor_cores: the tcgen05 kernel with `terms` split products (3: BF16x3,
-    6: BF16x6); otherwise the FP32 CUDA-core kernel.
+    6: BF16x6) on tiles of `tile_rows` (64 or 128) data rows; otherwise the
+    FP32 CUDA-core kernel.
     """
     A = np.ascontiguousarray(A, dtype=np.float32)
     B = np.ascontiguousarray(B, dtype=np.float64)
@@ -138,7 +142,7 @@ def test_legendre(A, B, tensor_cores=True, tri=False, terms=3):
     J = B.shape[1]
     assert B.shape == (M, J, K)
     D = np.zeros((M, Q, J), dtype=np.float32)
-    mode = int(terms) if tensor_cores else 0
+    mode = (int(terms) + (100 if tile_rows == 64 else 0)) if tensor_cores else 0
     rc = lib().sg_test_legendre(mode, M, Q, J, K, int(bool(tri)), _ptr(B), _ptr(A), _ptr(D))
     if rc:
         raise SgError(rc, "sg_test_legendre")
@@ -328,6 +332,13 @@ class CouplingStep:
         law = np.ascontiguousarray(law, dtype=np.int32)
         assert law.size == self.degree.size
         self._check(lib().sg_set_capsule_law(self._h, law.ctypes.data_as(ctypes.c_void_p)), "sg_set_capsule_law")
+
+    def set_legendre_tile_rows(self, rows):
+        """Data rows per tensor-core Legendre tile: 128 or 64 (results do not depend on it)."""
+        self._check(lib().sg_set_legendre_tile_rows(self._h, int(rows)), "sg_set_legendre_tile_rows")
+
+    def legendre_tile_rows(self):
+        return int(lib().sg_get_legendre_tile_rows(self._h))
 
     def set_legendre_terms(self, terms=0):
         """Split mode of the tensor-core Legendre products: 3 (BF16x3), 6 (BF16x6), 0 automatic by degree."""

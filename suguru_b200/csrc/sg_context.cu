@@ -368,11 +368,21 @@ int setup(sg_ctx* c) {
     SG_TRY(upload(c, dimg, img), "umma images");
     for (size_t pi2 = 0; pi2 < P.size(); ++pi2) P[pi2].Bimg = (const uint16_t*)dimg + img_off[pi2];
     for (int f = 0; f < 3; ++f) {
-      std::vector<LegWork> WF;
+      // work lists on 128-row and on 64-row tiles (the launches use the
+      // 128-row list unless sg_set_legendre_tile_rows or the autotuner switch)
+      for (int t = 0; t < 2; ++t) {
+        const int tm = t ? 64 : 128;
+        std::vector<LegWork> WT;
+        for (int r : roots[f])
+          for (int m = 0; m < P[r].M; ++m)
+            for (int q0 = 0; q0 < P[r].Q; q0 += tm) WT.push_back(LegWork{r, m, q0});
+        c->nlwT[t][f] = (int)WT.size();
+        SG_TRY(upload(c, tmp, WT), "work");
+        c->d_lwT[t][f] = (LegWork*)tmp;
+      }
+      c->tmF[f] = 128;
       for (int r : roots[f]) {
         const LegProblem& p = P[r];
-        for (int m = 0; m < p.M; ++m)
-          for (int q0 = 0; q0 < p.Q; q0 += 128) WF.push_back(LegWork{r, m, q0});
         const int chain[3] = {r, p.next[0], p.next[0] >= 0 ? p.next[1] : -1};
         LegLevels& lv = c->lvF[f];
         for (int l = 0; l < 3; ++l) {
@@ -383,9 +393,8 @@ int setup(sg_ctx* c) {
           lv.a_kp = std::max(lv.a_kp, P[q].Kp);
         }
       }
-      c->nlwF[f] = (int)WF.size();
-      SG_TRY(upload(c, tmp, WF), "work");
-      c->d_lwF[f] = (LegWork*)tmp;
+      c->nlwF[f] = c->nlwT[0][f];
+      c->d_lwF[f] = c->d_lwT[0][f];
     }
     c->leg_tc = true;
     assign_terms(c, P);
@@ -458,8 +467,8 @@ int dev_legendre(sg_ctx* c, int s) {
     // stages 0, 2, 4 launch the chained products; 1, 3, 5 ran inside them
     if (s % 2) return SG_OK;
     const int f = s / 2;
-    SG_TRY(launch_legendre_mma(c->d_probs, c->d_lwF[f], c->nlwF[f], c->lvF[f], c->leg_parts, c->d_err,
-                               c->num_sms, c->st),
+    SG_TRY(launch_legendre_mma(c->d_probs, c->d_lwF[f], c->nlwF[f], c->lvF[f], c->leg_parts, c->tmF[f],
+                               c->d_err, c->num_sms, c->st),
            "legendre (tensor cores)");
     c->launches += 1;
   } else {
@@ -894,6 +903,22 @@ int sg_get_legendre_terms(sg_ctx* c, int degree) {
   return terms_for(c, degree);
 }
 
+int sg_set_legendre_tile_rows(sg_ctx* c, int rows) {
+  if (!c) return SG_ERR_ARG;
+  if (rows != 64 && rows != 128) return fail(c, SG_ERR_ARG, "tile rows must be 64 or 128");
+  if (c->graph) return fail(c, SG_ERR_STATE, "release the captured graph first");
+  if (!c->mixed) return fail(c, SG_ERR_CONFIG, "the tensor-core path is the mixed-precision path");
+  const int t = rows == 64 ? 1 : 0;
+  for (int f = 0; f < 3; ++f) {
+    c->tmF[f] = rows;
+    c->nlwF[f] = c->nlwT[t][f];
+    c->d_lwF[f] = c->d_lwT[t][f];
+  }
+  return SG_OK;
+}
+
+int sg_get_legendre_tile_rows(sg_ctx* c) { return c ? c->tmF[0] : -1; }
+
 int sg_set_tensor_cores(sg_ctx* c, int on) {
   if (!c) return SG_ERR_ARG;
   if (c->graph) return fail(c, SG_ERR_STATE, "release the captured graph first");
@@ -970,6 +995,21 @@ int sg_autotune(sg_ctx* c, const void* u, const void* v, const void* w, const do
     }
   }
   if (rc == SG_OK && best >= 0) rc = set_point_split(c, bsplit);
+  // 3) tile rows of the tensor-core Legendre launches (mixed path)
+  if (rc == SG_OK && best >= 0 && c->leg_tc) {
+    int brows = c->tmF[0];
+    for (int rows : {128, 64}) {
+      if (rc != SG_OK) break;
+      rc = sg_set_legendre_tile_rows(c, rows);
+      float ms = 0.f;
+      if (rc == SG_OK) rc = time_step(&ms);
+      if (rc == SG_OK && ms < bms) {
+        brows = rows;
+        bms = ms;
+      }
+    }
+    if (rc == SG_OK) rc = sg_set_legendre_tile_rows(c, brows);
+  }
   c->cfg.async = async;
   cudaEventDestroy(e0);
   cudaEventDestroy(e1);

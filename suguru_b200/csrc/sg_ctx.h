@@ -64,9 +64,12 @@ struct sg_ctx {
   int leg_terms = 0;
   int leg_parts = 2;                  // bf16 parts staged per operand (3 if any group is BF16x6)
   std::vector<LegProblem> h_probs;    // host copy of d_probs (the split mode is rewritten in place)
-  LegWork* d_lwF[3] = {};  // root work items of the three chained launches
+  LegWork* d_lwF[3] = {};  // root work items of the three chained launches (tiles of tmF rows)
   int nlwF[3] = {};
+  LegWork* d_lwT[2][3] = {};  // the work items on 128-row [0] and 64-row [1] tiles
+  int nlwT[2][3] = {};
   LegLevels lvF[3] = {};    // shared-memory sizes of the three chained launches
+  int tmF[3] = {128, 128, 128};  // their tile rows (sg_set_legendre_tile_rows, the autotuner)
   int num_sms = 148;
   int* d_err = nullptr;   // device error flag (bounded waits that expired)
   int* h_err = nullptr;   // pinned copy, refreshed at the end of every step

@@ -130,12 +130,12 @@ struct LegLevels {
   int a_kp;
 };
 // Tensor-core (tcgen05, BF16x3 / BF16x6) contraction of FP32 problems; work
-// items are 128-row tiles of root problems and their chains.  nparts = 3 if
-// any problem reached is BF16x6, else 2.  d_err is set to 1 if an MMA or a
-// table copy wait times out, 2 if a problem does not fit the sizes of lv and
-// nparts or its mode differs along a chain.
+// items are tiles of tm (64 or 128) rows of root problems and their chains
+// (q0 a multiple of tm).  nparts = 3 if any problem reached is BF16x6, else 2.
+// d_err is set to 1 if an MMA or a table copy wait times out, 2 if a problem
+// does not fit the sizes of lv and nparts or its mode differs along a chain.
 cudaError_t launch_legendre_mma(const LegProblem* d_probs, const LegWork* d_work, int nwork, const LegLevels& lv,
-                                int nparts, int* d_err, int num_sms, cudaStream_t st);
+                                int nparts, int tm, int* d_err, int num_sms, cudaStream_t st);
 // Dense product on the tensor cores (sg_gemm.cu):
 //   C = alpha A B^T (+ bias[n]) (then GELU), A [M][K], B [N][K], K % 64 == 0.
 // split = 0: A, B bf16; split = 1: A, B FP32, split into bf16 hi/lo (BF16x3).

@@ -41,7 +41,6 @@ namespace sg {
 
 namespace {
 
-constexpr int MMA_M = 128;
 using namespace umma;
 
 }  // namespace
@@ -77,10 +76,10 @@ __device__ __forceinline__ void store_split(const float* x, int np, const Operan
 }
 
 // One thread issues the split products of every K step of 16 (largest terms
-// first), then commits.  bt: the level's table region.
-__device__ __forceinline__ void issue_mma(const LegProblem& P, int m, uint32_t tmem, const Operands& op,
+// first), then commits.  bt: the level's table region; tm: the tile's rows.
+__device__ __forceinline__ void issue_mma(const LegProblem& P, int m, int tm, uint32_t tmem, const Operands& op,
                                           const uint16_t* bt, uint64_t* bar) {
-  const uint32_t idesc = idesc_bf16(MMA_M, P.Jp);
+  const uint32_t idesc = idesc_bf16(tm, P.Jp);
   const uint32_t lbo = 128, sbo = (uint32_t)P.Kp * 16;
   const uint32_t pb = (uint32_t)(P.Jp * P.Kp) * 2u;  // bytes per table part
   const uint32_t a0 = smem_u32(op.a[0]), a1 = smem_u32(op.a[1]), b0 = smem_u32(bt), b1 = b0 + pb;
@@ -111,11 +110,17 @@ __device__ __forceinline__ void issue_mma(const LegProblem& P, int m, uint32_t t
 // the next product's bf16 hi/lo operand tile in shared memory, so the data
 // never leaves the SM between the two contractions.
 // A chain runs in its root's mode (one degree group: the same mode throughout).
-// smem (bf16): nparts A parts of 128 x lv.a_kp, then for each chain level l a
+// Tiles of TM = 128 data rows (M = 128: row r in TMEM lane r, so warp w
+// holds rows 32w..32w+31) or TM = 64 (M = 64: row r in lane (r mod 16) +
+// 32 floor(r / 16) -- the first half of every warp's 32-lane quadrant -- so
+// warp w holds rows 16w..16w+15 in its lanes 0..15); 64-row tiles double the
+// work items of a launch whose 128-row tiles would leave SMs idle.
+// smem (bf16): nparts A parts of TM x lv.a_kp, then for each chain level l a
 // table region of nparts x lv.jp[l] x lv.kp[l]; nparts = 3 when any problem of
 // the launch is BF16x6, else 2.  At the start of a work item one thread issues
 // the bulk copies of every level's table (each on its own mbarrier), so they
 // overlap the staging of the data rows and the earlier products.
+template <int TM>
 __global__ void __launch_bounds__(128) legendre_mma_kernel(const LegProblem* __restrict__ probs,
                                                            const LegWork* __restrict__ work, int nwork, LegLevels lv,
                                                            int nparts, int tmem_cols, int* __restrict__ err) {
@@ -128,9 +133,9 @@ __global__ void __launch_bounds__(128) legendre_mma_kernel(const LegProblem* __r
     uint16_t* p = (uint16_t*)smem_raw;
     for (int i = 0; i < 3; ++i) {
       op.a[i] = p;
-      if (i + 1 < nparts) p += MMA_M * lv.a_kp;
+      if (i + 1 < nparts) p += TM * lv.a_kp;
     }
-    p = (uint16_t*)smem_raw + nparts * MMA_M * lv.a_kp;
+    p = (uint16_t*)smem_raw + nparts * TM * lv.a_kp;
     for (int l = 0; l < 3; ++l) {
       op.b[l] = p;
       p += nparts * lv.jp[l] * lv.kp[l];
@@ -159,7 +164,7 @@ __global__ void __launch_bounds__(128) legendre_mma_kernel(const LegProblem* __r
     const int m = wk.m, q0 = wk.q0;
     int pid = wk.prob;
     const LegProblem& R = probs[pid];
-    const int nq = min(MMA_M, R.Q - q0);
+    const int nq = min(TM, R.Q - q0);
     const int np = parts_of(R);
     // the chain: level 0 the root, 1 its next[0], 2 its next[1] (only after a level 1)
     const int chain[3] = {pid, R.next[0], R.next[0] >= 0 ? R.next[1] : -1};
@@ -181,33 +186,35 @@ __global__ void __launch_bounds__(128) legendre_mma_kernel(const LegProblem* __r
           pending |= 1 << l;
         }
     }
-    // ---- data rows of the root: FP32 -> bf16 parts.  Thread q stages row q
-    // of the tile; all of its loads (up to 8 core-matrix rows of 8 values)
-    // are issued before any is split and stored, so their latencies overlap.
+    // ---- data rows of the root: FP32 -> bf16 parts.  Thread tid stages
+    // row tid % TM of the tile, every (128/TM)-th core-matrix row of 8 values
+    // starting at tid / TM; all of its loads (up to 8 core-matrix rows) are
+    // issued before any is split and stored, so their latencies overlap.
     {
-      const int K = R.K, KC = R.Kp >> 3, q = tid;
+      constexpr int NPH = 128 / TM;
+      const int K = R.K, KC = R.Kp >> 3, q = tid % TM, ph = tid / TM;
       const float* row = nullptr;
       if (q < nq) {
         const int qq = q0 + q, c = qq / R.rpc, r = qq - c * R.rpc;
         row = (const float*)R.A + (long long)c * R.sAc + (long long)r * R.sAr + (long long)m * R.sAm;
       }
-      for (int kc0 = 0; kc0 < KC; kc0 += 8) {
+      for (int kc0 = ph; kc0 < KC; kc0 += 8 * NPH) {
         float x[8][8];
 #pragma unroll
         for (int u = 0; u < 8; ++u) {
-          const int k0 = (kc0 + u) << 3;
-          if (row && kc0 + u < KC && R.vecA && k0 + 8 <= K) {
+          const int kc = kc0 + u * NPH, k0 = kc << 3;
+          if (row && kc < KC && R.vecA && k0 + 8 <= K) {
             const float4 a = *(const float4*)(row + k0), b = *(const float4*)(row + k0 + 4);
             x[u][0] = a.x; x[u][1] = a.y; x[u][2] = a.z; x[u][3] = a.w;
             x[u][4] = b.x; x[u][5] = b.y; x[u][6] = b.z; x[u][7] = b.w;
           } else {
 #pragma unroll
-            for (int i = 0; i < 8; ++i) x[u][i] = (row && kc0 + u < KC && k0 + i < K) ? row[k0 + i] : 0.f;
+            for (int i = 0; i < 8; ++i) x[u][i] = (row && kc < KC && k0 + i < K) ? row[k0 + i] : 0.f;
           }
         }
 #pragma unroll
         for (int u = 0; u < 8; ++u)
-          if (kc0 + u < KC) store_split(x[u], np, op, cm_offset(q, kc0 + u, KC));
+          if (kc0 + u * NPH < KC) store_split(x[u], np, op, cm_offset(q, kc0 + u * NPH, KC));
       }
     }
     // ---- the root, then its chained products: one MMA group per problem
@@ -224,7 +231,7 @@ __global__ void __launch_bounds__(128) legendre_mma_kernel(const LegProblem* __r
         pending &= ~(1 << level);
         tphase[level] ^= 1u;
         if (landed)
-          issue_mma(P, m, tmem, op, op.b[level], &s_bar);
+          issue_mma(P, m, TM, tmem, op, op.b[level], &s_bar);
         else
           atomicExch(err, 1);
       }
@@ -242,12 +249,14 @@ __global__ void __launch_bounds__(128) legendre_mma_kernel(const LegProblem* __r
       // chained products of the root take its rows as their A operand
       const bool chain = level == 0 && P.next[0] >= 0;
       const int KC2 = P.Jp >> 3;  // next K padded = this J padded
-      // ---- epilogue: warp w holds rows 32w..32w+31 of the tile (TMEM lanes)
+      // ---- epilogue: warp w holds rows 32w..32w+31 of a 128-row tile, rows
+      // 16w..16w+15 of a 64-row tile (its lanes 0..15)
       {
-        const int q = warp * 32 + lane;
+        const bool lane_row = TM == 128 || lane < 16;
+        const int q = TM == 128 ? warp * 32 + lane : warp * 16 + lane;
         const int J = P.J;
         float* drow = nullptr;
-        if (q < nq) {
+        if (lane_row && q < nq) {
           const int qq = q0 + q, c = qq / P.rpc, r = qq - c * P.rpc;
           drow = (float*)P.D + (long long)c * P.sDc + (long long)r * P.sDr + (long long)m * P.sDm;
         }
@@ -265,7 +274,7 @@ __global__ void __launch_bounds__(128) legendre_mma_kernel(const LegProblem* __r
                 if (j0 + i < J) drow[j0 + i] = v[i];
             }
           }
-          if (chain) {  // root MMA is complete: its A tile is free for the next operand
+          if (chain && lane_row) {  // root MMA is complete: its A tile is free for the next operand
 #pragma unroll
             for (int h = 0; h < 2; ++h) {
               float x[8];
@@ -311,15 +320,16 @@ __global__ void __launch_bounds__(128) legendre_mma_kernel(const LegProblem* __r
   if (warp == 0) tmem_free(tmem, (uint32_t)tmem_cols);
 }
 
-size_t legendre_mma_smem(const LegLevels& lv, int nparts) {
-  size_t e = (size_t)MMA_M * lv.a_kp;
+size_t legendre_mma_smem(const LegLevels& lv, int nparts, int tm) {
+  size_t e = (size_t)tm * lv.a_kp;
   for (int l = 0; l < 3; ++l) e += (size_t)lv.jp[l] * lv.kp[l];
   return (size_t)nparts * sizeof(uint16_t) * e;
 }
 
 cudaError_t launch_legendre_mma(const LegProblem* d_probs, const LegWork* d_work, int nwork, const LegLevels& lv,
-                                int nparts, int* d_err, int num_sms, cudaStream_t st) {
+                                int nparts, int tm, int* d_err, int num_sms, cudaStream_t st) {
   if (nwork <= 0) return cudaSuccess;
+  if (tm != 64 && tm != 128) return cudaErrorInvalidValue;
   int maxJp = 0;
   for (int l = 0; l < 3; ++l) {
     if (lv.jp[l] < 0 || lv.jp[l] > 256 || (lv.jp[l] & 15) || lv.kp[l] < 0 || (lv.kp[l] & 15))
@@ -333,15 +343,23 @@ cudaError_t launch_legendre_mma(const LegProblem* d_probs, const LegWork* d_work
   int cols = 32;
   while (cols < maxJp) cols <<= 1;
   const int per_sm = 512 / cols < 4 ? 512 / cols : 4;
-  size_t smem = legendre_mma_smem(lv, nparts);
+  size_t smem = legendre_mma_smem(lv, nparts, tm);
   // (per_sm + 1) CTAs of this size exceed the SM's 228 KB of shared memory
   const size_t floor_smem = (size_t)(228 * 1024) / (size_t)(per_sm + 1);
   if (smem < floor_smem) smem = floor_smem;
   if (smem > (size_t)227 * 1024) return cudaErrorInvalidValue;
-  cudaError_t e = cudaFuncSetAttribute(legendre_mma_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-  if (e != cudaSuccess) return e;
   const int grid = nwork < num_sms * per_sm ? nwork : num_sms * per_sm;
-  legendre_mma_kernel<<<grid, 128, smem, st>>>(d_probs, d_work, nwork, lv, nparts, cols, d_err);
+  if (tm == 64) {
+    cudaError_t e = cudaFuncSetAttribute(legendre_mma_kernel<64>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         (int)smem);
+    if (e != cudaSuccess) return e;
+    legendre_mma_kernel<64><<<grid, 128, smem, st>>>(d_probs, d_work, nwork, lv, nparts, cols, d_err);
+  } else {
+    cudaError_t e = cudaFuncSetAttribute(legendre_mma_kernel<128>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         (int)smem);
+    if (e != cudaSuccess) return e;
+    legendre_mma_kernel<128><<<grid, 128, smem, st>>>(d_probs, d_work, nwork, lv, nparts, cols, d_err);
+  }
   return cudaGetLastError();
 }
 

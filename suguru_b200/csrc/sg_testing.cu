@@ -13,8 +13,11 @@ using namespace sg;
 extern "C" int sg_test_legendre(int tensor_cores, int M, int Q, int J, int K, int tri, const double* B,
                                 const float* A, float* D) {
   if (M < 1 || Q < 1 || J < 1 || K < 1 || J > 256 || K > 256 || !B || !A || !D) return 5;
-  if (tensor_cores != 0 && tensor_cores != 1 && tensor_cores != 3 && tensor_cores != 6) return 5;
-  const int terms = tensor_cores == 6 ? 6 : 3;
+  // tensor_cores: 0 CUDA cores; 1 or 3 BF16x3, 6 BF16x6 on 128-row tiles; +100 for 64-row tiles
+  const int tm = tensor_cores >= 100 ? 64 : 128, mode = tensor_cores % 100;
+  if (mode != 0 && mode != 1 && mode != 3 && mode != 6) return 5;
+  if (tensor_cores >= 100 && mode == 0) return 5;
+  const int terms = mode == 6 ? 6 : 3;
   const int Jp = (J + 15) / 16 * 16, Kp = (K + 15) / 16 * 16;
   // problem: A[m][q][k] rows, B[m][j][k], D[m][q][j]
   LegProblem p{};
@@ -41,7 +44,7 @@ extern "C" int sg_test_legendre(int tensor_cores, int M, int Q, int J, int K, in
   std::vector<float> Bf((size_t)M * J * K);
   for (size_t i = 0; i < Bf.size(); ++i) Bf[i] = (float)B[i];
   std::vector<LegWork> work;
-  const int qt = tensor_cores ? 128 : 32;
+  const int qt = tensor_cores ? tm : 32;
   for (int m = 0; m < M; ++m)
     for (int q0 = 0; q0 < Q; q0 += qt) work.push_back(LegWork{0, m, q0});
   void *dA = nullptr, *dB = nullptr, *dD = nullptr, *dI = nullptr, *dP = nullptr, *dW = nullptr, *dE = nullptr;
@@ -75,7 +78,7 @@ extern "C" int sg_test_legendre(int tensor_cores, int M, int Q, int J, int K, in
         lv.kp[0] = Kp;
         lv.a_kp = Kp;
         ok(launch_legendre_mma((const LegProblem*)dP, (const LegWork*)dW, (int)work.size(), lv, terms == 6 ? 3 : 2,
-                               (int*)dE, sms, 0));
+                               tm, (int*)dE, sms, 0));
       } else {
         ok(launch_legendre<float>((const LegProblem*)dP, (const LegWork*)dW, (int)work.size(), J, K, 0));
       }

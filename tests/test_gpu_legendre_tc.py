@@ -35,10 +35,11 @@ def _case(M, Q, J, K, seed):
     return A, B, exact, scale
 
 
+@pytest.mark.parametrize("tile_rows", [128, 64])
 @pytest.mark.parametrize("shape", SHAPES)
-def test_tensor_core_contraction(cuda, shape):
+def test_tensor_core_contraction(cuda, shape, tile_rows):
     A, B, exact, scale = _case(*shape, seed=sum(shape))
-    D = run_legendre(A, B, tensor_cores=True)
+    D = run_legendre(A, B, tensor_cores=True, tile_rows=tile_rows)
     assert np.isfinite(D).all()
     err = np.abs(D - exact) / scale
     assert err.max() <= 3e-5, err.max()
@@ -46,11 +47,12 @@ def test_tensor_core_contraction(cuda, shape):
     assert np.median(err) <= 2e-6
 
 
+@pytest.mark.parametrize("tile_rows", [128, 64])
 @pytest.mark.parametrize("shape", SHAPES)
-def test_tensor_core_six_products(cuda, shape):
+def test_tensor_core_six_products(cuda, shape, tile_rows):
     A, B, exact, scale = _case(*shape, seed=11 + sum(shape))
-    D6 = run_legendre(A, B, tensor_cores=True, terms=6)
-    D3 = run_legendre(A, B, tensor_cores=True, terms=3)
+    D6 = run_legendre(A, B, tensor_cores=True, terms=6, tile_rows=tile_rows)
+    D3 = run_legendre(A, B, tensor_cores=True, terms=3, tile_rows=tile_rows)
     e6 = np.abs(D6 - exact) / scale
     e3 = np.abs(D3 - exact) / scale
     assert e6.max() <= 1e-6, e6.max()

@@ -131,3 +131,24 @@ def test_point_split_does_not_change_results(cuda, precision):
             assert np.array_equal(a, b)
     with pytest.raises(SgError):
         cs.set_point_split(9)
+
+
+def test_legendre_tile_rows_do_not_change_results(cuda):
+    # 64-row tiles (M = 64 products, rows in the first half of each TMEM
+    # quadrant) against 128-row tiles: every row is the same dot product
+    wl = W.small_config()
+    u, v, w = (a.astype(np.float32) for a in wl.velocity())
+    cs = CouplingStep(wl.grid, wl.degree, wl.radius, precision="mixed")
+    assert cs.legendre_tile_rows() == 128
+    a = cs.step(u, v, w, wl.x, wl.y, wl.z)
+    a = {k: [x.copy() for x in val] if isinstance(val, tuple) or isinstance(val, list) else val.copy()
+         for k, val in a.items()}
+    cs.set_legendre_tile_rows(64)
+    assert cs.legendre_tile_rows() == 64
+    b = cs.step(u, v, w, wl.x, wl.y, wl.z)
+    for k in ("u", "f", "n", "fgrid"):
+        for x, y in zip(a[k], b[k]):
+            assert np.array_equal(x, y), k
+    assert np.array_equal(a["area"], b["area"])
+    with pytest.raises(SgError):
+        cs.set_legendre_tile_rows(96)
