@@ -346,7 +346,7 @@ int setup(sg_ctx* c) {
       if (cfg.surrogate) roots[2].push_back(base + 6);
     }
   }
-  // tensor-core operands: bf16 hi/lo images of every problem's table, and
+  // tensor-core operands: the three bf16 parts of every problem's table, and
   // work lists of 128-row tiles of the root problems (FP32 data only)
   if (c->mixed) {
     std::vector<uint16_t> img;

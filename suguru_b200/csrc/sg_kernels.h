@@ -81,11 +81,6 @@ struct DegreeTables {
   // cos/sin(m phi_j), [m][j], on both longitude grids
   void* trigD[2] = {nullptr, nullptr};  // [2][N][mD]
   void* trigO[2] = {nullptr, nullptr};  // [2][N][mO]
-  // BF16x3 split operands in UMMA canonical K-major layout (mixed path)
-  void* umma_syn_D = nullptr;
-  void* umma_ana_D = nullptr;
-  void* umma_syn_O = nullptr;
-  void* umma_ana_O = nullptr;
 };
 
 // One batched Legendre contraction over the capsules of one degree group.

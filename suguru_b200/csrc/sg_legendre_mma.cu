@@ -107,7 +107,7 @@ __device__ __forceinline__ void issue_mma(const LegProblem& P, int m, int tm, ui
 // Work items name root problems; a root's next[] problems take its output
 // rows as their A operand for the same (m, tile) and run in the same CTA: the
 // accumulator is read once from TMEM, written to global memory, and split into
-// the next product's bf16 hi/lo operand tile in shared memory, so the data
+// the next product's bf16 operand parts in shared memory, so the data
 // never leaves the SM between the two contractions.
 // A chain runs in its root's mode (one degree group: the same mode throughout).
 // Tiles of TM = 128 data rows (M = 128: row r in TMEM lane r, so warp w

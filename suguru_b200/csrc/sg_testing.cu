@@ -1,7 +1,8 @@
 // sg_testing.cu -- test hooks (include/sg_testing.h): run one batched
 // Legendre contraction through the tensor-core or the CUDA-core kernel on
 // caller data, so that the tests can check the UMMA operand layout, the
-// BF16x3 split and the epilogue element by element against numpy.
+// BF16x3 and BF16x6 splits, the 64- and 128-row tiles and the epilogue element
+// by element against numpy.
 #include <cstring>
 #include <vector>
 
