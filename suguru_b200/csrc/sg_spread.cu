@@ -15,12 +15,16 @@
 // is exact and associative, so the field is bitwise independent of the order
 // in which threads add (no floating-point atomics, deterministic run to run).
 //
-//  - FP32: one signed 32-bit word per cell and component.  The scale is the
-//    smaller of two powers of two: one that puts 0.3 * sum over the tile's
-//    entries of max_c |f_c * area / dV| below 2^30 (every 3-D kernel weight is
-//    at most (2/3)^3 < 0.3, so no cell sum can reach 2^31), and one that puts
-//    0.3 * the largest single max_c |f_c * area / dV| below 2^22, so that every
-//    contribution v satisfies |v| < 2^22.  Then one FMA, v + 1.5 * 2^23, rounds
+//  - FP32: one signed 32-bit word per cell and component.  With m =
+//    max_c |f_c * area / dV| per entry, the scale is the smaller of two powers
+//    of two: one that puts 0.3 * sum over the tile's entries of m below 2^30
+//    (every 3-D kernel weight is at most (2/3)^3 < 0.3, so no cell sum can
+//    reach 2^31), and one that puts 0.3 * the largest m below 2^22, so that
+//    every contribution v satisfies |v| < 2^22.  The sum of m is needed only
+//    above 2^8 entries (below, count * largest m bounds it tightly enough)
+//    and is then an exact integer sum of m rounded up to 2^-12 of the largest
+//    m's binade, so that the scale, like the cell sums, is independent of the
+//    order of the entries.  Then one FMA, v + 1.5 * 2^23, rounds
 //    v to the nearest integer (ties to even) in the low mantissa bits of a
 //    float whose exponent is fixed, and the integer is its bit pattern minus
 //    that of 1.5 * 2^23 -- no conversion instruction per contribution.  The
@@ -76,6 +80,14 @@ struct Fixed<double> {
   }
 };
 
+// the smallest e with b < 2^e (0 for b <= 0), at least -60 so that the
+// scales stay finite in float
+__device__ __forceinline__ int exp_above(double b) {
+  int ex = 0;
+  if (b > 0.0) frexp(b, &ex);
+  return ex < -60 ? -60 : ex;
+}
+
 }  // namespace
 
 // Force records cf = F * (A / dV) and their largest component magnitude
@@ -110,7 +122,8 @@ __global__ void __launch_bounds__(256) spread_kernel(IBGrid g, const int* __rest
   // contributions falling outside the tile, so that the walk has no branches
   constexpr int NCP = NC + 32;
   __shared__ __align__(16) unsigned int acc[NW][3][NCP];
-  __shared__ T s_red[2][8];
+  __shared__ T s_red[8];
+  __shared__ unsigned long long s_sum[8];
   long long tot[NT][3];
 #pragma unroll
   for (int r = 0; r < NT; ++r) tot[r][0] = tot[r][1] = tot[r][2] = 0;
@@ -124,43 +137,47 @@ __global__ void __launch_bounds__(256) spread_kernel(IBGrid g, const int* __rest
 
   if (e1 > e0) {
     for (int q = tid; q < NW * 3 * NCP / 4; q += 256) ((uint4*)&acc[0][0][0])[q] = make_uint4(0u, 0u, 0u, 0u);
-    // ---- fixed-point scale: FP32 from the sum, FP64 from the maximum of
-    // max_c |f_c * area / dV| over the tile's entries (fixed reduction order)
-    T red = T(0), rmax = T(0);
-    for (int e = e0 + tid; e < e1; e += 256) {
-      const T m = frc[entries[e]].cf[3];
-      red = F32 ? red + m : fmax(red, m);
-      rmax = fmax(rmax, m);
-    }
+    // ---- fixed-point scale from m = max_c |f_c * area / dV| over the tile's
+    // entries.  Only order-independent quantities enter it -- the largest m,
+    // the entry count and an integer sum -- so that the scale, like the sums,
+    // does not depend on the order in which the binning listed the entries.
+    T rmax = T(0);
+    for (int e = e0 + tid; e < e1; e += 256) rmax = fmax(rmax, frc[entries[e]].cf[3]);
 #pragma unroll
-    for (int o = 16; o > 0; o >>= 1) {
-      const T other = __shfl_xor_sync(0xffffffffu, red, o);
-      red = F32 ? red + other : fmax(red, other);
-      rmax = fmax(rmax, __shfl_xor_sync(0xffffffffu, rmax, o));
-    }
-    if (lane == 0) {
-      s_red[0][warp] = red;
-      s_red[1][warp] = rmax;
-    }
+    for (int o = 16; o > 0; o >>= 1) rmax = fmax(rmax, __shfl_xor_sync(0xffffffffu, rmax, o));
+    if (lane == 0) s_red[warp] = rmax;
     __syncthreads();
-    red = s_red[0][0];
-    rmax = s_red[1][0];
+    rmax = s_red[0];
 #pragma unroll
-    for (int q = 1; q < 8; ++q) {
-      red = F32 ? red + s_red[0][q] : fmax(red, s_red[0][q]);
-      rmax = fmax(rmax, s_red[1][q]);
-    }
-    int ex = 0;
-    const double bound = F32 ? 0.3 * (double)red : (double)red * (double)(e1 - e0);
-    if (bound > 0.0) frexp(bound, &ex);  // bound < 2^ex
-    if (ex < -60) ex = -60;              // keeps the scale finite in float
-    int sh = QB - ex;                    // |sum| < 2^QB
-    if constexpr (F32) {                 // and every single contribution below 2^22
-      int ex1 = 0;
-      const double b1 = 0.3 * (double)rmax;
-      if (b1 > 0.0) frexp(b1, &ex1);
-      if (ex1 < -60) ex1 = -60;
-      sh = min(sh, 22 - ex1);
+    for (int q = 1; q < 8; ++q) rmax = fmax(rmax, s_red[q]);
+    const int cnt = e1 - e0;
+    // FP64: |sum| < 2^QB from the largest m times the entry count
+    int sh = QB - exp_above((double)rmax * (double)(F32 ? 0.3 * cnt : cnt));
+    if constexpr (F32) {
+      // every single contribution below 2^22 ...
+      const int sh1 = 22 - exp_above(0.3 * (double)rmax);
+      if (sh < sh1) {
+        // ... and, where the count bound would cost precision (more than 2^8
+        // entries), |sum| < 2^30 from 0.3 * sum of m, taken as an exact integer
+        // sum of m rounded up to multiples of 2^-12 of the largest m's binade
+        int exr = 0;
+        frexp((double)rmax, &exr);  // rmax < 2^exr
+        const double u = ldexp(1.0, 12 - exr);
+        unsigned long long s = 0;
+        for (int e = e0 + tid; e < e1; e += 256) {
+          const double v = (double)frc[entries[e]].cf[3] * u;  // < 2^12, exact
+          s += v > 0.0 ? (unsigned long long)ceil(v) : 0ull;
+        }
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+        if (lane == 0) s_sum[warp] = s;
+        __syncthreads();
+        s = 0;
+#pragma unroll
+        for (int q = 0; q < 8; ++q) s += s_sum[q];
+        sh = QB - exp_above(0.3 * ldexp((double)s, exr - 12));
+      }
+      sh = min(sh, sh1);
     }
     const T scale = (T)ldexp(1.0, sh);
     iscale = (T)ldexp(1.0, -sh);
