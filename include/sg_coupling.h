@@ -113,6 +113,24 @@ int sg_surf_vol(sg_ctx* ctx, const double* X, const double* Y, const double* Z,
                 const void* NX, const void* NY, const void* NZ, const void* AREA,
                 const double* exy1_prev, double* out);
 
+/* collisions (collisions.f90:10-32): FZ += the Morse-potential force of the
+ * wall z = 0 on every point closer than rad0, summed over the wall's lattice
+ * images (j dy, k dx) within the cutoff:
+ *   fc = sum 2 col/rep^2 (e^{2 betacol (rad0-ss)} - e^{betacol (rad0-ss)})
+ *        |z/ss| min(area, dx^2)/max(area, dx^2),  ss < rad0,
+ * in FP64, added to FZ with one rounding.  A point exactly on the wall gives
+ * 0/0 in |z/ss|, as in the reference.  The constants are those of the
+ * reference's param.f90:57,64 (col = 5.68533e-2, betacol = 15.36,
+ * rad0 = 2.5 dz, rep = Rep = 0.0016), set once with sg_set_wall_collisions.
+ * in_step = 1 makes sg_step (and a graph captured from it) apply the force
+ * between the membrane force and the spreading, as main.f90:229-233 calls
+ * complagrforces, collisions, lagr2eulr; then FZ returned by sg_step includes
+ * it.  sg_membrane_force never includes it (complagrforces does not).
+ * Returns SG_ERR_STATE from sg_collisions before any parameters are set, and
+ * from sg_set_wall_collisions while a captured graph exists. */
+int sg_set_wall_collisions(sg_ctx* ctx, int in_step, double col, double betacol, double rad0, double rep);
+int sg_collisions(sg_ctx* ctx, const double* Z, const void* AREA, void* FZ);
+
 /* Spreading for callers that cannot allocate device memory.  It has no
  * counterpart in the reference; it is sg_spread (lagr2eulr) without a
  * context.  It is for host codes whose device memory is all owned by their

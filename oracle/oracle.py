@@ -179,6 +179,15 @@ def update_pos(dt, lz, x, y, z, u, v, w):
     return x, y, z
 
 
+def collisions(z, area, fz, dx, dy, col=5.68533e-2, betacol=15.36, rep=0.0016, rad0=None, dz=None):
+    """collisions.f90:10-32: returns fz + the wall force (rad0 defaults to 2.5 dz)."""
+    if rad0 is None:
+        rad0 = 2.5 * dz
+    out = _f64(fz).copy()
+    lib().or_collisions(z.size, _p(_f64(z)), _p(_f64(area)), dx, dy, col, betacol, rep, rad0, _p(out))
+    return out
+
+
 def surf_vol(x, y, z, nx, ny, nz, area, exy1_prev=0.0):
     out = np.zeros(7)
     lib().or_surf_vol(x.size, *[_p(_f64(a)) for a in (x, y, z, nx, ny, nz, area)], float(exy1_prev), _p(out))

@@ -38,7 +38,7 @@ EXPORTS = ["sg_create", "sg_destroy", "sg_last_error", "sg_synchronize", "sg_int
            "sg_surrogate_params", "sg_surrogate_set_linear", "sg_surrogate_train", "sg_surrogate_predict",
            "sg_surrogate_set_trust", "sg_surrogate_last_counts", "sg_set_point_split", "sg_get_point_split",
            "sg_set_tensor_cores", "sg_set_legendre_terms", "sg_get_legendre_terms", "sg_set_capsule_law",
-           "sg_set_legendre_tile_rows", "sg_get_legendre_tile_rows"]
+           "sg_set_legendre_tile_rows", "sg_get_legendre_tile_rows", "sg_set_wall_collisions", "sg_collisions"]
 # test hooks declared in include/sg_testing.h
 TEST_EXPORTS = ["sg_test_legendre", "sg_test_gemm", "sg_test_mlp_grad"]
 WORKLOAD_EXPORTS = ["sg_prescribed_flow"]  # include/sg_workload.h
@@ -86,6 +86,8 @@ def lib():
     L.sg_step.argtypes = [vp] * 20
     L.sg_update_pos.argtypes = [vp, ctypes.c_double] + [vp] * 6
     L.sg_surf_vol.argtypes = [vp] * 10
+    L.sg_set_wall_collisions.argtypes = [vp, ctypes.c_int] + [ctypes.c_double] * 4
+    L.sg_collisions.argtypes = [vp] * 4
     L.sg_gauss.argtypes = [ctypes.c_int, dp, dp]
     L.sg_legendre.argtypes = [ctypes.c_double, ctypes.c_int, ctypes.c_int, dp, dp, dp]
     L.sg_last_launch_count.argtypes = [vp]
@@ -447,6 +449,20 @@ class CouplingStep:
         """Update_Pos.f90:95-126 -- in place on X, Y, Z."""
         self._check(lib().sg_update_pos(self._h, ctypes.c_double(dt), *map(_ptr, (X, Y, Z, U, V, W))),
                     "sg_update_pos")
+
+    def set_wall_collisions(self, in_step=True, col=5.68533e-2, betacol=15.36, rad0=None, rep=0.0016):
+        """Constants of collisions.f90 (param.f90:57,64; rad0 defaults to 2.5 dz).
+        in_step: sg_step applies the wall force between the membrane force and
+        the spreading, as main.f90:229-233 does."""
+        if rad0 is None:
+            rad0 = 2.5 * self.grid[5]
+        self._check(lib().sg_set_wall_collisions(self._h, int(bool(in_step)), float(col), float(betacol),
+                                                 float(rad0), float(rep)), "sg_set_wall_collisions")
+
+    def collisions(self, Z, AREA, FZ):
+        """collisions.f90:10-32 -- FZ += wall force, in place."""
+        self._check(lib().sg_collisions(self._h, *map(_ptr, (Z, AREA, FZ))), "sg_collisions")
+        return FZ
 
     def surf_vol(self, X, Y, Z, NX, NY, NZ, AREA, exy1_prev=None):
         """surf_vol.f90:12 -- [ncap, 7]: volume, area, exy1, exy2, centroid."""

@@ -613,6 +613,10 @@ int run_step(sg_ctx* c, int what, const void* u, const void* v, const void* w, c
   SG_RET(mark(2));
   if (what & 2) {
     SG_RET(dev_forces<T>(c, dX, dY, dZ, L[3], L[4], L[5], L[6], L[7], L[8], L[9]));
+    if (c->wall_in_step && (what & 4)) {  // call collisions between complagrforces and lagr2eulr (main.f90:229-233)
+      SG_TRY(launch_collisions<T>(c->npts, c->wall, dZ, L[9], L[5], c->ibw.frc, c->grid.dvi, c->st), "collisions");
+      c->launches += c->npts > 0 ? 1 : 0;
+    }
     if (host) {
       void* outs[7] = {FX, FY, FZ, NX, NY, NZ, A};
       for (int q = 0; q < 7; ++q) SG_RET(d2h(c, outs[q], L[3 + q], lb));
@@ -808,6 +812,42 @@ int sg_update_pos(sg_ctx* c, double dt, double* X, double* Y, double* Z, const v
     SG_RET(d2h(c, Y, dY, pb));
     SG_RET(d2h(c, Z, dZ, pb));
   }
+  return finish(c);
+}
+
+int sg_set_wall_collisions(sg_ctx* c, int in_step, double col, double betacol, double rad0, double rep) {
+  if (!c) return SG_ERR_ARG;
+  if (c->graph) return fail(c, SG_ERR_STATE, "release the captured graph first");
+  if (!std::isfinite(col) || !std::isfinite(betacol) || !(rad0 > 0.0) || !std::isfinite(rad0) || !(rep > 0.0) ||
+      !std::isfinite(rep))
+    return fail(c, SG_ERR_ARG, "wall collision parameters must be finite, rad0 and rep positive");
+  c->wall = sg::WallParams{col, betacol, rad0, rep, c->cfg.lx / c->cfg.itot, c->cfg.ly / c->cfg.jtot};
+  c->wall_set = true;
+  c->wall_in_step = in_step != 0;
+  return SG_OK;
+}
+
+int sg_collisions(sg_ctx* c, const double* Z, const void* AREA, void* FZ) {
+  if (!c) return SG_ERR_ARG;
+  if (!c->wall_set) return fail(c, SG_ERR_STATE, "wall collision parameters not set (sg_set_wall_collisions)");
+  SG_RET(check_ptrs(c, {Z, AREA, FZ}));
+  const bool host = c->cfg.mem == SG_MEM_HOST;
+  const size_t pb = sizeof(double) * c->npts, lb = c->esz * c->npts;
+  const double* dZ = Z;
+  const void* dA = AREA;
+  void* dF = FZ;
+  if (host) {
+    SG_RET(h2d(c, c->s_Z, Z, pb));
+    SG_RET(h2d(c, c->s_lag[9], AREA, lb));
+    SG_RET(h2d(c, c->s_lag[5], FZ, lb));
+    dZ = c->s_Z; dA = c->s_lag[9]; dF = c->s_lag[5];
+  }
+  cudaError_t e = c->mixed ? launch_collisions<float>(c->npts, c->wall, dZ, (const float*)dA, (float*)dF, nullptr,
+                                                      c->grid.dvi, c->st)
+                           : launch_collisions<double>(c->npts, c->wall, dZ, (const double*)dA, (double*)dF, nullptr,
+                                                       c->grid.dvi, c->st);
+  if (e != cudaSuccess) return cuda_fail(c, e, "collisions");
+  if (host) SG_RET(d2h(c, FZ, dF, lb));
   return finish(c);
 }
 

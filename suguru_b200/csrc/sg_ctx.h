@@ -53,6 +53,9 @@ struct sg_ctx {
   RowWork* d_wfin = nullptr;
   int nwpos = 0, nwmem = 0, nwsh = 0, nwfin = 0;
   int point_split = 1;  // work items per capsule of the pointwise kernels
+  // wall collision force (collisions.f90): parameters set, and applied inside sg_step
+  bool wall_set = false, wall_in_step = false;
+  sg::WallParams wall{};
   LegProblem* d_probs = nullptr;
   LegWork* d_lw[6] = {};
   int nlw[6] = {};

@@ -24,6 +24,34 @@ __global__ void update_pos_kernel(long n, double dt, double lz, double* __restri
   Z[p] = z;
 }
 
+// collisions.f90:10-32: the Morse-potential force of the wall z = 0 on every
+// point closer than rad0, summed over the wall's lattice images
+// (j dy, k dx) within the cutoff, added to fz.  Evaluated in FP64 in the
+// reference's operation order (including its k dx spacing under a bound taken
+// from dy, and |z / ss|, which is 0/0 for a point exactly on the wall); the
+// sum is added to FZ with one rounding.
+template <class T>
+__global__ void collisions_kernel(long n, WallParams wp, const double* __restrict__ Z, const T* __restrict__ A,
+                                  T* __restrict__ FZ, ForceRec<T>* __restrict__ frc, double dvi) {
+  const long p = (long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (p >= n) return;
+  const double z = Z[p], a = (double)A[p], dx2 = wp.dx * wp.dx;
+  const long jm = lround(sqrt(fmax(wp.rad0 * wp.rad0 - z * z, 0.)) * (1.0 / wp.dy));
+  if (jm == 0 && !(fabs(z) < wp.rad0)) return;  // no lattice image within the cutoff: fc = 0
+  const double amp = 2. * (wp.col / (wp.rep * wp.rep));
+  const double ratio = fmin(a, dx2) / fmax(a, dx2);
+  double fc = 0.;
+  for (long j = -jm; j <= jm; ++j)
+    for (long k = -jm; k <= jm; ++k) {
+      const double ss = sqrt(z * z + (j * wp.dy) * (j * wp.dy) + (k * wp.dx) * (k * wp.dx));
+      if (ss < wp.rad0)
+        fc += amp * (exp(2. * wp.betacol * (wp.rad0 - ss)) - exp(wp.betacol * (wp.rad0 - ss))) * fabs(z / ss) * ratio;
+    }
+  const T fz = (T)((double)FZ[p] + fc);
+  FZ[p] = fz;
+  if (frc) frc[p].cf[2] = fz * (A[p] * (T)dvi);
+}
+
 // One block per capsule; deterministic tree reductions in FP64.
 template <class T>
 __global__ void __launch_bounds__(256) surf_vol_kernel(const CapInfo* __restrict__ caps, const double* __restrict__ X,
@@ -122,6 +150,14 @@ cudaError_t launch_update_pos(long n, double dt, double lz, double* X, double* Y
 }
 
 template <class T>
+cudaError_t launch_collisions(long n, const WallParams& wp, const double* Z, const T* A, T* FZ, void* frc, double dvi,
+                              cudaStream_t st) {
+  if (n <= 0) return cudaSuccess;
+  collisions_kernel<T><<<(unsigned)((n + 255) / 256), 256, 0, st>>>(n, wp, Z, A, FZ, (ForceRec<T>*)frc, dvi);
+  return cudaGetLastError();
+}
+
+template <class T>
 cudaError_t launch_surf_vol(int ncap, const CapInfo* caps, const double* X, const double* Y, const double* Z,
                             const T* NX, const T* NY, const T* NZ, const T* AREA, const double* exy1_prev,
                             double* out, cudaStream_t st) {
@@ -141,6 +177,10 @@ template cudaError_t launch_update_pos<double>(long, double, double, double*, do
                                                const double*, const double*, cudaStream_t);
 template cudaError_t launch_update_pos<float>(long, double, double, double*, double*, double*, const float*,
                                               const float*, const float*, cudaStream_t);
+template cudaError_t launch_collisions<double>(long, const WallParams&, const double*, const double*, double*, void*,
+                                                double, cudaStream_t);
+template cudaError_t launch_collisions<float>(long, const WallParams&, const double*, const float*, float*, void*,
+                                               double, cudaStream_t);
 template cudaError_t launch_surf_vol<double>(int, const CapInfo*, const double*, const double*, const double*,
                                              const double*, const double*, const double*, const double*,
                                              const double*, double*, cudaStream_t);

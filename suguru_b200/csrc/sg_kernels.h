@@ -19,8 +19,8 @@ struct alignas(16) PosRec {
   int b[4];
   T f[4];
 };
-// Per point, for the spread: cf[c] = F_c * area / dV (c = 0..2) and
-// cf[3] = max_c |cf[c]| (the bound of the fixed-point scale).
+// Per point, for the spread: cf[c] = F_c * area / dV (c = 0..2); cf[3] pads
+// the record to 16 (FP32) or 32 (FP64) bytes and is written as zero.
 template <class T>
 struct alignas(16) ForceRec {
   T cf[4];
@@ -225,6 +225,16 @@ cudaError_t launch_final(const RowWork* work, int nwork, const CapInfo* caps, co
 template <class T>
 cudaError_t launch_update_pos(long n, double dt, double lz, double* X, double* Y, double* Z, const T* U, const T* V,
                               const T* W, cudaStream_t st);
+// Wall collision force of collisions.f90:10-32 (constants of param.f90:57,64)
+struct WallParams {
+  double col, betacol, rad0, rep, dx, dy;
+};
+// FZ += the wall force of each point (in place).  With frc, the spread's force
+// records are brought up to date as well (cf[2] = FZ * (A * dvi)), as
+// pack_forces would compute them.
+template <class T>
+cudaError_t launch_collisions(long n, const WallParams& wp, const double* Z, const T* A, T* FZ, void* frc, double dvi,
+                              cudaStream_t st);
 template <class T>
 cudaError_t launch_surf_vol(int ncap, const CapInfo* caps, const double* X, const double* Y, const double* Z,
                             const T* NX, const T* NY, const T* NZ, const T* AREA, const double* exy1_prev,

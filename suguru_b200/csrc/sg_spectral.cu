@@ -730,7 +730,7 @@ __global__ void __launch_bounds__(256) final_kernel(const RowWork* __restrict__ 
             rc.cf[0] = (h ? ev[0] - od[0] : ev[0] + od[0]) * s;
             rc.cf[1] = (h ? ev[1] - od[1] : ev[1] + od[1]) * s;
             rc.cf[2] = (h ? ev[2] - od[2] : ev[2] + od[2]) * s;
-            rc.cf[3] = fmax(fabs(rc.cf[0]), fmax(fabs(rc.cf[1]), fabs(rc.cf[2])));
+            rc.cf[3] = T(0);
             frc[p + h * H] = rc;
           }
         }

@@ -10,28 +10,30 @@
 // point whose stencil reaches the tile, listed by the binning pass -- are
 // processed one point per thread: the thread evaluates the point's 1-D kernel
 // weights and adds its contributions to the cells of the stencil that lie in
-// the tile.  Sums are kept in shared memory in fixed point with a per-tile
-// power-of-two scale and added with 32-bit integer atomics: integer addition
-// is exact and associative, so the field is bitwise independent of the order
-// in which threads add (no floating-point atomics, deterministic run to run).
+// the tile.  Sums are kept in shared memory in fixed point with per-tile,
+// per-component power-of-two scales and added with 32-bit integer atomics:
+// integer addition is exact and associative, so the field is bitwise
+// independent of the order in which threads add (no floating-point atomics,
+// deterministic run to run).  Each component has its own scale, so that its
+// relative precision does not depend on the other components' magnitudes.
 //
-//  - FP32: one signed 32-bit word per cell and component.  With m =
-//    max_c |f_c * area / dV| per entry, the scale is the smaller of two powers
-//    of two: one that puts 0.3 * sum over the tile's entries of m below 2^30
-//    (every 3-D kernel weight is at most (2/3)^3 < 0.3, so no cell sum can
-//    reach 2^31), and one that puts 0.3 * the largest m below 2^22, so that
-//    every contribution v satisfies |v| < 2^22.  The sum of m is needed only
-//    above 2^8 entries (below, count * largest m bounds it tightly enough)
-//    and is then an exact integer sum of m rounded up to 2^-12 of the largest
-//    m's binade, so that the scale, like the cell sums, is independent of the
-//    order of the entries.  Then one FMA, v + 1.5 * 2^23, rounds
-//    v to the nearest integer (ties to even) in the low mantissa bits of a
-//    float whose exponent is fixed, and the integer is its bit pattern minus
-//    that of 1.5 * 2^23 -- no conversion instruction per contribution.  The
-//    fixed-point step is 2^-22 of 0.3 times the largest contribution's force,
-//    below FP32 rounding of a typical cell value.
-//  - FP64: 64-bit fixed point (|sum| < 2^56 from the tile's largest
-//    contribution times its entry count) kept as three limbs of 19 bits, the
+//  - FP32: one signed 32-bit word per cell and component.  With m_c =
+//    |f_c * area / dV| per entry, the scale of component c is the smaller of
+//    two powers of two: one that puts 0.3 * sum over the tile's entries of m_c
+//    below 2^30 (every 3-D kernel weight is at most (2/3)^3 < 0.3, so no cell
+//    sum can reach 2^31), and one that puts 0.3 * the largest m_c below 2^22,
+//    so that every contribution v satisfies |v| < 2^22.  The sum is needed
+//    only above 2^8 entries (below, count * largest m_c bounds it tightly
+//    enough) and is then an exact integer sum of m_c rounded up to 2^-12 of
+//    the largest m_c's binade, so that the scales, like the cell sums, are
+//    independent of the order of the entries.  Then one FMA, v + 1.5 * 2^23,
+//    rounds v to the nearest integer (ties to even) in the low mantissa bits
+//    of a float whose exponent is fixed, and the integer is its bit pattern
+//    minus that of 1.5 * 2^23 -- no conversion instruction per contribution.
+//    The fixed-point step is 2^-22 of 0.3 times the component's largest
+//    contribution, below FP32 rounding of a typical cell value.
+//  - FP64: 64-bit fixed point (|sum| < 2^56 from the component's largest
+//    contribution in the tile times its entry count) kept as three limbs of 19 bits, the
 //    lower two unsigned, so that the atomics stay native 32-bit adds; with at
 //    most 4096 contributions per pass no limb can overflow, and between passes
 //    the limbs are folded into 64-bit registers.
@@ -80,18 +82,31 @@ struct Fixed<double> {
   }
 };
 
-// the smallest e with b < 2^e (0 for b <= 0), at least -60 so that the
-// scales stay finite in float
+// The smallest e with b < 2^e (0 for b <= 0), at least -60 so that the
+// scales stay finite in float: the exponent field of b read directly (these
+// run once per thread and tile, so no library frexp/ldexp calls).
 __device__ __forceinline__ int exp_above(double b) {
-  int ex = 0;
-  if (b > 0.0) frexp(b, &ex);
-  return ex < -60 ? -60 : ex;
+  if (!(b > 0.0)) return 0;
+  const int e = (int)((__double_as_longlong(b) >> 52) & 0x7ff) - 1022;
+  return e < -60 ? -60 : e;
+}
+
+// exact 2^e, built from its exponent field inside the normal range
+template <class T>
+__device__ __forceinline__ T pow2(int e);
+template <>
+__device__ __forceinline__ float pow2<float>(int e) {
+  return (e >= -126 && e <= 127) ? __int_as_float((e + 127) << 23) : (float)ldexp(1.0, e);
+}
+template <>
+__device__ __forceinline__ double pow2<double>(int e) {
+  return (e >= -1022 && e <= 1023) ? __longlong_as_double((long long)(e + 1023) << 52) : ldexp(1.0, e);
 }
 
 }  // namespace
 
-// Force records cf = F * (A / dV) and their largest component magnitude
-// (interp_spread.f90:870-874 multiplies by area / dVeul in this order).
+// Force records cf = F * (A / dV) (interp_spread.f90:870-874 multiplies by
+// area / dVeul in this order).
 template <class T>
 __global__ void pack_forces_kernel(long n, double dvi, const T* __restrict__ FX, const T* __restrict__ FY,
                                    const T* __restrict__ FZ, const T* __restrict__ A, ForceRec<T>* __restrict__ frc) {
@@ -102,12 +117,12 @@ __global__ void pack_forces_kernel(long n, double dvi, const T* __restrict__ FX,
   r.cf[0] = FX[p] * s;
   r.cf[1] = FY[p] * s;
   r.cf[2] = FZ[p] * s;
-  r.cf[3] = fmax(fabs(r.cf[0]), fmax(fabs(r.cf[1]), fabs(r.cf[2])));
+  r.cf[3] = T(0);
   frc[p] = r;
 }
 
 template <class T, int TX, int TY, int TZ>
-__global__ void __launch_bounds__(256) spread_kernel(IBGrid g, const int* __restrict__ entries,
+__global__ void __launch_bounds__(256, sizeof(T) == 4 ? 4 : 2) spread_kernel(IBGrid g, const int* __restrict__ entries,
                                                      const int* __restrict__ starts,
                                                      const PosRec<T>* __restrict__ pos,
                                                      const ForceRec<T>* __restrict__ frc, T* __restrict__ ox,
@@ -122,8 +137,8 @@ __global__ void __launch_bounds__(256) spread_kernel(IBGrid g, const int* __rest
   // contributions falling outside the tile, so that the walk has no branches
   constexpr int NCP = NC + 32;
   __shared__ __align__(16) unsigned int acc[NW][3][NCP];
-  __shared__ T s_red[8];
-  __shared__ unsigned long long s_sum[8];
+  __shared__ T s_red[3][8];
+  __shared__ unsigned long long s_sum[3][8];
   long long tot[NT][3];
 #pragma unroll
   for (int r = 0; r < NT; ++r) tot[r][0] = tot[r][1] = tot[r][2] = 0;
@@ -133,54 +148,97 @@ __global__ void __launch_bounds__(256) spread_kernel(IBGrid g, const int* __rest
   const int cw = min(TX, g.itot - TX * tx), ch = min(TY, g.jtot - TY * ty), cd = min(TZ, g.ktot - TZ * tz);
   const int i0 = 1 + TX * tx, j0 = 1 + TY * ty, k0 = 1 + TZ * tz;
   const int e0 = starts[tile], e1 = starts[tile + 1];
-  T iscale = T(0);
+  T iscale[3] = {T(0), T(0), T(0)};
 
   if (e1 > e0) {
     for (int q = tid; q < NW * 3 * NCP / 4; q += 256) ((uint4*)&acc[0][0][0])[q] = make_uint4(0u, 0u, 0u, 0u);
-    // ---- fixed-point scale from m = max_c |f_c * area / dV| over the tile's
-    // entries.  Only order-independent quantities enter it -- the largest m,
-    // the entry count and an integer sum -- so that the scale, like the sums,
-    // does not depend on the order in which the binning listed the entries.
-    T rmax = T(0);
-    for (int e = e0 + tid; e < e1; e += 256) rmax = fmax(rmax, frc[entries[e]].cf[3]);
+    // ---- fixed-point scales, one per component c, from m_c = |f_c * area / dV|
+    // over the tile's entries.  Only order-independent quantities enter them
+    // -- the largest m_c, the entry count and an integer sum -- so that the
+    // scales, like the sums, do not depend on the order of the entries.  A
+    // scale per component keeps each component's relative precision when
+    // another one is much larger (a wall force of collisions.f90 beside a
+    // membrane force).
+    T rmax[3] = {T(0), T(0), T(0)};
+    for (int e = e0 + tid; e < e1; e += 256) {
+      const ForceRec<T> fo = frc[entries[e]];
 #pragma unroll
-    for (int o = 16; o > 0; o >>= 1) rmax = fmax(rmax, __shfl_xor_sync(0xffffffffu, rmax, o));
-    if (lane == 0) s_red[warp] = rmax;
+      for (int c = 0; c < 3; ++c) rmax[c] = fmax(rmax[c], fabs(fo.cf[c]));
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1)
+#pragma unroll
+      for (int c = 0; c < 3; ++c) rmax[c] = fmax(rmax[c], __shfl_xor_sync(0xffffffffu, rmax[c], o));
+    if (lane == 0)
+#pragma unroll
+      for (int c = 0; c < 3; ++c) s_red[c][warp] = rmax[c];
     __syncthreads();
-    rmax = s_red[0];
 #pragma unroll
-    for (int q = 1; q < 8; ++q) rmax = fmax(rmax, s_red[q]);
+    for (int c = 0; c < 3; ++c) {
+      rmax[c] = s_red[c][0];
+#pragma unroll
+      for (int q = 1; q < 8; ++q) rmax[c] = fmax(rmax[c], s_red[c][q]);
+    }
     const int cnt = e1 - e0;
-    // FP64: |sum| < 2^QB from the largest m times the entry count
-    int sh = QB - exp_above((double)rmax * (double)(F32 ? 0.3 * cnt : cnt));
+    // FP64: |sum| < 2^QB from the largest m_c times the entry count
+    int sh[3];
+#pragma unroll
+    for (int c = 0; c < 3; ++c) sh[c] = QB - exp_above((double)rmax[c] * (double)(F32 ? 0.3 * cnt : cnt));
     if constexpr (F32) {
       // every single contribution below 2^22 ...
-      const int sh1 = 22 - exp_above(0.3 * (double)rmax);
-      if (sh < sh1) {
+      int sh1[3];
+      bool dense = false;
+#pragma unroll
+      for (int c = 0; c < 3; ++c) {
+        sh1[c] = 22 - exp_above(0.3 * (double)rmax[c]);
+        dense = dense || sh[c] < sh1[c];
+      }
+      if (dense) {  // uniform across the CTA: computed from the block-wide maxima
         // ... and, where the count bound would cost precision (more than 2^8
-        // entries), |sum| < 2^30 from 0.3 * sum of m, taken as an exact integer
-        // sum of m rounded up to multiples of 2^-12 of the largest m's binade
-        int exr = 0;
-        frexp((double)rmax, &exr);  // rmax < 2^exr
-        const double u = ldexp(1.0, 12 - exr);
-        unsigned long long s = 0;
+        // entries), |sum| < 2^30 from 0.3 * sum of m_c, taken as an exact
+        // integer sum of m_c rounded up to multiples of 2^-12 of the largest
+        // m_c's binade
+        int exr[3];
+        double u[3];
+        unsigned long long sm[3] = {0ull, 0ull, 0ull};
+#pragma unroll
+        for (int c = 0; c < 3; ++c) {
+          exr[c] = exp_above((double)rmax[c]);  // rmax_c < 2^exr
+          u[c] = pow2<double>(12 - exr[c]);
+        }
         for (int e = e0 + tid; e < e1; e += 256) {
-          const double v = (double)frc[entries[e]].cf[3] * u;  // < 2^12, exact
-          s += v > 0.0 ? (unsigned long long)ceil(v) : 0ull;
+          const ForceRec<T> fo = frc[entries[e]];
+#pragma unroll
+          for (int c = 0; c < 3; ++c) {
+            const double v = fabs((double)fo.cf[c]) * u[c];  // < 2^12, exact
+            sm[c] += v > 0.0 ? (unsigned long long)ceil(v) : 0ull;
+          }
         }
 #pragma unroll
-        for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
-        if (lane == 0) s_sum[warp] = s;
-        __syncthreads();
-        s = 0;
+        for (int o = 16; o > 0; o >>= 1)
 #pragma unroll
-        for (int q = 0; q < 8; ++q) s += s_sum[q];
-        sh = QB - exp_above(0.3 * ldexp((double)s, exr - 12));
+          for (int c = 0; c < 3; ++c) sm[c] += __shfl_xor_sync(0xffffffffu, sm[c], o);
+        if (lane == 0)
+#pragma unroll
+          for (int c = 0; c < 3; ++c) s_sum[c][warp] = sm[c];
+        __syncthreads();
+#pragma unroll
+        for (int c = 0; c < 3; ++c) {
+          unsigned long long t = 0;
+#pragma unroll
+          for (int q = 0; q < 8; ++q) t += s_sum[c][q];
+          if (sh[c] < sh1[c]) sh[c] = QB - exp_above(0.3 * ((double)t * pow2<double>(exr[c] - 12)));
+        }
       }
-      sh = min(sh, sh1);
+#pragma unroll
+      for (int c = 0; c < 3; ++c) sh[c] = min(sh[c], sh1[c]);
     }
-    const T scale = (T)ldexp(1.0, sh);
-    iscale = (T)ldexp(1.0, -sh);
+    T scale[3];
+#pragma unroll
+    for (int c = 0; c < 3; ++c) {
+      scale[c] = pow2<T>(sh[c]);
+      iscale[c] = pow2<T>(-sh[c]);
+    }
 
     // ---- one point per thread, in passes of at most PASS entries
     for (int c0 = e0; c0 < e1; c0 += Fixed<T>::PASS) {
@@ -197,8 +255,8 @@ __global__ void __launch_bounds__(256) spread_kernel(IBGrid g, const int* __rest
         const ForceRec<T> fo = frc[p];
         const int bb[3] = {rec.b[0], rec.b[1], rec.b[2]};
         const T fr[3] = {rec.f[0], rec.f[1], rec.f[2]};
-        // scaled forces; scale is a power of two, so this multiply is exact
-        const T cf[3] = {fo.cf[0] * scale, fo.cf[1] * scale, fo.cf[2] * scale};
+        // scaled forces; each scale is a power of two, so these multiplies are exact
+        const T cf[3] = {fo.cf[0] * scale[0], fo.cf[1] * scale[1], fo.cf[2] * scale[2]};
         // 1-D weights: the three nonzero values of the 3-point kernel around the
         // nearest node share one square root.  With r = (nearest node) - c,
         // |r| <= 1/2, s = sqrt(1 - 3 r^2):
@@ -302,14 +360,14 @@ __global__ void __launch_bounds__(256) spread_kernel(IBGrid g, const int* __rest
     T vu = T(0), vv = T(0), vw = T(0);
     if (e1 > e0) {
       if constexpr (F32) {
-        // one rounding of the fixed-point value; iscale is a power of two
-        vu = (float)(int)acc[0][0][q] * iscale;
-        vv = (float)(int)acc[0][1][q] * iscale;
-        vw = (float)(int)acc[0][2][q] * iscale;
+        // one rounding of the fixed-point value; each iscale is a power of two
+        vu = (float)(int)acc[0][0][q] * iscale[0];
+        vv = (float)(int)acc[0][1][q] * iscale[1];
+        vw = (float)(int)acc[0][2][q] * iscale[2];
       } else {
-        vu = (double)tot[r][0] * iscale;
-        vv = (double)tot[r][1] * iscale;
-        vw = (double)tot[r][2] * iscale;
+        vu = (double)tot[r][0] * iscale[0];
+        vv = (double)tot[r][1] * iscale[1];
+        vw = (double)tot[r][2] * iscale[2];
       }
     }
     const int i = i0 + lx, j = j0 + ly, k = k0 + lz;
