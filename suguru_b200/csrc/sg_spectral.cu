@@ -491,6 +491,169 @@ __global__ void __launch_bounds__(256, sizeof(T) == 4 ? 3 : 2) membrane_kernel(c
   }
 }
 
+// ------------------------------------------------- membrane, FP32 pairs ---
+// The FP32 membrane kernel with the longitude synthesis and the forward DFT
+// on packed pairs (sm_100 f32x2 arithmetic: __ffma2_rn and friends compute
+// each lane as an IEEE FP32 operation).  In the synthesis the pair is
+// (even m, odd m): the two half-turn sums of membrane_kernel take one
+// instruction per operation.  In the forward DFT it is (even j, odd j): two
+// partial sums, added at the end.  Staging keeps a pair's 18 values
+// interleaved, [m pair][k][m parity], and the trig table of the synthesis
+// holds (cos m, cos m+1, sin m, sin m+1) per point, so that a thread reads
+// its operands with 16-byte loads; an odd N pads the last pair with zeros.
+constexpr int kGP = 36;  // staged floats per m pair: 18 values x (even m, odd m)
+
+__device__ __forceinline__ float2 p2fma(float2 a, float2 b, float2 c) { return __ffma2_rn(a, b, c); }
+__device__ __forceinline__ float2 p2mul(float2 a, float2 b) { return __fmul2_rn(a, b); }
+__device__ __forceinline__ float2 p2add(float2 a, float2 b) { return __fadd2_rn(a, b); }
+
+// synth_m for the m pair (2 mp, 2 mp + 1) at one point: g = the pair's staged
+// block, t = (cos, cos, sin, sin) of the two m at the point, fm = (m, m + 1)
+__device__ __forceinline__ void synth_pair(const float* g, float4 t, float2 fm, float2 (&acc)[5][3]) {
+  const float2 cm = make_float2(t.x, t.y), nsm = make_float2(-t.z, -t.w), ncm = make_float2(-t.x, -t.y);
+  const float2 nfm2 = make_float2(-fm.x * fm.x, -fm.y * fm.y);
+  const float4* gq = (const float4*)g;
+#pragma unroll
+  for (int c = 0; c < 3; ++c) {
+    // k = 6c .. 6c+5: P, dP, d2P of the cos row, then of the sin row
+    const float4 x0 = gq[3 * c], x1 = gq[3 * c + 1], x2 = gq[3 * c + 2];
+    const float2 P_a = make_float2(x0.x, x0.y), D_a = make_float2(x0.z, x0.w), E_a = make_float2(x1.x, x1.y);
+    const float2 P_b = make_float2(x1.z, x1.w), D_b = make_float2(x2.x, x2.y), E_b = make_float2(x2.z, x2.w);
+    const float2 t0P = p2fma(P_a, cm, p2mul(P_b, nsm));                      // P_a cm - P_b sm
+    const float2 t1P = p2mul(fm, p2fma(P_a, nsm, p2mul(P_b, ncm)));          // m (-P_a sm - P_b cm)
+    acc[0][c] = p2fma(D_a, cm, p2fma(D_b, nsm, acc[0][c]));                  // vat1
+    acc[1][c] = p2add(acc[1][c], t1P);                                       // vat2
+    acc[2][c] = p2fma(E_a, cm, p2fma(E_b, nsm, acc[2][c]));                  // deFvat1(:,1)
+    acc[3][c] = p2fma(fm, p2fma(D_a, nsm, p2mul(D_b, ncm)), acc[3][c]);      // deFvat1(:,2)
+    acc[4][c] = p2fma(nfm2, t0P, acc[4][c]);                                 // deFvat2(:,2)
+  }
+}
+
+__global__ void __launch_bounds__(256, 3) membrane_kernel_f2(const RowWork* __restrict__ work, int nwork,
+                                                             const CapInfo* __restrict__ caps,
+                                                             const GroupDev* __restrict__ groups,
+                                                             const int* __restrict__ sur_flag, int* __restrict__ err) {
+  (void)err;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5, nwarp = blockDim.x >> 5;
+  for (int w = blockIdx.x; w < nwork; w += gridDim.x) {
+    const RowWork it = work[w];
+    const CapInfo ci = caps[it.cap];
+    const float hf = (float)(0.5 * ci.gs), csk = (float)ci.csk;  // hf_gscell = 0.5 gscell (sph.f90:35)
+    const bool normals_only = sur_flag && sur_flag[it.cap];
+    const GroupDev gd = groups[it.group];
+    const int N = gd.N, nD = gd.nD, mD = gd.mD, H = mD >> 1, NP = (N + 1) >> 1;
+    const int RP = (int)blockDim.x / H > 0 ? (int)blockDim.x / H : 1;  // rows per chunk, H threads each
+    const int SR = NP * kGP + 4;      // staged row stride (one 16-byte pad)
+    const int TS = H + 2;             // row stride of the DFT trig table (8-byte aligned rows)
+    const int OS = 2 * H + 4;         // output line: half-turn sums at [j], differences at [H + 2 + j]
+    float* sG = (float*)smem_raw;                       // [RP][SR]
+    float4* sTP = (float4*)(sG + RP * SR);              // [NP][H]
+    float* sTrig = (float*)(sTP + NP * H);              // [2N][TS]: cos m phi_j (rows m), sin (rows N + m)
+    float* sOut = sTrig + 2 * N * TS;                   // [RP][6][OS]
+    const float* G = (const float*)gd.buf.G + (long long)ci.gidx * (18 * N * nD);  // [ccs][m][kind][lat]
+    const float* trig = (const float*)gd.trigD[1];
+    const float* lat = (const float*)gd.latD[1];
+    float* Fout = (float*)gd.buf.Fout + (long long)ci.gidx * 12 * N * nD;
+    const float sfn = 2.0f / (float)mD;
+    const float R = (float)ci.R;
+    __syncthreads();  // the previous item's reads of shared memory are done
+    for (int q = tid; q < NP * H; q += blockDim.x) {
+      const int mp = q / H, j = q - mp * H, m = 2 * mp;
+      const bool odd = m + 1 < N;
+      sTP[q] = make_float4(trig[m * mD + j], odd ? trig[(m + 1) * mD + j] : 0.0f, trig[(N + m) * mD + j],
+                           odd ? trig[(N + m + 1) * mD + j] : 0.0f);
+    }
+    for (int q = tid; q < 2 * N * H; q += blockDim.x) {
+      const int hm = q / H, j = q - hm * H;
+      sTrig[hm * TS + j] = trig[hm * mD + j];
+    }
+    for (int rb = it.row0; rb < it.row0 + it.nrows; rb += RP) {
+      const int rows = min(RP, it.row0 + it.nrows - rb);
+      __syncthreads();  // the previous chunk's staged rows and outputs are consumed
+      // stage the chunk's rows to [row][m pair][k][m parity], k = 3 ccs + kind;
+      // a warp reads runs of `rows` consecutive latitudes of one (ccs, m, kind)
+      for (int q = tid; q < 18 * N * rows; q += blockDim.x) {
+        const int e = q / rows, r = q - e * rows;  // e = (ccs N + m) 3 + kind
+        const int kind = e % 3, cm_ = e / 3, m = cm_ % N, ccs = cm_ / N;
+        sG[r * SR + (m >> 1) * kGP + 2 * (3 * ccs + kind) + (m & 1)] = G[(long long)e * nD + rb + r];
+      }
+      if (N & 1)
+        for (int q = tid; q < 18 * rows; q += blockDim.x) {
+          const int r = q / 18, k = q - r * 18;
+          sG[r * SR + (N >> 1) * kGP + 2 * k + 1] = 0.0f;
+        }
+      __syncthreads();
+      {
+        const int r = tid / H, j = tid - (tid / H) * H;
+        if (r < rows) {
+          const int i = rb + r;
+          float2 acc[5][3];
+#pragma unroll
+          for (int a = 0; a < 5; ++a)
+#pragma unroll
+            for (int c = 0; c < 3; ++c) acc[a][c] = make_float2(0.0f, 0.0f);
+          const float* g = sG + r * SR;
+          for (int mp = 0; mp < NP; ++mp)
+            synth_pair(g + mp * kGP, sTP[mp * H + j], make_float2((float)(2 * mp), (float)(2 * mp + 1)), acc);
+          // point j = even + odd, point j + mD/2 = even - odd
+          float ev[5][3], od[5][3];
+#pragma unroll
+          for (int a = 0; a < 5; ++a)
+#pragma unroll
+            for (int c = 0; c < 3; ++c) {
+              ev[a][c] = acc[a][c].x + acc[a][c].y;
+              od[a][c] = acc[a][c].x - acc[a][c].y;
+            }
+          const float st = lat[4 * i], ct = lat[4 * i + 1];
+          const float cp = sTrig[1 * TS + j], sp = sTrig[(N + 1) * TS + j];
+          float fa[3], na[3], fb[3], nb[3];
+          point_force<float>(ev, st, ct, cp, sp, R, hf, csk, ci.law, normals_only, fa, na);
+          point_force<float>(od, st, ct, -cp, -sp, R, hf, csk, ci.law, normals_only, fb, nb);
+          float* o = sOut + r * 6 * OS;
+          const float va[6] = {fa[0], fa[1], fa[2], na[0], na[1], na[2]};
+          const float vb[6] = {fb[0], fb[1], fb[2], nb[0], nb[1], nb[2]};
+#pragma unroll
+          for (int f = 0; f < 6; ++f) {
+            o[f * OS + j] = va[f] + vb[f];
+            o[f * OS + H + 2 + j] = va[f] - vb[f];
+          }
+        }
+      }
+      __syncthreads();
+      // forward DFT of the six outputs per row: warp = (row, field) line, lane
+      // p < 2N = trig row p (cos m = p, sin m = p - N); even and odd j summed
+      // as a pair
+      for (int line = warp; line < rows * 6; line += nwarp) {
+        const int f = line % 6, rr = line / 6;
+        const float* o = sOut + line * OS;
+        for (int p = lane; p < 2 * N; p += 32) {
+          const int m = p < N ? p : p - N;
+          const float2* oo = (const float2*)(o + ((m & 1) ? H + 2 : 0));
+          const float2* t = (const float2*)(sTrig + p * TS);
+          float2 a2 = make_float2(0.0f, 0.0f);
+          for (int jj = 0; jj < (H >> 1); ++jj) a2 = p2fma(oo[jj], t[jj], a2);
+          Fout[((long long)f * 2 * N + p) * nD + rb + rr] = (p < N ? sfn : -sfn) * (a2.x + a2.y);
+        }
+      }
+    }
+  }
+}
+
+// Shared memory (bytes) of membrane_kernel_f2 for degrees up to nmax: the
+// largest over n <= nmax of staged rows RP (NP kGP + 4), the pair trig table
+// NP H float4, the DFT trig table 2n (H + 2) and outputs RP 6 (2H + 4), with
+// H = 2n, NP = ceil(n / 2) and RP = max(1, 256 / H).
+static size_t membrane_f2_smem(int nmax) {
+  size_t e = 0;
+  for (size_t n = 1; n <= (size_t)nmax; ++n) {
+    const size_t H = 2 * n, NP = (n + 1) / 2, RP = 256 / H > 0 ? 256 / H : 1;
+    const size_t en = RP * (NP * kGP + 4) + NP * H * 4 + 2 * n * (H + 2) + RP * 6 * (2 * H + 4) + 64;
+    if (en > e) e = en;
+  }
+  return sizeof(float) * e;
+}
+
 // ------------------------------------------------- SH-grid stage ----------
 // cal_unitO_filter (sph1.f90:1378-1402): truncated normals on the SH grid,
 // renormalised; cal_surface_metric_sph__OPT (sph3.f90:186-277): |a1 x a2| on
@@ -821,11 +984,19 @@ template <class T>
 cudaError_t launch_membrane(const RowWork* work, int nwork, const CapInfo* caps, const GroupDev* groups,
                             const int* sur_flag, int nmax, int* err, cudaStream_t st) {
   if (nwork <= 0) return cudaSuccess;
-  const size_t smem = pointwise_smem<T>(kMembrane, nmax);
-  cudaError_t e = cudaFuncSetAttribute(membrane_kernel<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-  if (e != cudaSuccess) return e;
-  membrane_kernel<T><<<persistent_grid(membrane_kernel<T>, smem, nwork), kPointThreads, smem, st>>>(
-      work, nwork, caps, groups, sur_flag, err);
+  if constexpr (sizeof(T) == 4) {
+    const size_t smem = membrane_f2_smem(nmax);
+    cudaError_t e = cudaFuncSetAttribute(membrane_kernel_f2, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e != cudaSuccess) return e;
+    membrane_kernel_f2<<<persistent_grid(membrane_kernel_f2, smem, nwork), kPointThreads, smem, st>>>(
+        work, nwork, caps, groups, sur_flag, err);
+  } else {
+    const size_t smem = pointwise_smem<T>(kMembrane, nmax);
+    cudaError_t e = cudaFuncSetAttribute(membrane_kernel<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e != cudaSuccess) return e;
+    membrane_kernel<T><<<persistent_grid(membrane_kernel<T>, smem, nwork), kPointThreads, smem, st>>>(
+        work, nwork, caps, groups, sur_flag, err);
+  }
   return cudaGetLastError();
 }
 
