@@ -102,7 +102,9 @@ int sg_step(sg_ctx* ctx, const void* u, const void* v, const void* w,
             void* FX, void* FY, void* FZ, void* NX, void* NY, void* NZ, void* AREA,
             void* fx, void* fy, void* fz);
 
-/* Update_Pos.f90:95-126: X += U*dt, then clamp z into [0, lz]. */
+/* Update_Pos.f90:95-180: X += U*dt, clamp z into [0, lz], then shift every
+ * point of a capsule by -lx (+lx) when the capsule's centroid is beyond lx
+ * (below 0), and likewise in y. */
 int sg_update_pos(sg_ctx* ctx, double dt, double* X, double* Y, double* Z,
                   const void* U, const void* V, const void* W);
 

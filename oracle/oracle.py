@@ -47,6 +47,8 @@ def lib():
         L.or_spread.argtypes = [i, i, i, d, d, d, i, l] + [_dp] * 10
         L.or_update_pos.argtypes = [l, d, d] + [_dp] * 6
         L.or_update_pos.restype = None
+        L.or_update_pos_capsules.argtypes = [ctypes.c_int, ctypes.POINTER(ctypes.c_long), d, d, d, d] + [_dp] * 6
+        L.or_update_pos_capsules.restype = None
         L.or_surf_vol.argtypes = [l] + [_dp] * 7 + [d, _dp]
         L.or_surf_vol.restype = None
         L.or_collisions.argtypes = [l, _dp, _dp, d, d, d, d, d, d, _dp]
@@ -186,6 +188,15 @@ def collisions(z, area, fz, dx, dy, col=5.68533e-2, betacol=15.36, rep=0.0016, r
     out = _f64(fz).copy()
     lib().or_collisions(z.size, _p(_f64(z)), _p(_f64(area)), dx, dy, col, betacol, rep, rad0, _p(out))
     return out
+
+
+def update_pos_capsules(offsets, dt, lx, ly, lz, x, y, z, u, v, w):
+    """Update_Pos.f90:95-180 with the periodic shift of capsules whose centroid left the box."""
+    x, y, z = _f64(x).copy(), _f64(y).copy(), _f64(z).copy()
+    off = np.ascontiguousarray(offsets, dtype=np.int64)
+    lib().or_update_pos_capsules(off.size - 1, off.ctypes.data_as(ctypes.POINTER(ctypes.c_long)), dt, lx, ly, lz,
+                                 _p(x), _p(y), _p(z), _p(_f64(u)), _p(_f64(v)), _p(_f64(w)))
+    return x, y, z
 
 
 def surf_vol(x, y, z, nx, ny, nz, area, exy1_prev=0.0):

@@ -1042,6 +1042,24 @@ void or_update_pos(long npts, double dt, double lz, double* xp, double* yp, doub
   }
 }
 
+void or_update_pos_capsules(int ncap, const long* off, double dt, double lx, double ly, double lz, double* xp,
+                            double* yp, double* zp, const double* ul, const double* vl, const double* wl) {
+  // Update_Pos.f90:95-99 and 118-126 per point, then :131-180 per capsule:
+  // sequential centroid, shift by one period when it has left the box
+  or_update_pos(off[ncap], dt, lz, xp, yp, zp, ul, vl, wl);
+  for (int p = 0; p < ncap; ++p) {
+    const long a = off[p], b = off[p + 1];
+    double x = 0., y = 0.;
+    for (long l = a; l < b; ++l) { x += xp[l]; y += yp[l]; }
+    x /= (double)(b - a);
+    y /= (double)(b - a);
+    if (x > lx) for (long l = a; l < b; ++l) xp[l] = xp[l] - lx;
+    if (x < 0.) for (long l = a; l < b; ++l) xp[l] = xp[l] + lx;
+    if (y > ly) for (long l = a; l < b; ++l) yp[l] = yp[l] - ly;
+    if (y < 0.) for (long l = a; l < b; ++l) yp[l] = yp[l] + ly;
+  }
+}
+
 void or_surf_vol(long nl, const double* x, const double* y, const double* z, const double* nx, const double* ny,
                  const double* nz, const double* area, double exy1_prev, double* out) {
   double xm = 0, ym = 0, zm = 0;

@@ -82,6 +82,11 @@ int or_spread(int itot, int jtot, int ktot, double dx, double dy, double dz, int
 /* Update_Pos.f90:95-126: forward Euler + wall clamp to [0,lz]. */
 void or_update_pos(long npts, double dt, double lz, double* xp, double* yp, double* zp,
                    const double* ul, const double* vl, const double* wl);
+/* Update_Pos.f90:95-180 for ncap capsules (points off[p] .. off[p+1]-1):
+ * or_update_pos, then each capsule's sequential centroid and its shift by
+ * one period in x or y when the centroid has left [0, lx] x [0, ly]. */
+void or_update_pos_capsules(int ncap, const long* off, double dt, double lx, double ly, double lz, double* xp,
+                            double* yp, double* zp, const double* ul, const double* vl, const double* wl);
 
 /* surf_vol.f90:12-131 for one capsule of nl points.  out[0]=volume,
  * out[1]=total area, out[2]=exy1, out[3]=exy2, out[4..6]=centroid.

@@ -802,10 +802,11 @@ int sg_update_pos(sg_ctx* c, double dt, double* X, double* Y, double* Z, const v
     dX = c->s_X; dY = c->s_Y; dZ = c->s_Z;
     dU = c->s_lag[0]; dV = c->s_lag[1]; dW = c->s_lag[2];
   }
-  cudaError_t e = c->mixed ? launch_update_pos<float>(c->npts, dt, c->cfg.lz, dX, dY, dZ, (const float*)dU,
-                                                      (const float*)dV, (const float*)dW, c->st)
-                           : launch_update_pos<double>(c->npts, dt, c->cfg.lz, dX, dY, dZ, (const double*)dU,
-                                                       (const double*)dV, (const double*)dW, c->st);
+  const sg_config& f = c->cfg;
+  cudaError_t e = c->mixed ? launch_update_pos<float>(f.ncap, c->d_caps, dt, f.lx, f.ly, f.lz, dX, dY, dZ,
+                                                      (const float*)dU, (const float*)dV, (const float*)dW, c->st)
+                           : launch_update_pos<double>(f.ncap, c->d_caps, dt, f.lx, f.ly, f.lz, dX, dY, dZ,
+                                                       (const double*)dU, (const double*)dV, (const double*)dW, c->st);
   if (e != cudaSuccess) return cuda_fail(c, e, "update_pos");
   if (host) {
     SG_RET(d2h(c, X, dX, pb));

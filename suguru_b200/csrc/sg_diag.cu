@@ -1,8 +1,9 @@
 // sg_diag.cu -- position update and capsule diagnostics.
 //
-// Update_Pos.f90:95-126: forward-Euler advection of the force points with the
-// interpolated velocity and the wall clamp z in [0, lz].  The master/slave
-// migration of Update_Pos.f90:58-72 has no counterpart on one GPU.
+// Update_Pos.f90:95-180: forward-Euler advection of the force points with the
+// interpolated velocity, the wall clamp z in [0, lz], and the periodic shift
+// of a capsule whose centroid has left the box.  The master/slave migration
+// of Update_Pos.f90:58-72 has no counterpart on one GPU.
 // surf_vol.f90:12-131: centroid, volume by the 1000-layer radial quadrature,
 // inertia tensor -> Taylor deformation exy1, exy2; all in FP64.
 #include "sg_common.cuh"
@@ -10,18 +11,62 @@
 
 namespace sg {
 
+// One block per capsule: advection and wall clamp of every point
+// (Update_Pos.f90:95-99, 118-126), then the capsule's centroid and, when it
+// has left the periodic box in x or y, the shift of all its points by one
+// period (Update_Pos.f90:131-180; the reference's centroid is a sequential
+// sum, this one a fixed tree in FP64, so the two agree unless the centroid
+// lies within rounding of a box face).
 template <class T>
-__global__ void update_pos_kernel(long n, double dt, double lz, double* __restrict__ X, double* __restrict__ Y,
-                                  double* __restrict__ Z, const T* __restrict__ U, const T* __restrict__ V,
-                                  const T* __restrict__ W) {
-  long p = (long)blockIdx.x * blockDim.x + threadIdx.x;
-  if (p >= n) return;
-  X[p] = X[p] + ((double)U[p] * dt);
-  Y[p] = Y[p] + ((double)V[p] * dt);
-  double z = Z[p] + ((double)W[p] * dt);
-  if (z < 0.) z = 0.;
-  else if (z > lz) z = lz;
-  Z[p] = z;
+__global__ void __launch_bounds__(256) update_pos_kernel(const CapInfo* __restrict__ caps, double dt, double lx,
+                                                         double ly, double lz, double* __restrict__ X,
+                                                         double* __restrict__ Y, double* __restrict__ Z,
+                                                         const T* __restrict__ U, const T* __restrict__ V,
+                                                         const T* __restrict__ W) {
+  __shared__ double s_sum[2][8];
+  const CapInfo ci = caps[blockIdx.x];
+  const long long p0 = ci.pt_off, nl = 8LL * (ci.L + 1) * (ci.L + 1);
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  double sx = 0.0, sy = 0.0;
+  for (long long l = tid; l < nl; l += 256) {
+    const long long p = p0 + l;
+    // x + (u dt) with two roundings, as the reference's expression (no fused multiply-add)
+    const double x = __dadd_rn(X[p], __dmul_rn((double)U[p], dt));
+    const double y = __dadd_rn(Y[p], __dmul_rn((double)V[p], dt));
+    double z = __dadd_rn(Z[p], __dmul_rn((double)W[p], dt));
+    if (z < 0.) z = 0.;
+    else if (z > lz) z = lz;
+    X[p] = x;
+    Y[p] = y;
+    Z[p] = z;
+    sx += x;
+    sy += y;
+  }
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) {
+    sx += __shfl_xor_sync(0xffffffffu, sx, o);
+    sy += __shfl_xor_sync(0xffffffffu, sy, o);
+  }
+  if (lane == 0) {
+    s_sum[0][warp] = sx;
+    s_sum[1][warp] = sy;
+  }
+  __syncthreads();
+  sx = sy = 0.0;
+#pragma unroll
+  for (int q = 0; q < 8; ++q) {
+    sx += s_sum[0][q];
+    sy += s_sum[1][q];
+  }
+  const double xm = sx / (double)nl, ym = sy / (double)nl;
+  const double shx = xm > lx ? -lx : (xm < 0. ? lx : 0.);
+  const double shy = ym > ly ? -ly : (ym < 0. ? ly : 0.);
+  if (shx == 0. && shy == 0.) return;  // uniform across the block
+  for (long long l = tid; l < nl; l += 256) {
+    const long long p = p0 + l;
+    if (shx != 0.) X[p] = X[p] + shx;
+    if (shy != 0.) Y[p] = Y[p] + shy;
+  }
 }
 
 // collisions.f90:10-32: the Morse-potential force of the wall z = 0 on every
@@ -142,10 +187,10 @@ __global__ void __launch_bounds__(256) surf_vol_kernel(const CapInfo* __restrict
 }
 
 template <class T>
-cudaError_t launch_update_pos(long n, double dt, double lz, double* X, double* Y, double* Z, const T* U, const T* V,
-                              const T* W, cudaStream_t st) {
-  if (n <= 0) return cudaSuccess;
-  update_pos_kernel<T><<<(unsigned)((n + 255) / 256), 256, 0, st>>>(n, dt, lz, X, Y, Z, U, V, W);
+cudaError_t launch_update_pos(int ncap, const CapInfo* caps, double dt, double lx, double ly, double lz, double* X,
+                              double* Y, double* Z, const T* U, const T* V, const T* W, cudaStream_t st) {
+  if (ncap <= 0) return cudaSuccess;
+  update_pos_kernel<T><<<ncap, 256, 0, st>>>(caps, dt, lx, ly, lz, X, Y, Z, U, V, W);
   return cudaGetLastError();
 }
 
@@ -173,10 +218,11 @@ cudaError_t launch_surf_vol(int ncap, const CapInfo* caps, const double* X, cons
   return cudaGetLastError();
 }
 
-template cudaError_t launch_update_pos<double>(long, double, double, double*, double*, double*, const double*,
-                                               const double*, const double*, cudaStream_t);
-template cudaError_t launch_update_pos<float>(long, double, double, double*, double*, double*, const float*,
-                                              const float*, const float*, cudaStream_t);
+template cudaError_t launch_update_pos<double>(int, const CapInfo*, double, double, double, double, double*,
+                                               double*, double*, const double*, const double*, const double*,
+                                               cudaStream_t);
+template cudaError_t launch_update_pos<float>(int, const CapInfo*, double, double, double, double, double*, double*,
+                                              double*, const float*, const float*, const float*, cudaStream_t);
 template cudaError_t launch_collisions<double>(long, const WallParams&, const double*, const double*, double*, void*,
                                                 double, cudaStream_t);
 template cudaError_t launch_collisions<float>(long, const WallParams&, const double*, const float*, float*, void*,

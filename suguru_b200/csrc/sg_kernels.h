@@ -223,8 +223,8 @@ cudaError_t launch_final(const RowWork* work, int nwork, const CapInfo* caps, co
                          cudaStream_t st);
 
 template <class T>
-cudaError_t launch_update_pos(long n, double dt, double lz, double* X, double* Y, double* Z, const T* U, const T* V,
-                              const T* W, cudaStream_t st);
+cudaError_t launch_update_pos(int ncap, const CapInfo* caps, double dt, double lx, double ly, double lz, double* X,
+                              double* Y, double* Z, const T* U, const T* V, const T* W, cudaStream_t st);
 // Wall collision force of collisions.f90:10-32 (constants of param.f90:57,64)
 struct WallParams {
   double col, betacol, rad0, rep, dx, dy;

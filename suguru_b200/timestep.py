@@ -14,6 +14,8 @@ and last step and the CUDA-event time of the stepping loop; `compare` runs the
 mixed and the FP64 paths from the same start and reports the drift of each
 and their difference.
 """
+import os
+
 import numpy as np
 
 from . import workloads as W
@@ -67,7 +69,7 @@ class PrescribedFlow:
 
 
 def run(wl, steps, precision="mixed", dt=None, surrogate_params=None, trust=None, omega=None, stream=None,
-        graph=True, tune=True):
+        graph=True, tune=True, output_dir=None, output_every=100, restart_every=None):
     """Advect the capsules of `wl` for `steps` steps; returns diagnostics and timing.
 
     graph: capture one step (flow evaluation, coupling step, Update_Pos and
@@ -75,8 +77,15 @@ def run(wl, steps, precision="mixed", dt=None, surrogate_params=None, trust=None
     it `steps` times, so that no host work is left between the steps.
     tune: let the library's autotuner pick the spreading tile and the capsule
     split first (untimed; the points do not move).
+    output_dir: every `output_every` steps write the reference's outputs there
+    (Capsule###step#######.txt, center_velocity.txt, epsilonxy.txt; main.f90:
+    455-476), and every `restart_every` steps its restart file
+    allpartdata####### (loadd.f90:147-670; capsules of one degree only).  The
+    host writes between the replays, so a run with outputs times them too.
     """
     import torch
+    if restart_every and len(set(int(L) for L in wl.degree)) > 1:
+        raise ValueError("allpartdata holds capsules of one point count; this batch has several degrees")
     dx = wl.grid[3]
     dt = 0.01 * dx if dt is None else dt
     omega = frequencies(len(wl.modes["phase"])) if omega is None else omega
@@ -101,6 +110,24 @@ def run(wl, steps, precision="mixed", dt=None, surrogate_params=None, trust=None
             return out.cpu().numpy()
 
         d0 = diag()
+        start = [x.cpu().numpy() for x in X]
+
+        def outputs(done):  # the state after `done` steps
+            from . import particle_io as PIO
+            cs.synchronize()
+            pos = [x.cpu().numpy() for x in X]
+            vel = [lag[q].double().cpu().numpy() for q in range(3)]
+            sv = cs.surf_vol(*X, lag[6], lag[7], lag[8], lag[9]).cpu().numpy()
+            PIO.write_step_outputs(output_dir, done, done * dt, wl.offsets, pos, vel, sv[-1, 2], sv[-1, 3])
+            if restart_every and done % restart_every == 0:
+                frc = [lag[q].double().cpu().numpy() for q in range(3, 6)]
+                scal, arr = PIO.particle_state(wl.offsets, pos, velocity=vel, force=frc,
+                                               area=lag[9].double().cpu().numpy(), volume=sv[:, 0],
+                                               volume0=d0[:, 0], initial=start)
+                PIO.write_allpartdata(os.path.join(output_dir, PIO.allpartdata_name(done)), scal, arr)
+
+        def due(done):
+            return output_dir is not None and done % output_every == 0
         on_sur = fb = 0
         e0 = torch.cuda.Event(enable_timing=True)
         e1 = torch.cuda.Event(enable_timing=True)
@@ -118,8 +145,10 @@ def run(wl, steps, precision="mixed", dt=None, surrogate_params=None, trust=None
                 cs.update_pos(dt, *X, lag[0], lag[1], lag[2])
                 t_dev.add_(dt)
             e0.record(st)
-            for _ in range(steps):
+            for s in range(steps):
                 g.replay()
+                if due(s + 1):
+                    outputs(s + 1)
             e1.record(st)
         else:
             e0.record(st)
@@ -127,6 +156,8 @@ def run(wl, steps, precision="mixed", dt=None, surrogate_params=None, trust=None
                 u, v, w = flow(s * dt)
                 cs.step(u, v, w, *X, lag_out=lag, eul_out=eul)
                 cs.update_pos(dt, *X, lag[0], lag[1], lag[2])
+                if due(s + 1):
+                    outputs(s + 1)
             e1.record(st)
         torch.cuda.synchronize()
         ms = e0.elapsed_time(e1)

@@ -7,6 +7,12 @@
 3. Twenty steps, mixed vs FP64 from the same start: positions agree to 1e-6
    of the capsule radius, and the per-capsule volume and area (surf_vol from
    each path's own normals and areas) within the mixed tolerance 1e-4.
+4. A capsule whose centroid has left the periodic box is shifted back by one
+   period in x or y (Update_Pos.f90:131-180), bit for bit as the oracle does;
+   the others are only advected.
+5. A run that writes the reference's output and restart files every few
+   steps follows the same trajectory bit for bit, and the files hold its
+   positions (7 digits in the text files, exact in allpartdata).
 """
 import numpy as np
 import pytest
@@ -39,11 +45,11 @@ def test_fp64_trajectory_matches_oracle(cuda):
     steps, dt = 3, 0.01 * wl.grid[3]
     got = TS.run(wl, steps, precision="fp64", omega=om)
     x, y, z = wl.x.copy(), wl.y.copy(), wl.z.copy()
-    lz = wl.grid[2] * wl.grid[5]
+    lx, ly, lz = (wl.grid[q] * wl.grid[q + 3] for q in range(3))
     for s in range(steps):
         u, v, w = wl.velocity(t=s * dt, omega=om)
         ul, vl, wlv = O.interp(wl.grid, u, v, w, x, y, z)
-        x, y, z = O.update_pos(dt, lz, x, y, z, ul, vl, wlv)
+        x, y, z = O.update_pos_capsules(wl.offsets, dt, lx, ly, lz, x, y, z, ul, vl, wlv)
     for g, r in zip(got["positions"], (x, y, z)):
         assert np.abs(g - r).max() <= 1e-12 * np.abs(r).max()
 
@@ -56,3 +62,56 @@ def test_mixed_vs_fp64_drift(cuda):
     assert r["volume_mixed_vs_fp64"] <= 1e-4
     assert r["area_mixed_vs_fp64"] <= 1e-4
     assert r["mixed_steps_per_s"] > 0 and r["fp64_steps_per_s"] > 0
+
+
+@pytest.mark.parametrize("precision", ["fp64", "mixed"])
+def test_update_pos_shifts_capsules_back_into_the_box(cuda, precision):
+    from suguru_b200.coupling import CouplingStep
+    wl = W.small_config(ncap=4, seed=11)
+    lx, ly, lz = (wl.grid[q] * wl.grid[q + 3] for q in range(3))
+    off = wl.offsets
+    x, y, z = wl.x.copy(), wl.y.copy(), wl.z.copy()
+    # capsule 0 past x = lx, capsule 1 below y = 0, capsule 2 past both, capsule 3 inside
+    for k, (dx_, dy_) in enumerate([(lx, 0.0), (0.0, -ly), (lx, ly), (0.0, 0.0)]):
+        s = slice(off[k], off[k + 1])
+        x[s] += dx_
+        y[s] += dy_
+    rng = np.random.default_rng(5)
+    dt = 0.01 * wl.grid[3]
+    dtype = np.float64 if precision == "fp64" else np.float32
+    U = [rng.normal(size=wl.npts).astype(dtype) for _ in range(3)]
+    rx, ry, rz = O.update_pos_capsules(off, dt, lx, ly, lz, x, y, z, *(u.astype(np.float64) for u in U))
+    cs = CouplingStep(wl.grid, wl.degree, wl.radius, precision=precision)
+    gx, gy, gz = x.copy(), y.copy(), z.copy()
+    cs.update_pos(dt, gx, gy, gz, *U)
+    for g, r in zip((gx, gy, gz), (rx, ry, rz)):
+        assert np.array_equal(g, r)
+    for k in range(wl.ncap):
+        s = slice(off[k], off[k + 1])
+        assert 0.0 <= rx[s].mean() <= lx and 0.0 <= ry[s].mean() <= ly
+
+
+def test_reference_outputs_of_a_run(cuda, tmp_path):
+    from suguru_b200 import particle_io as PIO
+    wl = W.small_config(ncap=2, degrees=(7,))
+    om = TS.frequencies(len(wl.modes["phase"]))
+    plain = TS.run(wl, 4, precision="fp64", omega=om, tune=False)
+    out = TS.run(wl, 4, precision="fp64", omega=om, tune=False, output_dir=str(tmp_path), output_every=2,
+                 restart_every=4)
+    for a, b in zip(out["positions"], plain["positions"]):
+        assert np.array_equal(a, b)  # writing the files does not change the trajectory
+    off = wl.offsets
+    for k in range(wl.ncap):
+        x, y, z = PIO.read_capsule_txt(tmp_path / PIO.capsule_txt_name(k + 1, 4))
+        for g, r in zip((x, y, z), out["positions"]):
+            assert np.all(np.abs(g - r[off[k]:off[k + 1]]) <= 5e-7 * np.abs(r[off[k]:off[k + 1]]))
+        assert (tmp_path / PIO.capsule_txt_name(k + 1, 2)).exists()
+    assert len((tmp_path / "center_velocity.txt").read_text().splitlines()) == 2 * wl.ncap
+    assert len((tmp_path / "epsilonxy.txt").read_text().splitlines()) == 2 * wl.ncap
+    nl = int(off[1] - off[0])
+    scal, arr = PIO.read_allpartdata(tmp_path / PIO.allpartdata_name(4), wl.ncap, nl)
+    assert np.array_equal(arr[1, PIO.PARTICLE_ARRAYS.index("zfp")], out["positions"][2][off[1]:off[2]])
+    assert np.array_equal(arr[0, PIO.PARTICLE_ARRAYS.index("xfp0")], wl.x[off[0]:off[1]])
+    # the file's volumes come from the last step's normals and areas (surf_vol after Update_Pos,
+    # as the reference orders them); run() recomputes both at the final shape
+    assert np.allclose(scal[:, 4], out["vol"], rtol=1e-2)
