@@ -133,6 +133,28 @@ int sg_surf_vol(sg_ctx* ctx, const double* X, const double* Y, const double* Z,
 int sg_set_wall_collisions(sg_ctx* ctx, int in_step, double col, double betacol, double rad0, double rep);
 int sg_collisions(sg_ctx* ctx, const double* Z, const void* AREA, void* FZ);
 
+/* indicator (indicator.f90:19-182) on the main mesh (the overlap mesh,
+ * ifoverlap = 1, is off by default): the capsules raised by ktot/4 dz,
+ * G = normals * area spread with cell-centre weights (lagr2eulrind,
+ * interp_spread.f90:978-1387), its central-difference divergence, the
+ * Poisson solve of solver1d after initsolver(0) (periodic x, y by FFT,
+ * Neumann z by the reference's elimination), the shift back, boundind, the
+ * 0.01 / 0.9 thresholds on the interior; visc = visc0 (1 + (lambda - 1) I)
+ * with boundp; and, when fy / fz are not NULL, forcey += .5 (I_j + I_j+1)
+ * sin(thetainc) (ta/rep^2)^(1/4), forcez += .5 (I_k + I_k+1) (-cos(thetainc))
+ * (ta/rep^2)^(1/4) on the interior.  indic, visc, fy, fz are fields in the
+ * Eulerian layout above (visc, fy, fz may be NULL); NX.. AREA are the
+ * normals and areas of sg_membrane_force.  The constants are those of
+ * param.f90:52,57 (visc0 = 1/Rep, lambda, thetainc in radians, ta, Rep).
+ * sg_set_indicator_params allocates the indicator's workspace and FFT plans
+ * (itot even, ktot >= 4); sg_indicator allocates nothing and returns
+ * SG_ERR_STATE before the parameters are set.  Computed in FP64 in both
+ * precisions (the mixed path rounds its FP32 outputs once). */
+int sg_set_indicator_params(sg_ctx* ctx, double visc0, double lambda, double thetainc, double ta, double rep);
+int sg_indicator(sg_ctx* ctx, const double* X, const double* Y, const double* Z,
+                 const void* NX, const void* NY, const void* NZ, const void* AREA,
+                 void* indic, void* visc, void* fy, void* fz);
+
 /* Spreading for callers that cannot allocate device memory.  It has no
  * counterpart in the reference; it is sg_spread (lagr2eulr) without a
  * context.  It is for host codes whose device memory is all owned by their

@@ -45,6 +45,7 @@ def lib():
         L.or_capsule_spectra.argtypes = [i, d, d, d] + [_dp] * 7
         L.or_interp.argtypes = [i, i, i, d, d, d, i, _dp, _dp, _dp, l, _dp, _dp, _dp, _dp, _dp, _dp]
         L.or_spread.argtypes = [i, i, i, d, d, d, i, l] + [_dp] * 10
+        L.or_spread_ind.argtypes = [i, i, i, d, d, d, i, l] + [_dp] * 10
         L.or_update_pos.argtypes = [l, d, d] + [_dp] * 6
         L.or_update_pos.restype = None
         L.or_update_pos_capsules.argtypes = [ctypes.c_int, ctypes.POINTER(ctypes.c_long), d, d, d, d] + [_dp] * 6
@@ -173,6 +174,99 @@ def spread(grid, x, y, z, fx, fy, fz, area, faithful=False):
     lib().or_spread(itot, jtot, ktot, dx, dy, dz, int(faithful), x.size, _p(_f64(x)), _p(_f64(y)), _p(_f64(z)),
                     _p(_f64(fx)), _p(_f64(fy)), _p(_f64(fz)), _p(_f64(area)), _p(gx), _p(gy), _p(gz))
     return gx, gy, gz
+
+
+def spread_ind(grid, x, y, z, nx, ny, nz, area, faithful=False):
+    """lagr2eulrind (interp_spread.f90:978-1387): gx, gy, gz on (0:i1,0:j1,0:k1)."""
+    itot, jtot, ktot, dx, dy, dz = grid
+    shape = (ktot + 2, jtot + 2, itot + 2)
+    gx, gy, gz = np.zeros(shape), np.zeros(shape), np.zeros(shape)
+    lib().or_spread_ind(itot, jtot, ktot, dx, dy, dz, int(faithful), x.size, _p(_f64(x)), _p(_f64(y)), _p(_f64(z)),
+                        _p(_f64(nx)), _p(_f64(ny)), _p(_f64(nz)), _p(_f64(area)), _p(gx), _p(gy), _p(gz))
+    return gx, gy, gz
+
+
+def boundp(f):
+    """boundp / boundind (bound.f90:88-139): Neumann z halos, then periodic x, y halo copies."""
+    f[0] = f[1]
+    f[-1] = f[-2]
+    f[:, :, -1] = f[:, :, 1]
+    f[:, :, 0] = f[:, :, -2]
+    f[:, -1, :] = f[:, 1, :]
+    f[:, 0, :] = f[:, -2, :]
+    return f
+
+
+def poisson_solver1d(rhs, dx, dy, dz):
+    """solver1d with initsolver(0) (solver.f90:43-157, initsolver.f90:11-100): the second-order
+    Laplacian, periodic in x and y (real FFTs; eigenvalues -4/dx^2 sin^2(pi m / itot) and the
+    same in y, initsolver.f90:111-130) and Neumann in z (b(1) += a(1), b(kmax) += c(kmax)),
+    solved per mode by the reference's tridiagonal elimination, whose last pivot is exactly zero
+    for the mean mode, which is then set to zero.  rhs: [kmax, jtot, itot] interior values."""
+    kmax, jtot, itot = rhs.shape
+    dzi = 1.0 / dz
+    a = np.full(kmax, dzi * dzi)
+    c = np.full(kmax, dzi * dzi)
+    b = -(a + c)
+    b[0] += a[0]
+    b[-1] += c[-1]
+    a[0] = 0.0
+    c[-1] = 0.0
+    # xrt(2m) = -4 dxi^2 sin(2m pi / (2 itot))^2 (initsolver.f90:111-116), likewise yrt
+    dxi, dyi = 1.0 / dx, 1.0 / dy
+    lx = -4.0 * dxi * dxi * np.sin((2 * np.arange(itot // 2 + 1)) * np.pi / (2.0 * itot)) ** 2
+    jm = np.minimum(np.arange(jtot), jtot - np.arange(jtot))  # complex y modes j and jtot - j share yrt
+    ly = -4.0 * dyi * dyi * np.sin((2 * jm) * np.pi / (2.0 * jtot)) ** 2
+    lam = ly[:, None] + lx[None, :]
+    p = np.fft.rfft2(rhs, axes=(1, 2))
+    d = np.zeros(p.shape)
+    z = 1.0 / (b[0] + lam)
+    d[0] = c[0] * z
+    p[0] = p[0] * z
+    for k in range(1, kmax - 1):
+        z = 1.0 / ((b[k] + lam) - a[k] * d[k - 1])
+        d[k] = c[k] * z
+        p[k] = (p[k] - a[k] * p[k - 1]) * z
+    z = (b[-1] + lam) - a[-1] * d[-2]
+    nz = z != 0.0
+    p[-1] = np.where(nz, (p[-1] - a[-1] * p[-2]) / np.where(nz, z, 1.0), 0.0)
+    for k in range(kmax - 2, -1, -1):
+        p[k] = p[k] - d[k] * p[k + 1]
+    return np.fft.irfft2(p, s=(jtot, itot), axes=(1, 2))
+
+
+def indicator(grid, x, y, z, nx, ny, nz, area, visc0=1.0 / 0.0016, lam=1.0, thetainc=70.0 * np.pi / 180.0,
+              ta=1160000.0, rep=0.0016, fy=None, fz=None):
+    """indicator.f90:19-182 without the overlap mesh: the capsules raised by ktot/4 dz, G by
+    lagr2eulrind, its central-difference divergence, the Poisson solve, boundind, the shift
+    back, the 0.01 / 0.9 thresholds on the interior, the viscosity visc0 (1 + (lambda - 1) I)
+    with boundp, and the centrifugal terms added to fy, fz (interior cells).
+    Returns dict(g=(gx, gy, gz), indi=..., indic=..., visc=..., fy=..., fz=...)."""
+    itot, jtot, ktot, dx, dy, dz = grid
+    q = ktot // 4
+    gx, gy, gz = spread_ind(grid, x, y, _f64(z) + q * dz, nx, ny, nz, area)
+    shape = gx.shape
+    dg = ((gx[1:-1, 1:-1, 2:] - gx[1:-1, 1:-1, :-2]) * 0.5 * (1.0 / dx)
+          + (gy[1:-1, 2:, 1:-1] - gy[1:-1, :-2, 1:-1]) * 0.5 * (1.0 / dy)
+          + (gz[2:, 1:-1, 1:-1] - gz[:-2, 1:-1, 1:-1]) * 0.5 * (1.0 / dz))
+    indi = np.zeros(shape)
+    indi[1:-1, 1:-1, 1:-1] = poisson_solver1d(dg, dx, dy, dz)
+    boundp(indi)
+    indic = np.zeros(shape)
+    indic[1:ktot - q + 1, 1:-1, 1:-1] = indi[1 + q:ktot + 1, 1:-1, 1:-1]
+    boundp(indic)
+    inner = indic[1:-1, 1:-1, 1:-1]
+    inner[inner < 0.01] = 0.0
+    inner[inner >= 0.9] = 1.0
+    visc = np.zeros(shape)
+    visc[1:-1, 1:-1, 1:-1] = visc0 * (1.0 + (lam - 1.0) * indic[1:-1, 1:-1, 1:-1])
+    boundp(visc)
+    fy = np.zeros(shape) if fy is None else _f64(fy).copy()
+    fz = np.zeros(shape) if fz is None else _f64(fz).copy()
+    amp = (ta / rep ** 2) ** 0.25
+    fy[1:-1, 1:-1, 1:-1] += 0.5 * (indic[1:-1, 1:-1, 1:-1] + indic[1:-1, 2:, 1:-1]) * np.sin(thetainc) * amp
+    fz[1:-1, 1:-1, 1:-1] += 0.5 * (indic[1:-1, 1:-1, 1:-1] + indic[2:, 1:-1, 1:-1]) * (-np.cos(thetainc)) * amp
+    return dict(g=(gx, gy, gz), dg=dg, indi=indi, indic=indic, visc=visc, fy=fy, fz=fz)
 
 
 def update_pos(dt, lz, x, y, z, u, v, w):

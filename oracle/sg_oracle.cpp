@@ -763,9 +763,11 @@ struct Grid {
 // Cells touched by one point, per image, in the reference's clipped window.
 // Calls fn(i,j,k, kxs,kx, kys,ky, kzs,kz) for every window cell.
 template <class F>
-void window_faithful(const Grid& g, double xc, double yc, double zc, F&& fn) {
+void window_faithful(const Grid& g, double xc, double yc, double zc, F&& fn, int kc0 = 1, int kc1 = -1) {
   // interp_spread.f90:340-378: window nint(c-2)..nint(c+2), clipped to
   // [1,imax]x[1,jmax]x[1,kmax]; periodic x,y via image copies (:72-145).
+  // lagr2eulrind (:1311-1316) clips z to [0,kmax+1] instead: kc0, kc1.
+  if (kc1 < 0) kc1 = g.ktot;
   double cz = zc;
   for (int sx = -1; sx <= 1; ++sx)
     for (int sy = -1; sy <= 1; ++sy) {
@@ -774,10 +776,10 @@ void window_faithful(const Grid& g, double xc, double yc, double zc, F&& fn) {
       long kl = nint_(cz - 2.), kh = nint_(cz + 2.);
       if (il < 1) il = 1;
       if (jl < 1) jl = 1;
-      if (kl < 1) kl = 1;
+      if (kl < kc0) kl = kc0;
       if (ih > g.itot) ih = g.itot;
       if (jh > g.jtot) jh = g.jtot;
-      if (kh > g.ktot) kh = g.ktot;
+      if (kh > kc1) kh = kc1;
       if (il > ih || jl > jh) continue;
       for (long k = kl; k <= kh; ++k) {
         double czs = (1. * k) - cz, czz = czs - 0.5;
@@ -798,7 +800,8 @@ void window_faithful(const Grid& g, double xc, double yc, double zc, F&& fn) {
 // Same cells via modular wrap over the 4-wide candidate window (exact
 // equivalent: the 5-wide window covers the kernel support |r|<1.5).
 template <class F>
-void window_fast(const Grid& g, double xc, double yc, double zc, F&& fn) {
+void window_fast(const Grid& g, double xc, double yc, double zc, F&& fn, int kc0 = 1, int kc1 = -1) {
+  if (kc1 < 0) kc1 = g.ktot;
   long fx = (long)std::floor(xc), fy = (long)std::floor(yc), fz = (long)std::floor(zc);
   double kxs[4], kx[4], kys[4], ky[4], kzs[4], kz[4];
   for (int t = 0; t < 4; ++t) {
@@ -809,7 +812,7 @@ void window_fast(const Grid& g, double xc, double yc, double zc, F&& fn) {
   }
   for (int tk = 0; tk < 4; ++tk) {
     long k = fz - 1 + tk;
-    if (k < 1 || k > g.ktot) continue;
+    if (k < kc0 || k > kc1) continue;
     for (int tj = 0; tj < 4; ++tj) {
       long j = fy - 1 + tj;
       long jw = ((j - 1) % g.jtot + g.jtot) % g.jtot + 1;
@@ -880,6 +883,35 @@ void halo_copy(const Grid& g, double* f) {
       f[fidx(i, g.jtot + 1, k, ldi, ldj)] = f[fidx(i, 1, k, ldi, ldj)];
       f[fidx(i, 0, k, ldi, ldj)] = f[fidx(i, g.jtot, k, ldi, ldj)];
     }
+}
+
+// lagr2eulrind (interp_spread.f90:978-1387): g = sum_l n_l phi(x) phi(y)
+// phi(z) area_l / dV with cell-centre weights in all three directions for
+// all three components (:1319-1343), z window clipped to [0, kmax+1] (the
+// wall halo planes keep their contributions), then the periodic x and y halo
+// copies (:1371-1382).
+void spread_ind_all(const Grid& g, bool faithful, long npts, const double* xp, const double* yp, const double* zp,
+                    const double* nxl, const double* nyl, const double* nzl, const double* area, double dVi,
+                    double* gx, double* gy, double* gz) {
+  const int ldi = g.itot + 2, ldj = g.jtot + 2;
+  const long ntot = (long)ldi * ldj * (g.ktot + 2);
+  std::memset(gx, 0, sizeof(double) * ntot);
+  std::memset(gy, 0, sizeof(double) * ntot);
+  std::memset(gz, 0, sizeof(double) * ntot);
+  for (long p = 0; p < npts; ++p) {
+    double cx = xp[p] * g.dxi, cy = yp[p] * g.dyi, cz = zp[p] * g.dzi;
+    auto acc = [&](int i, int j, int k, double, double kx, double, double ky, double, double kz) {
+      long o = fidx(i, j, k, ldi, ldj);
+      gx[o] += nxl[p] * kx * ky * kz * (area[p] * dVi);
+      gy[o] += nyl[p] * kx * ky * kz * (area[p] * dVi);
+      gz[o] += nzl[p] * kx * ky * kz * (area[p] * dVi);
+    };
+    if (faithful) window_faithful(g, cx, cy, cz, acc, 0, g.ktot + 1);
+    else window_fast(g, cx, cy, cz, acc, 0, g.ktot + 1);
+  }
+  halo_copy(g, gx);
+  halo_copy(g, gy);
+  halo_copy(g, gz);
 }
 
 int nthreads_of(int req) {
@@ -1019,6 +1051,14 @@ int or_interp(int itot, int jtot, int ktot, double dx, double dy, double dz, int
               double* ul, double* vl, double* wl) {
   Grid g{itot, jtot, ktot, 1.0 / dx, 1.0 / dy, 1.0 / dz};
   interp_points(g, faithful != 0, u, v, w, 0, npts, xp, yp, zp, ul, vl, wl);
+  return 0;
+}
+
+int or_spread_ind(int itot, int jtot, int ktot, double dx, double dy, double dz, int faithful, long npts,
+                  const double* xp, const double* yp, const double* zp, const double* nxl, const double* nyl,
+                  const double* nzl, const double* area, double* gx, double* gy, double* gz) {
+  Grid g{itot, jtot, ktot, 1.0 / dx, 1.0 / dy, 1.0 / dz};
+  spread_ind_all(g, faithful != 0, npts, xp, yp, zp, nxl, nyl, nzl, area, 1.0 / (dx * dy * dz), gx, gy, gz);
   return 0;
 }
 

@@ -79,6 +79,13 @@ int or_spread(int itot, int jtot, int ktot, double dx, double dy, double dz, int
               const double* fxl, const double* fyl, const double* fzl, const double* area,
               double* fx, double* fy, double* fz);
 
+/* lagr2eulrind (interp_spread.f90:978-1387): normals * area spread with
+ * cell-centre weights in every direction, z window [0, kmax+1], periodic
+ * x, y halo copies.  Fields (0:i1,0:j1,0:k1), x fastest. */
+int or_spread_ind(int itot, int jtot, int ktot, double dx, double dy, double dz, int faithful, long npts,
+                  const double* xp, const double* yp, const double* zp, const double* nxl, const double* nyl,
+                  const double* nzl, const double* area, double* gx, double* gy, double* gz);
+
 /* Update_Pos.f90:95-126: forward Euler + wall clamp to [0,lz]. */
 void or_update_pos(long npts, double dt, double lz, double* xp, double* yp, double* zp,
                    const double* ul, const double* vl, const double* wl);

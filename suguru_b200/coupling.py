@@ -38,7 +38,8 @@ EXPORTS = ["sg_create", "sg_destroy", "sg_last_error", "sg_synchronize", "sg_int
            "sg_surrogate_params", "sg_surrogate_set_linear", "sg_surrogate_train", "sg_surrogate_predict",
            "sg_surrogate_set_trust", "sg_surrogate_last_counts", "sg_set_point_split", "sg_get_point_split",
            "sg_set_tensor_cores", "sg_set_legendre_terms", "sg_get_legendre_terms", "sg_set_capsule_law",
-           "sg_set_legendre_tile_rows", "sg_get_legendre_tile_rows", "sg_set_wall_collisions", "sg_collisions"]
+           "sg_set_legendre_tile_rows", "sg_get_legendre_tile_rows", "sg_set_wall_collisions", "sg_collisions",
+           "sg_set_indicator_params", "sg_indicator"]
 # test hooks declared in include/sg_testing.h
 TEST_EXPORTS = ["sg_test_legendre", "sg_test_gemm", "sg_test_mlp_grad"]
 WORKLOAD_EXPORTS = ["sg_prescribed_flow"]  # include/sg_workload.h
@@ -88,6 +89,8 @@ def lib():
     L.sg_surf_vol.argtypes = [vp] * 10
     L.sg_set_wall_collisions.argtypes = [vp, ctypes.c_int] + [ctypes.c_double] * 4
     L.sg_collisions.argtypes = [vp] * 4
+    L.sg_set_indicator_params.argtypes = [vp] + [ctypes.c_double] * 5
+    L.sg_indicator.argtypes = [vp] * 12
     L.sg_gauss.argtypes = [ctypes.c_int, dp, dp]
     L.sg_legendre.argtypes = [ctypes.c_double, ctypes.c_int, ctypes.c_int, dp, dp, dp]
     L.sg_last_launch_count.argtypes = [vp]
@@ -463,6 +466,19 @@ class CouplingStep:
         """collisions.f90:10-32 -- FZ += wall force, in place."""
         self._check(lib().sg_collisions(self._h, *map(_ptr, (Z, AREA, FZ))), "sg_collisions")
         return FZ
+
+    def set_indicator_params(self, visc0=1.0 / 0.0016, lam=1.0, thetainc=70.0 * np.pi / 180.0, ta=1160000.0,
+                             rep=0.0016):
+        """Constants of indicator.f90 (param.f90:52,57); allocates the indicator's workspace."""
+        self._check(lib().sg_set_indicator_params(self._h, float(visc0), float(lam), float(thetainc), float(ta),
+                                                  float(rep)), "sg_set_indicator_params")
+
+    def indicator(self, X, Y, Z, NX, NY, NZ, AREA, fy=None, fz=None, out=None):
+        """indicator.f90:19-182 -- (indic, visc); fy, fz (optional) get the centrifugal terms in place."""
+        indic, visc = out if out is not None else self._eul(2)
+        self._check(lib().sg_indicator(self._h, *map(_ptr, (X, Y, Z, NX, NY, NZ, AREA, indic, visc, fy, fz))),
+                    "sg_indicator")
+        return indic, visc
 
     def surf_vol(self, X, Y, Z, NX, NY, NZ, AREA, exy1_prev=None):
         """surf_vol.f90:12 -- [ncap, 7]: volume, area, exy1, exy2, centroid."""

@@ -721,6 +721,7 @@ void sg_destroy(sg_ctx* c) {
   if (c->st) cudaStreamSynchronize(c->st);
   if (c->graph_exec) cudaGraphExecDestroy(c->graph_exec);
   if (c->graph) cudaGraphDestroy(c->graph);
+  indicator_free(c);
   for (void* p : c->allocs) cudaFree(p);
   for (int k = 0; k <= SG_NSTAGE; ++k)
     if (c->ev[k]) cudaEventDestroy(c->ev[k]);
@@ -849,6 +850,58 @@ int sg_collisions(sg_ctx* c, const double* Z, const void* AREA, void* FZ) {
                                                        c->grid.dvi, c->st);
   if (e != cudaSuccess) return cuda_fail(c, e, "collisions");
   if (host) SG_RET(d2h(c, FZ, dF, lb));
+  return finish(c);
+}
+
+int sg_set_indicator_params(sg_ctx* c, double visc0, double lambda, double thetainc, double ta, double rep) {
+  if (!c) return SG_ERR_ARG;
+  if (c->graph) return fail(c, SG_ERR_STATE, "release the captured graph first");
+  SG_RET(indicator_setup(c, visc0, lambda, thetainc, ta, rep));
+  SG_TRY(cudaDeviceSynchronize(), "indicator setup");
+  return SG_OK;
+}
+
+int sg_indicator(sg_ctx* c, const double* X, const double* Y, const double* Z, const void* NX, const void* NY,
+                 const void* NZ, const void* AREA, void* indic, void* visc, void* fy, void* fz) {
+  if (!c) return SG_ERR_ARG;
+  if (!c->ind.ready) return fail(c, SG_ERR_STATE, "indicator parameters not set (sg_set_indicator_params)");
+  if (!indic) return fail(c, SG_ERR_ARG, "null indicator field");
+  SG_RET(check_ptrs(c, {X, Y, Z, NX, NY, NZ, AREA}));
+  const bool host = c->cfg.mem == SG_MEM_HOST;
+  const size_t pb = sizeof(double) * c->npts, lb = c->esz * c->npts, fb = c->esz * c->nfield;
+  const double *dX = X, *dY = Y, *dZ = Z;
+  const void *dN[3] = {NX, NY, NZ}, *dA = AREA;
+  void *dI = indic, *dV = visc, *dFy = fy, *dFz = fz;
+  if (host) {
+    SG_RET(h2d(c, c->s_X, X, pb));
+    SG_RET(h2d(c, c->s_Y, Y, pb));
+    SG_RET(h2d(c, c->s_Z, Z, pb));
+    for (int q = 0; q < 3; ++q) {
+      SG_RET(h2d(c, c->s_lag[6 + q], dN[q], lb));
+      dN[q] = c->s_lag[6 + q];
+    }
+    SG_RET(h2d(c, c->s_lag[9], AREA, lb));
+    dX = c->s_X; dY = c->s_Y; dZ = c->s_Z; dA = c->s_lag[9];
+    dI = c->s_f[0];
+    dV = visc ? c->s_f[1] : nullptr;
+    if (fy) SG_RET(h2d(c, c->s_u, fy, fb));
+    if (fz) SG_RET(h2d(c, c->s_v, fz, fb));
+    dFy = fy ? c->s_u : nullptr;
+    dFz = fz ? c->s_v : nullptr;
+  }
+  c->launches = 0;
+  if (c->mixed)
+    SG_RET(indicator_run<float>(c, dX, dY, dZ, (const float*)dN[0], (const float*)dN[1], (const float*)dN[2],
+                                (const float*)dA, (float*)dI, (float*)dV, (float*)dFy, (float*)dFz));
+  else
+    SG_RET(indicator_run<double>(c, dX, dY, dZ, (const double*)dN[0], (const double*)dN[1], (const double*)dN[2],
+                                 (const double*)dA, (double*)dI, (double*)dV, (double*)dFy, (double*)dFz));
+  if (host) {
+    SG_RET(d2h(c, indic, dI, fb));
+    if (visc) SG_RET(d2h(c, visc, dV, fb));
+    if (fy) SG_RET(d2h(c, fy, dFy, fb));
+    if (fz) SG_RET(d2h(c, fz, dFz, fb));
+  }
   return finish(c);
 }
 

@@ -121,6 +121,20 @@ struct sg_ctx {
   float sur_trust[5] = {0.f, 0.f, 0.f, 0.f, 0.f};  // amp_max, ratio_max, c_min, c_max, enabled
   // Lagrangian scratch for sg_capsule_spectra in device mode (allocated on first use)
   void* spec_scratch[7] = {};
+  // indicator function (sg_indicator.cu), set up by sg_set_indicator_params
+  struct IndState {
+    bool ready = false, have_plans = false;
+    double visc0 = 0, lambda = 1, sin_t = 0, mcos_t = 0, amp = 0;
+    sg::IBGrid grid{};       // ktot + 2 planes: interior k = 0 .. kmax + 1 of the real grid
+    sg::IBWork w{};          // FP64 records of the normals
+    double* zr = nullptr;    // raised z of the points
+    double* g = nullptr;     // gx, gy, gz on the taller grid
+    double* r = nullptr;     // real FFT input / output [ktot][jtot][itot]
+    void* c = nullptr;       // modes [ktot][jtot][itot/2 + 1] (double2)
+    double* d = nullptr;     // elimination multipliers [ktot][modes]
+    double* tab = nullptr;   // a, b, c rows [3][ktot], xrt [itot/2 + 1], yrt [jtot]
+    int plan_f = 0, plan_b = 0;  // cufftHandle
+  } ind;
 };
 
 namespace sg {
@@ -155,6 +169,13 @@ int sur_step_post(sg_ctx* c);  // after Legendre stage 2
 const int* sur_flags(sg_ctx* c);
 // force pipeline only, outputs into device arrays lag[0..6] (sg_context.cu)
 int run_forces_only(sg_ctx* c, const double* X, const double* Y, const double* Z, void* const* lag);
+
+// indicator function (sg_indicator.cu)
+int indicator_setup(sg_ctx* c, double visc0, double lambda, double thetainc, double ta, double rep);
+void indicator_free(sg_ctx* c);
+template <class T>
+int indicator_run(sg_ctx* c, const double* X, const double* Y, const double* Z, const T* NX, const T* NY, const T* NZ,
+                  const T* A, T* indic, T* visc, T* fy, T* fz);
 
 template <class P>
 cudaError_t dalloc(sg_ctx* c, P*& p, size_t bytes) {

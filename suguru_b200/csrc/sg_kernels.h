@@ -54,6 +54,10 @@ cudaError_t launch_pack_forces(const IBGrid& g, long n, const T* FX, const T* FY
 // Spreads the force records of w.frc (points binned in w).
 template <class T>
 cudaError_t launch_spread(const IBGrid& g, const IBWork& w, T* ox, T* oy, T* oz, cudaStream_t st);
+// The same with cell-centre weights in every direction for every component
+// (lagr2eulrind); FP64 only, tile shapes 0 and 3.
+template <class T>
+cudaError_t launch_spread_centred(const IBGrid& g, const IBWork& w, T* ox, T* oy, T* oz, cudaStream_t st);
 
 // ------------------------------------------------------------ host tables --
 // Gauss-Legendre colatitudes north->south and weights (gaqd.f:45 semantics).

@@ -121,7 +121,10 @@ __global__ void pack_forces_kernel(long n, double dvi, const T* __restrict__ FX,
   frc[p] = r;
 }
 
-template <class T, int TX, int TY, int TZ>
+// CTR: cell-centre weights in every direction for every component (the
+// indicator's lagr2eulrind, interp_spread.f90:1319-1343) instead of the
+// staggered ones.
+template <class T, int TX, int TY, int TZ, bool CTR>
 __global__ void __launch_bounds__(256, sizeof(T) == 4 ? 4 : 2) spread_kernel(IBGrid g, const int* __restrict__ entries,
                                                      const int* __restrict__ starts,
                                                      const PosRec<T>* __restrict__ pos,
@@ -303,16 +306,16 @@ __global__ void __launch_bounds__(256, sizeof(T) == 4 ? 4 : 2) spread_kernel(IBG
         for (int c = 0; c < 3; ++c) {
 #pragma unroll
           for (int iz = 0; iz < 3; ++iz) {
-            const int cz_ = (c == 2) ? lcF[2][iz] : lcC[2][iz];
-            const T wz = (c == 2) ? wF[2][iz] : wC[2][iz];
+            const int cz_ = (!CTR && c == 2) ? lcF[2][iz] : lcC[2][iz];
+            const T wz = (!CTR && c == 2) ? wF[2][iz] : wC[2][iz];
 #pragma unroll
             for (int iy = 0; iy < 3; ++iy) {
-              const int cyz = cz_ + ((c == 1) ? lcF[1][iy] : lcC[1][iy]);
-              const T pyz = cf[c] * (((c == 1) ? wF[1][iy] : wC[1][iy]) * wz);
+              const int cyz = cz_ + ((!CTR && c == 1) ? lcF[1][iy] : lcC[1][iy]);
+              const T pyz = cf[c] * (((!CTR && c == 1) ? wF[1][iy] : wC[1][iy]) * wz);
 #pragma unroll
               for (int ix = 0; ix < 3; ++ix) {
-                const int cell = cyz + ((c == 0) ? lcF[0][ix] : lcC[0][ix]);
-                const T wx = (c == 0) ? wF[0][ix] : wC[0][ix];
+                const int cell = cyz + ((!CTR && c == 0) ? lcF[0][ix] : lcC[0][ix]);
+                const T wx = (!CTR && c == 0) ? wF[0][ix] : wC[0][ix];
                 // valid cells are below NC, the negative ones wrap above it
                 const unsigned slot = min((unsigned)cell, (unsigned)trash);
                 if constexpr (F32) {
@@ -404,10 +407,10 @@ __global__ void __launch_bounds__(256, sizeof(T) == 4 ? 4 : 2) spread_kernel(IBG
   }
 }
 
-template <class T, int TX, int TY, int TZ>
+template <class T, int TX, int TY, int TZ, bool CTR = false>
 static void spread_one(const IBGrid& g, const IBWork& w, T* ox, T* oy, T* oz, cudaStream_t st) {
-  spread_kernel<T, TX, TY, TZ><<<g.ntiles, 256, 0, st>>>(g, w.entries, w.starts, (const PosRec<T>*)w.pos,
-                                                          (const ForceRec<T>*)w.frc, ox, oy, oz);
+  spread_kernel<T, TX, TY, TZ, CTR><<<g.ntiles, 256, 0, st>>>(g, w.entries, w.starts, (const PosRec<T>*)w.pos,
+                                                               (const ForceRec<T>*)w.frc, ox, oy, oz);
 }
 
 template <class T>
@@ -429,6 +432,17 @@ cudaError_t launch_spread(const IBGrid& g, const IBWork& w, T* ox, T* oy, T* oz,
     case 2:
       if constexpr (sizeof(T) == 4) { spread_one<T, 32, 8, 8>(g, w, ox, oy, oz, st); break; }
       return cudaErrorInvalidValue;
+    default: return cudaErrorInvalidValue;
+  }
+  return cudaGetLastError();
+}
+
+template <>
+cudaError_t launch_spread_centred<double>(const IBGrid& g, const IBWork& w, double* ox, double* oy, double* oz,
+                                          cudaStream_t st) {
+  switch (g.shape) {
+    case 0: spread_one<double, 32, 8, 4, true>(g, w, ox, oy, oz, st); break;
+    case 3: spread_one<double, 8, 8, 4, true>(g, w, ox, oy, oz, st); break;
     default: return cudaErrorInvalidValue;
   }
   return cudaGetLastError();
