@@ -155,6 +155,29 @@ int sg_indicator(sg_ctx* ctx, const double* X, const double* Y, const double* Z,
                  const void* NX, const void* NY, const void* NZ, const void* AREA,
                  void* indic, void* visc, void* fy, void* fz);
 
+/* One step of the reference's FFT flow solver (fsolver = 'f',
+ * main.f90:333-347), FP64 contexts only: fftuvw (fftuvw.f90:13-127: pressure
+ * gradient plus the IB force, momxp..momzp; Adams-Bashforth convection from
+ * the velocities uo (level n) and uoo (level n-1), momxad..momzad; implicit
+ * Helmholtz solves of solver1d after initsolver(3) for w and initsolver(2)
+ * for u, v), bounduvw, fillps, solver1d after initsolver(1), boundp, correc,
+ * bounduvw, p += the pressure correction and boundp.  All arrays are fields
+ * in the Eulerian layout above with their halos set as bounduvw / boundp
+ * leave them; p (the reference's pnew) is updated in place; u, v, w receive
+ * the new velocity.  fx, fy, fz are the IB force (sg_spread, plus the
+ * centrifugal terms of sg_indicator when used).  sg_set_flow_params takes
+ * Rep (param.f90:57) and the wall values of v, vb2 = v(0) + v(1) and
+ * vt2 = v(k1) + v(kmax) (0, 0 for no-slip walls, iniu 'zer'; lz shear and
+ * -lz shear for 'cou'; 2 bulk_v_sup for free slip), and allocates the
+ * solver's workspace (itot even, ktot >= 4; in host memory mode also device
+ * copies of the 13 fields).  The flow solver of the Crank-Nicolson path
+ * (fsolver = 'c', crnk.f90) is not provided. */
+int sg_set_flow_params(sg_ctx* ctx, double rep, double vb2, double vt2);
+int sg_flow_step(sg_ctx* ctx, double dt, const double* uo, const double* vo, const double* wo,
+                 const double* uoo, const double* voo, const double* woo, double* p,
+                 const double* fx, const double* fy, const double* fz,
+                 double* u, double* v, double* w);
+
 /* Spreading for callers that cannot allocate device memory.  It has no
  * counterpart in the reference; it is sg_spread (lagr2eulr) without a
  * context.  It is for host codes whose device memory is all owned by their

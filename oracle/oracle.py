@@ -197,21 +197,45 @@ def boundp(f):
     return f
 
 
-def poisson_solver1d(rhs, dx, dy, dz):
-    """solver1d with initsolver(0) (solver.f90:43-157, initsolver.f90:11-100): the second-order
-    Laplacian, periodic in x and y (real FFTs; eigenvalues -4/dx^2 sin^2(pi m / itot) and the
-    same in y, initsolver.f90:111-130) and Neumann in z (b(1) += a(1), b(kmax) += c(kmax)),
-    solved per mode by the reference's tridiagonal elimination, whose last pivot is exactly zero
-    for the mean mode, which is then set to zero.  rhs: [kmax, jtot, itot] interior values."""
-    kmax, jtot, itot = rhs.shape
+def solver_rows(kmax, dz, e, shift=0.0):
+    """initsolver(e) rows a, b, c (initsolver.f90:20-100): e = 0, 1 Neumann at both walls;
+    e = 2 the no-slip ghost rows of u, v and b -= Rep/dt; e = 3 the w rows (w = 0 at the top
+    face: an identity last row) and b -= Rep/dt.  shift = Rep/dt."""
     dzi = 1.0 / dz
     a = np.full(kmax, dzi * dzi)
     c = np.full(kmax, dzi * dzi)
     b = -(a + c)
-    b[0] += a[0]
-    b[-1] += c[-1]
-    a[0] = 0.0
-    c[-1] = 0.0
+    if e in (0, 1):
+        b[0] = b[0] + a[0]
+        b[-1] = b[-1] + c[-1]
+        a[0] = 0.0
+        c[-1] = 0.0
+    else:
+        if e == 2:
+            b[0] = b[0] - a[0]
+            b[-1] = b[-1] - c[-1]
+            a[0] = 0.0
+            c[-1] = 0.0
+        else:
+            b[-1] = 1.0
+            a[0] = 0.0
+            a[-1] = 0.0
+            c[-1] = 0.0
+        b = b - shift
+        if e == 3:
+            b[-1] = 1.0
+    return a, b, c
+
+
+def poisson_solver1d(rhs, dx, dy, dz, e=0, shift=0.0):
+    """solver1d after initsolver(e) (solver.f90:43-157, initsolver.f90:11-130): the
+    second-order Laplacian (minus shift = Rep/dt for e = 2, 3), periodic in x and y (real
+    FFTs; eigenvalues -4/dx^2 sin^2(pi m / itot) and the same in y, initsolver.f90:111-130)
+    and the rows of solver_rows in z, solved per mode by the reference's tridiagonal
+    elimination: for e = 0, 1 its last pivot is exactly zero for the mean mode, which is then
+    set to zero; for e = 3 the last row takes no eigenvalue.  rhs: [kmax, jtot, itot]."""
+    kmax, jtot, itot = rhs.shape
+    a, b, c = solver_rows(kmax, dz, e, shift)
     # xrt(2m) = -4 dxi^2 sin(2m pi / (2 itot))^2 (initsolver.f90:111-116), likewise yrt
     dxi, dyi = 1.0 / dx, 1.0 / dy
     lx = -4.0 * dxi * dxi * np.sin((2 * np.arange(itot // 2 + 1)) * np.pi / (2.0 * itot)) ** 2
@@ -227,12 +251,116 @@ def poisson_solver1d(rhs, dx, dy, dz):
         z = 1.0 / ((b[k] + lam) - a[k] * d[k - 1])
         d[k] = c[k] * z
         p[k] = (p[k] - a[k] * p[k - 1]) * z
-    z = (b[-1] + lam) - a[-1] * d[-2]
+    z = ((b[-1] + lam) if e != 3 else b[-1]) - a[-1] * d[-2]
     nz = z != 0.0
     p[-1] = np.where(nz, (p[-1] - a[-1] * p[-2]) / np.where(nz, z, 1.0), 0.0)
     for k in range(kmax - 2, -1, -1):
         p[k] = p[k] - d[k] * p[k + 1]
     return np.fft.irfft2(p, s=(jtot, itot), axes=(1, 2))
+
+
+def bounduvw(u, v, w, vb2=0.0, vt2=0.0):
+    """bounduvw (bound.f90:7-86): walls u(0) = -u(1), v(0) = vb2 - v(1), w(0) = 0,
+    u(k1) = -u(kmax), v(k1) = vt2 - v(kmax), w(kmax) = 0, w(k1) = w(kmax-1) (vb2 = vt2 = 0
+    for iniu 'zer', 'poi', 'log' with no-slip walls; 2 bulk_v_sup both for free slip;
+    lz shear and -lz shear for 'cou'); then the periodic x, y halo copies."""
+    u[0] = -u[1]
+    v[0] = vb2 - v[1]
+    w[0] = 0.0
+    u[-1] = -u[-2]
+    v[-1] = vt2 - v[-2]
+    w[-2] = 0.0
+    w[-1] = w[-3]
+    for f in (u, v, w):
+        f[:, :, -1] = f[:, :, 1]
+        f[:, :, 0] = f[:, :, -2]
+        f[:, -1, :] = f[:, 1, :]
+        f[:, 0, :] = f[:, -2, :]
+
+
+def _sh(f, dk, dj, di):
+    """f at (i + di, j + dj, k + dk) over the interior, f of shape (k1+1, j1+1, i1+1)."""
+    K, J, I = f.shape
+    return f[1 + dk:K - 1 + dk, 1 + dj:J - 1 + dj, 1 + di:I - 1 + di]
+
+
+def _adv(U, V, W, comp, dxi, dyi, dzi):
+    """The convective flux differences of momxad / momyad / momzad (mom.f90:9-54, 136-181,
+    266-311) at one time level: returns the three (p, m) pairs of the x, y and z faces."""
+    S = _sh
+    if comp == 0:
+        xp = 0.25 * (S(U, 0, 0, 1) + S(U, 0, 0, 0)) * (S(U, 0, 0, 1) + S(U, 0, 0, 0))
+        xm = 0.25 * (S(U, 0, 0, -1) + S(U, 0, 0, 0)) * (S(U, 0, 0, -1) + S(U, 0, 0, 0))
+        yp = 0.25 * (S(U, 0, 1, 0) + S(U, 0, 0, 0)) * (S(V, 0, 0, 1) + S(V, 0, 0, 0))
+        ym = 0.25 * (S(U, 0, -1, 0) + S(U, 0, 0, 0)) * (S(V, 0, -1, 1) + S(V, 0, -1, 0))
+        zp = 0.25 * (S(U, 1, 0, 0) + S(U, 0, 0, 0)) * (S(W, 0, 0, 1) + S(W, 0, 0, 0))
+        zm = 0.25 * (S(U, -1, 0, 0) + S(U, 0, 0, 0)) * (S(W, -1, 0, 1) + S(W, -1, 0, 0))
+    elif comp == 1:
+        xp = 0.25 * (S(U, 0, 0, 0) + S(U, 0, 1, 0)) * (S(V, 0, 0, 0) + S(V, 0, 0, 1))
+        xm = 0.25 * (S(U, 0, 0, -1) + S(U, 0, 1, -1)) * (S(V, 0, 0, 0) + S(V, 0, 0, -1))
+        yp = 0.25 * (S(V, 0, 0, 0) + S(V, 0, 1, 0)) * (S(V, 0, 0, 0) + S(V, 0, 1, 0))
+        ym = 0.25 * (S(V, 0, 0, 0) + S(V, 0, -1, 0)) * (S(V, 0, 0, 0) + S(V, 0, -1, 0))
+        zp = 0.25 * (S(W, 0, 0, 0) + S(W, 0, 1, 0)) * (S(V, 1, 0, 0) + S(V, 0, 0, 0))
+        zm = 0.25 * (S(W, -1, 0, 0) + S(W, -1, 1, 0)) * (S(V, -1, 0, 0) + S(V, 0, 0, 0))
+    else:
+        xp = 0.25 * (S(W, 0, 0, 0) + S(W, 0, 0, 1)) * (S(U, 0, 0, 0) + S(U, 1, 0, 0))
+        xm = 0.25 * (S(W, 0, 0, 0) + S(W, 0, 0, -1)) * (S(U, 0, 0, -1) + S(U, 1, 0, -1))
+        yp = 0.25 * (S(W, 0, 0, 0) + S(W, 0, 1, 0)) * (S(V, 0, 0, 0) + S(V, 1, 0, 0))
+        ym = 0.25 * (S(W, 0, 0, 0) + S(W, 0, -1, 0)) * (S(V, 0, -1, 0) + S(V, 1, -1, 0))
+        zp = 0.25 * (S(W, 0, 0, 0) + S(W, 1, 0, 0)) * (S(W, 0, 0, 0) + S(W, 1, 0, 0))
+        zm = 0.25 * (S(W, 0, 0, 0) + S(W, -1, 0, 0)) * (S(W, 0, 0, 0) + S(W, -1, 0, 0))
+    return (xp, xm), (yp, ym), (zp, zm)
+
+
+def momad(comp, uo, vo, wo, uoo, voo, woo, dxi, dyi, dzi):
+    """momxad / momyad / momzad: Adams-Bashforth convection, 1.5 (level n) - 0.5 (level n-1)."""
+    (xp, xm), (yp, ym), (zp, zm) = _adv(uo, vo, wo, comp, dxi, dyi, dzi)
+    (xpo, xmo), (ypo, ymo), (zpo, zmo) = _adv(uoo, voo, woo, comp, dxi, dyi, dzi)
+    return (dxi * ((1.5 * (-xp + xm)) - (.5 * (-xpo + xmo)))
+            + dyi * ((1.5 * (-yp + ym)) - (.5 * (-ypo + ymo)))
+            + dzi * ((1.5 * (-zp + zm)) - (.5 * (-zpo + zmo))))
+
+
+def flow_step(grid, dt, rep, uo, vo, wo, uoo, voo, woo, pnew, fx, fy, fz, vb2=0.0, vt2=0.0):
+    """One step of the reference's FFT flow solver (fsolver = 'f', main.f90:333-347):
+    fftuvw (fftuvw.f90:13-127: pressure gradient and IB force, momxp..momzp; Adams-Bashforth
+    convection, momxad..momzad; the implicit Helmholtz solves of w with initsolver(3) and of
+    u, v with initsolver(2)), bounduvw, fillps, solver1d after initsolver(1), boundp, correc,
+    bounduvw, pnew += p, boundp.  Fields (0:i1,0:j1,0:k1) as [k][j][i]; uo.. is the velocity
+    at the start of the step (the reference's unew = uo), uoo the one before.  Returns
+    (u, v, w, pnew) at the end of the step."""
+    itot, jtot, ktot, dx, dy, dz = grid
+    dxi, dyi, dzi = 1.0 / dx, 1.0 / dy, 1.0 / dz
+    I = (slice(1, -1),) * 3
+    S = _sh
+    rhs = []
+    for comp, (f, dq) in enumerate(((fx, (0, 0, 1)), (fy, (0, 1, 0)), (fz, (1, 0, 0)))):
+        dxyz = (dxi, dyi, dzi)[comp]
+        durk = (-dxyz * ((S(pnew, *dq) - S(pnew, 0, 0, 0)))) + f[I]
+        d = -durk
+        d = d - momad(comp, uo, vo, wo, uoo, voo, woo, dxi, dyi, dzi)
+        d = d - ((uo, vo, wo)[comp][I] / dt)
+        rhs.append(d * rep)
+    shift = rep / dt
+    rhs[2][-1] = 0.0
+    u, v, w = (np.zeros_like(uo) for _ in range(3))
+    w[I] = poisson_solver1d(rhs[2], dx, dy, dz, e=3, shift=shift)
+    u[I] = poisson_solver1d(rhs[0], dx, dy, dz, e=2, shift=shift)
+    v[I] = poisson_solver1d(rhs[1], dx, dy, dz, e=2, shift=shift)
+    bounduvw(u, v, w, vb2, vt2)
+    dti = 1.0 / dt
+    ps = ((S(w, 0, 0, 0) - S(w, -1, 0, 0)) * (dti * dzi) + (S(v, 0, 0, 0) - S(v, 0, -1, 0)) * (dti * dyi)
+          + (S(u, 0, 0, 0) - S(u, 0, 0, -1)) * (dti * dxi))
+    p = np.zeros_like(uo)
+    p[I] = poisson_solver1d(ps, dx, dy, dz, e=1)
+    boundp(p)
+    u[I] = u[I] - (dt * dxi) * (S(p, 0, 0, 1) - S(p, 0, 0, 0))
+    v[I] = v[I] - (dt * dyi) * (S(p, 0, 1, 0) - S(p, 0, 0, 0))
+    w[I] = w[I] - (dt * dzi) * (S(p, 1, 0, 0) - S(p, 0, 0, 0))
+    bounduvw(u, v, w, vb2, vt2)
+    pn = _f64(pnew) + p
+    boundp(pn)
+    return u, v, w, pn
 
 
 def indicator(grid, x, y, z, nx, ny, nz, area, visc0=1.0 / 0.0016, lam=1.0, thetainc=70.0 * np.pi / 180.0,

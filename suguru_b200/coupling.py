@@ -39,7 +39,7 @@ EXPORTS = ["sg_create", "sg_destroy", "sg_last_error", "sg_synchronize", "sg_int
            "sg_surrogate_set_trust", "sg_surrogate_last_counts", "sg_set_point_split", "sg_get_point_split",
            "sg_set_tensor_cores", "sg_set_legendre_terms", "sg_get_legendre_terms", "sg_set_capsule_law",
            "sg_set_legendre_tile_rows", "sg_get_legendre_tile_rows", "sg_set_wall_collisions", "sg_collisions",
-           "sg_set_indicator_params", "sg_indicator"]
+           "sg_set_indicator_params", "sg_indicator", "sg_set_flow_params", "sg_flow_step"]
 # test hooks declared in include/sg_testing.h
 TEST_EXPORTS = ["sg_test_legendre", "sg_test_gemm", "sg_test_mlp_grad"]
 WORKLOAD_EXPORTS = ["sg_prescribed_flow"]  # include/sg_workload.h
@@ -91,6 +91,8 @@ def lib():
     L.sg_collisions.argtypes = [vp] * 4
     L.sg_set_indicator_params.argtypes = [vp] + [ctypes.c_double] * 5
     L.sg_indicator.argtypes = [vp] * 12
+    L.sg_set_flow_params.argtypes = [vp] + [ctypes.c_double] * 3
+    L.sg_flow_step.argtypes = [vp, ctypes.c_double] + [vp] * 13
     L.sg_gauss.argtypes = [ctypes.c_int, dp, dp]
     L.sg_legendre.argtypes = [ctypes.c_double, ctypes.c_int, ctypes.c_int, dp, dp, dp]
     L.sg_last_launch_count.argtypes = [vp]
@@ -479,6 +481,18 @@ class CouplingStep:
         self._check(lib().sg_indicator(self._h, *map(_ptr, (X, Y, Z, NX, NY, NZ, AREA, indic, visc, fy, fz))),
                     "sg_indicator")
         return indic, visc
+
+    def set_flow_params(self, rep=0.0016, vb2=0.0, vt2=0.0):
+        """Rep and the wall values of v of the FFT flow solver (FP64 contexts)."""
+        self._check(lib().sg_set_flow_params(self._h, float(rep), float(vb2), float(vt2)), "sg_set_flow_params")
+
+    def flow_step(self, dt, uo, vo, wo, uoo, voo, woo, p, fx, fy, fz, out=None):
+        """fsolver = 'f' (main.f90:333-347): returns (u, v, w) after one step; p is updated in place."""
+        u, v, w = out if out is not None else self._eul(3)
+        self._check(lib().sg_flow_step(self._h, ctypes.c_double(dt),
+                                       *map(_ptr, (uo, vo, wo, uoo, voo, woo, p, fx, fy, fz, u, v, w))),
+                    "sg_flow_step")
+        return u, v, w
 
     def surf_vol(self, X, Y, Z, NX, NY, NZ, AREA, exy1_prev=None):
         """surf_vol.f90:12 -- [ncap, 7]: volume, area, exy1, exy2, centroid."""

@@ -721,7 +721,7 @@ void sg_destroy(sg_ctx* c) {
   if (c->st) cudaStreamSynchronize(c->st);
   if (c->graph_exec) cudaGraphExecDestroy(c->graph_exec);
   if (c->graph) cudaGraphDestroy(c->graph);
-  indicator_free(c);
+  poisson_free(c);
   for (void* p : c->allocs) cudaFree(p);
   for (int k = 0; k <= SG_NSTAGE; ++k)
     if (c->ev[k]) cudaEventDestroy(c->ev[k]);
@@ -901,6 +901,46 @@ int sg_indicator(sg_ctx* c, const double* X, const double* Y, const double* Z, c
     if (visc) SG_RET(d2h(c, visc, dV, fb));
     if (fy) SG_RET(d2h(c, fy, dFy, fb));
     if (fz) SG_RET(d2h(c, fz, dFz, fb));
+  }
+  return finish(c);
+}
+
+int sg_set_flow_params(sg_ctx* c, double rep, double vb2, double vt2) {
+  if (!c) return SG_ERR_ARG;
+  if (c->graph) return fail(c, SG_ERR_STATE, "release the captured graph first");
+  SG_RET(flow_setup(c, rep, vb2, vt2));
+  SG_TRY(cudaDeviceSynchronize(), "flow setup");
+  return SG_OK;
+}
+
+int sg_flow_step(sg_ctx* c, double dt, const double* uo, const double* vo, const double* wo, const double* uoo,
+                 const double* voo, const double* woo, double* p, const double* fx, const double* fy,
+                 const double* fz, double* u, double* v, double* w) {
+  if (!c) return SG_ERR_ARG;
+  if (!c->flow.ready) return fail(c, SG_ERR_STATE, "flow parameters not set (sg_set_flow_params)");
+  if (!(dt > 0.0) || !std::isfinite(dt)) return fail(c, SG_ERR_ARG, "dt must be positive and finite");
+  SG_RET(check_ptrs(c, {uo, vo, wo, uoo, voo, woo, p, fx, fy, fz, u, v, w}));
+  const bool host = c->cfg.mem == SG_MEM_HOST;
+  const size_t fb = sizeof(double) * c->nfield;
+  const double* in[10] = {uo, vo, wo, uoo, voo, woo, p, fx, fy, fz};
+  double* out[3] = {u, v, w};
+  const double* din[10];
+  double* dout[3];
+  for (int q = 0; q < 10; ++q) din[q] = in[q];
+  for (int q = 0; q < 3; ++q) dout[q] = out[q];
+  if (host) {
+    for (int q = 0; q < 10; ++q) {
+      SG_RET(h2d(c, c->flow.stage[q], in[q], fb));
+      din[q] = (const double*)c->flow.stage[q];
+    }
+    for (int q = 0; q < 3; ++q) dout[q] = (double*)c->flow.stage[10 + q];
+  }
+  c->launches = 0;
+  SG_RET(flow_run(c, dt, din[0], din[1], din[2], din[3], din[4], din[5], (double*)din[6], din[7], din[8], din[9],
+                  dout[0], dout[1], dout[2]));
+  if (host) {
+    SG_RET(d2h(c, p, din[6], fb));
+    for (int q = 0; q < 3; ++q) SG_RET(d2h(c, out[q], dout[q], fb));
   }
   return finish(c);
 }

@@ -121,20 +121,33 @@ struct sg_ctx {
   float sur_trust[5] = {0.f, 0.f, 0.f, 0.f, 0.f};  // amp_max, ratio_max, c_min, c_max, enabled
   // Lagrangian scratch for sg_capsule_spectra in device mode (allocated on first use)
   void* spec_scratch[7] = {};
+  // solver1d on the GPU (sg_poisson.cu), shared by the indicator and the flow solver
+  struct PoissonState {
+    bool ready = false, have_plans = false;
+    double* r = nullptr;     // real FFT input / output [ktot][jtot][itot]
+    void* c = nullptr;       // modes [ktot][jtot][itot/2 + 1] (double2)
+    double* d = nullptr;     // elimination multipliers [ktot][modes]
+    double* tab = nullptr;   // xrt [itot/2 + 1], yrt [jtot]
+    int plan_f = 0, plan_b = 0;  // cufftHandle
+  } pois;
   // indicator function (sg_indicator.cu), set up by sg_set_indicator_params
   struct IndState {
-    bool ready = false, have_plans = false;
+    bool ready = false;
     double visc0 = 0, lambda = 1, sin_t = 0, mcos_t = 0, amp = 0;
     sg::IBGrid grid{};       // ktot + 2 planes: interior k = 0 .. kmax + 1 of the real grid
     sg::IBWork w{};          // FP64 records of the normals
     double* zr = nullptr;    // raised z of the points
     double* g = nullptr;     // gx, gy, gz on the taller grid
-    double* r = nullptr;     // real FFT input / output [ktot][jtot][itot]
-    void* c = nullptr;       // modes [ktot][jtot][itot/2 + 1] (double2)
-    double* d = nullptr;     // elimination multipliers [ktot][modes]
-    double* tab = nullptr;   // a, b, c rows [3][ktot], xrt [itot/2 + 1], yrt [jtot]
-    int plan_f = 0, plan_b = 0;  // cufftHandle
   } ind;
+  // flow solver (sg_flow_solver.cu), set up by sg_set_flow_params
+  struct FlowState {
+    bool ready = false;
+    double rep = 1, vb2 = 0, vt2 = 0;
+    double* ru = nullptr;    // right-hand sides of u and v, [ktot][jtot][itot]
+    double* rv = nullptr;
+    double* p = nullptr;     // pressure correction with halos
+    void* stage[13] = {};    // device copies of the fields in host memory mode
+  } flow;
 };
 
 namespace sg {
@@ -170,12 +183,23 @@ const int* sur_flags(sg_ctx* c);
 // force pipeline only, outputs into device arrays lag[0..6] (sg_context.cu)
 int run_forces_only(sg_ctx* c, const double* X, const double* Y, const double* Z, void* const* lag);
 
+// solver1d (sg_poisson.cu): FFT buffers and plans made once per context;
+// poisson_solve replaces r ([ktot][jtot][itot], interior values) with
+// itot * jtot times the solution of the rows of initsolver(e) (shift = Rep/dt
+// for e = 2, 3): the FFT pair is left unnormalised.
+int poisson_setup(sg_ctx* c);
+void poisson_free(sg_ctx* c);
+int poisson_solve(sg_ctx* c, double* r, int e, double shift, cudaStream_t st);
 // indicator function (sg_indicator.cu)
 int indicator_setup(sg_ctx* c, double visc0, double lambda, double thetainc, double ta, double rep);
-void indicator_free(sg_ctx* c);
 template <class T>
 int indicator_run(sg_ctx* c, const double* X, const double* Y, const double* Z, const T* NX, const T* NY, const T* NZ,
                   const T* A, T* indic, T* visc, T* fy, T* fz);
+// flow solver (sg_flow_solver.cu), FP64 fields
+int flow_setup(sg_ctx* c, double rep, double vb2, double vt2);
+int flow_run(sg_ctx* c, double dt, const double* uo, const double* vo, const double* wo, const double* uoo,
+             const double* voo, const double* woo, double* p, const double* fx, const double* fy, const double* fz,
+             double* u, double* v, double* w);
 
 template <class P>
 cudaError_t dalloc(sg_ctx* c, P*& p, size_t bytes) {

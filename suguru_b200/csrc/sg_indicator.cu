@@ -9,10 +9,7 @@
 //     kmax + 1 of the real grid.
 //  2. The central-difference divergence of g (:49-66) is the right-hand side
 //     of the Poisson equation that solver1d solves after initsolver(0)
-//     (solver.f90:43-157, initsolver.f90:11-130): a real 2-D FFT per z
-//     plane (cuFFT), per (x, y) mode the reference's tridiagonal elimination
-//     in z with its Neumann rows and its zero last pivot for the mean mode,
-//     and the inverse FFT.
+//     (sg_poisson.cu).
 //  3. indic = the solution lowered back by ktot/4 planes (zero above), its
 //     halos from boundind (bound.f90:113-139: Neumann z, periodic x, y) taken
 //     before the 0.01 / 0.9 thresholds, which apply to the interior only
@@ -21,18 +18,13 @@
 //     interior (:156-180).
 // Everything runs in FP64; the mixed path converts its FP32 inputs and
 // rounds its FP32 outputs once.
-#include <cufft.h>
-
 #include <cmath>
-#include <vector>
 
 #include "sg_common.cuh"
 #include "sg_ctx.h"
 
 namespace sg {
 namespace {
-
-constexpr double kPi = 3.14159265358979323846264338327950288;
 
 __global__ void raise_z_kernel(long n, double off, const double* __restrict__ Z, double* __restrict__ Zr) {
   const long p = (long)blockIdx.x * blockDim.x + threadIdx.x;
@@ -74,63 +66,6 @@ __global__ void divergence_kernel(IndGrid g, const double* __restrict__ gx, cons
   const double dgy = __dmul_rn((gy[o + g.ldi] - gy[o - g.ldi]) * .5, g.dyi);
   const double dgz = __dmul_rn((gz[o + plane] - gz[o - plane]) * .5, g.dzi);
   rhs[q] = __dadd_rn(__dadd_rn(dgx, dgy), dgz);
-}
-
-// solver1d's elimination in z (solver.f90:84-129) for every (x, y) mode of
-// the transformed right-hand side c[k][mode]; d[k][mode] holds the
-// multipliers.  The operations keep the reference's order and roundings
-// (no fused multiply-add), so the mean mode's last pivot is exactly zero
-// whenever it is in exact arithmetic, and that mode's top value is then zero.
-__global__ void tridiag_kernel(int kmax, int nmodes, int nxm, const double* __restrict__ abc,
-                               const double* __restrict__ xrt, const double* __restrict__ yrt,
-                               double2* __restrict__ c, double* __restrict__ d) {
-  const int m = blockIdx.x * blockDim.x + threadIdx.x;
-  if (m >= nmodes) return;
-  const double* a = abc;
-  const double* b = abc + kmax;
-  const double* cc = abc + 2 * kmax;
-  const double lam = __dadd_rn(xrt[m % nxm], yrt[m / nxm]);
-  double z = __drcp_rn(__dadd_rn(b[0], lam));
-  double dk = __dmul_rn(cc[0], z);
-  double2 p = c[m];
-  p.x = __dmul_rn(p.x, z);
-  p.y = __dmul_rn(p.y, z);
-  c[m] = p;
-  d[m] = dk;
-  for (int k = 1; k < kmax - 1; ++k) {
-    const long o = (long)k * nmodes + m;
-    z = __drcp_rn(__dsub_rn(__dadd_rn(b[k], lam), __dmul_rn(a[k], dk)));
-    dk = __dmul_rn(cc[k], z);
-    double2 q = c[o];
-    q.x = __dmul_rn(__dsub_rn(q.x, __dmul_rn(a[k], p.x)), z);
-    q.y = __dmul_rn(__dsub_rn(q.y, __dmul_rn(a[k], p.y)), z);
-    c[o] = q;
-    d[o] = dk;
-    p = q;
-  }
-  {
-    const int k = kmax - 1;
-    const long o = (long)k * nmodes + m;
-    z = __dsub_rn(__dadd_rn(b[k], lam), __dmul_rn(a[k], dk));
-    double2 q = c[o];
-    if (z != 0.0) {
-      q.x = __ddiv_rn(__dsub_rn(q.x, __dmul_rn(a[k], p.x)), z);
-      q.y = __ddiv_rn(__dsub_rn(q.y, __dmul_rn(a[k], p.y)), z);
-    } else {
-      q.x = q.y = 0.0;
-    }
-    c[o] = q;
-    p = q;
-  }
-  for (int k = kmax - 2; k >= 0; --k) {
-    const long o = (long)k * nmodes + m;
-    const double dd = d[o];
-    double2 q = c[o];
-    q.x = __dsub_rn(q.x, __dmul_rn(dd, p.x));
-    q.y = __dsub_rn(q.y, __dmul_rn(dd, p.y));
-    c[o] = q;
-    p = q;
-  }
 }
 
 struct IndPost {
@@ -200,10 +135,10 @@ unsigned blocks(long n) { return (unsigned)((n + 255) / 256); }
 
 int indicator_setup(sg_ctx* c, double visc0, double lambda, double thetainc, double ta, double rep) {
   const sg_config& f = c->cfg;
-  if (!(f.itot % 2 == 0) || f.ktot < 4) return fail(c, SG_ERR_CONFIG, "the indicator needs an even itot and ktot >= 4");
   if (!std::isfinite(visc0) || !std::isfinite(lambda) || !std::isfinite(thetainc) || !(ta >= 0.0) ||
       !std::isfinite(ta) || !(rep > 0.0) || !std::isfinite(rep))
     return fail(c, SG_ERR_ARG, "indicator parameters must be finite, ta >= 0 and rep > 0");
+  SG_RET(poisson_setup(c));
   auto& s = c->ind;
   s.visc0 = visc0;
   s.lambda = lambda;
@@ -224,57 +159,10 @@ int indicator_setup(sg_ctx* c, double visc0, double lambda, double thetainc, dou
   SG_TRY(dalloc(c, s.w.counts, sizeof(int) * g.ntiles), "alloc");
   SG_TRY(dalloc(c, s.w.starts, sizeof(int) * (g.ntiles + 1)), "alloc");
   SG_TRY(dalloc(c, s.w.fill, sizeof(int) * g.ntiles), "alloc");
-  void* p = nullptr;
-  SG_TRY(dalloc(c, p, sizeof(double) * std::max(np, 1L)), "alloc");
-  s.zr = (double*)p;
-  const long gsz = (long)g.ldi * g.ldj * g.ldk;
-  SG_TRY(dalloc(c, p, sizeof(double) * 3 * gsz), "alloc");
-  s.g = (double*)p;
-  const long nreal = (long)f.itot * f.jtot * f.ktot, nxm = f.itot / 2 + 1, nmodes = nxm * f.jtot;
-  SG_TRY(dalloc(c, p, sizeof(double) * nreal), "alloc");
-  s.r = (double*)p;
-  SG_TRY(dalloc(c, p, sizeof(double2) * nmodes * f.ktot), "alloc");
-  s.c = p;
-  SG_TRY(dalloc(c, p, sizeof(double) * nmodes * f.ktot), "alloc");
-  s.d = (double*)p;
-  // initsolver(0): tridiagonal rows (:20-39) and the eigenvalues xrt, yrt
-  // (:111-130) for the modes of a real transform in x and a complex one in y
-  std::vector<double> abc(3 * f.ktot), xrt(nxm), yrt(f.jtot);
-  const double dzi = 1.0 / dz, dxi = f.itot / f.lx, dyi = f.jtot / f.ly;
-  for (int k = 0; k < f.ktot; ++k) {
-    abc[k] = dzi * dzi;
-    abc[2 * f.ktot + k] = dzi * dzi;
-    abc[f.ktot + k] = -(abc[k] + abc[2 * f.ktot + k]);
-  }
-  abc[f.ktot] = abc[f.ktot] + abc[0];
-  abc[2 * f.ktot - 1] = abc[2 * f.ktot - 1] + abc[3 * f.ktot - 1];
-  abc[0] = 0.;
-  abc[3 * f.ktot - 1] = 0.;
-  for (long m = 0; m < nxm; ++m) xrt[m] = -4. * dxi * dxi * std::pow(std::sin((double)(2 * m) * kPi / (2. * f.itot)), 2.);
-  for (int j = 0; j < f.jtot; ++j) {
-    const int jm = std::min(j, f.jtot - j);
-    yrt[j] = -4. * dyi * dyi * std::pow(std::sin((double)(2 * jm) * kPi / (2. * f.jtot)), 2.);
-  }
-  SG_TRY(dalloc(c, p, sizeof(double) * (3 * f.ktot + nxm + f.jtot)), "alloc");
-  s.tab = (double*)p;
-  SG_TRY(cudaMemcpy(s.tab, abc.data(), sizeof(double) * abc.size(), cudaMemcpyHostToDevice), "upload");
-  SG_TRY(cudaMemcpy(s.tab + 3 * f.ktot, xrt.data(), sizeof(double) * nxm, cudaMemcpyHostToDevice), "upload");
-  SG_TRY(cudaMemcpy(s.tab + 3 * f.ktot + nxm, yrt.data(), sizeof(double) * f.jtot, cudaMemcpyHostToDevice), "upload");
-  int n2[2] = {f.jtot, f.itot};
-  if (cufftPlanMany(&s.plan_f, 2, n2, nullptr, 1, 0, nullptr, 1, 0, CUFFT_D2Z, f.ktot) != CUFFT_SUCCESS ||
-      cufftPlanMany(&s.plan_b, 2, n2, nullptr, 1, 0, nullptr, 1, 0, CUFFT_Z2D, f.ktot) != CUFFT_SUCCESS)
-    return fail(c, SG_ERR_CUDA, "cuFFT plan");
-  s.have_plans = true;
+  SG_TRY(dalloc(c, s.zr, sizeof(double) * std::max(np, 1L)), "alloc");
+  SG_TRY(dalloc(c, s.g, sizeof(double) * 3 * (size_t)g.ldi * g.ldj * g.ldk), "alloc");
   s.ready = true;
   return SG_OK;
-}
-
-void indicator_free(sg_ctx* c) {
-  if (c->ind.have_plans) {
-    cufftDestroy(c->ind.plan_f);
-    cufftDestroy(c->ind.plan_b);
-    c->ind.have_plans = false;
-  }
 }
 
 template <class T>
@@ -295,25 +183,19 @@ int indicator_run(sg_ctx* c, const double* X, const double* Y, const double* Z, 
   SG_TRY(launch_bin<double>(g, np, X, Y, s.zr, s.w, st), "indicator binning");
   const long gsz = (long)g.ldi * g.ldj * g.ldk;
   SG_TRY(launch_spread_centred<double>(g, s.w, s.g, s.g + gsz, s.g + 2 * gsz, st), "indicator spread");
-  // 2. divergence, FFT, elimination in z, inverse FFT
+  // 2. divergence, then solver1d after initsolver(0)
   IndGrid ig{f.itot, f.jtot, f.ktot, g.ldi, g.ldj, g.dxi, g.dyi, g.dzi};
   const long nreal = (long)f.itot * f.jtot * f.ktot;
-  divergence_kernel<<<blocks(nreal), 256, 0, st>>>(ig, s.g, s.g + gsz, s.g + 2 * gsz, s.r);
-  if (cufftSetStream(s.plan_f, st) != CUFFT_SUCCESS || cufftSetStream(s.plan_b, st) != CUFFT_SUCCESS ||
-      cufftExecD2Z(s.plan_f, s.r, (cufftDoubleComplex*)s.c) != CUFFT_SUCCESS)
-    return fail(c, SG_ERR_CUDA, "cuFFT forward");
-  const int nxm = f.itot / 2 + 1, nmodes = nxm * f.jtot;
-  tridiag_kernel<<<blocks(nmodes), 256, 0, st>>>(f.ktot, nmodes, nxm, s.tab, s.tab + 3 * f.ktot,
-                                                  s.tab + 3 * f.ktot + nxm, (double2*)s.c, s.d);
-  if (cufftExecZ2D(s.plan_b, (cufftDoubleComplex*)s.c, s.r) != CUFFT_SUCCESS)
-    return fail(c, SG_ERR_CUDA, "cuFFT inverse");
+  double* r = c->pois.r;
+  divergence_kernel<<<blocks(nreal), 256, 0, st>>>(ig, s.g, s.g + gsz, s.g + 2 * gsz, r);
+  SG_RET(poisson_solve(c, r, 0, 0.0, st));
   // 3. indicator, viscosity, centrifugal terms
   IndPost P{ig, q, 1.0 / ((double)f.itot * f.jtot), s.visc0, s.lambda - 1.};
   const long nf = (long)g.ldi * g.ldj * (f.ktot + 2);
-  indic_kernel<T><<<blocks(nf), 256, 0, st>>>(P, s.r, indic, visc);
-  if (fy || fz) centrifugal_kernel<T><<<blocks(nreal), 256, 0, st>>>(P, s.r, s.sin_t, s.mcos_t, s.amp, fy, fz);
+  indic_kernel<T><<<blocks(nf), 256, 0, st>>>(P, r, indic, visc);
+  if (fy || fz) centrifugal_kernel<T><<<blocks(nreal), 256, 0, st>>>(P, r, s.sin_t, s.mcos_t, s.amp, fy, fz);
   SG_TRY(cudaGetLastError(), "indicator");
-  c->launches += 6 + (np > 0 ? 2 : 0) + ((fy || fz) ? 1 : 0);
+  c->launches += 5 + (np > 0 ? 2 : 0) + ((fy || fz) ? 1 : 0);
   return SG_OK;
 }
 
