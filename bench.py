@@ -38,8 +38,9 @@ def parse_args():
     p.add_argument("--steps", type=int, default=20)
     p.add_argument("--warmup", type=int, default=5)
     p.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    p.add_argument("--config", default="c1", choices=["c0", "c1", "c2", "c4"],
-                   help="c4: the 200-step time-stepped run of config 2 (steps/s, area/volume drift)")
+    p.add_argument("--config", default="c1", choices=["c0", "c1", "c2", "c4", "coupled"],
+                   help="c4: the 200-step time-stepped run of config 2 (steps/s, area/volume drift); "
+                        "coupled: the IB solver with the FFT flow solver on config 1's grid and capsules (FP64)")
     p.add_argument("--c4-steps", type=int, default=200)
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--only", default=None, choices=["mixed", "fp64"],
@@ -58,7 +59,7 @@ def parse_args():
 
 
 def workload(name):
-    return {"c0": W.config0, "c1": W.config1, "c2": W.config2}[name]()
+    return {"c0": W.config0, "c1": W.config1, "c2": W.config2, "coupled": W.config1}[name]()
 
 
 def load_peaks():
@@ -437,6 +438,56 @@ def run_c4(args, rank):
     return 0
 
 
+def run_coupled(args, rank):
+    """The coupled IB + flow solver (main.f90:172-347, fsolver 'f') on config 1's grid and
+    capsules in FP64: steps/s with and without the indicator, the stages, and the oracle's
+    main loop timed on the host for one step."""
+    import torch
+    from suguru_b200.ib_solver import IBSolver
+    if rank != 0:
+        return 0
+    torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", "0")))
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle as O
+    wl = W.config1()
+    u0 = list(wl.velocity())
+    O.bounduvw(*u0)
+    dt, rep = 0.01 * wl.grid[3], 0.0016  # Rep of param.f90:57
+    ind = dict(visc0=1.0 / rep, lam=1.0, thetainc=70.0 * np.pi / 180.0, ta=1160000.0, rep=rep)
+    out = {}
+    for name, indicator in (("without_indicator", None), ("with_indicator", ind)):
+        sol = IBSolver(wl, dt, rep, u0, indicator=indicator)
+        sol.run(args.warmup)
+        ms = sol.run(args.steps)
+        out[name] = {"steps_per_s": args.steps / (ms / 1e3), "ms_per_step": ms / args.steps,
+                     "stages_ms": sol.stage_times(3)}
+        del sol
+    cpu = None
+    if not args.no_cpu_baseline:
+        cores = os.cpu_count() or 1
+        x, y, z = wl.x.copy(), wl.y.copy(), wl.z.copy()
+        t0 = time.perf_counter()
+        r = O.coupling_step(wl.grid, wl.degree, wl.radius, *u0, x, y, z, wl.gs, wl.csk, nthreads=cores)
+        o = O.indicator(wl.grid, x, y, z, *r["n"], r["area"], fy=r["fgrid"][1], fz=r["fgrid"][2], **ind)
+        lx, ly, lz = (wl.grid[q] * wl.grid[q + 3] for q in range(3))
+        O.update_pos_capsules(wl.offsets, dt, lx, ly, lz, x, y, z, *r["u"])
+        O.flow_step(wl.grid, dt, rep, *u0, *u0, np.zeros_like(u0[0]), r["fgrid"][0], o["fy"], o["fz"])
+        sec = time.perf_counter() - t0
+        cpu = {"value": 1.0 / sec, "unit": "steps/s", "cores": cores, "kind": "port",
+               "sample": "one full step of the oracle's main loop with the indicator at this size (C coupling "
+                         "step on all host threads, numpy indicator and flow step)"}
+    head = out["with_indicator"]
+    print(json.dumps({
+        "metric": "coupled IB + FFT flow solver steps/s, config 1 grid and capsules, 1 B200",
+        "value": head["steps_per_s"], "unit": "steps/s", "n_gpus": 1, "steps": args.steps, "warmup": args.warmup,
+        "higher_is_better": True, "dtype": "f64", "data": "synthetic (seeded shapes and initial velocity modes)",
+        "config": {"workload": "256 capsules, L = 15 (524,288 points), grid 256x256x128, Rep = 0.0016, "
+                               "dt = 0.01 dx, indicator on (visc0 = 1/Rep, lambda = 1, thetainc = 70 deg, "
+                               "ta = 1.16e6)", "points": int(wl.npts)},
+        "with_indicator": head, "without_indicator": out["without_indicator"], "cpu_baseline": cpu}))
+    return 0
+
+
 def cpu_reference(wl, ncaps, steps, warmup, faithful=True):
     """The CPU FP64 restatement of the reference path (oracle, reference loop
     structure) on a bounded sample of the workload: the first `ncaps` capsules,
@@ -483,6 +534,8 @@ def main():
         return 0
     if args.config == "c4":
         return run_c4(args, rank)
+    if args.config == "coupled":
+        return run_coupled(args, rank)
     res = run_ours(args)
     if rank == 0 and res is not None:
         if not args.no_cpu_baseline:

@@ -81,18 +81,12 @@ struct Fields {
   const double *uo, *vo, *wo, *uoo, *voo, *woo, *p, *fx, *fy, *fz;
 };
 
-// fftuvw's right-hand sides into the solver's layout [k-1][j-1][i-1]
+// fftuvw's right-hand sides of u, v and w into the solver's layout
+// [k-1][j-1][i-1], one thread per interior cell for all three (the stencils
+// share most of their loads)
 template <int C>
-__global__ void momentum_rhs_kernel(FGrid g, Fields F, double dt, double rep, double* __restrict__ rhs) {
-  const long n = (long)g.itot * g.jtot * g.ktot;
-  const long q = (long)blockIdx.x * blockDim.x + threadIdx.x;
-  if (q >= n) return;
-  int i, j, k;
-  cell_of(g, q, i, j, k);
-  if (C == 2 && k == g.ktot) {  // dwdt(i,j,kmax) = 0 (fftuvw.f90:86-92)
-    rhs[q] = 0.0;
-    return;
-  }
+__device__ __forceinline__ double momentum_rhs(const FGrid& g, const Fields& F, double dt, double rep, int i, int j,
+                                               int k) {
   const long o = at(g, i, j, k);
   const long step = C == 0 ? 1 : (C == 1 ? g.ldi : g.plane);
   const double dd = C == 0 ? g.dxi : (C == 1 ? g.dyi : g.dzi);
@@ -106,7 +100,19 @@ __global__ void momentum_rhs_kernel(FGrid g, Fields F, double dt, double rep, do
   double d = -durk;
   d = d - ad;
   d = d - (vo[o] / dt);
-  rhs[q] = d * rep;
+  return d * rep;
+}
+
+__global__ void momentum_rhs_kernel(FGrid g, Fields F, double dt, double rep, double* __restrict__ ru,
+                                    double* __restrict__ rv, double* __restrict__ rw) {
+  const long n = (long)g.itot * g.jtot * g.ktot;
+  const long q = (long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (q >= n) return;
+  int i, j, k;
+  cell_of(g, q, i, j, k);
+  ru[q] = momentum_rhs<0>(g, F, dt, rep, i, j, k);
+  rv[q] = momentum_rhs<1>(g, F, dt, rep, i, j, k);
+  rw[q] = k == g.ktot ? 0.0 : momentum_rhs<2>(g, F, dt, rep, i, j, k);  // dwdt(i,j,kmax) = 0 (fftuvw.f90:86-92)
 }
 
 // interior values of a field from a solution (times the FFT pair's 1/n)
@@ -120,23 +126,42 @@ __global__ void from_solution_kernel(FGrid g, const double* __restrict__ sol, do
 }
 
 // bounduvw (mode 0: u; 1: v with wall values vb2, vt2; 2: w) or boundp (mode
-// 3): every cell outside the interior, and the w row kmax, from the rule of
-// bound.f90:7-139 applied at the interior column it copies
+// 3) on the cells outside the interior, from the rule of bound.f90:7-139 at
+// the interior column each copies.  One thread per halo cell: the two z
+// planes (all i, j), then the two y rows (k = 1..kmax, all i), then the two
+// x columns (k = 1..kmax, j = 1..jmax).  The w row kmax of the interior is
+// already zero: its right-hand side is zero and its row the identity.
 __global__ void halo_kernel(FGrid g, int mode, double vb2, double vt2, double* __restrict__ f) {
-  const long n = (long)g.ldi * g.ldj * (g.ktot + 2);
-  const long o = (long)blockIdx.x * blockDim.x + threadIdx.x;
-  if (o >= n) return;
-  const int i = (int)(o % g.ldi), j = (int)((o / g.ldi) % g.ldj), k = (int)(o / g.plane);
-  const bool inx = i >= 1 && i <= g.itot, iny = j >= 1 && j <= g.jtot, inz = k >= 1 && k <= g.ktot;
-  if (mode == 2 && k == g.ktot) {  // w(i,j,kmax) = 0, halos included
-    f[o] = 0.0;
+  const long nz = 2L * g.ldi * g.ldj, ny = 2L * g.ldi * g.ktot, nx = 2L * g.jtot * g.ktot;
+  long q = (long)blockIdx.x * blockDim.x + threadIdx.x;
+  int i, j, k;
+  if (q < nz) {
+    k = q < g.plane ? 0 : g.ktot + 1;
+    q %= g.plane;
+    j = (int)(q / g.ldi);
+    i = (int)(q % g.ldi);
+  } else if ((q -= nz) < ny) {
+    const long side = (long)g.ldi * g.ktot;
+    j = q < side ? 0 : g.jtot + 1;
+    q %= side;
+    k = 1 + (int)(q / g.ldi);
+    i = (int)(q % g.ldi);
+  } else if ((q -= ny) < nx) {
+    const long side = (long)g.jtot * g.ktot;
+    i = q < side ? 0 : g.itot + 1;
+    q %= side;
+    k = 1 + (int)(q / g.jtot);
+    j = 1 + (int)(q % g.jtot);
+  } else {
     return;
   }
-  if (inx && iny && inz) return;
+  const long o = at(g, i, j, k);
   const int is = i == 0 ? g.itot : (i == g.itot + 1 ? 1 : i);
   const int js = j == 0 ? g.jtot : (j == g.jtot + 1 ? 1 : j);
   double v;
-  if (inz) {
+  if (mode == 2 && k == g.ktot) {  // w(i,j,kmax) = 0 in the halos too
+    v = 0.0;
+  } else if (k >= 1 && k <= g.ktot) {
     v = f[at(g, is, js, k)];
   } else if (k == 0) {
     const double f1 = f[at(g, is, js, 1)];
@@ -219,14 +244,12 @@ int flow_run(sg_ctx* c, double dt, const double* uo, const double* vo, const dou
   const IBGrid& ib = c->grid;
   FGrid g{f.itot, f.jtot, f.ktot, ib.ldi, ib.ldj, (long)ib.ldi * ib.ldj, 1.0 / (f.lx / f.itot),
           1.0 / (f.ly / f.jtot), 1.0 / (f.lz / f.ktot)};
-  const long nreal = (long)f.itot * f.jtot * f.ktot, nf = c->nfield;
+  const long nreal = (long)f.itot * f.jtot * f.ktot, nf = c->nfield - nreal;  // halo cells
   const double inv_n = 1.0 / ((double)f.itot * f.jtot), shift = s.rep / dt;
   double* rw = c->pois.r;
   Fields F{uo, vo, wo, uoo, voo, woo, p, fx, fy, fz};
   // fftuvw: right-hand sides, then w (initsolver(3)) and u, v (initsolver(2))
-  momentum_rhs_kernel<0><<<blocks(nreal), 256, 0, st>>>(g, F, dt, s.rep, s.ru);
-  momentum_rhs_kernel<1><<<blocks(nreal), 256, 0, st>>>(g, F, dt, s.rep, s.rv);
-  momentum_rhs_kernel<2><<<blocks(nreal), 256, 0, st>>>(g, F, dt, s.rep, rw);
+  momentum_rhs_kernel<<<blocks(nreal), 256, 0, st>>>(g, F, dt, s.rep, s.ru, s.rv, rw);
   SG_TRY(cudaGetLastError(), "momentum");
   SG_RET(poisson_solve(c, rw, 3, shift, st));
   from_solution_kernel<<<blocks(nreal), 256, 0, st>>>(g, rw, inv_n, w);
@@ -250,7 +273,7 @@ int flow_run(sg_ctx* c, double dt, const double* uo, const double* vo, const dou
   add_interior_kernel<<<blocks(nreal), 256, 0, st>>>(g, s.p, p);
   halo_kernel<<<blocks(nf), 256, 0, st>>>(g, 3, 0.0, 0.0, p);
   SG_TRY(cudaGetLastError(), "flow step");
-  c->launches += 17;
+  c->launches += 15;
   return SG_OK;
 }
 

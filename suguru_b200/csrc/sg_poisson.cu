@@ -64,12 +64,23 @@ __device__ __forceinline__ Rows solver_row(int k, int kmax, int e, double dzi, d
   return r;
 }
 
-__global__ void tridiag_kernel(int kmax, int nmodes, int nxm, int e, double dzi, double shift,
-                               const double* __restrict__ xrt, const double* __restrict__ yrt,
-                               double2* __restrict__ c, double* __restrict__ d) {
+// A thread per mode walks its column of kmax planes twice; the columns of
+// neighbouring threads are adjacent in memory, and the loads of the next
+// kPre planes are issued ahead of the dependent arithmetic (a ring of
+// registers), since one column per thread leaves few warps to hide latency.
+constexpr int kPre = 8;
+
+__global__ void __launch_bounds__(128) tridiag_kernel(int kmax, int nmodes, int nxm, int e, double dzi, double shift,
+                                                      const double* __restrict__ xrt, const double* __restrict__ yrt,
+                                                      double2* __restrict__ c, double* __restrict__ d) {
   const int m = blockIdx.x * blockDim.x + threadIdx.x;
   if (m >= nmodes) return;
+  const long nm = nmodes;
   const double lam = __dadd_rn(xrt[m % nxm], yrt[m / nxm]);
+  double2 ring[kPre];
+#pragma unroll
+  for (int t = 0; t < kPre; ++t)
+    if (1 + t < kmax) ring[t] = c[(1 + t) * nm + m];
   Rows r = solver_row(0, kmax, e, dzi, shift);
   double z = __drcp_rn(__dadd_rn(r.b, lam));
   double dk = __dmul_rn(r.c, z);
@@ -78,42 +89,67 @@ __global__ void tridiag_kernel(int kmax, int nmodes, int nxm, int e, double dzi,
   p.y = __dmul_rn(p.y, z);
   c[m] = p;
   d[m] = dk;
-  for (int k = 1; k < kmax - 1; ++k) {
-    const long o = (long)k * nmodes + m;
-    r = solver_row(k, kmax, e, dzi, shift);
-    z = __drcp_rn(__dsub_rn(__dadd_rn(r.b, lam), __dmul_rn(r.a, dk)));
-    dk = __dmul_rn(r.c, z);
-    double2 q = c[o];
-    q.x = __dmul_rn(__dsub_rn(q.x, __dmul_rn(r.a, p.x)), z);
-    q.y = __dmul_rn(__dsub_rn(q.y, __dmul_rn(r.a, p.y)), z);
-    c[o] = q;
-    d[o] = dk;
-    p = q;
+  // forward elimination, rows 1 .. kmax-2
+  for (int k0 = 1; k0 < kmax - 1; k0 += kPre) {
+#pragma unroll
+    for (int t = 0; t < kPre; ++t) {
+      const int k = k0 + t;
+      if (k < kmax - 1) {
+        double2 q = ring[t];
+        if (k + kPre < kmax) ring[t] = c[(k + kPre) * nm + m];
+        r = solver_row(k, kmax, e, dzi, shift);
+        z = __drcp_rn(__dsub_rn(__dadd_rn(r.b, lam), __dmul_rn(r.a, dk)));
+        dk = __dmul_rn(r.c, z);
+        q.x = __dmul_rn(__dsub_rn(q.x, __dmul_rn(r.a, p.x)), z);
+        q.y = __dmul_rn(__dsub_rn(q.y, __dmul_rn(r.a, p.y)), z);
+        c[k * nm + m] = q;
+        d[k * nm + m] = dk;
+        p = q;
+      }
+    }
   }
   {
     const int k = kmax - 1;
-    const long o = (long)k * nmodes + m;
     r = solver_row(k, kmax, e, dzi, shift);
     const double bb = e == 3 ? r.b : __dadd_rn(r.b, lam);
     z = __dsub_rn(bb, __dmul_rn(r.a, dk));
-    double2 q = c[o];
+    double2 q = c[k * nm + m];
     if (z != 0.0) {
       q.x = __ddiv_rn(__dsub_rn(q.x, __dmul_rn(r.a, p.x)), z);
       q.y = __ddiv_rn(__dsub_rn(q.y, __dmul_rn(r.a, p.y)), z);
     } else {
       q.x = q.y = 0.0;
     }
-    c[o] = q;
+    c[k * nm + m] = q;
     p = q;
   }
-  for (int k = kmax - 2; k >= 0; --k) {
-    const long o = (long)k * nmodes + m;
-    const double dd = d[o];
-    double2 q = c[o];
-    q.x = __dsub_rn(q.x, __dmul_rn(dd, p.x));
-    q.y = __dsub_rn(q.y, __dmul_rn(dd, p.y));
-    c[o] = q;
-    p = q;
+  // back substitution, rows kmax-2 .. 0
+  double dring[kPre];
+#pragma unroll
+  for (int t = 0; t < kPre; ++t) {
+    const int k = kmax - 2 - t;
+    if (k >= 0) {
+      ring[t] = c[k * nm + m];
+      dring[t] = d[k * nm + m];
+    }
+  }
+  for (int k0 = kmax - 2; k0 >= 0; k0 -= kPre) {
+#pragma unroll
+    for (int t = 0; t < kPre; ++t) {
+      const int k = k0 - t;
+      if (k >= 0) {
+        double2 q = ring[t];
+        const double dd = dring[t];
+        if (k - kPre >= 0) {
+          ring[t] = c[(k - kPre) * nm + m];
+          dring[t] = d[(k - kPre) * nm + m];
+        }
+        q.x = __dsub_rn(q.x, __dmul_rn(dd, p.x));
+        q.y = __dsub_rn(q.y, __dmul_rn(dd, p.y));
+        c[k * nm + m] = q;
+        p = q;
+      }
+    }
   }
 }
 
@@ -171,7 +207,7 @@ int poisson_solve(sg_ctx* c, double* r, int e, double shift, cudaStream_t st) {
       cufftExecD2Z(s.plan_f, r, (cufftDoubleComplex*)s.c) != CUFFT_SUCCESS)
     return fail(c, SG_ERR_CUDA, "cuFFT forward");
   const int nxm = f.itot / 2 + 1, nmodes = nxm * f.jtot;
-  tridiag_kernel<<<(unsigned)((nmodes + 255) / 256), 256, 0, st>>>(f.ktot, nmodes, nxm, e, 1.0 / (f.lz / f.ktot), shift,
+  tridiag_kernel<<<(unsigned)((nmodes + 127) / 128), 128, 0, st>>>(f.ktot, nmodes, nxm, e, 1.0 / (f.lz / f.ktot), shift,
                                                                      s.tab, s.tab + nxm, (double2*)s.c, s.d);
   SG_TRY(cudaGetLastError(), "solver1d");
   if (cufftExecZ2D(s.plan_b, (cufftDoubleComplex*)s.c, r) != CUFFT_SUCCESS) return fail(c, SG_ERR_CUDA, "cuFFT inverse");

@@ -46,19 +46,38 @@ class IBSolver:
             self.ind = [torch.zeros_like(self.u[0]) for _ in range(2)]
             self.unext = [torch.zeros_like(self.u[0]) for _ in range(3)]
 
-    def step(self):
+    def step(self, marks=None):
+        """One step; marks: optional list of 5 CUDA events recorded between the stages
+        (coupling step, indicator, Update_Pos, flow step)."""
         cs, L = self.cs, self.lag
+        mark = (lambda q: marks[q].record(self.st)) if marks else (lambda q: None)
         with self.torch.cuda.stream(self.st):
             # uoo <- uo <- unew (buffers rotate; u still holds unew for the interpolation)
             self.uoo, self.uo = self.uo, self.uoo
             for a, b in zip(self.uo, self.u):
                 a.copy_(b)
+            mark(0)
             cs.step(*self.u, *self.X, lag_out=L, eul_out=self.force)
+            mark(1)
             if self.indicator:
                 cs.indicator(*self.X, L[6], L[7], L[8], L[9], fy=self.force[1], fz=self.force[2], out=self.ind)
+            mark(2)
             cs.update_pos(self.dt, *self.X, L[0], L[1], L[2])
+            mark(3)
             cs.flow_step(self.dt, *self.uo, *self.uoo, self.p, *self.force, out=self.unext)
+            mark(4)
             self.u, self.unext = self.unext, self.u
+
+    def stage_times(self, steps):
+        """Mean ms per stage over `steps` steps: coupling step, indicator, Update_Pos, flow step."""
+        torch = self.torch
+        ev = [torch.cuda.Event(enable_timing=True) for _ in range(5)]
+        acc = np.zeros(4)
+        for _ in range(steps):
+            self.step(marks=ev)
+            torch.cuda.synchronize()
+            acc += [ev[q].elapsed_time(ev[q + 1]) for q in range(4)]
+        return dict(zip(("coupling_step", "indicator", "update_pos", "flow_step"), (acc / steps).tolist()))
 
     def run(self, steps):
         """Advance `steps` steps; returns the CUDA-event time in ms."""
