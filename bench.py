@@ -58,6 +58,15 @@ def parse_args():
     return p.parse_args()
 
 
+WORKLOAD_LABELS = {
+    "c0": "single capsule, SH degree 15 (2,048 points), grid 128x64x64, dx=1/32, Skalak Gs=1 C=1",
+    "c1": "dense suspension: 256 capsules, SH degree 15 (524,288 points), grid 256x256x128, dx=1/32, "
+          "Skalak Gs=1 C=1",
+    "c2": "uneven batch: 1024 capsules, SH degree 7-23 (1,526,248 points), grid 512x256x256, dx=1/32, "
+          "Skalak Gs=1 C=1",
+}
+
+
 def workload(name):
     return {"c0": W.config0, "c1": W.config1, "c2": W.config2, "coupled": W.config1}[name]()
 
@@ -372,8 +381,7 @@ def run_ours(args):
                      "BF16x6 from 16 up unless --legendre-terms forces one, FP32 accumulation; "
                      "FP64 positions, centroids, tables)",
             "data": "synthetic (seeded shapes and velocity modes, no reference fixtures exist)",
-            "config": {"workload": "dense suspension: 256 capsules, SH degree 15 (524,288 points), "
-                                   "grid 256x256x128, dx=1/32, Skalak Gs=1 C=1",
+            "config": {"workload": WORKLOAD_LABELS[args.config],
                        "path": path, "points": n, "parallelism": "replicas" if world > 1 else
                        "single GPU", "l2": "flushed (256 MB write) between timed iterations",
                        "spread_tile": head["tile"], "spread_tile_fp64": fp64["tile"],
@@ -526,8 +534,7 @@ def main():
             "metric": "Lagrangian pts/s per IB step, mixed+surrogate vs FP64 plain, 1 B200, <=1e-4 err",
             "value": val, "unit": "points/s", "n_gpus": 0, "steps": max(1, min(args.steps, 3)),
             "warmup": min(args.warmup, 1), "ms_per_step": dt * 1e3, "higher_is_better": True,
-            "config": {"workload": "dense suspension: 256 capsules, SH degree 15, grid 256x256x128",
-                       "sample": sample},
+            "config": {"workload": WORKLOAD_LABELS.get(args.config, WORKLOAD_LABELS["c1"]), "sample": sample},
             "cpu_baseline": {"value": val, "unit": "points/s", "cores": cores, "kind": "port", "sample": sample},
             "e2e": {"value": val, "unit": "points/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
         }))
