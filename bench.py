@@ -165,6 +165,7 @@ def run_ours(args):
     import torch
     import torch.distributed as dist
     from suguru_b200.coupling import CouplingStep
+    from suguru_b200 import replicas as R
 
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
@@ -256,11 +257,7 @@ def run_ours(args):
                 launches += cs.last_launch_count()
             torch.cuda.synchronize()
         cs.graph_release()
-        ms = sum(a.elapsed_time(b) for a, b in zip(e0, e1))
-        if world > 1:
-            t = torch.tensor([ms], device=dev)
-            dist.all_reduce(t, op=dist.ReduceOp.MAX)
-            ms = float(t.item())
+        ms = R.max_over_ranks(sum(a.elapsed_time(b) for a, b in zip(e0, e1)))
         return dict(ms_per_step=ms / args.steps, stages=stages,
                     launches=launches, clocks=clk.summary(), s=4 if precision != "fp64" else 8,
                     tile="x".join(map(str, cs_tile_shape(tile))), out=[t.clone() for t in lag + eul])
@@ -343,11 +340,7 @@ def run_ours(args):
     t0 = time.perf_counter()
     for _ in range(args.steps):
         cs_h.step(hu, hv, hw, *hX, lag_out=hlag, eul_out=heul)
-    e2e_s = (time.perf_counter() - t0) / args.steps
-    if world > 1:
-        t = torch.tensor([e2e_s], device=dev)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        e2e_s = float(t.item())
+    e2e_s = R.max_over_ranks((time.perf_counter() - t0) / args.steps)
     cs_h.close()
     nfield = int(np.prod(cs_h.field_shape))
     h2d = 3 * nfield * 4 + 3 * n * 8
