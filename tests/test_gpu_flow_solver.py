@@ -100,3 +100,16 @@ def test_refusals(cuda):
     with pytest.raises(SgError) as e:
         cm.set_flow_params(1.0)
     assert e.value.code == 1
+
+
+def test_one_step_on_non_cubic_cells(cuda):
+    grid = (32, 24, 20, 1 / 16, 1 / 12, 1 / 20)
+    vel, p, f = _state(grid, 8)
+    dt, rep = 1e-3, 0.6
+    ru, rv, rw, rp = O.flow_step(grid, dt, rep, *vel, p, *f)
+    cs = _ctx(grid)
+    cs.set_flow_params(rep)
+    pg = p.copy()
+    u, v, w = cs.flow_step(dt, *vel, pg, *f)
+    for g, r in ((u, ru), (v, rv), (w, rw), (pg, rp)):
+        assert np.abs(g - r).max() <= 1e-10 * np.abs(r).max()
