@@ -103,13 +103,17 @@ __device__ __forceinline__ double momentum_rhs(const FGrid& g, const Fields& F, 
   return d * rep;
 }
 
-__global__ void momentum_rhs_kernel(FGrid g, Fields F, double dt, double rep, double* __restrict__ ru,
-                                    double* __restrict__ rv, double* __restrict__ rw) {
-  const long n = (long)g.itot * g.jtot * g.ktot;
-  const long q = (long)blockIdx.x * blockDim.x + threadIdx.x;
-  if (q >= n) return;
-  int i, j, k;
-  cell_of(g, q, i, j, k);
+// Blocks of 32 x 8 cells in (x, y) at one z level, so that the stencil's y
+// neighbours of a warp are mostly the block's own loads (L1), not L2's.
+__global__ void __launch_bounds__(256) momentum_rhs_kernel(FGrid g, Fields F, double dt, double rep,
+                                                           double* __restrict__ ru, double* __restrict__ rv,
+                                                           double* __restrict__ rw) {
+  const int nbx = (g.itot + 31) / 32;
+  const int i = (int)(blockIdx.x % nbx) * 32 + (int)(threadIdx.x & 31) + 1;
+  const int j = (int)(blockIdx.x / nbx) * 8 + (int)(threadIdx.x >> 5) + 1;
+  const int k = (int)blockIdx.y + 1;
+  if (i > g.itot || j > g.jtot) return;
+  const long q = ((long)(k - 1) * g.jtot + (j - 1)) * g.itot + (i - 1);
   ru[q] = momentum_rhs<0>(g, F, dt, rep, i, j, k);
   rv[q] = momentum_rhs<1>(g, F, dt, rep, i, j, k);
   rw[q] = k == g.ktot ? 0.0 : momentum_rhs<2>(g, F, dt, rep, i, j, k);  // dwdt(i,j,kmax) = 0 (fftuvw.f90:86-92)
@@ -249,7 +253,8 @@ int flow_run(sg_ctx* c, double dt, const double* uo, const double* vo, const dou
   double* rw = c->pois.r;
   Fields F{uo, vo, wo, uoo, voo, woo, p, fx, fy, fz};
   // fftuvw: right-hand sides, then w (initsolver(3)) and u, v (initsolver(2))
-  momentum_rhs_kernel<<<blocks(nreal), 256, 0, st>>>(g, F, dt, s.rep, s.ru, s.rv, rw);
+  const dim3 mgrid((unsigned)(((f.itot + 31) / 32) * ((f.jtot + 7) / 8)), (unsigned)f.ktot);
+  momentum_rhs_kernel<<<mgrid, 256, 0, st>>>(g, F, dt, s.rep, s.ru, s.rv, rw);
   SG_TRY(cudaGetLastError(), "momentum");
   SG_RET(poisson_solve(c, rw, 3, shift, st));
   from_solution_kernel<<<blocks(nreal), 256, 0, st>>>(g, rw, inv_n, w);
