@@ -12,6 +12,7 @@ only the indicator itself is compared:
   - mixed: FP32 inputs and outputs, the same computation in FP64 inside,
     within 1e-6;
   - the sphere's indicator integrates to its volume within 3 %;
+  - host and device memory give the same bits;
   - sg_indicator before sg_set_indicator_params is refused.
 """
 import numpy as np
@@ -96,3 +97,20 @@ def test_refused_before_setup(cuda, case):
     with pytest.raises(SgError) as e:
         cs.indicator(wl.x, wl.y, wl.z, *N, A)
     assert e.value.code == 6
+
+
+def test_device_memory_same_bits(cuda, case):
+    torch = cuda
+    wl, N, A, fy0, fz0, _ = case
+    cs = CouplingStep(wl.grid, wl.degree, wl.radius, precision="fp64")
+    cs.set_indicator_params(**PARAMS)
+    fy, fz = fy0.copy(), fz0.copy()
+    ih, vh = cs.indicator(wl.x, wl.y, wl.z, *N, A, fy=fy, fz=fz)
+    cd = CouplingStep(wl.grid, wl.degree, wl.radius, precision="fp64", mem="device")
+    cd.set_indicator_params(**PARAMS)
+    dev = lambda a: torch.from_numpy(np.ascontiguousarray(a)).cuda()
+    fyd, fzd = dev(fy0), dev(fz0)
+    idv, vdv = cd.indicator(*map(dev, (wl.x, wl.y, wl.z)), *map(dev, N), dev(A), fy=fyd, fz=fzd)
+    torch.cuda.synchronize()
+    for h, d in ((ih, idv), (vh, vdv), (fy, fyd), (fz, fzd)):
+        assert np.array_equal(h, d.cpu().numpy())
