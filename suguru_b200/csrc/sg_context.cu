@@ -431,6 +431,11 @@ int setup(sg_ctx* c) {
   SG_TRY(cudaEventCreateWithFlags(&c->ev_bin, cudaEventDisableTiming), "cudaEventCreate");
   SG_TRY(cudaEventCreateWithFlags(&c->ev_join, cudaEventDisableTiming), "cudaEventCreate");
   if (cfg.mem == SG_MEM_HOST) {
+    SG_TRY(cudaStreamCreateWithFlags(&c->st3, cudaStreamNonBlocking), "cudaStreamCreate");
+    SG_TRY(cudaEventCreateWithFlags(&c->ev_frc, cudaEventDisableTiming), "cudaEventCreate");
+    SG_TRY(cudaEventCreateWithFlags(&c->ev_join3, cudaEventDisableTiming), "cudaEventCreate");
+  }
+  if (cfg.mem == SG_MEM_HOST) {
     SG_TRY(dalloc(c, c->s_u, E * c->nfield), "alloc");
     SG_TRY(dalloc(c, c->s_v, E * c->nfield), "alloc");
     SG_TRY(dalloc(c, c->s_w, E * c->nfield), "alloc");
@@ -566,7 +571,9 @@ int run_step(sg_ctx* c, int what, const void* u, const void* v, const void* w, c
   // interpolation; the spread waits for the binning, and st waits for st2
   // before the step ends.  In host memory the velocity upload on one stream
   // also overlaps the downloads on the other (the spread does not read the
-  // velocity).  A captured graph takes the same fork and join.
+  // velocity).  In host memory the force downloads go to a third stream that
+  // forks after the force stage, so that they run beside the spread.  A
+  // captured graph takes the same forks and joins.
   const bool dual = c->st2 && (what & 1) && (what & 6) && !c->profiling;
   cudaStream_t sB = dual ? c->st2 : c->st;
   if (host) {
@@ -618,8 +625,18 @@ int run_step(sg_ctx* c, int what, const void* u, const void* v, const void* w, c
       c->launches += c->npts > 0 ? 1 : 0;
     }
     if (host) {
+      // beside the spread when one follows: the download direction then has no gap while it runs
+      const bool side = dual && (what & 4) && c->st3;
+      if (side) {
+        SG_TRY(cudaEventRecord(c->ev_frc, c->st), "event");
+        SG_TRY(cudaStreamWaitEvent(c->st3, c->ev_frc, 0), "stream wait");
+      }
       void* outs[7] = {FX, FY, FZ, NX, NY, NZ, A};
-      for (int q = 0; q < 7; ++q) SG_RET(d2h(c, outs[q], L[3 + q], lb));
+      for (int q = 0; q < 7; ++q) SG_RET(d2h(c, outs[q], L[3 + q], lb, side ? c->st3 : nullptr));
+      if (side) {
+        SG_TRY(cudaEventRecord(c->ev_join3, c->st3), "event");
+        c->join3 = true;
+      }
     }
   }
   SG_RET(mark(3));
@@ -638,6 +655,10 @@ int run_step(sg_ctx* c, int what, const void* u, const void* v, const void* w, c
   c->ev_used[2] = (what & 2) != 0;
   c->ev_used[3] = (what & 4) != 0;
   if (dual) SG_TRY(cudaStreamWaitEvent(c->st, c->ev_join, 0), "stream wait");
+  if (c->join3) {
+    SG_TRY(cudaStreamWaitEvent(c->st, c->ev_join3, 0), "stream wait");
+    c->join3 = false;
+  }
   if (what & 2)  // bounded waits of the force kernels
     SG_TRY(cudaMemcpyAsync(c->h_err, c->d_err, sizeof(int), cudaMemcpyDeviceToHost, c->st), "error flag");
   SG_TRY(cudaGetLastError(), "step");
@@ -732,6 +753,12 @@ void sg_destroy(sg_ctx* c) {
   }
   if (c->ev_bin) cudaEventDestroy(c->ev_bin);
   if (c->ev_join) cudaEventDestroy(c->ev_join);
+  if (c->st3) {
+    cudaStreamSynchronize(c->st3);
+    cudaStreamDestroy(c->st3);
+  }
+  if (c->ev_frc) cudaEventDestroy(c->ev_frc);
+  if (c->ev_join3) cudaEventDestroy(c->ev_join3);
   if (c->h_err) cudaFreeHost(c->h_err);
   if (c->h_sur_count) cudaFreeHost(c->h_sur_count);
   delete c;

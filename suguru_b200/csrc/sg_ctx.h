@@ -95,6 +95,10 @@ struct sg_ctx {
   // overlap the force branch's in the other direction; events join the two
   cudaStream_t st2 = nullptr;
   cudaEvent_t ev_bin = nullptr, ev_join = nullptr;
+  // host memory: the force downloads on a third stream, beside the spread
+  cudaStream_t st3 = nullptr;
+  cudaEvent_t ev_frc = nullptr, ev_join3 = nullptr;
+  bool join3 = false;
   std::vector<void*> allocs;
   std::string err;
   int launches = 0;
