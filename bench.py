@@ -456,8 +456,9 @@ def run_coupled(args, rank):
     dt, rep = 0.01 * wl.grid[3], 0.0016  # Rep of param.f90:57
     ind = dict(visc0=1.0 / rep, lam=1.0, thetainc=70.0 * np.pi / 180.0, ta=1160000.0, rep=rep)
     out = {}
-    for name, indicator in (("without_indicator", None), ("with_indicator", ind)):
-        sol = IBSolver(wl, dt, rep, u0, indicator=indicator)
+    for name, indicator, prec in (("without_indicator", None, "fp64"), ("with_indicator", ind, "fp64"),
+                                  ("with_indicator_mixed_ib_step", ind, "mixed")):
+        sol = IBSolver(wl, dt, rep, u0, indicator=indicator, precision=prec)
         sol.run(args.warmup)
         ms = sol.run(args.steps, graph=True)
         out[name] = {"steps_per_s": args.steps / (ms / 1e3), "ms_per_step": ms / args.steps,
@@ -485,7 +486,8 @@ def run_coupled(args, rank):
         "config": {"workload": "256 capsules, L = 15 (524,288 points), grid 256x256x128, Rep = 0.0016, "
                                "dt = 0.01 dx, indicator on (visc0 = 1/Rep, lambda = 1, thetainc = 70 deg, "
                                "ta = 1.16e6)", "points": int(wl.npts)},
-        "with_indicator": head, "without_indicator": out["without_indicator"], "cpu_baseline": cpu}))
+        "with_indicator": head, "without_indicator": out["without_indicator"],
+        "with_indicator_mixed_ib_step": out["with_indicator_mixed_ib_step"], "cpu_baseline": cpu}))
     return 0
 
 

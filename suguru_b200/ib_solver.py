@@ -19,21 +19,33 @@ from .coupling import CouplingStep
 class IBSolver:
     """State on the device (torch tensors): positions X, velocities u (unew),
     uo, uoo, pressure p, the force fields and, with the indicator, indic and
-    visc.  u0: initial (u, v, w) fields meeting bounduvw (numpy, FP64)."""
+    visc.  u0: initial (u, v, w) fields meeting bounduvw (numpy, FP64).
 
-    def __init__(self, wl, dt, rep, u0, walls=(0.0, 0.0), indicator=None, collisions=False, stream=None):
+    precision: "fp64" runs every stage in FP64; "mixed" runs the coupling step
+    (interpolation, membrane force, spread) and Update_Pos on a mixed-precision
+    context, from an FP32 copy of the velocity, and widens its force fields,
+    normals and areas to FP64 for the indicator and the flow solver, which
+    stay FP64."""
+
+    def __init__(self, wl, dt, rep, u0, walls=(0.0, 0.0), indicator=None, collisions=False, stream=None,
+                 precision="fp64"):
         import torch
         self.torch = torch
         self.dt = float(dt)
         self.st = torch.cuda.Stream() if stream is None else stream
         self.cs = CouplingStep(wl.grid, wl.degree, wl.radius, wl.gs, wl.csk, precision="fp64", mem="device",
                                stream=self.st.cuda_stream, async_=True)
+        self.mixed = precision == "mixed"
+        self.cs_ib = self.cs
+        if self.mixed:
+            self.cs_ib = CouplingStep(wl.grid, wl.degree, wl.radius, wl.gs, wl.csk, precision="mixed",
+                                      mem="device", stream=self.st.cuda_stream, async_=True)
         self.cs.set_flow_params(rep, *walls)
         self.indicator = indicator is not None
         if self.indicator:
             self.cs.set_indicator_params(**indicator)
         if collisions:
-            self.cs.set_wall_collisions(in_step=True)
+            self.cs_ib.set_wall_collisions(in_step=True)
         dev = lambda a: torch.from_numpy(np.ascontiguousarray(a, dtype=np.float64)).cuda()
         with torch.cuda.stream(self.st):
             self.X = [dev(a) for a in (wl.x, wl.y, wl.z)]
@@ -45,6 +57,10 @@ class IBSolver:
             self.force = [torch.zeros_like(self.u[0]) for _ in range(3)]
             self.ind = [torch.zeros_like(self.u[0]) for _ in range(2)]
             self.unext = [torch.zeros_like(self.u[0]) for _ in range(3)]
+            if self.mixed:  # the mixed step's own buffers
+                self.u32 = [torch.zeros(self.u[0].shape, dtype=torch.float32, device="cuda") for _ in range(3)]
+                self.lag32 = [torch.zeros(wl.npts, dtype=torch.float32, device="cuda") for _ in range(10)]
+                self.force32 = [torch.zeros_like(self.u32[0]) for _ in range(3)]
         self.stepped = False
 
     def step(self, marks=None):
@@ -58,12 +74,24 @@ class IBSolver:
             for a, b in zip(self.uo, self.u):
                 a.copy_(b)
             mark(0)
-            cs.step(*self.u, *self.X, lag_out=L, eul_out=self.force)
+            if self.mixed:
+                for a, b in zip(self.u32, self.u):
+                    a.copy_(b)
+                self.cs_ib.step(*self.u32, *self.X, lag_out=self.lag32, eul_out=self.force32)
+                for a, b in zip(self.force, self.force32):
+                    a.copy_(b)
+                for q in range(6, 10):  # normals and areas for the indicator
+                    L[q].copy_(self.lag32[q])
+            else:
+                cs.step(*self.u, *self.X, lag_out=L, eul_out=self.force)
             mark(1)
             if self.indicator:
                 cs.indicator(*self.X, L[6], L[7], L[8], L[9], fy=self.force[1], fz=self.force[2], out=self.ind)
             mark(2)
-            cs.update_pos(self.dt, *self.X, L[0], L[1], L[2])
+            if self.mixed:
+                self.cs_ib.update_pos(self.dt, *self.X, *self.lag32[0:3])
+            else:
+                cs.update_pos(self.dt, *self.X, L[0], L[1], L[2])
             mark(3)
             cs.flow_step(self.dt, *self.uo, *self.uoo, self.p, *self.force, out=self.unext)
             mark(4)

@@ -70,3 +70,20 @@ def test_graph_replay_is_bitwise_the_eager_loop(cuda):
         for x, y in zip(sa[k], sb[k]):
             assert np.array_equal(x, y), k
     assert np.array_equal(sa["p"], sb["p"])
+
+
+def test_mixed_coupling_step_within_the_mixed_tolerance(cuda):
+    wl = W.small_config()
+    u0 = list(wl.velocity())
+    O.bounduvw(*u0)
+    dt, rep = 0.01 * wl.grid[3], 0.5
+    a = IBSolver(wl, dt, rep, u0, indicator=IND)
+    a.run(3)
+    b = IBSolver(wl, dt, rep, u0, indicator=IND, precision="mixed")
+    b.run(3, graph=True)
+    sa, sb = a.state(), b.state()
+    size = wl.grid[0] * wl.grid[3]
+    for x, y in zip(sa["X"], sb["X"]):
+        assert np.abs(x - y).max() <= 1e-7 * size
+    for x, y in zip(sa["u"], sb["u"]):
+        assert np.abs(x - y).max() <= 1e-4 * np.abs(x).max()
