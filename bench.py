@@ -161,6 +161,26 @@ def rel_l2_t(a, b):
     return float(d / torch.clamp(torch.linalg.vector_norm(b.double().ravel()), min=1e-300))
 
 
+def legendre_roofline(r, tc_peak, peak_kind):
+    """Tensor-pipe roofline of the Legendre contractions of one step: the
+    algorithmic flops (2 x multiply-adds of the transforms, triangular zeros
+    left out) over the summed CUDA-event time of the contraction launches,
+    against the measured dense bf16 peak divided by the split products per
+    product (3 for BF16x3, 6 for BF16x6: each FP32-accurate product costs that
+    many bf16 products).  issue_frac is the issued tensor-core work (padded
+    tiles x split products) over the bf16 peak: how busy the tensor pipe was."""
+    w, t_ms, terms = r["work"], r["stages"]["contract"], max(r["terms"], 1)
+    if t_ms <= 0 or w["issued_flops"] <= 0:
+        return None
+    achieved = w["flops"] / (t_ms / 1e3) / 1e12
+    peak = tc_peak / terms
+    return {"kernel": "legendre_mma_kernel (tcgen05, BF16x%d), %d launches per step" % (terms, w["launches"]),
+            "bound": "tensor", "flops_per_step": w["flops"], "issued_flops_per_step": w["issued_flops"],
+            "ms_per_step": t_ms, "achieved": achieved, "peak": peak, "unit": "TFLOP/s", "frac": achieved / peak,
+            "peak_kind": "%s bf16 dense / %d (BF16x%d)" % (peak_kind, terms, terms),
+            "issue_frac": w["issued_flops"] / (t_ms / 1e3) / 1e12 / tc_peak}
+
+
 def run_ours(args):
     import torch
     import torch.distributed as dist
@@ -228,7 +248,7 @@ def run_ours(args):
         for _ in range(args.warmup):
             cs.step(*uvw, *X, lag_out=lag, eul_out=eul)
         # stage split of one step (CUDA events between the stages)
-        stages = {k: 0.0 for k in ("bin", "interp", "membrane", "spread")}
+        stages = {k: 0.0 for k in ("bin", "interp", "membrane", "spread", "contract")}
         nst = 3
         for _ in range(nst):
             flush.zero_()
@@ -258,7 +278,8 @@ def run_ours(args):
             torch.cuda.synchronize()
         cs.graph_release()
         ms = R.max_over_ranks(sum(a.elapsed_time(b) for a, b in zip(e0, e1)))
-        return dict(ms_per_step=ms / args.steps, stages=stages,
+        return dict(ms_per_step=ms / args.steps, stages=stages, work=cs.contraction_work(),
+                    terms=cs.legendre_terms(15) if precision != "fp64" else 0,
                     launches=launches, clocks=clk.summary(), s=4 if precision != "fp64" else 8,
                     tile="x".join(map(str, cs_tile_shape(tile))), out=[t.clone() for t in lag + eul])
 
@@ -389,6 +410,7 @@ def run_ours(args):
             "roofline": {"kernel": "spread_kernel<float> (deterministic gather spread)", "bound": "hbm",
                          "achieved": achieved, "peak": hbm_peak, "unit": "GB/s", "frac": achieved / hbm_peak,
                          "peak_kind": peak_kind, "algorithmic_bytes": sbytes, "traffic": traffic},
+            "roofline_legendre": legendre_roofline(head, tc_peak, peak_kind),
             "e2e": {"value": world * n / e2e_s, "unit": "points/s", "h2d_bytes_per_step": h2d,
                     "d2h_bytes_per_step": d2h, "ms_per_step": e2e_s * 1e3},
             "gpu_launches": head["launches"],
@@ -491,17 +513,17 @@ def run_coupled(args, rank):
     return 0
 
 
-def cpu_reference(wl, ncaps, steps, warmup, faithful=True):
+def cpu_reference(wl, ncaps, steps, warmup, faithful=True, cores=None):
     """The CPU FP64 restatement of the reference path (oracle, reference loop
     structure) on a bounded sample of the workload: the first `ncaps` capsules,
-    all host threads."""
+    all host threads (or `cores` of them)."""
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
     import oracle as O
     ncaps = min(ncaps, wl.ncap)
     npts = int(wl.offsets[ncaps])
     u, v, w = wl.velocity()
     x, y, z = wl.x[:npts], wl.y[:npts], wl.z[:npts]
-    cores = os.cpu_count() or 1
+    cores = cores or os.cpu_count() or 1
     for _ in range(warmup):
         O.coupling_step(wl.grid, wl.degree[:ncaps], wl.radius[:ncaps], u, v, w, x, y, z, wl.gs, wl.csk,
                         faithful=faithful, nthreads=cores)
@@ -520,15 +542,15 @@ def main():
         if rank != 0:
             return 0
         wl = workload(args.config)
-        val, cores, npts, dt = cpu_reference(wl, args.cpu_sample_caps, max(1, min(args.steps, 3)),
-                                             min(args.warmup, 1))
+        steps, warmup = max(1, args.steps), max(0, args.warmup)
+        val, cores, npts, dt = cpu_reference(wl, args.cpu_sample_caps, steps, warmup)
         sample = "first %d of %d capsules (%d points), full grid, %d OpenMP threads, FP64" % (
             min(args.cpu_sample_caps, wl.ncap), wl.ncap, npts, cores)
         print(json.dumps({
             "impl": "reference",
             "metric": "Lagrangian pts/s per IB step, mixed+surrogate vs FP64 plain, 1 B200, <=1e-4 err",
-            "value": val, "unit": "points/s", "n_gpus": 0, "steps": max(1, min(args.steps, 3)),
-            "warmup": min(args.warmup, 1), "ms_per_step": dt * 1e3, "higher_is_better": True,
+            "value": val, "unit": "points/s", "n_gpus": 0, "steps": steps,
+            "warmup": warmup, "ms_per_step": dt * 1e3, "higher_is_better": True,
             "config": {"workload": WORKLOAD_LABELS.get(args.config, WORKLOAD_LABELS["c1"]), "sample": sample},
             "cpu_baseline": {"value": val, "unit": "points/s", "cores": cores, "kind": "port", "sample": sample},
             "e2e": {"value": val, "unit": "points/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
@@ -547,6 +569,12 @@ def main():
                                    "sample": "oracle (reference loop structure, FP64) on the first %d capsules "
                                              "(%d points) of the workload, full grid, %.2f s/step"
                                              % (min(args.cpu_sample_caps, wl.ncap), npts, dt)}
+            # the same restatement on one host core, over a smaller sample
+            c1 = max(1, min(8, args.cpu_sample_caps))
+            v1, _, n1, t1 = cpu_reference(wl, c1, 1, 0, cores=1)
+            res["cpu_baseline"]["single_core"] = {
+                "value": v1, "unit": "points/s", "cores": 1,
+                "sample": "first %d capsules (%d points), full grid, one thread, %.2f s/step" % (c1, n1, t1)}
         print(json.dumps(res))
     return 0
 

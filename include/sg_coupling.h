@@ -13,8 +13,8 @@
  *
  * None of those subroutines takes arguments; they act on module globals
  * (common.f90:6-9,67-90).  The functions below take the same arrays as plain
- * pointers, so a thin iso_c_binding shim keeps the Fortran
- * names and packs ap(p)%xfp... into contiguous buffers.
+ * pointers, so a thin iso_c_binding shim keeps the Fortran names and packs
+ * ap(p)%xfp... into contiguous buffers.
  *
  * Conventions
  *  - Eulerian arrays: Fortran (0:i1,0:j1,0:k1), x fastest, i1=itot+1 etc.
@@ -187,9 +187,13 @@ int sg_flow_step(sg_ctx* ctx, double dt, const double* uo, const double* vo, con
  * (npts each, FP64), and the fields fx,fy,fz in the Eulerian layout above.
  * The binning scratch is one fixed array of SG_NOALLOC_SCRATCH_BYTES compiled
  * into the library; every GPU that loads the library holds it until exit.
+ * Output tiles: 32x8x4 cells when itot >= 32 and neither itot mod 32 nor
+ * jtot mod 8 is 1 or 2, else 8x8x4 when neither itot mod 8 nor jtot mod 8 is
+ * 1 or 2; a grid that neither fits returns SG_ERR_ARG.  The tile count is
+ * ceil(itot/TX) ceil(jtot/TY) ceil(ktot/TZ) of the shape chosen.
  * Limits: npts <= SG_NOALLOC_MAX_POINTS and at most SG_NOALLOC_MAX_TILES
- * output tiles (32x8x4 cells each, 8x8x4 when itot < 32); a larger problem
- * returns SG_ERR_TOO_LARGE before doing anything.  The first call on a device
+ * output tiles; a larger problem returns SG_ERR_TOO_LARGE before doing
+ * anything.  The first call on a device
  * looks up the array's device address (cudaGetSymbolAddress), so make that
  * first call before any stream capture.  Work is queued on `stream` (NULL:
  * the default stream) and the call returns without waiting.  All calls share
@@ -332,15 +336,27 @@ int sg_graph_launch(sg_ctx* ctx);
 int sg_graph_release(sg_ctx* ctx);
 
 /* Stage timing with CUDA events on the context stream.  When enabled, each
- * step call records events around its stages; sg_stage_times returns the last
- * step's milliseconds for SG_STAGE_* (bin, interp, membrane, spread). */
+ * step call records events around its stages (and runs them on one stream);
+ * sg_stage_times returns the last step's milliseconds for SG_STAGE_* (bin,
+ * interp, membrane, spread) and, as SG_STAGE_CONTRACT, the summed time of the
+ * Legendre contraction launches inside the membrane stage (tensor-core
+ * launches in mixed precision, CUDA-core launches in FP64). */
 #define SG_STAGE_BIN 0
 #define SG_STAGE_INTERP 1
 #define SG_STAGE_MEMBRANE 2
 #define SG_STAGE_SPREAD 3
-#define SG_NSTAGE 4
+#define SG_STAGE_CONTRACT 4
+#define SG_NSTAGE 5
 int sg_set_profiling(sg_ctx* ctx, int on);
 int sg_stage_times(sg_ctx* ctx, float* ms, int n);
+
+/* Work of one step's Legendre contractions (no counterpart in the reference):
+ * out[0] = algorithmic flops (2 x the multiply-adds of the transforms, with
+ * the products the triangular structure makes zero left out: synthesis terms
+ * of degree n < m and analysis outputs of degree n < m), out[1] = flops the
+ * tensor cores issue (padded tiles times the split products; 0 on the CUDA-core
+ * path), out[2] = contraction launches per step. */
+int sg_contraction_work(const sg_ctx* ctx, double* out);
 
 #ifdef __cplusplus
 }

@@ -25,8 +25,9 @@ def _sources():
 
 
 def _headers_mtime():
+    inc = os.path.join(ROOT, "include")
     hs = [os.path.join(CSRC, f) for f in os.listdir(CSRC) if f.endswith((".h", ".cuh"))]
-    hs.append(os.path.join(ROOT, "include", "sg_coupling.h"))
+    hs += [os.path.join(inc, f) for f in os.listdir(inc) if f.endswith(".h")]
     return max(os.path.getmtime(h) for h in hs if os.path.exists(h))
 
 

@@ -39,12 +39,13 @@ EXPORTS = ["sg_create", "sg_destroy", "sg_last_error", "sg_synchronize", "sg_int
            "sg_surrogate_set_trust", "sg_surrogate_last_counts", "sg_set_point_split", "sg_get_point_split",
            "sg_set_tensor_cores", "sg_set_legendre_terms", "sg_get_legendre_terms", "sg_set_capsule_law",
            "sg_set_legendre_tile_rows", "sg_get_legendre_tile_rows", "sg_set_wall_collisions", "sg_collisions",
-           "sg_set_indicator_params", "sg_indicator", "sg_set_flow_params", "sg_flow_step"]
+           "sg_set_indicator_params", "sg_indicator", "sg_set_flow_params", "sg_flow_step",
+           "sg_contraction_work"]
 # test hooks declared in include/sg_testing.h
 TEST_EXPORTS = ["sg_test_legendre", "sg_test_gemm", "sg_test_mlp_grad"]
 WORKLOAD_EXPORTS = ["sg_prescribed_flow"]  # include/sg_workload.h
 TILE_SHAPES = ((32, 8, 4), (16, 16, 8), (32, 8, 8), (8, 8, 4))
-STAGES = ("bin", "interp", "membrane", "spread")
+STAGES = ("bin", "interp", "membrane", "spread", "contract")
 
 
 class SgError(RuntimeError):
@@ -98,6 +99,7 @@ def lib():
     L.sg_last_launch_count.argtypes = [vp]
     L.sg_set_profiling.argtypes = [vp, ctypes.c_int]
     L.sg_stage_times.argtypes = [vp, ctypes.POINTER(ctypes.c_float), ctypes.c_int]
+    L.sg_contraction_work.argtypes = [vp, dp]
     ip = ctypes.POINTER(ctypes.c_int)
     L.sg_set_tile_shape.argtypes = [vp, ctypes.c_int]
     L.sg_set_point_split.argtypes = [vp, ctypes.c_int]
@@ -515,8 +517,17 @@ class CouplingStep:
     def set_profiling(self, on=True):
         self._check(lib().sg_set_profiling(self._h, int(bool(on))), "sg_set_profiling")
 
+    def contraction_work(self):
+        """Flops of one step's Legendre contractions: algorithmic, issued on the
+        tensor cores (0 on the CUDA-core path), and the number of launches."""
+        out = (ctypes.c_double * 3)()
+        self._check(lib().sg_contraction_work(self._h, out), "sg_contraction_work")
+        return {"flops": out[0], "issued_flops": out[1], "launches": int(out[2])}
+
     def stage_times(self):
-        """Milliseconds of the last step's stages (CUDA events on the context stream)."""
+        """Milliseconds of the last step's stages (CUDA events on the context
+        stream); "contract" is the Legendre contraction launches inside the
+        membrane stage."""
         ms = (ctypes.c_float * len(STAGES))()
         self._check(lib().sg_stage_times(self._h, ms, len(STAGES)), "sg_stage_times")
         return dict(zip(STAGES, list(ms)))

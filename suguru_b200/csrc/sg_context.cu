@@ -203,11 +203,12 @@ int setup(sg_ctx* c) {
   // FP32 spreads on 16 x 16 x 8 tiles (fewer points straddle a tile edge);
   // FP64 keeps 1024-cell tiles for its three-limb shared accumulators
   const int shape = (c->mixed && cfg.itot >= 16 && cfg.jtot >= 16) ? 1 : -1;
-  if (!make_ib_grid(cfg.itot, cfg.jtot, cfg.ktot, cfg.lx, cfg.ly, cfg.lz, c->grid, shape) &&
-      !make_ib_grid(cfg.itot, cfg.jtot, cfg.ktot, cfg.lx, cfg.ly, cfg.lz, c->grid, -1))
+  const unsigned allowed = c->mixed ? kAllTileShapes : kFp64TileShapes;
+  if (!make_ib_grid(cfg.itot, cfg.jtot, cfg.ktot, cfg.lx, cfg.ly, cfg.lz, c->grid, shape, allowed) &&
+      !make_ib_grid(cfg.itot, cfg.jtot, cfg.ktot, cfg.lx, cfg.ly, cfg.lz, c->grid, -1, allowed))
     return fail(c, SG_ERR_CONFIG,
                 "grid out of range: need itot, jtot >= 8, (itot+2)(jtot+2)(ktot+2) < 2^31, and a tile shape whose "
-                "last tile in x and y is not 1 or 2 cells wide");
+                "last tile in x and y is not 1 or 2 cells wide (FP64: 32x8x4 or 8x8x4)");
   const IBGrid& g = c->grid;
   c->nfield = (long long)g.ldi * g.ldj * g.ldk;
   // capsules, offsets, degree groups
@@ -345,6 +346,7 @@ int setup(sg_ctx* c) {
       roots[2].push_back(base + 5);
       if (cfg.surrogate) roots[2].push_back(base + 6);
     }
+    for (int f = 0; f < 3; ++f) c->leg_roots[f] = roots[f];
   }
   // tensor-core operands: the three bf16 parts of every problem's table, and
   // work lists of 128-row tiles of the root problems (FP32 data only)
@@ -466,18 +468,31 @@ int dev_interp(sg_ctx* c, const T* u, const T* v, const T* w, T* U, T* V, T* W, 
   return SG_OK;
 }
 
+// Events around one contraction launch when the step is profiled (the
+// SG_STAGE_CONTRACT time is their sum).
+int con_mark(sg_ctx* c, int end) {
+  if (!c->profiling || c->capturing || !c->ev_con[0][0] || c->ncon >= sg_ctx::kMaxContract) return SG_OK;
+  SG_TRY(cudaEventRecord(c->ev_con[end][c->ncon], c->st), "event");
+  if (end) ++c->ncon;
+  return SG_OK;
+}
+
 template <class T>
 int dev_legendre(sg_ctx* c, int s) {
   if (sizeof(T) == 4 && c->leg_tc) {
     // stages 0, 2, 4 launch the chained products; 1, 3, 5 ran inside them
     if (s % 2) return SG_OK;
     const int f = s / 2;
+    SG_RET(con_mark(c, 0));
     SG_TRY(launch_legendre_mma(c->d_probs, c->d_lwF[f], c->nlwF[f], c->lvF[f], c->leg_parts, c->tmF[f],
                                c->d_err, c->num_sms, c->st),
            "legendre (tensor cores)");
+    SG_RET(con_mark(c, 1));
     c->launches += 1;
   } else {
+    SG_RET(con_mark(c, 0));
     SG_TRY(launch_legendre<T>(c->d_probs, c->d_lw[s], c->nlw[s], c->maxJ[s], c->maxK[s], c->st), "legendre");
+    SG_RET(con_mark(c, 1));
     c->launches += 1;
   }
   return SG_OK;
@@ -487,6 +502,7 @@ template <class T>
 int dev_forces(sg_ctx* c, const double* X, const double* Y, const double* Z, T* FX, T* FY, T* FZ, T* NX, T* NY,
                T* NZ, T* A) {
   const int nc = c->cfg.ncap;
+  c->ncon = 0;
   if (nc == 0) return SG_OK;
   SG_TRY(launch_posfwd<T>(c->d_wpos, c->nwpos, c->d_caps, c->d_groups, X, Y, Z, c->nmax, c->st), "posfwd");
   SG_RET(dev_legendre<T>(c, 0));
@@ -744,8 +760,11 @@ void sg_destroy(sg_ctx* c) {
   if (c->graph) cudaGraphDestroy(c->graph);
   poisson_free(c);
   for (void* p : c->allocs) cudaFree(p);
-  for (int k = 0; k <= SG_NSTAGE; ++k)
+  for (int k = 0; k <= sg_ctx::kMarkStages; ++k)
     if (c->ev[k]) cudaEventDestroy(c->ev[k]);
+  for (int e = 0; e < 2; ++e)
+    for (int k = 0; k < sg_ctx::kMaxContract; ++k)
+      if (c->ev_con[e][k]) cudaEventDestroy(c->ev_con[e][k]);
   if (c->own_stream && c->st) cudaStreamDestroy(c->st);
   if (c->st2) {
     cudaStreamSynchronize(c->st2);
@@ -1023,8 +1042,11 @@ int sg_last_launch_count(const sg_ctx* c) { return c ? c->launches : 0; }
 
 int sg_set_profiling(sg_ctx* c, int on) {
   if (!c) return SG_ERR_ARG;
-  if (on && !c->ev[0])
-    for (int k = 0; k <= SG_NSTAGE; ++k) SG_TRY(cudaEventCreate(&c->ev[k]), "cudaEventCreate");
+  if (on && !c->ev[0]) {
+    for (int k = 0; k <= sg_ctx::kMarkStages; ++k) SG_TRY(cudaEventCreate(&c->ev[k]), "cudaEventCreate");
+    for (int e = 0; e < 2; ++e)
+      for (int k = 0; k < sg_ctx::kMaxContract; ++k) SG_TRY(cudaEventCreate(&c->ev_con[e][k]), "cudaEventCreate");
+  }
   c->profiling = on != 0;
   return SG_OK;
 }
@@ -1039,7 +1061,9 @@ int sg_set_tile_shape(sg_ctx* c, int shape) {
   if (c->graph) return fail(c, SG_ERR_STATE, "release the captured graph before changing the tile shape");
   IBGrid g{};
   const sg_config& cfg = c->cfg;
-  if (!make_ib_grid(cfg.itot, cfg.jtot, cfg.ktot, cfg.lx, cfg.ly, cfg.lz, g, shape) || g.ntiles > c->max_tiles)
+  if (!make_ib_grid(cfg.itot, cfg.jtot, cfg.ktot, cfg.lx, cfg.ly, cfg.lz, g, shape,
+                    c->mixed ? kAllTileShapes : kFp64TileShapes) ||
+      g.ntiles > c->max_tiles)
     return fail(c, SG_ERR_ARG, "tile shape not valid for this grid");
   c->grid = g;
   return SG_OK;
@@ -1233,11 +1257,64 @@ int sg_graph_release(sg_ctx* c) {
 int sg_stage_times(sg_ctx* c, float* ms, int n) {
   if (!c || !ms) return SG_ERR_ARG;
   if (!c->profiling) return fail(c, SG_ERR_STATE, "profiling is off");
-  SG_TRY(cudaEventSynchronize(c->ev[SG_NSTAGE]), "event sync");
-  for (int k = 0; k < n && k < SG_NSTAGE; ++k) {
+  SG_TRY(cudaEventSynchronize(c->ev[sg_ctx::kMarkStages]), "event sync");
+  for (int k = 0; k < n && k < sg_ctx::kMarkStages; ++k) {
     float t = 0.f;
     if (c->ev_used[k]) SG_TRY(cudaEventElapsedTime(&t, c->ev[k], c->ev[k + 1]), "elapsed");
     ms[k] = t;
+  }
+  if (n > SG_STAGE_CONTRACT) {
+    float sum = 0.f;
+    for (int k = 0; k < c->ncon && c->ev_used[SG_STAGE_MEMBRANE]; ++k) {
+      float t = 0.f;
+      SG_TRY(cudaEventElapsedTime(&t, c->ev_con[0][k], c->ev_con[1][k]), "elapsed");
+      sum += t;
+    }
+    ms[SG_STAGE_CONTRACT] = sum;
+  }
+  return SG_OK;
+}
+
+int sg_contraction_work(const sg_ctx* c, double* out) {
+  if (!c || !out) return SG_ERR_ARG;
+  out[0] = out[1] = out[2] = 0.0;
+  if (c->cfg.ncap == 0) return SG_OK;
+  // algorithmic multiply-adds of one problem: rows x sum over m of the
+  // products that are not zero by the triangular structure (synthesis: terms
+  // n >= m of the K = N coefficients; analysis: outputs n >= m of J = N)
+  auto useful = [](const LegProblem& p) {
+    double s = 0;
+    for (int m = 0; m < p.M; ++m) {
+      const int k = p.tri ? std::max(p.K - m, 0) : p.K;
+      const int j = (p.kind == 1 || p.kind == 3) ? std::max(p.J - m, 0) : p.J;
+      s += (double)j * k;
+    }
+    return 2.0 * p.Q * s;
+  };
+  if (c->leg_tc) {
+    for (int f = 0; f < 3; ++f) {
+      const int tm = c->tmF[f];
+      for (int r : c->leg_roots[f]) {
+        const LegProblem& p = c->h_probs[r];
+        const int chain[3] = {r, p.next[0], p.next[0] >= 0 ? p.next[1] : -1};
+        for (int q : chain) {
+          if (q < 0) continue;
+          const LegProblem& pq = c->h_probs[q];
+          out[0] += useful(pq);
+          const double tiles = (double)((pq.Q + tm - 1) / tm);
+          double mk = 0;  // issued K per m (the kernel skips whole K steps below m in a synthesis)
+          for (int m = 0; m < pq.M; ++m) mk += pq.Kp - (pq.tri ? 16 * (m >> 4) : 0);
+          out[1] += 2.0 * tiles * tm * pq.Jp * mk * pq.terms;
+        }
+      }
+    }
+    out[2] = 3;
+  } else {
+    // CUDA-core path: the six stages over every problem of the context
+    // (the tensor-core split problems appended after them are not launched)
+    const size_t nplain = c->h_probs.size() - (c->mixed ? 2 * c->groups.size() : 0);
+    for (size_t i = 0; i < nplain; ++i) out[0] += useful(c->h_probs[i]);
+    out[2] = 6;
   }
   return SG_OK;
 }

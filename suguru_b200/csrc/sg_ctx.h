@@ -103,8 +103,15 @@ struct sg_ctx {
   std::string err;
   int launches = 0;
   bool profiling = false;
-  cudaEvent_t ev[SG_NSTAGE + 1] = {};
-  bool ev_used[SG_NSTAGE] = {};
+  // stage marks: ev[k] .. ev[k+1] bound stage k of SG_STAGE_BIN..SPREAD
+  static constexpr int kMarkStages = 4;
+  cudaEvent_t ev[kMarkStages + 1] = {};
+  bool ev_used[kMarkStages] = {};
+  // the Legendre contraction launches of the last profiled step (start, end)
+  static constexpr int kMaxContract = 8;
+  cudaEvent_t ev_con[2][kMaxContract] = {};
+  int ncon = 0;
+  std::vector<int> leg_roots[3];  // root problems of the three tensor-core launches
   int max_tiles = 0;            // binning arrays are sized for the largest tile count
   bool capturing = false;       // inside sg_graph_capture: no synchronisation, no events
   cudaGraph_t graph = nullptr;  // captured step (device memory mode)

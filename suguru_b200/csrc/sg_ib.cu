@@ -247,14 +247,16 @@ template cudaError_t launch_interp<double>(const IBGrid&, long, const IBWork&, c
 template cudaError_t launch_interp<float>(const IBGrid&, long, const IBWork&, const float*, const float*, const float*,
                                           float*, float*, float*, cudaStream_t);
 
-bool make_ib_grid(int itot, int jtot, int ktot, double lx, double ly, double lz, IBGrid& g, int shape) {
+bool make_ib_grid(int itot, int jtot, int ktot, double lx, double ly, double lz, IBGrid& g, int shape,
+                  unsigned allowed) {
   if (itot < 8 || jtot < 8 || ktot < 1) return false;
   if (shape >= kNumTileShapes) return false;
+  if (shape >= 0 && !((allowed >> shape) & 1u)) return false;
   // a last tile of 1 or 2 cells in a periodic dimension would let a
   // stencil wrap across three tiles
   auto fits = [&](int s) {
     const int rx = itot % kTileShapes[s].TX, ry = jtot % kTileShapes[s].TY;
-    return rx != 1 && rx != 2 && ry != 1 && ry != 2;
+    return ((allowed >> s) & 1u) && rx != 1 && rx != 2 && ry != 1 && ry != 2;
   };
   if (shape < 0) {
     // default tile shape: 32 x 8 x 4 (128-byte rows in x), 8 x 8 x 4 on

@@ -38,8 +38,15 @@ struct IBWork {
 // shape: index into kTileShapes, or -1 for the default of the grid size.
 // A shape whose last tile in x or y would have 1 or 2 cells is rejected (a
 // stencil could then reach three tiles in that periodic dimension); shape -1
-// takes the first shape that fits.
-bool make_ib_grid(int itot, int jtot, int ktot, double lx, double ly, double lz, IBGrid& g, int shape = -1);
+// takes the first shape that fits.  `allowed` is a bit mask of the shapes the
+// caller's spread kernel has (kFp64TileShapes for FP64 spreading, whose
+// shared accumulators hold at most 1024 cells); shapes outside it are never
+// chosen, so a grid that no allowed shape fits is refused here, before any
+// launch.
+constexpr unsigned kAllTileShapes = 0xFu;
+constexpr unsigned kFp64TileShapes = (1u << 0) | (1u << 3);
+bool make_ib_grid(int itot, int jtot, int ktot, double lx, double ly, double lz, IBGrid& g, int shape = -1,
+                  unsigned allowed = kAllTileShapes);
 template <class T>
 cudaError_t launch_bin(const IBGrid& g, long n, const double* X, const double* Y, const double* Z, IBWork& w,
                        cudaStream_t st);

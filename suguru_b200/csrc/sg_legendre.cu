@@ -58,7 +58,15 @@ cudaError_t launch_legendre(const LegProblem* d_probs, const LegWork* d_work, in
                             cudaStream_t st) {
   if (nwork <= 0) return cudaSuccess;
   size_t smem = sizeof(T) * (size_t)(maxJ + LEG_QT) * (maxK + 1);
-  cudaError_t e = cudaFuncSetAttribute(legendre_kernel<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  // the table slice and the row tile must fit the device's opt-in limit
+  // (SH degree 31 in FP64: (3*64 + 32) * 33 * 8 = 59 KB); refuse on the host
+  // rather than launch with a request the device cannot grant
+  int dev = 0, optin = 0;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e == cudaSuccess) e = cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
+  if (e != cudaSuccess) return e;
+  if (smem > (size_t)optin) return cudaErrorInvalidValue;
+  e = cudaFuncSetAttribute(legendre_kernel<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   if (e != cudaSuccess) return e;
   legendre_kernel<T><<<nwork, 256, smem, st>>>(d_probs, d_work, nwork);
   return cudaGetLastError();

@@ -78,7 +78,7 @@ extern "C" int sg_spread_noalloc(int itot, int jtot, int ktot, double lx, double
   if (npts > 0 && (!X || !Y || !Z || !FX || !FY || !FZ || !AREA)) return SG_ERR_ARG;
   if (!(lx > 0 && ly > 0 && lz > 0)) return SG_ERR_ARG;
   IBGrid g{};
-  if (!make_ib_grid(itot, jtot, ktot, lx, ly, lz, g)) return SG_ERR_ARG;
+  if (!make_ib_grid(itot, jtot, ktot, lx, ly, lz, g, -1, kFp64TileShapes)) return SG_ERR_ARG;
   if (npts > SG_NOALLOC_MAX_POINTS || g.ntiles > SG_NOALLOC_MAX_TILES) return SG_ERR_TOO_LARGE;
   void* base = nullptr;
   if (scratch_address(&base) != cudaSuccess) return SG_ERR_CUDA;

@@ -97,3 +97,23 @@ def test_invalid_config_rejected(lib, bad):
 def test_null_arguments(lib):
     assert lib.sg_create(None, None) == 5  # SG_ERR_ARG
     assert lib.sg_interp(None, *([None] * 9)) == 5
+
+
+def test_spread_noalloc_refuses_before_any_device_work(lib):
+    """sg_spread_noalloc checks the grid and the sizes on the host before it
+    looks up its scratch array or queues anything, so on a machine without a
+    GPU these refusals still come back as their own codes (not SG_ERR_CUDA).
+    The field pointers are never dereferenced on these paths."""
+    buf = (ctypes.c_double * 4)()
+    p = ctypes.cast(buf, ctypes.c_void_p)
+    dx = 1.0 / 16
+    f = lib.sg_spread_noalloc
+    # jtot = 25 = 1 mod 8: neither FP64 tile shape (32x8x4, 8x8x4) fits
+    assert f(64, 25, 16, 64 * dx, 25 * dx, 16 * dx, 0, None, None, None, None, None, None, None,
+             p, p, p, None) == 5  # SG_ERR_ARG
+    # 512 x 256 x 256 on 32x8x4 tiles: 16 * 32 * 64 = 32768 tiles > SG_NOALLOC_MAX_TILES
+    assert f(512, 256, 256, 512 * dx, 256 * dx, 256 * dx, 0, None, None, None, None, None, None, None,
+             p, p, p, None) == 7  # SG_ERR_TOO_LARGE
+    # 65,537 points > SG_NOALLOC_MAX_POINTS
+    assert f(64, 48, 40, 4.0, 3.0, 2.5, 65537, p, p, p, p, p, p, p, p, p, p, None) == 7
+

@@ -51,6 +51,24 @@ def test_grid_without_a_valid_tile_shape_is_refused(cuda):
         CouplingStep(grid, wl.degree, wl.radius, precision="fp64")
 
 
+def test_grid_only_a_wide_tile_fits(cuda):
+    # jtot = 25 = 1 mod 8: of the tile shapes only 16x16x8 fits, which the
+    # FP32 spread has and the FP64 spread (at most 1024 cells per tile) has
+    # not.  The FP64 context is refused at set-up with SG_ERR_CONFIG, before
+    # any launch; the mixed context spreads on 16x16x8 tiles and matches the
+    # oracle.
+    grid = (64, 25, 40)
+    wl, f, a, ref = _case(grid, seed=33)
+    with pytest.raises(SgError) as e:
+        CouplingStep(wl.grid, wl.degree, wl.radius, precision="fp64")
+    assert e.value.code == 1  # SG_ERR_CONFIG
+    cs = CouplingStep(wl.grid, wl.degree, wl.radius, precision="mixed")
+    assert cs.tile_shape()[1:] == (16, 16, 8)
+    got = cs.lagr2eulr(wl.x, wl.y, wl.z, *(x.astype(np.float32) for x in f), a.astype(np.float32))
+    for g, r in zip(got, ref):
+        assert rel_l2(g, r) <= 1e-4
+
+
 @pytest.mark.parametrize("precision", ["fp64", "mixed"])
 def test_unaligned_output_fields(cuda, precision):
     torch = cuda

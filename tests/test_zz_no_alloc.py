@@ -59,3 +59,20 @@ def test_spread_noalloc_rejects_oversize(cuda):
     rc = coupling.lib().sg_spread_noalloc(itot, jtot, ktot, itot * dx, jtot * dy, ktot * dz, too_many,
                                           p, p, p, p, p, p, p, p, p, p, None)
     assert rc == 7  # SG_ERR_TOO_LARGE
+
+
+def test_spread_noalloc_rejects_too_many_tiles(cuda):
+    # 512 x 256 x 256 cells on 32x8x4 tiles: 32768 tiles > SG_NOALLOC_MAX_TILES
+    # (16384).  The arrays are real and of full size, although the call
+    # refuses on the host before it queues anything.
+    torch = cuda
+    itot, jtot, ktot, dx = 512, 256, 256, 1.0 / 32
+    fld = [torch.zeros((ktot + 2, jtot + 2, itot + 2), dtype=torch.float64, device="cuda") for _ in range(3)]
+    pts = torch.full((7, 64), 1.0, dtype=torch.float64, device="cuda")
+    p = lambda t: ctypes.c_void_p(t.data_ptr())
+    rc = coupling.lib().sg_spread_noalloc(itot, jtot, ktot, itot * dx, jtot * dx, ktot * dx, 64,
+                                          *[p(pts[q]) for q in range(7)], p(fld[0]), p(fld[1]), p(fld[2]), None)
+    assert rc == 7  # SG_ERR_TOO_LARGE
+    torch.cuda.synchronize()
+    assert all(float(f.abs().max()) == 0.0 for f in fld)  # nothing was written
+
