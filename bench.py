@@ -47,7 +47,7 @@ def parse_args():
                    help="time one path only, no e2e (for profiler captures)")
     p.add_argument("--cpu-sample-caps", type=int, default=64)
     p.add_argument("--no-surrogate", action="store_true", help="skip training and timing the surrogate path")
-    p.add_argument("--tile", type=int, default=None, choices=[0, 1, 2, 3],
+    p.add_argument("--tile", type=int, default=None, choices=[0, 1, 2, 3, 4, 5, 6],
                    help="fixed spreading tile shape (index into TILE_SHAPES; FP64 takes shape 0) instead of the "
                         "autotuner, so that profiler captures see one launch sequence")
     p.add_argument("--legendre-terms", type=int, default=0, choices=[0, 3, 6],
@@ -152,7 +152,8 @@ def spread_bytes(wl, s):
 
 def cs_tile_shape(shape):
     from suguru_b200.coupling import TILE_SHAPES
-    return TILE_SHAPES[shape]
+    t = TILE_SHAPES[shape]
+    return ("rows",) + t[1:] if t[0] == 0 else t
 
 
 def rel_l2_t(a, b):

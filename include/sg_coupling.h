@@ -276,10 +276,12 @@ int sg_last_launch_count(const sg_ctx* ctx);
 
 /* Spreading tile shape (no counterpart in the reference, whose spreading loops
  * over points, interp_spread.f90:817-884).  shape indexes the cell tiles
- * 0: 32x8x4, 1: 16x16x8, 2: 32x8x8, 3: 8x8x4, or -1 for the grid's default;
- * FP64 contexts take shapes 0 and 3 only.  Results do not depend on the shape
- * beyond rounding of the per-tile fixed-point scale.  Not allowed while a
- * graph is captured. */
+ * 0: 32x8x4, 1: 16x16x8, 2: 32x8x8, 3: 8x8x4, 4: whole x rows x 4 x 4,
+ * 5: whole x rows x 8 x 4, 6: 32x16x4, or -1 for the grid's default; FP64 contexts take
+ * shapes 0 and 3 only, and the row tiles need 12 (itot TY TZ + 32) bytes of
+ * shared memory, at most 200 KiB.  Results do not depend on the shape beyond
+ * rounding of the per-tile fixed-point scale.  Not allowed while a graph is
+ * captured.  sg_get_tile_shape reports a row tile's TX as itot. */
 int sg_set_tile_shape(sg_ctx* ctx, int shape);
 int sg_get_tile_shape(const sg_ctx* ctx, int* shape, int* tx, int* ty, int* tz);
 

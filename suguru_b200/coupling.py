@@ -44,7 +44,8 @@ EXPORTS = ["sg_create", "sg_destroy", "sg_last_error", "sg_synchronize", "sg_int
 # test hooks declared in include/sg_testing.h
 TEST_EXPORTS = ["sg_test_legendre", "sg_test_gemm", "sg_test_mlp_grad"]
 WORKLOAD_EXPORTS = ["sg_prescribed_flow"]  # include/sg_workload.h
-TILE_SHAPES = ((32, 8, 4), (16, 16, 8), (32, 8, 8), (8, 8, 4))
+# spreading tile shapes (cells); 0 in x: whole x rows (FP32 only)
+TILE_SHAPES = ((32, 8, 4), (16, 16, 8), (32, 8, 8), (8, 8, 4), (0, 4, 4), (0, 8, 4), (32, 16, 4))
 STAGES = ("bin", "interp", "membrane", "spread", "contract")
 
 

@@ -377,7 +377,8 @@ int setup(sg_ctx* c) {
         std::vector<LegWork> WT;
         for (int r : roots[f])
           for (int m = 0; m < P[r].M; ++m)
-            for (int q0 = 0; q0 < P[r].Q; q0 += tm) WT.push_back(LegWork{r, m, q0});
+            for (int q0 = 0; q0 < P[r].Q; q0 += tm)
+              WT.push_back(LegWork{r, m, q0, P[r].next[0], P[r].next[0] >= 0 ? P[r].next[1] : -1});
         c->nlwT[t][f] = (int)WT.size();
         SG_TRY(upload(c, tmp, WT), "work");
         c->d_lwT[t][f] = (LegWork*)tmp;

@@ -83,46 +83,43 @@ __global__ void bin_points_kernel(IBGrid g, long n, const double* __restrict__ X
 }
 
 // Exclusive scan of tile counts by one block of 1024 threads; starts has
-// ntiles+1 entries.  Chunks of 1024 tiles are read coalesced and scanned with
-// warp shuffles, carrying the running total from chunk to chunk.
+// ntiles+1 entries.  Thread t owns the run of `per` consecutive tiles starting
+// at t * per: it sums its run, the block scans the 1024 run totals (warp
+// shuffles, then one warp over the 32 warp totals), and each thread writes its
+// run's starts from its offset -- one pass over the counts, two barriers.
 __global__ void __launch_bounds__(1024) scan_counts_kernel(int ntiles, const int* __restrict__ counts,
                                                            int* __restrict__ starts, int* __restrict__ fill) {
   __shared__ int warp_sum[32];
-  __shared__ int carry;
   const int t = threadIdx.x, lane = t & 31, warp = t >> 5;
-  if (t == 0) carry = 0;
+  const int per = (ntiles + 1023) / 1024;
+  const int b0 = t * per, b1 = min(b0 + per, ntiles);
+  int run = 0;
+  for (int i = b0; i < b1; ++i) run += counts[i];
+  int x = run;  // inclusive scan of the run totals within the warp
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    const int y = __shfl_up_sync(0xffffffffu, x, o);
+    if (lane >= o) x += y;
+  }
+  if (lane == 31) warp_sum[warp] = x;
   __syncthreads();
-  for (int base = 0; base < ntiles; base += 1024) {
-    const int i = base + t;
-    const int v = i < ntiles ? counts[i] : 0;
-    int x = v;  // inclusive scan within the warp
+  if (warp == 0) {
+    int w = warp_sum[lane];
 #pragma unroll
     for (int o = 1; o < 32; o <<= 1) {
-      const int y = __shfl_up_sync(0xffffffffu, x, o);
-      if (lane >= o) x += y;
+      const int y = __shfl_up_sync(0xffffffffu, w, o);
+      if (lane >= o) w += y;
     }
-    if (lane == 31) warp_sum[warp] = x;
-    __syncthreads();
-    if (warp == 0) {
-      int w = warp_sum[lane];
-#pragma unroll
-      for (int o = 1; o < 32; o <<= 1) {
-        const int y = __shfl_up_sync(0xffffffffu, w, o);
-        if (lane >= o) w += y;
-      }
-      warp_sum[lane] = w;
-    }
-    __syncthreads();
-    const int excl = carry + (warp > 0 ? warp_sum[warp - 1] : 0) + x - v;
-    if (i < ntiles) {
-      starts[i] = excl;
-      fill[i] = 0;
-    }
-    __syncthreads();  // every thread has read carry and warp_sum
-    if (t == 1023) carry = excl + v;
-    __syncthreads();
+    warp_sum[lane] = w;
   }
-  if (t == 0) starts[ntiles] = carry;
+  __syncthreads();
+  int excl = (warp > 0 ? warp_sum[warp - 1] : 0) + x - run;
+  for (int i = b0; i < b1; ++i) {
+    starts[i] = excl;
+    fill[i] = 0;
+    excl += counts[i];
+  }
+  if (t == 1023) starts[ntiles] = warp_sum[31];
 }
 
 template <class T>
@@ -255,7 +252,9 @@ bool make_ib_grid(int itot, int jtot, int ktot, double lx, double ly, double lz,
   // a last tile of 1 or 2 cells in a periodic dimension would let a
   // stencil wrap across three tiles
   auto fits = [&](int s) {
-    const int rx = itot % kTileShapes[s].TX, ry = jtot % kTileShapes[s].TY;
+    const TileShape& t = kTileShapes[s];
+    if (t.TX == 0 && 4ull * 3 * ((unsigned long long)itot * t.TY * t.TZ + 32) > kRowTileSmemMax) return false;
+    const int rx = t.TX ? itot % t.TX : 0, ry = jtot % t.TY;
     return ((allowed >> s) & 1u) && rx != 1 && rx != 2 && ry != 1 && ry != 2;
   };
   if (shape < 0) {
@@ -283,7 +282,7 @@ bool make_ib_grid(int itot, int jtot, int ktot, double lx, double ly, double lz,
   g.dzi = 1.0 / dz;
   g.dvi = 1.0 / (dx * dy * dz);
   g.shape = shape;
-  g.TX = kTileShapes[shape].TX;
+  g.TX = kTileShapes[shape].TX ? kTileShapes[shape].TX : itot;
   g.TY = kTileShapes[shape].TY;
   g.TZ = kTileShapes[shape].TZ;
   g.ntx = (itot + g.TX - 1) / g.TX;

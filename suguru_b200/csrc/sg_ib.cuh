@@ -18,11 +18,15 @@ namespace sg {
 
 // Spreading tile shapes (cells).  FP64 spreading takes shapes of at most 1024
 // cells (three 32-bit limbs per cell and component in static shared memory).
+// TX = 0 stands for whole x rows (TX = itot): FP32 row tiles, whose fixed-point
+// sums take 3 (itot TY TZ + 32) words of dynamic shared memory, at most
+// kRowTileSmemMax bytes.
 struct TileShape {
   int TX, TY, TZ;
 };
-constexpr TileShape kTileShapes[] = {{32, 8, 4}, {16, 16, 8}, {32, 8, 8}, {8, 8, 4}};
-constexpr int kNumTileShapes = 4;
+constexpr TileShape kTileShapes[] = {{32, 8, 4}, {16, 16, 8}, {32, 8, 8}, {8, 8, 4}, {0, 4, 4}, {0, 8, 4}, {32, 16, 4}};
+constexpr int kNumTileShapes = 7;
+constexpr unsigned kRowTileSmemMax = 200u * 1024u;
 
 struct IBGrid {
   int itot, jtot, ktot;  // interior cells (imax, jmax, kmax)

@@ -43,7 +43,7 @@ struct IBWork {
 // shared accumulators hold at most 1024 cells); shapes outside it are never
 // chosen, so a grid that no allowed shape fits is refused here, before any
 // launch.
-constexpr unsigned kAllTileShapes = 0xFu;
+constexpr unsigned kAllTileShapes = 0x7Fu;
 constexpr unsigned kFp64TileShapes = (1u << 0) | (1u << 3);
 bool make_ib_grid(int itot, int jtot, int ktot, double lx, double ly, double lz, IBGrid& g, int shape = -1,
                   unsigned allowed = kAllTileShapes);
@@ -122,6 +122,10 @@ struct LegProblem {
 
 struct LegWork {  // one tile of a problem
   int prob, m, q0;
+  // tensor-core path: the root's chained problems (its next[0], then next[1]
+  // after a next[0]), -1 for none -- carried here so that a CTA can fetch the
+  // whole chain at once
+  int lvl1 = -1, lvl2 = -1;
 };
 
 template <class T>

@@ -33,6 +33,8 @@
 // MMAs and commits them to an mbarrier; all threads wait with a bounded spin
 // (error flag, no trap, on timeout), read the accumulator with tcgen05.ld and
 // store the rows.
+#include <algorithm>
+
 #include "sg_common.cuh"
 #include "sg_kernels.h"
 #include "sg_umma.cuh"
@@ -76,9 +78,10 @@ __device__ __forceinline__ void store_split(const float* x, int np, const Operan
 }
 
 // One thread issues the split products of every K step of 16 (largest terms
-// first), then commits.  bt: the level's table region; tm: the tile's rows.
+// first) into the accumulator at tmem.  bt: the level's table region; tm: the
+// tile's rows.  The caller commits.
 __device__ __forceinline__ void issue_mma(const LegProblem& P, int m, int tm, uint32_t tmem, const Operands& op,
-                                          const uint16_t* bt, uint64_t* bar) {
+                                          const uint16_t* bt) {
   const uint32_t idesc = idesc_bf16(tm, P.Jp);
   const uint32_t lbo = 128, sbo = (uint32_t)P.Kp * 16;
   const uint32_t pb = (uint32_t)(P.Jp * P.Kp) * 2u;  // bytes per table part
@@ -99,7 +102,6 @@ __device__ __forceinline__ void issue_mma(const LegProblem& P, int m, int tm, ui
       mma_bf16(tmem, desc(a1 + o, lbo, sbo), desc(b1 + o, lbo, sbo), idesc, 1);
     }
   }
-  commit(bar);
 }
 
 }  // namespace
@@ -107,27 +109,50 @@ __device__ __forceinline__ void issue_mma(const LegProblem& P, int m, int tm, ui
 // Work items name root problems; a root's next[] problems take its output
 // rows as their A operand for the same (m, tile) and run in the same CTA: the
 // accumulator is read once from TMEM, written to global memory, and split into
-// the next product's bf16 operand parts in shared memory, so the data
-// never leaves the SM between the two contractions.
+// the next product's bf16 operand parts in shared memory, so the data never
+// leaves the SM between the two contractions.  The two chained products share
+// that operand, so they are issued together (level 1 at TMEM column 0, level 2
+// at column off2) under one commit, and read back in one epilogue.
 // A chain runs in its root's mode (one degree group: the same mode throughout).
-// Tiles of TM = 128 data rows (M = 128: row r in TMEM lane r, so warp w
-// holds rows 32w..32w+31) or TM = 64 (M = 64: row r in lane (r mod 16) +
-// 32 floor(r / 16) -- the first half of every warp's 32-lane quadrant -- so
-// warp w holds rows 16w..16w+15 in its lanes 0..15); 64-row tiles double the
-// work items of a launch whose 128-row tiles would leave SMs idle.
-// smem (bf16): nparts A parts of TM x lv.a_kp, then for each chain level l a
-// table region of nparts x lv.jp[l] x lv.kp[l]; nparts = 3 when any problem of
-// the launch is BF16x6, else 2.  At the start of a work item one thread issues
-// the bulk copies of every level's table (each on its own mbarrier), so they
-// overlap the staging of the data rows and the earlier products.
+// Tiles of TM = 128 data rows (M = 128: row r in TMEM lane r) or TM = 64
+// (M = 64: row r in lane (r mod 16) + 32 floor(r / 16) -- the first half of
+// every 32-lane quadrant).
+//
+// CTAs of kLegThreads = 256 threads (8 warps), up to three per SM, so that
+// every work item of a launch is resident at once (the items are short
+// chains of dependent phases; their latencies overlap across CTAs).  Warp w
+// reads TMEM lane quadrant w % 4 (the hardware ties a warp to the quadrant of
+// its index mod 4) and column group w / 4 of every 32-column slab, so the two
+// warps of a quadrant read a row's columns in parallel; the slab goes through
+// shared memory (s_slab, row stride 33 words) and every warp then writes
+// whole rows of it to global memory as contiguous runs.  The data rows are
+// staged by all threads in coalesced 32-byte pieces.
+// smem (bf16, dynamic): nparts A parts of TM x lv.a_kp, then for each chain
+// level l a table region of nparts x lv.jp[l] x lv.kp[l]; nparts = 3 when any
+// problem of the launch is BF16x6, else 2.  At the start of a work item one
+// thread issues the bulk copies of every level's table (each on its own
+// mbarrier), so they overlap the staging of the data rows and the root product.
+constexpr int kLegThreads = 256;
+constexpr int kLegGroups = kLegThreads / 128;  // warps per TMEM lane quadrant
+constexpr int kSlab = 16 * kLegGroups;         // columns per slab
+constexpr int kLegPerSm = 3;                   // CTAs per SM (registers: launch bounds)
+
 template <int TM>
-__global__ void __launch_bounds__(128) legendre_mma_kernel(const LegProblem* __restrict__ probs,
-                                                           const LegWork* __restrict__ work, int nwork, LegLevels lv,
-                                                           int nparts, int tmem_cols, int* __restrict__ err) {
+__global__ void __launch_bounds__(kLegThreads, kLegPerSm) legendre_mma_kernel(const LegProblem* __restrict__ probs,
+                                                                    const LegWork* __restrict__ work, int nwork,
+                                                                    LegLevels lv, int nparts, int tmem_cols,
+                                                                    int off2, int* __restrict__ err) {
   extern __shared__ __align__(128) unsigned char smem_raw[];
   __shared__ __align__(8) uint64_t s_bar;
   __shared__ __align__(8) uint64_t s_tbar[3];
   __shared__ uint32_t s_tmem;
+  // the work item's chain of problems, copied from global memory by the whole
+  // CTA in one round of independent loads instead of field by field
+  __shared__ __align__(16) LegProblem s_p[3];
+  // element offsets of the tile's rows in the root's A (staging) and in a
+  // level's D (epilogue), -1 past the problem's last row
+  __shared__ long long s_roff[2][TM];
+  __shared__ float s_slab[TM * (kSlab + 1)];
   Operands op;
   {
     uint16_t* p = (uint16_t*)smem_raw;
@@ -142,10 +167,9 @@ __global__ void __launch_bounds__(128) legendre_mma_kernel(const LegProblem* __r
     }
   }
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  const int quad = warp & 3, cgrp = warp >> 2;  // TMEM lane quadrant, column group
 
-  if (warp == 0) {
-    tmem_alloc(&s_tmem, (uint32_t)tmem_cols);
-  }
+  if (warp == 0) tmem_alloc(&s_tmem, (uint32_t)tmem_cols);
   if (tid == 0) {
     mbar_init(&s_bar, 1);
     for (int l = 0; l < 3; ++l) mbar_init(&s_tbar[l], 1);
@@ -154,84 +178,106 @@ __global__ void __launch_bounds__(128) legendre_mma_kernel(const LegProblem* __r
   __syncthreads();
   fence_after();
   const uint32_t tmem = s_tmem;
-  uint32_t phase = 0;             // MMA commits
-  uint32_t tphase[3] = {0, 0, 0};  // table copies, per level (a level completes one phase per item using it)
+  uint32_t phase = 0;              // MMA commits
+  uint32_t tphase[3] = {0, 0, 0};  // table copies, per level (one phase per item that uses the level)
   int pending = 0;                 // levels whose copy was issued and not yet waited for (thread 0)
   bool ok = true;
+  // this thread's TMEM row: quadrant quad, lane -> tile row (TM = 64: lanes 0-15 only)
+  const bool lane_row = TM == 128 || lane < 16;
+  const int q = TM == 128 ? quad * 32 + lane : quad * 16 + lane;
 
+  constexpr int PW = (int)(sizeof(LegProblem) / sizeof(int));
   for (int it = blockIdx.x; it < nwork && ok; it += gridDim.x) {
     const LegWork wk = work[it];
     const int m = wk.m, q0 = wk.q0;
-    int pid = wk.prob;
-    const LegProblem& R = probs[pid];
+    // the chain: level 0 the root, 1 its next[0], 2 its next[1] (only after a level 1)
+    const int lvl[3] = {wk.prob, wk.lvl1, wk.lvl1 >= 0 ? wk.lvl2 : -1};
+    for (int l = 0; l < 3; ++l)
+      if (lvl[l] >= 0)
+        for (int i = tid; i < PW; i += kLegThreads) ((int*)&s_p[l])[i] = ((const int*)&probs[lvl[l]])[i];
+    __syncthreads();
+    const LegProblem& R = s_p[0];
     const int nq = min(TM, R.Q - q0);
     const int np = parts_of(R);
-    // the chain: level 0 the root, 1 its next[0], 2 its next[1] (only after a level 1)
-    const int chain[3] = {pid, R.next[0], R.next[0] >= 0 ? R.next[1] : -1};
-    bool fits = np <= nparts;
+    bool fits = np <= nparts && (R.Kp >> 3) <= 8 && (lvl[2] < 0 || off2 >= lv.jp[1]);
     for (int l = 0; l < 3; ++l)
-      if (chain[l] >= 0) {
-        const LegProblem& P = probs[chain[l]];
+      if (lvl[l] >= 0) {
+        const LegProblem& P = s_p[l];
         fits = fits && parts_of(P) == np && P.Jp <= lv.jp[l] && P.Kp <= lv.kp[l] && P.Kp <= lv.a_kp;
       }
     if (!fits) {  // the launch's shared memory was sized for other problems (uniform per CTA)
       if (tid == 0) atomicExch(err, 2);
+      __syncthreads();  // every thread has read s_p before the next item overwrites it
       continue;
     }
     if (tid == 0) {
       fence_async_smem();  // earlier generic accesses of the regions before the async copies
       for (int l = 0; l < 3; ++l)
-        if (chain[l] >= 0) {
-          fetch_table(probs[chain[l]], m, op.b[l], &s_tbar[l]);
+        if (lvl[l] >= 0) {
+          fetch_table(s_p[l], m, op.b[l], &s_tbar[l]);
           pending |= 1 << l;
         }
     }
-    // ---- data rows of the root: FP32 -> bf16 parts.  Thread tid stages
-    // row tid % TM of the tile, every (128/TM)-th core-matrix row of 8 values
-    // starting at tid / TM; all of its loads (up to 8 core-matrix rows) are
-    // issued before any is split and stored, so their latencies overlap.
-    {
-      constexpr int NPH = 128 / TM;
-      const int K = R.K, KC = R.Kp >> 3, q = tid % TM, ph = tid / TM;
-      const float* row = nullptr;
-      if (q < nq) {
-        const int qq = q0 + q, c = qq / R.rpc, r = qq - c * R.rpc;
-        row = (const float*)R.A + (long long)c * R.sAc + (long long)r * R.sAr + (long long)m * R.sAm;
+    // ---- data rows of the root: FP32 -> bf16 parts.  Row offsets first (one
+    // division per row), then the rows are read in coalesced pieces: with KC =
+    // Kp/8 chunks of 8 values per row, thread t takes chunk t % KC of rows
+    // t / KC + u (kLegThreads / KC); all of a thread's loads are issued before
+    // any is split.
+    if (tid < TM) {
+      long long o = -1;
+      if (tid < nq) {
+        const int qq = q0 + tid, c = qq / R.rpc, r = qq - c * R.rpc;
+        o = (long long)c * R.sAc + (long long)r * R.sAr + (long long)m * R.sAm;
       }
-      for (int kc0 = ph; kc0 < KC; kc0 += 8 * NPH) {
-        float x[8][8];
+      s_roff[0][tid] = o;
+    }
+    __syncthreads();
+    {
+      const float* Ab = (const float*)R.A;
+      const int K = R.K, KC = R.Kp >> 3, rpp = kLegThreads / KC, kc = tid % KC, r0 = tid / KC, k0 = kc << 3;
+      constexpr int NU = 128 * 8 / kLegThreads;  // passes: KC <= 8 and TM <= 128
+      float x[NU][8];
 #pragma unroll
-        for (int u = 0; u < 8; ++u) {
-          const int kc = kc0 + u * NPH, k0 = kc << 3;
-          if (row && kc < KC && R.vecA && k0 + 8 <= K) {
-            const float4 a = *(const float4*)(row + k0), b = *(const float4*)(row + k0 + 4);
-            x[u][0] = a.x; x[u][1] = a.y; x[u][2] = a.z; x[u][3] = a.w;
-            x[u][4] = b.x; x[u][5] = b.y; x[u][6] = b.z; x[u][7] = b.w;
-          } else {
+      for (int u = 0; u < NU; ++u) {
+        const int row = r0 + u * rpp;
+        const long long o = (r0 < rpp && row < TM) ? s_roff[0][row] : -1;
+        if (o >= 0 && R.vecA && k0 + 8 <= K) {
+          const float4 a = *(const float4*)(Ab + o + k0), b = *(const float4*)(Ab + o + k0 + 4);
+          x[u][0] = a.x; x[u][1] = a.y; x[u][2] = a.z; x[u][3] = a.w;
+          x[u][4] = b.x; x[u][5] = b.y; x[u][6] = b.z; x[u][7] = b.w;
+        } else {
 #pragma unroll
-            for (int i = 0; i < 8; ++i) x[u][i] = (row && kc < KC && k0 + i < K) ? row[k0 + i] : 0.f;
-          }
+          for (int i = 0; i < 8; ++i) x[u][i] = (o >= 0 && k0 + i < K) ? Ab[o + k0 + i] : 0.f;
         }
+      }
 #pragma unroll
-        for (int u = 0; u < 8; ++u)
-          if (kc0 + u * NPH < KC) store_split(x[u], np, op, cm_offset(q, kc0 + u * NPH, KC));
+      for (int u = 0; u < NU; ++u) {
+        const int row = r0 + u * rpp;
+        if (r0 < rpp && row < TM) store_split(x[u], np, op, cm_offset(row, kc, KC));
       }
     }
-    // ---- the root, then its chained products: one MMA group per problem
-    for (int level = 0; level < 3 && ok; ++level) {
-      const LegProblem& P = probs[pid];
+    // ---- stage 0: the root; stage 1: its chained products (levels 1 and 2,
+    // one commit)
+    const bool chained = lvl[1] >= 0;
+    for (int stage = 0; stage < 2 && ok; ++stage) {
+      if (stage == 1 && !chained) break;
       fence_async_smem();  // generic-proxy smem writes -> visible to the tensor core
       fence_before();
       __syncthreads();
       fence_after();
       if (tid == 0) {
-        // the level's table has landed (bounded wait; on timeout the MMA wait
+        // each level's table has landed (bounded wait; on timeout the MMA wait
         // below runs out too and the CTA leaves with the error flag set)
-        const bool landed = mbar_wait(&s_tbar[level], tphase[level]);
-        pending &= ~(1 << level);
-        tphase[level] ^= 1u;
+        bool landed = true;
+        for (int l = stage == 0 ? 0 : 1; l <= (stage == 0 ? 0 : 2); ++l) {
+          if (lvl[l] < 0) continue;
+          landed = mbar_wait(&s_tbar[l], tphase[l]) && landed;
+          pending &= ~(1 << l);
+          tphase[l] ^= 1u;
+          if (landed) issue_mma(s_p[l], m, TM, tmem + (uint32_t)(l == 2 ? off2 : 0), op, op.b[l]);
+        }
         if (landed)
-          issue_mma(P, m, TM, tmem, op, op.b[level], &s_bar);
+          commit(&s_bar);
         else
           atomicExch(err, 1);
       }
@@ -246,60 +292,59 @@ __global__ void __launch_bounds__(128) legendre_mma_kernel(const LegProblem* __r
       }
       phase ^= 1u;
       fence_after();
-      // chained products of the root take its rows as their A operand
-      const bool chain = level == 0 && P.next[0] >= 0;
-      const int KC2 = P.Jp >> 3;  // next K padded = this J padded
-      // ---- epilogue: warp w holds rows 32w..32w+31 of a 128-row tile, rows
-      // 16w..16w+15 of a 64-row tile (its lanes 0..15)
-      {
-        const bool lane_row = TM == 128 || lane < 16;
-        const int q = TM == 128 ? warp * 32 + lane : warp * 16 + lane;
-        const int J = P.J;
-        float* drow = nullptr;
-        if (lane_row && q < nq) {
-          const int qq = q0 + q, c = qq / P.rpc, r = qq - c * P.rpc;
-          drow = (float*)P.D + (long long)c * P.sDc + (long long)r * P.sDr + (long long)m * P.sDm;
+      // ---- epilogue of each level of this stage
+      for (int l = stage == 0 ? 0 : 1; l <= (stage == 0 ? 0 : 2); ++l) {
+        if (lvl[l] < 0) continue;
+        const LegProblem& P = s_p[l];
+        const bool split_next = stage == 0 && chained;  // root: its rows become the next A operand
+        const int J = P.J, KC2 = P.Jp >> 3;
+        const uint32_t cbase = l == 2 ? (uint32_t)off2 : 0u;
+        if (cgrp == 0 && lane_row) {
+          long long o = -1;
+          if (q < nq) {
+            const int qq = q0 + q, c = qq / P.rpc, r = qq - c * P.rpc;
+            o = (long long)c * P.sDc + (long long)r * P.sDr + (long long)m * P.sDm;
+          }
+          s_roff[1][q] = o;
         }
-        for (int j0 = 0; j0 < P.Jp; j0 += 16) {
-          float v[16];
-          tmem_ld16(tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)j0, v);
-          if (drow) {
-            if (P.vecD && j0 + 16 <= J) {
+        float* Db = (float*)P.D;
+        for (int jc = 0; jc < P.Jp; jc += kSlab) {
+          const int j0 = jc + 16 * cgrp;
+          const bool mine = j0 < P.Jp;  // uniform per warp
+          uint32_t raw[16];
+          if (mine) {
+            tmem_ld16_nowait(tmem + ((uint32_t)(quad * 32) << 16) + cbase + (uint32_t)j0, raw);
+            tmem_wait_ld();
+            if (lane_row) {
+              float v[16];
 #pragma unroll
-              for (int i = 0; i < 16; i += 4)
-                *(float4*)(drow + j0 + i) = make_float4(v[i], v[i + 1], v[i + 2], v[i + 3]);
-            } else {
+              for (int i = 0; i < 16; ++i) {
+                v[i] = __uint_as_float(raw[i]);
+                s_slab[q * (kSlab + 1) + 16 * cgrp + i] = v[i];
+              }
+              if (split_next) {
 #pragma unroll
-              for (int i = 0; i < 16; ++i)
-                if (j0 + i < J) drow[j0 + i] = v[i];
+                for (int h = 0; h < 2; ++h) {
+                  float xs[8];
+#pragma unroll
+                  for (int i = 0; i < 8; ++i) xs[i] = (j0 + 8 * h + i < J && q < nq) ? v[8 * h + i] : 0.f;
+                  store_split(xs, np, op, cm_offset(q, (j0 >> 3) + h, KC2));
+                }
+              }
             }
           }
-          if (chain && lane_row) {  // root MMA is complete: its A tile is free for the next operand
+          __syncthreads();  // the slab and the row offsets are complete
+          const int ncol = min(kSlab, J - jc);
+          for (int rr = warp; rr < TM; rr += kLegThreads / 32) {
+            const long long o = s_roff[1][rr];
+            if (o >= 0)
 #pragma unroll
-            for (int h = 0; h < 2; ++h) {
-              float x[8];
-#pragma unroll
-              for (int i = 0; i < 8; ++i) x[i] = (j0 + 8 * h + i < J && q < nq) ? v[8 * h + i] : 0.f;
-              store_split(x, np, op, cm_offset(q, (j0 >> 3) + h, KC2));
-            }
+              for (int c0 = 0; c0 < kSlab; c0 += 32)
+                if (c0 + lane < ncol) Db[o + jc + c0 + lane] = s_slab[rr * (kSlab + 1) + c0 + lane];
           }
+          __syncthreads();  // the slab is consumed before the next one is written
         }
       }
-      if (level == 0) {
-        if (!chain) break;
-        pid = P.next[0];
-      } else if (level == 1) {
-        // the second chained product of the root (same A operand), if any
-        const int n2 = probs[wk.prob].next[1];
-        if (n2 < 0) break;
-        pid = n2;
-      } else {
-        break;
-      }
-      // all TMEM reads and operand writes are done before the next MMA
-      fence_before();
-      __syncthreads();
-      fence_after();
     }
     fence_before();
     __syncthreads();  // TMEM reads and smem operands done before the next tile
@@ -330,35 +375,38 @@ cudaError_t launch_legendre_mma(const LegProblem* d_probs, const LegWork* d_work
                                 int nparts, int tm, int* d_err, int num_sms, cudaStream_t st) {
   if (nwork <= 0) return cudaSuccess;
   if (tm != 64 && tm != 128) return cudaErrorInvalidValue;
-  int maxJp = 0;
-  for (int l = 0; l < 3; ++l) {
+  for (int l = 0; l < 3; ++l)
     if (lv.jp[l] < 0 || lv.jp[l] > 256 || (lv.jp[l] & 15) || lv.kp[l] < 0 || (lv.kp[l] & 15))
       return cudaErrorInvalidValue;
-    maxJp = lv.jp[l] > maxJp ? lv.jp[l] : maxJp;
-  }
-  if (lv.jp[0] < 16 || lv.kp[0] < 16 || lv.a_kp < 16 || (lv.a_kp & 15)) return cudaErrorInvalidValue;
+  if (lv.jp[0] < 16 || lv.kp[0] < 16 || lv.a_kp < 16 || (lv.a_kp & 15) || lv.a_kp > 64) return cudaErrorInvalidValue;
   if (nparts != 2 && nparts != 3) return cudaErrorInvalidValue;
-  // TMEM columns: a power of two >= 32 covering N = Jp; CTAs per SM limited
-  // (through shared memory) so that their allocations always fit in 512 columns
+  // TMEM columns: the root's accumulator at column 0; the chained products at
+  // columns 0 (level 1) and off2 (level 2, 32-column aligned) at the same
+  // time; a power of two >= 32 covering both
+  const int off2 = (lv.jp[1] + 31) / 32 * 32;
+  const int need = std::max(lv.jp[0], off2 + lv.jp[2]);
   int cols = 32;
-  while (cols < maxJp) cols <<= 1;
-  const int per_sm = 512 / cols < 4 ? 512 / cols : 4;
-  size_t smem = legendre_mma_smem(lv, nparts, tm);
-  // (per_sm + 1) CTAs of this size exceed the SM's 228 KB of shared memory
-  const size_t floor_smem = (size_t)(228 * 1024) / (size_t)(per_sm + 1);
-  if (smem < floor_smem) smem = floor_smem;
-  if (smem > (size_t)227 * 1024) return cudaErrorInvalidValue;
+  while (cols < need) cols <<= 1;
+  if (cols > 512) return cudaErrorInvalidValue;
+  const size_t smem = legendre_mma_smem(lv, nparts, tm);
+  cudaFuncAttributes fa{};
+  cudaError_t e = tm == 64 ? cudaFuncGetAttributes(&fa, legendre_mma_kernel<64>)
+                           : cudaFuncGetAttributes(&fa, legendre_mma_kernel<128>);
+  if (e != cudaSuccess) return e;
+  if (smem + fa.sharedSizeBytes > (size_t)227 * 1024) return cudaErrorInvalidValue;
+  // up to kLegPerSm CTAs per SM, fewer when their TMEM allocations would not
+  // all fit in the SM's 512 columns (a CTA that cannot allocate would wait)
+  const int per_sm = std::min(kLegPerSm, 512 / cols);
   const int grid = nwork < num_sms * per_sm ? nwork : num_sms * per_sm;
   if (tm == 64) {
-    cudaError_t e = cudaFuncSetAttribute(legendre_mma_kernel<64>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                         (int)smem);
+    e = cudaFuncSetAttribute(legendre_mma_kernel<64>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e != cudaSuccess) return e;
-    legendre_mma_kernel<64><<<grid, 128, smem, st>>>(d_probs, d_work, nwork, lv, nparts, cols, d_err);
+    legendre_mma_kernel<64><<<grid, kLegThreads, smem, st>>>(d_probs, d_work, nwork, lv, nparts, cols, off2, d_err);
   } else {
-    cudaError_t e = cudaFuncSetAttribute(legendre_mma_kernel<128>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                         (int)smem);
+    e = cudaFuncSetAttribute(legendre_mma_kernel<128>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e != cudaSuccess) return e;
-    legendre_mma_kernel<128><<<grid, 128, smem, st>>>(d_probs, d_work, nwork, lv, nparts, cols, d_err);
+    legendre_mma_kernel<128><<<grid, kLegThreads, smem, st>>>(d_probs, d_work, nwork, lv, nparts, cols, off2,
+                                                              d_err);
   }
   return cudaGetLastError();
 }

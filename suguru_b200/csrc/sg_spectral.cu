@@ -29,6 +29,32 @@ constexpr int pidx() {
   return sizeof(T) == 8 ? 0 : 1;
 }
 
+// Thread mapping of the staging loops: thread t takes row r = t % RP of every
+// (t / RP + k blockDim / RP)-th staged element, so that no loop iteration
+// divides by a runtime value; the threads past the last whole group of RP
+// stay idle.  Element offsets come from per-item tables in shared memory.
+struct StageMap {
+  int r, e0, es;
+  bool on;
+};
+__device__ __forceinline__ StageMap stage_map(int RP) {
+  StageMap m;
+  m.es = (int)blockDim.x / RP;
+  m.r = (int)threadIdx.x % RP;
+  m.e0 = (int)threadIdx.x / RP;
+  m.on = (int)threadIdx.x < m.es * RP;
+  return m;
+}
+
+// The trig table rows hm < nrow, columns j < H, of a [nrow][ld] global table
+// into [nrow][ts] shared rows.
+template <class T>
+__device__ __forceinline__ void stage_trig(T* dst, int ts, const T* src, int ld, int nrow, int H) {
+  const StageMap sm = stage_map(H);
+  if (sm.on)
+    for (int hm = sm.e0; hm < nrow; hm += sm.es) dst[hm * ts + sm.r] = src[hm * ld + sm.r];
+}
+
 // Division in the pointwise geometry and mechanics: the FP32 path uses the
 // fast reciprocal-based division (2 ulp), the FP64 path the IEEE division.
 template <class T>
@@ -67,12 +93,30 @@ __global__ void __launch_bounds__(256) posfwd_kernel(const RowWork* __restrict__
     const RowWork it = work[w];
     const CapInfo ci = caps[it.cap];
     {
+      // the thread's points in batches of 8: the 24 loads of a batch are all
+      // issued before any is summed (these are the step's first reads of the
+      // positions, from HBM), then added in the same order as one at a time
       const long long n = 8LL * ci.N * ci.N;
       double sx = 0, sy = 0, sz = 0;
-      for (long long p = tid; p < n; p += blockDim.x) {
-        sx += X[ci.pt_off + p];
-        sy += Y[ci.pt_off + p];
-        sz += Z[ci.pt_off + p];
+      const double* Xc = X + ci.pt_off;
+      const double* Yc = Y + ci.pt_off;
+      const double* Zc = Z + ci.pt_off;
+      for (long long p0 = tid; p0 < n; p0 += 8LL * blockDim.x) {
+        double bx[8], by[8], bz[8];
+#pragma unroll
+        for (int u = 0; u < 8; ++u) {
+          const long long p = p0 + (long long)u * blockDim.x;
+          const bool in = p < n;
+          bx[u] = in ? Xc[p] : 0.0;
+          by[u] = in ? Yc[p] : 0.0;
+          bz[u] = in ? Zc[p] : 0.0;
+        }
+#pragma unroll
+        for (int u = 0; u < 8; ++u) {
+          sx += bx[u];
+          sy += by[u];
+          sz += bz[u];
+        }
       }
       __syncthreads();  // the previous item's reads of s_cen are done
       s_cen[0][tid] = sx;
@@ -101,10 +145,7 @@ __global__ void __launch_bounds__(256) posfwd_kernel(const RowWork* __restrict__
     const double c0 = s_cen[0][0] / nl, c1 = s_cen[1][0] / nl, c2 = s_cen[2][0] / nl;
     T* Fpos = (T*)gd.buf.Fpos + (long long)ci.gidx * 6 * N * nD;
     __syncthreads();  // the previous item's reads of shared memory are done
-    for (int q = tid; q < 2 * N * H; q += blockDim.x) {
-      const int hm = q / H, j = q - hm * H;
-      sTrig[hm * hP + j] = trig[hm * mD + j];
-    }
+    stage_trig<T>(sTrig, hP, trig, mD, 2 * N, H);
     for (int rb = it.row0; rb < it.row0 + it.nrows; rb += RP) {
       const int rows = min(RP, it.row0 + it.nrows - rb);
       __syncthreads();
@@ -410,6 +451,7 @@ __global__ void __launch_bounds__(256, sizeof(T) == 4 ? 3 : 2) membrane_kernel(c
     T* sG = (T*)smem_raw;                  // [RP][SR]
     T* sTrig = sG + RP * SR;               // [2N][H+1]: cos m phi_j (rows m), sin m phi_j (rows N+m), j < H
     T* sOut = sTrig + 2 * N * (H + 1);     // [RP][6][2H+2]: sum over the half turn at [j], difference at [H+1+j]
+    int* sOff = (int*)(sOut + RP * 6 * (2 * H + 2));  // [18N] staged offset of element e
     const T* G = (const T*)gd.buf.G + (long long)ci.gidx * (18 * N * nD);  // [ccs][m][kind][lat]
     const T* trig = (const T*)gd.trigD[pidx<T>()];
     const T* lat = (const T*)gd.latD[pidx<T>()];
@@ -417,20 +459,19 @@ __global__ void __launch_bounds__(256, sizeof(T) == 4 ? 3 : 2) membrane_kernel(c
     const T sfn = T(2) / T(mD);
     const T R = (T)ci.R;
     __syncthreads();  // the previous item's reads of shared memory are done
-    for (int q = tid; q < 2 * N * H; q += blockDim.x) {
-      const int hm = q / H, j = q - hm * H;
-      sTrig[hm * (H + 1) + j] = trig[hm * mD + j];
+    stage_trig<T>(sTrig, H + 1, trig, mD, 2 * N, H);
+    for (int e = tid; e < 18 * N; e += blockDim.x) {  // e = (ccs N + m) 3 + kind
+      const int kind = e % 3, cm_ = e / 3, m = cm_ % N, ccs = cm_ / N;
+      sOff[e] = m * kGK + 3 * ccs + kind;
     }
+    const StageMap sm = stage_map(RP);
     for (int rb = it.row0; rb < it.row0 + it.nrows; rb += RP) {
       const int rows = min(RP, it.row0 + it.nrows - rb);
       __syncthreads();  // the previous chunk's staged rows and outputs are consumed
       // stage the chunk's rows, transposed to [row][m][3 ccs + kind]; a warp
-      // reads runs of `rows` consecutive latitudes of one (ccs, m, kind)
-      for (int q = tid; q < 18 * N * rows; q += blockDim.x) {
-        const int e = q / rows, r = q - e * rows;  // e = (ccs N + m) 3 + kind
-        const int kind = e % 3, cm_ = e / 3, m = cm_ % N, ccs = cm_ / N;
-        sG[r * SR + m * kGK + 3 * ccs + kind] = G[(long long)e * nD + rb + r];
-      }
+      // reads runs of RP consecutive latitudes of one (ccs, m, kind)
+      if (sm.on && sm.r < rows)
+        for (int e = sm.e0; e < 18 * N; e += sm.es) sG[sm.r * SR + sOff[e]] = G[(long long)e * nD + rb + sm.r];
       __syncthreads();
       {
         const int r = tid / H, j = tid - (tid / H) * H;
@@ -551,6 +592,7 @@ __global__ void __launch_bounds__(256, 3) membrane_kernel_f2(const RowWork* __re
     float4* sTP = (float4*)(sG + RP * SR);              // [NP][H]
     float* sTrig = (float*)(sTP + NP * H);              // [2N][TS]: cos m phi_j (rows m), sin (rows N + m)
     float* sOut = sTrig + 2 * N * TS;                   // [RP][6][OS]
+    int* sOff = (int*)(sOut + RP * 6 * OS);              // [18N] staged offset of element e
     const float* G = (const float*)gd.buf.G + (long long)ci.gidx * (18 * N * nD);  // [ccs][m][kind][lat]
     const float* trig = (const float*)gd.trigD[1];
     const float* lat = (const float*)gd.latD[1];
@@ -558,26 +600,29 @@ __global__ void __launch_bounds__(256, 3) membrane_kernel_f2(const RowWork* __re
     const float sfn = 2.0f / (float)mD;
     const float R = (float)ci.R;
     __syncthreads();  // the previous item's reads of shared memory are done
-    for (int q = tid; q < NP * H; q += blockDim.x) {
-      const int mp = q / H, j = q - mp * H, m = 2 * mp;
-      const bool odd = m + 1 < N;
-      sTP[q] = make_float4(trig[m * mD + j], odd ? trig[(m + 1) * mD + j] : 0.0f, trig[(N + m) * mD + j],
-                           odd ? trig[(N + m + 1) * mD + j] : 0.0f);
+    {
+      const StageMap tm = stage_map(H);
+      if (tm.on)
+        for (int mp = tm.e0; mp < NP; mp += tm.es) {
+          const int j = tm.r, m = 2 * mp;
+          const bool odd = m + 1 < N;
+          sTP[mp * H + j] = make_float4(trig[m * mD + j], odd ? trig[(m + 1) * mD + j] : 0.0f,
+                                        trig[(N + m) * mD + j], odd ? trig[(N + m + 1) * mD + j] : 0.0f);
+        }
     }
-    for (int q = tid; q < 2 * N * H; q += blockDim.x) {
-      const int hm = q / H, j = q - hm * H;
-      sTrig[hm * TS + j] = trig[hm * mD + j];
+    stage_trig<float>(sTrig, TS, trig, mD, 2 * N, H);
+    for (int e = tid; e < 18 * N; e += blockDim.x) {  // e = (ccs N + m) 3 + kind
+      const int kind = e % 3, cm_ = e / 3, m = cm_ % N, ccs = cm_ / N;
+      sOff[e] = (m >> 1) * kGP + 2 * (3 * ccs + kind) + (m & 1);
     }
+    const StageMap sm = stage_map(RP);
     for (int rb = it.row0; rb < it.row0 + it.nrows; rb += RP) {
       const int rows = min(RP, it.row0 + it.nrows - rb);
       __syncthreads();  // the previous chunk's staged rows and outputs are consumed
       // stage the chunk's rows to [row][m pair][k][m parity], k = 3 ccs + kind;
-      // a warp reads runs of `rows` consecutive latitudes of one (ccs, m, kind)
-      for (int q = tid; q < 18 * N * rows; q += blockDim.x) {
-        const int e = q / rows, r = q - e * rows;  // e = (ccs N + m) 3 + kind
-        const int kind = e % 3, cm_ = e / 3, m = cm_ % N, ccs = cm_ / N;
-        sG[r * SR + (m >> 1) * kGP + 2 * (3 * ccs + kind) + (m & 1)] = G[(long long)e * nD + rb + r];
-      }
+      // a warp reads runs of RP consecutive latitudes of one (ccs, m, kind)
+      if (sm.on && sm.r < rows)
+        for (int e = sm.e0; e < 18 * N; e += sm.es) sG[sm.r * SR + sOff[e]] = G[(long long)e * nD + rb + sm.r];
       if (N & 1)
         for (int q = tid; q < 18 * rows; q += blockDim.x) {
           const int r = q / 18, k = q - r * 18;
@@ -641,14 +686,15 @@ __global__ void __launch_bounds__(256, 3) membrane_kernel_f2(const RowWork* __re
 }
 
 // Shared memory (bytes) of membrane_kernel_f2 for degrees up to nmax: the
-// largest over n <= nmax of staged rows RP (NP kGP + 4), the pair trig table
+// largest over n <= nmax of staged rows RP (NP kGP + 4), the staging offsets
+// 18n, the pair trig table
 // NP H float4, the DFT trig table 2n (H + 2) and outputs RP 6 (2H + 4), with
 // H = 2n, NP = ceil(n / 2) and RP = max(1, 256 / H).
 static size_t membrane_f2_smem(int nmax) {
   size_t e = 0;
   for (size_t n = 1; n <= (size_t)nmax; ++n) {
     const size_t H = 2 * n, NP = (n + 1) / 2, RP = 256 / H > 0 ? 256 / H : 1;
-    const size_t en = RP * (NP * kGP + 4) + NP * H * 4 + 2 * n * (H + 2) + RP * 6 * (2 * H + 4) + 64;
+    const size_t en = RP * (NP * kGP + 4) + NP * H * 4 + 2 * n * (H + 2) + RP * 6 * (2 * H + 4) + 18 * n + 64;
     if (en > e) e = en;
   }
   return sizeof(float) * e;
@@ -701,6 +747,7 @@ __global__ void __launch_bounds__(256) shgrid_kernel(const RowWork* __restrict__
     T* sG = (T*)smem_raw;                 // [RP][SR]
     T* sTrig = sG + RP * SR;              // [2N][H+1]
     T* sOut = sTrig + 2 * N * hP;         // [RP][4][2H+2]
+    int* sOff = (int*)(sOut + RP * 4 * lP);  // [18N][2]: staged offset and source row of element e
     const T* GO = (const T*)gd.buf.GO + (long long)ci.gidx * (24 * N * nO);  // [rr][m][kind][lat]
     const T* trig = (const T*)gd.trigO[pidx<T>()];
     const T* lat = (const T*)gd.latO[pidx<T>()];
@@ -708,21 +755,22 @@ __global__ void __launch_bounds__(256) shgrid_kernel(const RowWork* __restrict__
     const T sfn = T(2) / T(mO);
     const T R = (T)ci.R;
     __syncthreads();  // the previous item's reads of shared memory are done
-    for (int q = tid; q < 2 * N * H; q += blockDim.x) {
-      const int hm = q / H, j = q - hm * H;
-      sTrig[hm * hP + j] = trig[hm * mO + j];
+    stage_trig<T>(sTrig, hP, trig, mO, 2 * N, H);
+    // staged elements e = (s, c, cs, m) with s = 0 normal P (rr = 2c+cs,
+    // kind 0), s = 1 shape P (rr = 2(3+c)+cs, kind 0), s = 2 shape dP (kind 1)
+    for (int e = tid; e < 18 * N; e += blockDim.x) {
+      const int m = e % N, t = e / N, cs = t & 1, c = (t >> 1) % 3, sk = t / 6;
+      const int rr = sk == 0 ? 2 * c + cs : 2 * (3 + c) + cs, kind = sk == 2 ? 1 : 0;
+      sOff[2 * e] = m * kSK + 6 * c + 2 * sk + cs;
+      sOff[2 * e + 1] = (rr * N + m) * 2 + kind;
     }
+    const StageMap sm = stage_map(RP);
     for (int rb = it.row0; rb < it.row0 + it.nrows; rb += RP) {
       const int rows = min(RP, it.row0 + it.nrows - rb);
       __syncthreads();
-      // stage: e = (s, c, cs, m) with s = 0 normal P (rr = 2c+cs, kind 0),
-      // s = 1 shape P (rr = 2(3+c)+cs, kind 0), s = 2 shape dP (kind 1)
-      for (int q = tid; q < 18 * N * rows; q += blockDim.x) {
-        const int e = q / rows, r = q - e * rows;
-        const int m = e % N, t = e / N, cs = t & 1, c = (t >> 1) % 3, sk = t / 6;
-        const int rr = sk == 0 ? 2 * c + cs : 2 * (3 + c) + cs, kind = sk == 2 ? 1 : 0;
-        sG[r * SR + m * kSK + 6 * c + 2 * sk + cs] = GO[(long long)((rr * N + m) * 2 + kind) * nO + rb + r];
-      }
+      if (sm.on && sm.r < rows)
+        for (int e = sm.e0; e < 18 * N; e += sm.es)
+          sG[sm.r * SR + sOff[2 * e]] = GO[(long long)sOff[2 * e + 1] * nO + rb + sm.r];
       __syncthreads();
       const int r = tid / H, j = tid - (tid / H) * H;
       if (r < rows) {
@@ -822,22 +870,19 @@ __global__ void __launch_bounds__(256) final_kernel(const RowWork* __restrict__ 
     const int SR = N * kFK + 16 / (int)sizeof(T);
     T* sG = (T*)smem_raw;         // [RP][SR]
     T* sTrig = sG + RP * SR;      // [2N][H+1]
+    int* sOff = (int*)(sTrig + 2 * N * hP);  // [14N] staged offset of element e = rr N + m
     const T* GF = (const T*)gd.buf.GF + (long long)ci.gidx * (14 * N * nD);  // [rr][m][lat]
     const T* trig = (const T*)gd.trigD[pidx<T>()];
     const T* lat = (const T*)gd.latD[pidx<T>()];
     __syncthreads();  // the previous item's reads of shared memory are done
-    for (int q = tid; q < 2 * N * H; q += blockDim.x) {
-      const int hm = q / H, j = q - hm * H;
-      sTrig[hm * hP + j] = trig[hm * mD + j];
-    }
+    stage_trig<T>(sTrig, hP, trig, mD, 2 * N, H);
+    for (int e = tid; e < 14 * N; e += blockDim.x) sOff[e] = (e % N) * kFK + e / N;
+    const StageMap sm = stage_map(RP);
     for (int rb = it.row0; rb < it.row0 + it.nrows; rb += RP) {
       const int rows = min(RP, it.row0 + it.nrows - rb);
       __syncthreads();
-      for (int q = tid; q < 14 * N * rows; q += blockDim.x) {
-        const int e = q / rows, r = q - e * rows;  // e = rr N + m
-        const int m = e % N, rr = e / N;
-        sG[r * SR + m * kFK + rr] = GF[(long long)e * nD + rb + r];
-      }
+      if (sm.on && sm.r < rows)
+        for (int e = sm.e0; e < 14 * N; e += sm.es) sG[sm.r * SR + sOff[e]] = GF[(long long)e * nD + rb + sm.r];
       __syncthreads();
       const int r = tid / H, j = tid - (tid / H) * H;
       if (r < rows) {
@@ -938,29 +983,32 @@ size_t pointwise_smem(int kind, int nmax) {
       }
       break;
     case kMembrane:
-      // staged rows RP (n kGK + pad) with RP = max(1, 256 / 2n), the half-turn
+      // staged rows RP (n kGK + pad) with RP = max(1, 256 / 2n), 18n staging offsets, the half-turn
       // trig table 2n (2n + 1), outputs RP 6 (4n + 2): the largest over the
       // degrees n <= N (smaller degrees stage more rows per chunk)
       for (size_t n = 1; n <= N; ++n) {
         const size_t RP = kPointThreads / (2 * n) > 0 ? kPointThreads / (2 * n) : 1;
-        const size_t en = RP * (n * kGK + 16 / sizeof(T)) + 2 * n * (2 * n + 1) + RP * 6 * (4 * n + 2) + 64;
+        const size_t en = RP * (n * kGK + 16 / sizeof(T)) + 2 * n * (2 * n + 1) + RP * 6 * (4 * n + 2) +
+                          (18 * n * sizeof(int) + sizeof(T) - 1) / sizeof(T) + 64;
         if (en > e) e = en;
       }
       break;
     case kShgrid:
-      // staged rows RP (n kSK + pad) with RP = max(1, 256 / n), trig 2n (n + 1),
+      // staged rows RP (n kSK + pad) with RP = max(1, 256 / n), 36n staging offsets, trig 2n (n + 1),
       // outputs RP 4 (2n + 2)
       for (size_t n = 1; n <= N; ++n) {
         const size_t RP = kPointThreads / n > 0 ? kPointThreads / n : 1;
-        const size_t en = RP * (n * kSK + 16 / sizeof(T)) + 2 * n * (n + 1) + RP * 4 * (2 * n + 2) + 64;
+        const size_t en = RP * (n * kSK + 16 / sizeof(T)) + 2 * n * (n + 1) + RP * 4 * (2 * n + 2) +
+                          (36 * n * sizeof(int) + sizeof(T) - 1) / sizeof(T) + 64;
         if (en > e) e = en;
       }
       break;
     default:
-      // staged rows RP (n kFK + pad) with RP = max(1, 256 / 2n), trig 2n (2n + 1)
+      // staged rows RP (n kFK + pad) with RP = max(1, 256 / 2n), 14n staging offsets, trig 2n (2n + 1)
       for (size_t n = 1; n <= N; ++n) {
         const size_t RP = kPointThreads / (2 * n) > 0 ? kPointThreads / (2 * n) : 1;
-        const size_t en = RP * (n * kFK + 16 / sizeof(T)) + 2 * n * (2 * n + 1) + 64;
+        const size_t en = RP * (n * kFK + 16 / sizeof(T)) + 2 * n * (2 * n + 1) +
+                          (14 * n * sizeof(int) + sizeof(T) - 1) / sizeof(T) + 64;
         if (en > e) e = en;
       }
       break;

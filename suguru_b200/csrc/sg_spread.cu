@@ -105,63 +105,21 @@ __device__ __forceinline__ double pow2<double>(int e) {
 
 }  // namespace
 
-// Force records cf = F * (A / dV) (interp_spread.f90:870-874 multiplies by
-// area / dVeul in this order).
+// Fixed-point scales of one tile, one per component c, from m_c = |f_c *
+// area / dV| over the tile's entries e0..e1 (blocks of 256 threads).  Only
+// order-independent quantities enter them -- the largest m_c, the entry count
+// and an integer sum -- so that the scales, like the sums, do not depend on
+// the order of the entries.  A scale per component keeps each component's
+// relative precision when another one is much larger (a wall force of
+// collisions.f90 beside a membrane force).  scale[c] = 2^sh, iscale = 2^-sh.
 template <class T>
-__global__ void pack_forces_kernel(long n, double dvi, const T* __restrict__ FX, const T* __restrict__ FY,
-                                   const T* __restrict__ FZ, const T* __restrict__ A, ForceRec<T>* __restrict__ frc) {
-  const long p = (long)blockIdx.x * blockDim.x + threadIdx.x;
-  if (p >= n) return;
-  const T s = A[p] * (T)dvi;
-  ForceRec<T> r;
-  r.cf[0] = FX[p] * s;
-  r.cf[1] = FY[p] * s;
-  r.cf[2] = FZ[p] * s;
-  r.cf[3] = T(0);
-  frc[p] = r;
-}
-
-// CTR: cell-centre weights in every direction for every component (the
-// indicator's lagr2eulrind, interp_spread.f90:1319-1343) instead of the
-// staggered ones.
-template <class T, int TX, int TY, int TZ, bool CTR>
-__global__ void __launch_bounds__(256, sizeof(T) == 4 ? 4 : 2) spread_kernel(IBGrid g, const int* __restrict__ entries,
-                                                     const int* __restrict__ starts,
-                                                     const PosRec<T>* __restrict__ pos,
-                                                     const ForceRec<T>* __restrict__ frc, T* __restrict__ ox,
-                                                     T* __restrict__ oy, T* __restrict__ oz) {
+__device__ __forceinline__ void tile_scales(int e0, int e1, const int* __restrict__ entries,
+                                            const ForceRec<T>* __restrict__ frc, T (*s_red)[8],
+                                            unsigned long long (*s_sum)[8], T* scale, T* iscale) {
   constexpr bool F32 = sizeof(T) == 4;
-  constexpr int NC = TX * TY * TZ;
-  constexpr int NW = Fixed<T>::NW;
   constexpr int QB = Fixed<T>::QB;
-  constexpr int CPT = (NC + 255) / 256;  // cells per thread in the fold / write loops
-  constexpr int NT = F32 ? 1 : CPT;      // FP64 keeps running 64-bit totals
-  // per (limb, component): NC cells and 32 per-lane trash words that take the
-  // contributions falling outside the tile, so that the walk has no branches
-  constexpr int NCP = NC + 32;
-  __shared__ __align__(16) unsigned int acc[NW][3][NCP];
-  __shared__ T s_red[3][8];
-  __shared__ unsigned long long s_sum[3][8];
-  long long tot[NT][3];
-#pragma unroll
-  for (int r = 0; r < NT; ++r) tot[r][0] = tot[r][1] = tot[r][2] = 0;
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-  const int tile = blockIdx.x;
-  const int tx = tile % g.ntx, ty = (tile / g.ntx) % g.nty, tz = tile / (g.ntx * g.nty);
-  const int cw = min(TX, g.itot - TX * tx), ch = min(TY, g.jtot - TY * ty), cd = min(TZ, g.ktot - TZ * tz);
-  const int i0 = 1 + TX * tx, j0 = 1 + TY * ty, k0 = 1 + TZ * tz;
-  const int e0 = starts[tile], e1 = starts[tile + 1];
-  T iscale[3] = {T(0), T(0), T(0)};
-
-  if (e1 > e0) {
-    for (int q = tid; q < NW * 3 * NCP / 4; q += 256) ((uint4*)&acc[0][0][0])[q] = make_uint4(0u, 0u, 0u, 0u);
-    // ---- fixed-point scales, one per component c, from m_c = |f_c * area / dV|
-    // over the tile's entries.  Only order-independent quantities enter them
-    // -- the largest m_c, the entry count and an integer sum -- so that the
-    // scales, like the sums, do not depend on the order of the entries.  A
-    // scale per component keeps each component's relative precision when
-    // another one is much larger (a wall force of collisions.f90 beside a
-    // membrane force).
+  {
     T rmax[3] = {T(0), T(0), T(0)};
     for (int e = e0 + tid; e < e1; e += 256) {
       const ForceRec<T> fo = frc[entries[e]];
@@ -236,12 +194,66 @@ __global__ void __launch_bounds__(256, sizeof(T) == 4 ? 4 : 2) spread_kernel(IBG
 #pragma unroll
       for (int c = 0; c < 3; ++c) sh[c] = min(sh[c], sh1[c]);
     }
-    T scale[3];
 #pragma unroll
     for (int c = 0; c < 3; ++c) {
       scale[c] = pow2<T>(sh[c]);
       iscale[c] = pow2<T>(-sh[c]);
     }
+  }
+}
+
+// Force records cf = F * (A / dV) (interp_spread.f90:870-874 multiplies by
+// area / dVeul in this order).
+template <class T>
+__global__ void pack_forces_kernel(long n, double dvi, const T* __restrict__ FX, const T* __restrict__ FY,
+                                   const T* __restrict__ FZ, const T* __restrict__ A, ForceRec<T>* __restrict__ frc) {
+  const long p = (long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (p >= n) return;
+  const T s = A[p] * (T)dvi;
+  ForceRec<T> r;
+  r.cf[0] = FX[p] * s;
+  r.cf[1] = FY[p] * s;
+  r.cf[2] = FZ[p] * s;
+  r.cf[3] = T(0);
+  frc[p] = r;
+}
+
+// CTR: cell-centre weights in every direction for every component (the
+// indicator's lagr2eulrind, interp_spread.f90:1319-1343) instead of the
+// staggered ones.
+template <class T, int TX, int TY, int TZ, bool CTR>
+__global__ void __launch_bounds__(256, sizeof(T) == 4 ? 4 : 2) spread_kernel(IBGrid g, const int* __restrict__ entries,
+                                                     const int* __restrict__ starts,
+                                                     const PosRec<T>* __restrict__ pos,
+                                                     const ForceRec<T>* __restrict__ frc, T* __restrict__ ox,
+                                                     T* __restrict__ oy, T* __restrict__ oz) {
+  constexpr bool F32 = sizeof(T) == 4;
+  constexpr int NC = TX * TY * TZ;
+  constexpr int NW = Fixed<T>::NW;
+  constexpr int CPT = (NC + 255) / 256;  // cells per thread in the fold / write loops
+  constexpr int NT = F32 ? 1 : CPT;      // FP64 keeps running 64-bit totals
+  // per (limb, component): NC cells and 32 per-lane trash words that take the
+  // contributions falling outside the tile, so that the walk has no branches
+  constexpr int NCP = NC + 32;
+  __shared__ __align__(16) unsigned int acc[NW][3][NCP];
+  __shared__ T s_red[3][8];
+  __shared__ unsigned long long s_sum[3][8];
+  long long tot[NT][3];
+#pragma unroll
+  for (int r = 0; r < NT; ++r) tot[r][0] = tot[r][1] = tot[r][2] = 0;
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  const int tile = blockIdx.x;
+  const int tx = tile % g.ntx, ty = (tile / g.ntx) % g.nty, tz = tile / (g.ntx * g.nty);
+  const int cw = min(TX, g.itot - TX * tx), ch = min(TY, g.jtot - TY * ty), cd = min(TZ, g.ktot - TZ * tz);
+  const int i0 = 1 + TX * tx, j0 = 1 + TY * ty, k0 = 1 + TZ * tz;
+  const int e0 = starts[tile], e1 = starts[tile + 1];
+  T iscale[3] = {T(0), T(0), T(0)};
+
+  if (e1 > e0) {
+    for (int q = tid; q < NW * 3 * NCP / 4; q += 256) ((uint4*)&acc[0][0][0])[q] = make_uint4(0u, 0u, 0u, 0u);
+    // ---- fixed-point scales, one per component (tile_scales)
+    T scale[3];
+    tile_scales<T>(e0, e1, entries, frc, s_red, s_sum, scale, iscale);
 
     // ---- one point per thread, in passes of at most PASS entries
     for (int c0 = e0; c0 < e1; c0 += Fixed<T>::PASS) {
@@ -407,6 +419,165 @@ __global__ void __launch_bounds__(256, sizeof(T) == 4 ? 4 : 2) spread_kernel(IBG
   }
 }
 
+// FP32 spreading on tiles of whole x rows: TY x TZ rows of itot cells (the x
+// direction is periodic, so a row tile holds every x cell a stencil can reach
+// and needs no x halo).  The fixed-point sums, scales and the walk are those
+// of spread_kernel; what changes is the write: each warp writes whole rows of
+// the Fortran field, i = 0 .. itot + 1 with both periodic x-halo copies, as
+// runs of consecutive words, so that the misaligned 258-float rows of the
+// reference layout split 32-byte sectors only at row ends.  Tiles at a y face
+// also write the periodic y-halo rows, and tiles at a z wall the zero halo
+// planes.  Shared memory (dynamic): 3 components x (itot TY TZ + 32) words.
+template <int TY, int TZ>
+__global__ void __launch_bounds__(256, 4) spread_rows_kernel(IBGrid g, const int* __restrict__ entries,
+                                                             const int* __restrict__ starts,
+                                                             const PosRec<float>* __restrict__ pos,
+                                                             const ForceRec<float>* __restrict__ frc,
+                                                             float* __restrict__ ox, float* __restrict__ oy,
+                                                             float* __restrict__ oz) {
+  extern __shared__ __align__(16) unsigned int racc[];  // [3][NCP]
+  __shared__ float s_red[3][8];
+  __shared__ unsigned long long s_sum[3][8];
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  const int NX = g.itot, NC = NX * TY * TZ, NCP = NC + 32;
+  const int tile = blockIdx.x;
+  const int ty = tile % g.nty, tz = tile / g.nty;
+  const int ch = min(TY, g.jtot - TY * ty), cd = min(TZ, g.ktot - TZ * tz);
+  const int j0 = 1 + TY * ty, k0 = 1 + TZ * tz;
+  const int e0 = starts[tile], e1 = starts[tile + 1];
+  float iscale[3] = {0.f, 0.f, 0.f};
+  if (e1 > e0) {
+    for (int q = tid; q < 3 * NCP / 4; q += 256) ((uint4*)racc)[q] = make_uint4(0u, 0u, 0u, 0u);
+    float scale[3];
+    tile_scales<float>(e0, e1, entries, frc, s_red, s_sum, scale, iscale);
+    const int trash = NC + lane;
+    for (int eb = e0; eb < e1; eb += 256) {
+      const int k = min(256, e1 - eb), nw = (k + 31) >> 5;
+      const int idx = lane * nw + warp;
+      if (warp >= nw || idx >= k) continue;
+      const int p = entries[eb + idx];
+      const PosRec<float> rec = pos[p];
+      const ForceRec<float> fo = frc[p];
+      const float cf[3] = {fo.cf[0] * scale[0], fo.cf[1] * scale[1], fo.cf[2] * scale[2]};
+      float wF[3][3], wC[3][3];
+      bool hi[3];
+#pragma unroll
+      for (int d = 0; d < 3; ++d) {
+        delta3_face<float>(rec.f[d], wF[d], hi[d]);
+        delta3_centre<float>(rec.f[d], wC[d]);
+      }
+      // cell offsets at o = -1..2 per dimension (kOut outside the tile; x is
+      // always inside: the row is whole and periodic)
+      int lcF[3][3], lcC[3][3];
+#pragma unroll
+      for (int d = 0; d < 3; ++d) {
+        int lc[4];
+#pragma unroll
+        for (int t = 0; t < 4; ++t) {
+          if (d == 0) {
+            lc[t] = wrap_near(rec.b[0] + t - 1, NX) - 1;
+          } else if (d == 1) {
+            const int b = wrap_near(rec.b[1] + t - 1, g.jtot) - j0;
+            lc[t] = (b >= 0 && b < ch) ? NX * b : kOut;
+          } else {
+            const int kk = rec.b[2] + t - 1;
+            lc[t] = (kk - k0 >= 0 && kk - k0 < cd && kk >= 1 && kk <= g.ktot) ? NX * TY * (kk - k0) : kOut;
+          }
+        }
+#pragma unroll
+        for (int q = 0; q < 3; ++q) {
+          lcF[d][q] = hi[d] ? lc[q + 1] : lc[q];
+          lcC[d][q] = lc[q + 1];
+        }
+      }
+#pragma unroll
+      for (int c = 0; c < 3; ++c) {
+        unsigned int* a = racc + c * NCP;
+#pragma unroll
+        for (int iz = 0; iz < 3; ++iz) {
+          const int cz_ = c == 2 ? lcF[2][iz] : lcC[2][iz];
+          const float wz = c == 2 ? wF[2][iz] : wC[2][iz];
+#pragma unroll
+          for (int iy = 0; iy < 3; ++iy) {
+            const int cyz = cz_ + (c == 1 ? lcF[1][iy] : lcC[1][iy]);
+            const float pyz = cf[c] * ((c == 1 ? wF[1][iy] : wC[1][iy]) * wz);
+#pragma unroll
+            for (int ix = 0; ix < 3; ++ix) {
+              const int cell = cyz + (c == 0 ? lcF[0][ix] : lcC[0][ix]);
+              const float wx = c == 0 ? wF[0][ix] : wC[0][ix];
+              const unsigned slot = min((unsigned)cell, (unsigned)trash);
+              const float t = fmaf(pyz, wx, kMagic);
+              atomicAdd(&a[slot], (unsigned int)(__float_as_int(t) - kMagicBits));
+            }
+          }
+        }
+      }
+    }
+    __syncthreads();
+  }
+  // ---- write: one warp per row of the tile, i = 0 .. itot + 1 in runs of 32
+  const bool any = e1 > e0;
+  const int ldi = g.ldi, ldj = g.ldj;
+  for (int r = warp; r < ch * cd; r += 8) {
+    const int ly = r % ch, lz = r / ch;
+    const int j = j0 + ly, k = k0 + lz;
+    // rows this one is copied to: itself and its periodic y-halo image
+    const int jh = j == 1 ? g.jtot + 1 : (j == g.jtot ? 0 : -1);
+    const int zp = k == 1 ? 0 : (k == g.ktot ? g.ktot + 1 : -1);  // zero wall-halo plane beside it
+    const int base = NX * (ly + TY * lz);
+    const long long o0 = (long long)ldi * (j + (long long)ldj * k);
+    const long long oh = jh >= 0 ? (long long)ldi * (jh + (long long)ldj * k) : -1;
+    for (int i = lane; i < ldi; i += 32) {
+      const int xi = i == 0 ? NX - 1 : (i == NX + 1 ? 0 : i - 1);
+      float vu = 0.f, vv = 0.f, vw = 0.f;
+      if (any) {
+        vu = (float)(int)racc[base + xi] * iscale[0];
+        vv = (float)(int)racc[NCP + base + xi] * iscale[1];
+        vw = (float)(int)racc[2 * NCP + base + xi] * iscale[2];
+      }
+      ox[o0 + i] = vu;
+      oy[o0 + i] = vv;
+      oz[o0 + i] = vw;
+      if (oh >= 0) {
+        ox[oh + i] = vu;
+        oy[oh + i] = vv;
+        oz[oh + i] = vw;
+      }
+      if (zp >= 0) {
+        const long long z0 = (long long)ldi * (j + (long long)ldj * zp);
+        ox[z0 + i] = 0.f;
+        oy[z0 + i] = 0.f;
+        oz[z0 + i] = 0.f;
+        if (jh >= 0) {
+          const long long z1 = (long long)ldi * (jh + (long long)ldj * zp);
+          ox[z1 + i] = 0.f;
+          oy[z1 + i] = 0.f;
+          oz[z1 + i] = 0.f;
+        }
+      }
+    }
+  }
+}
+
+// Dynamic shared memory of a row tile (bytes), 0 when it exceeds what one CTA
+// can hold.
+static size_t rows_smem(int itot, int TY, int TZ) {
+  const size_t b = sizeof(unsigned int) * 3 * ((size_t)itot * TY * TZ + 32);
+  return b <= kRowTileSmemMax ? b : 0;
+}
+
+template <int TY, int TZ>
+static cudaError_t spread_rows(const IBGrid& g, const IBWork& w, float* ox, float* oy, float* oz, cudaStream_t st) {
+  const size_t smem = rows_smem(g.itot, TY, TZ);
+  if (!smem || g.TX != g.itot || g.TY != TY || g.TZ != TZ) return cudaErrorInvalidValue;
+  cudaError_t e = cudaFuncSetAttribute(spread_rows_kernel<TY, TZ>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                       (int)smem);
+  if (e != cudaSuccess) return e;
+  spread_rows_kernel<TY, TZ><<<g.ntiles, 256, smem, st>>>(g, w.entries, w.starts, (const PosRec<float>*)w.pos,
+                                                         (const ForceRec<float>*)w.frc, ox, oy, oz);
+  return cudaGetLastError();
+}
+
 template <class T, int TX, int TY, int TZ, bool CTR = false>
 static void spread_one(const IBGrid& g, const IBWork& w, T* ox, T* oy, T* oz, cudaStream_t st) {
   spread_kernel<T, TX, TY, TZ, CTR><<<g.ntiles, 256, 0, st>>>(g, w.entries, w.starts, (const PosRec<T>*)w.pos,
@@ -431,6 +602,15 @@ cudaError_t launch_spread(const IBGrid& g, const IBWork& w, T* ox, T* oy, T* oz,
       return cudaErrorInvalidValue;
     case 2:
       if constexpr (sizeof(T) == 4) { spread_one<T, 32, 8, 8>(g, w, ox, oy, oz, st); break; }
+      return cudaErrorInvalidValue;
+    case 4:
+      if constexpr (sizeof(T) == 4) return spread_rows<4, 4>(g, w, ox, oy, oz, st);
+      return cudaErrorInvalidValue;
+    case 5:
+      if constexpr (sizeof(T) == 4) return spread_rows<8, 4>(g, w, ox, oy, oz, st);
+      return cudaErrorInvalidValue;
+    case 6:
+      if constexpr (sizeof(T) == 4) { spread_one<T, 32, 16, 4>(g, w, ox, oy, oz, st); break; }
       return cudaErrorInvalidValue;
     default: return cudaErrorInvalidValue;
   }

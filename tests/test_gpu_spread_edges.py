@@ -63,7 +63,7 @@ def test_grid_only_a_wide_tile_fits(cuda):
         CouplingStep(wl.grid, wl.degree, wl.radius, precision="fp64")
     assert e.value.code == 1  # SG_ERR_CONFIG
     cs = CouplingStep(wl.grid, wl.degree, wl.radius, precision="mixed")
-    assert cs.tile_shape()[1:] == (16, 16, 8)
+    assert cs.tile_shape()[1] == (16, 16, 8)
     got = cs.lagr2eulr(wl.x, wl.y, wl.z, *(x.astype(np.float32) for x in f), a.astype(np.float32))
     for g, r in zip(got, ref):
         assert rel_l2(g, r) <= 1e-4
@@ -93,3 +93,30 @@ def test_unaligned_output_fields(cuda, precision):
         assert torch.equal(g, s)
         assert float(b[0]) == 7.0  # nothing written before the field
         assert rel_l2(g.cpu().numpy(), r) <= tol
+
+
+@pytest.mark.parametrize("shape", [4, 5])
+@pytest.mark.parametrize("grid", [(61, 47, 40), (67, 51, 37), (64, 48, 40)])
+def test_row_tiles(cuda, grid, shape):
+    # whole-x-row tiles (FP32): ragged y and z, periodic x inside the tile,
+    # halos written row by row; into an output shifted off its alignment, with
+    # nothing written outside the field; bitwise equal on a repeat
+    torch = cuda
+    wl, f, a, ref = _case(grid, seed=34)
+    dev = torch.device("cuda", 0)
+    cs = CouplingStep(wl.grid, wl.degree, wl.radius, precision="mixed", mem="device")
+    cs.set_tile_shape(shape)
+    X = [torch.from_numpy(x).to(dev) for x in (wl.x, wl.y, wl.z)]
+    F = [torch.from_numpy(x.astype(np.float32)).to(dev) for x in f]
+    A = torch.from_numpy(a.astype(np.float32)).to(dev)
+    n = int(np.prod(cs.field_shape))
+    bufs = [torch.full((n + 2,), 7.0, dtype=torch.float32, device=dev) for _ in range(3)]
+    shifted = [b[1:n + 1].view(cs.field_shape) for b in bufs]
+    cs.lagr2eulr(*X, *F, A, out=shifted)
+    again = [o.clone() for o in cs.lagr2eulr(*X, *F, A)]
+    torch.cuda.synchronize()
+    for s_, b, g2, r in zip(shifted, bufs, again, ref):
+        assert float(b[0]) == 7.0 and float(b[-1]) == 7.0
+        assert torch.equal(s_, g2)
+        assert rel_l2(s_.cpu().numpy(), r) <= 1e-4
+
