@@ -223,6 +223,19 @@ int sg_set_capsule_membrane(sg_ctx* ctx, const double* gs, const double* csk);
 #define SG_LAW_NEO_HOOKEAN 1
 int sg_set_capsule_law(sg_ctx* ctx, const int* law);
 
+/* Bending modulus per capsule (host array of ncap, NULL = all 0): a nonzero
+ * eb adds the bending terms of ibend = 1 (param.f90:90-91, eb = cbend gscell)
+ * to the membrane force: the moment tensor from the curvature change
+ * (cal_moment_deri, sph.f90:1236-1372), its transverse shear (cal_Q,
+ * sph.f90:1375-1424) and the curvature-membrane products (cal_bcurmix,
+ * sph.f90:1427-1454) in the equilibrium sums (sph.f90:1705-1709).  The
+ * first nonzero modulus sets up the third and fourth theta-derivative
+ * tables (sphharm.c:110-145) and one more contraction per step; with every
+ * modulus 0 the step is the plain (ibend = 0) one.  Capsules with bending
+ * never take the surrogate.  SG_ERR_ARG for a non-finite value,
+ * SG_ERR_STATE while a graph is captured. */
+int sg_set_capsule_bending(sg_ctx* ctx, const double* eb);
+
 /* Spectral coefficients of the plain membrane model, per capsule: the
  * displacement from the reference sphere after the centroid is removed
  * (the analysis of cal_3dcrd_spectral_coeff, sph1.f90:29-79) and the force

@@ -59,6 +59,7 @@ def lib():
         L.or_membrane_law.argtypes = [i, d, d, _dp, _dp, d, d, _dp]
         L.or_membrane_law.restype = None
         L.or_complagrforces_law.argtypes = [i, d, d, d, i, i] + [_dp] * 10
+        L.or_complagrforces_bend.argtypes = [i, d, d, d, i, d, i] + [_dp] * 10
         L.or_coupling_step.argtypes = ([i, i, i, d, d, d, i, _ip, _dp, d, d, i, i] + [_dp] * 20)
         _LIB = L
     return _LIB
@@ -135,16 +136,18 @@ def kerneltest():
     return lib().or_kerneltest()
 
 
-def complagrforces(L, radius, x, y, z, gs=1.0, csk=1.0, faithful=False, law=0):
+def complagrforces(L, radius, x, y, z, gs=1.0, csk=1.0, faithful=False, law=0, eb=0.0):
     """One capsule: flat force-grid positions -> (f[3,nl], n[3,nl], area[nl]).
 
-    law: 0 Skalak (membmodel.c:81-99), 1 neo-Hookean (membmodel.c:60-79)."""
+    law: 0 Skalak (membmodel.c:81-99), 1 neo-Hookean (membmodel.c:60-79).
+    eb: bending modulus; nonzero adds the bending terms of ibend = 1
+    (sph.f90:1705-1709), 0 is the reference with ibend = 0."""
     nl = 8 * (L + 1) ** 2
     x, y, z = _f64(x), _f64(y), _f64(z)
     assert x.size == nl
     out = [np.zeros(nl) for _ in range(7)]
-    rc = lib().or_complagrforces_law(L, radius, gs, csk, int(law), int(faithful), _p(x), _p(y), _p(z),
-                                     *[_p(o) for o in out])
+    rc = lib().or_complagrforces_bend(L, radius, gs, csk, int(law), float(eb), int(faithful), _p(x), _p(y),
+                                      _p(z), *[_p(o) for o in out])
     assert rc == 0, rc
     return np.stack(out[0:3]), np.stack(out[3:6]), out[6]
 

@@ -128,6 +128,28 @@ void legendre_full(double th, int nn, std::vector<double>& T, std::vector<double
   ladder(D, D2);
 }
 
+// The same with the third and fourth theta derivatives (cal_legendre_deri4_array,
+// sphharm.c:110-145, converted to theta as sph3.f90:72-95 does): the ladder
+// applied twice more (d/dtheta of P^m_n involves P^{m-1}_n and P^{m+1}_n of the
+// same degree only, so every order stays exact).
+void legendre_full4(double th, int nn, std::vector<double>& T, std::vector<double>& D, std::vector<double>& D2,
+                    std::vector<double>& D3, std::vector<double>& D4) {
+  legendre_full(th, nn, T, D, D2);
+  auto at = [&](const std::vector<double>& A, int m, int n) -> double {
+    return (m < 0 || m > n || n >= nn) ? 0.0 : A[(size_t)m * nn + n];
+  };
+  auto ladder = [&](const std::vector<double>& A, std::vector<double>& B) {
+    B.assign((size_t)nn * nn, 0.0);
+    for (int m = 0; m < nn; ++m)
+      for (int n = m; n < nn; ++n)
+        B[(size_t)m * nn + n] = m == 0 ? -std::sqrt((double)n * (n + 1.0)) * at(A, 1, n)
+                                       : 0.5 * (std::sqrt((n + m) * (n - m + 1.0)) * at(A, m - 1, n) -
+                                                std::sqrt((n + m + 1.0) * (n - m)) * at(A, m + 1, n));
+  };
+  ladder(D2, D3);
+  ladder(D3, D4);
+}
+
 // Analysis/synthesis plan for a Gauss grid nlat x nlon (shagci/shsgci work).
 struct Plan {
   int nlat, nlon, l, lm1;
@@ -282,6 +304,25 @@ inline void cross(const double* u, const double* v, double* w) {
 }
 inline double dot(const double* u, const double* v) { return u[0] * v[0] + u[1] * v[1] + u[2] * v[2]; }
 
+// The tensors of the bending terms at one point, in the reference's Fortran
+// index order through 1-based accessors: bcur(b,a) = b_ab, bcurde1(c,b,a) =
+// d b_ab / d xi^c, bcurde2(d,c,b,a), conat(b,a) = a^ab, conatd1(l,b,a),
+// conatd2(l,lm,b,a), christof(g,b,a), chrisderi(l,lm,b,a) = d christof(lm,b,a)
+// / d xi^l.
+struct BendTensors {
+  double bc[2][2], bd1[2][2][2], bd2[2][2][2][2];
+  double ca[2][2], cad1[2][2][2], cad2[2][2][2][2];
+  double ch[2][2][2], chd[2][2][2][2];
+  double& bcur(int b, int a) { return bc[b - 1][a - 1]; }
+  double& bcurde1(int c, int b, int a) { return bd1[c - 1][b - 1][a - 1]; }
+  double& bcurde2(int d, int c, int b, int a) { return bd2[d - 1][c - 1][b - 1][a - 1]; }
+  double& conat(int b, int a) { return ca[b - 1][a - 1]; }
+  double& conatd1(int l, int b, int a) { return cad1[l - 1][b - 1][a - 1]; }
+  double& conatd2(int l, int m, int b, int a) { return cad2[l - 1][m - 1][b - 1][a - 1]; }
+  double& christof(int g, int b, int a) { return ch[g - 1][b - 1][a - 1]; }
+  double& chrisderi(int l, int m, int b, int a) { return chd[l - 1][m - 1][b - 1][a - 1]; }
+};
+
 // ----------------------------------------------------- capsule geometry -----
 // Per-degree state: grids, cached synthesis tables (sph3.f90:46-105 saved
 // tables), and the reference-sphere contravariant metric conAR/conARd1
@@ -296,6 +337,11 @@ struct Capsule {
   std::vector<double> cosO, sinO;     // on SH grid [m*mO+j]
   std::vector<double> conAR, conARd1; // [pt*4 + (a*2+b)], [pt*8 + al*4 + (a*2+b)]
   std::vector<double> wgtdsinf;       // [i] (independent of j)
+  // bending (ibend = 1): third and fourth theta derivatives on the dealias
+  // grid, and the reference sphere's tensors conAR, conARd1, conARd2, BR,
+  // BRd1, BRd2 (sph.f90:153-161), built on first use
+  std::vector<double> d3PD, d4PD;
+  std::vector<BendTensors> refB;
 };
 
 // Geometry fields on the dealias grid, one point.
@@ -334,6 +380,48 @@ void synth_basis(const Capsule& C, const double* a, const double* b, std::vector
             o[6 + c] += h * P2[n] * t0;   // deFvat1(:,1)
             o[9 + c] += h * P1[n] * t1;   // deFvat1(:,2)
             o[12 + c] += h * P[n] * t2;   // deFvat2(:,2)
+          }
+        }
+      }
+    }
+}
+
+// cal_co_tang_basis2 with ibend = 1 (sph3.f90:137-180): the 15 values of
+// synth_basis, then cdeSvat(:,1..4) (12) and cdeTvat(:,1..5) (15) per point.
+void synth_basis_bend(const Capsule& C, const double* a, const double* b, std::vector<double>& out42) {
+  const int N = C.N, nD = C.nD, mD = C.mD;
+  out42.assign((size_t)nD * mD * 42, 0.0);
+  for (int i = 0; i < nD; ++i)
+    for (int j = 0; j < mD; ++j) {
+      double* o = &out42[((size_t)i * mD + j) * 42];
+      for (int m = 0; m < N; ++m) {
+        double cm = C.cosD[(size_t)m * mD + j], sm = C.sinD[(size_t)m * mD + j];
+        const size_t t = ((size_t)i * N + m) * N;
+        const double *P = &C.PD[t], *P1 = &C.dPD[t], *P2 = &C.d2PD[t], *P3 = &C.d3PD[t], *P4 = &C.d4PD[t];
+        double h = (m == 0) ? 0.5 : 1.0;  // sph3.f90:98-102
+        for (int n = m; n < N; ++n) {
+          for (int c = 0; c < 3; ++c) {
+            double am = a[(size_t)c * N * N + (size_t)m * N + n];
+            double bm = b[(size_t)c * N * N + (size_t)m * N + n];
+            double t0 = am * cm - bm * sm;
+            double t1 = m * (am * (-sm) - bm * cm);
+            double t2 = -(double)m * m * t0;
+            double t3 = (double)m * m * m * (am * sm + bm * cm);
+            double t4 = (double)m * m * m * m * t0;
+            o[0 + c] += h * P1[n] * t0;   // vat1
+            o[3 + c] += h * P[n] * t1;    // vat2
+            o[6 + c] += h * P2[n] * t0;   // deFvat1(:,1)
+            o[9 + c] += h * P1[n] * t1;   // deFvat1(:,2)
+            o[12 + c] += h * P[n] * t2;   // deFvat2(:,2)
+            o[15 + c] += h * P3[n] * t0;  // deSvat(:,1)
+            o[18 + c] += h * P2[n] * t1;  // deSvat(:,2)
+            o[21 + c] += h * P1[n] * t2;  // deSvat(:,3)
+            o[24 + c] += h * P[n] * t3;   // deSvat(:,4)
+            o[27 + c] += h * P4[n] * t0;  // deTvat(:,1)
+            o[30 + c] += h * P3[n] * t1;  // deTvat(:,2)
+            o[33 + c] += h * P2[n] * t2;  // deTvat(:,3)
+            o[36 + c] += h * P1[n] * t3;  // deTvat(:,4)
+            o[39 + c] += h * P[n] * t4;   // deTvat(:,5)
           }
         }
       }
@@ -450,7 +538,12 @@ void membrane_law(int law, double hf, double csk, double I1, double I2, const do
 // Mechanics at one point: sph.f90:1668-1715 with cal_Js_I1_I2_deri
 // (sph.f90:1115-1156), the membrane law (membrane_law) and
 // calculate_cauchy_tensor_deri (sph.f90:1179-1234).  A* = reference (conAR).
-void mechanics(const Geo& G, const double* A, const double* Ad, double hf, double csk, int law, double* f) {
+struct BendQ {  // bending terms of the equilibrium (sph.f90:1705-1709)
+  double bm[2][2];  // bcurmix(be,al) at [be-1][al-1]
+  double Q[2], Qcode;
+};
+void mechanics(const Geo& G, const double* A, const double* Ad, double hf, double csk, int law, double* f,
+               const BendQ* bq = nullptr) {
   const double A11 = A[0], A22 = A[3], A12 = A[1];
   const double c11 = G.cat[0], c22 = G.cat[1], c12 = G.cat[2];
   double abs_conA = A11 * A22 - A12 * A12;
@@ -495,7 +588,283 @@ void mechanics(const Geo& G, const double* A, const double* Ad, double hf, doubl
   double q2 = Td12[0] + Td22[1] + ch(1, 1, 1) * T12 + ch(2, 1, 1) * T22 + ch(1, 2, 2) * T12 + ch(2, 2, 2) * T22 +
               ch(1, 2, 1) * T11 + ch(2, 2, 1) * T12 + ch(1, 2, 2) * T12 + ch(2, 2, 2) * T22;
   double q3 = T11 * G.bcur[0] + T22 * G.bcur[1] + 2 * T12 * G.bcur[2];
+  if (bq) {  // ibend = 1 (sph.f90:1705-1709)
+    q1 = q1 - bq->bm[0][0] * bq->Q[0] - bq->bm[1][0] * bq->Q[1];
+    q2 = q2 - bq->bm[0][1] * bq->Q[0] - bq->bm[1][1] * bq->Q[1];
+    q3 = q3 + bq->Qcode;
+  }
   for (int c = 0; c < 3; ++c) f[c] = q1 * G.a1[c] + q2 * G.a2[c] + q3 * G.n[c];
+}
+
+// ---------------------------------------------------- bending (ibend = 1) ---
+// cal_curvature_derivative (sph.f90:479-731), cal_contra_second_derivative
+// (sph1.f90:299-542), the ibend part of cal_christof (sph.f90:802-890) and
+// cal_contra_metric_second_deri (sph.f90:962-1111) at one point, from the
+// geometry G and the synthesised third (S: x_ttt, x_ttp, x_tpp, x_ppp) and
+// fourth (T: x_tttt, x_tttp, x_ttpp, x_tppp, x_pppp) derivatives, with the
+// reference's expressions term for term (including its chrisderi(2,2,1,2),
+// whose second product is cderi1(:,2) . conderi2(:,2)).
+void bend_tensors(const Geo& G, const double (*S)[3], const double (*T)[3], BendTensors& B) {
+  const double* cderi1[2] = {G.d11, G.d12};
+  const double* cderi2[2] = {G.d12, G.d22};
+  const double* cderi3[2] = {G.nde[0], G.nde[1]};
+  const double* conderi1[2] = {G.cd1[0], G.cd1[1]};
+  const double* conderi2[2] = {G.cd2[0], G.cd2[1]};
+  const double* n = G.n;
+  const double *c1 = G.c1, *c2 = G.c2;
+  B.bcur(1, 1) = G.bcur[0];
+  B.bcur(2, 2) = G.bcur[1];
+  B.bcur(1, 2) = B.bcur(2, 1) = G.bcur[2];
+  B.conat(1, 1) = G.conat[0];
+  B.conat(2, 2) = G.conat[1];
+  B.conat(1, 2) = B.conat(2, 1) = G.conat[2];
+  for (int al = 1; al <= 2; ++al) {
+    B.conatd1(al, 1, 1) = G.conatd1[al - 1][0];
+    B.conatd1(al, 2, 2) = G.conatd1[al - 1][1];
+    B.conatd1(al, 1, 2) = B.conatd1(al, 2, 1) = G.conatd1[al - 1][2];
+  }
+  for (int g = 1; g <= 2; ++g)
+    for (int b = 1; b <= 2; ++b)
+      for (int a = 1; a <= 2; ++a) B.christof(g, b, a) = G.chf[(g - 1) + 2 * (b - 1) + 4 * (a - 1)];
+  // ---- cal_curvature_derivative
+  B.bcurde1(1, 1, 1) = dot(S[0], n) + dot(cderi1[0], cderi3[0]);
+  B.bcurde1(2, 1, 1) = dot(S[1], n) + dot(cderi1[0], cderi3[1]);
+  B.bcurde1(1, 2, 2) = dot(S[2], n) + dot(cderi2[1], cderi3[0]);
+  B.bcurde1(2, 2, 2) = dot(S[3], n) + dot(cderi2[1], cderi3[1]);
+  B.bcurde1(1, 1, 2) = dot(S[1], n) + dot(cderi2[0], cderi3[0]);
+  B.bcurde1(1, 2, 1) = B.bcurde1(1, 1, 2);
+  B.bcurde1(2, 1, 2) = dot(S[2], n) + dot(cderi2[0], cderi3[1]);
+  B.bcurde1(2, 2, 1) = B.bcurde1(2, 1, 2);
+  double nS[3][3];  // cderiS3(:,1..3): n_tt, n_pp, n_tp
+  for (int c = 0; c < 3; ++c) {
+    nS[0][c] = -(B.bcurde1(1, 1, 1) * c1[c] + B.bcurde1(1, 2, 1) * c2[c] + B.bcur(1, 1) * conderi1[0][c] +
+                 B.bcur(1, 2) * conderi2[0][c]);
+    nS[1][c] = -(B.bcurde1(2, 1, 2) * c1[c] + B.bcurde1(2, 2, 2) * c2[c] + B.bcur(2, 1) * conderi1[1][c] +
+                 B.bcur(2, 2) * conderi2[1][c]);
+    nS[2][c] = -(B.bcurde1(2, 1, 1) * c1[c] + B.bcurde1(2, 2, 1) * c2[c] + B.bcur(1, 1) * conderi1[1][c] +
+                 B.bcur(1, 2) * conderi2[1][c]);
+  }
+  auto bd2 = [&](const double* t, const double* s1, const double* n1, const double* s2, const double* n2,
+                 const double* x, const double* ns) { return dot(t, n) + dot(s1, n1) + dot(s2, n2) + dot(x, ns); };
+  B.bcurde2(1, 1, 1, 1) = bd2(T[0], S[0], cderi3[0], S[0], cderi3[0], cderi1[0], nS[0]);
+  B.bcurde2(2, 1, 1, 1) = bd2(T[1], S[0], cderi3[1], S[1], cderi3[0], cderi1[0], nS[2]);
+  B.bcurde2(1, 2, 1, 1) = B.bcurde2(2, 1, 1, 1);
+  B.bcurde2(2, 2, 1, 1) = bd2(T[2], S[1], cderi3[1], S[1], cderi3[1], cderi1[0], nS[1]);
+  B.bcurde2(1, 1, 2, 2) = bd2(T[2], S[2], cderi3[0], S[2], cderi3[0], cderi2[1], nS[0]);
+  B.bcurde2(2, 1, 2, 2) = bd2(T[3], S[2], cderi3[1], S[3], cderi3[0], cderi2[1], nS[2]);
+  B.bcurde2(1, 2, 2, 2) = B.bcurde2(2, 1, 2, 2);
+  B.bcurde2(2, 2, 2, 2) = bd2(T[4], S[3], cderi3[1], S[3], cderi3[1], cderi2[1], nS[1]);
+  B.bcurde2(1, 1, 2, 1) = bd2(T[1], S[1], cderi3[0], S[1], cderi3[0], cderi1[1], nS[0]);
+  B.bcurde2(1, 1, 1, 2) = B.bcurde2(1, 1, 2, 1);
+  B.bcurde2(2, 1, 2, 1) = bd2(T[2], S[1], cderi3[1], S[2], cderi3[0], cderi1[1], nS[2]);
+  B.bcurde2(1, 2, 2, 1) = B.bcurde2(2, 1, 2, 1);
+  B.bcurde2(2, 1, 1, 2) = B.bcurde2(2, 1, 2, 1);
+  B.bcurde2(1, 2, 1, 2) = B.bcurde2(2, 1, 2, 1);
+  B.bcurde2(2, 2, 2, 1) = bd2(T[3], S[2], cderi3[1], S[2], cderi3[1], cderi1[1], nS[1]);
+  B.bcurde2(2, 2, 1, 2) = B.bcurde2(2, 2, 2, 1);
+  // ---- cal_contra_second_derivative: condeS1(:,1..3), condeS2(:,1..3)
+  double cS1[3][3], cS2[3][3];
+  {
+    const double* a1 = G.a1;
+    const double* a2 = G.a2;
+    const double* a1de[2] = {cderi1[0], cderi1[1]};
+    const double* a2de[2] = {cderi2[0], cderi2[1]};
+    const double* n3de[2] = {cderi3[0], cderi3[1]};
+    // adeS = cdeSvat: adeS(:,1) = S[0] (a1_tt), (:,2) = S[1], (:,3) = S[2], (:,4) = S[3]
+    double a2_n3[3], n3_a1[3], a2de_n3[2][3], a2_n3de[2][3], n3de_a1[2][3], n3_a1de[2][3];
+    cross(a2, n, a2_n3);
+    cross(n, a1, n3_a1);
+    for (int al = 0; al < 2; ++al) {
+      cross(a2de[al], n, a2de_n3[al]);
+      cross(a2, n3de[al], a2_n3de[al]);
+      cross(n3de[al], a1, n3de_a1[al]);
+      cross(n, a1de[al], n3_a1de[al]);
+    }
+    const double g = dot(a1, a2_n3);
+    double gde[2], gdeS[3];
+    for (int al = 0; al < 2; ++al) {
+      double vt[3];
+      for (int c = 0; c < 3; ++c) vt[c] = a2de_n3[al][c] + a2_n3de[al][c];
+      gde[al] = dot(a1de[al], a2_n3) + dot(a1, vt);
+    }
+    double a2_n3deS[3][3], a2de_n3de[2][2][3], a2deS_n3[3][3], n3_a1deS[3][3], n3de_a1de[2][2][3], n3deS_a1[3][3];
+    for (int al = 0; al < 3; ++al) cross(a2, nS[al], a2_n3deS[al]);
+    for (int al = 0; al < 2; ++al)
+      for (int al2 = 0; al2 < 2; ++al2) cross(a2de[al], n3de[al2], a2de_n3de[al][al2]);  // (:,al2,al)
+    cross(S[1], n, a2deS_n3[0]);
+    cross(S[3], n, a2deS_n3[1]);
+    cross(S[2], n, a2deS_n3[2]);
+    cross(n, S[0], n3_a1deS[0]);
+    cross(n, S[2], n3_a1deS[1]);
+    cross(n, S[1], n3_a1deS[2]);
+    for (int al = 0; al < 2; ++al)
+      for (int al2 = 0; al2 < 2; ++al2) cross(n3de[al], a1de[al2], n3de_a1de[al][al2]);  // (:,al2,al)
+    for (int al = 0; al < 3; ++al) cross(nS[al], a1, n3deS_a1[al]);
+    // gdeS(1..3): tt, pp, tp.  X(:,al2,al) is stored X[al][al2].
+    auto gdes = [&](const double* adeS_, int i1, int i2, int ia, int ib, const double* v3) {
+      double v1[3], v2[3];
+      for (int c = 0; c < 3; ++c) {
+        v1[c] = a2de_n3[ia][c] + a2_n3de[ia][c];
+        v2[c] = a2de_n3[ib][c] + a2_n3de[ib][c];
+      }
+      return dot(adeS_, a2_n3) + dot(a1de[i1], v1) + dot(a1de[i2], v2) + dot(a1, v3);
+    };
+    double v3[3][3];
+    for (int c = 0; c < 3; ++c) {
+      v3[0][c] = a2deS_n3[0][c] + a2de_n3de[0][0][c] + a2de_n3de[0][0][c] + a2_n3deS[0][c];
+      v3[1][c] = a2deS_n3[1][c] + a2de_n3de[1][1][c] + a2de_n3de[1][1][c] + a2_n3deS[1][c];
+      v3[2][c] = a2deS_n3[2][c] + a2de_n3de[0][1][c] + a2de_n3de[1][0][c] + a2_n3deS[2][c];
+    }
+    gdeS[0] = gdes(S[0], 0, 0, 0, 0, v3[0]);
+    gdeS[1] = gdes(S[2], 1, 1, 1, 1, v3[1]);
+    gdeS[2] = gdes(S[1], 0, 1, 1, 0, v3[2]);
+    const double ginv1 = 1. / g, ginv2 = ginv1 * ginv1, ginv3 = ginv1 * ginv2;
+    // (index pairs of the three second derivatives: tt -> (1,1), pp -> (2,2), tp -> (1,2))
+    const int I[3] = {0, 1, 0}, J[3] = {0, 1, 1};
+    for (int k = 0; k < 3; ++k) {
+      const int i = I[k], j = J[k];
+      double w1[3], w2[3];
+      for (int c = 0; c < 3; ++c) {
+        w1[c] = a2deS_n3[k][c] + a2de_n3de[i][j][c] + a2de_n3de[j][i][c] + a2_n3deS[k][c];
+        w2[c] = n3deS_a1[k][c] + n3de_a1de[i][j][c] + n3de_a1de[j][i][c] + n3_a1deS[k][c];
+      }
+      // condeS1(:,1) = 2 ginv3 gde(1) gde(1) a2_n3 - ginv2 gdeS(1) a2_n3 - ginv2 gde(1)(..)(:,1)
+      //               - ginv2 gde(1)(..)(:,1) + ginv1 (...); the tp entry pairs gde(2)gde(1),
+      //               gde(1) with (:,2) and gde(2) with (:,1)
+      const double gg = k == 2 ? gde[1] * gde[0] : gde[i] * gde[i];
+      for (int c = 0; c < 3; ++c) {
+        cS1[k][c] = 2 * ginv3 * gg * a2_n3[c] - ginv2 * gdeS[k] * a2_n3[c] -
+                    ginv2 * gde[i] * (a2de_n3[j][c] + a2_n3de[j][c]) -
+                    ginv2 * gde[j] * (a2de_n3[i][c] + a2_n3de[i][c]) + ginv1 * w1[c];
+        cS2[k][c] = 2 * ginv3 * gg * n3_a1[c] - ginv2 * gdeS[k] * n3_a1[c] -
+                    ginv2 * gde[i] * (n3de_a1[j][c] + n3_a1de[j][c]) -
+                    ginv2 * gde[j] * (n3de_a1[i][c] + n3_a1de[i][c]) + ginv1 * w2[c];
+      }
+    }
+  }
+  // ---- cal_christof, ibend part
+  auto CD = [&](const double* sv, const double* cv, const double* xd, const double* cd) {
+    return dot(sv, cv) + dot(xd, cd);
+  };
+  B.chrisderi(1, 1, 1, 1) = CD(S[0], c1, cderi1[0], conderi1[0]);
+  B.chrisderi(2, 1, 1, 1) = CD(S[1], c1, cderi1[0], conderi1[1]);
+  B.chrisderi(1, 2, 1, 1) = CD(S[1], c1, cderi1[1], conderi1[0]);
+  B.chrisderi(2, 2, 1, 1) = CD(S[2], c1, cderi1[1], conderi1[1]);
+  B.chrisderi(1, 1, 2, 1) = CD(S[0], c2, cderi1[0], conderi2[0]);
+  B.chrisderi(2, 1, 2, 1) = CD(S[1], c2, cderi1[0], conderi2[1]);
+  B.chrisderi(1, 2, 2, 1) = CD(S[1], c2, cderi1[1], conderi2[0]);
+  B.chrisderi(2, 2, 2, 1) = CD(S[2], c2, cderi1[1], conderi2[1]);
+  B.chrisderi(1, 2, 1, 2) = CD(S[2], c1, cderi2[1], conderi1[0]);
+  B.chrisderi(2, 2, 1, 2) = CD(S[3], c1, cderi1[1], conderi2[1]);  // as the reference writes it
+  B.chrisderi(1, 2, 2, 2) = CD(S[2], c2, cderi2[1], conderi2[0]);
+  B.chrisderi(2, 2, 2, 2) = CD(S[3], c2, cderi2[1], conderi2[1]);
+  for (int l = 1; l <= 2; ++l)
+    for (int b = 1; b <= 2; ++b) B.chrisderi(l, 1, b, 2) = B.chrisderi(l, 2, b, 1);
+  // ---- cal_contra_metric_second_deri: conatd2(l,lm,b,a), a^a_{lm l} . a^b + ...
+  const double* cv[2] = {c1, c2};
+  const double* cdv[2][2] = {{conderi1[0], conderi1[1]}, {conderi2[0], conderi2[1]}};  // [vec][al]
+  const double* cSv[2][3] = {{cS1[0], cS1[1], cS1[2]}, {cS2[0], cS2[1], cS2[2]}};   // [vec][tt,pp,tp]
+  auto CM = [&](int va, int vb, int s, int l1, int l2) {
+    return dot(cSv[va][s], cv[vb]) + dot(cdv[va][l1], cdv[vb][l2]) + dot(cdv[va][l2], cdv[vb][l1]) +
+           dot(cv[va], cSv[vb][s]);
+  };
+  B.conatd2(1, 1, 1, 1) = CM(0, 0, 0, 0, 0);
+  B.conatd2(2, 2, 1, 1) = CM(0, 0, 1, 1, 1);
+  B.conatd2(2, 1, 1, 1) = CM(0, 0, 2, 0, 1);
+  B.conatd2(1, 2, 1, 1) = B.conatd2(2, 1, 1, 1);
+  B.conatd2(1, 1, 2, 2) = CM(1, 1, 0, 0, 0);
+  B.conatd2(2, 2, 2, 2) = CM(1, 1, 1, 1, 1);
+  B.conatd2(2, 1, 2, 2) = CM(1, 1, 2, 0, 1);
+  B.conatd2(1, 2, 2, 2) = B.conatd2(2, 1, 2, 2);
+  B.conatd2(2, 1, 2, 1) = CM(0, 1, 2, 0, 1);
+  B.conatd2(1, 2, 2, 1) = B.conatd2(2, 1, 2, 1);
+  B.conatd2(2, 1, 1, 2) = B.conatd2(2, 1, 2, 1);
+  B.conatd2(1, 2, 1, 2) = B.conatd2(2, 1, 2, 1);
+  B.conatd2(1, 1, 2, 1) = CM(0, 1, 0, 0, 0);
+  B.conatd2(1, 1, 1, 2) = B.conatd2(1, 1, 2, 1);
+  B.conatd2(2, 2, 2, 1) = CM(0, 1, 1, 1, 1);
+  B.conatd2(2, 2, 1, 2) = B.conatd2(2, 2, 2, 1);
+}
+
+// cal_moment_deri (sph.f90:1236-1372), cal_Q (:1375-1424) and cal_bcurmix
+// (:1427-1454) at one point: X the deformed surface, R the reference
+// sphere (conAR.., BR.. of sph.f90:153-161), EB the bending modulus.
+void bend_q(BendTensors& X, BendTensors& R, double EB, BendQ& out) {
+  double mom[2][2] = {{0, 0}, {0, 0}}, momdF[2][2][2] = {}, momdS = 0;
+  auto a = [&](int i, int j) { return X.conat(i, j); };
+  auto ad1 = [&](int i, int j, int k) { return X.conatd1(i, j, k); };
+  auto ad2 = [&](int i, int j, int k, int l) { return X.conatd2(i, j, k, l); };
+  auto b = [&](int i, int j) { return X.bcur(i, j); };
+  auto bd1 = [&](int i, int j, int k) { return X.bcurde1(i, j, k); };
+  auto bd2 = [&](int i, int j, int k, int l) { return X.bcurde2(i, j, k, l); };
+  auto AR = [&](int i, int j) { return R.conat(i, j); };
+  auto ARd1 = [&](int i, int j, int k) { return R.conatd1(i, j, k); };
+  auto ARd2 = [&](int i, int j, int k, int l) { return R.conatd2(i, j, k, l); };
+  auto BRI = [&](int i, int j) { return R.bcur(i, j); };
+  auto BRId1 = [&](int i, int j, int k) { return R.bcurde1(i, j, k); };
+  auto BRId2 = [&](int i, int j, int k, int l) { return R.bcurde2(i, j, k, l); };
+  for (int al = 1; al <= 2; ++al)
+    for (int be = 1; be <= 2; ++be) {
+      for (int gam = 1; gam <= 2; ++gam)
+        for (int gamp = 1; gamp <= 2; ++gamp)
+          momdS = momdS + ad2(be, al, be, gam) * (AR(gamp, al) * BRI(gam, gamp) - a(gamp, al) * b(gam, gamp)) +
+                  ad1(al, be, gam) * (ARd1(be, gamp, al) * BRI(gam, gamp) + AR(gamp, al) * BRId1(be, gam, gamp) -
+                                      ad1(be, gamp, al) * b(gam, gamp) - a(gamp, al) * bd1(be, gam, gamp)) +
+                  ad1(be, be, gam) * (ARd1(al, gamp, al) * BRI(gam, gamp) + AR(gamp, al) * BRId1(al, gam, gamp) -
+                                      ad1(al, gamp, al) * b(gam, gamp) - a(gamp, al) * bd1(al, gam, gamp)) +
+                  a(be, gam) * (ARd2(be, al, gamp, al) * BRI(gam, gamp) + ARd1(al, gamp, al) * BRId1(be, gam, gamp) +
+                                ARd1(be, gamp, al) * BRId1(al, gam, gamp) + AR(gamp, al) * BRId2(be, al, gam, gamp) -
+                                ad2(be, al, gamp, al) * b(gam, gamp) - ad1(al, gamp, al) * bd1(be, gam, gamp) -
+                                ad1(be, gamp, al) * bd1(al, gam, gamp) - a(gamp, al) * bd2(be, al, gam, gamp));
+      if (al == 2 && be == 1) continue;
+      for (int gam = 1; gam <= 2; ++gam)
+        for (int gamp = 1; gamp <= 2; ++gamp)
+          mom[be - 1][al - 1] = mom[be - 1][al - 1] + a(be, gam) * (AR(gamp, al) * BRI(gam, gamp) -
+                                                                  a(gamp, al) * b(gam, gamp));
+      for (int l = 1; l <= 2; ++l)
+        for (int gam = 1; gam <= 2; ++gam)
+          for (int gamp = 1; gamp <= 2; ++gamp)
+            momdF[l - 1][be - 1][al - 1] =
+                momdF[l - 1][be - 1][al - 1] +
+                ad1(l, be, gam) * (AR(gamp, al) * BRI(gam, gamp) - a(gamp, al) * b(gam, gamp)) +
+                a(be, gam) * (ARd1(l, gamp, al) * BRI(gam, gamp) + AR(gamp, al) * BRId1(l, gam, gamp) -
+                              ad1(l, gamp, al) * b(gam, gamp) - a(gamp, al) * bd1(l, gam, gamp));
+    }
+  mom[0][1] = mom[1][0];
+  for (int l = 0; l < 2; ++l) momdF[l][0][1] = momdF[l][1][0];
+  for (int i = 0; i < 2; ++i)
+    for (int j = 0; j < 2; ++j) {
+      mom[i][j] = mom[i][j] * EB;
+      for (int l = 0; l < 2; ++l) momdF[l][i][j] = momdF[l][i][j] * EB;
+    }
+  momdS = momdS * EB;
+  // cal_Q: Q(be), Qcode = Q^be|be
+  auto M = [&](int i, int j) { return mom[i - 1][j - 1]; };
+  auto MF = [&](int l, int i, int j) { return momdF[l - 1][i - 1][j - 1]; };
+  auto CH = [&](int g, int bb, int aa) { return X.christof(g, bb, aa); };
+  auto CHD = [&](int l, int g, int bb, int aa) { return X.chrisderi(l, g, bb, aa); };
+  double Q[2] = {0, 0}, Qcode = momdS;
+  for (int be = 1; be <= 2; ++be)
+    for (int al = 1; al <= 2; ++al) {
+      Q[be - 1] = Q[be - 1] + MF(al, be, al);
+      for (int lm = 1; lm <= 2; ++lm) {
+        Q[be - 1] = Q[be - 1] + CH(lm, al, al) * M(be, lm) + CH(lm, be, al) * M(lm, al);
+        Qcode = Qcode + CHD(be, lm, al, al) * M(be, lm) + CH(lm, al, al) * MF(be, be, lm) +
+                CHD(be, lm, be, al) * M(lm, al) + CH(lm, be, al) * MF(be, lm, al);
+      }
+    }
+  for (int be = 1; be <= 2; ++be)
+    for (int lm = 1; lm <= 2; ++lm) Qcode = Qcode + Q[lm - 1] * CH(lm, be, be);
+  // cal_bcurmix: bcurmix(be,al) = sum_lm conat(lm,al) bcur(be,lm)
+  for (int al = 1; al <= 2; ++al)
+    for (int be = 1; be <= 2; ++be) {
+      double v = 0;
+      for (int lm = 1; lm <= 2; ++lm) v = v + a(lm, al) * b(be, lm);
+      out.bm[be - 1][al - 1] = v;
+    }
+  out.Q[0] = Q[0];
+  out.Q[1] = Q[1];
+  out.Qcode = Qcode;
 }
 
 // Reference-sphere setup (capsule_init_cal_coeff, sph.f90:16-191).
@@ -515,18 +884,22 @@ std::shared_ptr<Capsule> build_capsule(int L, double R) {
   C->wD.resize(C->nD);
   gauss(C->nO, C->thO.data(), C->wO.data());
   gauss(C->nD, C->thD.data(), C->wD.data());
-  std::vector<double> T, D, D2;
+  std::vector<double> T, D, D2, D3, D4;
   C->PD.assign((size_t)C->nD * N * N, 0.0);
   C->dPD = C->PD;
   C->d2PD = C->PD;
+  C->d3PD = C->PD;
+  C->d4PD = C->PD;
   for (int i = 0; i < C->nD; ++i) {
-    legendre_full(C->thD[i], N + 2, T, D, D2);
+    legendre_full4(C->thD[i], N + 2, T, D, D2, D3, D4);
     for (int m = 0; m < N; ++m)
       for (int n = m; n < N; ++n) {
         size_t o = ((size_t)i * N + m) * N + n;
         C->PD[o] = T[(size_t)m * (N + 2) + n];
         C->dPD[o] = D[(size_t)m * (N + 2) + n];
         C->d2PD[o] = D2[(size_t)m * (N + 2) + n];
+        C->d3PD[o] = D3[(size_t)m * (N + 2) + n];
+        C->d4PD[o] = D4[(size_t)m * (N + 2) + n];
       }
   }
   C->PO.assign((size_t)C->nO * N * N, 0.0);
@@ -590,6 +963,17 @@ std::shared_ptr<Capsule> build_capsule(int L, double R) {
       C->conARd1[p * 8 + al * 4 + 3] = G.conatd1[al][1];
       C->conARd1[p * 8 + al * 4 + 1] = G.conatd1[al][2];
       C->conARd1[p * 8 + al * 4 + 2] = G.conatd1[al][2];
+    }
+  }
+  // the reference sphere's bending tensors (cal_contra_metric_deri with
+  // ibend = 1, sph.f90:153-161, 193-299)
+  {
+    std::vector<double> f42;
+    synth_basis_bend(*C, a.data(), b.data(), f42);
+    C->refB.resize(np);
+    for (size_t p = 0; p < np; ++p) {
+      geometry(&f42[p * 42], G);
+      bend_tensors(G, (const double(*)[3]) & f42[p * 42 + 15], (const double(*)[3]) & f42[p * 42 + 27], C->refB[p]);
     }
   }
   return C;
@@ -658,7 +1042,7 @@ void surface_metric(const Capsule& C, const double* a, const double* b, double* 
 int capsule_force(int L, double R, double gs, double csk, int law, bool faithful,
                   const double* xfp, const double* yfp, const double* zfp,
                   double* fxl, double* fyl, double* fzl, double* xn, double* yn, double* zn, double* area,
-                  double* shape_a, double* shape_b, double* force_a, double* force_b) {
+                  double* shape_a, double* shape_b, double* force_a, double* force_b, double eb = 0.0) {
   if (L < 2 || L > 63 || !(R > 0)) return 1;
   auto Cp = get_capsule(L, R);
   const Capsule& C = *Cp;
@@ -692,16 +1076,30 @@ int capsule_force(int L, double R, double gs, double csk, int law, bool faithful
   for (int c = 0; c < 3; ++c) analysis(*pO, &xs[c * nS], &a[(size_t)c * N * N], &b[(size_t)c * N * N]);
   if (shape_a) std::memcpy(shape_a, a.data(), sizeof(double) * a.size());
   if (shape_b) std::memcpy(shape_b, b.data(), sizeof(double) * b.size());
-  // (3) geometry + mechanics on the dealias grid
-  std::vector<double> f15;
-  synth_basis(C, a.data(), b.data(), f15);
+  // (3) geometry + mechanics on the dealias grid; with bending (eb != 0,
+  // ibend = 1) the third and fourth derivatives, the moment and transverse
+  // shear terms of cal_spectral_force (sph.f90:1636-1709)
   std::vector<double> fN(3 * nF), unitN(3 * nF);
   const double hf = 0.5 * gs;  // sph.f90:35 hf_gscell
   Geo G;
+  const int nv = eb != 0.0 ? 42 : 15;
+  std::vector<double> fv;
+  if (eb != 0.0)
+    synth_basis_bend(C, a.data(), b.data(), fv);
+  else
+    synth_basis(C, a.data(), b.data(), fv);
   for (size_t p = 0; p < nF; ++p) {
-    geometry(&f15[p * 15], G);
+    geometry(&fv[p * nv], G);
     double f[3];
-    mechanics(G, &C.conAR[p * 4], &C.conARd1[p * 8], hf, csk, law, f);
+    if (eb != 0.0) {
+      BendTensors X;
+      BendQ bq;
+      bend_tensors(G, (const double(*)[3]) & fv[p * nv + 15], (const double(*)[3]) & fv[p * nv + 27], X);
+      bend_q(X, const_cast<BendTensors&>(C.refB[p]), eb, bq);
+      mechanics(G, &C.conAR[p * 4], &C.conARd1[p * 8], hf, csk, law, f, &bq);
+    } else {
+      mechanics(G, &C.conAR[p * 4], &C.conARd1[p * 8], hf, csk, law, f);
+    }
     for (int c = 0; c < 3; ++c) {
       fN[c * nF + p] = f[c];
       unitN[c * nF + p] = G.n[c];
@@ -1032,6 +1430,13 @@ int or_complagrforces(int L, double radius, double gs, double csk, int faithful,
 }
 
 // complagrforces with a chosen membrane law (0 Skalak, 1 neo-Hookean)
+int or_complagrforces_bend(int L, double radius, double gs, double csk, int law, double eb, int faithful,
+                           const double* xfp, const double* yfp, const double* zfp, double* fx, double* fy,
+                           double* fz, double* nx, double* ny, double* nz, double* area) {
+  return capsule_force(L, radius, gs, csk, law, faithful != 0, xfp, yfp, zfp, fx, fy, fz, nx, ny, nz, area, nullptr,
+                       nullptr, nullptr, nullptr, eb);
+}
+
 int or_complagrforces_law(int L, double radius, double gs, double csk, int law, int faithful, const double* xfp,
                           const double* yfp, const double* zfp, double* fx, double* fy, double* fz, double* nx,
                           double* ny, double* nz, double* area) {

@@ -58,6 +58,18 @@ int or_complagrforces_law(int L, double radius, double gs, double csk, int law, 
                           double* fx, double* fy, double* fz,
                           double* nx, double* ny, double* nz, double* area);
 
+/* Same with the bending terms of ibend = 1 (param.f90:90-91): eb is the
+ * bending modulus (ebend = cbend gscell); the third and fourth derivatives of
+ * the shape (sph3.f90:137-180), the curvature and metric derivatives
+ * (sph.f90:479-731, 802-890, 962-1111, sph1.f90:299-542), the moment, the
+ * transverse shear and their terms in the equilibrium (sph.f90:1236-1454,
+ * 1705-1709), with the reference sphere's tensors as the reference state.
+ * eb = 0 gives or_complagrforces_law. */
+int or_complagrforces_bend(int L, double radius, double gs, double csk, int law, double eb, int faithful,
+                           const double* xfp, const double* yfp, const double* zfp,
+                           double* fx, double* fy, double* fz,
+                           double* nx, double* ny, double* nz, double* area);
+
 /* Same, but also returns the dealias-grid pointwise force before filtering
  * (fxN..) and the shape coefficients; used by the surrogate data path tests.
  * coef: [3][m*N+n] a then b (each 3*N*N); fcoef: force coefficients (degree<N)

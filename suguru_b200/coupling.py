@@ -40,7 +40,7 @@ EXPORTS = ["sg_create", "sg_destroy", "sg_last_error", "sg_synchronize", "sg_int
            "sg_set_tensor_cores", "sg_set_legendre_terms", "sg_get_legendre_terms", "sg_set_capsule_law",
            "sg_set_legendre_tile_rows", "sg_get_legendre_tile_rows", "sg_set_wall_collisions", "sg_collisions",
            "sg_set_indicator_params", "sg_indicator", "sg_set_flow_params", "sg_flow_step",
-           "sg_contraction_work"]
+           "sg_contraction_work", "sg_set_capsule_bending"]
 # test hooks declared in include/sg_testing.h
 TEST_EXPORTS = ["sg_test_legendre", "sg_test_gemm", "sg_test_mlp_grad"]
 WORKLOAD_EXPORTS = ["sg_prescribed_flow"]  # include/sg_workload.h
@@ -106,6 +106,7 @@ def lib():
     L.sg_set_point_split.argtypes = [vp, ctypes.c_int]
     L.sg_set_tensor_cores.argtypes = [vp, ctypes.c_int]
     L.sg_set_capsule_law.argtypes = [vp, vp]
+    L.sg_set_capsule_bending.argtypes = [vp, vp]
     L.sg_set_legendre_tile_rows.argtypes = [vp, ctypes.c_int]
     L.sg_get_legendre_tile_rows.argtypes = [vp]
     L.sg_set_legendre_terms.argtypes = [vp, ctypes.c_int]
@@ -342,6 +343,12 @@ class CouplingStep:
         law = np.ascontiguousarray(law, dtype=np.int32)
         assert law.size == self.degree.size
         self._check(lib().sg_set_capsule_law(self._h, law.ctypes.data_as(ctypes.c_void_p)), "sg_set_capsule_law")
+
+    def set_capsule_bending(self, eb):
+        """Bending modulus per capsule (0 = the ibend = 0 force; sph.f90:1705-1709)."""
+        eb = np.ascontiguousarray(np.broadcast_to(np.asarray(eb, dtype=np.float64), self.degree.shape))
+        self._check(lib().sg_set_capsule_bending(self._h, eb.ctypes.data_as(ctypes.c_void_p)),
+                    "sg_set_capsule_bending")
 
     def set_legendre_tile_rows(self, rows):
         """Data rows per tensor-core Legendre tile: 128 or 64 (results do not depend on it)."""

@@ -26,6 +26,9 @@ constexpr int kSixTermDegree = 16;
 
 int terms_for(const sg_ctx* c, int degree) {
   if (c->leg_terms) return c->leg_terms;
+  // the bending terms take fourth derivatives of the analysed shape, which
+  // amplify the product error about as L^4: FP32-level products throughout
+  if (c->bend) return 6;
   return degree >= kSixTermDegree ? 6 : 3;
 }
 
@@ -149,6 +152,109 @@ LegProblem prob(const void* A, long long sAc, long long sAr, long long sAm, cons
   return p;
 }
 
+// The per-group constants the kernels read (tables, buffers) to the device.
+int upload_groups(sg_ctx* c) {
+  std::vector<GroupDev> gdev(c->groups.size());
+  for (size_t gi = 0; gi < c->groups.size(); ++gi) {
+    const Group& gr = c->groups[gi];
+    GroupDev& d = gdev[gi];
+    d.L = gr.L; d.N = gr.N; d.nD = gr.nD; d.mD = gr.mD; d.nO = gr.nO; d.mO = gr.mO;
+    for (int q = 0; q < 2; ++q) {
+      d.latD[q] = gr.tab.latD[q]; d.latO[q] = gr.tab.latO[q];
+      d.trigD[q] = gr.tab.trigD[q]; d.trigO[q] = gr.tab.trigO[q];
+    }
+    d.buf = gr.buf;
+  }
+  if (!gdev.empty())
+    SG_TRY(cudaMemcpy(c->d_groups, gdev.data(), sizeof(GroupDev) * gdev.size(), cudaMemcpyHostToDevice), "groups");
+  return SG_OK;
+}
+
+// Bending set-up (first sg_set_capsule_bending with a nonzero modulus): per
+// degree group the FP64 table of the third and fourth theta derivatives
+// (kind 4: syn_B[m][kind nD + i][n], m = 0 halved as the other synthesis
+// tables, sph3.f90:72-102), the buffer GB of their series, and the synthesis
+// problem S1b (A = the shape's coefficients, as S1), with its work lists for
+// the CUDA-core and the tensor-core launch.
+int bend_setup(sg_ctx* c) {
+  if (c->bend_ready) return SG_OK;
+  const size_t E = c->esz;
+  const int pi = c->mixed ? 1 : 0;
+  std::vector<LegProblem> P = c->h_probs;
+  std::vector<LegWork> W, WT;
+  int maxJ = 0, maxK = 0;
+  std::vector<int> ids;
+  for (size_t gi = 0; gi < c->groups.size(); ++gi) {
+    Group& gr = c->groups[gi];
+    const int N = gr.N, nD = gr.nD, n = (int)gr.caps.size();
+    std::vector<double> th(nD), wq(nD), d3((size_t)N * N), d4((size_t)N * N);
+    host_gauss(nD, th.data(), wq.data());
+    std::vector<double> synB((size_t)N * 2 * nD * N, 0.0);
+    for (int i = 0; i < nD; ++i) {
+      host_legendre_d34(th[i], N, N, d3.data(), d4.data());
+      for (int m = 0; m < N; ++m) {
+        const double h = (m == 0) ? 0.5 : 1.0;
+        for (int q = 0; q < N; ++q) {
+          synB[((size_t)m * 2 * nD + 0 * nD + i) * N + q] = h * d3[(size_t)m * N + q];
+          synB[((size_t)m * 2 * nD + 1 * nD + i) * N + q] = h * d4[(size_t)m * N + q];
+        }
+      }
+    }
+    gr.h_tab[4] = synB;
+    SG_TRY(upload2<double>(c, gr.tab.syn_B, synB), "bending tables");
+    SG_TRY(dalloc(c, gr.buf.GB, E * (size_t)n * 12 * N * nD), "alloc");
+    const long long LN = N, LD = nD;
+    ids.push_back((int)P.size());
+    add_problem(P, W, prob(gr.buf.Cpos, 6 * LN * LN, LN * LN, LN, gr.tab.syn_B[pi], 2 * LD * LN, gr.buf.GB,
+                           6 * LN * 2 * LD, LN * 2 * LD, 2 * LD, 6, n, N, 2 * nD, N, 1, (int)gi, 4),
+                maxJ, maxK);
+  }
+  if (c->mixed) {
+    std::vector<uint16_t> img;
+    std::vector<size_t> off;
+    LegLevels lv{};
+    for (int id : ids) {
+      LegProblem& p = P[id];
+      p.Jp = (p.J + 15) / 16 * 16;
+      p.Kp = (p.K + 15) / 16 * 16;
+      p.sBimg = 3LL * p.Jp * p.Kp;
+      off.push_back(img.size());
+      img.resize(img.size() + (size_t)p.M * p.sBimg);
+      const std::vector<double>& hb = c->groups[p.group].h_tab[4];
+      host_umma_image(hb.data(), p.sBm, p.M, p.J, p.K, p.Jp, p.Kp, img.data() + off.back());
+      auto al4 = [](const void* ptr) { return ((uintptr_t)ptr & 15u) == 0; };
+      p.vecA = (al4(p.A) && p.sAc % 4 == 0 && p.sAr % 4 == 0 && p.sAm % 4 == 0 && p.K % 8 == 0) ? 1 : 0;
+      p.vecD = (al4(p.D) && p.sDc % 4 == 0 && p.sDr % 4 == 0 && p.sDm % 4 == 0 && p.J % 4 == 0) ? 1 : 0;
+      lv.jp[0] = std::max(lv.jp[0], p.Jp);
+      lv.kp[0] = std::max(lv.kp[0], p.Kp);
+      lv.a_kp = std::max(lv.a_kp, p.Kp);
+      for (int m = 0; m < p.M; ++m)
+        for (int q0 = 0; q0 < p.Q; q0 += 128) WT.push_back(LegWork{id, m, q0});
+    }
+    void* dimg = nullptr;
+    SG_TRY(upload(c, dimg, img), "umma images");
+    for (size_t k = 0; k < ids.size(); ++k) P[ids[k]].Bimg = (const uint16_t*)dimg + off[k];
+    c->lvB = lv;
+    void* tmp = nullptr;
+    SG_TRY(upload(c, tmp, WT), "work");
+    c->d_lwBT = (LegWork*)tmp;
+    c->nlwBT = (int)WT.size();
+  }
+  void* tmp = nullptr;
+  SG_TRY(upload(c, tmp, W), "work");
+  c->d_lwB = (LegWork*)tmp;
+  c->nlwB = (int)W.size();
+  c->maxJB = maxJ;
+  c->maxKB = maxK;
+  c->h_probs = P;
+  assign_terms(c, c->h_probs);
+  SG_TRY(upload(c, tmp, c->h_probs), "problems");
+  c->d_probs = (LegProblem*)tmp;
+  SG_RET(upload_groups(c));
+  c->bend_ready = true;
+  return SG_OK;
+}
+
 // Work items of the persistent pointwise kernels: every capsule split into
 // `split` row ranges (each item stages the capsule's whole input block),
 // largest degree first so that the heaviest items start early.  More items
@@ -250,23 +356,12 @@ int setup(sg_ctx* c) {
     SG_TRY(dalloc(c, gr.buf.Csh, E * n * 8 * N * N), "alloc");
     SG_TRY(dalloc(c, gr.buf.GF, E * n * 14 * N * gr.nD), "alloc");
   }
-  std::vector<GroupDev> gdev(c->groups.size());
-  for (size_t gi = 0; gi < c->groups.size(); ++gi) {
-    const Group& gr = c->groups[gi];
-    GroupDev& d = gdev[gi];
-    d.L = gr.L; d.N = gr.N; d.nD = gr.nD; d.mD = gr.mD; d.nO = gr.nO; d.mO = gr.mO;
-    for (int q = 0; q < 2; ++q) {
-      d.latD[q] = gr.tab.latD[q]; d.latO[q] = gr.tab.latO[q];
-      d.trigD[q] = gr.tab.trigD[q]; d.trigO[q] = gr.tab.trigO[q];
-    }
-    d.buf = gr.buf;
-  }
   void* tmp = nullptr;
   SG_TRY(upload(c, tmp, caps), "caps");
   c->d_caps = (CapInfo*)tmp;
   c->h_caps = caps;
-  SG_TRY(upload(c, tmp, gdev), "groups");
-  c->d_groups = (GroupDev*)tmp;
+  SG_TRY(dalloc(c, c->d_groups, sizeof(GroupDev) * std::max<size_t>(c->groups.size(), 1)), "alloc");
+  SG_RET(upload_groups(c));
   // capsule work lists of the persistent pointwise kernels (set_point_split)
   const size_t maxitems = (size_t)kMaxPointSplit * std::max(ncap, 1);
   SG_TRY(dalloc(c, c->d_wpos, sizeof(RowWork) * maxitems), "alloc");
@@ -510,9 +605,25 @@ int dev_forces(sg_ctx* c, const double* X, const double* Y, const double* Z, T* 
   const bool f32 = sizeof(T) == 4;
   if (f32) SG_RET(sur_step_pre(c));  // surrogate force and its residual check
   SG_RET(dev_legendre<T>(c, 1));
-  SG_TRY(launch_membrane<T>(c->d_wmem, c->nwmem, c->d_caps, c->d_groups, f32 ? sur_flags(c) : nullptr, c->nmax,
-                            c->d_err, c->st),
-         "membrane");
+  if (c->bend) {
+    // the third and fourth derivative series of the shape (problem S1b)
+    SG_RET(con_mark(c, 0));
+    if (f32 && c->leg_tc)
+      SG_TRY(launch_legendre_mma(c->d_probs, c->d_lwBT, c->nlwBT, c->lvB, c->leg_parts, 128, c->d_err, c->num_sms,
+                                 c->st),
+             "legendre (bending)");
+    else
+      SG_TRY(launch_legendre<T>(c->d_probs, c->d_lwB, c->nlwB, c->maxJB, c->maxKB, c->st), "legendre (bending)");
+    SG_RET(con_mark(c, 1));
+    c->launches += 1;
+    SG_TRY(launch_membrane_bend<T>(c->d_wmem, c->nwmem, c->d_caps, c->d_groups, f32 ? sur_flags(c) : nullptr,
+                                   c->nmax, c->st),
+           "membrane (bending)");
+  } else {
+    SG_TRY(launch_membrane<T>(c->d_wmem, c->nwmem, c->d_caps, c->d_groups, f32 ? sur_flags(c) : nullptr, c->nmax,
+                              c->d_err, c->st),
+           "membrane");
+  }
   SG_RET(dev_legendre<T>(c, 2));
   if (f32) SG_RET(sur_step_post(c));
   SG_RET(dev_legendre<T>(c, 3));
@@ -1049,6 +1160,27 @@ int sg_set_profiling(sg_ctx* c, int on) {
       for (int k = 0; k < sg_ctx::kMaxContract; ++k) SG_TRY(cudaEventCreate(&c->ev_con[e][k]), "cudaEventCreate");
   }
   c->profiling = on != 0;
+  return SG_OK;
+}
+
+int sg_set_capsule_bending(sg_ctx* c, const double* eb) {
+  if (!c) return SG_ERR_ARG;
+  if (c->graph) return fail(c, SG_ERR_STATE, "release the captured graph first");
+  bool any = false;
+  for (int k = 0; k < c->cfg.ncap; ++k) {
+    const double v = eb ? eb[k] : 0.0;
+    if (!std::isfinite(v)) return fail(c, SG_ERR_ARG, "bending modulus must be finite");
+    any = any || v != 0.0;
+  }
+  SG_TRY(cudaStreamSynchronize(c->st), "synchronize");
+  if (any) SG_RET(bend_setup(c));
+  for (int k = 0; k < c->cfg.ncap; ++k) c->h_caps[k].eb = eb ? eb[k] : 0.0;
+  c->bend = any;
+  assign_terms(c, c->h_probs);
+  SG_TRY(cudaMemcpy(c->d_probs, c->h_probs.data(), sizeof(LegProblem) * c->h_probs.size(), cudaMemcpyHostToDevice),
+         "problems");
+  SG_TRY(cudaMemcpy(c->d_caps, c->h_caps.data(), sizeof(CapInfo) * c->h_caps.size(), cudaMemcpyHostToDevice),
+         "upload");
   return SG_OK;
 }
 

@@ -18,7 +18,7 @@ struct Group {
   std::vector<int> caps;
   DegreeTables tab;
   SpecBuffers buf{};
-  std::vector<double> h_tab[4];  // host FP64 syn_D, ana_D, syn_O, ana_O (by LegProblem::kind)
+  std::vector<double> h_tab[5];  // host FP64 syn_D, ana_D, syn_O, ana_O, syn_B (by LegProblem::kind)
 };
 
 }  // namespace sg
@@ -112,6 +112,15 @@ struct sg_ctx {
   cudaEvent_t ev_con[2][kMaxContract] = {};
   int ncon = 0;
   std::vector<int> leg_roots[3];  // root problems of the three tensor-core launches
+  // bending (sg_set_capsule_bending): the synthesis of the third and fourth
+  // theta derivatives, one problem per group, as its own contraction launch
+  bool bend = false;        // some capsule has a nonzero bending modulus
+  bool bend_ready = false;  // tables, buffers and problems set up
+  LegWork* d_lwB = nullptr;   // CUDA-core work list (32-row tiles)
+  int nlwB = 0, maxJB = 0, maxKB = 0;
+  LegWork* d_lwBT = nullptr;  // tensor-core work list (128-row tiles)
+  int nlwBT = 0;
+  LegLevels lvB{};
   int max_tiles = 0;            // binning arrays are sized for the largest tile count
   bool capturing = false;       // inside sg_graph_capture: no synchronisation, no events
   cudaGraph_t graph = nullptr;  // captured step (device memory mode)
@@ -134,12 +143,14 @@ struct sg_ctx {
   void* spec_scratch[7] = {};
   // solver1d on the GPU (sg_poisson.cu), shared by the indicator and the flow solver
   struct PoissonState {
-    bool ready = false, have_plans = false;
+    bool ready = false;
     double* r = nullptr;     // real FFT input / output [ktot][jtot][itot]
-    void* c = nullptr;       // modes [ktot][jtot][itot/2 + 1] (double2)
-    double* d = nullptr;     // elimination multipliers [ktot][modes]
+    void* c = nullptr;       // modes [ktot][jtot][nmp] (double2), nmp = itot/2 + 1 rounded up to 8
+    double* d = nullptr;     // elimination multipliers [ktot][jtot][nmp] (only when ktot > 288)
     double* tab = nullptr;   // xrt [itot/2 + 1], yrt [jtot]
-    int plan_f = 0, plan_b = 0;  // cufftHandle
+    double2* w = nullptr;    // twiddles of the row and column FFTs, then the row split's W^k
+    double2* wpost = nullptr;
+    alignas(8) unsigned char plan_x[128], plan_y[128];  // FFT plans (factorisations), see sg_poisson.cu
   } pois;
   // indicator function (sg_indicator.cu), set up by sg_set_indicator_params
   struct IndState {
@@ -197,10 +208,18 @@ int run_forces_only(sg_ctx* c, const double* X, const double* Y, const double* Z
 // solver1d (sg_poisson.cu): FFT buffers and plans made once per context;
 // poisson_solve replaces r ([ktot][jtot][itot], interior values) with
 // itot * jtot times the solution of the rows of initsolver(e) (shift = Rep/dt
-// for e = 2, 3): the FFT pair is left unnormalised.
+// for e = 2, 3): the FFT pair is left unnormalised.  With out, the solution
+// times out->scale goes to the interior of a field with a one-cell halo
+// instead (value (i, j, k), 0-based, at f[(k+1) plane + (j+1) ldi + i+1]),
+// and r is left holding intermediate values.
+struct PoisOut {
+  double* f;
+  long ldi, plane;
+  double scale;
+};
 int poisson_setup(sg_ctx* c);
 void poisson_free(sg_ctx* c);
-int poisson_solve(sg_ctx* c, double* r, int e, double shift, cudaStream_t st);
+int poisson_solve(sg_ctx* c, double* r, int e, double shift, cudaStream_t st, const PoisOut* out = nullptr);
 // indicator function (sg_indicator.cu)
 int indicator_setup(sg_ctx* c, double visc0, double lambda, double thetainc, double ta, double rep);
 template <class T>

@@ -119,16 +119,6 @@ __global__ void __launch_bounds__(256) momentum_rhs_kernel(FGrid g, Fields F, do
   rw[q] = k == g.ktot ? 0.0 : momentum_rhs<2>(g, F, dt, rep, i, j, k);  // dwdt(i,j,kmax) = 0 (fftuvw.f90:86-92)
 }
 
-// interior values of a field from a solution (times the FFT pair's 1/n)
-__global__ void from_solution_kernel(FGrid g, const double* __restrict__ sol, double inv_n, double* __restrict__ f) {
-  const long n = (long)g.itot * g.jtot * g.ktot;
-  const long q = (long)blockIdx.x * blockDim.x + threadIdx.x;
-  if (q >= n) return;
-  int i, j, k;
-  cell_of(g, q, i, j, k);
-  f[at(g, i, j, k)] = sol[q] * inv_n;
-}
-
 // bounduvw (mode 0: u; 1: v with wall values vb2, vt2; 2: w) or boundp (mode
 // 3) on the cells outside the interior, from the rule of bound.f90:7-139 at
 // the interior column each copies.  One thread per halo cell: the two z
@@ -256,19 +246,18 @@ int flow_run(sg_ctx* c, double dt, const double* uo, const double* vo, const dou
   const dim3 mgrid((unsigned)(((f.itot + 31) / 32) * ((f.jtot + 7) / 8)), (unsigned)f.ktot);
   momentum_rhs_kernel<<<mgrid, 256, 0, st>>>(g, F, dt, s.rep, s.ru, s.rv, rw);
   SG_TRY(cudaGetLastError(), "momentum");
-  SG_RET(poisson_solve(c, rw, 3, shift, st));
-  from_solution_kernel<<<blocks(nreal), 256, 0, st>>>(g, rw, inv_n, w);
-  SG_RET(poisson_solve(c, s.ru, 2, shift, st));
-  from_solution_kernel<<<blocks(nreal), 256, 0, st>>>(g, s.ru, inv_n, u);
-  SG_RET(poisson_solve(c, s.rv, 2, shift, st));
-  from_solution_kernel<<<blocks(nreal), 256, 0, st>>>(g, s.rv, inv_n, v);
+  // each solution goes, times 1 / (itot jtot), straight into its field
+  const PoisOut ow{w, g.ldi, g.plane, inv_n}, ou{u, g.ldi, g.plane, inv_n}, ov{v, g.ldi, g.plane, inv_n},
+      op{s.p, g.ldi, g.plane, inv_n};
+  SG_RET(poisson_solve(c, rw, 3, shift, st, &ow));
+  SG_RET(poisson_solve(c, s.ru, 2, shift, st, &ou));
+  SG_RET(poisson_solve(c, s.rv, 2, shift, st, &ov));
   halo_kernel<<<blocks(nf), 256, 0, st>>>(g, 0, s.vb2, s.vt2, u);
   halo_kernel<<<blocks(nf), 256, 0, st>>>(g, 1, s.vb2, s.vt2, v);
   halo_kernel<<<blocks(nf), 256, 0, st>>>(g, 2, s.vb2, s.vt2, w);
   // projection: fillps, solver1d after initsolver(1), boundp, correc, bounduvw
   fillps_kernel<<<blocks(nreal), 256, 0, st>>>(g, 1.0 / dt, u, v, w, rw);
-  SG_RET(poisson_solve(c, rw, 1, 0.0, st));
-  from_solution_kernel<<<blocks(nreal), 256, 0, st>>>(g, rw, inv_n, s.p);
+  SG_RET(poisson_solve(c, rw, 1, 0.0, st, &op));
   halo_kernel<<<blocks(nf), 256, 0, st>>>(g, 3, 0.0, 0.0, s.p);
   correc_kernel<<<blocks(nreal), 256, 0, st>>>(g, dt, s.p, u, v, w);
   halo_kernel<<<blocks(nf), 256, 0, st>>>(g, 0, s.vb2, s.vt2, u);
@@ -278,7 +267,7 @@ int flow_run(sg_ctx* c, double dt, const double* uo, const double* vo, const dou
   add_interior_kernel<<<blocks(nreal), 256, 0, st>>>(g, s.p, p);
   halo_kernel<<<blocks(nf), 256, 0, st>>>(g, 3, 0.0, 0.0, p);
   SG_TRY(cudaGetLastError(), "flow step");
-  c->launches += 15;
+  c->launches += 12;
   return SG_OK;
 }
 

@@ -72,6 +72,8 @@ void host_gauss(int n, double* th, double* w);
 // SPHEREPACK-normalised P, dP/dtheta, d2P/dtheta2 at one colatitude as
 // [m*nn+n] for m<mm, n<nn (zero for n<m).
 void host_legendre(double th, int mm, int nn, double* P, double* dP, double* d2P);
+// The third and fourth theta derivatives, same layout.
+void host_legendre_d34(double th, int mm, int nn, double* d3P, double* d4P);
 
 // ---------------------------------------------------------- spectral stage --
 // Per-degree constant data on the device (built from FP64 host tables).
@@ -86,6 +88,8 @@ struct DegreeTables {
   void* ana_D[2] = {nullptr, nullptr};
   void* syn_O[2] = {nullptr, nullptr};
   void* ana_O[2] = {nullptr, nullptr};
+  //  syn_B : j = kind*nD + i (kind 0: d3P, 1: d4P, m=0 row halved), k = n   (J=2nD, K=N; bending)
+  void* syn_B[2] = {nullptr, nullptr};
   // per-latitude data: sin, cos of theta on both grids, area weight w/sin*dphi
   void* latD[2] = {nullptr, nullptr};  // [nD][4]: sin, cos, wgtdsinf, theta
   void* latO[2] = {nullptr, nullptr};  // [nO][4]
@@ -198,6 +202,7 @@ struct CapInfo {  // per capsule, device
   long long gidx;     // index within its degree group
   double R;
   double gs, csk;     // shear modulus and (Skalak) area-dilation constant
+  double eb;          // bending modulus (ebend, param.f90:91); 0: no bending terms
 };
 
 struct SpecBuffers {  // per degree group base pointers (T)
@@ -210,6 +215,7 @@ struct SpecBuffers {  // per degree group base pointers (T)
   void* Fsh;    // [ncap_g][4][2][N][nO]
   void* Csh;    // [ncap_g][4][2][N][N]    n0 n1 n2 surfmet
   void* GF;     // [ncap_g][7][2][N][nD]   f0 f1 f2 n0 n1 n2 surfmet (P only)
+  void* GB;     // [ncap_g][3][2][N][2*nD] third and fourth theta-derivative series (bending only)
 };
 
 struct GroupDev {  // device copy of per-group constants; [0] double, [1] float
@@ -236,6 +242,12 @@ template <class T>
 cudaError_t launch_final(const RowWork* work, int nwork, const CapInfo* caps, const GroupDev* groups, T* FX, T* FY,
                          T* FZ, T* NX, T* NY, T* NZ, T* AREA, void* frc, double dvi, int nmax, int* err,
                          cudaStream_t st);
+
+// The membrane kernel with the bending terms (sg_bending.cu): every capsule
+// of the work list, reading the group buffers G and GB.
+template <class T>
+cudaError_t launch_membrane_bend(const RowWork* work, int nwork, const CapInfo* caps, const GroupDev* groups,
+                                 const int* sur_flag, int nmax, cudaStream_t st);
 
 template <class T>
 cudaError_t launch_update_pos(int ncap, const CapInfo* caps, double dt, double lx, double ly, double lz, double* X,

@@ -107,7 +107,8 @@ __global__ void sur_trust_kernel(const CapInfo* __restrict__ caps, const int* __
   if (t == 0) {
     const float amp = ampv[b], lin = sqrtf(red[0][0]), res = sqrtf(red[1][0]);
     const float C = xb[0];
-    const bool ok = caps[capids[b]].law == SG_LAW_SKALAK && amp <= amp_max && res <= ratio_max * lin &&
+    const bool ok = caps[capids[b]].law == SG_LAW_SKALAK && caps[capids[b]].eb == 0.0 && amp <= amp_max &&
+                    res <= ratio_max * lin &&
                     C >= c_min && C <= c_max;
     flag[capids[b]] = ok ? 1 : 0;
     atomicAdd(&count[ok ? 0 : 1], 1);

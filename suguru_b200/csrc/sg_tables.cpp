@@ -101,6 +101,33 @@ void host_legendre(double th, int mm, int nn, double* P, double* dP, double* d2P
     }
 }
 
+void host_legendre_d34(double th, int mm, int nn, double* d3P, double* d4P) {
+  // d/dtheta of P^m_n is a combination of P^{m-1}_n and P^{m+1}_n (the ladder
+  // of host_legendre), so the third and fourth derivatives come from applying
+  // it to the second and third
+  const int nt = nn + 2;
+  std::vector<double> D2f((size_t)nt * nt), T3((size_t)nt * nt, 0.0), T4((size_t)nt * nt, 0.0);
+  host_legendre(th, nt, nt, nullptr, nullptr, D2f.data());
+  auto at = [&](const std::vector<double>& A, int m, int n) -> double {
+    return (m < 0 || m > n || n >= nt) ? 0.0 : A[(size_t)m * nt + n];
+  };
+  auto ladder = [&](const std::vector<double>& A, std::vector<double>& B) {
+    for (int m = 0; m < nt; ++m)
+      for (int n = m; n < nt; ++n)
+        B[(size_t)m * nt + n] = (m == 0) ? -std::sqrt((double)n * (n + 1.0)) * at(A, 1, n)
+                                         : 0.5 * (std::sqrt((n + m) * (n - m + 1.0)) * at(A, m - 1, n) -
+                                                  std::sqrt((n + m + 1.0) * (n - m)) * at(A, m + 1, n));
+  };
+  ladder(D2f, T3);
+  ladder(T3, T4);
+  for (int m = 0; m < mm; ++m)
+    for (int n = 0; n < nn; ++n) {
+      const size_t o = (size_t)m * nn + n, q = (size_t)m * nt + n;
+      const bool ok = n >= m && m < nt;
+      if (d3P) d3P[o] = ok ? T3[q] : 0.0;
+      if (d4P) d4P[o] = ok ? T4[q] : 0.0;
+    }
+}
 
 // ---------------------------------------------------------------- bf16 split
 // Round-to-nearest-even FP32 -> bf16 (bit pattern), and back.

@@ -50,6 +50,25 @@ def test_one_step(cuda, walls):
         assert np.abs(g - r).max() <= 1e-10 * np.abs(r).max()
 
 
+@pytest.mark.parametrize("grid", [(64, 64, 12, 1 / 16, 1 / 16, 1 / 16), (256, 128, 8, 1 / 32, 1 / 16, 1 / 8),
+                                  (128, 256, 6, 1 / 16, 1 / 32, 1 / 8), (512, 32, 5, 1 / 64, 1 / 8, 1 / 8),
+                                  (32, 24, 300, 1 / 16, 1 / 16, 1 / 64)])
+def test_one_step_transform_paths(cuda, grid):
+    """Register-resident transforms for power-of-two lengths (rows of 32 to
+    256 complex values, columns of 32 to 256) beside the mixed-radix ones, and
+    the elimination kept in shared memory (ktot <= 288) or streamed through
+    global memory (ktot = 300)."""
+    vel, p, f = _state(grid, 9)
+    dt, rep = 1e-3, 0.8
+    ru, rv, rw, rp = O.flow_step(grid, dt, rep, *vel, p, *f)
+    cs = _ctx(grid)
+    cs.set_flow_params(rep)
+    pg = p.copy()
+    u, v, w = cs.flow_step(dt, *vel, pg, *f)
+    for g, r in ((u, ru), (v, rv), (w, rw), (pg, rp)):
+        assert np.abs(g - r).max() <= 1e-10 * np.abs(r).max()
+
+
 def test_five_steps_and_divergence(cuda):
     vel, p, f = _state(GRID, 5)
     dt, rep = 1e-3, 0.5
