@@ -373,8 +373,14 @@ def run_ours(args):
         head = mixed
         path = "mixed (surrogate off)"
         if sur is not None:
-            head = sur["variants"][1e-4]["r"]
-            path = "mixed + surrogate, residual check calibrated for 1e-4 force error"
+            v4 = sur["variants"][1e-4]
+            head = v4["r"]
+            if v4["on_surrogate"] > 0:
+                path = ("mixed + surrogate: %d of %d capsules on the network, per-capsule checks calibrated "
+                        "for 1e-4 force error" % (v4["on_surrogate"], v4["on_surrogate"] + v4["fallback"]))
+            else:
+                path = ("mixed plain: the surrogate's limits calibrated for 1e-4 force error admit no capsule "
+                        "(held-out median error %.1e), so the step runs without it" % sur["med_net"])
         value = world * n / (head["ms_per_step"] / 1e3)
         fp64_value = world * n / (fp64["ms_per_step"] / 1e3)
         sp_ms = head["stages"]["spread"]

@@ -341,9 +341,11 @@ __global__ void __launch_bounds__(256) membrane_bend_kernel(const RowWork* __res
       const int rows = min(RP, it.row0 + it.nrows - rb);
       __syncthreads();  // the previous chunk's staged rows and outputs are consumed
       if (son && sr < rows) {
-        for (int e = se0; e < 18 * N; e += ses) sG[sr * SR + sOff[e]] = Gs[(long long)e * nD + rb + sr];
-        for (int e = se0; e < 12 * N; e += ses) sG[sr * SR + sOff[18 * N + e]] = Gb[(long long)e * nD + rb + sr];
+        for (int e = se0; e < 18 * N; e += ses) stage_async(&sG[sr * SR + sOff[e]], &Gs[(long long)e * nD + rb + sr]);
+        for (int e = se0; e < 12 * N; e += ses)
+          stage_async(&sG[sr * SR + sOff[18 * N + e]], &Gb[(long long)e * nD + rb + sr]);
       }
+      stage_wait();
       __syncthreads();
       {
         const int r = tid / mD, j = tid - (tid / mD) * mD;

@@ -72,6 +72,21 @@ SG_HD T dot3(const T* u, const T* v) {
 }
 
 #if defined(__CUDACC__)
+// Asynchronous copy of one 4- or 8-byte element from global to shared memory
+// (cp.async, no register round trip): a staging loop issues all of its
+// copies before any completes; stage_wait() waits for this thread's copies,
+// and a barrier after it publishes them to the block.
+template <class T>
+__device__ __forceinline__ void stage_async(T* dst, const T* src) {
+  static_assert(sizeof(T) == 4 || sizeof(T) == 8, "element size");
+  const unsigned d = (unsigned)__cvta_generic_to_shared(dst);
+  if constexpr (sizeof(T) == 4)
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 4;" ::"r"(d), "l"(src) : "memory");
+  else
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 8;" ::"r"(d), "l"(src) : "memory");
+}
+__device__ __forceinline__ void stage_wait() { asm volatile("cp.async.wait_all;" ::: "memory"); }
+
 // Bounded spin on a global flag; returns false on timeout (never traps).
 __device__ __forceinline__ bool spin_until_ge(volatile int* flag, int target, long long max_iter) {
   for (long long it = 0; it < max_iter; ++it) {

@@ -365,6 +365,7 @@ int setup(sg_ctx* c) {
   // capsule work lists of the persistent pointwise kernels (set_point_split)
   const size_t maxitems = (size_t)kMaxPointSplit * std::max(ncap, 1);
   SG_TRY(dalloc(c, c->d_wpos, sizeof(RowWork) * maxitems), "alloc");
+  SG_TRY(dalloc(c, c->d_cen, sizeof(double) * 3 * std::max(c->cfg.ncap, 1)), "alloc");
   SG_TRY(dalloc(c, c->d_wmem, sizeof(RowWork) * maxitems), "alloc");
   SG_TRY(dalloc(c, c->d_wsh, sizeof(RowWork) * maxitems), "alloc");
   SG_TRY(dalloc(c, c->d_wfin, sizeof(RowWork) * maxitems), "alloc");
@@ -600,7 +601,8 @@ int dev_forces(sg_ctx* c, const double* X, const double* Y, const double* Z, T* 
   const int nc = c->cfg.ncap;
   c->ncon = 0;
   if (nc == 0) return SG_OK;
-  SG_TRY(launch_posfwd<T>(c->d_wpos, c->nwpos, c->d_caps, c->d_groups, X, Y, Z, c->nmax, c->st), "posfwd");
+  SG_TRY(launch_posfwd<T>(c->d_wpos, c->nwpos, c->d_caps, c->d_groups, X, Y, Z, nc, c->d_cen, c->nmax, c->st),
+         "posfwd");
   SG_RET(dev_legendre<T>(c, 0));
   const bool f32 = sizeof(T) == 4;
   if (f32) SG_RET(sur_step_pre(c));  // surrogate force and its residual check
@@ -633,7 +635,7 @@ int dev_forces(sg_ctx* c, const double* X, const double* Y, const double* Z, T* 
   SG_TRY(launch_final<T>(c->d_wfin, c->nwfin, c->d_caps, c->d_groups, FX, FY, FZ, NX, NY, NZ, A, c->ibw.frc,
                          c->grid.dvi, c->nmax, c->d_err, c->st),
          "final");
-  c->launches += 4;  // posfwd, membrane, shgrid, final (Legendre launches counted above)
+  c->launches += 5;  // centroids, posfwd, membrane, shgrid, final (Legendre launches counted above)
   return SG_OK;
 }
 

@@ -75,6 +75,7 @@ struct sg_ctx {
   int tmF[3] = {128, 128, 128};  // their tile rows (sg_set_legendre_tile_rows, the autotuner)
   int num_sms = 148;
   int* d_err = nullptr;   // device error flag (bounded waits that expired)
+  double* d_cen = nullptr;  // capsule centroids of the step (posfwd scratch)
   int* h_err = nullptr;   // pinned copy, refreshed at the end of every step
   int nmax = 0;
   // host-mode staging
@@ -146,7 +147,12 @@ struct sg_ctx {
     bool ready = false;
     double* r = nullptr;     // real FFT input / output [ktot][jtot][itot]
     void* c = nullptr;       // modes [ktot][jtot][nmp] (double2), nmp = itot/2 + 1 rounded up to 8
-    double* d = nullptr;     // elimination multipliers [ktot][jtot][nmp] (only when ktot > 288)
+    // elimination tables per row type e = 0..3 (sg_poisson.cu): pivots z and
+    // multipliers d, [ktot][jtot][nmp] each, for the shift they were made with
+    double* zt[4] = {nullptr, nullptr, nullptr, nullptr};
+    double* dt[4] = {nullptr, nullptr, nullptr, nullptr};
+    double tshift[4] = {0, 0, 0, 0};
+    bool tvalid[4] = {false, false, false, false};
     double* tab = nullptr;   // xrt [itot/2 + 1], yrt [jtot]
     double2* w = nullptr;    // twiddles of the row and column FFTs, then the row split's W^k
     double2* wpost = nullptr;
@@ -217,7 +223,7 @@ struct PoisOut {
   long ldi, plane;
   double scale;
 };
-int poisson_setup(sg_ctx* c);
+int poisson_setup(sg_ctx* c, unsigned types);  // types: bit e for each row type e the caller solves
 void poisson_free(sg_ctx* c);
 int poisson_solve(sg_ctx* c, double* r, int e, double shift, cudaStream_t st, const PoisOut* out = nullptr);
 // indicator function (sg_indicator.cu)

@@ -212,7 +212,7 @@ int flow_setup(sg_ctx* c, double rep, double vb2, double vt2) {
   if (c->mixed) return fail(c, SG_ERR_CONFIG, "the flow solver runs on FP64 contexts");
   if (!(rep > 0.0) || !std::isfinite(rep) || !std::isfinite(vb2) || !std::isfinite(vt2))
     return fail(c, SG_ERR_ARG, "rep must be positive and finite, the wall values finite");
-  SG_RET(poisson_setup(c));
+  SG_RET(poisson_setup(c, (1u << 1) | (1u << 2) | (1u << 3)));
   auto& s = c->flow;
   s.rep = rep;
   s.vb2 = vb2;

@@ -138,7 +138,7 @@ int indicator_setup(sg_ctx* c, double visc0, double lambda, double thetainc, dou
   if (!std::isfinite(visc0) || !std::isfinite(lambda) || !std::isfinite(thetainc) || !(ta >= 0.0) ||
       !std::isfinite(ta) || !(rep > 0.0) || !std::isfinite(rep))
     return fail(c, SG_ERR_ARG, "indicator parameters must be finite, ta >= 0 and rep > 0");
-  SG_RET(poisson_setup(c));
+  SG_RET(poisson_setup(c, 1u << 0));
   auto& s = c->ind;
   s.visc0 = visc0;
   s.lambda = lambda;

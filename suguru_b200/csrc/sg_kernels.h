@@ -229,7 +229,8 @@ struct GroupDev {  // device copy of per-group constants; [0] double, [1] float
 
 template <class T>
 cudaError_t launch_posfwd(const RowWork* work, int nwork, const CapInfo* caps, const GroupDev* groups,
-                          const double* X, const double* Y, const double* Z, int nmax, cudaStream_t st);
+                          const double* X, const double* Y, const double* Z, int ncap, double* cen, int nmax,
+                          cudaStream_t st);  // cen: 3 ncap doubles of scratch (the centroids)
 template <class T>
 cudaError_t launch_membrane(const RowWork* work, int nwork, const CapInfo* caps, const GroupDev* groups,
                             const int* sur_flag, int nmax, int* err, cudaStream_t st);

@@ -33,7 +33,6 @@
 
 #include "sg_common.cuh"
 #include "sg_ctx.h"
-#include "sg_umma.cuh"
 
 namespace sg {
 namespace {
@@ -75,61 +74,101 @@ __device__ __forceinline__ Rows solver_row(int k, int kmax, int e, double dzi, d
   return r;
 }
 
-// Generic elimination (any ktot): a thread per mode walks its column of kmax
-// planes twice; the columns of neighbouring threads are adjacent in memory,
-// and the loads of the next kPre planes are issued ahead of the dependent
-// arithmetic (a ring of registers).  Modes are laid out [k][j][m] with
-// nmp >= nxm slots per y row; slots m >= nxm are padding and skipped.
-constexpr int kPre = 8;
+// The elimination split in two.  Its pivots and multipliers depend only on
+// the mode's eigenvalue, the row type e and the shift, not on the right-hand
+// side, so tri_coeff_kernel runs the reference's forward recurrence for them
+// once per (e, shift) and tabulates, per plane k and mode slot,
+//   z_k = 1 / (b_k + lam - a_k d_{k-1})  (k < kmax-1; d_{-1} = 0),
+//   d_k = c_k z_k                        (k < kmax-1),
+//   z_{kmax-1} = bb - a d_{kmax-2}        (the last pivot itself, bb = b + lam
+//                                          except for e = 3),
+// with the same operations in the same order (no fused multiply-add), so a
+// solve with the tables gives the bits of the one-pass elimination.  The
+// solve (tri_apply_kernel) is then two first-order sweeps per mode:
+//   q_0 = r_0 z_0, q_k = (r_k - a_k q_{k-1}) z_k, the last row divided by its
+//   pivot (or set to zero when the pivot is exactly zero: the mean mode of
+//   the Neumann rows, as the reference does), then x_k = q_k - d_k x_{k+1}.
+// A thread per mode; the columns of neighbouring threads are adjacent in
+// memory, and the loads of the next kPre planes are issued ahead of the
+// dependent arithmetic (a ring of registers).  Modes are laid out [k][j][m]
+// with nmp >= nxm slots per y row; slots m >= nxm are padding and skipped.
+constexpr int kPre = 32;
 
-__global__ void __launch_bounds__(128) tridiag_kernel(int kmax, int jtot, int nmp, int nxm, int e, double dzi,
-                                                      double shift, const double* __restrict__ xrt,
-                                                      const double* __restrict__ yrt, double2* __restrict__ c,
-                                                      double* __restrict__ d) {
+__global__ void __launch_bounds__(128) tri_coeff_kernel(int kmax, int jtot, int nmp, int nxm, int e, double dzi,
+                                                        double shift, const double* __restrict__ xrt,
+                                                        const double* __restrict__ yrt, double* __restrict__ zt,
+                                                        double* __restrict__ dt) {
   const long nm = (long)jtot * nmp;
   const long m = (long)blockIdx.x * blockDim.x + threadIdx.x;
   if (m >= nm || m % nmp >= nxm) return;
   const double lam = __dadd_rn(xrt[m % nmp], yrt[m / nmp]);
-  double2 ring[kPre];
-#pragma unroll
-  for (int t = 0; t < kPre; ++t)
-    if (1 + t < kmax) ring[t] = c[(1 + t) * nm + m];
   Rows r = solver_row(0, kmax, e, dzi, shift);
   double z = __drcp_rn(__dadd_rn(r.b, lam));
   double dk = __dmul_rn(r.c, z);
+  zt[m] = z;
+  dt[m] = dk;
+  for (int k = 1; k < kmax - 1; ++k) {
+    r = solver_row(k, kmax, e, dzi, shift);
+    z = __drcp_rn(__dsub_rn(__dadd_rn(r.b, lam), __dmul_rn(r.a, dk)));
+    dk = __dmul_rn(r.c, z);
+    zt[k * nm + m] = z;
+    dt[k * nm + m] = dk;
+  }
+  r = solver_row(kmax - 1, kmax, e, dzi, shift);
+  const double bb = e == 3 ? r.b : __dadd_rn(r.b, lam);
+  zt[(kmax - 1) * nm + m] = __dsub_rn(bb, __dmul_rn(r.a, dk));
+}
+
+__global__ void __launch_bounds__(128) tri_apply_kernel(int kmax, int jtot, int nmp, int nxm, int e, double dzi,
+                                                        const double* __restrict__ zt, const double* __restrict__ dt,
+                                                        double2* __restrict__ c) {
+  const long nm = (long)jtot * nmp;
+  const long m = (long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (m >= nm || m % nmp >= nxm) return;
+  // a_k of solver_row: 0 in row 0, dzi^2 in rows 1 .. kmax-2, and in row
+  // kmax-1 dzi^2 except for e = 3 (the identity row of w at the top)
+  const double a = __dmul_rn(dzi, dzi), a_last = e == 3 ? 0.0 : a;
+  double2 ring[kPre];
+  double zring[kPre];
+#pragma unroll
+  for (int t = 0; t < kPre; ++t)
+    if (1 + t < kmax) {
+      ring[t] = c[(1 + t) * nm + m];
+      zring[t] = zt[(1 + t) * nm + m];
+    }
   double2 p = c[m];
-  p.x = __dmul_rn(p.x, z);
-  p.y = __dmul_rn(p.y, z);
-  c[m] = p;
-  d[m] = dk;
-  // forward elimination, rows 1 .. kmax-2
+  {
+    const double z = zt[m];
+    p.x = __dmul_rn(p.x, z);
+    p.y = __dmul_rn(p.y, z);
+    c[m] = p;
+  }
+  // forward sweep, rows 1 .. kmax-2
   for (int k0 = 1; k0 < kmax - 1; k0 += kPre) {
 #pragma unroll
     for (int t = 0; t < kPre; ++t) {
       const int k = k0 + t;
       if (k < kmax - 1) {
         double2 q = ring[t];
-        if (k + kPre < kmax) ring[t] = c[(k + kPre) * nm + m];
-        r = solver_row(k, kmax, e, dzi, shift);
-        z = __drcp_rn(__dsub_rn(__dadd_rn(r.b, lam), __dmul_rn(r.a, dk)));
-        dk = __dmul_rn(r.c, z);
-        q.x = __dmul_rn(__dsub_rn(q.x, __dmul_rn(r.a, p.x)), z);
-        q.y = __dmul_rn(__dsub_rn(q.y, __dmul_rn(r.a, p.y)), z);
+        const double z = zring[t];
+        if (k + kPre < kmax) {
+          ring[t] = c[(k + kPre) * nm + m];
+          zring[t] = zt[(k + kPre) * nm + m];
+        }
+        q.x = __dmul_rn(__dsub_rn(q.x, __dmul_rn(a, p.x)), z);
+        q.y = __dmul_rn(__dsub_rn(q.y, __dmul_rn(a, p.y)), z);
         c[k * nm + m] = q;
-        d[k * nm + m] = dk;
         p = q;
       }
     }
   }
   {
     const int k = kmax - 1;
-    r = solver_row(k, kmax, e, dzi, shift);
-    const double bb = e == 3 ? r.b : __dadd_rn(r.b, lam);
-    z = __dsub_rn(bb, __dmul_rn(r.a, dk));
+    const double z = zt[k * nm + m];
     double2 q = c[k * nm + m];
     if (z != 0.0) {
-      q.x = __ddiv_rn(__dsub_rn(q.x, __dmul_rn(r.a, p.x)), z);
-      q.y = __ddiv_rn(__dsub_rn(q.y, __dmul_rn(r.a, p.y)), z);
+      q.x = __ddiv_rn(__dsub_rn(q.x, __dmul_rn(a_last, p.x)), z);
+      q.y = __ddiv_rn(__dsub_rn(q.y, __dmul_rn(a_last, p.y)), z);
     } else {
       q.x = q.y = 0.0;
     }
@@ -137,13 +176,12 @@ __global__ void __launch_bounds__(128) tridiag_kernel(int kmax, int jtot, int nm
     p = q;
   }
   // back substitution, rows kmax-2 .. 0
-  double dring[kPre];
 #pragma unroll
   for (int t = 0; t < kPre; ++t) {
     const int k = kmax - 2 - t;
     if (k >= 0) {
       ring[t] = c[k * nm + m];
-      dring[t] = d[k * nm + m];
+      zring[t] = dt[k * nm + m];
     }
   }
   for (int k0 = kmax - 2; k0 >= 0; k0 -= kPre) {
@@ -152,10 +190,10 @@ __global__ void __launch_bounds__(128) tridiag_kernel(int kmax, int jtot, int nm
       const int k = k0 - t;
       if (k >= 0) {
         double2 q = ring[t];
-        const double dd = dring[t];
+        const double dd = zring[t];
         if (k - kPre >= 0) {
           ring[t] = c[(k - kPre) * nm + m];
-          dring[t] = d[(k - kPre) * nm + m];
+          zring[t] = dt[(k - kPre) * nm + m];
         }
         q.x = __dsub_rn(q.x, __dmul_rn(dd, p.x));
         q.y = __dsub_rn(q.y, __dmul_rn(dd, p.y));
@@ -164,118 +202,6 @@ __global__ void __launch_bounds__(128) tridiag_kernel(int kmax, int jtot, int nm
       }
     }
   }
-}
-
-// The same elimination (the same operations in the same order, so the same
-// bits) with a block of kTriModes consecutive mode slots staged in shared
-// memory for the whole column: one warp, a lane per slot.  The block's rows
-// arrive as one bulk copy per plane (kTriModes x 16 B), kTriChunk planes per
-// mbarrier, so the forward sweep starts on the first chunk while the others
-// are in flight; the multipliers stay in shared memory; the back substitution
-// sends each finished chunk home with bulk stores.  HBM traffic is one read
-// and one write of the modes.  Shared memory: 24 B x kTriModes x kmax.
-constexpr int kTriModes = 32;
-constexpr int kTriChunk = 16;
-constexpr int kTriMaxChunks = 18;  // kmax <= 288
-
-__global__ void __launch_bounds__(kTriModes) tridiag_smem_kernel(int kmax, int jtot, int nmp, int nxm, int e,
-                                                                 double dzi, double shift,
-                                                                 const double* __restrict__ xrt,
-                                                                 const double* __restrict__ yrt,
-                                                                 double2* __restrict__ c, int* __restrict__ err) {
-  using namespace umma;
-  extern __shared__ __align__(16) unsigned char tsm[];
-  __shared__ __align__(8) uint64_t bar[kTriMaxChunks];
-  double2* sq = (double2*)tsm;                   // [kmax][kTriModes]
-  double* sd = (double*)(sq + kmax * kTriModes);  // [kmax][kTriModes]
-  const int lane = threadIdx.x;
-  const long nm = (long)jtot * nmp;
-  const long m0 = (long)blockIdx.x * kTriModes;
-  const int cnt = (int)min((long)kTriModes, nm - m0);  // a multiple of 8 (nmp is)
-  const int nch = (kmax + kTriChunk - 1) / kTriChunk;
-  const uint32_t rowb = (uint32_t)cnt * 16u;
-  if (lane == 0) {
-    for (int ch = 0; ch < nch; ++ch) mbar_init(&bar[ch], 1);
-    fence_async_smem();
-    for (int ch = 0; ch < nch; ++ch) {
-      const int k0 = ch * kTriChunk, k1 = min(kmax, k0 + kTriChunk);
-      mbar_expect_tx(&bar[ch], rowb * (uint32_t)(k1 - k0));
-      for (int k = k0; k < k1; ++k) bulk_g2s_tx(sq + k * kTriModes, c + k * nm + m0, rowb, &bar[ch]);
-    }
-  }
-  __syncwarp();
-  const long m = m0 + lane;
-  const bool act = lane < cnt && m % nmp < nxm;
-  const double lam = act ? __dadd_rn(xrt[m % nmp], yrt[m / nmp]) : 0.0;
-  bool ok = true;
-  double dk = 0.0;
-  double2 p = make_double2(0.0, 0.0);
-  for (int ch = 0; ch < nch && ok; ++ch) {
-    ok = mbar_wait(&bar[ch], 0);
-    if (!ok) break;
-    const int k0 = ch * kTriChunk, k1 = min(kmax, k0 + kTriChunk);
-    if (!act) continue;
-    for (int k = k0; k < k1; ++k) {
-      const Rows r = solver_row(k, kmax, e, dzi, shift);
-      double2 q = sq[k * kTriModes + lane];
-      if (k == 0) {
-        const double z = __drcp_rn(__dadd_rn(r.b, lam));
-        dk = __dmul_rn(r.c, z);
-        q.x = __dmul_rn(q.x, z);
-        q.y = __dmul_rn(q.y, z);
-        sd[k * kTriModes + lane] = dk;
-      } else if (k < kmax - 1) {
-        const double z = __drcp_rn(__dsub_rn(__dadd_rn(r.b, lam), __dmul_rn(r.a, dk)));
-        dk = __dmul_rn(r.c, z);
-        q.x = __dmul_rn(__dsub_rn(q.x, __dmul_rn(r.a, p.x)), z);
-        q.y = __dmul_rn(__dsub_rn(q.y, __dmul_rn(r.a, p.y)), z);
-        sd[k * kTriModes + lane] = dk;
-      } else {
-        const double bb = e == 3 ? r.b : __dadd_rn(r.b, lam);
-        const double z = __dsub_rn(bb, __dmul_rn(r.a, dk));
-        if (z != 0.0) {
-          q.x = __ddiv_rn(__dsub_rn(q.x, __dmul_rn(r.a, p.x)), z);
-          q.y = __ddiv_rn(__dsub_rn(q.y, __dmul_rn(r.a, p.y)), z);
-        } else {
-          q.x = q.y = 0.0;
-        }
-      }
-      sq[k * kTriModes + lane] = q;
-      p = q;
-    }
-  }
-  ok = __all_sync(0xffffffffu, ok);
-  if (!ok) {
-    // a copy that never completed: record it, give the others a bounded
-    // chance to land in this block's shared memory, and write nothing back
-    if (lane == 0) {
-      atomicExch(err, 3);
-      for (int ch = 0; ch < nch; ++ch) mbar_wait(&bar[ch], 0);
-    }
-    __syncwarp();
-    return;
-  }
-  // back substitution, rows kmax-2 .. 0; a chunk is final once its lowest row is
-  for (int ch = nch - 1; ch >= 0; --ch) {
-    const int k0 = ch * kTriChunk, k1 = min(kmax, k0 + kTriChunk);
-    if (act)
-      for (int k = min(k1 - 1, kmax - 2); k >= k0; --k) {
-        double2 q = sq[k * kTriModes + lane];
-        const double dd = sd[k * kTriModes + lane];
-        q.x = __dsub_rn(q.x, __dmul_rn(dd, p.x));
-        q.y = __dsub_rn(q.y, __dmul_rn(dd, p.y));
-        sq[k * kTriModes + lane] = q;
-        p = q;
-      }
-    fence_async_smem();
-    __syncwarp();
-    if (lane == 0) {
-      for (int k = k0; k < k1; ++k) bulk_s2g(c + k * nm + m0, sq + k * kTriModes, rowb);
-      bulk_commit();
-    }
-  }
-  if (lane == 0) bulk_wait_all();
-  __syncwarp();
 }
 
 // ---------------------------------------------------------------- FFT ---
@@ -501,8 +427,8 @@ __global__ void __launch_bounds__(kFftThreads) fft_cols(int ncols, int ld, int c
 // sequence's slot in shared memory, element e at e ^ ((e >> 3) & 7): every
 // read and write pattern of the passes then puts the 8 lanes of a quarter
 // warp on 8 different 16-byte bank groups.  Radices: 32 = 8.4, 64 = 8.8,
-// 128 = 8.4.4, 256 = 8.8.4.  Twiddles W_N^t (t < N) come from a table in
-// shared memory; the 8-point DFT uses sqrt(1/2) as a constant.
+// 128 = 8.4.4, 256 = 8.8.4.  Twiddles come from per-pass tables in shared
+// memory (TwTab); the 8-point DFT uses sqrt(1/2) as a constant.
 __device__ __forceinline__ int swz(int e) { return e ^ ((e >> 3) & 7); }
 
 template <int R>
@@ -549,17 +475,52 @@ __device__ __forceinline__ void dft_reg(double2* v, int sign) {
   }
 }
 
-// v[b R + r] = x[j_b + r N/R] on entry; V[q] of butterfly b in v[b R + q] on exit
+// Twiddles of a pass (NS > 1) as their own table, tp[(r-1) NS + k] =
+// W_{NS R}^{r k}: the lanes of a quarter warp (consecutive k) read
+// consecutive 16-byte values.  Tables of a length's passes lie one after the
+// other: 32: 24 values; 64: 56; 128: 24 + 96; 256: 56 + 192.
+template <int N> struct TwTab;
+template <> struct TwTab<32> { static constexpr int size = 24, off2 = 0, off3 = 0; };
+template <> struct TwTab<64> { static constexpr int size = 56, off2 = 0, off3 = 0; };
+template <> struct TwTab<128> { static constexpr int size = 120, off2 = 0, off3 = 24; };
+template <> struct TwTab<256> { static constexpr int size = 248, off2 = 0, off3 = 56; };
+
 template <int N, int R, int NS>
-__device__ __forceinline__ void pass_reg(double2 (&v)[8], int tau, const double2* __restrict__ tw, int sign) {
-  constexpr int TPS = N / 8, NB = 8 / R, STEP = N / (NS * R);
+__device__ __forceinline__ void fill_pass_tw(double2* tp, const double2* __restrict__ tw_g, int tid, int nthr) {
+  for (int i = tid; i < (R - 1) * NS; i += nthr) {
+    const int r = i / NS + 1, k = i % NS;
+    tp[i] = tw_g[r * k * (N / (NS * R))];
+  }
+}
+
+// the pass tables of length N from the table W_N^t (t < N) in global memory
+template <int N>
+__device__ __forceinline__ void fill_tw(double2* tp, const double2* __restrict__ tw_g, int tid, int nthr) {
+  if constexpr (N == 32) {
+    fill_pass_tw<32, 4, 8>(tp, tw_g, tid, nthr);
+  } else if constexpr (N == 64) {
+    fill_pass_tw<64, 8, 8>(tp, tw_g, tid, nthr);
+  } else if constexpr (N == 128) {
+    fill_pass_tw<128, 4, 8>(tp + TwTab<128>::off2, tw_g, tid, nthr);
+    fill_pass_tw<128, 4, 32>(tp + TwTab<128>::off3, tw_g, tid, nthr);
+  } else {
+    fill_pass_tw<256, 8, 8>(tp + TwTab<256>::off2, tw_g, tid, nthr);
+    fill_pass_tw<256, 4, 64>(tp + TwTab<256>::off3, tw_g, tid, nthr);
+  }
+}
+
+// v[b R + r] = x[j_b + r N/R] on entry; V[q] of butterfly b in v[b R + q] on
+// exit; tp: this pass's twiddle table (unused when NS = 1)
+template <int N, int R, int NS>
+__device__ __forceinline__ void pass_reg(double2 (&v)[8], int tau, const double2* __restrict__ tp, int sign) {
+  constexpr int TPS = N / 8, NB = 8 / R;
 #pragma unroll
   for (int b = 0; b < NB; ++b) {
     const int j = tau + b * TPS, k = j & (NS - 1);
     if constexpr (NS > 1) {
 #pragma unroll
       for (int r = 1; r < R; ++r) {
-        double2 t = tw[r * k * STEP];
+        double2 t = tp[(r - 1) * NS + k];
         if (sign > 0) t = cconj(t);
         v[b * R + r] = cmul(v[b * R + r], t);
       }
@@ -602,7 +563,8 @@ template <> struct LastPass<256> { static constexpr int R = 4, NS = 64; };
 // v holds x[tau + r TPS] (the first pass's inputs); on exit v[b R + q] holds
 // the transform at out_pos<N, LastPass R, LastPass NS>(tau, b, q).  Every lane
 // of the warp calls it (the passes synchronise the warp); seq is the
-// sequence's shared-memory slot (N values, swizzled).
+// sequence's shared-memory slot (N values, swizzled), tw the pass tables
+// (fill_tw).
 template <int N>
 __device__ __forceinline__ void fft_reg(double2 (&v)[8], double2* seq, int tau, const double2* __restrict__ tw,
                                         int sign) {
@@ -618,21 +580,21 @@ __device__ __forceinline__ void fft_reg(double2 (&v)[8], double2* seq, int tau, 
     pass_reg<N, 8, 8>(v, tau, tw, sign);
   } else if constexpr (N == 128) {
     load_pass<N, 4>(v, seq, tau);
-    pass_reg<N, 4, 8>(v, tau, tw, sign);
+    pass_reg<N, 4, 8>(v, tau, tw + TwTab<N>::off2, sign);
     __syncwarp();
     store_pass<N, 4, 8>(v, seq, tau);
     __syncwarp();
     load_pass<N, 4>(v, seq, tau);
-    pass_reg<N, 4, 32>(v, tau, tw, sign);
+    pass_reg<N, 4, 32>(v, tau, tw + TwTab<N>::off3, sign);
   } else {
     static_assert(N == 256, "length");
     load_pass<N, 8>(v, seq, tau);
-    pass_reg<N, 8, 8>(v, tau, tw, sign);
+    pass_reg<N, 8, 8>(v, tau, tw + TwTab<N>::off2, sign);
     __syncwarp();
     store_pass<N, 8, 8>(v, seq, tau);
     __syncwarp();
     load_pass<N, 4>(v, seq, tau);
-    pass_reg<N, 4, 64>(v, tau, tw, sign);
+    pass_reg<N, 4, 64>(v, tau, tw + TwTab<N>::off3, sign);
   }
 }
 
@@ -652,9 +614,9 @@ __global__ void __launch_bounds__(kRegThreads) rows_r2c_reg(long nrows, int ld, 
                                                            const double2* __restrict__ wp_g,
                                                            const double* __restrict__ src, double2* __restrict__ dst) {
   constexpr int TPS = N / 8, SPC = kRegThreads / TPS, LD = N + 1;
-  __shared__ double2 tw[N], wp[N + 1];
+  __shared__ double2 tw[TwTab<N>::size], wp[N + 1];
   __shared__ double2 buf[SPC * LD];
-  for (int t = threadIdx.x; t < N; t += kRegThreads) tw[t] = tw_g[t];
+  fill_tw<N>(tw, tw_g, threadIdx.x, kRegThreads);
   for (int t = threadIdx.x; t <= N; t += kRegThreads) wp[t] = wp_g[t];
   const int sq = threadIdx.x / TPS, tau = threadIdx.x % TPS;
   const long row = (long)blockIdx.x * SPC + sq;
@@ -705,9 +667,9 @@ __global__ void __launch_bounds__(kRegThreads) rows_c2r_reg(long nrows, int ld, 
                                                            const double2* __restrict__ src, double* __restrict__ dst,
                                                            RowsOut out) {
   constexpr int TPS = N / 8, SPC = kRegThreads / TPS, LD = N + 1;
-  __shared__ double2 tw[N], wp[N + 1];
+  __shared__ double2 tw[TwTab<N>::size], wp[N + 1];
   __shared__ double2 buf[SPC * LD];
-  for (int t = threadIdx.x; t < N; t += kRegThreads) tw[t] = tw_g[t];
+  fill_tw<N>(tw, tw_g, threadIdx.x, kRegThreads);
   for (int t = threadIdx.x; t <= N; t += kRegThreads) wp[t] = wp_g[t];
   const int sq = threadIdx.x / TPS, tau = threadIdx.x % TPS;
   const long row = (long)blockIdx.x * SPC + sq;
@@ -760,9 +722,9 @@ template <int N>
 __global__ void __launch_bounds__(kRegThreads) cols_reg(int ncols, int ld, const double2* __restrict__ tw_g, int sign,
                                                        double2* __restrict__ data) {
   constexpr int TPS = N / 8, CB = kRegThreads / TPS, LD = N + 1, YS = kRegThreads / CB;
-  __shared__ double2 tw[N];
+  __shared__ double2 tw[TwTab<N>::size];
   __shared__ double2 buf[CB * LD];
-  for (int t = threadIdx.x; t < N; t += kRegThreads) tw[t] = tw_g[t];
+  fill_tw<N>(tw, tw_g, threadIdx.x, kRegThreads);
   double2* plane = data + (long)blockIdx.y * N * ld;
   const int c0 = blockIdx.x * CB;
   {
@@ -826,25 +788,36 @@ std::vector<double> twiddles(int n) {  // exp(-2 pi i t / n) as (re, im) pairs
 namespace {
 bool pow2_fast(int n) { return n == 32 || n == 64 || n == 128 || n == 256; }
 int mode_stride(int itot) { return (itot / 2 + 1 + 7) / 8 * 8; }  // nxm rounded up to 8 slots (128 B)
-bool tri_smem(int ktot) { return ktot <= kTriChunk * kTriMaxChunks; }
 }  // namespace
 
-int poisson_setup(sg_ctx* c) {
+int poisson_setup(sg_ctx* c, unsigned types) {
   auto& s = c->pois;
-  if (s.ready) return SG_OK;
   const sg_config& f = c->cfg;
-  if (f.itot % 2 != 0 || f.ktot < 4) return fail(c, SG_ERR_CONFIG, "solver1d here needs an even itot and ktot >= 4");
-  const long nreal = (long)f.itot * f.jtot * f.ktot, nxm = f.itot / 2 + 1;
   const long nslots = (long)mode_stride(f.itot) * f.jtot;
   void* p = nullptr;
+  if (s.ready) {
+    for (int e = 0; e < 4; ++e)
+      if ((types >> e & 1u) && !s.zt[e]) {
+        SG_TRY(dalloc(c, p, sizeof(double) * nslots * f.ktot), "alloc");
+        s.zt[e] = (double*)p;
+        SG_TRY(dalloc(c, p, sizeof(double) * nslots * f.ktot), "alloc");
+        s.dt[e] = (double*)p;
+      }
+    return SG_OK;
+  }
+  if (f.itot % 2 != 0 || f.ktot < 4) return fail(c, SG_ERR_CONFIG, "solver1d here needs an even itot and ktot >= 4");
+  const long nreal = (long)f.itot * f.jtot * f.ktot, nxm = f.itot / 2 + 1;
   SG_TRY(dalloc(c, p, sizeof(double) * nreal), "alloc");
   s.r = (double*)p;
   SG_TRY(dalloc(c, p, sizeof(double2) * nslots * f.ktot), "alloc");
   s.c = p;
-  if (!tri_smem(f.ktot)) {
-    SG_TRY(dalloc(c, p, sizeof(double) * nslots * f.ktot), "alloc");
-    s.d = (double*)p;
-  }
+  for (int e = 0; e < 4; ++e)
+    if (types >> e & 1u) {
+      SG_TRY(dalloc(c, p, sizeof(double) * nslots * f.ktot), "alloc");
+      s.zt[e] = (double*)p;
+      SG_TRY(dalloc(c, p, sizeof(double) * nslots * f.ktot), "alloc");
+      s.dt[e] = (double*)p;
+    }
   // initsolver.f90:111-130: xrt(2m) = xrt(2m+1) = -4 dxi^2 sin(2m pi / (2 itot))^2, the
   // modes of a real transform in x; in y the complex modes j and jtot - j share yrt
   std::vector<double> tab(nxm + f.jtot);
@@ -880,10 +853,6 @@ int poisson_setup(sg_ctx* c) {
   static_assert(sizeof(FftPlan) <= sizeof(s.plan_x), "plan storage");
   std::memcpy(s.plan_x, &px, sizeof(px));
   std::memcpy(s.plan_y, &py, sizeof(py));
-  if (tri_smem(f.ktot))
-    SG_TRY(cudaFuncSetAttribute(tridiag_smem_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                (int)(24 * kTriModes * f.ktot)),
-           "solver1d");
   s.ready = true;
   return SG_OK;
 }
@@ -960,18 +929,26 @@ int poisson_solve(sg_ctx* c, double* r, int e, double shift, cudaStream_t st, co
     fft_cols<<<gc, kFftThreads, sm_c, st>>>(nxm, ld, cpc, py, -1, modes);
   }
   const double dzi = 1.0 / (f.lz / f.ktot);
-  if (tri_smem(f.ktot))
-    tridiag_smem_kernel<<<(unsigned)((nslots + kTriModes - 1) / kTriModes), kTriModes, 24 * kTriModes * f.ktot, st>>>(
-        f.ktot, f.jtot, ld, nxm, e, dzi, shift, s.tab, s.tab + nxm, modes, c->d_err);
-  else
-    tridiag_kernel<<<(unsigned)((nslots + 127) / 128), 128, 0, st>>>(f.ktot, f.jtot, ld, nxm, e, dzi, shift, s.tab,
-                                                                     s.tab + nxm, modes, s.d);
+  const unsigned gt = (unsigned)((nslots + 127) / 128);
+  int launches = 5;
+  if (e < 0 || e > 3 || !s.zt[e]) return fail(c, SG_ERR_STATE, "solver1d: tables of this row type were not set up");
+  if (!s.tvalid[e] || s.tshift[e] != shift) {
+    // (re)build the tables for this shift; inside a stream capture the build
+    // is recorded but has not run, so they are not marked valid for the
+    // direct calls that may come before the graph's first launch
+    cudaStreamCaptureStatus cap = cudaStreamCaptureStatusNone;
+    SG_TRY(cudaStreamIsCapturing(st, &cap), "solver1d");
+    tri_coeff_kernel<<<gt, 128, 0, st>>>(f.ktot, f.jtot, ld, nxm, e, dzi, shift, s.tab, s.tab + nxm, s.zt[e], s.dt[e]);
+    s.tvalid[e] = cap == cudaStreamCaptureStatusNone;
+    s.tshift[e] = shift;
+    launches += 1;
+  }
+  tri_apply_kernel<<<gt, 128, 0, st>>>(f.ktot, f.jtot, ld, nxm, e, dzi, s.zt[e], s.dt[e], modes);
   if (cols_fast) {
     SG_POW2_DISPATCH(f.jtot, SG_COLS_I)
   } else {
     fft_cols<<<gc, kFftThreads, sm_c, st>>>(nxm, ld, cpc, py, +1, modes);
   }
-  int launches = 5;
   if (rows_fast) {
     SG_POW2_DISPATCH(n, SG_C2R)
   } else {

@@ -67,59 +67,68 @@ __device__ __forceinline__ void stage_trig(T* dst, int ts, const T* src, int ld,
 // so an even m sums the pair sums and an odd m the pair differences over
 // j < mD/2.
 // The capsule's centroid (the mean of its points, subtracted before the
-// analysis) is computed by each item itself: 256 strided FP64 sums reduced by
-// a fixed tree, so every item of a capsule gets the same value.
+// analysis) comes from centroid_kernel, launched just before.
+//
+// Centroids: one CTA per capsule, 256 strided FP64 sums (the thread's points
+// in batches of 8: the 24 loads of a batch are all issued before any is
+// summed; these are the step's first reads of the positions, from HBM), then
+// added in the same order as one at a time and reduced by a fixed tree, so
+// the result does not depend on the launch.
+__global__ void __launch_bounds__(256) centroid_kernel(int ncap, const CapInfo* __restrict__ caps,
+                                                       const double* __restrict__ X, const double* __restrict__ Y,
+                                                       const double* __restrict__ Z, double* __restrict__ cen) {
+  __shared__ double s_cen[3][256];
+  const int tid = threadIdx.x, cap = blockIdx.x;
+  if (cap >= ncap) return;
+  const CapInfo ci = caps[cap];
+  const long long n = 8LL * ci.N * ci.N;
+  double sx = 0, sy = 0, sz = 0;
+  const double* Xc = X + ci.pt_off;
+  const double* Yc = Y + ci.pt_off;
+  const double* Zc = Z + ci.pt_off;
+  for (long long p0 = tid; p0 < n; p0 += 8LL * blockDim.x) {
+    double bx[8], by[8], bz[8];
+#pragma unroll
+    for (int u = 0; u < 8; ++u) {
+      const long long p = p0 + (long long)u * blockDim.x;
+      const bool in = p < n;
+      bx[u] = in ? Xc[p] : 0.0;
+      by[u] = in ? Yc[p] : 0.0;
+      bz[u] = in ? Zc[p] : 0.0;
+    }
+#pragma unroll
+    for (int u = 0; u < 8; ++u) {
+      sx += bx[u];
+      sy += by[u];
+      sz += bz[u];
+    }
+  }
+  s_cen[0][tid] = sx;
+  s_cen[1][tid] = sy;
+  s_cen[2][tid] = sz;
+  __syncthreads();
+  for (int o = blockDim.x / 2; o > 0; o >>= 1) {
+    if (tid < o) {
+      s_cen[0][tid] += s_cen[0][tid + o];
+      s_cen[1][tid] += s_cen[1][tid + o];
+      s_cen[2][tid] += s_cen[2][tid + o];
+    }
+    __syncthreads();
+  }
+  if (tid < 3) cen[3 * cap + tid] = s_cen[tid][0] / (double)n;
+}
+
 template <class T>
 __global__ void __launch_bounds__(256) posfwd_kernel(const RowWork* __restrict__ work, int nwork,
                                                      const CapInfo* __restrict__ caps,
                                                      const GroupDev* __restrict__ groups, const double* __restrict__ X,
-                                                     const double* __restrict__ Y, const double* __restrict__ Z) {
+                                                     const double* __restrict__ Y, const double* __restrict__ Z,
+                                                     const double* __restrict__ cen) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
-  __shared__ double s_cen[3][256];
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5, nwarp = blockDim.x >> 5;
   for (int w = blockIdx.x; w < nwork; w += gridDim.x) {
     const RowWork it = work[w];
     const CapInfo ci = caps[it.cap];
-    {
-      // the thread's points in batches of 8: the 24 loads of a batch are all
-      // issued before any is summed (these are the step's first reads of the
-      // positions, from HBM), then added in the same order as one at a time
-      const long long n = 8LL * ci.N * ci.N;
-      double sx = 0, sy = 0, sz = 0;
-      const double* Xc = X + ci.pt_off;
-      const double* Yc = Y + ci.pt_off;
-      const double* Zc = Z + ci.pt_off;
-      for (long long p0 = tid; p0 < n; p0 += 8LL * blockDim.x) {
-        double bx[8], by[8], bz[8];
-#pragma unroll
-        for (int u = 0; u < 8; ++u) {
-          const long long p = p0 + (long long)u * blockDim.x;
-          const bool in = p < n;
-          bx[u] = in ? Xc[p] : 0.0;
-          by[u] = in ? Yc[p] : 0.0;
-          bz[u] = in ? Zc[p] : 0.0;
-        }
-#pragma unroll
-        for (int u = 0; u < 8; ++u) {
-          sx += bx[u];
-          sy += by[u];
-          sz += bz[u];
-        }
-      }
-      __syncthreads();  // the previous item's reads of s_cen are done
-      s_cen[0][tid] = sx;
-      s_cen[1][tid] = sy;
-      s_cen[2][tid] = sz;
-      __syncthreads();
-      for (int o = blockDim.x / 2; o > 0; o >>= 1) {
-        if (tid < o) {
-          s_cen[0][tid] += s_cen[0][tid + o];
-          s_cen[1][tid] += s_cen[1][tid + o];
-          s_cen[2][tid] += s_cen[2][tid + o];
-        }
-        __syncthreads();
-      }
-    }
     const GroupDev gd = groups[it.group];
     const int N = gd.N, nD = gd.nD, mD = gd.mD, H = mD >> 1, hP = H + 1, lP = 2 * H + 2;
     const int RP = (int)blockDim.x / H > 0 ? (int)blockDim.x / H : 1;
@@ -129,8 +138,7 @@ __global__ void __launch_bounds__(256) posfwd_kernel(const RowWork* __restrict__
     const double* trig64 = (const double*)gd.trigD[0];
     const T* trig = (const T*)gd.trigD[pidx<T>()];
     const double R = ci.R;
-    const double nl = (double)(8LL * ci.N * ci.N);
-    const double c0 = s_cen[0][0] / nl, c1 = s_cen[1][0] / nl, c2 = s_cen[2][0] / nl;
+    const double c0 = cen[3 * it.cap], c1 = cen[3 * it.cap + 1], c2 = cen[3 * it.cap + 2];
     T* Fpos = (T*)gd.buf.Fpos + (long long)ci.gidx * 6 * N * nD;
     __syncthreads();  // the previous item's reads of shared memory are done
     stage_trig<T>(sTrig, hP, trig, mD, 2 * N, H);
@@ -313,7 +321,8 @@ __global__ void __launch_bounds__(256, sizeof(T) == 4 ? 3 : 2) membrane_kernel(c
       // stage the chunk's rows, transposed to [row][m][3 ccs + kind]; a warp
       // reads runs of RP consecutive latitudes of one (ccs, m, kind)
       if (sm.on && sm.r < rows)
-        for (int e = sm.e0; e < 18 * N; e += sm.es) sG[sm.r * SR + sOff[e]] = G[(long long)e * nD + rb + sm.r];
+        for (int e = sm.e0; e < 18 * N; e += sm.es) stage_async(&sG[sm.r * SR + sOff[e]], &G[(long long)e * nD + rb + sm.r]);
+      stage_wait();
       __syncthreads();
       {
         const int r = tid / H, j = tid - (tid / H) * H;
@@ -464,12 +473,13 @@ __global__ void __launch_bounds__(256, 3) membrane_kernel_f2(const RowWork* __re
       // stage the chunk's rows to [row][m pair][k][m parity], k = 3 ccs + kind;
       // a warp reads runs of RP consecutive latitudes of one (ccs, m, kind)
       if (sm.on && sm.r < rows)
-        for (int e = sm.e0; e < 18 * N; e += sm.es) sG[sm.r * SR + sOff[e]] = G[(long long)e * nD + rb + sm.r];
+        for (int e = sm.e0; e < 18 * N; e += sm.es) stage_async(&sG[sm.r * SR + sOff[e]], &G[(long long)e * nD + rb + sm.r]);
       if (N & 1)
         for (int q = tid; q < 18 * rows; q += blockDim.x) {
           const int r = q / 18, k = q - r * 18;
           sG[r * SR + (N >> 1) * kGP + 2 * k + 1] = 0.0f;
         }
+      stage_wait();
       __syncthreads();
       {
         const int r = tid / H, j = tid - (tid / H) * H;
@@ -612,7 +622,8 @@ __global__ void __launch_bounds__(256) shgrid_kernel(const RowWork* __restrict__
       __syncthreads();
       if (sm.on && sm.r < rows)
         for (int e = sm.e0; e < 18 * N; e += sm.es)
-          sG[sm.r * SR + sOff[2 * e]] = GO[(long long)sOff[2 * e + 1] * nO + rb + sm.r];
+          stage_async(&sG[sm.r * SR + sOff[2 * e]], &GO[(long long)sOff[2 * e + 1] * nO + rb + sm.r]);
+      stage_wait();
       __syncthreads();
       const int r = tid / H, j = tid - (tid / H) * H;
       if (r < rows) {
@@ -724,7 +735,8 @@ __global__ void __launch_bounds__(256) final_kernel(const RowWork* __restrict__ 
       const int rows = min(RP, it.row0 + it.nrows - rb);
       __syncthreads();
       if (sm.on && sm.r < rows)
-        for (int e = sm.e0; e < 14 * N; e += sm.es) sG[sm.r * SR + sOff[e]] = GF[(long long)e * nD + rb + sm.r];
+        for (int e = sm.e0; e < 14 * N; e += sm.es) stage_async(&sG[sm.r * SR + sOff[e]], &GF[(long long)e * nD + rb + sm.r]);
+      stage_wait();
       __syncthreads();
       const int r = tid / H, j = tid - (tid / H) * H;
       if (r < rows) {
@@ -860,13 +872,14 @@ size_t pointwise_smem(int kind, int nmax) {
 
 template <class T>
 cudaError_t launch_posfwd(const RowWork* work, int nwork, const CapInfo* caps, const GroupDev* groups, const double* X,
-                          const double* Y, const double* Z, int nmax, cudaStream_t st) {
-  if (nwork <= 0) return cudaSuccess;
+                          const double* Y, const double* Z, int ncap, double* cen, int nmax, cudaStream_t st) {
+  if (nwork <= 0 || ncap <= 0) return cudaSuccess;
+  centroid_kernel<<<ncap, 256, 0, st>>>(ncap, caps, X, Y, Z, cen);
   const size_t smem = pointwise_smem<T>(kPosfwd, nmax);
   cudaError_t e = cudaFuncSetAttribute(posfwd_kernel<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   if (e != cudaSuccess) return e;
   posfwd_kernel<T><<<persistent_grid(posfwd_kernel<T>, smem, nwork), kPointThreads, smem, st>>>(
-      work, nwork, caps, groups, X, Y, Z);
+      work, nwork, caps, groups, X, Y, Z, cen);
   return cudaGetLastError();
 }
 
@@ -917,7 +930,7 @@ cudaError_t launch_final(const RowWork* work, int nwork, const CapInfo* caps, co
 
 #define SG_INST(T)                                                                                                    \
   template cudaError_t launch_posfwd<T>(const RowWork*, int, const CapInfo*, const GroupDev*, const double*,         \
-                                        const double*, const double*, int, cudaStream_t);                           \
+                                        const double*, const double*, int, double*, int, cudaStream_t);             \
   template cudaError_t launch_membrane<T>(const RowWork*, int, const CapInfo*, const GroupDev*, const int*, int,     \
                                           int*, cudaStream_t);                                                      \
   template cudaError_t launch_shgrid<T>(const RowWork*, int, const CapInfo*, const GroupDev*, int, int*,             \
