@@ -178,6 +178,21 @@ int sg_flow_step(sg_ctx* ctx, double dt, const double* uo, const double* vo, con
                  const double* fx, const double* fy, const double* fz,
                  double* u, double* v, double* w);
 
+/* The overlap mesh's lid (interpolation.f90:10-69, ifoverlap = 1): the main
+ * mesh's u, v, w, p and indicator (FP64, Eulerian layout above) bilinearly
+ * interpolated at the plane between z cells nf and nf + 1 onto the nodes
+ * (i, j), 0 <= i <= itot nr + 1, 0 <= j <= jtot nr + 1, of the finer mesh
+ * (nr = main cell / fine cell, param.f90:33-41): node (i, j) at
+ * x = i dx/nr + (1 - 1/nr) dx / 2, y likewise.  u, v, p and the indicator are
+ * the mean of planes nf and nf + 1, w its value at nf + 1.  Outputs
+ * ub, vb, wb, pb, indb: (itot nr + 2) x (jtot nr + 2) doubles, i fastest, the
+ * reference's (0:i1c, 0:j1c) arrays.  Bitwise the oracle's.  SG_ERR_ARG for
+ * nr < 2 or nf outside 0 <= nf <= kmax.  In host memory mode the first call
+ * allocates its device staging (two planes per field and the lid). */
+int sg_overlap_lid(sg_ctx* ctx, int nf, int nr, const double* u, const double* v, const double* w,
+                   const double* p, const double* indic, double* ub, double* vb, double* wb, double* pb,
+                   double* indb);
+
 /* Spreading for callers that cannot allocate device memory.  It has no
  * counterpart in the reference; it is sg_spread (lagr2eulr) without a
  * context.  It is for host codes whose device memory is all owned by their
@@ -222,6 +237,19 @@ int sg_set_capsule_membrane(sg_ctx* ctx, const double* gs, const double* csk);
 #define SG_LAW_SKALAK 0
 #define SG_LAW_NEO_HOOKEAN 1
 int sg_set_capsule_law(sg_ctx* ctx, const int* law);
+
+/* Force stage of the mixed path: fused (on = 1) runs the whole
+ * stage -- centroid, longitude DFTs, the eight Legendre contractions in FP32
+ * on CUDA cores, the pointwise geometry and mechanics, the SH-grid filter and
+ * the final synthesis -- in one kernel, one CTA per capsule; staged (on = 0)
+ * runs it as separate launches (the default), with the contractions on the
+ * tensor cores (sg_set_tensor_cores).  Fused gives the bits of the staged
+ * stage with FP32 contractions (sg_set_tensor_cores(0)), in one launch, at
+ * about the staged stage's time.  Capsules that bend, and steps with the surrogate
+ * on, always take the staged stage.  SG_ERR_CONFIG on an FP64 context,
+ * SG_ERR_STATE while a graph is captured.  sg_get_fused_force: 1 or 0. */
+int sg_set_fused_force(sg_ctx* ctx, int on);
+int sg_get_fused_force(sg_ctx* ctx);
 
 /* Bending modulus per capsule (host array of ncap, NULL = all 0): a nonzero
  * eb adds the bending terms of ibend = 1 (param.f90:90-91, eb = cbend gscell)

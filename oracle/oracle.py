@@ -189,6 +189,45 @@ def spread_ind(grid, x, y, z, nx, ny, nz, area, faithful=False):
     return gx, gy, gz
 
 
+def overlap_lid(grid, nf, nr, u, v, w, p, indic):
+    """interpolation (interpolation.f90:10-69) on one rank: the lid of the overlap mesh.
+
+    grid = (itot, jtot, ktot, dx, dy, dz) with lx = itot dx as the library's
+    context takes it; fields [k][j][i] with halos (the reference's (0:i1,0:j1,0:k1)).
+    Returns ub, vb, wb, pb, indb [jtot nr + 2][itot nr + 2] (the (0:i1c,0:j1c)
+    arrays).  dx = 1/(itot/lx) and dxc = 1/(itotc/lx) as param.f90:25-26,40-41
+    evaluate them; every expression in the reference's order (numpy: no fused
+    multiply-adds)."""
+    itot, jtot = grid[0], grid[1]
+    lx, ly = itot * grid[3], jtot * grid[4]
+    dx, dy = 1.0 / (itot / lx), 1.0 / (jtot / ly)
+    dxc, dyc = 1.0 / ((itot * nr) / lx), 1.0 / ((jtot * nr) / ly)
+    i = np.arange(itot * nr + 2, dtype=np.float64)[None, :]
+    j = np.arange(jtot * nr + 2, dtype=np.float64)[:, None]
+    xp = (i * dxc) + ((0.5 * (1.0 - (1.0 / nr))) * dx)
+    yp = (j * dyc) + ((0.5 * (1.0 - (1.0 / nr))) * dy)
+    fx, fy = np.floor(xp / dx), np.floor(yp / dy)
+    x1, x2 = fx * dx, (fx + 1.0) * dx
+    y1, y2 = fy * dy, (fy + 1.0) * dy
+    den = (x2 - x1) * (y2 - y1)
+    c11 = ((x2 - xp) * (y2 - yp)) / den
+    c12 = ((x2 - xp) * (yp - y1)) / den
+    c21 = ((xp - x1) * (y2 - yp)) / den
+    c22 = ((xp - x1) * (yp - y1)) / den
+    im = np.broadcast_to(fx.astype(np.int64), c11.shape)
+    jm = np.broadcast_to(fy.astype(np.int64), c11.shape)
+    out = []
+    for q, f in enumerate((u, v, w, p, indic)):
+        lo, hi = f[nf], f[nf + 1]
+        if q == 2:  # w at the face nf + 1
+            g = lambda jj, ii: hi[jj, ii]
+        else:
+            g = lambda jj, ii: 0.5 * (lo[jj, ii] + hi[jj, ii])
+        q11, q12, q21, q22 = g(jm, im), g(jm + 1, im), g(jm, im + 1), g(jm + 1, im + 1)
+        out.append((((c11 * q11) + (c12 * q12)) + (c21 * q21)) + (c22 * q22))
+    return out
+
+
 def boundp(f):
     """boundp / boundind (bound.f90:88-139): Neumann z halos, then periodic x, y halo copies."""
     f[0] = f[1]

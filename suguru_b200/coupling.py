@@ -40,7 +40,8 @@ EXPORTS = ["sg_create", "sg_destroy", "sg_last_error", "sg_synchronize", "sg_int
            "sg_set_tensor_cores", "sg_set_legendre_terms", "sg_get_legendre_terms", "sg_set_capsule_law",
            "sg_set_legendre_tile_rows", "sg_get_legendre_tile_rows", "sg_set_wall_collisions", "sg_collisions",
            "sg_set_indicator_params", "sg_indicator", "sg_set_flow_params", "sg_flow_step",
-           "sg_contraction_work", "sg_set_capsule_bending"]
+           "sg_contraction_work", "sg_set_capsule_bending", "sg_overlap_lid", "sg_set_fused_force",
+           "sg_get_fused_force"]
 # test hooks declared in include/sg_testing.h
 TEST_EXPORTS = ["sg_test_legendre", "sg_test_gemm", "sg_test_mlp_grad"]
 WORKLOAD_EXPORTS = ["sg_prescribed_flow"]  # include/sg_workload.h
@@ -107,6 +108,9 @@ def lib():
     L.sg_set_tensor_cores.argtypes = [vp, ctypes.c_int]
     L.sg_set_capsule_law.argtypes = [vp, vp]
     L.sg_set_capsule_bending.argtypes = [vp, vp]
+    L.sg_set_fused_force.argtypes = [vp, ctypes.c_int]
+    L.sg_get_fused_force.argtypes = [vp]
+    L.sg_overlap_lid.argtypes = [vp, ctypes.c_int, ctypes.c_int] + [vp] * 10
     L.sg_set_legendre_tile_rows.argtypes = [vp, ctypes.c_int]
     L.sg_get_legendre_tile_rows.argtypes = [vp]
     L.sg_set_legendre_terms.argtypes = [vp, ctypes.c_int]
@@ -344,11 +348,34 @@ class CouplingStep:
         assert law.size == self.degree.size
         self._check(lib().sg_set_capsule_law(self._h, law.ctypes.data_as(ctypes.c_void_p)), "sg_set_capsule_law")
 
+    def set_fused_force(self, on=True):
+        """Mixed path: the whole force stage in one kernel per capsule (FP32 contractions) or staged."""
+        self._check(lib().sg_set_fused_force(self._h, int(bool(on))), "sg_set_fused_force")
+
+    def fused_force(self):
+        return bool(lib().sg_get_fused_force(self._h))
+
     def set_capsule_bending(self, eb):
         """Bending modulus per capsule (0 = the ibend = 0 force; sph.f90:1705-1709)."""
         eb = np.ascontiguousarray(np.broadcast_to(np.asarray(eb, dtype=np.float64), self.degree.shape))
         self._check(lib().sg_set_capsule_bending(self._h, eb.ctypes.data_as(ctypes.c_void_p)),
                     "sg_set_capsule_bending")
+
+    def overlap_lid(self, nf, nr, u, v, w, p, indic, out=None):
+        """interpolation.f90:10-69: ub, vb, wb, pb, indb on the (itot nr + 2) x (jtot nr + 2) lid nodes."""
+        itot, jtot = self.grid[0], self.grid[1]
+        shape = (jtot * nr + 2, itot * nr + 2)
+        for a in (u, v, w, p, indic):
+            assert str(a.dtype) in ("float64", "torch.float64"), "the lid takes FP64 fields"
+        if out is None:
+            if self.mem == "host":
+                out = [np.zeros(shape) for _ in range(5)]
+            else:
+                import torch
+                out = [torch.zeros(shape, dtype=torch.float64, device=u.device) for _ in range(5)]
+        self._check(lib().sg_overlap_lid(self._h, int(nf), int(nr), *map(_ptr, (u, v, w, p, indic)),
+                                         *map(_ptr, out)), "sg_overlap_lid")
+        return out
 
     def set_legendre_tile_rows(self, rows):
         """Data rows per tensor-core Legendre tile: 128 or 64 (results do not depend on it)."""

@@ -72,6 +72,26 @@ SG_HD T dot3(const T* u, const T* v) {
 }
 
 #if defined(__CUDACC__)
+// Lets a kernel take up to the device's opt-in limit of dynamic shared memory
+// (less its static shared memory).  Every launcher sets this one value
+// instead of its own request: a kernel launched with different requests
+// (the Legendre stages, contexts of different degrees) would otherwise carry
+// whatever its last launcher set, and a launch outside that launcher's
+// sequence -- a CUDA graph node replayed on its own, as a profiler does --
+// could ask for more than that limit and fail to launch.  The launch's own
+// request still sets its occupancy.
+template <class K>
+inline cudaError_t smem_limit_max(K kernel) {
+  int dev = 0, optin = 0;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e == cudaSuccess) e = cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
+  cudaFuncAttributes fa{};
+  if (e == cudaSuccess) e = cudaFuncGetAttributes(&fa, kernel);
+  if (e == cudaSuccess)
+    e = cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, optin - (int)fa.sharedSizeBytes);
+  return e;
+}
+
 // Asynchronous copy of one 4- or 8-byte element from global to shared memory
 // (cp.async, no register round trip): a staging loop issues all of its
 // copies before any completes; stage_wait() waits for this thread's copies,

@@ -366,6 +366,17 @@ int setup(sg_ctx* c) {
   const size_t maxitems = (size_t)kMaxPointSplit * std::max(ncap, 1);
   SG_TRY(dalloc(c, c->d_wpos, sizeof(RowWork) * maxitems), "alloc");
   SG_TRY(dalloc(c, c->d_cen, sizeof(double) * 3 * std::max(c->cfg.ncap, 1)), "alloc");
+  {
+    // the fused force stage's capsule order: largest degree first, then index
+    std::vector<int> order(c->cfg.ncap);
+    for (int k = 0; k < c->cfg.ncap; ++k) order[k] = k;
+    std::stable_sort(order.begin(), order.end(),
+                     [&](int a, int b) { return c->h_caps[a].N > c->h_caps[b].N; });
+    void* tmp = nullptr;
+    if (order.empty()) order.push_back(0);
+    SG_TRY(upload(c, tmp, order), "order");
+    c->d_order = (int*)tmp;
+  }
   SG_TRY(dalloc(c, c->d_wmem, sizeof(RowWork) * maxitems), "alloc");
   SG_TRY(dalloc(c, c->d_wsh, sizeof(RowWork) * maxitems), "alloc");
   SG_TRY(dalloc(c, c->d_wfin, sizeof(RowWork) * maxitems), "alloc");
@@ -501,6 +512,12 @@ int setup(sg_ctx* c) {
   c->h_probs = P;
   SG_TRY(upload(c, tmp, P), "problems");
   c->d_probs = (LegProblem*)tmp;
+  if (c->mixed) {
+    // the fused force stage: the per-group problems 8 g .. 8 g + 7 with their
+    // FP32 tables; its staged A rows take rpc M K floats at most
+    for (size_t q = 0; q < 8 * c->groups.size(); ++q)
+      c->fused_cf = std::max(c->fused_cf, (size_t)P[q].rpc * P[q].M * P[q].K);
+  }
   for (int s = 0; s < 6; ++s) {
     c->nlw[s] = (int)W[s].size();
     SG_TRY(upload(c, tmp, W[s]), "work");
@@ -601,6 +618,15 @@ int dev_forces(sg_ctx* c, const double* X, const double* Y, const double* Z, T* 
   const int nc = c->cfg.ncap;
   c->ncon = 0;
   if (nc == 0) return SG_OK;
+  if constexpr (sizeof(T) == 4) {
+    if (c->fused && !c->bend && !sur_flags(c)) {
+      SG_TRY(launch_force_fused(c->d_order, nc, c->d_caps, c->d_groups, c->d_probs, X, Y, Z, c->d_cen, FX, FY, FZ, NX,
+                                NY, NZ, A, c->ibw.frc, c->grid.dvi, c->nmax, c->fused_cf, c->st),
+             "force (fused)");
+      c->launches += 1;
+      return SG_OK;
+    }
+  }
   SG_TRY(launch_posfwd<T>(c->d_wpos, c->nwpos, c->d_caps, c->d_groups, X, Y, Z, nc, c->d_cen, c->nmax, c->st),
          "posfwd");
   SG_RET(dev_legendre<T>(c, 0));
@@ -1105,6 +1131,56 @@ int sg_flow_step(sg_ctx* c, double dt, const double* uo, const double* vo, const
   return finish(c);
 }
 
+int sg_overlap_lid(sg_ctx* c, int nf, int nr, const double* u, const double* v, const double* w, const double* p,
+                   const double* indic, double* ub, double* vb, double* wb, double* pb, double* indb) {
+  if (!c) return SG_ERR_ARG;
+  const sg_config& g = c->cfg;
+  if (nr < 2) return fail(c, SG_ERR_ARG, "overlap mesh: nr (main cell / fine cell) must be at least 2");
+  if (nf < 0 || nf + 1 > g.ktot + 1) return fail(c, SG_ERR_ARG, "overlap mesh: need 0 <= nf and nf + 1 <= kmax + 1");
+  SG_RET(check_ptrs(c, {u, v, w, p, indic, ub, vb, wb, pb, indb}));
+  const long ldi = g.itot + 2, plane = ldi * (g.jtot + 2);
+  const int ni = g.itot * nr + 2, nj = g.jtot * nr + 2;
+  const size_t nlid = (size_t)ni * nj;
+  LidArgs a{};
+  a.ldi = ldi;
+  a.plane = plane;
+  a.ni = ni;
+  a.nj = nj;
+  // param.f90:25-26, 40-41: dx = 1/(itot/lx), dxc = 1/(itotc/lx), itotc = itot nr
+  a.dx = 1.0 / ((double)g.itot / g.lx);
+  a.dy = 1.0 / ((double)g.jtot / g.ly);
+  a.dxc = 1.0 / ((double)(g.itot * nr) / g.lx);
+  a.dyc = 1.0 / ((double)(g.jtot * nr) / g.ly);
+  a.offx = (0.5 * (1.0 - (1.0 / nr))) * a.dx;
+  a.offy = (0.5 * (1.0 - (1.0 / nr))) * a.dy;
+  const double* in[5] = {u, v, w, p, indic};
+  double* out[5] = {ub, vb, wb, pb, indb};
+  const bool host = g.mem == SG_MEM_HOST;
+  if (host) {
+    // only planes nf and nf + 1 are read: those, and the lid, are staged on the device
+    if (!c->ovl_in) SG_TRY(dalloc(c, c->ovl_in, sizeof(double) * 10 * plane), "alloc");
+    if (c->ovl_out_n < nlid) {
+      SG_TRY(dalloc(c, c->ovl_out, sizeof(double) * 5 * nlid), "alloc");
+      c->ovl_out_n = nlid;
+    }
+    for (int f = 0; f < 5; ++f) {
+      SG_RET(h2d(c, c->ovl_in + 2 * f * plane, in[f] + (long)nf * plane, sizeof(double) * 2 * plane));
+      a.f[f] = c->ovl_in + 2 * f * plane;
+      a.o[f] = c->ovl_out + f * nlid;
+    }
+  } else {
+    for (int f = 0; f < 5; ++f) {
+      a.f[f] = in[f] + (long)nf * plane;
+      a.o[f] = out[f];
+    }
+  }
+  c->launches = 1;
+  SG_TRY(launch_overlap_lid(a, c->st), "overlap lid");
+  if (host)
+    for (int f = 0; f < 5; ++f) SG_RET(d2h(c, out[f], a.o[f], sizeof(double) * nlid));
+  return finish(c);
+}
+
 int sg_surf_vol(sg_ctx* c, const double* X, const double* Y, const double* Z, const void* NX, const void* NY,
                 const void* NZ, const void* AREA, const double* exy1_prev, double* out) {
   if (!c) return SG_ERR_ARG;
@@ -1164,6 +1240,16 @@ int sg_set_profiling(sg_ctx* c, int on) {
   c->profiling = on != 0;
   return SG_OK;
 }
+
+int sg_set_fused_force(sg_ctx* c, int on) {
+  if (!c) return SG_ERR_ARG;
+  if (c->graph) return fail(c, SG_ERR_STATE, "release the captured graph first");
+  if (!c->mixed && on) return fail(c, SG_ERR_CONFIG, "the fused force stage is the mixed-precision path's");
+  c->fused = on != 0;
+  return SG_OK;
+}
+
+int sg_get_fused_force(sg_ctx* c) { return c ? (c->fused ? 1 : 0) : -1; }
 
 int sg_set_capsule_bending(sg_ctx* c, const double* eb) {
   if (!c) return SG_ERR_ARG;

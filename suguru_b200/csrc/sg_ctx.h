@@ -62,6 +62,11 @@ struct sg_ctx {
   int maxJ[6] = {}, maxK[6] = {};
   // tensor-core Legendre path (mixed precision): 128-row work lists
   bool leg_tc = false;
+  // fused force stage (mixed path): one CTA per capsule runs every stage
+  // (sg_set_fused_force); used when no capsule bends and the surrogate is off
+  bool fused = false;
+  int* d_order = nullptr;      // the capsules, largest degree first
+  size_t fused_cf = 0;         // largest rpc M K over the contractions (staged floats)
   // split mode of the tensor-core contractions: 0 automatic (BF16x6 from
   // degree kSixTermDegree up, BF16x3 below), 3 or 6 for every group
   int leg_terms = 0;
@@ -76,6 +81,9 @@ struct sg_ctx {
   int num_sms = 148;
   int* d_err = nullptr;   // device error flag (bounded waits that expired)
   double* d_cen = nullptr;  // capsule centroids of the step (posfwd scratch)
+  double* ovl_in = nullptr;   // sg_overlap_lid in host memory mode: planes nf, nf + 1 of 5 fields
+  double* ovl_out = nullptr;  // and the 5 lid arrays
+  size_t ovl_out_n = 0;
   int* h_err = nullptr;   // pinned copy, refreshed at the end of every step
   int nmax = 0;
   // host-mode staging

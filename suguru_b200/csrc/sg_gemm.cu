@@ -215,11 +215,11 @@ cudaError_t launch_gemm(const GemmArgs& g, int* d_err, cudaStream_t st) {
   ga.ksplit = ks;
   cudaError_t e;
   if (g.split) {
-    e = cudaFuncSetAttribute(gemm_kernel<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    e = smem_limit_max(gemm_kernel<1>);
     if (e != cudaSuccess) return e;
     gemm_kernel<1><<<grid, 128, smem, st>>>(ga, d_err);
   } else {
-    e = cudaFuncSetAttribute(gemm_kernel<0>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    e = smem_limit_max(gemm_kernel<0>);
     if (e != cudaSuccess) return e;
     gemm_kernel<0><<<grid, 128, smem, st>>>(ga, d_err);
   }

@@ -231,6 +231,14 @@ template <class T>
 cudaError_t launch_posfwd(const RowWork* work, int nwork, const CapInfo* caps, const GroupDev* groups,
                           const double* X, const double* Y, const double* Z, int ncap, double* cen, int nmax,
                           cudaStream_t st);  // cen: 3 ncap doubles of scratch (the centroids)
+// The whole force stage, one CTA per capsule (sg_spectral.cu, mixed path):
+// order = the capsules, largest degree first; probs = the per-group problems
+// S0 S1 S2 S3a S3b S4 S5a S5b (FP32 tables); max_contract_floats = the
+// largest rpc M K over them.
+cudaError_t launch_force_fused(const int* order, int ncap, const CapInfo* caps, const GroupDev* groups,
+                               const LegProblem* probs, const double* X, const double* Y, const double* Z, double* cen,
+                               float* FX, float* FY, float* FZ, float* NX, float* NY, float* NZ, float* AREA, void* frc,
+                               double dvi, int nmax, size_t max_contract_floats, cudaStream_t st);
 template <class T>
 cudaError_t launch_membrane(const RowWork* work, int nwork, const CapInfo* caps, const GroupDev* groups,
                             const int* sur_flag, int nmax, int* err, cudaStream_t st);
@@ -267,5 +275,15 @@ template <class T>
 cudaError_t launch_surf_vol(int ncap, const CapInfo* caps, const double* X, const double* Y, const double* Z,
                             const T* NX, const T* NY, const T* NZ, const T* AREA, const double* exy1_prev,
                             double* out, cudaStream_t st);
+
+// Overlap mesh lid (sg_overlap.cu, interpolation.f90:10-69)
+struct LidArgs {
+  const double* f[5];  // u, v, w, p, indic, each at plane nf (plane nf + 1 one plane further)
+  long ldi, plane;     // row and plane strides of the fields
+  double* o[5];        // ub, vb, wb, pb, indb: [nj][ni]
+  int ni, nj;          // itot nr + 2, jtot nr + 2
+  double dx, dy, dxc, dyc, offx, offy;
+};
+cudaError_t launch_overlap_lid(const LidArgs& a, cudaStream_t st);
 
 }  // namespace sg

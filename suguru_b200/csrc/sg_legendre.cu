@@ -66,7 +66,7 @@ cudaError_t launch_legendre(const LegProblem* d_probs, const LegWork* d_work, in
   if (e == cudaSuccess) e = cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
   if (e != cudaSuccess) return e;
   if (smem > (size_t)optin) return cudaErrorInvalidValue;
-  e = cudaFuncSetAttribute(legendre_kernel<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  e = smem_limit_max(legendre_kernel<T>);
   if (e != cudaSuccess) return e;
   legendre_kernel<T><<<nwork, 256, smem, st>>>(d_probs, d_work, nwork);
   return cudaGetLastError();

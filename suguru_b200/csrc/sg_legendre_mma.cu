@@ -399,11 +399,11 @@ cudaError_t launch_legendre_mma(const LegProblem* d_probs, const LegWork* d_work
   const int per_sm = std::min(kLegPerSm, 512 / cols);
   const int grid = nwork < num_sms * per_sm ? nwork : num_sms * per_sm;
   if (tm == 64) {
-    e = cudaFuncSetAttribute(legendre_mma_kernel<64>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    e = smem_limit_max(legendre_mma_kernel<64>);
     if (e != cudaSuccess) return e;
     legendre_mma_kernel<64><<<grid, kLegThreads, smem, st>>>(d_probs, d_work, nwork, lv, nparts, cols, off2, d_err);
   } else {
-    e = cudaFuncSetAttribute(legendre_mma_kernel<128>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    e = smem_limit_max(legendre_mma_kernel<128>);
     if (e != cudaSuccess) return e;
     legendre_mma_kernel<128><<<grid, kLegThreads, smem, st>>>(d_probs, d_work, nwork, lv, nparts, cols, off2,
                                                               d_err);

@@ -18,6 +18,8 @@
 // The reference sphere x = R (sin t sin p, sin t cos p, cos t) (sph.f90:84-86)
 // is subtracted from the positions before the transforms and its geometry
 // added back analytically, so the transforms only carry the displacement.
+#include <algorithm>
+
 #include "sg_common.cuh"
 #include "sg_kernels.h"
 #include "sg_mechanics.cuh"
@@ -74,12 +76,11 @@ __device__ __forceinline__ void stage_trig(T* dst, int ts, const T* src, int ld,
 // summed; these are the step's first reads of the positions, from HBM), then
 // added in the same order as one at a time and reduced by a fixed tree, so
 // the result does not depend on the launch.
-__global__ void __launch_bounds__(256) centroid_kernel(int ncap, const CapInfo* __restrict__ caps,
-                                                       const double* __restrict__ X, const double* __restrict__ Y,
-                                                       const double* __restrict__ Z, double* __restrict__ cen) {
+__device__ __forceinline__ void centroid_block(int cap, const CapInfo* __restrict__ caps,
+                                               const double* __restrict__ X, const double* __restrict__ Y,
+                                               const double* __restrict__ Z, double* __restrict__ cen) {
   __shared__ double s_cen[3][256];
-  const int tid = threadIdx.x, cap = blockIdx.x;
-  if (cap >= ncap) return;
+  const int tid = threadIdx.x;
   const CapInfo ci = caps[cap];
   const long long n = 8LL * ci.N * ci.N;
   double sx = 0, sy = 0, sz = 0;
@@ -103,6 +104,7 @@ __global__ void __launch_bounds__(256) centroid_kernel(int ncap, const CapInfo* 
       sz += bz[u];
     }
   }
+  __syncthreads();  // the previous capsule's reads of s_cen are done
   s_cen[0][tid] = sx;
   s_cen[1][tid] = sy;
   s_cen[2][tid] = sz;
@@ -118,16 +120,21 @@ __global__ void __launch_bounds__(256) centroid_kernel(int ncap, const CapInfo* 
   if (tid < 3) cen[3 * cap + tid] = s_cen[tid][0] / (double)n;
 }
 
+__global__ void __launch_bounds__(256) centroid_kernel(int ncap, const CapInfo* __restrict__ caps,
+                                                       const double* __restrict__ X, const double* __restrict__ Y,
+                                                       const double* __restrict__ Z, double* __restrict__ cen) {
+  if ((int)blockIdx.x < ncap) centroid_block(blockIdx.x, caps, X, Y, Z, cen);
+}
+
 template <class T>
-__global__ void __launch_bounds__(256) posfwd_kernel(const RowWork* __restrict__ work, int nwork,
+__device__ __forceinline__ void posfwd_item(const RowWork it,
                                                      const CapInfo* __restrict__ caps,
                                                      const GroupDev* __restrict__ groups, const double* __restrict__ X,
                                                      const double* __restrict__ Y, const double* __restrict__ Z,
                                                      const double* __restrict__ cen) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5, nwarp = blockDim.x >> 5;
-  for (int w = blockIdx.x; w < nwork; w += gridDim.x) {
-    const RowWork it = work[w];
+  {
     const CapInfo ci = caps[it.cap];
     const GroupDev gd = groups[it.group];
     const int N = gd.N, nD = gd.nD, mD = gd.mD, H = mD >> 1, hP = H + 1, lP = 2 * H + 2;
@@ -183,6 +190,15 @@ __global__ void __launch_bounds__(256) posfwd_kernel(const RowWork* __restrict__
       }
     }
   }
+}
+
+template <class T>
+__global__ void __launch_bounds__(256) posfwd_kernel(const RowWork* __restrict__ work, int nwork,
+                                                     const CapInfo* __restrict__ caps,
+                                                     const GroupDev* __restrict__ groups, const double* __restrict__ X,
+                                                     const double* __restrict__ Y, const double* __restrict__ Z,
+                                                     const double* __restrict__ cen) {
+  for (int w = blockIdx.x; w < nwork; w += gridDim.x) posfwd_item<T>(work[w], caps, groups, X, Y, Z, cen);
 }
 
 // ------------------------------------------------- membrane pointwise -----
@@ -421,15 +437,14 @@ __device__ __forceinline__ void synth_pair(const float* g, float4 t, float2 fm, 
   }
 }
 
-__global__ void __launch_bounds__(256, 3) membrane_kernel_f2(const RowWork* __restrict__ work, int nwork,
+__device__ __forceinline__ void membrane_item_f2(const RowWork it,
                                                              const CapInfo* __restrict__ caps,
                                                              const GroupDev* __restrict__ groups,
                                                              const int* __restrict__ sur_flag, int* __restrict__ err) {
   (void)err;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5, nwarp = blockDim.x >> 5;
-  for (int w = blockIdx.x; w < nwork; w += gridDim.x) {
-    const RowWork it = work[w];
+  {
     const CapInfo ci = caps[it.cap];
     const float hf = (float)(0.5 * ci.gs), csk = (float)ci.csk;  // hf_gscell = 0.5 gscell (sph.f90:35)
     const bool normals_only = sur_flag && sur_flag[it.cap];
@@ -537,6 +552,13 @@ __global__ void __launch_bounds__(256, 3) membrane_kernel_f2(const RowWork* __re
   }
 }
 
+__global__ void __launch_bounds__(256, 3) membrane_kernel_f2(const RowWork* __restrict__ work, int nwork,
+                                                             const CapInfo* __restrict__ caps,
+                                                             const GroupDev* __restrict__ groups,
+                                                             const int* __restrict__ sur_flag, int* __restrict__ err) {
+  for (int w = blockIdx.x; w < nwork; w += gridDim.x) membrane_item_f2(work[w], caps, groups, sur_flag, err);
+}
+
 // Shared memory (bytes) of membrane_kernel_f2 for degrees up to nmax: the
 // largest over n <= nmax of staged rows RP (NP kGP + 4), the staging offsets
 // 18n, the pair trig table
@@ -583,14 +605,13 @@ __device__ __forceinline__ void load18(const T* g, T (&v)[18]) {
 }
 
 template <class T>
-__global__ void __launch_bounds__(256) shgrid_kernel(const RowWork* __restrict__ work, int nwork,
+__device__ __forceinline__ void shgrid_item(const RowWork it,
                                                      const CapInfo* __restrict__ caps,
                                                      const GroupDev* __restrict__ groups, int* __restrict__ err) {
   (void)err;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5, nwarp = blockDim.x >> 5;
-  for (int w = blockIdx.x; w < nwork; w += gridDim.x) {
-    const RowWork it = work[w];
+  {
     const CapInfo ci = caps[it.cap];
     const GroupDev gd = groups[it.group];
     const int N = gd.N, nO = gd.nO, mO = gd.mO, H = mO >> 1, hP = H + 1, lP = 2 * H + 2;
@@ -695,6 +716,13 @@ __global__ void __launch_bounds__(256) shgrid_kernel(const RowWork* __restrict__
   }
 }
 
+template <class T>
+__global__ void __launch_bounds__(256) shgrid_kernel(const RowWork* __restrict__ work, int nwork,
+                                                     const CapInfo* __restrict__ caps,
+                                                     const GroupDev* __restrict__ groups, int* __restrict__ err) {
+  for (int w = blockIdx.x; w < nwork; w += gridDim.x) shgrid_item<T>(work[w], caps, groups, err);
+}
+
 // ------------------------------------------------- final synthesis --------
 // TRSSPH SH grid -> force grid of force, normals and surface metric
 // (forcing.f90:67-88), area = surfmetDf * wgtdsinf (forcing.f90:91).
@@ -704,7 +732,7 @@ __global__ void __launch_bounds__(256) shgrid_kernel(const RowWork* __restrict__
 constexpr int kFK = 16;
 
 template <class T>
-__global__ void __launch_bounds__(256) final_kernel(const RowWork* __restrict__ work, int nwork,
+__device__ __forceinline__ void final_item(const RowWork it,
                                                     const CapInfo* __restrict__ caps,
                                                     const GroupDev* __restrict__ groups, T* __restrict__ FX,
                                                     T* __restrict__ FY, T* __restrict__ FZ, T* __restrict__ NX,
@@ -714,8 +742,7 @@ __global__ void __launch_bounds__(256) final_kernel(const RowWork* __restrict__ 
   (void)err;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   const int tid = threadIdx.x;
-  for (int w = blockIdx.x; w < nwork; w += gridDim.x) {
-    const RowWork it = work[w];
+  {
     const CapInfo ci = caps[it.cap];
     const GroupDev gd = groups[it.group];
     const int N = gd.N, nD = gd.nD, mD = gd.mD, H = mD >> 1, hP = H + 1;
@@ -801,6 +828,112 @@ __global__ void __launch_bounds__(256) final_kernel(const RowWork* __restrict__ 
   }
 }
 
+template <class T>
+__global__ void __launch_bounds__(256) final_kernel(const RowWork* __restrict__ work, int nwork,
+                                                    const CapInfo* __restrict__ caps,
+                                                    const GroupDev* __restrict__ groups, T* __restrict__ FX,
+                                                    T* __restrict__ FY, T* __restrict__ FZ, T* __restrict__ NX,
+                                                    T* __restrict__ NY, T* __restrict__ NZ, T* __restrict__ AREA,
+                                                    ForceRec<T>* __restrict__ frc, double dvi,
+                                                    int* __restrict__ err) {
+  for (int w = blockIdx.x; w < nwork; w += gridDim.x) final_item<T>(work[w], caps, groups, FX, FY, FZ, NX, NY, NZ, AREA, frc, dvi, err);
+}
+
+// ------------------------------------------------- fused force stage ------
+// The whole force stage of one capsule in one CTA (mixed path): centroid,
+// longitude DFT of the displacement, the eight Legendre contractions of its
+// degree group on CUDA cores in FP32, the membrane, SH-grid and final
+// pointwise stages.  Persistent CTAs take whole capsules, largest degree
+// first, and run the stages back to back with block barriers between them:
+// no launch boundary separates the stages, and on an SM the CTAs of other
+// capsules fill one capsule's waits.  The intermediates stay in the same
+// per-capsule global buffers as in the staged pipeline (in L2), and every
+// pointwise stage is the same device code, so the fused step gives the bits
+// of the staged step with FP32 contractions (sg_set_tensor_cores(0)).
+//
+// One capsule's rows of a problem, all m: D_m[r][j] = sum_{k >= k0}
+// A_m[r][k] B_m[j][k] with k0 = m for a synthesis (tri), in the same order
+// of k as legendre_kernel.  The capsule's A rows for every m are staged as
+// [m][k][r] (its R rows side by side), then thread task (m, j) forms the R
+// sums, reading B_m[j][k] from the (L2-resident) FP32 table.
+template <int R>
+__device__ __forceinline__ void contract_rows(const LegProblem& P, long long gidx, float* sA, int part, int nparts) {
+  const int M = P.M, J = P.J, K = P.K;
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5, nwarp = blockDim.x >> 5;
+  const float* A = (const float*)P.A + gidx * P.sAc;
+  float* D = (float*)P.D + gidx * P.sDc;
+  const float* B = (const float*)P.B;
+  __syncthreads();  // the previous stage's reads of shared memory are done
+  for (int rm = warp; rm < R * M; rm += nwarp) {
+    const int r = rm / M, m = rm - r * M;
+    const float* a = A + (long long)r * P.sAr + (long long)m * P.sAm;
+    for (int k = lane; k < K; k += 32) sA[(m * K + k) * R + r] = a[k];
+  }
+  __syncthreads();
+  const int stride = nparts * (int)blockDim.x;
+  for (int t = tid + part * (int)blockDim.x; t < M * J; t += stride) {
+    const int m = t / J, j = t - m * J;
+    const int k0 = P.tri ? m : 0;
+    const float* b = B + (long long)m * P.sBm + (long long)j * K;
+    const float* a = sA + m * K * R;
+    float acc[R];
+#pragma unroll
+    for (int r = 0; r < R; ++r) acc[r] = 0.0f;
+    for (int k = k0; k < K; ++k) {
+      const float bk = __ldg(b + k);
+#pragma unroll
+      for (int r = 0; r < R; ++r) acc[r] += a[k * R + r] * bk;
+    }
+    float* d = D + (long long)m * P.sDm + j;
+#pragma unroll
+    for (int r = 0; r < R; ++r) d[(long long)r * P.sDr] = acc[r];
+  }
+}
+
+// A capsule's rows of a problem; the tasks (m, j) are shared among nparts
+// CTAs (part = this CTA's share), each staging the whole A.
+__device__ __forceinline__ void contract_capsule(const LegProblem& P, long long gidx, float* sA, int part,
+                                                 int nparts) {
+  switch (P.rpc) {
+    case 6: contract_rows<6>(P, gidx, sA, part, nparts); break;
+    case 8: contract_rows<8>(P, gidx, sA, part, nparts); break;
+    default: contract_rows<12>(P, gidx, sA, part, nparts); break;
+  }
+}
+
+// Per degree group the problems are, in order, S0 S1 S2 S3a S3b S4 S5a S5b
+// (8 g .. 8 g + 7 of probs).
+__global__ void __launch_bounds__(256, 2) force_fused_kernel(
+    const int* __restrict__ order, int ncap, const CapInfo* __restrict__ caps, const GroupDev* __restrict__ groups,
+    const LegProblem* __restrict__ probs, const double* __restrict__ X, const double* __restrict__ Y,
+    const double* __restrict__ Z, double* __restrict__ cen, float* __restrict__ FX, float* __restrict__ FY,
+    float* __restrict__ FZ, float* __restrict__ NX, float* __restrict__ NY, float* __restrict__ NZ,
+    float* __restrict__ AREA, ForceRec<float>* __restrict__ frc, double dvi) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  float* sA = (float*)smem_raw;
+  for (int w = blockIdx.x; w < ncap; w += gridDim.x) {
+    const int cap = order[w];
+    const CapInfo ci = caps[cap];
+    const GroupDev gd = groups[ci.group];
+    const LegProblem* pg = probs + 8 * ci.group;
+    const RowWork dealias{cap, 0, gd.nD, ci.group}, shgrid{cap, 0, gd.nO, ci.group};
+    centroid_block(cap, caps, X, Y, Z, cen);
+    __syncthreads();  // the centroid is written
+    posfwd_item<float>(dealias, caps, groups, X, Y, Z, cen);
+    contract_capsule(pg[0], ci.gidx, sA, 0, 1);  // S0: analysis of the displacement
+    contract_capsule(pg[1], ci.gidx, sA, 0, 1);  // S1: P, dP, d2P series on the dealias grid
+    contract_capsule(pg[4], ci.gidx, sA, 0, 1);  // S3b: the shape on the SH grid
+    membrane_item_f2(dealias, caps, groups, nullptr, nullptr);
+    contract_capsule(pg[2], ci.gidx, sA, 0, 1);  // S2: analysis of force and normals
+    contract_capsule(pg[3], ci.gidx, sA, 0, 1);  // S3a: the normals on the SH grid
+    contract_capsule(pg[6], ci.gidx, sA, 0, 1);  // S5a: the force on the force grid
+    shgrid_item<float>(shgrid, caps, groups, nullptr);
+    contract_capsule(pg[5], ci.gidx, sA, 0, 1);  // S4: analysis of renormalised normals and surface metric
+    contract_capsule(pg[7], ci.gidx, sA, 0, 1);  // S5b: them on the force grid
+    final_item<float>(dealias, caps, groups, FX, FY, FZ, NX, NY, NZ, AREA, frc, dvi, nullptr);
+  }
+}
+
 // ------------------------------------------------- launchers --------------
 
 // Persistent launches: CTAs of 256 threads loop over the capsule work items
@@ -876,7 +1009,7 @@ cudaError_t launch_posfwd(const RowWork* work, int nwork, const CapInfo* caps, c
   if (nwork <= 0 || ncap <= 0) return cudaSuccess;
   centroid_kernel<<<ncap, 256, 0, st>>>(ncap, caps, X, Y, Z, cen);
   const size_t smem = pointwise_smem<T>(kPosfwd, nmax);
-  cudaError_t e = cudaFuncSetAttribute(posfwd_kernel<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  cudaError_t e = smem_limit_max(posfwd_kernel<T>);
   if (e != cudaSuccess) return e;
   posfwd_kernel<T><<<persistent_grid(posfwd_kernel<T>, smem, nwork), kPointThreads, smem, st>>>(
       work, nwork, caps, groups, X, Y, Z, cen);
@@ -889,13 +1022,13 @@ cudaError_t launch_membrane(const RowWork* work, int nwork, const CapInfo* caps,
   if (nwork <= 0) return cudaSuccess;
   if constexpr (sizeof(T) == 4) {
     const size_t smem = membrane_f2_smem(nmax);
-    cudaError_t e = cudaFuncSetAttribute(membrane_kernel_f2, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    cudaError_t e = smem_limit_max(membrane_kernel_f2);
     if (e != cudaSuccess) return e;
     membrane_kernel_f2<<<persistent_grid(membrane_kernel_f2, smem, nwork), kPointThreads, smem, st>>>(
         work, nwork, caps, groups, sur_flag, err);
   } else {
     const size_t smem = pointwise_smem<T>(kMembrane, nmax);
-    cudaError_t e = cudaFuncSetAttribute(membrane_kernel<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    cudaError_t e = smem_limit_max(membrane_kernel<T>);
     if (e != cudaSuccess) return e;
     membrane_kernel<T><<<persistent_grid(membrane_kernel<T>, smem, nwork), kPointThreads, smem, st>>>(
         work, nwork, caps, groups, sur_flag, err);
@@ -908,7 +1041,7 @@ cudaError_t launch_shgrid(const RowWork* work, int nwork, const CapInfo* caps, c
                           int* err, cudaStream_t st) {
   if (nwork <= 0) return cudaSuccess;
   const size_t smem = pointwise_smem<T>(kShgrid, nmax);
-  cudaError_t e = cudaFuncSetAttribute(shgrid_kernel<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  cudaError_t e = smem_limit_max(shgrid_kernel<T>);
   if (e != cudaSuccess) return e;
   shgrid_kernel<T><<<persistent_grid(shgrid_kernel<T>, smem, nwork), kPointThreads, smem, st>>>(work, nwork, caps,
                                                                                                   groups, err);
@@ -921,11 +1054,35 @@ cudaError_t launch_final(const RowWork* work, int nwork, const CapInfo* caps, co
                          cudaStream_t st) {
   if (nwork <= 0) return cudaSuccess;
   const size_t smem = pointwise_smem<T>(kFinal, nmax);
-  cudaError_t e = cudaFuncSetAttribute(final_kernel<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  cudaError_t e = smem_limit_max(final_kernel<T>);
   if (e != cudaSuccess) return e;
   final_kernel<T><<<persistent_grid(final_kernel<T>, smem, nwork), kPointThreads, smem, st>>>(
       work, nwork, caps, groups, FX, FY, FZ, NX, NY, NZ, AREA, (ForceRec<T>*)frc, dvi, err);
   return cudaGetLastError();
+}
+
+// Shared memory of the fused force stage: the largest of its pointwise
+// stages' and of the staged A rows (rpc M K floats) of its contractions.
+size_t fused_force_smem(int nmax, size_t max_contract_floats);
+
+cudaError_t launch_force_fused(const int* order, int ncap, const CapInfo* caps, const GroupDev* groups,
+                               const LegProblem* probs, const double* X, const double* Y, const double* Z, double* cen,
+                               float* FX, float* FY, float* FZ, float* NX, float* NY, float* NZ, float* AREA, void* frc,
+                               double dvi, int nmax, size_t max_contract_floats, cudaStream_t st) {
+  if (ncap <= 0) return cudaSuccess;
+  const size_t smem = fused_force_smem(nmax, max_contract_floats);
+  cudaError_t e = smem_limit_max(force_fused_kernel);
+  if (e != cudaSuccess) return e;
+  force_fused_kernel<<<persistent_grid(force_fused_kernel, smem, ncap), kPointThreads, smem, st>>>(
+      order, ncap, caps, groups, probs, X, Y, Z, cen, FX, FY, FZ, NX, NY, NZ, AREA, (ForceRec<float>*)frc, dvi);
+  return cudaGetLastError();
+}
+
+size_t fused_force_smem(int nmax, size_t max_contract_floats) {
+  size_t b = std::max(pointwise_smem<float>(kPosfwd, nmax), membrane_f2_smem(nmax));
+  b = std::max(b, pointwise_smem<float>(kShgrid, nmax));
+  b = std::max(b, pointwise_smem<float>(kFinal, nmax));
+  return std::max(b, sizeof(float) * max_contract_floats);
 }
 
 #define SG_INST(T)                                                                                                    \

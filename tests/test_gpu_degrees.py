@@ -4,7 +4,9 @@ Capsules of degree 2, 8 (odd N = 9), 16 (N = 17), 22 and 23 (N = 24: the
 largest tensor-core operands, J = 3 nD = 144 columns, 256 TMEM columns) are
 stepped together.  FP64 against the oracle at the FP64 tolerances, mixed
 within 1e-4 for every capsule, for every capsule split of the persistent
-kernels.  The mixed path's automatic split mode runs degrees >= 16 in BF16x6:
+kernels, with the mixed path's force stage fused (one kernel per capsule,
+FP32 contractions) and staged (tensor cores).  The staged mixed path's
+automatic split mode runs degrees >= 16 in BF16x6:
 forced to BF16x3, the degree-22 capsule's force error exceeds 1e-4 (the
 second derivatives of the shape amplify the ~2^-17 product error about as
 L^2), which the last test shows.
@@ -27,13 +29,15 @@ def case():
     return wl, ref
 
 
-@pytest.mark.parametrize("precision", ["fp64", "mixed"])
+@pytest.mark.parametrize("precision,fused", [("fp64", False), ("mixed", False), ("mixed", True)])
 @pytest.mark.parametrize("split", [1, 8])
-def test_uneven_degrees(cuda, case, precision, split):
+def test_uneven_degrees(cuda, case, precision, fused, split):
     wl, ref = case
     dt = np.float64 if precision == "fp64" else np.float32
     u, v, w = (a.astype(dt) for a in wl.velocity())
     cs = CouplingStep(wl.grid, wl.degree, wl.radius, precision=precision)
+    if precision == "mixed":
+        cs.set_fused_force(fused)
     cs.set_point_split(split)
     out = cs.step(u, v, w, wl.x, wl.y, wl.z)
     tol_f, tol_u = (1e-10, 1e-12) if precision == "fp64" else (1e-4, 1e-4)
@@ -59,6 +63,7 @@ def test_split_modes(cuda, case):
     wl, ref = case
     u, v, w = (a.astype(np.float32) for a in wl.velocity())
     cs = CouplingStep(wl.grid, wl.degree, wl.radius, precision="mixed")
+    cs.set_fused_force(False)  # the staged force stage, contractions on the tensor cores
     assert [cs.legendre_terms(L) for L in (2, 15, 16, 23)] == [3, 3, 6, 6]
     err = {}
     for terms in (3, 6):

@@ -139,6 +139,7 @@ def test_legendre_tile_rows_do_not_change_results(cuda):
     wl = W.small_config()
     u, v, w = (a.astype(np.float32) for a in wl.velocity())
     cs = CouplingStep(wl.grid, wl.degree, wl.radius, precision="mixed")
+    cs.set_fused_force(False)  # the tensor-core contractions of the staged force stage
     assert cs.legendre_tile_rows() == 128
     a = cs.step(u, v, w, wl.x, wl.y, wl.z)
     a = {k: [x.copy() for x in val] if isinstance(val, tuple) or isinstance(val, list) else val.copy()
