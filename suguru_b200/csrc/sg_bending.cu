@@ -303,6 +303,7 @@ __global__ void __launch_bounds__(256) membrane_bend_kernel(const RowWork* __res
                                                             const CapInfo* __restrict__ caps,
                                                             const GroupDev* __restrict__ groups,
                                                             const int* __restrict__ sur_flag) {
+  pdl_enter();
   extern __shared__ __align__(16) unsigned char smem_raw[];
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5, nwarp = blockDim.x >> 5;
   for (int w = blockIdx.x; w < nwork; w += gridDim.x) {
@@ -485,7 +486,7 @@ cudaError_t launch_membrane_bend(const RowWork* work, int nwork, const CapInfo* 
   if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, membrane_bend_kernel<T>, 256, smem) != cudaSuccess || per < 1)
     per = 1;
   const int grid = std::min(nwork, sms * per);
-  membrane_bend_kernel<T><<<grid, 256, smem, st>>>(work, nwork, caps, groups, sur_flag);
+  launch_pdl(membrane_bend_kernel<T>, dim3(grid), dim3(256), smem, st, work, nwork, caps, groups, sur_flag);
   return cudaGetLastError();
 }
 

@@ -92,6 +92,37 @@ inline cudaError_t smem_limit_max(K kernel) {
   return e;
 }
 
+// Programmatic dependent launch.  The step's kernels follow one another on
+// a stream; launched with launch_pdl, a kernel's grid may be set up while its
+// predecessor is still running.  Each such kernel calls pdl_wait() before it
+// reads anything an earlier kernel wrote (it returns once the predecessor has
+// completed and its writes are visible), and pdl_launch_dependents() to let
+// its own successor be set up: called by every CTA at its start, so the
+// successor's CTAs come only after all of this grid's CTAs are resident or
+// done.  In a kernel launched without the attribute both are no-ops.
+__device__ __forceinline__ void pdl_wait() { asm volatile("griddepcontrol.wait;" ::: "memory"); }
+__device__ __forceinline__ void pdl_launch_dependents() { asm volatile("griddepcontrol.launch_dependents;" ::: "memory"); }
+__device__ __forceinline__ void pdl_enter() {
+  pdl_wait();
+  pdl_launch_dependents();
+}
+
+template <class... KArgs, class... Args>
+inline cudaError_t launch_pdl(void (*kernel)(KArgs...), dim3 grid, dim3 block, size_t smem, cudaStream_t st,
+                              Args... args) {
+  cudaLaunchConfig_t cfg{};
+  cfg.gridDim = grid;
+  cfg.blockDim = block;
+  cfg.dynamicSmemBytes = smem;
+  cfg.stream = st;
+  cudaLaunchAttribute at[1];
+  at[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+  at[0].val.programmaticStreamSerializationAllowed = 1;
+  cfg.attrs = at;
+  cfg.numAttrs = 1;
+  return cudaLaunchKernelEx(&cfg, kernel, args...);
+}
+
 // Asynchronous copy of one 4- or 8-byte element from global to shared memory
 // (cp.async, no register round trip): a staging loop issues all of its
 // copies before any completes; stage_wait() waits for this thread's copies,

@@ -50,6 +50,7 @@ template <class T>
 __global__ void bin_points_kernel(IBGrid g, long n, const double* __restrict__ X, const double* __restrict__ Y,
                                   const double* __restrict__ Z, PosRec<T>* __restrict__ pos,
                                   int* __restrict__ counts) {
+  pdl_enter();
   const long p = (long)blockIdx.x * blockDim.x + threadIdx.x;
   const bool valid = p < n;
   int tx[2] = {0, 0}, ty[2] = {0, 0}, tz[2] = {0, 0}, nx = 0, ny = 0, nz = 0;
@@ -89,6 +90,7 @@ __global__ void bin_points_kernel(IBGrid g, long n, const double* __restrict__ X
 // run's starts from its offset -- one pass over the counts, two barriers.
 __global__ void __launch_bounds__(1024) scan_counts_kernel(int ntiles, const int* __restrict__ counts,
                                                            int* __restrict__ starts, int* __restrict__ fill) {
+  pdl_enter();
   __shared__ int warp_sum[32];
   const int t = threadIdx.x, lane = t & 31, warp = t >> 5;
   const int per = (ntiles + 1023) / 1024;
@@ -125,6 +127,7 @@ __global__ void __launch_bounds__(1024) scan_counts_kernel(int ntiles, const int
 template <class T>
 __global__ void bin_scatter_kernel(IBGrid g, long n, const PosRec<T>* __restrict__ pos,
                                    const int* __restrict__ starts, int* __restrict__ fill, int* __restrict__ entries) {
+  pdl_enter();
   const long p = (long)blockIdx.x * blockDim.x + threadIdx.x;
   int tx[2] = {0, 0}, ty[2] = {0, 0}, tz[2] = {0, 0}, nx = 0, ny = 0, nz = 0;
   if (p < n) {
@@ -164,6 +167,7 @@ __global__ void __launch_bounds__(256) interp_kernel(IBGrid g, long n, const Pos
                                                      const T* __restrict__ u, const T* __restrict__ v,
                                                      const T* __restrict__ w, T* __restrict__ U, T* __restrict__ V,
                                                      T* __restrict__ W) {
+  pdl_enter();
   const long t = (long)blockIdx.x * blockDim.x + threadIdx.x;
   if (t >= 3 * n) return;
   const int c = (int)(t / n);
@@ -218,10 +222,10 @@ cudaError_t launch_bin(const IBGrid& g, long n, const double* X, const double* Y
   cudaError_t e = cudaMemsetAsync(w.counts, 0, sizeof(int) * g.ntiles, st);
   if (e != cudaSuccess) return e;
   if (n > 0)
-    bin_points_kernel<T><<<(unsigned)((n + 255) / 256), 256, 0, st>>>(g, n, X, Y, Z, (PosRec<T>*)w.pos, w.counts);
-  scan_counts_kernel<<<1, 1024, 0, st>>>(g.ntiles, w.counts, w.starts, w.fill);
+    launch_pdl(bin_points_kernel<T>, dim3((unsigned)((n + 255) / 256)), dim3(256), 0, st, g, n, X, Y, Z, (PosRec<T>*)w.pos, w.counts);
+  launch_pdl(scan_counts_kernel, dim3(1), dim3(1024), 0, st, g.ntiles, w.counts, w.starts, w.fill);
   if (n > 0)
-    bin_scatter_kernel<T><<<(unsigned)((n + 255) / 256), 256, 0, st>>>(g, n, (const PosRec<T>*)w.pos, w.starts,
+    launch_pdl(bin_scatter_kernel<T>, dim3((unsigned)((n + 255) / 256)), dim3(256), 0, st, g, n, (const PosRec<T>*)w.pos, w.starts,
                                                                         w.fill, w.entries);
   return cudaGetLastError();
 }
@@ -230,7 +234,7 @@ template <class T>
 cudaError_t launch_interp(const IBGrid& g, long n, const IBWork& w, const T* u, const T* v, const T* ww, T* U, T* V,
                           T* W, cudaStream_t st) {
   if (n <= 0) return cudaSuccess;
-  interp_kernel<T><<<(unsigned)((3 * n + 255) / 256), 256, 0, st>>>(g, n, (const PosRec<T>*)w.pos, u, v, ww, U, V,
+  launch_pdl(interp_kernel<T>, dim3((unsigned)((3 * n + 255) / 256)), dim3(256), 0, st, g, n, (const PosRec<T>*)w.pos, u, v, ww, U, V,
                                                                      W);
   return cudaGetLastError();
 }

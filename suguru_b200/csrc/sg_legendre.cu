@@ -17,6 +17,7 @@ constexpr int LEG_QT = 32;
 template <class T>
 __global__ void __launch_bounds__(256) legendre_kernel(const LegProblem* __restrict__ probs,
                                                        const LegWork* __restrict__ work, int nwork) {
+  pdl_enter();
   extern __shared__ __align__(16) unsigned char smem_raw[];
   if ((int)blockIdx.x >= nwork) return;
   const LegWork wk = work[blockIdx.x];
@@ -68,7 +69,7 @@ cudaError_t launch_legendre(const LegProblem* d_probs, const LegWork* d_work, in
   if (smem > (size_t)optin) return cudaErrorInvalidValue;
   e = smem_limit_max(legendre_kernel<T>);
   if (e != cudaSuccess) return e;
-  legendre_kernel<T><<<nwork, 256, smem, st>>>(d_probs, d_work, nwork);
+  launch_pdl(legendre_kernel<T>, dim3(nwork), dim3(256), smem, st, d_probs, d_work, nwork);
   return cudaGetLastError();
 }
 

@@ -142,6 +142,7 @@ __global__ void __launch_bounds__(kLegThreads, kLegPerSm) legendre_mma_kernel(co
                                                                     const LegWork* __restrict__ work, int nwork,
                                                                     LegLevels lv, int nparts, int tmem_cols,
                                                                     int off2, int* __restrict__ err) {
+  pdl_enter();
   extern __shared__ __align__(128) unsigned char smem_raw[];
   __shared__ __align__(8) uint64_t s_bar;
   __shared__ __align__(8) uint64_t s_tbar[3];
@@ -401,11 +402,11 @@ cudaError_t launch_legendre_mma(const LegProblem* d_probs, const LegWork* d_work
   if (tm == 64) {
     e = smem_limit_max(legendre_mma_kernel<64>);
     if (e != cudaSuccess) return e;
-    legendre_mma_kernel<64><<<grid, kLegThreads, smem, st>>>(d_probs, d_work, nwork, lv, nparts, cols, off2, d_err);
+    launch_pdl(legendre_mma_kernel<64>, dim3(grid), dim3(kLegThreads), smem, st, d_probs, d_work, nwork, lv, nparts, cols, off2, d_err);
   } else {
     e = smem_limit_max(legendre_mma_kernel<128>);
     if (e != cudaSuccess) return e;
-    legendre_mma_kernel<128><<<grid, kLegThreads, smem, st>>>(d_probs, d_work, nwork, lv, nparts, cols, off2,
+    launch_pdl(legendre_mma_kernel<128>, dim3(grid), dim3(kLegThreads), smem, st, d_probs, d_work, nwork, lv, nparts, cols, off2,
                                                               d_err);
   }
   return cudaGetLastError();

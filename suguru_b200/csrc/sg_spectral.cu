@@ -123,6 +123,7 @@ __device__ __forceinline__ void centroid_block(int cap, const CapInfo* __restric
 __global__ void __launch_bounds__(256) centroid_kernel(int ncap, const CapInfo* __restrict__ caps,
                                                        const double* __restrict__ X, const double* __restrict__ Y,
                                                        const double* __restrict__ Z, double* __restrict__ cen) {
+  pdl_enter();
   if ((int)blockIdx.x < ncap) centroid_block(blockIdx.x, caps, X, Y, Z, cen);
 }
 
@@ -198,6 +199,7 @@ __global__ void __launch_bounds__(256) posfwd_kernel(const RowWork* __restrict__
                                                      const GroupDev* __restrict__ groups, const double* __restrict__ X,
                                                      const double* __restrict__ Y, const double* __restrict__ Z,
                                                      const double* __restrict__ cen) {
+  pdl_enter();
   for (int w = blockIdx.x; w < nwork; w += gridDim.x) posfwd_item<T>(work[w], caps, groups, X, Y, Z, cen);
 }
 
@@ -302,6 +304,7 @@ __global__ void __launch_bounds__(256, sizeof(T) == 4 ? 3 : 2) membrane_kernel(c
                                                        const CapInfo* __restrict__ caps,
                                                        const GroupDev* __restrict__ groups,
                                                        const int* __restrict__ sur_flag, int* __restrict__ err) {
+  pdl_enter();
   (void)err;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5, nwarp = blockDim.x >> 5;
@@ -556,6 +559,7 @@ __global__ void __launch_bounds__(256, 3) membrane_kernel_f2(const RowWork* __re
                                                              const CapInfo* __restrict__ caps,
                                                              const GroupDev* __restrict__ groups,
                                                              const int* __restrict__ sur_flag, int* __restrict__ err) {
+  pdl_enter();
   for (int w = blockIdx.x; w < nwork; w += gridDim.x) membrane_item_f2(work[w], caps, groups, sur_flag, err);
 }
 
@@ -720,6 +724,7 @@ template <class T>
 __global__ void __launch_bounds__(256) shgrid_kernel(const RowWork* __restrict__ work, int nwork,
                                                      const CapInfo* __restrict__ caps,
                                                      const GroupDev* __restrict__ groups, int* __restrict__ err) {
+  pdl_enter();
   for (int w = blockIdx.x; w < nwork; w += gridDim.x) shgrid_item<T>(work[w], caps, groups, err);
 }
 
@@ -836,6 +841,7 @@ __global__ void __launch_bounds__(256) final_kernel(const RowWork* __restrict__ 
                                                     T* __restrict__ NY, T* __restrict__ NZ, T* __restrict__ AREA,
                                                     ForceRec<T>* __restrict__ frc, double dvi,
                                                     int* __restrict__ err) {
+  pdl_enter();
   for (int w = blockIdx.x; w < nwork; w += gridDim.x) final_item<T>(work[w], caps, groups, FX, FY, FZ, NX, NY, NZ, AREA, frc, dvi, err);
 }
 
@@ -1007,11 +1013,11 @@ template <class T>
 cudaError_t launch_posfwd(const RowWork* work, int nwork, const CapInfo* caps, const GroupDev* groups, const double* X,
                           const double* Y, const double* Z, int ncap, double* cen, int nmax, cudaStream_t st) {
   if (nwork <= 0 || ncap <= 0) return cudaSuccess;
-  centroid_kernel<<<ncap, 256, 0, st>>>(ncap, caps, X, Y, Z, cen);
+  launch_pdl(centroid_kernel, dim3(ncap), dim3(256), 0, st, ncap, caps, X, Y, Z, cen);
   const size_t smem = pointwise_smem<T>(kPosfwd, nmax);
   cudaError_t e = smem_limit_max(posfwd_kernel<T>);
   if (e != cudaSuccess) return e;
-  posfwd_kernel<T><<<persistent_grid(posfwd_kernel<T>, smem, nwork), kPointThreads, smem, st>>>(
+  launch_pdl(posfwd_kernel<T>, dim3(persistent_grid(posfwd_kernel<T>, smem, nwork)), dim3(kPointThreads), smem, st, 
       work, nwork, caps, groups, X, Y, Z, cen);
   return cudaGetLastError();
 }
@@ -1024,13 +1030,13 @@ cudaError_t launch_membrane(const RowWork* work, int nwork, const CapInfo* caps,
     const size_t smem = membrane_f2_smem(nmax);
     cudaError_t e = smem_limit_max(membrane_kernel_f2);
     if (e != cudaSuccess) return e;
-    membrane_kernel_f2<<<persistent_grid(membrane_kernel_f2, smem, nwork), kPointThreads, smem, st>>>(
+    launch_pdl(membrane_kernel_f2, dim3(persistent_grid(membrane_kernel_f2, smem, nwork)), dim3(kPointThreads), smem, st, 
         work, nwork, caps, groups, sur_flag, err);
   } else {
     const size_t smem = pointwise_smem<T>(kMembrane, nmax);
     cudaError_t e = smem_limit_max(membrane_kernel<T>);
     if (e != cudaSuccess) return e;
-    membrane_kernel<T><<<persistent_grid(membrane_kernel<T>, smem, nwork), kPointThreads, smem, st>>>(
+    launch_pdl(membrane_kernel<T>, dim3(persistent_grid(membrane_kernel<T>, smem, nwork)), dim3(kPointThreads), smem, st, 
         work, nwork, caps, groups, sur_flag, err);
   }
   return cudaGetLastError();
@@ -1043,7 +1049,7 @@ cudaError_t launch_shgrid(const RowWork* work, int nwork, const CapInfo* caps, c
   const size_t smem = pointwise_smem<T>(kShgrid, nmax);
   cudaError_t e = smem_limit_max(shgrid_kernel<T>);
   if (e != cudaSuccess) return e;
-  shgrid_kernel<T><<<persistent_grid(shgrid_kernel<T>, smem, nwork), kPointThreads, smem, st>>>(work, nwork, caps,
+  launch_pdl(shgrid_kernel<T>, dim3(persistent_grid(shgrid_kernel<T>, smem, nwork)), dim3(kPointThreads), smem, st, work, nwork, caps,
                                                                                                   groups, err);
   return cudaGetLastError();
 }
@@ -1056,7 +1062,7 @@ cudaError_t launch_final(const RowWork* work, int nwork, const CapInfo* caps, co
   const size_t smem = pointwise_smem<T>(kFinal, nmax);
   cudaError_t e = smem_limit_max(final_kernel<T>);
   if (e != cudaSuccess) return e;
-  final_kernel<T><<<persistent_grid(final_kernel<T>, smem, nwork), kPointThreads, smem, st>>>(
+  launch_pdl(final_kernel<T>, dim3(persistent_grid(final_kernel<T>, smem, nwork)), dim3(kPointThreads), smem, st, 
       work, nwork, caps, groups, FX, FY, FZ, NX, NY, NZ, AREA, (ForceRec<T>*)frc, dvi, err);
   return cudaGetLastError();
 }

@@ -207,6 +207,7 @@ __device__ __forceinline__ void tile_scales(int e0, int e1, const int* __restric
 template <class T>
 __global__ void pack_forces_kernel(long n, double dvi, const T* __restrict__ FX, const T* __restrict__ FY,
                                    const T* __restrict__ FZ, const T* __restrict__ A, ForceRec<T>* __restrict__ frc) {
+  pdl_enter();
   const long p = (long)blockIdx.x * blockDim.x + threadIdx.x;
   if (p >= n) return;
   const T s = A[p] * (T)dvi;
@@ -227,6 +228,7 @@ __global__ void __launch_bounds__(256, sizeof(T) == 4 ? 4 : 2) spread_kernel(IBG
                                                      const PosRec<T>* __restrict__ pos,
                                                      const ForceRec<T>* __restrict__ frc, T* __restrict__ ox,
                                                      T* __restrict__ oy, T* __restrict__ oz) {
+  pdl_enter();
   constexpr bool F32 = sizeof(T) == 4;
   constexpr int NC = TX * TY * TZ;
   constexpr int NW = Fixed<T>::NW;
@@ -435,6 +437,7 @@ __global__ void __launch_bounds__(256, 4) spread_rows_kernel(IBGrid g, const int
                                                              const ForceRec<float>* __restrict__ frc,
                                                              float* __restrict__ ox, float* __restrict__ oy,
                                                              float* __restrict__ oz) {
+  pdl_enter();
   extern __shared__ __align__(16) unsigned int racc[];  // [3][NCP]
   __shared__ float s_red[3][8];
   __shared__ unsigned long long s_sum[3][8];
@@ -572,14 +575,14 @@ static cudaError_t spread_rows(const IBGrid& g, const IBWork& w, float* ox, floa
   if (!smem || g.TX != g.itot || g.TY != TY || g.TZ != TZ) return cudaErrorInvalidValue;
   cudaError_t e = smem_limit_max(spread_rows_kernel<TY, TZ>);
   if (e != cudaSuccess) return e;
-  spread_rows_kernel<TY, TZ><<<g.ntiles, 256, smem, st>>>(g, w.entries, w.starts, (const PosRec<float>*)w.pos,
+  launch_pdl(spread_rows_kernel<TY, TZ>, dim3(g.ntiles), dim3(256), smem, st, g, w.entries, w.starts, (const PosRec<float>*)w.pos,
                                                          (const ForceRec<float>*)w.frc, ox, oy, oz);
   return cudaGetLastError();
 }
 
 template <class T, int TX, int TY, int TZ, bool CTR = false>
 static void spread_one(const IBGrid& g, const IBWork& w, T* ox, T* oy, T* oz, cudaStream_t st) {
-  spread_kernel<T, TX, TY, TZ, CTR><<<g.ntiles, 256, 0, st>>>(g, w.entries, w.starts, (const PosRec<T>*)w.pos,
+  launch_pdl(spread_kernel<T, TX, TY, TZ, CTR>, dim3(g.ntiles), dim3(256), 0, st, g, w.entries, w.starts, (const PosRec<T>*)w.pos,
                                                                (const ForceRec<T>*)w.frc, ox, oy, oz);
 }
 
@@ -587,7 +590,7 @@ template <class T>
 cudaError_t launch_pack_forces(const IBGrid& g, long n, const T* FX, const T* FY, const T* FZ, const T* A, IBWork& w,
                                cudaStream_t st) {
   if (n <= 0) return cudaSuccess;
-  pack_forces_kernel<T><<<(unsigned)((n + 255) / 256), 256, 0, st>>>(n, g.dvi, FX, FY, FZ, A, (ForceRec<T>*)w.frc);
+  launch_pdl(pack_forces_kernel<T>, dim3((unsigned)((n + 255) / 256)), dim3(256), 0, st, n, g.dvi, FX, FY, FZ, A, (ForceRec<T>*)w.frc);
   return cudaGetLastError();
 }
 
