@@ -310,6 +310,11 @@ def run_ours(args):
     # the force stage as one fused kernel (FP32 contractions on CUDA cores), as the comparison
     csm.set_fused_force(True)
     fused = time_path(csm, "mixed")
+    # the reference's default bending (ibend = 1, ebend = cbend gscell with cbend = 0.3, in
+    # units of the capsule radius)
+    csm.set_fused_force(False)
+    csm.set_capsule_bending(0.3 * wl.gs * wl.radius**2)
+    bending = time_path(csm, "mixed")
     csm.close()
 
     # ---- surrogate: linear response, plain-model training data, the library's training kernels
@@ -421,6 +426,12 @@ def run_ours(args):
                          "achieved": achieved, "peak": hbm_peak, "unit": "GB/s", "frac": achieved / hbm_peak,
                          "peak_kind": peak_kind, "algorithmic_bytes": sbytes, "traffic": traffic},
             "roofline_legendre": legendre_roofline(mixed, tc_peak, peak_kind),
+            "mixed_bending": {
+                "value": world * n / (bending["ms_per_step"] / 1e3), "unit": "points/s",
+                "ms_per_step": bending["ms_per_step"], "stages_ms": bending["stages"],
+                "note": "the same step with the reference's default bending (ibend = 1, cbend = 0.3): "
+                        "one more contraction for the third and fourth derivatives, the bending "
+                        "membrane kernel, BF16x6 products"},
             "mixed_fused_force": {
                 "value": world * n / (fused["ms_per_step"] / 1e3), "unit": "points/s",
                 "ms_per_step": fused["ms_per_step"], "stages_ms": fused["stages"],

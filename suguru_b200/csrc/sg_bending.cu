@@ -478,7 +478,7 @@ cudaError_t launch_membrane_bend(const RowWork* work, int nwork, const CapInfo* 
     e = std::max(e, en);
   }
   const size_t smem = sizeof(T) * e;
-  cudaError_t err = smem_limit_max(membrane_bend_kernel<T>);
+  cudaError_t err = smem_limit(membrane_bend_kernel<T>, smem);
   if (err != cudaSuccess) return err;
   int dev = 0, sms = 148, per = 1;
   cudaGetDevice(&dev);

@@ -72,40 +72,32 @@ SG_HD T dot3(const T* u, const T* v) {
 }
 
 #if defined(__CUDACC__)
-// Lets a kernel take up to the device's opt-in limit of dynamic shared memory
-// (less its static shared memory).  Every launcher sets this one value
-// instead of its own request: a kernel launched with different requests
-// (the Legendre stages, contexts of different degrees) would otherwise carry
-// whatever its last launcher set, and a launch outside that launcher's
-// sequence -- a CUDA graph node replayed on its own, as a profiler does --
-// could ask for more than that limit and fail to launch.  The launch's own
-// request still sets its occupancy.
+// Raises a kernel's dynamic shared-memory limit to at least `bytes`, and
+// never lowers it.  A kernel launched with different requests (the Legendre
+// stages, contexts of different degrees) would otherwise keep whatever its
+// last launcher set, and a launch outside that launcher's sequence -- a CUDA
+// graph node replayed on its own, as a profiler does -- could ask for more
+// than that and fail to launch.  The limit stays at the largest request
+// made, not the device maximum, which could otherwise steer the shared
+// memory / L1 split of the SMs that other kernels share.
 template <class K>
-inline cudaError_t smem_limit_max(K kernel) {
-  int dev = 0, optin = 0;
-  cudaError_t e = cudaGetDevice(&dev);
-  if (e == cudaSuccess) e = cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
+inline cudaError_t smem_limit(K kernel, size_t bytes) {
   cudaFuncAttributes fa{};
-  if (e == cudaSuccess) e = cudaFuncGetAttributes(&fa, kernel);
-  if (e == cudaSuccess)
-    e = cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, optin - (int)fa.sharedSizeBytes);
-  return e;
+  cudaError_t e = cudaFuncGetAttributes(&fa, kernel);
+  if (e != cudaSuccess || (size_t)fa.maxDynamicSharedSizeBytes >= bytes) return e;
+  return cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
 }
 
 // Programmatic dependent launch.  The step's kernels follow one another on
-// a stream; launched with launch_pdl, a kernel's grid may be set up while its
-// predecessor is still running.  Each such kernel calls pdl_wait() before it
-// reads anything an earlier kernel wrote (it returns once the predecessor has
-// completed and its writes are visible), and pdl_launch_dependents() to let
-// its own successor be set up: called by every CTA at its start, so the
-// successor's CTAs come only after all of this grid's CTAs are resident or
-// done.  In a kernel launched without the attribute both are no-ops.
-__device__ __forceinline__ void pdl_wait() { asm volatile("griddepcontrol.wait;" ::: "memory"); }
-__device__ __forceinline__ void pdl_launch_dependents() { asm volatile("griddepcontrol.launch_dependents;" ::: "memory"); }
-__device__ __forceinline__ void pdl_enter() {
-  pdl_wait();
-  pdl_launch_dependents();
-}
+// a stream; launched with launch_pdl, a kernel's grid is set up while its
+// predecessor is still running and starts as the predecessor's last CTAs
+// retire.  Each such kernel calls pdl_enter() first: it returns once the
+// predecessor has completed and its writes are visible.  The successor is
+// released implicitly as each CTA exits -- not earlier, since CTAs of a
+// successor that wait for their predecessor would hold SM slots that the
+// kernels of the step's other stream need.  Without the launch attribute the
+// wait is a no-op.
+__device__ __forceinline__ void pdl_enter() { asm volatile("griddepcontrol.wait;" ::: "memory"); }
 
 template <class... KArgs, class... Args>
 inline cudaError_t launch_pdl(void (*kernel)(KArgs...), dim3 grid, dim3 block, size_t smem, cudaStream_t st,

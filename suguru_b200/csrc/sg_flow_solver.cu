@@ -103,20 +103,26 @@ __device__ __forceinline__ double momentum_rhs(const FGrid& g, const Fields& F, 
   return d * rep;
 }
 
-// Blocks of 32 x 8 cells in (x, y) at one z level, so that the stencil's y
-// neighbours of a warp are mostly the block's own loads (L1), not L2's.
+// Blocks of 32 x 8 cells in (x, y) that march up kMomZ consecutive z levels,
+// so that the stencil's y neighbours of a warp are mostly the block's own
+// loads and its z neighbours the block's loads of the levels just before
+// and after (L1), not L2's.
+constexpr int kMomZ = 8;
+
 __global__ void __launch_bounds__(256) momentum_rhs_kernel(FGrid g, Fields F, double dt, double rep,
                                                            double* __restrict__ ru, double* __restrict__ rv,
                                                            double* __restrict__ rw) {
   const int nbx = (g.itot + 31) / 32;
   const int i = (int)(blockIdx.x % nbx) * 32 + (int)(threadIdx.x & 31) + 1;
   const int j = (int)(blockIdx.x / nbx) * 8 + (int)(threadIdx.x >> 5) + 1;
-  const int k = (int)blockIdx.y + 1;
   if (i > g.itot || j > g.jtot) return;
-  const long q = ((long)(k - 1) * g.jtot + (j - 1)) * g.itot + (i - 1);
-  ru[q] = momentum_rhs<0>(g, F, dt, rep, i, j, k);
-  rv[q] = momentum_rhs<1>(g, F, dt, rep, i, j, k);
-  rw[q] = k == g.ktot ? 0.0 : momentum_rhs<2>(g, F, dt, rep, i, j, k);  // dwdt(i,j,kmax) = 0 (fftuvw.f90:86-92)
+  const int k0 = (int)blockIdx.y * kMomZ + 1, k1 = min(k0 + kMomZ, g.ktot + 1);
+  for (int k = k0; k < k1; ++k) {
+    const long q = ((long)(k - 1) * g.jtot + (j - 1)) * g.itot + (i - 1);
+    ru[q] = momentum_rhs<0>(g, F, dt, rep, i, j, k);
+    rv[q] = momentum_rhs<1>(g, F, dt, rep, i, j, k);
+    rw[q] = k == g.ktot ? 0.0 : momentum_rhs<2>(g, F, dt, rep, i, j, k);  // dwdt(i,j,kmax) = 0 (fftuvw.f90:86-92)
+  }
 }
 
 // bounduvw (mode 0: u; 1: v with wall values vb2, vt2; 2: w) or boundp (mode
@@ -243,7 +249,7 @@ int flow_run(sg_ctx* c, double dt, const double* uo, const double* vo, const dou
   double* rw = c->pois.r;
   Fields F{uo, vo, wo, uoo, voo, woo, p, fx, fy, fz};
   // fftuvw: right-hand sides, then w (initsolver(3)) and u, v (initsolver(2))
-  const dim3 mgrid((unsigned)(((f.itot + 31) / 32) * ((f.jtot + 7) / 8)), (unsigned)f.ktot);
+  const dim3 mgrid((unsigned)(((f.itot + 31) / 32) * ((f.jtot + 7) / 8)), (unsigned)((f.ktot + kMomZ - 1) / kMomZ));
   momentum_rhs_kernel<<<mgrid, 256, 0, st>>>(g, F, dt, s.rep, s.ru, s.rv, rw);
   SG_TRY(cudaGetLastError(), "momentum");
   // each solution goes, times 1 / (itot jtot), straight into its field

@@ -215,11 +215,11 @@ cudaError_t launch_gemm(const GemmArgs& g, int* d_err, cudaStream_t st) {
   ga.ksplit = ks;
   cudaError_t e;
   if (g.split) {
-    e = smem_limit_max(gemm_kernel<1>);
+    e = smem_limit(gemm_kernel<1>, smem);
     if (e != cudaSuccess) return e;
     gemm_kernel<1><<<grid, 128, smem, st>>>(ga, d_err);
   } else {
-    e = smem_limit_max(gemm_kernel<0>);
+    e = smem_limit(gemm_kernel<0>, smem);
     if (e != cudaSuccess) return e;
     gemm_kernel<0><<<grid, 128, smem, st>>>(ga, d_err);
   }

@@ -84,44 +84,76 @@ __global__ void bin_points_kernel(IBGrid g, long n, const double* __restrict__ X
 }
 
 // Exclusive scan of tile counts by one block of 1024 threads; starts has
-// ntiles+1 entries.  Thread t owns the run of `per` consecutive tiles starting
-// at t * per: it sums its run, the block scans the 1024 run totals (warp
-// shuffles, then one warp over the 32 warp totals), and each thread writes its
-// run's starts from its offset -- one pass over the counts, two barriers.
+// ntiles+1 entries.  The tiles go in chunks of 1024 x 8: thread t owns the 8
+// consecutive tiles from chunk + 8t (two 16-byte loads and stores, a warp's
+// accesses contiguous), the block scans the 1024 run totals (warp shuffles,
+// then one warp over the 32 warp totals) and each thread writes its run's
+// starts from its offset plus the running total of the earlier chunks.
 __global__ void __launch_bounds__(1024) scan_counts_kernel(int ntiles, const int* __restrict__ counts,
                                                            int* __restrict__ starts, int* __restrict__ fill) {
   pdl_enter();
+  constexpr int V = 8;
   __shared__ int warp_sum[32];
+  __shared__ int s_carry;
   const int t = threadIdx.x, lane = t & 31, warp = t >> 5;
-  const int per = (ntiles + 1023) / 1024;
-  const int b0 = t * per, b1 = min(b0 + per, ntiles);
-  int run = 0;
-  for (int i = b0; i < b1; ++i) run += counts[i];
-  int x = run;  // inclusive scan of the run totals within the warp
+  if (t == 0) s_carry = 0;
+  for (int c0 = 0; c0 < ntiles; c0 += 1024 * V) {
+    const int b0 = c0 + t * V;
+    int v[V];
+    if (b0 + V <= ntiles) {
+      const int4 lo = *(const int4*)(counts + b0), hi = *(const int4*)(counts + b0 + 4);
+      v[0] = lo.x; v[1] = lo.y; v[2] = lo.z; v[3] = lo.w; v[4] = hi.x; v[5] = hi.y; v[6] = hi.z; v[7] = hi.w;
+    } else {
 #pragma unroll
-  for (int o = 1; o < 32; o <<= 1) {
-    const int y = __shfl_up_sync(0xffffffffu, x, o);
-    if (lane >= o) x += y;
-  }
-  if (lane == 31) warp_sum[warp] = x;
-  __syncthreads();
-  if (warp == 0) {
-    int w = warp_sum[lane];
+      for (int q = 0; q < V; ++q) v[q] = b0 + q < ntiles ? counts[b0 + q] : 0;
+    }
+    int run = 0;
+#pragma unroll
+    for (int q = 0; q < V; ++q) run += v[q];
+    int x = run;  // inclusive scan of the run totals within the warp
 #pragma unroll
     for (int o = 1; o < 32; o <<= 1) {
-      const int y = __shfl_up_sync(0xffffffffu, w, o);
-      if (lane >= o) w += y;
+      const int y = __shfl_up_sync(0xffffffffu, x, o);
+      if (lane >= o) x += y;
     }
-    warp_sum[lane] = w;
+    if (lane == 31) warp_sum[warp] = x;
+    __syncthreads();  // the warp totals, and s_carry from the previous chunk
+    if (warp == 0) {
+      int w = warp_sum[lane];
+#pragma unroll
+      for (int o = 1; o < 32; o <<= 1) {
+        const int y = __shfl_up_sync(0xffffffffu, w, o);
+        if (lane >= o) w += y;
+      }
+      warp_sum[lane] = w;
+    }
+    __syncthreads();
+    const int carry = s_carry, chunk_total = warp_sum[31];
+    int excl = carry + (warp > 0 ? warp_sum[warp - 1] : 0) + x - run;
+    int st[V];
+#pragma unroll
+    for (int q = 0; q < V; ++q) {
+      st[q] = excl;
+      excl += v[q];
+    }
+    if (b0 + V <= ntiles) {
+      *(int4*)(starts + b0) = make_int4(st[0], st[1], st[2], st[3]);
+      *(int4*)(starts + b0 + 4) = make_int4(st[4], st[5], st[6], st[7]);
+      *(int4*)(fill + b0) = make_int4(0, 0, 0, 0);
+      *(int4*)(fill + b0 + 4) = make_int4(0, 0, 0, 0);
+    } else {
+#pragma unroll
+      for (int q = 0; q < V; ++q)
+        if (b0 + q < ntiles) {
+          starts[b0 + q] = st[q];
+          fill[b0 + q] = 0;
+        }
+    }
+    __syncthreads();  // every thread has read s_carry and warp_sum
+    if (t == 0) s_carry = carry + chunk_total;
   }
   __syncthreads();
-  int excl = (warp > 0 ? warp_sum[warp - 1] : 0) + x - run;
-  for (int i = b0; i < b1; ++i) {
-    starts[i] = excl;
-    fill[i] = 0;
-    excl += counts[i];
-  }
-  if (t == 1023) starts[ntiles] = warp_sum[31];
+  if (t == 0) starts[ntiles] = s_carry;
 }
 
 template <class T>

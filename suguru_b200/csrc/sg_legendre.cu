@@ -67,7 +67,7 @@ cudaError_t launch_legendre(const LegProblem* d_probs, const LegWork* d_work, in
   if (e == cudaSuccess) e = cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
   if (e != cudaSuccess) return e;
   if (smem > (size_t)optin) return cudaErrorInvalidValue;
-  e = smem_limit_max(legendre_kernel<T>);
+  e = smem_limit(legendre_kernel<T>, smem);
   if (e != cudaSuccess) return e;
   launch_pdl(legendre_kernel<T>, dim3(nwork), dim3(256), smem, st, d_probs, d_work, nwork);
   return cudaGetLastError();

@@ -400,11 +400,11 @@ cudaError_t launch_legendre_mma(const LegProblem* d_probs, const LegWork* d_work
   const int per_sm = std::min(kLegPerSm, 512 / cols);
   const int grid = nwork < num_sms * per_sm ? nwork : num_sms * per_sm;
   if (tm == 64) {
-    e = smem_limit_max(legendre_mma_kernel<64>);
+    e = smem_limit(legendre_mma_kernel<64>, smem);
     if (e != cudaSuccess) return e;
     launch_pdl(legendre_mma_kernel<64>, dim3(grid), dim3(kLegThreads), smem, st, d_probs, d_work, nwork, lv, nparts, cols, off2, d_err);
   } else {
-    e = smem_limit_max(legendre_mma_kernel<128>);
+    e = smem_limit(legendre_mma_kernel<128>, smem);
     if (e != cudaSuccess) return e;
     launch_pdl(legendre_mma_kernel<128>, dim3(grid), dim3(kLegThreads), smem, st, d_probs, d_work, nwork, lv, nparts, cols, off2,
                                                               d_err);

@@ -905,10 +905,10 @@ int poisson_solve(sg_ctx* c, double* r, int e, double shift, cudaStream_t st, co
   const size_t sm_f = sizeof(double2) * 2 * rpc * n, sm_i = sizeof(double2) * rpc * (2 * n + nxm);
   const size_t sm_c = sizeof(double2) * 2 * cpc * (f.jtot + 1);
   if (!rows_fast) {
-    SG_TRY(smem_limit_max(fft_rows_r2c), "fft");
-    SG_TRY(smem_limit_max(fft_rows_c2r), "fft");
+    SG_TRY(smem_limit(fft_rows_r2c, sm_f), "fft");
+    SG_TRY(smem_limit(fft_rows_c2r, sm_i), "fft");
   }
-  if (!cols_fast) SG_TRY(smem_limit_max(fft_cols), "fft");
+  if (!cols_fast) SG_TRY(smem_limit(fft_cols, sm_c), "fft");
   const unsigned gr = (unsigned)((nrows + rpc - 1) / rpc);
   const dim3 gc((unsigned)((nxm + cpc - 1) / cpc), (unsigned)f.ktot);
   double2* modes = (double2*)s.c;

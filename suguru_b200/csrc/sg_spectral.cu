@@ -863,7 +863,7 @@ __global__ void __launch_bounds__(256) final_kernel(const RowWork* __restrict__ 
 // [m][k][r] (its R rows side by side), then thread task (m, j) forms the R
 // sums, reading B_m[j][k] from the (L2-resident) FP32 table.
 template <int R>
-__device__ __forceinline__ void contract_rows(const LegProblem& P, long long gidx, float* sA, int part, int nparts) {
+__device__ __forceinline__ void contract_rows(const LegProblem& P, long long gidx, float* sA) {
   const int M = P.M, J = P.J, K = P.K;
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5, nwarp = blockDim.x >> 5;
   const float* A = (const float*)P.A + gidx * P.sAc;
@@ -876,8 +876,7 @@ __device__ __forceinline__ void contract_rows(const LegProblem& P, long long gid
     for (int k = lane; k < K; k += 32) sA[(m * K + k) * R + r] = a[k];
   }
   __syncthreads();
-  const int stride = nparts * (int)blockDim.x;
-  for (int t = tid + part * (int)blockDim.x; t < M * J; t += stride) {
+  for (int t = tid; t < M * J; t += blockDim.x) {
     const int m = t / J, j = t - m * J;
     const int k0 = P.tri ? m : 0;
     const float* b = B + (long long)m * P.sBm + (long long)j * K;
@@ -896,14 +895,11 @@ __device__ __forceinline__ void contract_rows(const LegProblem& P, long long gid
   }
 }
 
-// A capsule's rows of a problem; the tasks (m, j) are shared among nparts
-// CTAs (part = this CTA's share), each staging the whole A.
-__device__ __forceinline__ void contract_capsule(const LegProblem& P, long long gidx, float* sA, int part,
-                                                 int nparts) {
+__device__ __forceinline__ void contract_capsule(const LegProblem& P, long long gidx, float* sA) {
   switch (P.rpc) {
-    case 6: contract_rows<6>(P, gidx, sA, part, nparts); break;
-    case 8: contract_rows<8>(P, gidx, sA, part, nparts); break;
-    default: contract_rows<12>(P, gidx, sA, part, nparts); break;
+    case 6: contract_rows<6>(P, gidx, sA); break;
+    case 8: contract_rows<8>(P, gidx, sA); break;
+    default: contract_rows<12>(P, gidx, sA); break;
   }
 }
 
@@ -926,16 +922,16 @@ __global__ void __launch_bounds__(256, 2) force_fused_kernel(
     centroid_block(cap, caps, X, Y, Z, cen);
     __syncthreads();  // the centroid is written
     posfwd_item<float>(dealias, caps, groups, X, Y, Z, cen);
-    contract_capsule(pg[0], ci.gidx, sA, 0, 1);  // S0: analysis of the displacement
-    contract_capsule(pg[1], ci.gidx, sA, 0, 1);  // S1: P, dP, d2P series on the dealias grid
-    contract_capsule(pg[4], ci.gidx, sA, 0, 1);  // S3b: the shape on the SH grid
+    contract_capsule(pg[0], ci.gidx, sA);  // S0: analysis of the displacement
+    contract_capsule(pg[1], ci.gidx, sA);  // S1: P, dP, d2P series on the dealias grid
+    contract_capsule(pg[4], ci.gidx, sA);  // S3b: the shape on the SH grid
     membrane_item_f2(dealias, caps, groups, nullptr, nullptr);
-    contract_capsule(pg[2], ci.gidx, sA, 0, 1);  // S2: analysis of force and normals
-    contract_capsule(pg[3], ci.gidx, sA, 0, 1);  // S3a: the normals on the SH grid
-    contract_capsule(pg[6], ci.gidx, sA, 0, 1);  // S5a: the force on the force grid
+    contract_capsule(pg[2], ci.gidx, sA);  // S2: analysis of force and normals
+    contract_capsule(pg[3], ci.gidx, sA);  // S3a: the normals on the SH grid
+    contract_capsule(pg[6], ci.gidx, sA);  // S5a: the force on the force grid
     shgrid_item<float>(shgrid, caps, groups, nullptr);
-    contract_capsule(pg[5], ci.gidx, sA, 0, 1);  // S4: analysis of renormalised normals and surface metric
-    contract_capsule(pg[7], ci.gidx, sA, 0, 1);  // S5b: them on the force grid
+    contract_capsule(pg[5], ci.gidx, sA);  // S4: analysis of renormalised normals and surface metric
+    contract_capsule(pg[7], ci.gidx, sA);  // S5b: them on the force grid
     final_item<float>(dealias, caps, groups, FX, FY, FZ, NX, NY, NZ, AREA, frc, dvi, nullptr);
   }
 }
@@ -1015,7 +1011,7 @@ cudaError_t launch_posfwd(const RowWork* work, int nwork, const CapInfo* caps, c
   if (nwork <= 0 || ncap <= 0) return cudaSuccess;
   launch_pdl(centroid_kernel, dim3(ncap), dim3(256), 0, st, ncap, caps, X, Y, Z, cen);
   const size_t smem = pointwise_smem<T>(kPosfwd, nmax);
-  cudaError_t e = smem_limit_max(posfwd_kernel<T>);
+  cudaError_t e = smem_limit(posfwd_kernel<T>, smem);
   if (e != cudaSuccess) return e;
   launch_pdl(posfwd_kernel<T>, dim3(persistent_grid(posfwd_kernel<T>, smem, nwork)), dim3(kPointThreads), smem, st, 
       work, nwork, caps, groups, X, Y, Z, cen);
@@ -1028,13 +1024,13 @@ cudaError_t launch_membrane(const RowWork* work, int nwork, const CapInfo* caps,
   if (nwork <= 0) return cudaSuccess;
   if constexpr (sizeof(T) == 4) {
     const size_t smem = membrane_f2_smem(nmax);
-    cudaError_t e = smem_limit_max(membrane_kernel_f2);
+    cudaError_t e = smem_limit(membrane_kernel_f2, smem);
     if (e != cudaSuccess) return e;
     launch_pdl(membrane_kernel_f2, dim3(persistent_grid(membrane_kernel_f2, smem, nwork)), dim3(kPointThreads), smem, st, 
         work, nwork, caps, groups, sur_flag, err);
   } else {
     const size_t smem = pointwise_smem<T>(kMembrane, nmax);
-    cudaError_t e = smem_limit_max(membrane_kernel<T>);
+    cudaError_t e = smem_limit(membrane_kernel<T>, smem);
     if (e != cudaSuccess) return e;
     launch_pdl(membrane_kernel<T>, dim3(persistent_grid(membrane_kernel<T>, smem, nwork)), dim3(kPointThreads), smem, st, 
         work, nwork, caps, groups, sur_flag, err);
@@ -1047,7 +1043,7 @@ cudaError_t launch_shgrid(const RowWork* work, int nwork, const CapInfo* caps, c
                           int* err, cudaStream_t st) {
   if (nwork <= 0) return cudaSuccess;
   const size_t smem = pointwise_smem<T>(kShgrid, nmax);
-  cudaError_t e = smem_limit_max(shgrid_kernel<T>);
+  cudaError_t e = smem_limit(shgrid_kernel<T>, smem);
   if (e != cudaSuccess) return e;
   launch_pdl(shgrid_kernel<T>, dim3(persistent_grid(shgrid_kernel<T>, smem, nwork)), dim3(kPointThreads), smem, st, work, nwork, caps,
                                                                                                   groups, err);
@@ -1060,7 +1056,7 @@ cudaError_t launch_final(const RowWork* work, int nwork, const CapInfo* caps, co
                          cudaStream_t st) {
   if (nwork <= 0) return cudaSuccess;
   const size_t smem = pointwise_smem<T>(kFinal, nmax);
-  cudaError_t e = smem_limit_max(final_kernel<T>);
+  cudaError_t e = smem_limit(final_kernel<T>, smem);
   if (e != cudaSuccess) return e;
   launch_pdl(final_kernel<T>, dim3(persistent_grid(final_kernel<T>, smem, nwork)), dim3(kPointThreads), smem, st, 
       work, nwork, caps, groups, FX, FY, FZ, NX, NY, NZ, AREA, (ForceRec<T>*)frc, dvi, err);
@@ -1077,7 +1073,7 @@ cudaError_t launch_force_fused(const int* order, int ncap, const CapInfo* caps, 
                                double dvi, int nmax, size_t max_contract_floats, cudaStream_t st) {
   if (ncap <= 0) return cudaSuccess;
   const size_t smem = fused_force_smem(nmax, max_contract_floats);
-  cudaError_t e = smem_limit_max(force_fused_kernel);
+  cudaError_t e = smem_limit(force_fused_kernel, smem);
   if (e != cudaSuccess) return e;
   force_fused_kernel<<<persistent_grid(force_fused_kernel, smem, ncap), kPointThreads, smem, st>>>(
       order, ncap, caps, groups, probs, X, Y, Z, cen, FX, FY, FZ, NX, NY, NZ, AREA, (ForceRec<float>*)frc, dvi);

@@ -573,7 +573,7 @@ template <int TY, int TZ>
 static cudaError_t spread_rows(const IBGrid& g, const IBWork& w, float* ox, float* oy, float* oz, cudaStream_t st) {
   const size_t smem = rows_smem(g.itot, TY, TZ);
   if (!smem || g.TX != g.itot || g.TY != TY || g.TZ != TZ) return cudaErrorInvalidValue;
-  cudaError_t e = smem_limit_max(spread_rows_kernel<TY, TZ>);
+  cudaError_t e = smem_limit(spread_rows_kernel<TY, TZ>, smem);
   if (e != cudaSuccess) return e;
   launch_pdl(spread_rows_kernel<TY, TZ>, dim3(g.ntiles), dim3(256), smem, st, g, w.entries, w.starts, (const PosRec<float>*)w.pos,
                                                          (const ForceRec<float>*)w.frc, ox, oy, oz);
