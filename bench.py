@@ -45,6 +45,8 @@ def parse_args():
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--only", default=None, choices=["mixed", "fp64"],
                    help="time one path only, no e2e (for profiler captures)")
+    p.add_argument("--bending", action="store_true",
+                   help="with --only: the reference's default bending (ibend = 1, cbend = 0.3) on every capsule")
     p.add_argument("--cpu-sample-caps", type=int, default=64)
     p.add_argument("--no-surrogate", action="store_true", help="skip training and timing the surrogate path")
     p.add_argument("--tile", type=int, default=None, choices=[0, 1, 2, 3, 4, 5, 6],
@@ -293,6 +295,8 @@ def run_ours(args):
 
     if args.only:
         cs = make_cs(args.only)
+        if args.bending:
+            cs.set_capsule_bending(0.3 * wl.gs * wl.radius**2)
         r = time_path(cs, args.only)
         cs.close()
         if rank == 0:

@@ -299,7 +299,7 @@ __device__ void bend_q(const Geo<T>& G, const BendT<T>& B, T R, T st, T ct, T eb
 constexpr int kBK = 30;
 
 template <class T>
-__global__ void __launch_bounds__(256) membrane_bend_kernel(const RowWork* __restrict__ work, int nwork,
+__global__ void __launch_bounds__(256, sizeof(T) == 4 ? 2 : 1) membrane_bend_kernel(const RowWork* __restrict__ work, int nwork,
                                                             const CapInfo* __restrict__ caps,
                                                             const GroupDev* __restrict__ groups,
                                                             const int* __restrict__ sur_flag) {
@@ -317,7 +317,8 @@ __global__ void __launch_bounds__(256) membrane_bend_kernel(const RowWork* __res
     const int SR = N * kBK + 2;
     T* sG = (T*)smem_raw;               // [RP][SR]
     T* sTrig = sG + RP * SR;            // [2N][mD]: cos m phi_j (rows m), sin (rows N + m)
-    T* sOut = sTrig + 2 * N * mD;       // [RP][6][mD]
+    T* sTrigT = sTrig + 2 * N * mD;     // [mD][2N]: the same, transposed for the forward DFT
+    T* sOut = sTrigT + 2 * N * mD;      // [RP][6][mD]
     int* sOff = (int*)(sOut + RP * 6 * mD);  // [30N]: staged offsets of G's then GB's elements
     const T* Gs = (const T*)gd.buf.G + (long long)ci.gidx * (18 * N * nD);   // [ccs][m][kind][lat]
     const T* Gb = (const T*)gd.buf.GB + (long long)ci.gidx * (12 * N * nD);  // [ccs][m][kind][lat]
@@ -328,6 +329,7 @@ __global__ void __launch_bounds__(256) membrane_bend_kernel(const RowWork* __res
     const T R = (T)ci.R;
     __syncthreads();  // the previous item's reads of shared memory are done
     for (int q = tid; q < 2 * N * mD; q += blockDim.x) sTrig[q] = trig[q];
+    for (int q = tid; q < 2 * N * mD; q += blockDim.x) sTrigT[q] = trig[(q % (2 * N)) * mD + q / (2 * N)];
     for (int e = tid; e < 18 * N; e += blockDim.x) {  // e = (ccs N + m) 3 + kind
       const int kind = e % 3, cm_ = e / 3, m = cm_ % N, ccs = cm_ / N;
       sOff[e] = m * kBK + 3 * ccs + kind;
@@ -450,14 +452,16 @@ __global__ void __launch_bounds__(256) membrane_bend_kernel(const RowWork* __res
       }
       __syncthreads();
       // forward DFT (shagc.f:364-380) of the six outputs per row: warp = (row,
-      // field) line, lane p < 2N = cos m = p, sin m = p - N
+      // field) line, lane p < 2N = cos m = p, sin m = p - N; the lanes read
+      // consecutive words of the transposed table (no bank conflicts) and the
+      // row's value as a broadcast
       for (int line = warp; line < rows * 6; line += nwarp) {
         const int fld = line % 6, rr = line / 6;
         const T* o = sOut + line * mD;
         for (int p = lane; p < 2 * N; p += 32) {
-          const T* t = sTrig + p * mD;
+          const T* t = sTrigT + p;
           T a = 0;
-          for (int jj = 0; jj < mD; ++jj) a += o[jj] * t[jj];
+          for (int jj = 0; jj < mD; ++jj) a += o[jj] * t[jj * 2 * N];
           Fout[((long long)fld * 2 * N + p) * nD + rb + rr] = (p < N ? sfn : -sfn) * a;
         }
       }
@@ -474,7 +478,7 @@ cudaError_t launch_membrane_bend(const RowWork* work, int nwork, const CapInfo* 
   size_t e = 0;  // shared memory (elements of T) over the degrees up to nmax
   for (size_t n = 1; n <= (size_t)nmax; ++n) {
     const size_t mD = 4 * n, RP = 256 / mD > 0 ? 256 / mD : 1;
-    const size_t en = RP * (n * kBK + 2) + 2 * n * mD + RP * 6 * mD + (30 * n * sizeof(int) + sizeof(T) - 1) / sizeof(T) + 8;
+    const size_t en = RP * (n * kBK + 2) + 4 * n * mD + RP * 6 * mD + (30 * n * sizeof(int) + sizeof(T) - 1) / sizeof(T) + 8;
     e = std::max(e, en);
   }
   const size_t smem = sizeof(T) * e;
