@@ -455,14 +455,21 @@ __global__ void __launch_bounds__(256, sizeof(T) == 4 ? 2 : 1) membrane_bend_ker
       // field) line, lane p < 2N = cos m = p, sin m = p - N; the lanes read
       // consecutive words of the transposed table (no bank conflicts) and the
       // row's value as a broadcast
-      for (int line = warp; line < rows * 6; line += nwarp) {
-        const int fld = line % 6, rr = line / 6;
-        const T* o = sOut + line * mD;
+      // (row, field triple) line per warp: one load of the trig value serves
+      // the triple's three fields (force or normal)
+      for (int line = warp; line < rows * 2; line += nwarp) {
+        const int f0 = 3 * (line & 1), rr = line >> 1;
+        const T* o = sOut + (rr * 6 + f0) * mD;
         for (int p = lane; p < 2 * N; p += 32) {
           const T* t = sTrigT + p;
-          T a = 0;
-          for (int jj = 0; jj < mD; ++jj) a += o[jj] * t[jj * 2 * N];
-          Fout[((long long)fld * 2 * N + p) * nD + rb + rr] = (p < N ? sfn : -sfn) * a;
+          T a[3] = {T(0), T(0), T(0)};
+          for (int jj = 0; jj < mD; ++jj) {
+            const T tt = t[jj * 2 * N];
+#pragma unroll
+            for (int f = 0; f < 3; ++f) a[f] += o[f * mD + jj] * tt;
+          }
+#pragma unroll
+          for (int f = 0; f < 3; ++f) Fout[((long long)(f0 + f) * 2 * N + p) * nD + rb + rr] = (p < N ? sfn : -sfn) * a[f];
         }
       }
     }

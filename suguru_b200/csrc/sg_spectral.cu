@@ -177,16 +177,22 @@ __device__ __forceinline__ void posfwd_item(const RowWork it,
       const T sfn = T(2) / T(mD);
       // lane p < 2N: trig row p (cos m = p, then sin m = p - N); rows of
       // Fpos are (comp, cos/sin, m), so the output row is c 2N + p
-      for (int line = warp; line < rows * 3; line += nwarp) {
-        const int c = line % 3, r = line / 3;
-        const T* o = sd + (r * 3 + c) * lP;
+      // one warp per row: one load of the lane's trig value serves the three
+      // components
+      for (int r = warp; r < rows; r += nwarp) {
+        const T* o = sd + r * 3 * lP;
         for (int p = lane; p < 2 * N; p += 32) {
           const int m = p < N ? p : p - N;
           const T* oo = o + ((m & 1) ? hP : 0);
           const T* t = sTrig + p * hP;
-          T a = 0;
-          for (int j = 0; j < H; ++j) a += oo[j] * t[j];
-          Fpos[(long long)(c * 2 * N + p) * nD + rb + r] = (p < N ? sfn : -sfn) * a;
+          T a[3] = {T(0), T(0), T(0)};
+          for (int j = 0; j < H; ++j) {
+            const T tt = t[j];
+#pragma unroll
+            for (int c = 0; c < 3; ++c) a[c] += oo[c * lP + j] * tt;
+          }
+#pragma unroll
+          for (int c = 0; c < 3; ++c) Fpos[(long long)(c * 2 * N + p) * nD + rb + r] = (p < N ? sfn : -sfn) * a[c];
         }
       }
     }
@@ -536,19 +542,26 @@ __device__ __forceinline__ void membrane_item_f2(const RowWork it,
         }
       }
       __syncthreads();
-      // forward DFT of the six outputs per row: warp = (row, field) line, lane
-      // p < 2N = trig row p (cos m = p, sin m = p - N); even and odd j summed
-      // as a pair
-      for (int line = warp; line < rows * 6; line += nwarp) {
-        const int f = line % 6, rr = line / 6;
-        const float* o = sOut + line * OS;
+      // forward DFT of the six outputs per row: warp = (row, field triple)
+      // line, lane p < 2N = trig row p (cos m = p, sin m = p - N); even and
+      // odd j summed as a pair; one load of the lane's trig pair serves the
+      // triple's three fields (force or normal)
+      for (int line = warp; line < rows * 2; line += nwarp) {
+        const int f0 = 3 * (line & 1), rr = line >> 1;
+        const float* o = sOut + (rr * 6 + f0) * OS;
         for (int p = lane; p < 2 * N; p += 32) {
           const int m = p < N ? p : p - N;
           const float2* oo = (const float2*)(o + ((m & 1) ? H + 2 : 0));
           const float2* t = (const float2*)(sTrig + p * TS);
-          float2 a2 = make_float2(0.0f, 0.0f);
-          for (int jj = 0; jj < (H >> 1); ++jj) a2 = p2fma(oo[jj], t[jj], a2);
-          Fout[((long long)f * 2 * N + p) * nD + rb + rr] = (p < N ? sfn : -sfn) * (a2.x + a2.y);
+          float2 a2[3] = {make_float2(0.0f, 0.0f), make_float2(0.0f, 0.0f), make_float2(0.0f, 0.0f)};
+          for (int jj = 0; jj < (H >> 1); ++jj) {
+            const float2 tt = t[jj];
+#pragma unroll
+            for (int f = 0; f < 3; ++f) a2[f] = p2fma(oo[f * (OS >> 1) + jj], tt, a2[f]);
+          }
+#pragma unroll
+          for (int f = 0; f < 3; ++f)
+            Fout[((long long)(f0 + f) * 2 * N + p) * nD + rb + rr] = (p < N ? sfn : -sfn) * (a2[f].x + a2[f].y);
         }
       }
     }
@@ -704,16 +717,23 @@ __device__ __forceinline__ void shgrid_item(const RowWork it,
         }
       }
       __syncthreads();
-      for (int line = warp; line < rows * 4; line += nwarp) {
-        const int f = line % 4, rr = line / 4;
-        const T* o = sOut + line * lP;
+      // (row, field pair) line per warp: one load of the lane's trig value
+      // serves two fields
+      for (int line = warp; line < rows * 2; line += nwarp) {
+        const int f0 = 2 * (line & 1), rr = line >> 1;
+        const T* o = sOut + (rr * 4 + f0) * lP;
         for (int p = lane; p < 2 * N; p += 32) {
           const int m = p < N ? p : p - N;
           const T* oo = o + ((m & 1) ? hP : 0);
           const T* t = sTrig + p * hP;
-          T a = 0;
-          for (int jj = 0; jj < H; ++jj) a += oo[jj] * t[jj];
-          Fsh[((long long)f * 2 * N + p) * nO + rb + rr] = (p < N ? sfn : -sfn) * a;
+          T a[2] = {T(0), T(0)};
+          for (int jj = 0; jj < H; ++jj) {
+            const T tt = t[jj];
+            a[0] += oo[jj] * tt;
+            a[1] += oo[lP + jj] * tt;
+          }
+#pragma unroll
+          for (int f = 0; f < 2; ++f) Fsh[((long long)(f0 + f) * 2 * N + p) * nO + rb + rr] = (p < N ? sfn : -sfn) * a[f];
         }
       }
     }
