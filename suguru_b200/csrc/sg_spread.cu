@@ -234,9 +234,13 @@ __global__ void __launch_bounds__(256, sizeof(T) == 4 ? 4 : 2) spread_kernel(IBG
   constexpr int NW = Fixed<T>::NW;
   constexpr int CPT = (NC + 255) / 256;  // cells per thread in the fold / write loops
   constexpr int NT = F32 ? 1 : CPT;      // FP64 keeps running 64-bit totals
-  // per (limb, component): NC cells and 32 per-lane trash words that take the
-  // contributions falling outside the tile, so that the walk has no branches
-  constexpr int NCP = NC + 32;
+  // per (limb, component): the cells, rows padded by one word (row stride
+  // RS = TX + 1, plane stride PS), so that lanes whose points sit at the same
+  // x in different rows or planes add to different banks, and 32 per-lane
+  // trash words that take the contributions falling outside the tile, so
+  // that the walk has no branches
+  constexpr int RS = TX + 1, PS = RS * TY, NCS = PS * TZ;
+  constexpr int NCP = NCS + 32;
   __shared__ __align__(16) unsigned int acc[NW][3][NCP];
   __shared__ T s_red[3][8];
   __shared__ unsigned long long s_sum[3][8];
@@ -300,10 +304,10 @@ __global__ void __launch_bounds__(256, sizeof(T) == 4 ? 4 : 2) spread_kernel(IBG
               lc[t] = (a >= 0 && a < cw) ? a : kOut;
             } else if (d == 1) {
               const int b = wrap_near(bb[1] + t - 1, g.jtot) - j0;
-              lc[t] = (b >= 0 && b < ch) ? TX * b : kOut;
+              lc[t] = (b >= 0 && b < ch) ? RS * b : kOut;
             } else {
               const int kk = bb[2] + t - 1;
-              lc[t] = (kk - k0 >= 0 && kk - k0 < cd && kk >= 1 && kk <= g.ktot) ? TX * TY * (kk - k0) : kOut;
+              lc[t] = (kk - k0 >= 0 && kk - k0 < cd && kk >= 1 && kk <= g.ktot) ? PS * (kk - k0) : kOut;
             }
           }
 #pragma unroll
@@ -315,7 +319,7 @@ __global__ void __launch_bounds__(256, sizeof(T) == 4 ? 4 : 2) spread_kernel(IBG
         // component c has face weights along dimension c, centre weights along
         // the others.  A cell outside the tile has a negative offset sum (kOut
         // in at least one dimension) and goes to this lane's trash word.
-        const int trash = NC + lane;
+        const int trash = NCS + lane;
 #pragma unroll
         for (int c = 0; c < 3; ++c) {
 #pragma unroll
@@ -330,7 +334,7 @@ __global__ void __launch_bounds__(256, sizeof(T) == 4 ? 4 : 2) spread_kernel(IBG
               for (int ix = 0; ix < 3; ++ix) {
                 const int cell = cyz + ((!CTR && c == 0) ? lcF[0][ix] : lcC[0][ix]);
                 const T wx = (!CTR && c == 0) ? wF[0][ix] : wC[0][ix];
-                // valid cells are below NC, the negative ones wrap above it
+                // valid cells are below NCS, the negative ones wrap above it
                 const unsigned slot = min((unsigned)cell, (unsigned)trash);
                 if constexpr (F32) {
                   const float t = fmaf(pyz, wx, kMagic);  // round(pyz * wx) in the low mantissa bits
@@ -350,11 +354,12 @@ __global__ void __launch_bounds__(256, sizeof(T) == 4 ? 4 : 2) spread_kernel(IBG
         for (int r = 0; r < NT; ++r) {
           const int q = tid + 256 * r;
           if (q < NC) {
+            const int sq = q % TX + RS * ((q / TX) % TY) + PS * (q / (TX * TY));  // padded slot
 #pragma unroll
             for (int c = 0; c < 3; ++c) {
-              tot[r][c] += Fixed<double>::fold(&acc[0][c][q], 3 * NCP);
+              tot[r][c] += Fixed<double>::fold(&acc[0][c][sq], 3 * NCP);
 #pragma unroll
-              for (int w = 0; w < NW; ++w) acc[w][c][q] = 0u;
+              for (int w = 0; w < NW; ++w) acc[w][c][sq] = 0u;
             }
           }
         }
@@ -378,9 +383,10 @@ __global__ void __launch_bounds__(256, sizeof(T) == 4 ? 4 : 2) spread_kernel(IBG
     if (e1 > e0) {
       if constexpr (F32) {
         // one rounding of the fixed-point value; each iscale is a power of two
-        vu = (float)(int)acc[0][0][q] * iscale[0];
-        vv = (float)(int)acc[0][1][q] * iscale[1];
-        vw = (float)(int)acc[0][2][q] * iscale[2];
+        const int sq = lx + RS * ly + PS * lz;
+        vu = (float)(int)acc[0][0][sq] * iscale[0];
+        vv = (float)(int)acc[0][1][sq] * iscale[1];
+        vw = (float)(int)acc[0][2][sq] * iscale[2];
       } else {
         vu = (double)tot[r][0] * iscale[0];
         vv = (double)tot[r][1] * iscale[1];
