@@ -480,8 +480,8 @@ __device__ __forceinline__ void dft_reg(double2* v, int sign) {
 // consecutive 16-byte values.  Tables of a length's passes lie one after the
 // other: 32: 24 values; 64: 56; 128: 24 + 96; 256: 56 + 192.
 template <int N> struct TwTab;
-template <> struct TwTab<32> { static constexpr int size = 24, off2 = 0, off3 = 0; };
-template <> struct TwTab<64> { static constexpr int size = 56, off2 = 0, off3 = 0; };
+template <> struct TwTab<32> { static constexpr int size = 24; };
+template <> struct TwTab<64> { static constexpr int size = 56; };
 template <> struct TwTab<128> { static constexpr int size = 120, off2 = 0, off3 = 24; };
 template <> struct TwTab<256> { static constexpr int size = 248, off2 = 0, off3 = 56; };
 

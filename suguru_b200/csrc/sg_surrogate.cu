@@ -18,7 +18,6 @@ namespace sg {
 
 namespace {
 
-__device__ __forceinline__ float gelu_f(float x) { return 0.5f * x * (1.f + erff(x * 0.70710678118654752f)); }
 // d/dx GELU = Phi(x) + x phi(x)
 __device__ __forceinline__ float gelu_grad(float x) {
   const float Phi = 0.5f * (1.f + erff(x * 0.70710678118654752f));
