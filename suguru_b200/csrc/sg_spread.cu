@@ -33,7 +33,8 @@
 //    The fixed-point step is 2^-22 of 0.3 times the component's largest
 //    contribution, below FP32 rounding of a typical cell value.
 //  - FP64: 64-bit fixed point (|sum| < 2^56 from the component's largest
-//    contribution in the tile times its entry count) kept as three limbs of 19 bits, the
+//    contribution in the tile times its entry count, or above 4096 entries
+//    from 0.3 * the same exact integer sum of m_c as FP32 takes) kept as three limbs of 19 bits, the
 //    lower two unsigned, so that the atomics stay native 32-bit adds; with at
 //    most 4096 contributions per pass no limb can overflow, and between passes
 //    the limbs are folded into 64-bit registers.
@@ -145,20 +146,25 @@ __device__ __forceinline__ void tile_scales(int e0, int e1, const int* __restric
     int sh[3];
 #pragma unroll
     for (int c = 0; c < 3; ++c) sh[c] = QB - exp_above((double)rmax[c] * (double)(F32 ? 0.3 * cnt : cnt));
-    if constexpr (F32) {
-      // every single contribution below 2^22 ...
-      int sh1[3];
-      bool dense = false;
+    // FP32: every single contribution below 2^22 ...
+    int sh1[3] = {QB, QB, QB};
+    bool need[3] = {false, false, false}, dense = false;
 #pragma unroll
-      for (int c = 0; c < 3; ++c) {
+    for (int c = 0; c < 3; ++c) {
+      if constexpr (F32) {
         sh1[c] = 22 - exp_above(0.3 * (double)rmax[c]);
-        dense = dense || sh[c] < sh1[c];
+        need[c] = sh[c] < sh1[c];
+      } else {
+        need[c] = cnt > MAXC;  // FP64: the count bound costs precision above one pass of entries
       }
+      dense = dense || need[c];
+    }
+    {
       if (dense) {  // uniform across the CTA: computed from the block-wide maxima
         // ... and, where the count bound would cost precision (more than 2^8
-        // entries), |sum| < 2^30 from 0.3 * sum of m_c, taken as an exact
+        // entries), |sum| < 2^QB from 0.3 * sum of m_c, taken as an exact
         // integer sum of m_c rounded up to multiples of 2^-12 of the largest
-        // m_c's binade
+        // m_c's binade (every 3-D weight is below 0.3)
         int exr[3];
         double u[3];
         unsigned long long sm[3] = {0ull, 0ull, 0ull};
@@ -188,11 +194,12 @@ __device__ __forceinline__ void tile_scales(int e0, int e1, const int* __restric
           unsigned long long t = 0;
 #pragma unroll
           for (int q = 0; q < 8; ++q) t += s_sum[c][q];
-          if (sh[c] < sh1[c]) sh[c] = QB - exp_above(0.3 * ((double)t * pow2<double>(exr[c] - 12)));
+          if (need[c]) sh[c] = QB - exp_above(0.3 * ((double)t * pow2<double>(exr[c] - 12)));
         }
       }
+      if constexpr (F32)
 #pragma unroll
-      for (int c = 0; c < 3; ++c) sh[c] = min(sh[c], sh1[c]);
+        for (int c = 0; c < 3; ++c) sh[c] = min(sh[c], sh1[c]);
     }
 #pragma unroll
     for (int c = 0; c < 3; ++c) {

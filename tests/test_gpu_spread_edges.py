@@ -120,3 +120,32 @@ def test_row_tiles(cuda, grid, shape):
         assert torch.equal(s_, g2)
         assert rel_l2(s_.cpu().numpy(), r) <= 1e-4
 
+
+
+@pytest.mark.parametrize("precision", ["fp64", "mixed"])
+def test_dense_tiles(cuda, precision):
+    # 24,576 points inside a box of 2 x 2 x 2 cells, so that a handful of
+    # tiles hold up to 24,576 entries each: the FP64 limbs are folded over
+    # several passes of 4,096 contributions, and the FP32 scales take the
+    # exact integer sum bound of dense tiles; forces of mixed magnitudes
+    dx = 1.0 / 16
+    grid = (64, 48, 40, dx, dx, dx)
+    degree = np.array([31, 31, 31], np.int32)  # 8 (L + 1)^2 = 8192 points each
+    radius = np.full(3, 0.25)
+    n = int(np.sum(8 * (degree + 1) ** 2))
+    rng = np.random.default_rng(37)
+    x = (20.3 + rng.uniform(0.0, 2.0, n)) * dx
+    y = (10.2 + rng.uniform(0.0, 2.0, n)) * dx
+    z = (17.6 + rng.uniform(0.0, 2.0, n)) * dx
+    f = rng.normal(size=(3, n)) * rng.choice([1e-3, 1.0, 30.0], size=(3, n))
+    a = rng.uniform(0.5, 1.5, n) * dx**2
+    ref = O.spread(grid, x, y, z, f[0], f[1], f[2], a)
+    cs = CouplingStep(grid, degree, radius, precision=precision)
+    dt = np.float64 if precision == "fp64" else np.float32
+    tol = 1e-12 if precision == "fp64" else 1e-4
+    args = (x, y, z, *(v.astype(dt) for v in f), a.astype(dt))
+    got = [g.copy() for g in cs.lagr2eulr(*args)]
+    again = cs.lagr2eulr(*args)
+    for g, g2, r in zip(got, again, ref):
+        assert np.array_equal(g, g2)
+        assert rel_l2(g, r) <= tol
