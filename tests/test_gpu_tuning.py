@@ -153,3 +153,38 @@ def test_legendre_tile_rows_do_not_change_results(cuda):
     assert np.array_equal(a["area"], b["area"])
     with pytest.raises(SgError):
         cs.set_legendre_tile_rows(96)
+
+
+@pytest.mark.parametrize("precision", ["fp64", "mixed"])
+def test_graph_replay_with_bending_and_collisions(cuda, precision):
+    # the captured step with every optional stage on: bending moduli (the
+    # extra contraction launch and the bending membrane kernel) and the wall
+    # force inside the step, capsules moved next to the bottom wall; the
+    # replay gives the eager step's bits
+    torch = cuda
+    wl = W.small_config(ncap=3, seed=23, degrees=(7, 16, 11))
+    dt = torch.float64 if precision == "fp64" else torch.float32
+    dev = lambda a, t=dt: torch.from_numpy(np.ascontiguousarray(a)).to("cuda", t)
+    st = torch.cuda.Stream()
+    cs = CouplingStep(wl.grid, wl.degree, wl.radius, wl.gs, wl.csk, precision=precision, mem="device",
+                      stream=st.cuda_stream)
+    cs.set_capsule_bending(0.3 * wl.gs * wl.radius**2)
+    cs.set_wall_collisions(in_step=True)
+    z = wl.z - wl.z.min() + 0.5 * wl.grid[5]  # the lowest point half a cell above the wall
+    u, v, w = (dev(x) for x in wl.velocity())
+    X, Y, Z = (dev(x, torch.float64) for x in (wl.x, wl.y, z))
+    lag = [torch.zeros(wl.npts, dtype=dt, device="cuda") for _ in range(10)]
+    eul = [torch.zeros_like(u) for _ in range(3)]
+    torch.cuda.synchronize()
+    cs.step(u, v, w, X, Y, Z, lag_out=lag, eul_out=eul)
+    torch.cuda.synchronize()
+    want = [t.clone() for t in lag + eul]
+    cs.graph_capture(u, v, w, X, Y, Z, lag, eul)
+    for t in lag + eul:
+        t.fill_(float("nan"))
+    torch.cuda.synchronize()
+    cs.graph_launch()
+    torch.cuda.synchronize()
+    for a, b in zip(lag + eul, want):
+        assert torch.equal(a, b)
+    cs.graph_release()
